@@ -1,0 +1,97 @@
+"""ctypes front end to the CPU restatement oracle (oracle/pdfxc_oracle.c).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg as the checker. Never used by the product path.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "libpdfxc_oracle.so")
+
+FUNCTIONALS = {"SVWN": 0, "HFS": 1, "HFB": 2, "BLYP": 3, "B88LYP": 3, "B3LYP": 4}
+GGA = {"HFB", "BLYP", "B88LYP", "B3LYP"}
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            import subprocess
+            subprocess.run(["make", "-C", HERE, "-s"], check=True)
+        _lib = ctypes.CDLL(LIB_PATH)
+    return _lib
+
+
+def _p(a, dt):
+    return np.ascontiguousarray(a, dtype=dt).ctypes.data_as(ctypes.c_void_p)
+
+
+def functional(name, ra, rb, gaa, gab, gbb):
+    """Vectorised over numpy inputs; returns (n, 6): f, vA, vB, vgAA, vgAB, vgBB."""
+    L = lib()
+    arr = np.broadcast_arrays(*(np.asarray(v, dtype=np.float64) for v in (ra, rb, gaa, gab, gbb)))
+    flat = [a.ravel() for a in arr]
+    out = np.zeros((len(flat[0]), 6))
+    o = np.zeros(6)
+    for i in range(len(flat[0])):
+        L.pdfxc_oracle_functional(ctypes.c_int(FUNCTIONALS[name]), *(ctypes.c_double(float(f[i])) for f in flat),
+                                  o.ctypes.data_as(ctypes.c_void_p))
+        out[i] = o
+    return out
+
+
+def _shell_args(sh):
+    keep = [np.ascontiguousarray(sh.shell_atom, np.int32), np.ascontiguousarray(sh.shell_l, np.int32),
+            np.ascontiguousarray(sh.shell_ao0, np.int32), np.ascontiguousarray(sh.shell_nprim, np.int32),
+            np.ascontiguousarray(sh.shell_p0, np.int32), np.ascontiguousarray(sh.prim_exp, np.float64),
+            np.ascontiguousarray(sh.prim_coef, np.float64), np.ascontiguousarray(sh.atom_xyz, np.float64)]
+    return keep, [k.ctypes.data_as(ctypes.c_void_p) for k in keep]
+
+
+def aos(sh, xyz):
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    n = len(xyz)
+    phi = np.zeros((n, sh.nao))
+    dphi = np.zeros((n, sh.nao, 3))
+    keep, args = _shell_args(sh)
+    lib().pdfxc_oracle_aos(ctypes.c_int(sh.nshell), ctypes.c_int(sh.nao), *args, ctypes.c_long(n),
+                           xyz.ctypes.data_as(ctypes.c_void_p), phi.ctypes.data_as(ctypes.c_void_p),
+                           dphi.ctypes.data_as(ctypes.c_void_p))
+    return phi, dphi
+
+
+def xc(name, sh, xyzw, PA, rho_cut=1e-16, threads=0):
+    """Returns dict(exc, nelec_alpha, vxc, rho)."""
+    xyzw = np.ascontiguousarray(xyzw, dtype=np.float64).reshape(-1, 4)
+    PA = np.ascontiguousarray(PA, dtype=np.float64)
+    n = len(xyzw)
+    gga = name in GGA
+    vxc = np.zeros((sh.nao, sh.nao))
+    rho = np.zeros((n, 4 if gga else 1))
+    exc = ctypes.c_double()
+    nel = ctypes.c_double()
+    keep, args = _shell_args(sh)
+    lib().pdfxc_oracle_xc(ctypes.c_int(FUNCTIONALS[name]), ctypes.c_int(sh.nshell), ctypes.c_int(sh.nao), *args,
+                          ctypes.c_long(n), xyzw.ctypes.data_as(ctypes.c_void_p), PA.ctypes.data_as(ctypes.c_void_p),
+                          ctypes.c_double(rho_cut), ctypes.byref(exc), ctypes.byref(nel),
+                          vxc.ctypes.data_as(ctypes.c_void_p), rho.ctypes.data_as(ctypes.c_void_p),
+                          ctypes.c_int(threads))
+    return {"exc": exc.value, "nelec_alpha": nel.value, "vxc": vxc, "rho": rho}
+
+
+def becke(atom_xyz, brad, xyz, owner, size_adjust=True):
+    atom_xyz = np.ascontiguousarray(atom_xyz, dtype=np.float64)
+    brad = np.ascontiguousarray(brad, dtype=np.float64)
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    owner = np.ascontiguousarray(owner, dtype=np.int32)
+    fac = np.zeros(len(xyz))
+    lib().pdfxc_oracle_becke(ctypes.c_int(len(atom_xyz)), atom_xyz.ctypes.data_as(ctypes.c_void_p),
+                             brad.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(int(size_adjust)),
+                             ctypes.c_long(len(xyz)), xyz.ctypes.data_as(ctypes.c_void_p),
+                             owner.ctypes.data_as(ctypes.c_void_p), fac.ctypes.data_as(ctypes.c_void_p))
+    return fac

@@ -1,0 +1,454 @@
+// Reference-oracle harness: drives ProteinDF's own DfCalcGridX, DfGenerateGrid
+// and DfFunctional_* objects (compiled unmodified from the reference tree by
+// oracle/ref/Makefile) on inputs written by the Python test tooling, and
+// writes their outputs to a flat binary file.
+//
+// TEST INFRASTRUCTURE ONLY: this program is the checker that pins the CPU
+// restatement (oracle/pdfxc_oracle.c) and the CUDA path, and the timed
+// "reference" CPU baseline. Nothing in the product links or runs it.
+//
+// Modes
+//   pdfxc_ref xc    <case.txt> <out.bin>   rho pass + Vxc pass of DfCalcGridX
+//   pdfxc_ref grid  <case.txt> <out.bin>   atom-centred grid + Becke weights
+//   pdfxc_ref func  <case.txt> <out.bin>   pointwise functional values
+//   pdfxc_ref lebedev - <out.bin>          unit-sphere Lebedev tables
+//
+// The XC mode follows DfCalcGridX::calcXCIntegForFockAndEnergy
+// (src/libpdf/DfCalcGridX.cpp:2280-2315): calcRho_{LDA,GGA}_part (:1862-1962)
+// on a grid matrix with xc-update = no, then buildVxc(gridMatrix, ...)
+// (:2056-2193). The grid mode calls the same private members that
+// DfGenerateGrid::generateGrid_atom (src/libpdf/DfGenerateGrid.cpp:934-1091)
+// calls, shell by shell, so that single-centre and partition weights can be
+// recorded separately.
+#include <omp.h>
+
+#include <chrono>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <iostream>
+#include <map>
+#include <sstream>
+#include <string>
+#include <vector>
+
+#include "DfCalcGridX.h"
+#define private public
+#define protected public
+#include "DfGenerateGrid.h"
+#undef private
+#undef protected
+#include "DfFunctional_B3LYP.h"
+#include "DfFunctional_B88LYP.h"
+#include "DfFunctional_Becke88.h"
+#include "DfFunctional_HFS.h"
+#include "DfFunctional_SVWN.h"
+#include "TlLebedevGrid.h"
+#include "TlPrdctbl.h"
+
+namespace {
+
+struct Case {
+    std::map<std::string, std::string> kv;
+    std::vector<std::string> atomSym;
+    std::vector<double> atomCharge, atomXyz;
+    // basis: element -> list of (shell, [(exp, coef)])
+    std::map<std::string, std::vector<std::pair<char, std::vector<std::pair<double, double>>>>> basis;
+    std::vector<std::string> basisOrder;
+
+    std::string get(const std::string& k, const std::string& dflt = "") const {
+        auto it = kv.find(k);
+        return it == kv.end() ? dflt : it->second;
+    }
+};
+
+Case readCase(const char* path) {
+    Case c;
+    std::ifstream in(path);
+    if (!in) {
+        std::fprintf(stderr, "cannot open %s\n", path);
+        std::exit(2);
+    }
+    std::string line;
+    while (std::getline(in, line)) {
+        std::istringstream ss(line);
+        std::string key;
+        if (!(ss >> key) || key[0] == '#') continue;
+        if (key == "atom") {
+            std::string sym;
+            double q, x, y, z;
+            ss >> sym >> q >> x >> y >> z;
+            c.atomSym.push_back(sym);
+            c.atomCharge.push_back(q);
+            c.atomXyz.insert(c.atomXyz.end(), {x, y, z});
+        } else if (key == "cgto") {
+            std::string el, shell;
+            int nprim;
+            ss >> el >> shell >> nprim;
+            std::vector<std::pair<double, double>> prims(nprim);
+            for (int i = 0; i < nprim; ++i) {
+                std::getline(in, line);
+                std::istringstream ps(line);
+                ps >> prims[i].first >> prims[i].second;
+            }
+            if (!c.basis.count(el)) c.basisOrder.push_back(el);
+            c.basis[el].push_back({shell[0], prims});
+        } else {
+            std::string rest;
+            std::getline(ss, rest);
+            const auto p = rest.find_first_not_of(' ');
+            c.kv[key] = (p == std::string::npos) ? "" : rest.substr(p);
+        }
+    }
+    return c;
+}
+
+TlSerializeData makeParam(const Case& c) {
+    TlSerializeData p;
+    p["method"] = "rks";
+    p["guess"] = "core";
+    p["K_engine"] = "conventional";
+    p["XC_engine"] = "grid";
+    p["xc_functional"] = c.get("functional", "SVWN");
+    p["xc-update"] = "no";
+    p["num_of_iterations"] = 1;
+    p["num_of_atoms"] = (int)c.atomSym.size();
+    p["xc-potential/grid-type"] = c.get("grid_type", "USER");
+    p["grid/num_of_radial_shells"] = c.get("nrad", "75");
+    p["grid/num_of_angular_points"] = c.get("nang", "302");
+    p["grid/radial_quadorature_method"] = c.get("radial", "GC");
+    p["grid/GC_mapping_type"] = c.get("gc_mapping", "TA");
+    p["grid/partitioning_method"] = c.get("partition", "Becke");
+    p["grid/pruning"] = c.get("pruning", "yes");
+    TlSerializeData atoms;
+    for (size_t i = 0; i < c.atomSym.size(); ++i) {
+        TlSerializeData a;
+        a["symbol"] = c.atomSym[i];
+        a["label"] = "";
+        a["charge"] = c.atomCharge[i];
+        TlSerializeData xyz;
+        for (int k = 0; k < 3; ++k) xyz.pushBack(c.atomXyz[3 * i + k]);
+        a["xyz"] = xyz;
+        atoms.pushBack(a);
+    }
+    p["coordinates"]["atoms"] = atoms;
+    for (const auto& el : c.basisOrder) {
+        TlSerializeData b;
+        b["name"] = "basis-" + el;
+        TlSerializeData cgtos;
+        for (const auto& sh : c.basis.at(el)) {
+            TlSerializeData cg;
+            cg["scale_factor"] = 1.0;
+            cg["shell_type"] = std::string(1, sh.first);
+            TlSerializeData prims;
+            for (const auto& pr : sh.second) {
+                TlSerializeData pg;
+                pg["exp"] = pr.first;
+                pg["coef"] = pr.second;
+                prims.pushBack(pg);
+            }
+            cg["pGTOs"] = prims;
+            cgtos.pushBack(cg);
+        }
+        b["cGTOs"] = cgtos;
+        p["basis_set"][el] = b;
+        p["basis_set_j"][el] = b;  // only to satisfy auxiliary-basis lookups
+        p["basis_set_xc"][el] = b;
+    }
+    return p;
+}
+
+std::vector<double> readDoubles(const std::string& path, size_t n) {
+    std::vector<double> v(n);
+    FILE* f = std::fopen(path.c_str(), "rb");
+    if (!f || std::fread(v.data(), sizeof(double), n, f) != n) {
+        std::fprintf(stderr, "cannot read %zu doubles from %s\n", n, path.c_str());
+        std::exit(2);
+    }
+    std::fclose(f);
+    return v;
+}
+
+// Output: records of [char name[32]][int64 n][n doubles].
+struct Out {
+    FILE* f;
+    explicit Out(const char* path) : f(std::fopen(path, "wb")) {
+        if (!f) {
+            std::fprintf(stderr, "cannot write %s\n", path);
+            std::exit(2);
+        }
+    }
+    ~Out() { std::fclose(f); }
+    void put(const char* name, const std::vector<double>& v) {
+        char nm[32] = {0};
+        std::strncpy(nm, name, 31);
+        const long long n = (long long)v.size();
+        std::fwrite(nm, 1, 32, f);
+        std::fwrite(&n, sizeof(n), 1, f);
+        std::fwrite(v.data(), sizeof(double), v.size(), f);
+    }
+    void put(const char* name, double x) { put(name, std::vector<double>(1, x)); }
+};
+
+bool isGGA(const std::string& fn) {
+    return fn == "B3LYP" || fn == "BLYP" || fn == "B88LYP" || fn == "HFB";
+}
+
+DfFunctional_LDA* makeLDA(const std::string& fn) {
+    if (fn == "SVWN") return new DfFunctional_SVWN();
+    if (fn == "HFS") return new DfFunctional_HFS();
+    std::fprintf(stderr, "unknown LDA functional %s\n", fn.c_str());
+    std::exit(2);
+}
+
+DfFunctional_GGA* makeGGA(const std::string& fn) {
+    if (fn == "B3LYP") return new DfFunctional_B3LYP();
+    if (fn == "BLYP" || fn == "B88LYP") return new DfFunctional_B88LYP();
+    if (fn == "HFB") return new DfFunctional_Becke88();
+    std::fprintf(stderr, "unknown GGA functional %s\n", fn.c_str());
+    std::exit(2);
+}
+
+class XcHarness : public DfCalcGridX {
+   public:
+    explicit XcHarness(TlSerializeData* p) : DfCalcGridX(p) {}
+    const TlOrbitalInfo& orb() const { return this->m_tlOrbInfo; }
+    int nao() const { return this->m_nNumOfAOs; }
+    using DfCalcGridX::buildVxc;
+    using DfCalcGridX::calcRho_GGA_part;
+    using DfCalcGridX::calcRho_LDA_part;
+    using DfCalcGridX::getAOs;
+    using DfCalcGridX::getDAOs;
+};
+
+class GridHarness : public DfGenerateGrid {
+   public:
+    explicit GridHarness(TlSerializeData* p) : DfGenerateGrid(p) {}
+    using DfGenerateGrid::generateGrid_atom;
+};
+
+double seconds_since(std::chrono::steady_clock::time_point t0) {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+int runXc(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    // DfObject reads num_of_AOs from the parameter set; build the AO table first.
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    XcHarness h(&param);
+
+    const std::string fn = c.get("functional", "SVWN");
+    const bool gga = isGGA(fn);
+    const long npts = std::atol(c.get("npts", "0").c_str());
+    const int ncol = gga ? 9 : 6;
+    const std::vector<double> grid = readDoubles(c.get("grid_file"), (size_t)npts * 5);
+    const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    const int nthreads = std::atoi(c.get("threads", "1").c_str());
+    omp_set_num_threads(nthreads > 0 ? nthreads : 1);
+
+    TlDenseGeneralMatrix_Lapack gridMat(npts, ncol);
+    for (long i = 0; i < npts; ++i)
+        for (int k = 0; k < 5; ++k) gridMat.set(i, k, grid[5 * i + k]);
+    TlDenseSymmetricMatrix_Lapack PA(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) PA.set(i, j, P[(size_t)i * N + j]);
+    TlDenseSymmetricMatrix_Lapack F(N);
+
+    const auto t0 = std::chrono::steady_clock::now();
+    if (gga) {
+        h.calcRho_GGA_part(PA, &gridMat);
+    } else {
+        h.calcRho_LDA_part(PA, &gridMat);
+    }
+    const double tRho = seconds_since(t0);
+    const auto t1 = std::chrono::steady_clock::now();
+    double exc = 0.0;
+    if (gga) {
+        DfFunctional_GGA* f = makeGGA(fn);
+        exc = h.buildVxc(gridMat, f, &F);
+        delete f;
+    } else {
+        DfFunctional_LDA* f = makeLDA(fn);
+        exc = h.buildVxc(gridMat, f, &F);
+        delete f;
+    }
+    const double tVxc = seconds_since(t1);
+
+    Out out(outPath);
+    out.put("exc", exc);
+    out.put("t_rho", tRho);
+    out.put("t_vxc", tVxc);
+    out.put("threads", (double)nthreads);
+    std::vector<double> vxc((size_t)N * N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j < N; ++j) vxc[(size_t)i * N + j] = F.get(i, j);
+    out.put("vxc", vxc);
+    std::vector<double> rho((size_t)npts * (ncol - 5));
+    double nel = 0.0;
+    for (long i = 0; i < npts; ++i) {
+        for (int k = 5; k < ncol; ++k) rho[(size_t)i * (ncol - 5) + (k - 5)] = gridMat.get(i, k);
+        nel += gridMat.get(i, DfCalcGridX::GM_WEIGHT) * gridMat.get(i, 5);
+    }
+    out.put("rho", rho);
+    out.put("nelec_alpha", nel);
+
+    // AO table as the reference normalises and orders it (TlOrbitalInfoObject).
+    const TlOrbitalInfo& orb = h.orb();
+    std::vector<double> aoAtom(N), aoType(N), aoNprim(N), aoExp, aoCoef;
+    for (int i = 0; i < N; ++i) {
+        aoAtom[i] = orb.getAtomIndex(i);
+        aoType[i] = orb.getBasisType(i);
+        aoNprim[i] = orb.getCgtoContraction(i);
+        for (int k = 0; k < orb.getCgtoContraction(i); ++k) {
+            aoExp.push_back(orb.getExponent(i, k));
+            aoCoef.push_back(orb.getCoefficient(i, k));
+        }
+    }
+    out.put("ao_atom", aoAtom);
+    out.put("ao_type", aoType);
+    out.put("ao_nprim", aoNprim);
+    out.put("ao_exp", aoExp);
+    out.put("ao_coef", aoCoef);
+
+    // AO values and gradients at the first few points (getAOs / getDAOs).
+    const long ndump = std::min<long>(npts, std::atol(c.get("ao_dump", "0").c_str()));
+    std::vector<double> phi, dphi;
+    for (long i = 0; i < ndump; ++i) {
+        const TlPosition r(grid[5 * i], grid[5 * i + 1], grid[5 * i + 2]);
+        std::vector<double> a, dx, dy, dz;
+        h.getAOs(r, &a);
+        h.getDAOs(r, &dx, &dy, &dz);
+        phi.insert(phi.end(), a.begin(), a.end());
+        for (int k = 0; k < N; ++k) dphi.insert(dphi.end(), {dx[k], dy[k], dz[k]});
+    }
+    out.put("phi", phi);
+    out.put("dphi", dphi);
+    return 0;
+}
+
+int runGrid(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    GridHarness g(&param);
+    const int natom = (int)c.atomSym.size();
+    TlDenseGeneralMatrix_Lapack I3(3, 3);
+    for (int k = 0; k < 3; ++k) I3.set(k, k, 1.0);
+
+    std::vector<double> pts, wsingle, wfinal, atomIdx, radii;
+    std::vector<double> finalGrid;  // x y z w atom, screened, per atom in order
+    for (int a = 0; a < natom; ++a) {
+        const int Z = TlPrdctbl::getAtomicNumber(c.atomSym[a]);
+        const double rM = TlPrdctbl::getBraggSlaterRadii(Z);
+        radii.push_back(rM);
+        radii.push_back(g.getCovalentRadiiForBecke(Z));
+        for (int i = 1; i <= g.nrgrid; ++i) {
+            double ri = 0.0, wr = 0.0;
+            if (g.radialGridType_ == DfGenerateGrid::RG_GaussChebyshev) {
+                g.getRadialAbscissaAndWeight_GaussChebyshev(rM, g.nrgrid, i, &ri, &wr);
+            } else {
+                g.getRadialAbscissaAndWeight_EulerMaclaurin(rM, g.nrgrid, i, &ri, &wr);
+            }
+            if (ri > 30.0) continue;
+            const int nang = g.getNumOfPrunedAnglarPoints(ri, g.nOgrid, Z);
+            std::vector<TlPosition> sph(nang);
+            std::vector<double> w(nang);
+            g.getSphericalGrids(nang, ri, wr, g.coord_[a], I3, &sph, &w);
+            std::vector<double> wp = w;
+            if (g.partitioningMethod_ == DfGenerateGrid::Paritioning_Becke) {
+                g.calcMultiCenterWeight_Becke(a, nang, sph, &wp);
+            } else {
+                g.calcMultiCenterWeight_SS(a, nang, sph, &wp);
+            }
+            for (int k = 0; k < nang; ++k) {
+                pts.insert(pts.end(), {sph[k].x(), sph[k].y(), sph[k].z()});
+                wsingle.push_back(w[k]);
+                wfinal.push_back(wp[k]);
+                atomIdx.push_back(a);
+            }
+        }
+        std::vector<double> x, y, z, w;
+        g.generateGrid_atom(I3, a, &x, &y, &z, &w);
+        for (size_t k = 0; k < x.size(); ++k) finalGrid.insert(finalGrid.end(), {x[k], y[k], z[k], w[k], (double)a});
+    }
+    Out out(outPath);
+    out.put("points", pts);
+    out.put("w_single", wsingle);
+    out.put("w_final", wfinal);
+    out.put("atom", atomIdx);
+    out.put("radii", radii);
+    out.put("grid", finalGrid);
+    return 0;
+}
+
+// Pointwise functional values through the overloads buildVxc uses
+// (RKS: src/libpdf/DfCalcGridX.cpp:2076-2087, :2164-2185) and the
+// open-shell ones the reference unit tests use.
+int runFunc(const Case& c, const char* outPath) {
+    const std::string fn = c.get("functional", "SVWN");
+    const long n = std::atol(c.get("npts", "0").c_str());
+    const std::vector<double> in = readDoubles(c.get("input_file"), (size_t)n * 5);
+    std::vector<double> res;  // per point: f, vrhoA, vrhoB, vgaa, vgab, vgbb, f_rks, vr_rks, vgaa_rks, vgab_rks
+    for (long i = 0; i < n; ++i) {
+        const double ra = in[5 * i], rb = in[5 * i + 1], gaa = in[5 * i + 2], gab = in[5 * i + 3], gbb = in[5 * i + 4];
+        double v[10] = {0};
+        if (isGGA(fn)) {
+            DfFunctional_GGA* f = makeGGA(fn);
+            v[0] = f->getFunctional(ra, rb, gaa, gab, gbb);
+            f->getDerivativeFunctional(ra, rb, gaa, gab, gbb, &v[1], &v[2], &v[3], &v[4], &v[5]);
+            v[6] = f->getFunctional(ra, gaa);
+            f->getDerivativeFunctional(ra, gaa, &v[7], &v[8], &v[9]);
+            delete f;
+        } else {
+            DfFunctional_LDA* f = makeLDA(fn);
+            v[0] = f->getFunctional(ra, rb);
+            f->getDerivativeFunctional(ra, rb, &v[1], &v[2]);
+            v[6] = f->getFunctional(ra, ra);
+            f->getDerivativeFunctional(ra, &v[7]);
+            delete f;
+        }
+        res.insert(res.end(), v, v + 10);
+    }
+    Out out(outPath);
+    out.put("values", res);
+    return 0;
+}
+
+// Unit-sphere Lebedev tables for every order the reference supports
+// (src/libpdftl/TlLebedevGrid.cpp), as used by getSphericalGrids.
+int runLebedev(const char* outPath) {
+    TlLebedevGrid leb;
+    const std::vector<int> orders = leb.getSupportedGridNumber();
+    Out out(outPath);
+    out.put("orders", std::vector<double>(orders.begin(), orders.end()));
+    for (int n : orders) {
+        std::vector<TlPosition> pts;
+        std::vector<double> w;
+        leb.getGrids(n, &pts, &w);
+        std::vector<double> v;
+        for (int k = 0; k < n; ++k) v.insert(v.end(), {pts[k].x(), pts[k].y(), pts[k].z(), w[k]});
+        char name[32];
+        std::snprintf(name, sizeof(name), "leb_%d", n);
+        out.put(name, v);
+    }
+    return 0;
+}
+
+}  // namespace
+
+int main(int argc, char** argv) {
+    if (argc != 4) {
+        std::fprintf(stderr, "usage: %s xc|grid|func <case.txt> <out.bin>\n", argv[0]);
+        return 2;
+    }
+    TlLogging::getInstance().setLevel(TlLogging::TL_WARN, TlLogging::TL_WARN);
+    const std::string mode = argv[1];
+    if (mode == "lebedev") return runLebedev(argv[3]);
+    const Case c = readCase(argv[2]);
+    if (mode == "xc") return runXc(c, argv[3]);
+    if (mode == "grid") return runGrid(c, argv[3]);
+    if (mode == "func") return runFunc(c, argv[3]);
+    std::fprintf(stderr, "unknown mode %s\n", argv[1]);
+    return 2;
+}

@@ -1,0 +1,88 @@
+"""I/O for the reference-oracle harness (oracle/_ref/pdfxc_ref).
+
+TEST INFRASTRUCTURE ONLY: used by tests/, the fixture generators under
+tests/golden/ and bench.py's reference arm. Writes the harness's case files
+(text key/value lines, atoms in bohr, raw basis-library contractions) and reads
+its flat output records ([char name[32]][int64 n][n float64]).
+"""
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_BIN = os.path.join(HERE, "_ref", "pdfxc_ref")
+
+
+def ref_available():
+    return os.path.exists(REF_BIN)
+
+
+def read_records(path):
+    out = {}
+    with open(path, "rb") as f:
+        while True:
+            name = f.read(32)
+            if len(name) < 32:
+                break
+            n = int(np.frombuffer(f.read(8), dtype=np.int64)[0])
+            out[name.rstrip(b"\0").decode()] = np.frombuffer(f.read(8 * n), dtype=np.float64).copy()
+    return out
+
+
+def write_case(path, symbols, charges, xyz_bohr, basis, kv):
+    """basis: {element: [{"shell": "s", "prims": [[exp, coef], ...]}, ...]}"""
+    with open(path, "w") as f:
+        for k, v in kv.items():
+            f.write(f"{k} {v}\n")
+        for s, q, r in zip(symbols, charges, np.asarray(xyz_bohr).reshape(-1, 3)):
+            f.write(f"atom {s} {q:.1f} {r[0]:.17g} {r[1]:.17g} {r[2]:.17g}\n")
+        for el in sorted(set(symbols), key=list(symbols).index):
+            for sh in basis[el]:
+                f.write(f"cgto {el} {sh['shell']} {len(sh['prims'])}\n")
+                for e, c in sh["prims"]:
+                    f.write(f"{e:.17g} {c:.17g}\n")
+
+
+def run(mode, case_path, out_path, threads=None, timeout=None):
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    env.setdefault("OMP_SCHEDULE", "dynamic")
+    subprocess.run([REF_BIN, mode, case_path, out_path], check=True, env=env, timeout=timeout)
+    return read_records(out_path)
+
+
+def run_xc(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, ao_dump=0,
+           threads=1, timeout=None):
+    """Reference rho + Vxc pass. grid5: (npts, 5) [x, y, z, w, atom]; PA: alpha density."""
+    os.makedirs(workdir, exist_ok=True)
+    gpath = os.path.join(workdir, "grid.bin")
+    ppath = os.path.join(workdir, "P.bin")
+    np.ascontiguousarray(grid5, dtype=np.float64).tofile(gpath)
+    np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
+    case = os.path.join(workdir, "case.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, {
+        "functional": functional, "npts": len(grid5), "grid_file": gpath,
+        "density_file": ppath, "ao_dump": ao_dump, "threads": threads})
+    return run("xc", case, os.path.join(workdir, "out.bin"), threads=threads, timeout=timeout)
+
+
+def run_grid(workdir, symbols, charges, xyz_bohr, basis, grid_kv):
+    os.makedirs(workdir, exist_ok=True)
+    case = os.path.join(workdir, "case.txt")
+    kv = {"functional": "SVWN"}
+    kv.update(grid_kv)
+    write_case(case, symbols, charges, xyz_bohr, basis, kv)
+    return run("grid", case, os.path.join(workdir, "grid_out.bin"))
+
+
+def run_func(workdir, functional, inputs5):
+    os.makedirs(workdir, exist_ok=True)
+    ipath = os.path.join(workdir, "func_in.bin")
+    np.ascontiguousarray(inputs5, dtype=np.float64).tofile(ipath)
+    case = os.path.join(workdir, "func.txt")
+    with open(case, "w") as f:
+        f.write(f"functional {functional}\nnpts {len(inputs5)}\ninput_file {ipath}\n")
+    r = run("func", case, os.path.join(workdir, "func_out.bin"))
+    return r["values"].reshape(-1, 10)
