@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Vxc build throughput of the B200 XC quadrature (grid points/s, ms per SCF iteration).
+
+Workload (default): a seeded 100-atom peptide-like chain (C:N:O:H = 30:8:10:52),
+cc-pVDZ (5d; the 6-31G** stand-in, ~930 AOs), B3LYP, ULTRA_FINE 99x590 grid
+(Euler-Maclaurin radial, pruned, Becke partition computed on the GPU), alpha
+density P_A = C C^T from the QR of a seeded N(0,1) N x 380 matrix. One step is
+one closed-shell Vxc build (rho pass + Vxc pass) of the whole grid.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py --impl reference ...   (the reference's CPU DfCalcGridX, sampled)
+
+Under torchrun (N > 1) every rank builds its own chain (seed + rank): the units
+are independent molecules, no data-path collective; value = all ranks' points
+/ the slowest rank's time (weak scaling).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Vxc build grid points/s"
+UNIT = "grid points/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--natoms", type=int, default=100)
+    ap.add_argument("--functional", default="B3LYP")
+    ap.add_argument("--grid", default="ULTRA_FINE")
+    ap.add_argument("--nocc", type=int, default=380)
+    ap.add_argument("--seed", type=int, default=1)
+    ap.add_argument("--cpu-sample", type=int, default=4000, help="grid points for the CPU baseline sample")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def workload(args, seed):
+    """Seeded chain, basis table, single-centre grid, density."""
+    from proteindf_b200 import basis, grids, systems
+    syms, xyz = systems.peptide_chain(args.natoms, seed=seed)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+    P, W, A = grids.molecular_grid(xyz, sh.atom_z, **grids.PRESETS[args.grid])
+    PA = 0.5 * systems.density_matrix(sh.nao, args.nocc, seed=seed)
+    brad = np.array([grids.BECKE_RADIUS[int(z)] for z in sh.atom_z])
+    return syms, xyz, sh, P, W, A, PA, brad
+
+
+def final_grid(eng, P, W, A, brad):
+    from proteindf_b200 import grids
+    w = eng.becke_weights(P, A, W, brad)
+    P2, W2, A2 = grids.screen_by_weight(P, w, A)
+    return np.concatenate([P2, W2[:, None]], axis=1), A2
+
+
+def config(args, npts, nao, **extra):
+    c = {"workload": f"{args.natoms}-atom peptide-like chain, cc-pVDZ, {args.functional}, {args.grid} grid",
+         "atoms": args.natoms, "n_ao": nao, "grid_points": int(npts), "functional": args.functional,
+         "grid": args.grid, "precision": args.precision, "nocc": args.nocc,
+         "l2": "flushed between timed steps (512 MiB write)"}
+    c.update(extra)
+    return c
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out, _ = self.proc.communicate()
+
+    def summary(self):
+        rows = [r.split(",") for r in (self.out or "").strip().splitlines() if r.count(",") >= 8]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({n for r in rows for n, v in zip(names, r[5:9]) if "Active" in v and "Not" not in v})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        return {}
+
+
+def fp64_gemm_peak(torch):
+    """Measured cuBLAS DGEMM throughput on this GPU (TFLOP/s), burst, best of 5."""
+    n = 8192
+    a = torch.randn(n, n, device="cuda", dtype=torch.float64)
+    b = torch.randn(n, n, device="cuda", dtype=torch.float64)
+    for _ in range(2):
+        torch.matmul(a, b)
+    best = 1e30
+    for _ in range(5):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        best = min(best, s.elapsed_time(e))
+    del a, b
+    return 2.0 * n ** 3 / (best * 1e-3) / 1e12
+
+
+def cpu_baseline(args, syms, xyz, grid5, PA, sample, reference_kind=True):
+    """Reference DfCalcGridX (oracle/_ref/pdfxc_ref) on a seeded sample of grid rows,
+    all host cores; per-point cost is position-independent in the reference (it
+    evaluates every AO at every point), so points/s extrapolates linearly."""
+    import tempfile
+    from oracle import refio
+    from proteindf_b200 import basis, systems
+    cores = os.cpu_count() or 1
+    rng = np.random.default_rng(0)
+    sel = np.sort(rng.choice(len(grid5), min(sample, len(grid5)), replace=False))
+    g = grid5[sel]
+    if reference_kind and refio.ref_available():
+        with tempfile.TemporaryDirectory() as d:
+            r = refio.run_xc(d, syms, systems.nuclear_charges(syms), xyz, basis.load_basis("cc-pVDZ"),
+                             args.functional, g, PA, threads=cores)
+        t = float(r["t_rho"][0] + r["t_vxc"][0])
+        kind = "reference"
+    else:
+        from oracle import oracle
+        sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+        t0 = time.perf_counter()
+        oracle.xc(args.functional, sh, g[:, :4], PA, threads=cores)
+        t = time.perf_counter() - t0
+        kind = "port"
+    return {"value": len(g) / t, "unit": UNIT, "cores": cores, "kind": kind,
+            "sample": f"{len(g)} of {len(grid5)} grid points (seed 0), rho pass + Vxc pass, {t:.1f} s"}
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    from proteindf_b200 import grids, systems
+    from oracle import oracle, refio
+    syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed)
+    # Becke weights on the CPU oracle for the reference arm (no GPU on its path)
+    fac = oracle.becke(xyz, brad, P, A)
+    P2, W2, A2 = grids.screen_by_weight(P, W * fac, A)
+    grid5 = np.concatenate([P2, W2[:, None], A2[:, None]], axis=1)
+    per_step = max(200, args.cpu_sample // 4)
+    vals = []
+    for i in range(args.warmup + args.steps):
+        cb = cpu_baseline(args, syms, xyz, grid5, PA, per_step)
+        if i >= args.warmup:
+            vals.append(cb["value"])
+    v = float(np.mean(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(grid5) / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded chain, reference-generated grid recipe)",
+            "config": config(args, len(grid5), sh.nao),
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
+                             "sample": f"{per_step} grid points per step, extrapolated to {len(grid5)}"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    from proteindf_b200.xc import XcEngine
+
+    syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed + rank)
+    eng = XcEngine(device=local, precision=args.precision)
+    eng.set_system(sh)
+    grid4, owner = final_grid(eng, P, W, A, brad)
+    eng.set_grid(grid4, owner)
+    stats = eng.grid_stats()
+    npts = len(grid4)
+    nao = sh.nao
+    dP = torch.tensor(PA, device=f"cuda:{local}")
+    dV = torch.empty_like(dP)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
+
+    for _ in range(args.warmup):
+        eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    prof_sum = {}
+    dev_ms = 0.0
+    launches = 0
+    barrier()
+    with ClockSampler(local) as clk:
+        wall0 = time.perf_counter()
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            exc, nel = eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+            p = eng.last_profile()
+            dev_ms += p["total_ms"]
+            launches += p["launches"]
+            for k, v in p.items():
+                prof_sum[k] = prof_sum.get(k, 0.0) + v
+        barrier()
+        wall = time.perf_counter() - wall0
+    t_dev = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        torch.distributed.all_reduce(t_dev, op=torch.distributed.ReduceOp.MAX)
+    ms_per_step = float(t_dev.item()) / args.steps
+    value = world * npts / (ms_per_step * 1e-3)
+
+    # end to end through the host API: P from pinned host memory in, Vxc out
+    pin_P = torch.empty((nao, nao), dtype=torch.float64, pin_memory=True)
+    pin_P.copy_(torch.from_numpy(PA))
+    pin_F = torch.zeros((nao, nao), dtype=torch.float64, pin_memory=True)
+    e2e_t = []
+    for i in range(max(1, args.steps)):
+        pin_F.zero_()
+        barrier()
+        t0 = time.perf_counter()
+        eng.build_vxc(args.functional, pin_P.numpy(), F=pin_F.numpy())
+        e2e_t.append(time.perf_counter() - t0)
+    t_e2e = torch.tensor([float(np.mean(e2e_t))], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        torch.distributed.all_reduce(t_e2e, op=torch.distributed.ReduceOp.MAX)
+
+    if rank == 0:
+        # roofline of the dominant contraction kernel
+        peaks = measured_peaks()
+        flops = stats["contraction_flops"]  # sum over blocks of 4 nb^2 np: both contractions
+        per = {k: prof_sum[k] / args.steps for k in ("ao_ms", "gemm_x_ms", "rho_ms", "gemm_v_ms", "finish_ms")}
+        top = max(("gemm_x_ms", "gemm_v_ms"), key=lambda k: per[k])
+        achieved = 0.5 * flops / (per[top] * 1e-3) / 1e12
+        if args.precision == "fp64":
+            peak = fp64_gemm_peak(torch)
+            peak_note = "measured cuBLAS FP64 DGEMM 8192^3 on this GPU (burst)"
+        else:
+            peak = peaks.get("bf16_tflops", 1590.0)
+            peak_note = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1.59 PFLOP/s"
+        roof = {"bound": "tensor", "kernel": top.replace("_ms", ""), "achieved": achieved, "peak": peak,
+                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_note,
+                "flops_per_build": 0.5 * flops, "stage_ms": per}
+        cpu = None
+        if not args.no_cpu_baseline:
+            grid5 = np.concatenate([grid4, owner[:, None].astype(np.float64)], axis=1)
+            cpu = cpu_baseline(args, syms, xyz, grid5, PA, args.cpu_sample)
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32/f64",
+                "data": "synthetic (seeded chain and density, ProteinDF grid recipe)",
+                "config": config(args, npts, nao, blocks=stats["nblocks"], mean_screened_aos=stats["mean_nb"]),
+                "exc": exc, "nelec_alpha": nel, "wall_s": wall,
+                "e2e": {"value": world * npts / float(t_e2e.item()), "unit": UNIT,
+                        "h2d_bytes_per_step": nao * nao * 8, "d2h_bytes_per_step": nao * nao * 8 + 16},
+                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,152 @@
+/*
+ * pdfxc.h -- C ABI of the B200 grid exchange-correlation quadrature.
+ *
+ * This is the boundary that replaces ProteinDF's DfCalcGridX engine
+ * (src/libpdf/DfCalcGridX.{h,cpp}). A host-side DfCalcGridX-compatible class
+ * (or any FFI) calls these entry points; they take plain pointers and sizes,
+ * never throw, and return a pdfxc_status (0 = success). One context drives
+ * one GPU; calls on a context are synchronous and not re-entrant.
+ *
+ * Units: coordinates in bohr, energies in hartree. Matrices are dense,
+ * row-major, n_ao x n_ao FP64. The closed-shell convention of the reference
+ * applies: the caller passes the alpha density P_A = P/2
+ * (src/libpdf/DfXCFunctional.cpp:133-139) and receives the alpha Kohn-Sham
+ * matrix, accumulated into (F += Vxc) as DfCalcGridX does
+ * (src/libpdf/DfCalcGridX.cpp:2351-2500).
+ */
+#ifndef PDFXC_H
+#define PDFXC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int pdfxc_status;
+
+enum {
+    PDFXC_OK = 0,
+    PDFXC_ERR_ARG = 1,      /* bad argument (null pointer, size out of range) */
+    PDFXC_ERR_CUDA = 2,     /* a CUDA runtime call failed; see pdfxc_last_error */
+    PDFXC_ERR_STATE = 3,    /* call out of order (e.g. build before set_grid) */
+    PDFXC_ERR_TIMEOUT = 4,  /* a bounded device wait expired */
+    PDFXC_ERR_NOMEM = 5,    /* device allocation failed */
+    PDFXC_ERR_UNSUPPORTED = 6
+};
+
+/* Functional identifiers; names as the reference's xc-potential keyword
+ * (src/libpdf/DfXCFunctional.cpp:70-104). */
+enum {
+    PDFXC_SVWN = 0,  /* Slater + VWN5 (LDA) */
+    PDFXC_HFS = 1,   /* Slater (LDA) */
+    PDFXC_HFB = 2,   /* Becke 88 (GGA) */
+    PDFXC_BLYP = 3,  /* Becke 88 + LYP (GGA) */
+    PDFXC_B3LYP = 4  /* 0.80 Slater + 0.72 B88 + 0.19 VWN3 + 0.81 LYP (GGA) */
+};
+
+enum {
+    PDFXC_PRECISION_FP64 = 0,  /* the drop-in: every product in FP64 */
+    PDFXC_PRECISION_MIXED = 1  /* tensor-core split-BF16 contractions, FP64 sums */
+};
+
+typedef struct {
+    int precision;       /* PDFXC_PRECISION_* */
+    int block_points;    /* grid points per block, 1..128 (default 128) */
+    double ao_cutoff;    /* drop a shell from a block when its value/gradient bound is below (default 1e-14) */
+    double rho_cutoff;   /* xc-density-threshold: points with rho_A <= it are skipped (default 1e-16) */
+    size_t workspace_bytes; /* device workspace budget for block intermediates (0 = default 4 GiB) */
+} pdfxc_options;
+
+typedef struct pdfxc_ctx pdfxc_ctx;
+
+/* Fill *opt with the defaults. */
+void pdfxc_default_options(pdfxc_options* opt);
+
+/* Create a context on CUDA device `device`. Replaces the DfCalcGridX
+ * constructor (src/libpdf/DfCalcGridX.cpp:47-74). */
+pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt);
+
+/* Molecule and basis (TlOrbitalInfo, src/libpdf/TlOrbitalInfoObject.cpp:38-256).
+ * Shells in AO order; shell s has angular momentum shell_l[s] in {0,1,2}
+ * (components s; px,py,pz; dxy,dxz,dyz,d(x2-y2),dz2), shell_nprim[s]
+ * primitives whose exponents/normalised coefficients follow consecutively in
+ * prim_exp/prim_coef. */
+pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
+                              const int* atom_z, int nshell, const int* shell_atom,
+                              const int* shell_l, const int* shell_nprim,
+                              const double* prim_exp, const double* prim_coef);
+
+/* The quadrature grid: npts rows of (x, y, z, w) with w the final
+ * (partitioned) weight, and the owning atom of each point -- the grid matrix
+ * columns GM_X..GM_ATOM_INDEX of src/libpdf/DfCalcGridX.h:35-54. Points are
+ * regrouped into spatial blocks and the per-block shell lists are screened
+ * here, once per geometry. */
+pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom);
+
+/* Becke partition weights with atomic-size adjustment
+ * (DfGenerateGrid::calcMultiCenterWeight_Becke, src/libpdf/DfGenerateGrid.cpp:1811-1876,
+ * Ps_uij :2043-2086): w_out[i] = w_single[i] * P_owner(r_i) / sum_m P_m(r_i).
+ * becke_radius[a] is the size-adjustment radius of atom a (0.35 for H,
+ * Bragg-Slater otherwise, :1958-1968). Requires pdfxc_set_system. */
+pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz,
+                                 const int* atom, const double* w_single,
+                                 const double* becke_radius, int size_adjust, double* w_out);
+
+/* One closed-shell XC build: rho pass + Vxc pass
+ * (DfCalcGridX::calcXCIntegForFockAndEnergy, src/libpdf/DfCalcGridX.cpp:2280-2315).
+ * PA: n_ao x n_ao alpha density (host). If incremental != 0 the density
+ * rho/grad rho of PA is added to the stored per-point values of the previous
+ * build (xc-update = yes, :1862-1889, PA is then the alpha density
+ * difference); otherwise they are recomputed from PA. F (host, n_ao x n_ao)
+ * is accumulated into: F += Vxc. exc receives the XC energy, nelec_alpha
+ * sum_i w_i rho_A(r_i) (DfCalcGridX::getWholeDensity, :2502-2537).
+ * Either of exc, nelec_alpha may be NULL. */
+pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, int incremental,
+                             double* F, double* exc, double* nelec_alpha);
+
+/* Same build on device-resident operands (d_PA, d_V: n_ao*n_ao FP64 device
+ * pointers; d_V is overwritten with Vxc, not accumulated), enqueued on the
+ * context's stream; exc/nelec_alpha are host pointers filled after the stream
+ * synchronises. */
+pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double* d_PA,
+                                    int incremental, double* d_V, double* exc,
+                                    double* nelec_alpha);
+
+/* Per-point densities of the last build in input point order: npts x 1
+ * (LDA: rho_A) or npts x 4 (GGA: rho_A, d/dx, d/dy, d/dz) -- the rho columns
+ * of the grid matrix (src/libpdf/DfCalcGridX.h:35-54). pdfxc_set_rho seeds
+ * them (restart with xc-update = yes). */
+pdfxc_status pdfxc_get_rho(pdfxc_ctx* ctx, int gga, double* rho);
+pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho);
+
+/* Statistics of the blocked grid: blocks, points (after padding), the sum of
+ * 4 * nb^2 * np over blocks (the algorithmic contraction FLOPs of one build)
+ * and the mean screened AO count per block. */
+pdfxc_status pdfxc_grid_stats(pdfxc_ctx* ctx, int64_t* nblocks, int64_t* npts_padded,
+                              double* contraction_flops, double* mean_nb);
+
+/* Device time (ms) of the last build, measured with CUDA events on the
+ * context's stream, split by stage and summed over the workspace chunks, and
+ * the number of kernels the build launched. */
+typedef struct {
+    float total_ms;     /* first to last event of the build */
+    float ao_ms;        /* basis-function (and gradient) evaluation */
+    float gemm_x_ms;    /* X = P_sub * phi contraction */
+    float rho_ms;       /* rho / grad rho reduction and the functional */
+    float gemm_v_ms;    /* Vxc += phi Z^T contraction */
+    float finish_ms;    /* symmetrisation and FP64 block sums */
+    int64_t launches;   /* kernels launched by the build */
+} pdfxc_profile;
+
+pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out);
+
+const char* pdfxc_last_error(const pdfxc_ctx* ctx);
+void pdfxc_destroy(pdfxc_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* PDFXC_H */

@@ -95,3 +95,15 @@ def becke(atom_xyz, brad, xyz, owner, size_adjust=True):
                              ctypes.c_long(len(xyz)), xyz.ctypes.data_as(ctypes.c_void_p),
                              owner.ctypes.data_as(ctypes.c_void_p), fac.ctypes.data_as(ctypes.c_void_p))
     return fac
+
+
+COMPONENTS = {"Slater": 0, "VWN5": 1, "VWN3": 2, "Becke88": 3, "Becke88_ExceptLDA": 4, "LYP": 5}
+
+
+def component(name, ra, rb, gaa, gab, gbb):
+    """One functional term (the reference's per-class objects); returns 6 values."""
+    o = np.zeros(6)
+    lib().pdfxc_oracle_component(ctypes.c_int(COMPONENTS[name]), ctypes.c_double(ra), ctypes.c_double(rb),
+                                 ctypes.c_double(gaa), ctypes.c_double(gab), ctypes.c_double(gbb),
+                                 o.ctypes.data_as(ctypes.c_void_p))
+    return o

@@ -77,8 +77,9 @@ static void vwn(int v3, double ra, double rb, double* f, double* va, double* vb)
     const vwn_par P = v3 ? VWN3_P : VWN5_P, F = v3 ? VWN3_F : VWN5_F, A = vwn_anti();
     const double ec_coef = 4.0 / (9.0 * (pow(2.0, 1.0 / 3.0) - 1.0));
     const double rho = ra + rb;
-    const double x = pow(3.0 / (4.0 * M_PI) / rho, 1.0 / 6.0);
-    const double zeta = (ra - rb) / rho;
+    const double inv = 1.0 / rho;
+    const double x = pow(3.0 / (4.0 * M_PI) * inv, 1.0 / 6.0);
+    const double zeta = (ra - rb) * inv;
     const double ep = vwn_eps(P, x), ef = vwn_eps(F, x), ea = vwn_eps(A, x);
     const double g = 9.0 / 8.0 * (pow(1.0 + zeta, 4.0 / 3.0) + pow(1.0 - zeta, 4.0 / 3.0) - 2.0);
     const double z3 = zeta * zeta * zeta, z4 = z3 * zeta;
@@ -91,7 +92,7 @@ static void vwn(int v3, double ra, double rb, double* f, double* va, double* vb)
     const double hp = ec_coef / ea * (efp - epp - (ef - ep) / ea * eap);
     const double t1 = -x / (6.0 * rho) * (epp + eap * g * (1.0 + h * z4) + ea * g * hp * z4);
     const double t2c = ea * (gp * (1.0 + h * z4) + 4.0 * g * h * z3);
-    const double dzA = (1.0 - zeta) / rho, dzB = -(1.0 + zeta) / rho;
+    const double dzA = inv * (1.0 - zeta), dzB = -inv * (1.0 + zeta);
     *va = (ra > 1.0e-20) ? EC + rho * (t1 + t2c * dzA) : 0.0;
     *vb = (rb > 1.0e-20) ? EC + rho * (t1 + t2c * dzB) : 0.0;
 }
@@ -272,6 +273,27 @@ int pdfxc_oracle_functional(int fn, double ra, double rb, double gaa, double gab
 }
 
 int pdfxc_oracle_is_gga(int fn) { return fn == FN_HFB || fn == FN_BLYP || fn == FN_B3LYP; }
+
+/* Single components, for the reference's per-class known-answer tests:
+ * 0 Slater, 1 VWN5, 2 VWN3, 3 Becke88, 4 Becke88 except LDA, 5 LYP. */
+int pdfxc_oracle_component(int comp, double ra, double rb, double gaa, double gab, double gbb,
+                           double* out) {
+    double f = 0, va = 0, vb = 0, vgaa = 0, vgab = 0, vgbb = 0;
+    switch (comp) {
+        case 0: slater(ra, rb, &f, &va, &vb); break;
+        case 1: vwn(0, ra, rb, &f, &va, &vb); break;
+        case 2: vwn(1, ra, rb, &f, &va, &vb); break;
+        case 3: b88(1, ra, rb, gaa, gbb, &f, &va, &vb, &vgaa, &vgbb); break;
+        case 4: b88(0, ra, rb, gaa, gbb, &f, &va, &vb, &vgaa, &vgbb); break;
+        case 5:
+            f = lyp_f(ra, rb, gaa, gab, gbb);
+            lyp_v(ra, rb, gaa, gab, gbb, &va, &vb, &vgaa, &vgab, &vgbb);
+            break;
+        default: return -1;
+    }
+    out[0] = f, out[1] = va, out[2] = vb, out[3] = vgaa, out[4] = vgab, out[5] = vgbb;
+    return 0;
+}
 
 /* ---------------- AO values: src/libpdf/DfCalcGridX.cpp:103-235, :667-769 ------
  * Shell table: per shell atom, L (0..2), first AO, nprim, first primitive.

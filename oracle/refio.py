@@ -49,7 +49,9 @@ def run(mode, case_path, out_path, threads=None, timeout=None):
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
     env.setdefault("OMP_SCHEDULE", "dynamic")
-    subprocess.run([REF_BIN, mode, case_path, out_path], check=True, env=env, timeout=timeout)
+    # the reference writes its log file into the working directory
+    subprocess.run([REF_BIN, mode, case_path, out_path], check=True, env=env, timeout=timeout,
+                   cwd=os.path.dirname(os.path.abspath(out_path)), stdout=subprocess.DEVNULL)
     return read_records(out_path)
 
 

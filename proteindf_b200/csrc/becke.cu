@@ -1,0 +1,75 @@
+// Becke partition weights on the device (K7).
+//
+// For point r owned by atom A (DfGenerateGrid::calcMultiCenterWeight_Becke,
+// src/libpdf/DfGenerateGrid.cpp:1811-1876, Ps_uij :2043-2086):
+//   P_m(r) = prod_{n != m} s(nu_mn),  s(nu) = (1 - f(f(f(nu)))) / 2,  f(x) = x (3 - x^2) / 2
+//   mu_mn  = (|r - R_m| - |r - R_n|) / |R_m - R_n|
+//   nu_mn  = mu_mn + a_mn (1 - mu_mn^2), a = u / (u^2 - 1), u = (R_m - R_n)/(R_m + R_n),
+//            a clamped to [-1/2, 1/2] (atomic size adjustment, Becke radii)
+//   w(r)   = w_single(r) * P_A(r) / sum_m P_m(r).
+// One thread per point; the atoms (coordinates and radius) are staged in
+// shared memory once per CTA. All arithmetic is FP64.
+#include <cuda_runtime.h>
+
+#include "pdfxc_internal.cuh"
+
+namespace pdfxc {
+
+namespace {
+
+__device__ __forceinline__ double becke_s(double nu) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) nu = 0.5 * nu * (3.0 - nu * nu);
+    return 0.5 * (1.0 - nu);
+}
+
+__global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atom_xyz, const double* __restrict__ brad,
+                                               int natom, int size_adjust, int64_t npts,
+                                               const double* __restrict__ xyz, const int* __restrict__ owner,
+                                               const double* __restrict__ w_single, double* __restrict__ w_out) {
+    extern __shared__ double4 atoms[];  // x, y, z, radius
+    for (int a = threadIdx.x; a < natom; a += blockDim.x)
+        atoms[a] = make_double4(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2], brad[a]);
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
+        const double rx = xyz[3 * i], ry = xyz[3 * i + 1], rz = xyz[3 * i + 2];
+        const int own = owner[i];
+        double tot = 0.0, pown = 0.0;
+        for (int m = 0; m < natom; ++m) {
+            const double4 A = atoms[m];
+            const double rm = sqrt((rx - A.x) * (rx - A.x) + (ry - A.y) * (ry - A.y) + (rz - A.z) * (rz - A.z));
+            double p = 1.0;
+            for (int n = 0; n < natom && p != 0.0; ++n) {
+                if (n == m) continue;
+                const double4 B = atoms[n];
+                const double rn = sqrt((rx - B.x) * (rx - B.x) + (ry - B.y) * (ry - B.y) + (rz - B.z) * (rz - B.z));
+                const double Rmn = sqrt((A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z));
+                double u = (rm - rn) * (1.0 / Rmn);
+                if (size_adjust) {
+                    const double au = (A.w - B.w) / (A.w + B.w);
+                    double a = au / (au * au - 1.0);
+                    a = a < -0.5 ? -0.5 : (a > 0.5 ? 0.5 : a);
+                    u = u + a * (1.0 - u * u);
+                }
+                p *= becke_s(u);
+            }
+            tot += p;
+            if (m == own) pown = p;
+        }
+        w_out[i] = w_single[i] * (pown / tot);
+    }
+}
+
+}  // namespace
+
+void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust, int64_t npts,
+                  const double* xyz, const int* owner, const double* w_single, double* w_out, cudaStream_t s) {
+    const int threads = 128;
+    int64_t blocks = (npts + threads - 1) / threads;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks < 1) blocks = 1;
+    k_becke<<<(unsigned)blocks, threads, sizeof(double4) * natom, s>>>(atom_xyz, brad, natom, size_adjust, npts, xyz,
+                                                                       owner, w_single, w_out);
+}
+
+}  // namespace pdfxc

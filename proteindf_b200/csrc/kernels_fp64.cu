@@ -1,0 +1,369 @@
+// FP64 drop-in kernels of the XC build.
+//
+// Per block of up to 128 grid points with its screened AO list (nb AOs, padded
+// to nbp rows), one build runs
+//   ao_eval      phi[mu][p], grad phi[k][mu][p]                (DfCalcGridX.cpp:667-769)
+//   gemm_x       X = P_sub * phi, P_sub = P_A[aos, aos]
+//   rho_functional  rho_A(p) = sum_mu phi X, grad rho_A = 2 sum_mu grad phi X
+//                (:865-931), the functional, Exc and electron-count partials,
+//                and the per-point Vxc coefficients (:2056-2193, :2455-2500)
+//   gemm_v       Vacc[aos, aos] += phi * Z^T with
+//                Z[nu][p] = 0.5 w vrho phi + c . grad phi, c = w (2 vgAA + vgAB) grad rho_A
+//   finish       V = Vacc + Vacc^T, FP64 block sums of Exc and the electron count
+// V = phi Z^T + Z phi^T reproduces the reference's element formula
+// V_ij += w vrho phi_i phi_j + phi_i (c . grad phi_j) + phi_j (c . grad phi_i).
+#include <cuda_runtime.h>
+
+#include "functional.cuh"
+#include "pdfxc_internal.cuh"
+
+namespace pdfxc {
+
+namespace {
+
+__device__ __forceinline__ void ang_factor(int t, double x, double y, double z, double a2, double& v,
+                                           double& dx, double& dy, double& dz) {
+    // Angular prefactor and its derivative factor for basis type t
+    // (DfCalcGridX.cpp:103-235): phi = sum_k c_k v e^{-a r^2},
+    // d phi / dx = sum_k c_k dx e^{-a r^2}, with a2 = 2a.
+    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+    switch (t) {
+        case 0: v = 1.0; dx = -a2 * x; dy = -a2 * y; dz = -a2 * z; break;
+        case 1: v = x; dx = -a2 * x * x + 1.0; dy = -a2 * x * y; dz = -a2 * x * z; break;
+        case 2: v = y; dx = -a2 * y * x; dy = -a2 * y * y + 1.0; dz = -a2 * y * z; break;
+        case 3: v = z; dx = -a2 * z * x; dy = -a2 * z * y; dz = -a2 * z * z + 1.0; break;
+        case 4: v = x * y; dx = -a2 * x * y * x + y; dy = -a2 * x * y * y + x; dz = -a2 * x * y * z; break;
+        case 5: v = z * x; dx = -a2 * x * z * x + z; dy = -a2 * x * z * y; dz = -a2 * x * z * z + x; break;
+        case 6: v = y * z; dx = -a2 * y * z * x; dy = -a2 * y * z * y + z; dz = -a2 * y * z * z + y; break;
+        case 7: {
+            v = 0.5 * (x * x - y * y);
+            dx = 0.5 * ((-a2 * x * x * x + 2.0 * x) - (-a2 * y * y * x));
+            dy = 0.5 * ((-a2 * x * x * y) - (-a2 * y * y * y + 2.0 * y));
+            dz = 0.5 * ((-a2 * x * x * z) - (-a2 * y * y * z));
+            break;
+        }
+        default: {
+            v = s3 * (z * z - 0.5 * (x * x + y * y));
+            const double xxX = -a2 * x * x * x + 2.0 * x, xxY = -a2 * x * x * y, xxZ = -a2 * x * x * z;
+            const double yyX = -a2 * y * y * x, yyY = -a2 * y * y * y + 2.0 * y, yyZ = -a2 * y * y * z;
+            const double zzX = -a2 * z * z * x, zzY = -a2 * z * z * y, zzZ = -a2 * z * z * z + 2.0 * z;
+            dx = s3 * (zzX - 0.5 * (xxX + yyX));
+            dy = s3 * (zzY - 0.5 * (xxY + yyY));
+            dz = s3 * (zzZ - 0.5 * (xxZ + yyZ));
+        }
+    }
+}
+
+// One CTA per block, 256 threads: the point is threadIdx.x % 128, the two
+// halves of the CTA take alternate shells. Stores are coalesced along points.
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_ao_eval(BasisView bas, GridView g, int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x & (BLOCK_PTS - 1);
+    const int half = threadIdx.x >> 7;
+    double* phi = reinterpret_cast<double*>(ws + m.ws);
+    double* dphi = phi + (size_t)m.nbp * BLOCK_PTS;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const int gp = blk * BLOCK_PTS + p;
+    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
+    for (int i = half; i < m.nsh; i += 2) {
+        const int s = g.blk_shells[m.sh0 + i];
+        const int row0 = g.blk_shell_row[m.sh0 + i];
+        const int a = bas.sh_atom[s];
+        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1],
+                     z = rz - bas.atom_xyz[3 * a + 2];
+        const double d2 = x * x + y * y + z * z;
+        const int L = bas.sh_l[s], n = 2 * L + 1, np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
+        double v[5] = {0, 0, 0, 0, 0}, gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0},
+               gz[5] = {0, 0, 0, 0, 0};
+        for (int k = 0; k < np; ++k) {
+            const double al = bas.p_exp[p0 + k];
+            if (al * d2 <= 30.0) {  // TOOBIG, DfCalcGridX.cpp:42, :690
+                const double e = bas.p_coef[p0 + k] * exp(-al * d2);
+                for (int c = 0; c < n; ++c) {
+                    double av, ax, ay, az;
+                    ang_factor(L * L + c, x, y, z, 2.0 * al, av, ax, ay, az);
+                    v[c] += av * e;
+                    if (GGA) gx[c] += ax * e, gy[c] += ay * e, gz[c] += az * e;
+                }
+            }
+        }
+        for (int c = 0; c < n; ++c) {
+            const size_t o = (size_t)(row0 + c) * BLOCK_PTS + p;
+            phi[o] = v[c];
+            if (GGA) {
+                dphi[o] = gx[c];
+                dphi[plane + o] = gy[c];
+                dphi[2 * plane + o] = gz[c];
+            }
+        }
+    }
+    // zero the padding rows
+    for (int r = m.nb + half; r < m.nbp; r += 2) {
+        const size_t o = (size_t)r * BLOCK_PTS + p;
+        phi[o] = 0.0;
+        if (GGA) dphi[o] = dphi[plane + o] = dphi[2 * plane + o] = 0.0;
+    }
+}
+
+// X[m][p] = sum_k P[aos[m]][aos[k]] phi[k][p]; tile 64 rows x 128 points, K step 16.
+// 256 threads; thread (ty, tx) owns rows ty*4 + i and points tx + 16 j.
+constexpr int GX_BM = 64, GX_BK = 16;
+__global__ void __launch_bounds__(256) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
+                                                int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.y;
+    const BlockMeta m = g.meta[blk];
+    const int m0 = blockIdx.x * GX_BM;
+    if (m0 >= m.nbp) return;
+    const double* phi = reinterpret_cast<const double*>(ws + m.ws);
+    // X follows the phi planes (1 for LDA, 4 with gradients); gridDim.z carries that count.
+    const int nplanes = gridDim.z;
+    double* X = reinterpret_cast<double*>(ws + m.ws) + (size_t)nplanes * m.nbp * BLOCK_PTS;
+    const int* aos = g.blk_aos + m.ao0;
+
+    __shared__ double As[GX_BK][GX_BM + 1];
+    __shared__ double Bs[GX_BK][BLOCK_PTS];
+    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
+    double acc[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+
+    for (int k0 = 0; k0 < m.nbp; k0 += GX_BK) {
+        // A tile: 64 x 16 gathered from P (4 per thread)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = t + q * 256;
+            const int r = e >> 4, c = e & 15;
+            const int gr = m0 + r, gc = k0 + c;
+            double v = 0.0;
+            if (gr < m.nb && gc < m.nb) v = P[(size_t)aos[gr] * nao + aos[gc]];
+            As[c][r] = v;
+        }
+        // B tile: 16 x 128 of phi (8 per thread, coalesced)
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int e = t + q * 256;
+            const int r = e >> 7, c = e & 127;
+            Bs[r][c] = phi[(size_t)(k0 + r) * BLOCK_PTS + c];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GX_BK; ++kk) {
+            double a[4], b[8];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) X[(size_t)(m0 + ty * 4 + i) * BLOCK_PTS + tx + 16 * j] = acc[i][j];
+}
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// One CTA (128 threads, one per point) per block.
+template <bool GGA>
+__global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int blk0, int fn, int incremental,
+                                                              double rho_cut, char* ws, double* rho_store,
+                                                              double* coef, double* blk_sum) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x;
+    const int nplanes = GGA ? 4 : 1;
+    const double* phi = reinterpret_cast<const double*>(ws + m.ws);
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const double* X = phi + nplanes * plane;
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    for (int r = 0; r < m.nb; ++r) {
+        const size_t o = (size_t)r * BLOCK_PTS + p;
+        const double x = X[o];
+        rho = fma(phi[o], x, rho);
+        if (GGA) {
+            gx = fma(phi[plane + o], x, gx);
+            gy = fma(phi[2 * plane + o], x, gy);
+            gz = fma(phi[3 * plane + o], x, gz);
+        }
+    }
+    gx *= 2.0, gy *= 2.0, gz *= 2.0;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    double* rs = rho_store + gp * 4;
+    if (incremental) {
+        rho += rs[0];
+        gx += rs[1], gy += rs[2], gz += rs[3];
+    }
+    rs[0] = rho, rs[1] = gx, rs[2] = gy, rs[3] = gz;
+    const double w = g.pw[gp];
+    double e = 0.0, a = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    if (w != 0.0 && rho > rho_cut) {
+        const double gam = gx * gx + gy * gy + gz * gz;
+        const XcOut o = eval_functional(fn, rho, rho, gam, gam, gam);
+        e = w * o.f;
+        a = 0.5 * w * o.va;
+        if (GGA) {
+            const double cc = w * (2.0 * o.vgaa + o.vgab);
+            cx = cc * gx, cy = cc * gy, cz = cc * gz;
+        }
+    }
+    double* cf = coef + gp * 4;
+    cf[0] = a, cf[1] = cx, cf[2] = cy, cf[3] = cz;
+    // block sums in FP64 (deterministic order)
+    __shared__ double red[2][BLOCK_PTS / 32];
+    double se = warp_sum(e), sn = warp_sum(w * rho);
+    if ((p & 31) == 0) red[0][p >> 5] = se, red[1][p >> 5] = sn;
+    __syncthreads();
+    if (p == 0) {
+        double E = 0.0, N = 0.0;
+        for (int i = 0; i < BLOCK_PTS / 32; ++i) E += red[0][i], N += red[1][i];
+        blk_sum[2 * blk] = E;
+        blk_sum[2 * blk + 1] = N;
+    }
+}
+
+// Vacc[aos[m]][aos[n]] += sum_p phi[m][p] Z[n][p], tile 64 x 64, K = 128 points in steps of 16.
+constexpr int GV_B = 64, GV_BK = 16;
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_gemm_v(GridView g, int blk0, const double* __restrict__ coef,
+                                                char* ws, double* Vacc, int nao, int tiles) {
+    const int blk = blk0 + blockIdx.y;
+    const BlockMeta m = g.meta[blk];
+    const int tm = blockIdx.x / tiles, tn = blockIdx.x % tiles;
+    const int m0 = tm * GV_B, n0 = tn * GV_B;
+    if (m0 >= m.nbp || n0 >= m.nbp) return;
+    const double* phi = reinterpret_cast<const double*>(ws + m.ws);
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const int* aos = g.blk_aos + m.ao0;
+    __shared__ double cf[4][BLOCK_PTS];
+    __shared__ double As[GV_BK][GV_B + 1];
+    __shared__ double Bs[GV_BK][GV_B + 1];
+    const int t = threadIdx.x;
+    for (int e = t; e < 4 * BLOCK_PTS; e += 256) {
+        const int pp = e >> 2, k = e & 3;
+        cf[k][pp] = coef[((size_t)blk * BLOCK_PTS + pp) * 4 + k];
+    }
+    const int tx = t & 15, ty = t >> 4;
+    double acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+    __syncthreads();
+    for (int k0 = 0; k0 < BLOCK_PTS; k0 += GV_BK) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const int e = t + q * 256;
+            const int r = e >> 4, c = e & 15;  // row within tile, point within K step
+            const int pp = k0 + c;
+            As[c][r] = phi[(size_t)(m0 + r) * BLOCK_PTS + pp];
+            const size_t on = (size_t)(n0 + r) * BLOCK_PTS + pp;
+            double z = cf[0][pp] * phi[on];
+            if (GGA)
+                z += cf[1][pp] * phi[plane + on] + cf[2][pp] * phi[2 * plane + on] +
+                     cf[3][pp] * phi[3 * plane + on];
+            Bs[c][r] = z;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < GV_BK; ++kk) {
+            double a[4], b[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const int r = m0 + ty * 4 + i;
+        if (r >= m.nb) continue;
+        const size_t rowoff = (size_t)aos[r] * nao;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int c = n0 + tx + 16 * j;
+            if (c < m.nb) atomicAdd(&Vacc[rowoff + aos[c]], acc[i][j]);
+        }
+    }
+}
+
+__global__ void k_symmetrize(const double* __restrict__ Vacc, double* V, int nao) {
+    const int64_t n2 = (int64_t)nao * nao;
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n2; e += (int64_t)gridDim.x * blockDim.x) {
+        const int i = (int)(e / nao), j = (int)(e % nao);
+        V[e] = Vacc[e] + Vacc[(int64_t)j * nao + i];
+    }
+}
+
+// Deterministic FP64 sum of the per-block partials: one CTA, fixed order.
+__global__ void k_block_sums(const double* __restrict__ blk_sum, int nblk, double* out) {
+    __shared__ double se[256], sn[256];
+    double e = 0.0, n = 0.0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x) e += blk_sum[2 * b], n += blk_sum[2 * b + 1];
+    se[threadIdx.x] = e, sn[threadIdx.x] = n;
+    __syncthreads();
+    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
+        if (threadIdx.x < s) se[threadIdx.x] += se[threadIdx.x + s], sn[threadIdx.x] += sn[threadIdx.x + s];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[0] = se[0], out[1] = sn[0];
+}
+
+}  // namespace
+
+void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, bool gga, char* ws,
+                    int /*max_nsh*/, cudaStream_t s) {
+    if (gga)
+        k_ao_eval<true><<<nblk, 256, 0, s>>>(b, g, blk0, ws);
+    else
+        k_ao_eval<false><<<nblk, 256, 0, s>>>(b, g, blk0, ws);
+}
+
+void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp,
+                          int nplanes, char* ws, cudaStream_t s) {
+    dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk, nplanes);
+    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws);
+}
+
+void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
+                           char* ws, double* rho, double* coef, double* blk_sum, cudaStream_t s) {
+    if (functional_is_gga(fn))
+        k_rho_functional<true><<<nblk, BLOCK_PTS, 0, s>>>(g, blk0, fn, incremental, rho_cut, ws, rho, coef, blk_sum);
+    else
+        k_rho_functional<false><<<nblk, BLOCK_PTS, 0, s>>>(g, blk0, fn, incremental, rho_cut, ws, rho, coef, blk_sum);
+}
+
+void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga, const double* coef, char* ws,
+                   double* Vacc, int nao, cudaStream_t s) {
+    const int tiles = (max_nbp + GV_B - 1) / GV_B;
+    dim3 grid(tiles * tiles, nblk);
+    if (gga)
+        k_gemm_v<true><<<grid, 256, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+    else
+        k_gemm_v<false><<<grid, 256, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+}
+
+void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk, double* scalars,
+                   cudaStream_t s) {
+    k_symmetrize<<<148 * 8, 256, 0, s>>>(Vacc, V, nao);
+    k_block_sums<<<1, 256, 0, s>>>(blk_sum, nblk, scalars);
+}
+
+}  // namespace pdfxc

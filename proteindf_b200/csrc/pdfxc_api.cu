@@ -1,0 +1,610 @@
+// libpdfxc C ABI: context, system and grid set-up (spatial blocking and
+// per-block basis screening, once per geometry) and the per-iteration build
+// orchestration. Every entry point catches C++ exceptions and reports a status.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "functional.cuh"
+#include "pdfxc_internal.cuh"
+
+using pdfxc::BLOCK_PTS;
+using pdfxc::BlockMeta;
+using pdfxc::Chunk;
+
+namespace {
+
+struct CudaError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
+#define PDFXC_CUDA(call)                                                                            \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            throw CudaError(std::string(#call) + ": " + cudaGetErrorString(e_));                    \
+    } while (0)
+
+template <class T>
+void dev_alloc(T** p, size_t n) {
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    if (n == 0) n = 1;
+    cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T));
+    if (e != cudaSuccess) {
+        *p = nullptr;
+        throw std::bad_alloc();
+    }
+}
+
+template <class T>
+void upload(T** p, const std::vector<T>& v, cudaStream_t s) {
+    dev_alloc(p, v.size());
+    if (!v.empty()) PDFXC_CUDA(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+template <class T>
+void dev_free(T*& p) {
+    if (p) cudaFree(p);
+    p = nullptr;
+}
+
+template <class F>
+pdfxc_status guarded(pdfxc_ctx* ctx, F&& f) {
+    if (!ctx) return PDFXC_ERR_ARG;
+    try {
+        cudaSetDevice(ctx->device);
+        return f();
+    } catch (const std::bad_alloc&) {
+        ctx->err = "device or host allocation failed";
+        return PDFXC_ERR_NOMEM;
+    } catch (const CudaError& e) {
+        ctx->err = e.what();
+        return PDFXC_ERR_CUDA;
+    } catch (const std::exception& e) {
+        ctx->err = e.what();
+        return PDFXC_ERR_ARG;
+    }
+}
+
+// Distance beyond which a shell's value and gradient bounds both stay below
+// `cutoff`: bound(r) = sum_k |c_k| e^{-a_k r^2} max(r^L, L r^(L-1) + 2 a_k r^(L+1)).
+double shell_cutoff_radius(int L, const double* e, const double* c, int np, double cutoff) {
+    double R = 0.0;
+    for (double r = 60.0; r > 0.0; r -= 0.01) {
+        double b = 0.0;
+        for (int k = 0; k < np; ++k) {
+            const double rl = std::pow(r, L);
+            const double g = std::max(rl, (L > 0 ? L * std::pow(r, L - 1) : 0.0) + 2.0 * e[k] * rl * r);
+            b += std::fabs(c[k]) * std::exp(-e[k] * r * r) * g;
+        }
+        if (b >= cutoff) {
+            R = r + 0.01;
+            break;
+        }
+    }
+    return R;
+}
+
+uint64_t spread3(uint64_t v) {
+    v &= 0x1fffff;
+    v = (v | v << 32) & 0x1f00000000ffffULL;
+    v = (v | v << 16) & 0x1f0000ff0000ffULL;
+    v = (v | v << 8) & 0x100f00f00f00f00fULL;
+    v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
+    v = (v | v << 2) & 0x1249249249249249ULL;
+    return v;
+}
+
+pdfxc::BasisView basis_view(const pdfxc_ctx* c) {
+    return {c->d_atom_xyz, c->d_sh_atom, c->d_sh_l, c->d_sh_nprim, c->d_sh_p0, c->d_sh_ao0, c->d_p_exp, c->d_p_coef};
+}
+
+pdfxc::GridView grid_view(const pdfxc_ctx* c) {
+    return {c->d_px, c->d_py, c->d_pz, c->d_pw, c->d_meta, c->d_blk_shells, c->d_blk_shell_row, c->d_blk_aos};
+}
+
+void free_grid(pdfxc_ctx* c) {
+    dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
+    dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
+    dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum);
+    if (c->d_ws) cudaFree(c->d_ws);
+    c->d_ws = nullptr;
+    c->nblk = 0;
+    c->npts = 0;
+    c->rho_valid = false;
+}
+
+}  // namespace
+
+extern "C" {
+
+void pdfxc_default_options(pdfxc_options* opt) {
+    if (!opt) return;
+    opt->precision = PDFXC_PRECISION_FP64;
+    opt->block_points = BLOCK_PTS;
+    opt->ao_cutoff = 1e-14;
+    opt->rho_cutoff = 1e-16;
+    opt->workspace_bytes = 0;
+}
+
+pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt) {
+    if (!out) return PDFXC_ERR_ARG;
+    *out = nullptr;
+    pdfxc_ctx* c = new (std::nothrow) pdfxc_ctx();
+    if (!c) return PDFXC_ERR_NOMEM;
+    pdfxc_default_options(&c->opt);
+    if (opt) c->opt = *opt;
+    if (c->opt.block_points <= 0 || c->opt.block_points > BLOCK_PTS) c->opt.block_points = BLOCK_PTS;
+    if (c->opt.workspace_bytes == 0) c->opt.workspace_bytes = size_t(4) << 30;
+    if (c->opt.precision != PDFXC_PRECISION_FP64 && c->opt.precision != PDFXC_PRECISION_MIXED) {
+        delete c;
+        return PDFXC_ERR_ARG;
+    }
+    c->device = device;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
+        delete c;
+        return PDFXC_ERR_CUDA;
+    }
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete c;
+        return PDFXC_ERR_CUDA;
+    }
+    for (auto& e : c->ev) cudaEventCreate(&e);
+    if (cudaMalloc(&c->d_scalars, 2 * sizeof(double)) != cudaSuccess) {
+        pdfxc_destroy(c);
+        return PDFXC_ERR_NOMEM;
+    }
+    *out = c;
+    return PDFXC_OK;
+}
+
+pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz, const int* atom_z, int nshell,
+                              const int* shell_atom, const int* shell_l, const int* shell_nprim,
+                              const double* prim_exp, const double* prim_coef) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (natom <= 0 || nshell <= 0 || !atom_xyz || !shell_atom || !shell_l || !shell_nprim || !prim_exp || !prim_coef) {
+            ctx->err = "pdfxc_set_system: empty system or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        ctx->natom = natom;
+        ctx->nshell = nshell;
+        ctx->h_atom_xyz.assign(atom_xyz, atom_xyz + 3 * natom);
+        ctx->h_atom_z.assign(natom, 0);
+        if (atom_z) ctx->h_atom_z.assign(atom_z, atom_z + natom);
+        ctx->h_sh_atom.assign(shell_atom, shell_atom + nshell);
+        ctx->h_sh_l.assign(shell_l, shell_l + nshell);
+        ctx->h_sh_nprim.assign(shell_nprim, shell_nprim + nshell);
+        ctx->h_sh_p0.resize(nshell);
+        ctx->h_sh_ao0.resize(nshell);
+        int np = 0, ao = 0;
+        for (int s = 0; s < nshell; ++s) {
+            if (shell_l[s] < 0 || shell_l[s] > 2 || shell_nprim[s] <= 0 || shell_atom[s] < 0 || shell_atom[s] >= natom) {
+                ctx->err = "pdfxc_set_system: shell " + std::to_string(s) + " out of range (only s, p, d shells)";
+                return PDFXC_ERR_ARG;
+            }
+            ctx->h_sh_p0[s] = np;
+            ctx->h_sh_ao0[s] = ao;
+            np += shell_nprim[s];
+            ao += 2 * shell_l[s] + 1;
+        }
+        ctx->nao = ao;
+        ctx->h_p_exp.assign(prim_exp, prim_exp + np);
+        ctx->h_p_coef.assign(prim_coef, prim_coef + np);
+        cudaStream_t s = ctx->stream;
+        upload(&ctx->d_atom_xyz, ctx->h_atom_xyz, s);
+        upload(&ctx->d_sh_atom, ctx->h_sh_atom, s);
+        upload(&ctx->d_sh_l, ctx->h_sh_l, s);
+        upload(&ctx->d_sh_nprim, ctx->h_sh_nprim, s);
+        upload(&ctx->d_sh_p0, ctx->h_sh_p0, s);
+        upload(&ctx->d_sh_ao0, ctx->h_sh_ao0, s);
+        upload(&ctx->d_p_exp, ctx->h_p_exp, s);
+        upload(&ctx->d_p_coef, ctx->h_p_coef, s);
+        const size_t n2 = (size_t)ao * ao;
+        dev_alloc(&ctx->d_P, n2);
+        dev_alloc(&ctx->d_V, n2);
+        dev_alloc(&ctx->d_Vacc, n2);
+        PDFXC_CUDA(cudaStreamSynchronize(s));
+        free_grid(ctx);
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->nao == 0) {
+            ctx->err = "pdfxc_set_grid: call pdfxc_set_system first";
+            return PDFXC_ERR_STATE;
+        }
+        if (npts <= 0 || !xyzw) {
+            ctx->err = "pdfxc_set_grid: empty grid or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        (void)atom;  // the owning atom is not needed by the quadrature itself
+        free_grid(ctx);
+        const int bp = ctx->opt.block_points;
+        // 1. spatial order: Morton code over the grid's bounding box
+        double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+        for (int64_t i = 0; i < npts; ++i)
+            for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], xyzw[4 * i + k]), hi[k] = std::max(hi[k], xyzw[4 * i + k]);
+        double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-12});
+        std::vector<std::pair<uint64_t, int64_t>> key(npts);
+        for (int64_t i = 0; i < npts; ++i) {
+            uint64_t q[3];
+            for (int k = 0; k < 3; ++k)
+                q[k] = (uint64_t)std::min(2097151.0, std::floor((xyzw[4 * i + k] - lo[k]) / span * 2097151.0));
+            key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, i};
+        }
+        std::sort(key.begin(), key.end());
+        const int nblk = (int)((npts + bp - 1) / bp);
+        std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
+        ctx->h_src.assign(px.size(), -1);
+        std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
+        ctx->h_meta.assign(nblk, BlockMeta{});
+        for (int b = 0; b < nblk; ++b) {
+            const int64_t i0 = (int64_t)b * bp, i1 = std::min<int64_t>(npts, i0 + bp);
+            double c[3] = {0, 0, 0};
+            for (int64_t i = i0; i < i1; ++i)
+                for (int k = 0; k < 3; ++k) c[k] += xyzw[4 * key[i].second + k];
+            for (int k = 0; k < 3; ++k) c[k] /= double(i1 - i0);
+            double r2 = 0.0;
+            for (int j = 0; j < BLOCK_PTS; ++j) {
+                const size_t slot = (size_t)b * BLOCK_PTS + j;
+                const int64_t i = i0 + j;
+                if (i < i1) {
+                    const double* r = xyzw + 4 * key[i].second;
+                    px[slot] = r[0], py[slot] = r[1], pz[slot] = r[2], pw[slot] = r[3];
+                    ctx->h_src[slot] = key[i].second;
+                    r2 = std::max(r2, (r[0] - c[0]) * (r[0] - c[0]) + (r[1] - c[1]) * (r[1] - c[1]) + (r[2] - c[2]) * (r[2] - c[2]));
+                } else {
+                    px[slot] = c[0], py[slot] = c[1], pz[slot] = c[2], pw[slot] = 0.0;
+                }
+            }
+            for (int k = 0; k < 3; ++k) cen[3 * b + k] = c[k];
+            rad[b] = std::sqrt(r2);
+            ctx->h_meta[b].npts = (int)(i1 - i0);
+        }
+        // 2. per-shell screening radius, then the per-block shell lists
+        std::vector<double> Rs(ctx->nshell);
+        for (int s = 0; s < ctx->nshell; ++s)
+            Rs[s] = shell_cutoff_radius(ctx->h_sh_l[s], &ctx->h_p_exp[ctx->h_sh_p0[s]], &ctx->h_p_coef[ctx->h_sh_p0[s]],
+                                        ctx->h_sh_nprim[s], ctx->opt.ao_cutoff);
+        std::vector<int> shells, rows, aos;
+        const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
+        double flops = 0.0, sum_nb = 0.0;
+        for (int b = 0; b < nblk; ++b) {
+            BlockMeta& m = ctx->h_meta[b];
+            m.sh0 = (int)shells.size();
+            m.ao0 = (int)aos.size();
+            int row = 0;
+            for (int s = 0; s < ctx->nshell; ++s) {
+                const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[s]];
+                const double d = std::sqrt((A[0] - cen[3 * b]) * (A[0] - cen[3 * b]) + (A[1] - cen[3 * b + 1]) * (A[1] - cen[3 * b + 1]) +
+                                           (A[2] - cen[3 * b + 2]) * (A[2] - cen[3 * b + 2]));
+                if (d - rad[b] > Rs[s]) continue;
+                shells.push_back(s);
+                rows.push_back(row);
+                const int n = 2 * ctx->h_sh_l[s] + 1;
+                for (int c = 0; c < n; ++c) aos.push_back(ctx->h_sh_ao0[s] + c);
+                row += n;
+            }
+            m.nsh = (int)shells.size() - m.sh0;
+            m.nb = row;
+            m.nbp = std::max(64, (row + 63) / 64 * 64);
+            flops += 4.0 * double(m.nb) * m.nb * m.npts;
+            sum_nb += m.nb;
+        }
+        // 3. chunks of blocks whose intermediates fit the workspace budget
+        ctx->chunks.clear();
+        size_t off = 0, max_ws = 0;
+        Chunk cur{0, 0, 0, 0};
+        for (int b = 0; b < nblk; ++b) {
+            const size_t need = pdfxc::block_ws_doubles(ctx->h_meta[b].nbp, gga_ws) * sizeof(double);
+            if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
+                cur.b1 = b;
+                cur.ws_bytes = off;
+                ctx->chunks.push_back(cur);
+                max_ws = std::max(max_ws, off);
+                cur = Chunk{b, b, 0, 0};
+                off = 0;
+            }
+            ctx->h_meta[b].ws = (int64_t)off;
+            off += need;
+            cur.max_nbp = std::max(cur.max_nbp, ctx->h_meta[b].nbp);
+        }
+        cur.b1 = nblk;
+        cur.ws_bytes = off;
+        ctx->chunks.push_back(cur);
+        max_ws = std::max(max_ws, off);
+
+        cudaStream_t s = ctx->stream;
+        upload(&ctx->d_px, px, s);
+        upload(&ctx->d_py, py, s);
+        upload(&ctx->d_pz, pz, s);
+        upload(&ctx->d_pw, pw, s);
+        upload(&ctx->d_meta, ctx->h_meta, s);
+        upload(&ctx->d_blk_shells, shells, s);
+        upload(&ctx->d_blk_shell_row, rows, s);
+        upload(&ctx->d_blk_aos, aos, s);
+        dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
+        dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
+        dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho, 0, sizeof(double) * (size_t)nblk * BLOCK_PTS * 4, s));
+        if (cudaMalloc(&ctx->d_ws, max_ws) != cudaSuccess) {
+            ctx->d_ws = nullptr;
+            throw std::bad_alloc();
+        }
+        ctx->ws_bytes = max_ws;
+        ctx->nblk = nblk;
+        ctx->npts = npts;
+        ctx->contraction_flops = flops;
+        ctx->mean_nb = sum_nb / nblk;
+        PDFXC_CUDA(cudaStreamSynchronize(s));
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
+                                 const double* w_single, const double* becke_radius, int size_adjust, double* w_out) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->natom == 0) {
+            ctx->err = "pdfxc_becke_weights: call pdfxc_set_system first";
+            return PDFXC_ERR_STATE;
+        }
+        if (npts <= 0 || !xyz || !atom || !w_single || !becke_radius || !w_out) {
+            ctx->err = "pdfxc_becke_weights: empty input or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        for (int64_t i = 0; i < npts; ++i)
+            if (atom[i] < 0 || atom[i] >= ctx->natom) {
+                ctx->err = "pdfxc_becke_weights: owner atom index out of range";
+                return PDFXC_ERR_ARG;
+            }
+        cudaStream_t s = ctx->stream;
+        double *d_xyz = nullptr, *d_ws = nullptr, *d_wo = nullptr, *d_br = nullptr;
+        int* d_own = nullptr;
+        try {
+            dev_alloc(&d_xyz, 3 * (size_t)npts);
+            dev_alloc(&d_ws, (size_t)npts);
+            dev_alloc(&d_wo, (size_t)npts);
+            dev_alloc(&d_br, (size_t)ctx->natom);
+            dev_alloc(&d_own, (size_t)npts);
+            PDFXC_CUDA(cudaMemcpyAsync(d_xyz, xyz, 3 * sizeof(double) * npts, cudaMemcpyHostToDevice, s));
+            PDFXC_CUDA(cudaMemcpyAsync(d_ws, w_single, sizeof(double) * npts, cudaMemcpyHostToDevice, s));
+            PDFXC_CUDA(cudaMemcpyAsync(d_br, becke_radius, sizeof(double) * ctx->natom, cudaMemcpyHostToDevice, s));
+            PDFXC_CUDA(cudaMemcpyAsync(d_own, atom, sizeof(int) * npts, cudaMemcpyHostToDevice, s));
+            pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, npts, d_xyz, d_own, d_ws, d_wo, s);
+            PDFXC_CUDA(cudaGetLastError());
+            PDFXC_CUDA(cudaMemcpyAsync(w_out, d_wo, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
+            PDFXC_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own);
+            throw;
+        }
+        dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own);
+        return PDFXC_OK;
+    });
+}
+
+}  // extern "C"
+
+namespace {
+
+// Enqueue one build on ctx->stream: d_PA -> ctx->d_V (= Vxc), scalars -> ctx->d_scalars.
+void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental) {
+    cudaStream_t s = ctx->stream;
+    const bool gga = pdfxc::functional_is_gga(fn);
+    const int nao = ctx->nao;
+    const pdfxc::BasisView bv = basis_view(ctx);
+    const pdfxc::GridView gv = grid_view(ctx);
+    char* ws = static_cast<char*>(ctx->d_ws);
+    const size_t nev = 5 * ctx->chunks.size() + 1;
+    while (ctx->stage_ev.size() < nev) {
+        cudaEvent_t e;
+        PDFXC_CUDA(cudaEventCreate(&e));
+        ctx->stage_ev.push_back(e);
+    }
+    PDFXC_CUDA(cudaEventRecord(ctx->ev[0], s));
+    PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc, 0, sizeof(double) * (size_t)nao * nao, s));
+    int64_t launches = 0;
+    for (size_t ci = 0; ci < ctx->chunks.size(); ++ci) {
+        const Chunk& c = ctx->chunks[ci];
+        cudaEvent_t* e = &ctx->stage_ev[5 * ci];
+        const int nb = c.b1 - c.b0;
+        PDFXC_CUDA(cudaEventRecord(e[0], s));
+        pdfxc::launch_ao_eval(bv, gv, c.b0, nb, gga, ws, 0, s);
+        PDFXC_CUDA(cudaEventRecord(e[1], s));
+        pdfxc::launch_gemm_x(gv, d_PA, nao, c.b0, nb, c.max_nbp, gga ? 4 : 1, ws, s);
+        PDFXC_CUDA(cudaEventRecord(e[2], s));
+        pdfxc::launch_rho_functional(gv, c.b0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho, ctx->d_coef,
+                                     ctx->d_blk_sum, s);
+        PDFXC_CUDA(cudaEventRecord(e[3], s));
+        pdfxc::launch_gemm_v(gv, c.b0, nb, c.max_nbp, gga, ctx->d_coef, ws, ctx->d_Vacc, nao, s);
+        PDFXC_CUDA(cudaEventRecord(e[4], s));
+        launches += 4;
+    }
+    pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum, ctx->nblk, ctx->d_scalars, s);
+    launches += 2;
+    PDFXC_CUDA(cudaGetLastError());
+    PDFXC_CUDA(cudaEventRecord(ctx->stage_ev[nev - 1], s));
+    PDFXC_CUDA(cudaEventRecord(ctx->ev[1], s));
+    ctx->last_profile.launches = launches;
+}
+
+// After the stream has synchronised: fold the stage events into last_profile.
+void collect_profile(pdfxc_ctx* ctx) {
+    pdfxc_profile& p = ctx->last_profile;
+    p.total_ms = p.ao_ms = p.gemm_x_ms = p.rho_ms = p.gemm_v_ms = p.finish_ms = 0.f;
+    PDFXC_CUDA(cudaEventElapsedTime(&p.total_ms, ctx->ev[0], ctx->ev[1]));
+    auto dt = [](cudaEvent_t a, cudaEvent_t b) {
+        float t = 0.f;
+        PDFXC_CUDA(cudaEventElapsedTime(&t, a, b));
+        return t;
+    };
+    for (size_t ci = 0; ci < ctx->chunks.size(); ++ci) {
+        cudaEvent_t* e = &ctx->stage_ev[5 * ci];
+        p.ao_ms += dt(e[0], e[1]);
+        p.gemm_x_ms += dt(e[1], e[2]);
+        p.rho_ms += dt(e[2], e[3]);
+        p.gemm_v_ms += dt(e[3], e[4]);
+    }
+    const size_t last = 5 * ctx->chunks.size();
+    p.finish_ms = dt(ctx->stage_ev[last - 1], ctx->stage_ev[last]);
+}
+
+pdfxc_status check_build(pdfxc_ctx* ctx, int functional, int incremental) {
+    if (ctx->nblk == 0) {
+        ctx->err = "pdfxc_build_vxc: call pdfxc_set_system and pdfxc_set_grid first";
+        return PDFXC_ERR_STATE;
+    }
+    if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP) {
+        ctx->err = "pdfxc_build_vxc: unknown functional id " + std::to_string(functional);
+        return PDFXC_ERR_ARG;
+    }
+    if (incremental && (!ctx->rho_valid || ctx->rho_gga != (int)pdfxc::functional_is_gga(functional))) {
+        ctx->err = "pdfxc_build_vxc: incremental build needs a previous build (or pdfxc_set_rho) of the same functional type";
+        return PDFXC_ERR_STATE;
+    }
+    return PDFXC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double* d_PA, int incremental, double* d_V,
+                                    double* exc, double* nelec_alpha) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        pdfxc_status st = check_build(ctx, functional, incremental);
+        if (st) return st;
+        if (!d_PA || !d_V) {
+            ctx->err = "pdfxc_build_vxc_device: null device pointer";
+            return PDFXC_ERR_ARG;
+        }
+        enqueue_build(ctx, functional, d_PA, incremental != 0);
+        const size_t n2 = (size_t)ctx->nao * ctx->nao;
+        PDFXC_CUDA(cudaMemcpyAsync(d_V, ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        double sc[2];
+        PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        collect_profile(ctx);
+        if (exc) *exc = sc[0];
+        if (nelec_alpha) *nelec_alpha = sc[1];
+        ctx->rho_valid = true;
+        ctx->rho_gga = pdfxc::functional_is_gga(functional);
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, int incremental, double* F, double* exc,
+                             double* nelec_alpha) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        pdfxc_status st = check_build(ctx, functional, incremental);
+        if (st) return st;
+        if (!PA || !F) {
+            ctx->err = "pdfxc_build_vxc: null host pointer";
+            return PDFXC_ERR_ARG;
+        }
+        const size_t n2 = (size_t)ctx->nao * ctx->nao;
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, n2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        enqueue_build(ctx, functional, ctx->d_P, incremental != 0);
+        std::vector<double> V(n2);
+        double sc[2];
+        PDFXC_CUDA(cudaMemcpyAsync(V.data(), ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        collect_profile(ctx);
+        for (size_t i = 0; i < n2; ++i) F[i] += V[i];
+        if (exc) *exc = sc[0];
+        if (nelec_alpha) *nelec_alpha = sc[1];
+        ctx->rho_valid = true;
+        ctx->rho_gga = pdfxc::functional_is_gga(functional);
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_get_rho(pdfxc_ctx* ctx, int gga, double* rho) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!rho) return PDFXC_ERR_ARG;
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_get_rho: no grid";
+            return PDFXC_ERR_STATE;
+        }
+        std::vector<double> r((size_t)ctx->nblk * BLOCK_PTS * 4);
+        PDFXC_CUDA(cudaMemcpyAsync(r.data(), ctx->d_rho, r.size() * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        const int nc = gga ? 4 : 1;
+        for (size_t slot = 0; slot < ctx->h_src.size(); ++slot) {
+            const int64_t i = ctx->h_src[slot];
+            if (i < 0) continue;
+            for (int k = 0; k < nc; ++k) rho[i * nc + k] = r[slot * 4 + k];
+        }
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!rho) return PDFXC_ERR_ARG;
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_set_rho: no grid";
+            return PDFXC_ERR_STATE;
+        }
+        std::vector<double> r((size_t)ctx->nblk * BLOCK_PTS * 4, 0.0);
+        const int nc = gga ? 4 : 1;
+        for (size_t slot = 0; slot < ctx->h_src.size(); ++slot) {
+            const int64_t i = ctx->h_src[slot];
+            if (i < 0) continue;
+            for (int k = 0; k < nc; ++k) r[slot * 4 + k] = rho[i * nc + k];
+        }
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_rho, r.data(), r.size() * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->rho_valid = true;
+        ctx->rho_gga = gga ? 1 : 0;
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_grid_stats(pdfxc_ctx* ctx, int64_t* nblocks, int64_t* npts_padded, double* contraction_flops,
+                              double* mean_nb) {
+    if (!ctx) return PDFXC_ERR_ARG;
+    if (nblocks) *nblocks = ctx->nblk;
+    if (npts_padded) *npts_padded = (int64_t)ctx->nblk * BLOCK_PTS;
+    if (contraction_flops) *contraction_flops = ctx->contraction_flops;
+    if (mean_nb) *mean_nb = ctx->mean_nb;
+    return PDFXC_OK;
+}
+
+pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out) {
+    if (!ctx || !out) return PDFXC_ERR_ARG;
+    *out = ctx->last_profile;
+    return PDFXC_OK;
+}
+
+const char* pdfxc_last_error(const pdfxc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
+
+void pdfxc_destroy(pdfxc_ctx* ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    free_grid(ctx);
+    dev_free(ctx->d_atom_xyz), dev_free(ctx->d_p_exp), dev_free(ctx->d_p_coef);
+    dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
+    dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars);
+    for (auto& e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->stage_ev) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+}  // extern "C"

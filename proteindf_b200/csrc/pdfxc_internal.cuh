@@ -1,0 +1,136 @@
+// Internal structures of libpdfxc: the device-resident system, the blocked
+// grid, and the launch interfaces of the kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/pdfxc.h"
+
+namespace pdfxc {
+
+constexpr int BLOCK_PTS = 128;  // grid points per block (padded with zero weight)
+
+// One spatial block of grid points and its screened basis.
+// Points live at [blk * BLOCK_PTS, (blk + 1) * BLOCK_PTS) of the SoA point arrays.
+struct BlockMeta {
+    int sh0;       // first entry in blk_shells / blk_shell_row
+    int nsh;       // screened shells
+    int ao0;       // first entry in blk_aos
+    int nb;        // screened AOs
+    int nbp;       // nb rounded up to the contraction tile
+    int npts;      // real points in the block (<= BLOCK_PTS)
+    int64_t ws;    // byte offset of this block's intermediates inside its chunk's workspace
+};
+
+// A contiguous range of blocks whose intermediates fit the workspace together.
+struct Chunk {
+    int b0, b1;
+    int max_nbp;
+    size_t ws_bytes;
+};
+
+// Device views of the basis (shell-major structure of arrays).
+struct BasisView {
+    const double* atom_xyz;
+    const int* sh_atom;
+    const int* sh_l;
+    const int* sh_nprim;
+    const int* sh_p0;
+    const int* sh_ao0;
+    const double* p_exp;
+    const double* p_coef;
+};
+
+// Device views of the blocked grid.
+struct GridView {
+    const double* px;  // [nblk * BLOCK_PTS]
+    const double* py;
+    const double* pz;
+    const double* pw;
+    const BlockMeta* meta;
+    const int* blk_shells;     // shell id
+    const int* blk_shell_row;  // local AO row of the shell's first component
+    const int* blk_aos;        // global AO index of each local row
+};
+
+}  // namespace pdfxc
+
+struct pdfxc_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    pdfxc_options opt{};
+    std::string err;
+
+    // system
+    int natom = 0, nshell = 0, nao = 0;
+    std::vector<double> h_atom_xyz;
+    std::vector<int> h_atom_z, h_sh_atom, h_sh_l, h_sh_nprim, h_sh_p0, h_sh_ao0;
+    std::vector<double> h_p_exp, h_p_coef;
+    double *d_atom_xyz = nullptr, *d_p_exp = nullptr, *d_p_coef = nullptr;
+    int *d_sh_atom = nullptr, *d_sh_l = nullptr, *d_sh_nprim = nullptr, *d_sh_p0 = nullptr,
+        *d_sh_ao0 = nullptr;
+
+    // blocked grid
+    int64_t npts = 0;
+    int nblk = 0;
+    std::vector<pdfxc::BlockMeta> h_meta;
+    std::vector<pdfxc::Chunk> chunks;
+    std::vector<int64_t> h_src;  // original index of each padded point slot (-1 = padding)
+    double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_pw = nullptr;
+    pdfxc::BlockMeta* d_meta = nullptr;
+    int *d_blk_shells = nullptr, *d_blk_shell_row = nullptr, *d_blk_aos = nullptr;
+    double contraction_flops = 0.0;
+    double mean_nb = 0.0;
+
+    // per-build buffers
+    void* d_ws = nullptr;
+    size_t ws_bytes = 0;
+    double* d_rho = nullptr;    // [nblk * BLOCK_PTS * 4]: rho, grad x, y, z
+    double* d_coef = nullptr;   // [nblk * BLOCK_PTS * 4]: 0.5 w vrho, c_x, c_y, c_z
+    double* d_blk_sum = nullptr;  // [nblk * 2]: per-block Exc, Nel
+    double* d_scalars = nullptr;  // [2]
+    double* d_P = nullptr;        // n_ao^2 staging for host-pointer builds
+    double* d_V = nullptr;        // n_ao^2
+    double* d_Vacc = nullptr;     // n_ao^2 non-symmetric accumulator
+    bool rho_valid = false;
+    int rho_gga = 0;
+
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    // stage events: per chunk 5 (before ao, gemm_x, rho, gemm_v, after gemm_v), then finish end
+    std::vector<cudaEvent_t> stage_ev;
+    pdfxc_profile last_profile{};
+};
+
+namespace pdfxc {
+
+// kernels_fp64.cu
+void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, bool gga,
+                    char* ws, int max_nsh, cudaStream_t s);
+void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp,
+                   int nplanes, char* ws, cudaStream_t s);
+void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental,
+                           double rho_cut, char* ws, double* rho, double* coef, double* blk_sum,
+                           cudaStream_t s);
+void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga, const double* coef,
+                   char* ws, double* Vacc, int nao, cudaStream_t s);
+void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk,
+                   double* scalars, cudaStream_t s);
+
+// becke.cu
+void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust,
+                  int64_t npts, const double* xyz, const int* owner, const double* w_single,
+                  double* w_out, cudaStream_t s);
+
+// Intermediates of one block inside its chunk workspace (doubles):
+//   phi   [nbp][BLOCK_PTS]           AO values, row = local AO
+//   dphi  [3][nbp][BLOCK_PTS]        gradients (GGA only)
+//   X     [nbp][BLOCK_PTS]           P_sub * phi
+__host__ __device__ inline size_t block_ws_doubles(int nbp, bool gga) {
+    return (size_t)nbp * BLOCK_PTS * (gga ? 5 : 2);
+}
+
+}  // namespace pdfxc

@@ -1,0 +1,187 @@
+"""ctypes front end of libpdfxc (the C ABI in include/pdfxc.h).
+
+The library is loaded from proteindf_b200/lib/libpdfxc.so; there is no
+fallback: if it is missing or a call fails, a RuntimeError says why.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libpdfxc.so")
+
+FUNCTIONALS = {"SVWN": 0, "HFS": 1, "HFB": 2, "BLYP": 3, "B88LYP": 3, "B3LYP": 4}
+GGA = {"HFB", "BLYP", "B88LYP", "B3LYP"}
+PRECISION = {"fp64": 0, "mixed": 1}
+
+# Every entry point include/pdfxc.h declares.
+EXPORTS = [
+    "pdfxc_default_options", "pdfxc_create", "pdfxc_set_system", "pdfxc_set_grid", "pdfxc_becke_weights",
+    "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
+    "pdfxc_last_profile", "pdfxc_last_error", "pdfxc_destroy",
+]
+
+
+class Options(ctypes.Structure):
+    _fields_ = [("precision", ctypes.c_int), ("block_points", ctypes.c_int), ("ao_cutoff", ctypes.c_double),
+                ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t)]
+
+
+class Profile(ctypes.Structure):
+    _fields_ = [("total_ms", ctypes.c_float), ("ao_ms", ctypes.c_float), ("gemm_x_ms", ctypes.c_float),
+                ("rho_ms", ctypes.c_float), ("gemm_v_ms", ctypes.c_float), ("finish_ms", ctypes.c_float),
+                ("launches", ctypes.c_int64)]
+
+
+_lib = None
+_vp = ctypes.c_void_p
+
+
+def load_library(path=LIB_PATH):
+    """Load libpdfxc.so and declare the C ABI's signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"libpdfxc.so not built ({path}); run `python -c 'import __graft_entry__ as g; g.build()'`")
+    L = ctypes.CDLL(path)
+    i32, i64, f64 = ctypes.c_int, ctypes.c_int64, ctypes.c_double
+    L.pdfxc_default_options.argtypes = [ctypes.POINTER(Options)]
+    L.pdfxc_create.argtypes = [ctypes.POINTER(_vp), i32, ctypes.POINTER(Options)]
+    L.pdfxc_set_system.argtypes = [_vp, i32, _vp, _vp, i32, _vp, _vp, _vp, _vp, _vp]
+    L.pdfxc_set_grid.argtypes = [_vp, i64, _vp, _vp]
+    L.pdfxc_becke_weights.argtypes = [_vp, i64, _vp, _vp, _vp, _vp, i32, _vp]
+    L.pdfxc_build_vxc.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
+    L.pdfxc_build_vxc_device.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
+    L.pdfxc_get_rho.argtypes = [_vp, i32, _vp]
+    L.pdfxc_set_rho.argtypes = [_vp, i32, _vp]
+    L.pdfxc_grid_stats.argtypes = [_vp, _vp, _vp, _vp, _vp]
+    L.pdfxc_last_profile.argtypes = [_vp, _vp]
+    L.pdfxc_last_error.argtypes = [_vp]
+    L.pdfxc_last_error.restype = ctypes.c_char_p
+    L.pdfxc_destroy.argtypes = [_vp]
+    L.pdfxc_destroy.restype = None
+    for name in EXPORTS:
+        if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
+            getattr(L, name).restype = i32
+    L.pdfxc_default_options.restype = None
+    _lib = L
+    return L
+
+
+def _ptr(a):
+    return a.ctypes.data_as(_vp)
+
+
+class XcEngine:
+    """One libpdfxc context on one GPU.
+
+    >>> eng = XcEngine(precision="fp64")
+    >>> eng.set_system(shell_table)
+    >>> eng.set_grid(xyzw, atom)
+    >>> exc, nel, V = eng.build_vxc("B3LYP", PA)
+    """
+
+    def __init__(self, device=0, precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16,
+                 workspace_bytes=0):
+        self.L = load_library()
+        opt = Options()
+        self.L.pdfxc_default_options(ctypes.byref(opt))
+        opt.precision = PRECISION[precision]
+        opt.block_points = block_points
+        opt.ao_cutoff = ao_cutoff
+        opt.rho_cutoff = rho_cutoff
+        opt.workspace_bytes = workspace_bytes
+        h = _vp()
+        st = self.L.pdfxc_create(ctypes.byref(h), device, ctypes.byref(opt))
+        if st != 0:
+            raise RuntimeError(f"pdfxc_create failed with status {st}")
+        self.h = h
+        self.nao = 0
+        self.npts = 0
+
+    def _check(self, st, what):
+        if st != 0:
+            msg = self.L.pdfxc_last_error(self.h)
+            raise RuntimeError(f"{what}: status {st}: {msg.decode() if msg else ''}")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.pdfxc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_system(self, sh):
+        """sh: proteindf_b200.basis.ShellTable."""
+        self._keep = [np.ascontiguousarray(a) for a in (
+            sh.atom_xyz.astype(np.float64), sh.atom_z.astype(np.int32), sh.shell_atom.astype(np.int32),
+            sh.shell_l.astype(np.int32), sh.shell_nprim.astype(np.int32), sh.prim_exp.astype(np.float64),
+            sh.prim_coef.astype(np.float64))]
+        k = self._keep
+        self._check(self.L.pdfxc_set_system(self.h, sh.natom, _ptr(k[0]), _ptr(k[1]), sh.nshell, _ptr(k[2]),
+                                            _ptr(k[3]), _ptr(k[4]), _ptr(k[5]), _ptr(k[6])), "pdfxc_set_system")
+        self.nao = sh.nao
+
+    def set_grid(self, xyzw, atom=None):
+        xyzw = np.ascontiguousarray(xyzw, dtype=np.float64).reshape(-1, 4)
+        atom = np.zeros(len(xyzw), np.int32) if atom is None else np.ascontiguousarray(atom, dtype=np.int32)
+        self._check(self.L.pdfxc_set_grid(self.h, len(xyzw), _ptr(xyzw), _ptr(atom)), "pdfxc_set_grid")
+        self.npts = len(xyzw)
+
+    def becke_weights(self, xyz, atom, w_single, becke_radius, size_adjust=True):
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        atom = np.ascontiguousarray(atom, dtype=np.int32)
+        ws = np.ascontiguousarray(w_single, dtype=np.float64)
+        br = np.ascontiguousarray(becke_radius, dtype=np.float64)
+        out = np.zeros(len(xyz))
+        self._check(self.L.pdfxc_becke_weights(self.h, len(xyz), _ptr(xyz), _ptr(atom), _ptr(ws), _ptr(br),
+                                               int(size_adjust), _ptr(out)), "pdfxc_becke_weights")
+        return out
+
+    def build_vxc(self, functional, PA, incremental=False, F=None):
+        """Host build. Returns (exc, nelec_alpha, F) with F += Vxc (a new zero matrix if F is None)."""
+        PA = np.ascontiguousarray(PA, dtype=np.float64)
+        if F is None:
+            F = np.zeros((self.nao, self.nao))
+        assert F.flags.c_contiguous and F.dtype == np.float64
+        exc = ctypes.c_double()
+        nel = ctypes.c_double()
+        self._check(self.L.pdfxc_build_vxc(self.h, FUNCTIONALS[functional], _ptr(PA), int(incremental), _ptr(F),
+                                           ctypes.byref(exc), ctypes.byref(nel)), "pdfxc_build_vxc")
+        return exc.value, nel.value, F
+
+    def build_vxc_device(self, functional, d_PA_ptr, d_V_ptr, incremental=False):
+        """Device build on raw device pointers (e.g. torch tensor .data_ptr()). Returns (exc, nelec_alpha)."""
+        exc = ctypes.c_double()
+        nel = ctypes.c_double()
+        self._check(self.L.pdfxc_build_vxc_device(self.h, FUNCTIONALS[functional], _vp(d_PA_ptr), int(incremental),
+                                                  _vp(d_V_ptr), ctypes.byref(exc), ctypes.byref(nel)),
+                    "pdfxc_build_vxc_device")
+        return exc.value, nel.value
+
+    def get_rho(self, gga):
+        out = np.zeros((self.npts, 4 if gga else 1))
+        self._check(self.L.pdfxc_get_rho(self.h, int(gga), _ptr(out)), "pdfxc_get_rho")
+        return out
+
+    def set_rho(self, rho, gga):
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        self._check(self.L.pdfxc_set_rho(self.h, int(gga), _ptr(rho)), "pdfxc_set_rho")
+
+    def grid_stats(self):
+        nb, npad = ctypes.c_int64(), ctypes.c_int64()
+        fl, mnb = ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.pdfxc_grid_stats(self.h, ctypes.byref(nb), ctypes.byref(npad), ctypes.byref(fl),
+                                            ctypes.byref(mnb)), "pdfxc_grid_stats")
+        return {"nblocks": nb.value, "npts_padded": npad.value, "contraction_flops": fl.value, "mean_nb": mnb.value}
+
+    def last_profile(self):
+        p = Profile()
+        self._check(self.L.pdfxc_last_profile(self.h, ctypes.byref(p)), "pdfxc_last_profile")
+        return {k: getattr(p, k) for k, _ in Profile._fields_}

@@ -1,0 +1,98 @@
+"""Generate the reference golden fixtures for the parity tests.
+
+Runs the ProteinDF reference itself (oracle/_ref/pdfxc_ref, built from the
+reference sources by oracle/ref/Makefile) on small seeded systems and stores
+its inputs and outputs as compressed .npz files beside this script:
+
+  ref_water2.npz   (H2O)2, cc-pVDZ (48 AOs), USER 75x302 GC-TA grid with Becke
+                   partitioning: single-centre and Becke weights of a point
+                   sample, the reference's final grid (a seeded sample of it),
+                   and per functional (SVWN, HFS, HFB, BLYP, B3LYP) Exc, Vxc,
+                   rho / grad rho; AO table and AO values at five points.
+  ref_chain12.npz  a 12-atom C/N/O/H chain, cc-pVDZ, same grid recipe, B3LYP
+                   and SVWN on a point sample.
+  ref_functionals.npz  functional values and first derivatives of all five
+                   functionals on a seeded log-uniform (rho, gamma) set, both
+                   the open-shell and the closed-shell overloads.
+
+usage (needs the reference tree): make -C oracle/ref && python tests/golden/make_ref_fixtures.py
+"""
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.abspath(os.path.join(HERE, "..", ".."))
+sys.path.insert(0, ROOT)
+from oracle import refio  # noqa: E402
+from proteindf_b200 import basis, systems  # noqa: E402
+
+GRID = {"nrad": 75, "nang": 302, "radial": "GC", "gc_mapping": "TA", "partition": "Becke", "pruning": "yes"}
+FUNCS = ["SVWN", "HFS", "HFB", "BLYP", "B3LYP"]
+
+
+def system_fixture(name, syms, xyz, nsample, funcs, nocc, seed):
+    b = basis.load_basis("cc-pVDZ")
+    q = systems.nuclear_charges(syms)
+    rng = np.random.default_rng(seed)
+    out = {"symbols": np.array(syms), "xyz": xyz, "grid_params": np.array([f"{k}={v}" for k, v in GRID.items()])}
+    with tempfile.TemporaryDirectory() as d:
+        g = refio.run_grid(d, syms, q, xyz, b, GRID)
+        pts = g["points"].reshape(-1, 3)
+        sel = np.sort(rng.choice(len(pts), min(4000, len(pts)), replace=False))
+        out["becke_points"] = pts[sel]
+        out["becke_atom"] = g["atom"][sel].astype(np.int32)
+        out["becke_w_single"] = g["w_single"][sel]
+        out["becke_w_final"] = g["w_final"][sel]
+        out["radii"] = g["radii"].reshape(-1, 2)  # Bragg-Slater, Becke radius per atom
+        full = g["grid"].reshape(-1, 5)
+        out["grid_npts_full"] = np.array(len(full))
+        out["grid_wsum_full"] = np.array(full[:, 3].sum())
+        sel = np.sort(rng.choice(len(full), min(nsample, len(full)), replace=False))
+        grid = full[sel]
+        out["grid"] = grid
+        sh = basis.ShellTable(syms, xyz, b)
+        P = systems.density_matrix(sh.nao, nocc, seed=seed)
+        PA = 0.5 * P
+        out["PA"] = PA
+        for fn in funcs:
+            r = refio.run_xc(d, syms, q, xyz, b, fn, grid, PA, ao_dump=5)
+            out[f"{fn}_exc"] = r["exc"]
+            out[f"{fn}_vxc"] = r["vxc"].reshape(sh.nao, sh.nao)
+            out[f"{fn}_rho"] = r["rho"].reshape(len(grid), -1)
+            out[f"{fn}_nelec_alpha"] = r["nelec_alpha"]
+        for k in ("ao_atom", "ao_type", "ao_nprim", "ao_exp", "ao_coef", "phi", "dphi"):
+            out[k] = r[k]
+    np.savez_compressed(os.path.join(HERE, name), **out)
+
+
+def functional_fixture():
+    rng = np.random.default_rng(7)
+    n = 400
+    ra = 10 ** rng.uniform(-12, 2, n)
+    rb = np.where(rng.random(n) < 0.5, ra, 10 ** rng.uniform(-12, 2, n))
+    gaa = 10 ** rng.uniform(-14, 3, n)
+    gbb = np.where(rb == ra, gaa, 10 ** rng.uniform(-14, 3, n))
+    gab = np.where(rb == ra, gaa, np.sqrt(gaa * gbb) * rng.uniform(-1, 1, n))
+    inp = np.stack([ra, rb, gaa, gab, gbb], axis=1)
+    out = {"inputs": inp}
+    with tempfile.TemporaryDirectory() as d:
+        for fn in FUNCS:
+            out[fn] = refio.run_func(d, fn, inp)
+    np.savez_compressed(os.path.join(HERE, "ref_functionals.npz"), **out)
+
+
+def main():
+    if not refio.ref_available():
+        raise SystemExit("build the reference harness first: make -C oracle/ref")
+    syms, xyz = systems.water_cluster(2, seed=0)
+    system_fixture("ref_water2.npz", syms, xyz, 6000, FUNCS, nocc=10, seed=0)
+    syms, xyz = systems.peptide_chain(12, seed=3)
+    system_fixture("ref_chain12.npz", syms, xyz, 5000, ["SVWN", "B3LYP"], nocc=20, seed=3)
+    functional_fixture()
+
+
+if __name__ == "__main__":
+    main()

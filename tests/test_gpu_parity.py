@@ -1,0 +1,166 @@
+"""CUDA path (libpdfxc through its C ABI) against the reference fixtures and the
+CPU oracle. Tolerances (FP64 drop-in): |dExc| <= 1e-8 Eh, max|dVxc| <= 1e-7
+against the reference; the AO screening cutoff (1e-14) is the only approximation
+the GPU path makes beyond summation order."""
+import numpy as np
+import pytest
+
+from conftest import golden, shell_table
+
+pytestmark = pytest.mark.gpu
+
+EXC_TOL = 1e-8
+VXC_TOL = 1e-7
+
+
+def engine(fx, **kw):
+    from proteindf_b200.xc import XcEngine
+    eng = XcEngine(**kw)
+    eng.set_system(shell_table(fx))
+    return eng
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "HFS", "HFB", "BLYP", "B3LYP"])
+def test_water2_vs_reference(water2, fn):
+    eng = engine(water2)
+    eng.set_grid(water2["grid"][:, :4], water2["grid"][:, 4].astype(np.int32))
+    exc, nel, V = eng.build_vxc(fn, water2["PA"])
+    assert abs(exc - water2[f"{fn}_exc"][0]) <= EXC_TOL
+    assert np.abs(V - water2[f"{fn}_vxc"]).max() <= VXC_TOL
+    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-9
+    rho = eng.get_rho(fn not in ("SVWN", "HFS"))
+    assert np.abs(rho - water2[f"{fn}_rho"]).max() <= 1e-9
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_chain12_vs_reference(chain12, fn):
+    eng = engine(chain12)
+    eng.set_grid(chain12["grid"][:, :4])
+    exc, nel, V = eng.build_vxc(fn, chain12["PA"])
+    assert abs(exc - chain12[f"{fn}_exc"][0]) <= EXC_TOL
+    assert np.abs(V - chain12[f"{fn}_vxc"]).max() <= VXC_TOL
+
+
+def test_vxc_accumulates_into_F(water2):
+    eng = engine(water2)
+    eng.set_grid(water2["grid"][:, :4])
+    F0 = np.arange(water2["PA"].size, dtype=np.float64).reshape(water2["PA"].shape) * 1e-3
+    F = F0.copy()
+    eng.build_vxc("B3LYP", water2["PA"], F=F)
+    assert np.abs((F - F0) - water2["B3LYP_vxc"]).max() <= VXC_TOL
+
+
+def test_full_grid_vs_oracle_water8():
+    """(H2O)8 on a full Becke grid sample: GPU vs the CPU oracle."""
+    from oracle import oracle
+    from proteindf_b200 import basis, grids, systems
+    syms, xyz = systems.water_cluster(8, seed=0)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis())
+    z = [1 if s == "H" else 8 for s in syms]
+    P, W, A = grids.molecular_grid(xyz, z, nrad=30, nang=110, radial="GC", mapping="TA", pruning=True)
+    from proteindf_b200.xc import XcEngine
+    eng = XcEngine()
+    eng.set_system(sh)
+    brad = np.array([grids.BECKE_RADIUS[zz] for zz in z])
+    w = eng.becke_weights(P, A, W, brad)
+    fac = oracle.becke(xyz, brad, P, A)
+    assert np.abs(w - W * fac).max() <= 1e-14 * np.abs(W).max()
+    P, W, A = grids.screen_by_weight(P, w, A)
+    rng = np.random.default_rng(1)
+    sel = np.sort(rng.choice(len(W), 20000, replace=False))
+    xyzw = np.concatenate([P[sel], W[sel, None]], axis=1)
+    PA = 0.5 * systems.density_matrix(sh.nao, 40, seed=0)
+    eng.set_grid(xyzw, A[sel])
+    for fn in ("SVWN", "B3LYP"):
+        exc, nel, V = eng.build_vxc(fn, PA)
+        ref = oracle.xc(fn, sh, xyzw, PA)
+        assert abs(exc - ref["exc"]) <= EXC_TOL
+        assert np.abs(V - ref["vxc"]).max() <= VXC_TOL
+        assert abs(nel - ref["nelec_alpha"]) <= 1e-9
+
+
+def test_becke_vs_reference(water2):
+    eng = engine(water2)
+    w = eng.becke_weights(water2["becke_points"], water2["becke_atom"], water2["becke_w_single"],
+                          water2["radii"][:, 1])
+    assert np.abs(w - water2["becke_w_final"]).max() <= 1e-15 * np.abs(water2["becke_w_single"]).max()
+
+
+def test_incremental_density_update(water2):
+    """xc-update = yes: a build on dP adds rho(dP) to the stored rho(P_prev)."""
+    eng = engine(water2)
+    eng.set_grid(water2["grid"][:, :4])
+    PA = water2["PA"]
+    rng = np.random.default_rng(3)
+    dP = rng.normal(scale=1e-3, size=PA.shape)
+    dP = 0.5 * (dP + dP.T)
+    eng.build_vxc("B3LYP", PA - dP)
+    exc_i, _, V_i = eng.build_vxc("B3LYP", dP, incremental=True)
+    exc_f, _, V_f = eng.build_vxc("B3LYP", PA)
+    assert abs(exc_i - exc_f) <= 1e-10
+    assert np.abs(V_i - V_f).max() <= 1e-9
+
+
+def test_rho_restart_roundtrip(water2):
+    eng = engine(water2)
+    eng.set_grid(water2["grid"][:, :4])
+    eng.build_vxc("BLYP", water2["PA"])
+    rho = eng.get_rho(True)
+    eng2 = engine(water2)
+    eng2.set_grid(water2["grid"][:, :4])
+    eng2.set_rho(rho, True)
+    exc, _, V = eng2.build_vxc("BLYP", np.zeros_like(water2["PA"]), incremental=True)
+    assert abs(exc - water2["BLYP_exc"][0]) <= EXC_TOL
+    assert np.abs(V - water2["BLYP_vxc"]).max() <= VXC_TOL
+
+
+def test_device_build_matches_host_build(water2):
+    import torch
+    eng = engine(water2)
+    eng.set_grid(water2["grid"][:, :4])
+    exc_h, nel_h, V_h = eng.build_vxc("B3LYP", water2["PA"])
+    dP = torch.tensor(water2["PA"], device="cuda", dtype=torch.float64)
+    dV = torch.empty_like(dP)
+    torch.cuda.synchronize()
+    exc_d, nel_d = eng.build_vxc_device("B3LYP", dP.data_ptr(), dV.data_ptr())
+    assert exc_d == exc_h and nel_d == nel_h
+    assert np.array_equal(dV.cpu().numpy(), V_h)
+
+
+def test_small_blocks_and_ragged_grid(water2):
+    """Blocks of 37 points (ragged last block) give the same result."""
+    eng = engine(water2, block_points=37)
+    g = water2["grid"][:4001]
+    eng.set_grid(g[:, :4])
+    exc, _, V = eng.build_vxc("SVWN", water2["PA"])
+    eng2 = engine(water2)
+    eng2.set_grid(g[:, :4])
+    exc2, _, V2 = eng2.build_vxc("SVWN", water2["PA"])
+    assert abs(exc - exc2) <= 1e-12
+    assert np.abs(V - V2).max() <= 1e-12
+
+
+def test_single_point_grid(water2):
+    eng = engine(water2)
+    g = water2["grid"][:1]
+    eng.set_grid(g[:, :4])
+    exc, nel, V = eng.build_vxc("B3LYP", water2["PA"])
+    from oracle import oracle
+    ref = oracle.xc("B3LYP", shell_table(water2), g[:, :4], water2["PA"])
+    assert abs(exc - ref["exc"]) <= 1e-12
+    assert np.abs(V - ref["vxc"]).max() <= 1e-12
+
+
+def test_errors_are_status_codes(water2):
+    from proteindf_b200.xc import XcEngine
+    eng = XcEngine()
+    with pytest.raises(RuntimeError, match="set_system"):
+        eng.set_grid(water2["grid"][:10, :4])
+    eng.set_system(shell_table(water2))
+    with pytest.raises(RuntimeError, match="set_grid"):
+        eng.build_vxc("SVWN", water2["PA"])
+    eng.set_grid(water2["grid"][:10, :4])
+    with pytest.raises(RuntimeError, match="incremental"):
+        eng.build_vxc("SVWN", water2["PA"], incremental=True)
+    with pytest.raises(RuntimeError, match="owner atom"):
+        eng.becke_weights(np.zeros((2, 3)), np.array([0, 99]), np.ones(2), np.ones(6))
