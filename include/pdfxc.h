@@ -57,6 +57,7 @@ typedef struct {
     double ao_cutoff;    /* drop a shell from a block when its value/gradient bound is below (default 1e-14) */
     double rho_cutoff;   /* xc-density-threshold: points with rho_A <= it are skipped (default 1e-16) */
     size_t workspace_bytes; /* device workspace budget for block intermediates (0 = default 4 GiB) */
+    int split_terms;     /* mixed path: 3 (hi*hi + hi*mid + mid*hi) or 6 (three-way split, default) */
 } pdfxc_options;
 
 typedef struct pdfxc_ctx pdfxc_ctx;

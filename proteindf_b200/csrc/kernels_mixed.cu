@@ -1,0 +1,477 @@
+// Mixed-precision XC build: the two contractions on tcgen05 tensor cores with
+// split-BF16 operands (v = hi + mid [+ lo], each BF16) and FP32 accumulation in
+// TMEM; AO values, weights, the functional, the per-block Exc / electron-count
+// sums and the Vxc accumulation stay in FP64.
+//
+// Per block (128 points, nb screened AOs padded to nbp = 128k):
+//   ao_mixed    phi, grad phi in FP64 -> FP32 copies (epilogue operands) and
+//               split-BF16 packed operands phi^T (rows = points, K = AOs) and
+//               phi (rows = AOs, K = points)
+//   pack_p      P_sub = P_A[aos, aos] as split-BF16 packed (rows = mu, K = nu)
+//   umma<RHO>   X^T = phi^T P_sub  (M = 128 points, N = 128 AOs per CTA, K = nbp);
+//               epilogue: rho(p) += sum_mu phi[mu][p] X^T[p][mu] and the
+//               gradient sums, FP64 atomics per point
+//   functional  rho -> Exc partials, 0.5 w vrho, c = w (2 vgAA + vgAB) grad rho
+//   pack_z      Z[nu][p] = 0.5 w vrho phi + c . grad phi, split-BF16 packed
+//   umma<VXC>   W = phi Z^T (M = N = 128 AOs per CTA, K = 128 points);
+//               epilogue: Vacc[aos, aos] += W in FP64
+// The split product keeps the terms hi*hi + hi*mid + mid*hi (3 terms) or, with
+// the three-way split, all terms of order <= 2^-24 (6 terms).
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include "functional.cuh"
+#include "pdfxc_internal.cuh"
+#include "umma.cuh"
+
+namespace pdfxc {
+
+namespace {
+
+using umma::packed_offset;
+
+__device__ __forceinline__ void split3(double v, __nv_bfloat16& h, __nv_bfloat16& m, __nv_bfloat16& l) {
+    h = __double2bfloat16(v);
+    const double r1 = v - (double)__bfloat162float(h);
+    m = __double2bfloat16(r1);
+    const double r2 = r1 - (double)__bfloat162float(m);
+    l = __double2bfloat16(r2);
+}
+
+__device__ __forceinline__ void ang_factor_m(int t, double x, double y, double z, double a2, double& v, double& dx,
+                                             double& dy, double& dz) {
+    const double s3 = 0.57735026918962576451;
+    switch (t) {
+        case 0: v = 1.0; dx = -a2 * x; dy = -a2 * y; dz = -a2 * z; break;
+        case 1: v = x; dx = -a2 * x * x + 1.0; dy = -a2 * x * y; dz = -a2 * x * z; break;
+        case 2: v = y; dx = -a2 * y * x; dy = -a2 * y * y + 1.0; dz = -a2 * y * z; break;
+        case 3: v = z; dx = -a2 * z * x; dy = -a2 * z * y; dz = -a2 * z * z + 1.0; break;
+        case 4: v = x * y; dx = -a2 * x * y * x + y; dy = -a2 * x * y * y + x; dz = -a2 * x * y * z; break;
+        case 5: v = z * x; dx = -a2 * x * z * x + z; dy = -a2 * x * z * y; dz = -a2 * x * z * z + x; break;
+        case 6: v = y * z; dx = -a2 * y * z * x; dy = -a2 * y * z * y + z; dz = -a2 * y * z * z + y; break;
+        case 7:
+            v = 0.5 * (x * x - y * y);
+            dx = 0.5 * ((-a2 * x * x * x + 2.0 * x) - (-a2 * y * y * x));
+            dy = 0.5 * ((-a2 * x * x * y) - (-a2 * y * y * y + 2.0 * y));
+            dz = 0.5 * ((-a2 * x * x * z) - (-a2 * y * y * z));
+            break;
+        default: {
+            v = s3 * (z * z - 0.5 * (x * x + y * y));
+            const double xxX = -a2 * x * x * x + 2.0 * x, xxY = -a2 * x * x * y, xxZ = -a2 * x * x * z;
+            const double yyX = -a2 * y * y * x, yyY = -a2 * y * y * y + 2.0 * y, yyZ = -a2 * y * y * z;
+            const double zzX = -a2 * z * z * x, zzY = -a2 * z * z * y, zzZ = -a2 * z * z * z + 2.0 * z;
+            dx = s3 * (zzX - 0.5 * (xxX + yyX));
+            dy = s3 * (zzY - 0.5 * (xxY + yyY));
+            dz = s3 * (zzZ - 0.5 * (xxZ + yyZ));
+        }
+    }
+}
+
+__device__ __forceinline__ void store_split(char* base, size_t plane, size_t off, double v) {
+    __nv_bfloat16 h, m, l;
+    split3(v, h, m, l);
+    *reinterpret_cast<__nv_bfloat16*>(base + off) = h;
+    *reinterpret_cast<__nv_bfloat16*>(base + plane + off) = m;
+    *reinterpret_cast<__nv_bfloat16*>(base + 2 * plane + off) = l;
+}
+
+// AO values for one block. 256 threads: point = tid % 128, halves take alternate shells.
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_ao_mixed(BasisView bas, GridView g, int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const MixedLayout L = mixed_layout(m.nbp);
+    char* base = ws + m.ws;
+    float* phi32 = reinterpret_cast<float*>(base + L.phi32);
+    char* phi1 = base + L.phi1;
+    char* phi2 = base + L.phi2;
+    const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+    const int p = threadIdx.x & (BLOCK_PTS - 1);
+    const int half = threadIdx.x >> 7;
+    const int gp = blk * BLOCK_PTS + p;
+    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
+    for (int i = half; i < m.nsh; i += 2) {
+        const int s = g.blk_shells[m.sh0 + i];
+        const int row0 = g.blk_shell_row[m.sh0 + i];
+        const int a = bas.sh_atom[s];
+        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
+        const double d2 = x * x + y * y + z * z;
+        const int Lq = bas.sh_l[s], n = 2 * Lq + 1, np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
+        for (int c = 0; c < n; ++c) {
+            double v = 0, gx = 0, gy = 0, gz = 0;
+            for (int k = 0; k < np; ++k) {
+                const double al = bas.p_exp[p0 + k];
+                if (al * d2 <= 30.0) {
+                    const double e = bas.p_coef[p0 + k] * exp(-al * d2);
+                    double av, ax, ay, az;
+                    ang_factor_m(Lq * Lq + c, x, y, z, 2.0 * al, av, ax, ay, az);
+                    v += av * e;
+                    if (GGA) gx += ax * e, gy += ay * e, gz += az * e;
+                }
+            }
+            const int mu = row0 + c;
+            const size_t o = (size_t)mu * BLOCK_PTS + p;
+            phi32[o] = (float)v;
+            if (GGA) {
+                phi32[plane32 + o] = (float)gx;
+                phi32[2 * plane32 + o] = (float)gy;
+                phi32[3 * plane32 + o] = (float)gz;
+            }
+            store_split(phi1, L.phi1_plane, packed_offset(p, mu, m.nbp), v);
+            store_split(phi2, L.phi2_plane, packed_offset(mu, p, BLOCK_PTS), v);
+        }
+    }
+    for (int mu = m.nb + half; mu < m.nbp; mu += 2) {
+        const size_t o = (size_t)mu * BLOCK_PTS + p;
+        phi32[o] = 0.f;
+        if (GGA) phi32[plane32 + o] = phi32[2 * plane32 + o] = phi32[3 * plane32 + o] = 0.f;
+        store_split(phi1, L.phi1_plane, packed_offset(p, mu, m.nbp), 0.0);
+        store_split(phi2, L.phi2_plane, packed_offset(mu, p, BLOCK_PTS), 0.0);
+    }
+}
+
+// P_sub of one block, split and packed; thread = (row mu, 8 consecutive nu) -> 16-byte stores.
+__global__ void __launch_bounds__(256) k_pack_p(GridView g, const double* __restrict__ P, int nao, int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const MixedLayout L = mixed_layout(m.nbp);
+    char* pp = ws + m.ws + L.ppack;
+    const int* aos = g.blk_aos + m.ao0;
+    const int groups = m.nbp / 8;
+    for (int e = threadIdx.x; e < m.nbp * groups; e += blockDim.x) {
+        const int mu = e / groups, nu0 = (e % groups) * 8;
+        __align__(16) __nv_bfloat16 h[8], md[8], lo[8];
+        const size_t row = mu < m.nb ? (size_t)aos[mu] * nao : 0;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int nu = nu0 + j;
+            const double v = (mu < m.nb && nu < m.nb) ? P[row + aos[nu]] : 0.0;
+            split3(v, h[j], md[j], lo[j]);
+        }
+        const size_t off = packed_offset(mu, nu0, m.nbp);
+        *reinterpret_cast<uint4*>(pp + off) = *reinterpret_cast<uint4*>(h);
+        *reinterpret_cast<uint4*>(pp + L.ppack_plane + off) = *reinterpret_cast<uint4*>(md);
+        *reinterpret_cast<uint4*>(pp + 2 * L.ppack_plane + off) = *reinterpret_cast<uint4*>(lo);
+    }
+}
+
+__device__ __forceinline__ double warp_sum_m(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// rho accumulators -> functional -> Vxc coefficients, per point (128 threads per block).
+template <bool GGA>
+__global__ void __launch_bounds__(BLOCK_PTS) k_functional_mixed(GridView g, int blk0, int fn, int incremental,
+                                                                double rho_cut, const double* rho_acc,
+                                                                double* rho_store, double* coef, double* blk_sum) {
+    const int blk = blk0 + blockIdx.x;
+    const int p = threadIdx.x;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    const double* ra = rho_acc + gp * 4;
+    double rho = ra[0], gx = 2.0 * ra[1], gy = 2.0 * ra[2], gz = 2.0 * ra[3];
+    double* rs = rho_store + gp * 4;
+    if (incremental) rho += rs[0], gx += rs[1], gy += rs[2], gz += rs[3];
+    rs[0] = rho, rs[1] = gx, rs[2] = gy, rs[3] = gz;
+    const double w = g.pw[gp];
+    double e = 0.0, a = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    if (w != 0.0 && rho > rho_cut) {
+        const double gam = gx * gx + gy * gy + gz * gz;
+        const XcOut o = eval_functional(fn, rho, rho, gam, gam, gam);
+        e = w * o.f;
+        a = 0.5 * w * o.va;
+        if (GGA) {
+            const double cc = w * (2.0 * o.vgaa + o.vgab);
+            cx = cc * gx, cy = cc * gy, cz = cc * gz;
+        }
+    }
+    double* cf = coef + gp * 4;
+    cf[0] = a, cf[1] = cx, cf[2] = cy, cf[3] = cz;
+    __shared__ double red[2][BLOCK_PTS / 32];
+    const double se = warp_sum_m(e), sn = warp_sum_m(w * rho);
+    if ((p & 31) == 0) red[0][p >> 5] = se, red[1][p >> 5] = sn;
+    __syncthreads();
+    if (p == 0) {
+        double E = 0.0, N = 0.0;
+        for (int i = 0; i < BLOCK_PTS / 32; ++i) E += red[0][i], N += red[1][i];
+        blk_sum[2 * blk] = E, blk_sum[2 * blk + 1] = N;
+    }
+}
+
+// Z[nu][p] = 0.5 w vrho phi + c . grad phi, split and packed (rows = AOs, K = points).
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_pack_z(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const MixedLayout L = mixed_layout(m.nbp);
+    const float* phi32 = reinterpret_cast<const float*>(ws + m.ws + L.phi32);
+    char* zp = ws + m.ws + L.zpack;
+    const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+    __shared__ double cf[4][BLOCK_PTS];
+    for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
+        cf[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
+    __syncthreads();
+    const int groups = BLOCK_PTS / 8;
+    for (int e = threadIdx.x; e < m.nbp * groups; e += blockDim.x) {
+        const int nu = e / groups, p0 = (e % groups) * 8;
+        __align__(16) __nv_bfloat16 h[8], md[8], lo[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const int p = p0 + j;
+            const size_t o = (size_t)nu * BLOCK_PTS + p;
+            double z = cf[0][p] * (double)phi32[o];
+            if (GGA)
+                z += cf[1][p] * (double)phi32[plane32 + o] + cf[2][p] * (double)phi32[2 * plane32 + o] +
+                     cf[3][p] * (double)phi32[3 * plane32 + o];
+            split3(z, h[j], md[j], lo[j]);
+        }
+        const size_t off = packed_offset(nu, p0, BLOCK_PTS);
+        *reinterpret_cast<uint4*>(zp + off) = *reinterpret_cast<uint4*>(h);
+        *reinterpret_cast<uint4*>(zp + L.zpack_plane + off) = *reinterpret_cast<uint4*>(md);
+        *reinterpret_cast<uint4*>(zp + 2 * L.zpack_plane + off) = *reinterpret_cast<uint4*>(lo);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// The tcgen05 contraction. One CTA (4 warps) computes one 128 x 128 FP32 tile
+// D = sum_terms A_i B_j^T over K in 64-wide slabs: warp 0 / lane 0 streams the
+// slabs of the needed split planes into a ring of shared-memory stages with
+// cp.async.bulk, warp 1 / lane 0 issues tcgen05.mma (M = 128, N = 128, K = 16)
+// into a 128-column TMEM accumulator, and all four warps run the epilogue on
+// their 32 TMEM lanes. Every wait is bounded; on expiry an error code is
+// recorded in *err and the CTA winds down (waiting, bounded, for its issued
+// MMAs) before freeing TMEM.
+enum { MODE_RHO = 0, MODE_VXC = 1 };
+
+struct UmmaParams {
+    int nterms;    // 3 or 6
+    int stages;    // ring depth
+    int* err;      // device error word
+    const double* dummy;
+};
+
+__constant__ int kTermA[6] = {0, 0, 1, 0, 1, 2};
+__constant__ int kTermB[6] = {0, 1, 0, 2, 1, 0};
+
+template <int MODE, bool GGA>
+__global__ void __launch_bounds__(128, 1)
+    k_umma(GridView g, int blk0, char* ws, UmmaParams prm, int tiles_max, double* rho_acc, double* Vacc, int nao) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int blk = blk0 + blockIdx.y;
+    const BlockMeta m = g.meta[blk];
+    const MixedLayout L = mixed_layout(m.nbp);
+    const int ntiles = m.nbp / umma::TILE_ROWS;
+    int mt, nt;
+    if (MODE == MODE_RHO) {
+        mt = 0, nt = blockIdx.x;
+        if (nt >= ntiles) return;
+    } else {
+        mt = blockIdx.x / tiles_max, nt = blockIdx.x % tiles_max;
+        if (mt >= ntiles || nt >= ntiles) return;
+    }
+    // once any CTA has recorded an expired wait, the rest of the grid exits at once
+    __shared__ int s_abort;
+    if (threadIdx.x == 0) s_abort = *reinterpret_cast<const volatile int*>(prm.err);
+    __syncthreads();
+    if (s_abort) return;
+    const int nA = prm.nterms == 3 ? 2 : 3, nB = nA;
+    const int S = prm.stages;
+    const uint32_t stage_bytes = (uint32_t)(nA + nB) * umma::SLAB_BYTES;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * stage_bytes);
+    uint64_t* empty = full + S;
+    uint64_t* done = empty + S;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+
+    // operands of this tile
+    const char* base = ws + m.ws;
+    const char *Ab, *Bb;
+    size_t Aplane, Bplane;
+    int nslabs;
+    if (MODE == MODE_RHO) {
+        Ab = base + L.phi1;  // rows = 128 points, K = nbp
+        Aplane = L.phi1_plane;
+        Bb = base + L.ppack + (size_t)nt * umma::TILE_ROWS * m.nbp * 2;  // rows = mu tile, K = nbp
+        Bplane = L.ppack_plane;
+        nslabs = m.nbp / umma::SLAB_K;
+    } else {
+        Ab = base + L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS * 2;  // rows = mu tile, K = 128 points
+        Aplane = L.phi2_plane;
+        Bb = base + L.zpack + (size_t)nt * umma::TILE_ROWS * BLOCK_PTS * 2;
+        Bplane = L.zpack_plane;
+        nslabs = BLOCK_PTS / umma::SLAB_K;
+    }
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) umma::tmem_alloc(tslot, 128);
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < S; ++s) umma::mbar_init(&full[s], 1), umma::mbar_init(&empty[s], 1);
+        umma::mbar_init(done, 1);
+        umma::mbar_init_fence();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+    bool ok = true;
+
+    if (warp == 0 && lane == 0) {  // producer
+        for (int j = 0; j < nslabs && ok; ++j) {
+            const int s = j % S;
+            if (j >= S && !umma::mbar_wait(&empty[s], ((j / S) - 1) & 1, prm.err)) {
+                ok = false;
+                atomicExch(prm.err, 1);
+                break;
+            }
+            uint8_t* st = smem + s * stage_bytes;
+            umma::mbar_expect_tx(&full[s], stage_bytes);
+            for (int a = 0; a < nA; ++a)
+                umma::bulk_g2s(st + a * umma::SLAB_BYTES, Ab + a * Aplane + (size_t)j * umma::SLAB_BYTES,
+                               umma::SLAB_BYTES, &full[s]);
+            for (int b = 0; b < nB; ++b)
+                umma::bulk_g2s(st + (nA + b) * umma::SLAB_BYTES, Bb + b * Bplane + (size_t)j * umma::SLAB_BYTES,
+                               umma::SLAB_BYTES, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {  // MMA issuer
+        const uint32_t idesc = umma::instr_desc_bf16(128, 128);
+        bool issued = false;
+        for (int j = 0; j < nslabs; ++j) {
+            const int s = j % S;
+            if (!umma::mbar_wait(&full[s], (j / S) & 1, prm.err)) {
+                ok = false;
+                atomicExch(prm.err, 2);
+                break;
+            }
+            umma::fence_after_sync();
+            const uint32_t st = umma::smem_u32(smem + s * stage_bytes);
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) {
+                for (int t = 0; t < prm.nterms; ++t) {
+                    const uint64_t ad = umma::smem_desc(st + kTermA[t] * umma::SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
+                    const uint64_t bd =
+                        umma::smem_desc(st + (nA + kTermB[t]) * umma::SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
+                    umma::mma_bf16(tmem, ad, bd, idesc, (j > 0 || kk > 0 || t > 0) ? 1u : 0u);
+                }
+            }
+            issued = true;
+            umma::mma_commit(&empty[s]);
+        }
+        if (issued) umma::mma_commit(done);
+        else umma::mbar_expect_tx(done, 0);  // nothing issued: complete the phase ourselves
+    }
+    __syncwarp();
+    bool waited = umma::mbar_wait(done, 0, prm.err);
+    if (!waited) atomicExch(prm.err, 3);
+    // one decision for the whole CTA: the epilogue below has CTA-wide barriers
+    const bool ready = __syncthreads_and(waited) != 0;
+    umma::fence_after_sync();
+
+    if (ready) {
+        const int row = warp * 32 + lane;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        if (MODE == MODE_RHO) {
+            const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+            const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+            for (int c0 = 0; c0 < 128; c0 += 16) {
+                float v[16];
+                umma::tmem_ld16(taddr + c0, v);
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const int mu = nt * 128 + c0 + c;
+                    if (mu >= m.nb) break;
+                    const size_t o = (size_t)mu * BLOCK_PTS + row;
+                    const double x = v[c];
+                    r += (double)phi32[o] * x;
+                    if (GGA) {
+                        gx += (double)phi32[plane32 + o] * x;
+                        gy += (double)phi32[2 * plane32 + o] * x;
+                        gz += (double)phi32[3 * plane32 + o] * x;
+                    }
+                }
+            }
+            double* acc = rho_acc + ((size_t)blk * BLOCK_PTS + row) * 4;
+            atomicAdd(acc, r);
+            if (GGA) atomicAdd(acc + 1, gx), atomicAdd(acc + 2, gy), atomicAdd(acc + 3, gz);
+        } else {
+            // stage 16 columns of all 128 rows in shared memory, then let each warp
+            // add two rows x 16 consecutive columns per instruction
+            float* tile = reinterpret_cast<float*>(smem);  // [128][17]
+            const int* aos = g.blk_aos + m.ao0;
+            for (int c0 = 0; c0 < 128; c0 += 16) {
+                float v[16];
+                umma::tmem_ld16(taddr + c0, v);
+#pragma unroll
+                for (int c = 0; c < 16; ++c) tile[row * 17 + c] = v[c];
+                __syncthreads();
+                const int c = threadIdx.x & 15;
+                const int nu = nt * 128 + c0 + c;
+                if (nu < m.nb) {
+                    const int anu = aos[nu];
+                    for (int rr = threadIdx.x >> 4; rr < 128; rr += 8) {
+                        const int mu = mt * 128 + rr;
+                        if (mu < m.nb) atomicAdd(&Vacc[(size_t)aos[mu] * nao + anu], (double)tile[rr * 17 + c]);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+}  // namespace
+
+size_t umma_smem_bytes(int nterms) {
+    const int nA = nterms == 3 ? 2 : 3;
+    const int S = nterms == 3 ? 3 : 2;
+    return (size_t)S * 2 * nA * umma::SLAB_BYTES + (2 * S + 1) * 8 + 16;
+}
+
+static UmmaParams umma_params(const MixedArgs& a) { return UmmaParams{a.nterms, a.nterms == 3 ? 3 : 2, a.err, nullptr}; }
+
+void mixed_prepare(const MixedArgs& a, cudaStream_t s) {
+    if (functional_is_gga(a.fn))
+        k_ao_mixed<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
+    else
+        k_ao_mixed<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
+    k_pack_p<<<a.nblk, 256, 0, s>>>(a.g, a.P, a.nao, a.blk0, a.ws);
+}
+
+void mixed_rho(const MixedArgs& a, cudaStream_t s) {
+    const int tiles = a.max_nbp / umma::TILE_ROWS;
+    const size_t smem = umma_smem_bytes(a.nterms);
+    if (functional_is_gga(a.fn)) {
+        cudaFuncSetAttribute(k_umma<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_umma<MODE_RHO, true><<<dim3(tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, umma_params(a), tiles,
+                                                                     a.rho_acc, a.Vacc, a.nao);
+    } else {
+        cudaFuncSetAttribute(k_umma<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_umma<MODE_RHO, false><<<dim3(tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, umma_params(a), tiles,
+                                                                      a.rho_acc, a.Vacc, a.nao);
+    }
+}
+
+void mixed_functional(const MixedArgs& a, cudaStream_t s) {
+    if (functional_is_gga(a.fn)) {
+        k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
+                                                              a.rho_store, a.coef, a.blk_sum);
+        k_pack_z<true><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+    } else {
+        k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
+                                                               a.rho_store, a.coef, a.blk_sum);
+        k_pack_z<false><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+    }
+}
+
+void mixed_vxc(const MixedArgs& a, cudaStream_t s) {
+    const int tiles = a.max_nbp / umma::TILE_ROWS;
+    const size_t smem = umma_smem_bytes(a.nterms);
+    cudaFuncSetAttribute(k_umma<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_umma<MODE_VXC, false><<<dim3(tiles * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, umma_params(a), tiles,
+                                                                          a.rho_acc, a.Vacc, a.nao);
+}
+
+}  // namespace pdfxc

@@ -115,7 +115,7 @@ pdfxc::GridView grid_view(const pdfxc_ctx* c) {
 void free_grid(pdfxc_ctx* c) {
     dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
     dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
-    dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum);
+    dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum), dev_free(c->d_rho_acc);
     if (c->d_ws) cudaFree(c->d_ws);
     c->d_ws = nullptr;
     c->nblk = 0;
@@ -134,6 +134,7 @@ void pdfxc_default_options(pdfxc_options* opt) {
     opt->ao_cutoff = 1e-14;
     opt->rho_cutoff = 1e-16;
     opt->workspace_bytes = 0;
+    opt->split_terms = 6;
 }
 
 pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt) {
@@ -145,6 +146,7 @@ pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt)
     if (opt) c->opt = *opt;
     if (c->opt.block_points <= 0 || c->opt.block_points > BLOCK_PTS) c->opt.block_points = BLOCK_PTS;
     if (c->opt.workspace_bytes == 0) c->opt.workspace_bytes = size_t(4) << 30;
+    if (c->opt.split_terms != 3 && c->opt.split_terms != 6) c->opt.split_terms = 6;
     if (c->opt.precision != PDFXC_PRECISION_FP64 && c->opt.precision != PDFXC_PRECISION_MIXED) {
         delete c;
         return PDFXC_ERR_ARG;
@@ -160,7 +162,8 @@ pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt)
         return PDFXC_ERR_CUDA;
     }
     for (auto& e : c->ev) cudaEventCreate(&e);
-    if (cudaMalloc(&c->d_scalars, 2 * sizeof(double)) != cudaSuccess) {
+    if (cudaMalloc(&c->d_scalars, 2 * sizeof(double)) != cudaSuccess ||
+        cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess || cudaMemset(c->d_err, 0, sizeof(int)) != cudaSuccess) {
         pdfxc_destroy(c);
         return PDFXC_ERR_NOMEM;
     }
@@ -280,6 +283,7 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
                                         ctx->h_sh_nprim[s], ctx->opt.ao_cutoff);
         std::vector<int> shells, rows, aos;
         const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
+        const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
         double flops = 0.0, sum_nb = 0.0;
         for (int b = 0; b < nblk; ++b) {
             BlockMeta& m = ctx->h_meta[b];
@@ -299,7 +303,7 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
             }
             m.nsh = (int)shells.size() - m.sh0;
             m.nb = row;
-            m.nbp = std::max(64, (row + 63) / 64 * 64);
+            m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
             flops += 4.0 * double(m.nb) * m.nb * m.npts;
             sum_nb += m.nb;
         }
@@ -308,7 +312,8 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
         size_t off = 0, max_ws = 0;
         Chunk cur{0, 0, 0, 0};
         for (int b = 0; b < nblk; ++b) {
-            const size_t need = pdfxc::block_ws_doubles(ctx->h_meta[b].nbp, gga_ws) * sizeof(double);
+            const size_t need = mixed ? pdfxc::mixed_layout(ctx->h_meta[b].nbp).total
+                                      : pdfxc::block_ws_doubles(ctx->h_meta[b].nbp, gga_ws) * sizeof(double);
             if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
                 cur.b1 = b;
                 cur.ws_bytes = off;
@@ -338,6 +343,7 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
         dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
         dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
         dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
+        if (mixed) dev_alloc(&ctx->d_rho_acc, (size_t)nblk * BLOCK_PTS * 4);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho, 0, sizeof(double) * (size_t)nblk * BLOCK_PTS * 4, s));
         if (cudaMalloc(&ctx->d_ws, max_ws) != cudaSuccess) {
             ctx->d_ws = nullptr;
@@ -416,7 +422,29 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     PDFXC_CUDA(cudaEventRecord(ctx->ev[0], s));
     PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc, 0, sizeof(double) * (size_t)nao * nao, s));
     int64_t launches = 0;
-    for (size_t ci = 0; ci < ctx->chunks.size(); ++ci) {
+    const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
+    if (mixed) {
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho_acc, 0, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s));
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+    }
+    for (size_t ci = 0; ci < ctx->chunks.size() && mixed; ++ci) {
+        const Chunk& c = ctx->chunks[ci];
+        cudaEvent_t* e = &ctx->stage_ev[5 * ci];
+        pdfxc::MixedArgs a{bv, gv, c.b0, c.b1 - c.b0, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
+                           ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
+                           ctx->d_Vacc, ctx->d_err};
+        PDFXC_CUDA(cudaEventRecord(e[0], s));
+        pdfxc::mixed_prepare(a, s);
+        PDFXC_CUDA(cudaEventRecord(e[1], s));
+        pdfxc::mixed_rho(a, s);
+        PDFXC_CUDA(cudaEventRecord(e[2], s));
+        pdfxc::mixed_functional(a, s);
+        PDFXC_CUDA(cudaEventRecord(e[3], s));
+        pdfxc::mixed_vxc(a, s);
+        PDFXC_CUDA(cudaEventRecord(e[4], s));
+        launches += 6;
+    }
+    for (size_t ci = 0; ci < ctx->chunks.size() && !mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
         cudaEvent_t* e = &ctx->stage_ev[5 * ci];
         const int nb = c.b1 - c.b0;
@@ -438,6 +466,13 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     PDFXC_CUDA(cudaEventRecord(ctx->stage_ev[nev - 1], s));
     PDFXC_CUDA(cudaEventRecord(ctx->ev[1], s));
     ctx->last_profile.launches = launches;
+}
+
+// After the stream has synchronised: the device error word (0 = no expired wait).
+int device_error(pdfxc_ctx* ctx) {
+    int code = 0;
+    PDFXC_CUDA(cudaMemcpy(&code, ctx->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    return code;
 }
 
 // After the stream has synchronised: fold the stage events into last_profile.
@@ -497,6 +532,10 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
         PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
         PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
         collect_profile(ctx);
+        if (int code = device_error(ctx)) {
+            ctx->err = "a bounded device wait expired in the tensor-core contraction (code " + std::to_string(code) + ")";
+            return PDFXC_ERR_TIMEOUT;
+        }
         if (exc) *exc = sc[0];
         if (nelec_alpha) *nelec_alpha = sc[1];
         ctx->rho_valid = true;
@@ -523,6 +562,10 @@ pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, i
         PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
         PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
         collect_profile(ctx);
+        if (int code = device_error(ctx)) {
+            ctx->err = "a bounded device wait expired in the tensor-core contraction (code " + std::to_string(code) + ")";
+            return PDFXC_ERR_TIMEOUT;
+        }
         for (size_t i = 0; i < n2; ++i) F[i] += V[i];
         if (exc) *exc = sc[0];
         if (nelec_alpha) *nelec_alpha = sc[1];
@@ -599,7 +642,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     free_grid(ctx);
     dev_free(ctx->d_atom_xyz), dev_free(ctx->d_p_exp), dev_free(ctx->d_p_coef);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
-    dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars);
+    dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : ctx->stage_ev) cudaEventDestroy(e);

@@ -92,6 +92,8 @@ struct pdfxc_ctx {
     double* d_rho = nullptr;    // [nblk * BLOCK_PTS * 4]: rho, grad x, y, z
     double* d_coef = nullptr;   // [nblk * BLOCK_PTS * 4]: 0.5 w vrho, c_x, c_y, c_z
     double* d_blk_sum = nullptr;  // [nblk * 2]: per-block Exc, Nel
+    double* d_rho_acc = nullptr;  // mixed path: [nblk * BLOCK_PTS * 4] rho partial sums of the contraction
+    int* d_err = nullptr;         // device error word (bounded waits that expired)
     double* d_scalars = nullptr;  // [2]
     double* d_P = nullptr;        // n_ao^2 staging for host-pointer builds
     double* d_V = nullptr;        // n_ao^2
@@ -132,5 +134,54 @@ void launch_becke(const double* atom_xyz, const double* brad, int natom, int siz
 __host__ __device__ inline size_t block_ws_doubles(int nbp, bool gga) {
     return (size_t)nbp * BLOCK_PTS * (gga ? 5 : 2);
 }
+
+// Intermediates of one block on the mixed path (byte offsets; nbp % 128 == 0).
+// Packed operands use the layout of umma.cuh, three split planes each.
+struct MixedLayout {
+    size_t phi32;                // FP32 phi and grad phi, [4][nbp][128]
+    size_t phi1, phi1_plane;     // phi^T packed: rows = 128 points, K = nbp AOs
+    size_t phi2, phi2_plane;     // phi packed: rows = nbp AOs, K = 128 points
+    size_t ppack, ppack_plane;   // P_sub packed: rows = nbp, K = nbp
+    size_t zpack, zpack_plane;   // Z packed: rows = nbp, K = 128 points
+    size_t total;
+};
+
+__host__ __device__ inline MixedLayout mixed_layout(int nbp) {
+    MixedLayout L;
+    size_t o = 0;
+    L.phi32 = o;
+    o += (size_t)4 * nbp * BLOCK_PTS * 4;
+    L.phi1 = o;
+    L.phi1_plane = (size_t)BLOCK_PTS * nbp * 2;
+    o += 3 * L.phi1_plane;
+    L.phi2 = o;
+    L.phi2_plane = (size_t)nbp * BLOCK_PTS * 2;
+    o += 3 * L.phi2_plane;
+    L.ppack = o;
+    L.ppack_plane = (size_t)nbp * nbp * 2;
+    o += 3 * L.ppack_plane;
+    L.zpack = o;
+    L.zpack_plane = (size_t)nbp * BLOCK_PTS * 2;
+    o += 3 * L.zpack_plane;
+    L.total = o;
+    return L;
+}
+
+// kernels_mixed.cu: the four stages of one chunk on the mixed path
+struct MixedArgs {
+    BasisView b;
+    GridView g;
+    int blk0, nblk, max_nbp, fn, incremental, nterms, nao;
+    double rho_cut;
+    const double* P;
+    char* ws;
+    double *rho_acc, *rho_store, *coef, *blk_sum, *Vacc;
+    int* err;
+};
+void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
+void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue
+void mixed_functional(const MixedArgs& a, cudaStream_t s);  // functional, Z packing
+void mixed_vxc(const MixedArgs& a, cudaStream_t s);         // Vacc += phi Z^T
+size_t umma_smem_bytes(int nterms);
 
 }  // namespace pdfxc

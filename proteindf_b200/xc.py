@@ -25,7 +25,7 @@ EXPORTS = [
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("block_points", ctypes.c_int), ("ao_cutoff", ctypes.c_double),
-                ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t)]
+                ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t), ("split_terms", ctypes.c_int)]
 
 
 class Profile(ctypes.Structure):
@@ -84,7 +84,7 @@ class XcEngine:
     """
 
     def __init__(self, device=0, precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16,
-                 workspace_bytes=0):
+                 workspace_bytes=0, split_terms=6):
         self.L = load_library()
         opt = Options()
         self.L.pdfxc_default_options(ctypes.byref(opt))
@@ -93,6 +93,7 @@ class XcEngine:
         opt.ao_cutoff = ao_cutoff
         opt.rho_cutoff = rho_cutoff
         opt.workspace_bytes = workspace_bytes
+        opt.split_terms = split_terms
         h = _vp()
         st = self.L.pdfxc_create(ctypes.byref(h), device, ctypes.byref(opt))
         if st != 0:

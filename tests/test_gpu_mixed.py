@@ -1,0 +1,81 @@
+"""Mixed-precision path (tcgen05 split-BF16 contractions, FP32 accumulation,
+FP64 weights / sums / Vxc accumulation) against the reference and the FP64
+GPU path. Tolerances are the stated accuracy of each split: the three-way
+split (6 products) targets FP32-level products, the two-way split (3 products)
+~2^-16 relative products."""
+import numpy as np
+import pytest
+
+from conftest import shell_table
+
+pytestmark = pytest.mark.gpu
+
+TOL = {6: (2e-7, 2e-6), 3: (2e-4, 2e-3)}  # split terms -> (|dExc| Eh, max|dVxc|)
+
+
+def engine(fx, **kw):
+    from proteindf_b200.xc import XcEngine
+    eng = XcEngine(**kw)
+    eng.set_system(shell_table(fx))
+    return eng
+
+
+@pytest.mark.parametrize("terms", [6, 3])
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_water2_mixed_vs_reference(water2, fn, terms):
+    eng = engine(water2, precision="mixed", split_terms=terms)
+    eng.set_grid(water2["grid"][:, :4])
+    exc, nel, V = eng.build_vxc(fn, water2["PA"])
+    dE = abs(exc - water2[f"{fn}_exc"][0])
+    dV = np.abs(V - water2[f"{fn}_vxc"]).max()
+    print(f"{fn} split{terms}: |dExc|={dE:.3e} max|dVxc|={dV:.3e}")
+    assert dE <= TOL[terms][0] and dV <= TOL[terms][1]
+    assert np.allclose(V, V.T, atol=0, rtol=0)
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_chain12_mixed_vs_reference(chain12, fn):
+    eng = engine(chain12, precision="mixed")
+    eng.set_grid(chain12["grid"][:, :4])
+    exc, nel, V = eng.build_vxc(fn, chain12["PA"])
+    dE = abs(exc - chain12[f"{fn}_exc"][0])
+    dV = np.abs(V - chain12[f"{fn}_vxc"]).max()
+    print(f"chain12 {fn}: |dExc|={dE:.3e} max|dVxc|={dV:.3e}")
+    assert dE <= TOL[6][0] and dV <= TOL[6][1]
+
+
+def test_mixed_vs_fp64_gpu_water8():
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    syms, xyz = systems.water_cluster(8, seed=0)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis())
+    z = [1 if s == "H" else 8 for s in syms]
+    P, W, A = grids.molecular_grid(xyz, z, nrad=40, nang=146, radial="GC", mapping="TA", pruning=True)
+    e64 = XcEngine()
+    e64.set_system(sh)
+    brad = np.array([grids.BECKE_RADIUS[zz] for zz in z])
+    w = e64.becke_weights(P, A, W, brad)
+    P, W, A = grids.screen_by_weight(P, w, A)
+    xyzw = np.concatenate([P, W[:, None]], axis=1)
+    PA = 0.5 * systems.density_matrix(sh.nao, 40, seed=0)
+    e64.set_grid(xyzw, A)
+    exc64, nel64, V64 = e64.build_vxc("B3LYP", PA)
+    em = XcEngine(precision="mixed")
+    em.set_system(sh)
+    em.set_grid(xyzw, A)
+    excm, nelm, Vm = em.build_vxc("B3LYP", PA)
+    print(f"(H2O)8 B3LYP mixed vs FP64: |dExc|={abs(excm - exc64):.3e} max|dVxc|={np.abs(Vm - V64).max():.3e}")
+    assert abs(excm - exc64) <= 1e-6
+    assert np.abs(Vm - V64).max() <= 1e-5
+    assert abs(nelm - nel64) <= 1e-6
+
+
+def test_mixed_incremental(water2):
+    eng = engine(water2, precision="mixed")
+    eng.set_grid(water2["grid"][:, :4])
+    PA = water2["PA"]
+    eng.build_vxc("B3LYP", 0.5 * PA)
+    exc_i, _, V_i = eng.build_vxc("B3LYP", 0.5 * PA, incremental=True)
+    exc_f, _, V_f = eng.build_vxc("B3LYP", PA)
+    assert abs(exc_i - exc_f) <= 1e-8
+    assert np.abs(V_i - V_f).max() <= 1e-7

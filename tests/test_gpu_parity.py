@@ -64,7 +64,7 @@ def test_full_grid_vs_oracle_water8():
     brad = np.array([grids.BECKE_RADIUS[zz] for zz in z])
     w = eng.becke_weights(P, A, W, brad)
     fac = oracle.becke(xyz, brad, P, A)
-    assert np.abs(w - W * fac).max() <= 1e-14 * np.abs(W).max()
+    assert np.all(np.abs(w - W * fac) <= 1e-13 * np.abs(W))
     P, W, A = grids.screen_by_weight(P, w, A)
     rng = np.random.default_rng(1)
     sel = np.sort(rng.choice(len(W), 20000, replace=False))
@@ -83,7 +83,8 @@ def test_becke_vs_reference(water2):
     eng = engine(water2)
     w = eng.becke_weights(water2["becke_points"], water2["becke_atom"], water2["becke_w_single"],
                           water2["radii"][:, 1])
-    assert np.abs(w - water2["becke_w_final"]).max() <= 1e-15 * np.abs(water2["becke_w_single"]).max()
+    # FP64 with a different operation order (fused multiply-adds): relative to each point's weight
+    assert np.all(np.abs(w - water2["becke_w_final"]) <= 1e-13 * np.abs(water2["becke_w_single"]))
 
 
 def test_incremental_density_update(water2):
