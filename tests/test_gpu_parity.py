@@ -124,8 +124,9 @@ def test_device_build_matches_host_build(water2):
     dV = torch.empty_like(dP)
     torch.cuda.synchronize()
     exc_d, nel_d = eng.build_vxc_device("B3LYP", dP.data_ptr(), dV.data_ptr())
-    assert exc_d == exc_h and nel_d == nel_h
-    assert np.array_equal(dV.cpu().numpy(), V_h)
+    # Vxc is accumulated with FP64 atomics: equal up to summation order
+    assert abs(exc_d - exc_h) <= 1e-13 and abs(nel_d - nel_h) <= 1e-13
+    assert np.abs(dV.cpu().numpy() - V_h).max() <= 1e-13
 
 
 def test_small_blocks_and_ragged_grid(water2):
