@@ -435,6 +435,80 @@ int runLebedev(const char* outPath) {
     return 0;
 }
 
+#ifdef PDFXC_DROPIN
+// Drop-in check (built as oracle/_ref/pdfxc_dropin, linked with libpdfxc):
+// the reference DfCalcGridX and DfCalcGridX_B200 on the same parameter set,
+// grid-matrix file and density, through the reference's own matrix classes,
+// for two SCF iterations (the second with xc-update on P_A/2, so the stored
+// rho columns of the first are read back from the grid-matrix file).
+}  // namespace
+#include "DfCalcGridX_B200.h"
+namespace {
+
+class GridFileWriter : public DfObject {
+   public:
+    explicit GridFileWriter(TlSerializeData* p) : DfObject(p) {}
+    void save(int iteration, const TlDenseGeneralMatrix_Lapack& g) { this->saveGridMatrix(iteration, g); }
+};
+
+template <class Engine, class Functional>
+double runEngine(TlSerializeData& param, int iteration, const TlDenseSymmetricMatrix_Lapack& P,
+                 Functional* f, TlDenseSymmetricMatrix_Lapack* F) {
+    param["num_of_iterations"] = iteration;
+    Engine e(&param);
+    return e.calcXCIntegForFockAndEnergy(P, f, F);
+}
+
+int runDropin(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    param["xc-update"] = "yes";
+    param["control"]["file_base_name"]["grid_matrix"] = "grid_%s.mat";
+    const std::string fn = c.get("functional", "SVWN");
+    const bool gga = isGGA(fn);
+    const long npts = std::atol(c.get("npts", "0").c_str());
+    const int ncol = gga ? 9 : 6;
+    const std::vector<double> grid = readDoubles(c.get("grid_file"), (size_t)npts * 5);
+    const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    TlDenseGeneralMatrix_Lapack gridMat(npts, ncol);
+    for (long i = 0; i < npts; ++i)
+        for (int k = 0; k < 5; ++k) gridMat.set(i, k, grid[5 * i + k]);
+    TlDenseSymmetricMatrix_Lapack PA(N), PA2(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) PA.set(i, j, P[(size_t)i * N + j]), PA2.set(i, j, 0.5 * P[(size_t)i * N + j]);
+    Out out(outPath);
+    for (int engine = 0; engine < 2; ++engine) {
+        GridFileWriter(&param).save(0, gridMat);
+        double e1 = 0, e2 = 0;
+        TlDenseSymmetricMatrix_Lapack F1(N), F2(N);
+        // iteration 1 with P_A/2, iteration 2 with the difference P_A/2 (xc-update)
+        if (gga) {
+            DfFunctional_GGA* f = makeGGA(fn);
+            e1 = engine ? runEngine<DfCalcGridX_B200>(param, 1, PA2, f, &F1) : runEngine<DfCalcGridX>(param, 1, PA2, f, &F1);
+            e2 = engine ? runEngine<DfCalcGridX_B200>(param, 2, PA2, f, &F2) : runEngine<DfCalcGridX>(param, 2, PA2, f, &F2);
+            delete f;
+        } else {
+            DfFunctional_LDA* f = makeLDA(fn);
+            e1 = engine ? runEngine<DfCalcGridX_B200>(param, 1, PA2, f, &F1) : runEngine<DfCalcGridX>(param, 1, PA2, f, &F1);
+            e2 = engine ? runEngine<DfCalcGridX_B200>(param, 2, PA2, f, &F2) : runEngine<DfCalcGridX>(param, 2, PA2, f, &F2);
+            delete f;
+        }
+        std::vector<double> v1((size_t)N * N), v2((size_t)N * N);
+        for (int i = 0; i < N; ++i)
+            for (int j = 0; j < N; ++j) v1[(size_t)i * N + j] = F1.get(i, j), v2[(size_t)i * N + j] = F2.get(i, j);
+        const char* tag = engine ? "b200" : "ref";
+        char name[32];
+        std::snprintf(name, sizeof(name), "%s_exc1", tag), out.put(name, e1);
+        std::snprintf(name, sizeof(name), "%s_exc2", tag), out.put(name, e2);
+        std::snprintf(name, sizeof(name), "%s_vxc1", tag), out.put(name, v1);
+        std::snprintf(name, sizeof(name), "%s_vxc2", tag), out.put(name, v2);
+    }
+    return 0;
+}
+#endif
+
 }  // namespace
 
 int main(int argc, char** argv) {
@@ -449,6 +523,9 @@ int main(int argc, char** argv) {
     if (mode == "xc") return runXc(c, argv[3]);
     if (mode == "grid") return runGrid(c, argv[3]);
     if (mode == "func") return runFunc(c, argv[3]);
+#ifdef PDFXC_DROPIN
+    if (mode == "dropin") return runDropin(c, argv[3]);
+#endif
     std::fprintf(stderr, "unknown mode %s\n", argv[1]);
     return 2;
 }

@@ -88,3 +88,27 @@ def run_func(workdir, functional, inputs5):
         f.write(f"functional {functional}\nnpts {len(inputs5)}\ninput_file {ipath}\n")
     r = run("func", case, os.path.join(workdir, "func_out.bin"))
     return r["values"].reshape(-1, 10)
+
+
+DROPIN_BIN = os.path.join(HERE, "_ref", "pdfxc_dropin")
+
+
+def dropin_available():
+    return os.path.exists(DROPIN_BIN)
+
+
+def run_dropin(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, timeout=None):
+    """Reference DfCalcGridX and DfCalcGridX_B200 on the same inputs, two SCF
+    iterations (P_A/2, then the difference P_A/2 with xc-update)."""
+    os.makedirs(os.path.join(workdir, "fl_Work"), exist_ok=True)
+    gpath = os.path.join(workdir, "grid.bin")
+    ppath = os.path.join(workdir, "P.bin")
+    np.ascontiguousarray(grid5, dtype=np.float64).tofile(gpath)
+    np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
+    case = os.path.join(workdir, "case.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, {
+        "functional": functional, "npts": len(grid5), "grid_file": gpath, "density_file": ppath})
+    out = os.path.join(workdir, "dropin.bin")
+    subprocess.run([DROPIN_BIN, "dropin", case, out], check=True, timeout=timeout, cwd=workdir,
+                   stdout=subprocess.DEVNULL)
+    return read_records(out)

@@ -422,7 +422,449 @@ __global__ void __launch_bounds__(128, 1)
     if (warp == 0) umma::tmem_dealloc(tmem, 128);
 }
 
+// ===========================================================================
+// Fixed-point slices on the INT8 tensor cores (the split-integer product of
+// Ozaki, Ogita, Oishi and Rump, 2012, on an integer unit). Each operand row
+// gets a power-of-two scale 2^e with |v| < 2^e and four signed 7-bit slices,
+// v = 2^e sum_{i=1..4} s_i 2^(-7 i) (slices rounded to nearest, the remainder
+// carried). A_i B_j^T is an exact integer product, accumulated exactly in
+// int32 TMEM; the products with i + j <= 5 are kept, one accumulator per
+// order k = i + j, and the epilogue forms 2^(eA + eB) sum_k 2^(-7 k) D_k in
+// FP64. The only rounding left is the slice truncation (~2^-28 of each row's
+// largest entry), which is unbiased; FP32 accumulation, whose rounding on the
+// tensor cores is toward zero, never occurs.
+
+__device__ __forceinline__ int oz_exponent(float m) { return m > 0.f ? ilogbf(m) + 1 : 0; }
+
+__device__ __forceinline__ void oz_slice(double v, int e, int8_t* s) {
+    double a = ldexp(v, -e);
+#pragma unroll
+    for (int i = 0; i < OZ_SLICES; ++i) {
+        a *= 128.0;
+        double q = rint(a);
+        q = fmin(fmax(q, -127.0), 127.0);
+        s[i] = (int8_t)q;
+        a -= q;
+    }
+}
+
+// 16 consecutive K values of one row -> four 16-byte slice stores.
+__device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
+    __align__(16) int8_t s[OZ_SLICES][16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        int8_t t[OZ_SLICES];
+        oz_slice(v[j], e, t);
+#pragma unroll
+        for (int i = 0; i < OZ_SLICES; ++i) s[i][j] = t[i];
+    }
+#pragma unroll
+    for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = *reinterpret_cast<uint4*>(s[i]);
+}
+
+// AO values (FP32 copy) and the row scales of phi^T (per point) and phi (per AO).
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_ao_oz(BasisView bas, GridView g, int blk0, char* ws) {
+    extern __shared__ unsigned int s_rowmax[];  // [nbp], float bits of max |phi| per AO
+    __shared__ float s_ptmax[2][BLOCK_PTS];
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp);
+    char* base = ws + m.ws;
+    float* phi32 = reinterpret_cast<float*>(base + L.phi32);
+    const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+    for (int r = threadIdx.x; r < m.nbp; r += blockDim.x) s_rowmax[r] = 0u;
+    __syncthreads();
+    const int p = threadIdx.x & (BLOCK_PTS - 1);
+    const int half = threadIdx.x >> 7;
+    const int gp = blk * BLOCK_PTS + p;
+    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
+    float ptmax = 0.f;
+    for (int i = half; i < m.nsh; i += 2) {
+        const int s = g.blk_shells[m.sh0 + i];
+        const int row0 = g.blk_shell_row[m.sh0 + i];
+        const int a = bas.sh_atom[s];
+        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
+        const double d2 = x * x + y * y + z * z;
+        const int Lq = bas.sh_l[s], n = 2 * Lq + 1, np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
+        for (int c = 0; c < n; ++c) {
+            double v = 0, gx = 0, gy = 0, gz = 0;
+            for (int k = 0; k < np; ++k) {
+                const double al = bas.p_exp[p0 + k];
+                if (al * d2 <= 30.0) {
+                    const double e = bas.p_coef[p0 + k] * exp(-al * d2);
+                    double av, ax, ay, az;
+                    ang_factor_m(Lq * Lq + c, x, y, z, 2.0 * al, av, ax, ay, az);
+                    v += av * e;
+                    if (GGA) gx += ax * e, gy += ay * e, gz += az * e;
+                }
+            }
+            const int mu = row0 + c;
+            const size_t o = (size_t)mu * BLOCK_PTS + p;
+            const float f = (float)v;
+            phi32[o] = f;
+            if (GGA) {
+                phi32[plane32 + o] = (float)gx;
+                phi32[2 * plane32 + o] = (float)gy;
+                phi32[3 * plane32 + o] = (float)gz;
+            }
+            ptmax = fmaxf(ptmax, fabsf(f));
+            atomicMax(&s_rowmax[mu], __float_as_uint(fabsf(f)));
+        }
+    }
+    for (int mu = m.nb + half; mu < m.nbp; mu += 2) {
+        const size_t o = (size_t)mu * BLOCK_PTS + p;
+        phi32[o] = 0.f;
+        if (GGA) phi32[plane32 + o] = phi32[2 * plane32 + o] = phi32[3 * plane32 + o] = 0.f;
+    }
+    s_ptmax[half][p] = ptmax;
+    __syncthreads();
+    int* e_pt = reinterpret_cast<int*>(base + L.e_pt);
+    int* e_phi = reinterpret_cast<int*>(base + L.e_phi);
+    if (threadIdx.x < BLOCK_PTS) e_pt[threadIdx.x] = oz_exponent(fmaxf(s_ptmax[0][threadIdx.x], s_ptmax[1][threadIdx.x]));
+    for (int r = threadIdx.x; r < m.nbp; r += blockDim.x) e_phi[r] = oz_exponent(__uint_as_float(s_rowmax[r]));
+}
+
+// Slices of phi^T (rows = points) and phi (rows = AOs).
+__global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp);
+    char* base = ws + m.ws;
+    const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+    const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
+    const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi);
+    double v[16];
+    const int g1 = m.nbp / 16;
+    for (int e = threadIdx.x; e < BLOCK_PTS * g1; e += blockDim.x) {  // phi^T: row p, 16 AOs
+        const int p = e % BLOCK_PTS, mu0 = (e / BLOCK_PTS) * 16;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = phi32[(size_t)(mu0 + j) * BLOCK_PTS + p];
+        oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
+    }
+    for (int e = threadIdx.x; e < m.nbp * (BLOCK_PTS / 16); e += blockDim.x) {  // phi: row mu, 16 points
+        const int mu = e / (BLOCK_PTS / 16), p0 = (e % (BLOCK_PTS / 16)) * 16;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = phi32[(size_t)mu * BLOCK_PTS + p0 + j];
+        oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), v, e_phi[mu]);
+    }
+}
+
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// P_sub slices, one warp per row mu: row scale first, then 16-column groups.
+__global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __restrict__ P, int nao, int blk0,
+                                                   char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp);
+    char* base = ws + m.ws;
+    int* e_p = reinterpret_cast<int*>(base + L.e_p);
+    const int* aos = g.blk_aos + m.ao0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double v[16];
+    for (int mu = warp; mu < m.nbp; mu += blockDim.x / 32) {
+        const bool live = mu < m.nb;
+        const double* row = live ? P + (size_t)aos[mu] * nao : P;
+        double mx = 0.0;
+        if (live)
+            for (int nu = lane; nu < m.nb; nu += 32) mx = fmax(mx, fabs(row[aos[nu]]));
+        mx = warp_max_d(mx);
+        const int e = oz_exponent((float)mx * 1.0000001f);
+        if (lane == 0) e_p[mu] = e;
+        for (int g0 = lane * 16; g0 < m.nbp; g0 += 32 * 16) {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int nu = g0 + j;
+                v[j] = (live && nu < m.nb) ? row[aos[nu]] : 0.0;
+            }
+            oz_store16(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, g0, m.nbp), v, e);
+        }
+    }
+}
+
+// Z slices, one warp per row nu (Z[nu][p] = 0.5 w vrho phi + c . grad phi).
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp);
+    char* base = ws + m.ws;
+    const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+    int* e_z = reinterpret_cast<int*>(base + L.e_z);
+    const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+    __shared__ double cf[4][BLOCK_PTS];
+    __shared__ double zrow[8][BLOCK_PTS];
+    for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
+        cf[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int nu = warp; nu < m.nbp; nu += 8) {
+        double mx = 0.0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int p = lane + 32 * j;
+            const size_t o = (size_t)nu * BLOCK_PTS + p;
+            double z = cf[0][p] * (double)phi32[o];
+            if (GGA)
+                z += cf[1][p] * (double)phi32[plane32 + o] + cf[2][p] * (double)phi32[2 * plane32 + o] +
+                     cf[3][p] * (double)phi32[3 * plane32 + o];
+            zrow[warp][p] = z;
+            mx = fmax(mx, fabs(z));
+        }
+        mx = warp_max_d(mx);
+        const int e = oz_exponent((float)mx * 1.0000001f);
+        if (lane == 0) e_z[nu] = e;
+        __syncwarp();
+        if (lane < BLOCK_PTS / 16)
+            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu, lane * 16, BLOCK_PTS),
+                       &zrow[warp][lane * 16], e);
+        __syncwarp();
+    }
+}
+
+// Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
+__constant__ int kOzA[10] = {1, 1, 2, 1, 2, 3, 1, 2, 3, 4};
+__constant__ int kOzB[10] = {1, 2, 1, 3, 2, 1, 4, 3, 2, 1};
+
+template <int MODE, bool GGA>
+__global__ void __launch_bounds__(128, 1)
+    k_oz(GridView g, int blk0, char* ws, int* err, int tiles_max, double* rho_acc, double* Vacc, int nao) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    constexpr int S = 3;
+    constexpr uint32_t stage_bytes = 2 * OZ_SLICES * umma::I8_SLAB_BYTES;  // 64 KiB
+    const int blk = blk0 + blockIdx.y;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp);
+    const int ntiles = m.nbp / umma::TILE_ROWS;
+    int mt, nt;
+    if (MODE == MODE_RHO) {
+        mt = 0, nt = blockIdx.x;
+        if (nt >= ntiles) return;
+    } else {
+        mt = blockIdx.x / tiles_max, nt = blockIdx.x % tiles_max;
+        if (mt >= ntiles || nt >= ntiles) return;
+    }
+    __shared__ int s_abort;
+    if (threadIdx.x == 0) s_abort = *reinterpret_cast<const volatile int*>(err);
+    __syncthreads();
+    if (s_abort) return;
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * stage_bytes);
+    uint64_t* empty = full + S;
+    uint64_t* done = empty + S;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
+
+    const char* base = ws + m.ws;
+    const char *Ab, *Bb;
+    size_t Aplane, Bplane;
+    int nslabs;
+    if (MODE == MODE_RHO) {
+        Ab = base + L.phi1;
+        Aplane = L.phi1_plane;
+        Bb = base + L.ppack + (size_t)nt * umma::TILE_ROWS * m.nbp;
+        Bplane = L.ppack_plane;
+        nslabs = m.nbp / (int)umma::I8_SLAB_K;
+    } else {
+        Ab = base + L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS;
+        Aplane = L.phi2_plane;
+        Bb = base + L.zpack + (size_t)nt * umma::TILE_ROWS * BLOCK_PTS;
+        Bplane = L.zpack_plane;
+        nslabs = BLOCK_PTS / (int)umma::I8_SLAB_K;
+    }
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (warp == 0) umma::tmem_alloc(tslot, 512);
+    if (threadIdx.x == 32) {
+        for (int s = 0; s < S; ++s) umma::mbar_init(&full[s], 1), umma::mbar_init(&empty[s], 1);
+        umma::mbar_init(done, 1);
+        umma::mbar_init_fence();
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = *tslot;
+
+    if (warp == 0 && lane == 0) {  // producer
+        for (int j = 0; j < nslabs; ++j) {
+            const int s = j % S;
+            if (j >= S && !umma::mbar_wait(&empty[s], ((j / S) - 1) & 1, err)) {
+                atomicExch(err, 1);
+                break;
+            }
+            uint8_t* st = smem + s * stage_bytes;
+            umma::mbar_expect_tx(&full[s], stage_bytes);
+            for (int a = 0; a < OZ_SLICES; ++a)
+                umma::bulk_g2s(st + a * umma::I8_SLAB_BYTES, Ab + a * Aplane + (size_t)j * umma::I8_SLAB_BYTES,
+                               umma::I8_SLAB_BYTES, &full[s]);
+            for (int b = 0; b < OZ_SLICES; ++b)
+                umma::bulk_g2s(st + (OZ_SLICES + b) * umma::I8_SLAB_BYTES,
+                               Bb + b * Bplane + (size_t)j * umma::I8_SLAB_BYTES, umma::I8_SLAB_BYTES, &full[s]);
+        }
+    } else if (warp == 1 && lane == 0) {  // MMA issuer
+        const uint32_t idesc = umma::instr_desc_s8(128, 128);
+        bool issued = false;
+        for (int j = 0; j < nslabs; ++j) {
+            const int s = j % S;
+            if (!umma::mbar_wait(&full[s], (j / S) & 1, err)) {
+                atomicExch(err, 2);
+                break;
+            }
+            umma::fence_after_sync();
+            const uint32_t st = umma::smem_u32(smem + s * stage_bytes);
+#pragma unroll
+            for (int kk = 0; kk < 2; ++kk) {
+#pragma unroll
+                for (int t = 0; t < 10; ++t) {
+                    const int i = kOzA[t], jj = kOzB[t];
+                    const uint32_t acc = tmem + (uint32_t)(i + jj - 2) * 128;
+                    const uint64_t ad =
+                        umma::smem_desc(st + (i - 1) * umma::I8_SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
+                    const uint64_t bd = umma::smem_desc(st + (OZ_SLICES + jj - 1) * umma::I8_SLAB_BYTES + kk * 4096,
+                                                        umma::LBO, umma::SBO);
+                    // the first product of each order starts its accumulator
+                    const bool first = (j == 0 && kk == 0 && (t == 0 || t == 1 || t == 3 || t == 6));
+                    umma::mma_s8(acc, ad, bd, idesc, first ? 0u : 1u);
+                }
+            }
+            issued = true;
+            umma::mma_commit(&empty[s]);
+        }
+        if (issued) umma::mma_commit(done);
+        else umma::mbar_expect_tx(done, 0);
+    }
+    __syncwarp();
+    bool waited = umma::mbar_wait(done, 0, err);
+    if (!waited) atomicExch(err, 3);
+    const bool ready = __syncthreads_and(waited) != 0;
+    umma::fence_after_sync();
+
+    if (ready) {
+        const int row = warp * 32 + lane;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+        const double w2 = 1.0 / 16384.0, w3 = w2 / 128.0, w4 = w3 / 128.0, w5 = w4 / 128.0;  // 2^-14 .. 2^-35
+        if (MODE == MODE_RHO) {
+            const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+            const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
+            const int* e_p = reinterpret_cast<const int*>(base + L.e_p);
+            const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+            const int ep = e_pt[row];
+            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+            for (int c0 = 0; c0 < 128; c0 += 16) {
+                uint32_t d2[16], d3[16], d4[16], d5[16];
+                umma::tmem_ld16_raw(taddr + c0, d2);
+                umma::tmem_ld16_raw(taddr + 128 + c0, d3);
+                umma::tmem_ld16_raw(taddr + 256 + c0, d4);
+                umma::tmem_ld16_raw(taddr + 384 + c0, d5);
+                umma::tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const int mu = nt * 128 + c0 + c;
+                    if (mu >= m.nb) break;
+                    const double s = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
+                                     (double)(int)d5[c] * w5;
+                    const double x = ldexp(s, ep + e_p[mu]);
+                    const size_t o = (size_t)mu * BLOCK_PTS + row;
+                    r += (double)phi32[o] * x;
+                    if (GGA) {
+                        gx += (double)phi32[plane32 + o] * x;
+                        gy += (double)phi32[2 * plane32 + o] * x;
+                        gz += (double)phi32[3 * plane32 + o] * x;
+                    }
+                }
+            }
+            double* acc = rho_acc + ((size_t)blk * BLOCK_PTS + row) * 4;
+            atomicAdd(acc, r);
+            if (GGA) atomicAdd(acc + 1, gx), atomicAdd(acc + 2, gy), atomicAdd(acc + 3, gz);
+        } else {
+            const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi);
+            const int* e_z = reinterpret_cast<const int*>(base + L.e_z);
+            const int* aos = g.blk_aos + m.ao0;
+            double* tile = reinterpret_cast<double*>(smem);  // [128][17]
+            const int mu_r = mt * 128 + row;
+            const int em = e_phi[mu_r];
+            for (int c0 = 0; c0 < 128; c0 += 16) {
+                uint32_t d2[16], d3[16], d4[16], d5[16];
+                umma::tmem_ld16_raw(taddr + c0, d2);
+                umma::tmem_ld16_raw(taddr + 128 + c0, d3);
+                umma::tmem_ld16_raw(taddr + 256 + c0, d4);
+                umma::tmem_ld16_raw(taddr + 384 + c0, d5);
+                umma::tmem_wait_ld();
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const double s = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
+                                     (double)(int)d5[c] * w5;
+                    tile[row * 17 + c] = ldexp(s, em + e_z[nt * 128 + c0 + c]);
+                }
+                __syncthreads();
+                const int c = threadIdx.x & 15;
+                const int nu = nt * 128 + c0 + c;
+                if (nu < m.nb) {
+                    const int anu = aos[nu];
+                    for (int rr = threadIdx.x >> 4; rr < 128; rr += 8) {
+                        const int mu = mt * 128 + rr;
+                        if (mu < m.nb) atomicAdd(&Vacc[(size_t)aos[mu] * nao + anu], tile[rr * 17 + c]);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 512);
+}
+
 }  // namespace
+
+size_t oz_smem_bytes() { return (size_t)3 * 2 * OZ_SLICES * umma::I8_SLAB_BYTES + 7 * 8 + 16; }
+
+void oz_prepare(const MixedArgs& a, cudaStream_t s) {
+    const size_t sm = sizeof(unsigned int) * a.max_nbp;
+    if (functional_is_gga(a.fn))
+        k_ao_oz<true><<<a.nblk, 256, sm, s>>>(a.b, a.g, a.blk0, a.ws);
+    else
+        k_ao_oz<false><<<a.nblk, 256, sm, s>>>(a.b, a.g, a.blk0, a.ws);
+    k_slice_phi<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
+    k_pack_p_oz<<<a.nblk, 256, 0, s>>>(a.g, a.P, a.nao, a.blk0, a.ws);
+}
+
+void oz_rho(const MixedArgs& a, cudaStream_t s) {
+    const int tiles = a.max_nbp / umma::TILE_ROWS;
+    const size_t smem = oz_smem_bytes();
+    if (functional_is_gga(a.fn)) {
+        cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_oz<MODE_RHO, true><<<dim3(tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, tiles, a.rho_acc,
+                                                                   a.Vacc, a.nao);
+    } else {
+        cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_oz<MODE_RHO, false><<<dim3(tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, tiles, a.rho_acc,
+                                                                    a.Vacc, a.nao);
+    }
+}
+
+void oz_functional(const MixedArgs& a, cudaStream_t s) {
+    if (functional_is_gga(a.fn)) {
+        k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
+                                                              a.rho_store, a.coef, a.blk_sum);
+        k_pack_z_oz<true><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+    } else {
+        k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
+                                                               a.rho_store, a.coef, a.blk_sum);
+        k_pack_z_oz<false><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+    }
+}
+
+void oz_vxc(const MixedArgs& a, cudaStream_t s) {
+    const int tiles = a.max_nbp / umma::TILE_ROWS;
+    const size_t smem = oz_smem_bytes();
+    cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_oz<MODE_VXC, false><<<dim3(tiles * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, tiles, a.rho_acc,
+                                                                        a.Vacc, a.nao);
+}
 
 size_t umma_smem_bytes(int nterms) {
     const int nA = nterms == 3 ? 2 : 3;

@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -112,7 +113,15 @@ pdfxc::GridView grid_view(const pdfxc_ctx* c) {
     return {c->d_px, c->d_py, c->d_pz, c->d_pw, c->d_meta, c->d_blk_shells, c->d_blk_shell_row, c->d_blk_aos};
 }
 
+void drop_graph(pdfxc_ctx* c) {
+    if (c->graph_exec) cudaGraphExecDestroy(c->graph_exec);
+    c->graph_exec = nullptr;
+    c->graph_fn = c->graph_inc = -1;
+    c->graph_P = nullptr;
+}
+
 void free_grid(pdfxc_ctx* c) {
+    drop_graph(c);
     dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
     dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
     dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum), dev_free(c->d_rho_acc);
@@ -146,12 +155,13 @@ pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt)
     if (opt) c->opt = *opt;
     if (c->opt.block_points <= 0 || c->opt.block_points > BLOCK_PTS) c->opt.block_points = BLOCK_PTS;
     if (c->opt.workspace_bytes == 0) c->opt.workspace_bytes = size_t(4) << 30;
-    if (c->opt.split_terms != 3 && c->opt.split_terms != 6) c->opt.split_terms = 6;
+    if (c->opt.split_terms != 3 && c->opt.split_terms != 6 && c->opt.split_terms != 10) c->opt.split_terms = 6;
     if (c->opt.precision != PDFXC_PRECISION_FP64 && c->opt.precision != PDFXC_PRECISION_MIXED) {
         delete c;
         return PDFXC_ERR_ARG;
     }
     c->device = device;
+    if (const char* g = std::getenv("PDFXC_GRAPH")) c->use_graph = std::atoi(g) != 0;
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || device < 0 || device >= ndev) {
         delete c;
@@ -312,8 +322,9 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
         size_t off = 0, max_ws = 0;
         Chunk cur{0, 0, 0, 0};
         for (int b = 0; b < nblk; ++b) {
-            const size_t need = mixed ? pdfxc::mixed_layout(ctx->h_meta[b].nbp).total
-                                      : pdfxc::block_ws_doubles(ctx->h_meta[b].nbp, gga_ws) * sizeof(double);
+            const size_t need = !mixed ? pdfxc::block_ws_doubles(ctx->h_meta[b].nbp, gga_ws) * sizeof(double)
+                                : ctx->opt.split_terms == 10 ? pdfxc::oz_layout(ctx->h_meta[b].nbp).total
+                                                             : pdfxc::mixed_layout(ctx->h_meta[b].nbp).total;
             if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
                 cur.b1 = b;
                 cur.ws_bytes = off;
@@ -419,7 +430,6 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         PDFXC_CUDA(cudaEventCreate(&e));
         ctx->stage_ev.push_back(e);
     }
-    PDFXC_CUDA(cudaEventRecord(ctx->ev[0], s));
     PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc, 0, sizeof(double) * (size_t)nao * nao, s));
     int64_t launches = 0;
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
@@ -433,16 +443,17 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         pdfxc::MixedArgs a{bv, gv, c.b0, c.b1 - c.b0, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
                            ctx->d_Vacc, ctx->d_err};
+        const bool oz = ctx->opt.split_terms == 10;
         PDFXC_CUDA(cudaEventRecord(e[0], s));
-        pdfxc::mixed_prepare(a, s);
+        oz ? pdfxc::oz_prepare(a, s) : pdfxc::mixed_prepare(a, s);
         PDFXC_CUDA(cudaEventRecord(e[1], s));
-        pdfxc::mixed_rho(a, s);
+        oz ? pdfxc::oz_rho(a, s) : pdfxc::mixed_rho(a, s);
         PDFXC_CUDA(cudaEventRecord(e[2], s));
-        pdfxc::mixed_functional(a, s);
+        oz ? pdfxc::oz_functional(a, s) : pdfxc::mixed_functional(a, s);
         PDFXC_CUDA(cudaEventRecord(e[3], s));
-        pdfxc::mixed_vxc(a, s);
+        oz ? pdfxc::oz_vxc(a, s) : pdfxc::mixed_vxc(a, s);
         PDFXC_CUDA(cudaEventRecord(e[4], s));
-        launches += 6;
+        launches += oz ? 7 : 6;
     }
     for (size_t ci = 0; ci < ctx->chunks.size() && !mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
@@ -464,7 +475,6 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     launches += 2;
     PDFXC_CUDA(cudaGetLastError());
     PDFXC_CUDA(cudaEventRecord(ctx->stage_ev[nev - 1], s));
-    PDFXC_CUDA(cudaEventRecord(ctx->ev[1], s));
     ctx->last_profile.launches = launches;
 }
 
@@ -480,9 +490,13 @@ void collect_profile(pdfxc_ctx* ctx) {
     pdfxc_profile& p = ctx->last_profile;
     p.total_ms = p.ao_ms = p.gemm_x_ms = p.rho_ms = p.gemm_v_ms = p.finish_ms = 0.f;
     PDFXC_CUDA(cudaEventElapsedTime(&p.total_ms, ctx->ev[0], ctx->ev[1]));
+    // stage timings are diagnostics: an event pair that cannot be timed reads 0
     auto dt = [](cudaEvent_t a, cudaEvent_t b) {
         float t = 0.f;
-        PDFXC_CUDA(cudaEventElapsedTime(&t, a, b));
+        if (cudaEventElapsedTime(&t, a, b) != cudaSuccess) {
+            cudaGetLastError();
+            t = 0.f;
+        }
         return t;
     };
     for (size_t ci = 0; ci < ctx->chunks.size(); ++ci) {
@@ -494,6 +508,37 @@ void collect_profile(pdfxc_ctx* ctx) {
     }
     const size_t last = 5 * ctx->chunks.size();
     p.finish_ms = dt(ctx->stage_ev[last - 1], ctx->stage_ev[last]);
+}
+
+// One build on ctx->stream. The sequence of launches is captured once into a
+// CUDA graph per (functional, incremental, density pointer) and replayed.
+void run_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental) {
+    if (!ctx->use_graph) {
+        PDFXC_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+        enqueue_build(ctx, fn, d_PA, incremental);
+        PDFXC_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
+        return;
+    }
+    if (!ctx->graph_exec || ctx->graph_fn != fn || ctx->graph_inc != (int)incremental || ctx->graph_P != d_PA) {
+        drop_graph(ctx);
+        cudaGraph_t g = nullptr;
+        PDFXC_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+        try {
+            enqueue_build(ctx, fn, d_PA, incremental);
+        } catch (...) {
+            cudaStreamEndCapture(ctx->stream, &g);
+            if (g) cudaGraphDestroy(g);
+            throw;
+        }
+        PDFXC_CUDA(cudaStreamEndCapture(ctx->stream, &g));
+        cudaError_t e = cudaGraphInstantiate(&ctx->graph_exec, g, 0);
+        cudaGraphDestroy(g);
+        PDFXC_CUDA(e);
+        ctx->graph_fn = fn, ctx->graph_inc = incremental, ctx->graph_P = d_PA;
+    }
+    PDFXC_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
+    PDFXC_CUDA(cudaGraphLaunch(ctx->graph_exec, ctx->stream));
+    PDFXC_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
 }
 
 pdfxc_status check_build(pdfxc_ctx* ctx, int functional, int incremental) {
@@ -525,7 +570,7 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
             ctx->err = "pdfxc_build_vxc_device: null device pointer";
             return PDFXC_ERR_ARG;
         }
-        enqueue_build(ctx, functional, d_PA, incremental != 0);
+        run_build(ctx, functional, d_PA, incremental != 0);
         const size_t n2 = (size_t)ctx->nao * ctx->nao;
         PDFXC_CUDA(cudaMemcpyAsync(d_V, ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         double sc[2];
@@ -555,7 +600,7 @@ pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, i
         }
         const size_t n2 = (size_t)ctx->nao * ctx->nao;
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, n2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
-        enqueue_build(ctx, functional, ctx->d_P, incremental != 0);
+        run_build(ctx, functional, ctx->d_P, incremental != 0);
         std::vector<double> V(n2);
         double sc[2];
         PDFXC_CUDA(cudaMemcpyAsync(V.data(), ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));

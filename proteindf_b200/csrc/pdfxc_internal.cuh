@@ -105,6 +105,12 @@ struct pdfxc_ctx {
     // stage events: per chunk 5 (before ao, gemm_x, rho, gemm_v, after gemm_v), then finish end
     std::vector<cudaEvent_t> stage_ev;
     pdfxc_profile last_profile{};
+
+    // one captured CUDA graph per build configuration (functional, incremental, density pointer)
+    bool use_graph = true;
+    cudaGraphExec_t graph_exec = nullptr;
+    int graph_fn = -1, graph_inc = -1;
+    const double* graph_P = nullptr;
 };
 
 namespace pdfxc {
@@ -167,6 +173,50 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
     return L;
 }
 
+// Intermediates of one block on the fixed-point (INT8 slice) path. Operands are
+// split into OZ_SLICES signed 7-bit slices with a power-of-two scale per row:
+// v = 2^e * sum_i s_i 2^(-7 i); slice planes are packed K-major in 64-byte slabs.
+constexpr int OZ_SLICES = 4;
+struct OzLayout {
+    size_t phi32;               // FP32 phi and grad phi, [4][nbp][128]
+    size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs
+    size_t phi2, phi2_plane;    // phi slices: rows = nbp AOs, K = 128 points
+    size_t ppack, ppack_plane;  // P_sub slices: rows = nbp, K = nbp
+    size_t zpack, zpack_plane;  // Z slices: rows = nbp, K = 128 points
+    size_t e_pt, e_phi, e_p, e_z;  // int exponents: per point (phi^T rows), per AO row of phi, P_sub, Z
+    size_t total;
+};
+
+__host__ __device__ inline OzLayout oz_layout(int nbp) {
+    auto a256 = [](size_t x) { return (x + 255) & ~size_t(255); };
+    OzLayout L;
+    size_t o = 0;
+    L.phi32 = o;
+    o = a256(o + (size_t)4 * nbp * BLOCK_PTS * 4);
+    L.phi1 = o;
+    L.phi1_plane = (size_t)BLOCK_PTS * nbp;
+    o = a256(o + OZ_SLICES * L.phi1_plane);
+    L.phi2 = o;
+    L.phi2_plane = (size_t)nbp * BLOCK_PTS;
+    o = a256(o + OZ_SLICES * L.phi2_plane);
+    L.ppack = o;
+    L.ppack_plane = (size_t)nbp * nbp;
+    o = a256(o + OZ_SLICES * L.ppack_plane);
+    L.zpack = o;
+    L.zpack_plane = (size_t)nbp * BLOCK_PTS;
+    o = a256(o + OZ_SLICES * L.zpack_plane);
+    L.e_pt = o;
+    o = a256(o + sizeof(int) * BLOCK_PTS);
+    L.e_phi = o;
+    o = a256(o + sizeof(int) * nbp);
+    L.e_p = o;
+    o = a256(o + sizeof(int) * nbp);
+    L.e_z = o;
+    o = a256(o + sizeof(int) * nbp);
+    L.total = o;
+    return L;
+}
+
 // kernels_mixed.cu: the four stages of one chunk on the mixed path
 struct MixedArgs {
     BasisView b;
@@ -183,5 +233,10 @@ void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub
 void mixed_functional(const MixedArgs& a, cudaStream_t s);  // functional, Z packing
 void mixed_vxc(const MixedArgs& a, cudaStream_t s);         // Vacc += phi Z^T
 size_t umma_smem_bytes(int nterms);
+// the same four stages with INT8 fixed-point slices (split_terms == 10)
+void oz_prepare(const MixedArgs& a, cudaStream_t s);
+void oz_rho(const MixedArgs& a, cudaStream_t s);
+void oz_functional(const MixedArgs& a, cudaStream_t s);
+void oz_vxc(const MixedArgs& a, cudaStream_t s);
 
 }  // namespace pdfxc

@@ -140,6 +140,48 @@ __device__ __forceinline__ void mma_commit(uint64_t* bar) {
                  : "memory");
 }
 
+// ---- INT8 operands (kind::i8, exact int32 accumulation) -------------------
+// Packed layout of an int8 matrix (R % 128 == 0 rows, K % 64 == 0 columns):
+// 128-row tiles, 64-byte K slabs (8 KiB), core matrices of 8 rows x 16 bytes
+// ordered [k16][r8] inside a slab. LBO = 2048 B, SBO = 128 B as for BF16;
+// one MMA consumes K = 32 (two 16-byte groups), step kk at kk * 4096 B.
+constexpr uint32_t I8_SLAB_K = 64;
+constexpr uint32_t I8_SLAB_BYTES = TILE_ROWS * I8_SLAB_K;  // 8 KiB
+
+__host__ __device__ inline size_t packed_offset_i8(int r, int k, int K) {
+    return (size_t)(r / 128) * 128 * K + (size_t)(k / 64) * I8_SLAB_BYTES +
+           (size_t)((((k % 64) / 16) * 16 + (r % 128) / 8) * 128 + (r % 8) * 16 + (k % 16));
+}
+
+// kind::i8: signed INT8 x signed INT8 -> S32, both K-major.
+__host__ __device__ constexpr uint32_t instr_desc_s8(int M, int N) {
+    return (2u << 4)                      // D format S32
+           | (1u << 7)                    // A format signed 8-bit
+           | (1u << 10)                   // B format signed 8-bit
+           | ((uint32_t)(N >> 3) << 17)   // N / 8
+           | ((uint32_t)(M >> 4) << 24);  // M / 16
+}
+
+__device__ __forceinline__ void mma_s8(uint32_t tmem_d, uint64_t adesc, uint64_t bdesc, uint32_t idesc,
+                                       uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}" ::"r"(tmem_d),
+        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+}
+
+// 32 lanes x 16 consecutive 32-bit columns per thread, raw bits.
+__device__ __forceinline__ void tmem_ld16_raw(uint32_t taddr, uint32_t* r) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+}
+
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+
 // 32 lanes x 16 consecutive 32-bit columns per thread.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float* v) {
     uint32_t r[16];

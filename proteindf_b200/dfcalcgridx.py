@@ -1,0 +1,92 @@
+"""Host mirror of ProteinDF's DfCalcGridX interface on top of libpdfxc.
+
+The reference class (src/libpdf/DfCalcGridX.h:72-212) is constructed from
+the parameter set (`coordinates`, `basis_set`, `xc-density-threshold`,
+`xc-update`, ...), reads the grid matrix written by DfGenerateGrid, and is
+called once per SCF iteration through
+
+    double calcXCIntegForFockAndEnergy(const P_A, DfFunctional_{LDA,GGA}*, F_A*)
+
+which accumulates Vxc into F_A and returns Exc (src/libpdf/DfCalcGridX.cpp:2280-2315).
+This class keeps those names, argument meanings and side effects: F_A is
+accumulated into (+=), the per-point rho columns of the grid matrix are
+updated (and, with xc-update = yes, the next call adds rho(dP) to them), and
+getWholeDensity returns sum_i w_i rho_A(r_i) (:2502-2537). Functionals are
+named as the reference's xc-potential keyword (DfXCFunctional.cpp:70-104).
+
+Open-shell overloads are not provided (they raise NotImplementedError).
+"""
+import numpy as np
+
+from . import basis as _basis
+from .xc import FUNCTIONALS, GGA, XcEngine
+
+GM_X, GM_Y, GM_Z, GM_WEIGHT, GM_ATOM_INDEX = 0, 1, 2, 3, 4
+GM_RHO_ALPHA = 5
+
+
+class DfCalcGridX:
+    def __init__(self, pdf_param, grid_matrix=None, device=0, precision="fp64"):
+        """pdf_param: {"coordinates": [(symbol, (x, y, z) bohr), ...],
+        "basis_set": name or {element: shells}, "xc-density-threshold": float,
+        "xc-update": "yes"|"no", "xc-potential": name}."""
+        self.param = dict(pdf_param)
+        atoms = self.param["coordinates"]
+        symbols = [a[0] for a in atoms]
+        xyz = np.array([a[1] for a in atoms], dtype=np.float64)
+        bs = self.param.get("basis_set", "cc-pVDZ")
+        bdata = _basis.load_basis(bs) if isinstance(bs, str) else bs
+        self.orbital_info = _basis.ShellTable(symbols, xyz, bdata)
+        self.num_of_AOs = self.orbital_info.nao
+        cut = self.param.get("xc-density-threshold", 1e-16)
+        self.is_update_xc = str(self.param.get("xc-update", "yes")).lower() != "no"
+        self._engine = XcEngine(device=device, precision=precision, rho_cutoff=float(cut))
+        self._engine.set_system(self.orbital_info)
+        self._iteration = 0
+        self._grid = None
+        self._functional_is_gga = None
+        if grid_matrix is not None:
+            self.setGridMatrix(grid_matrix)
+
+    # grid matrix (DfObject::getGridMatrix / saveGridMatrix, src/libpdf/DfObject.h:955-972)
+    def setGridMatrix(self, grid_matrix):
+        g = np.ascontiguousarray(grid_matrix, dtype=np.float64)
+        self._grid = g
+        self._engine.set_grid(g[:, :4], g[:, GM_ATOM_INDEX].astype(np.int32))
+        if g.shape[1] > GM_RHO_ALPHA:
+            gga = g.shape[1] >= GM_RHO_ALPHA + 4
+            self._engine.set_rho(g[:, GM_RHO_ALPHA:GM_RHO_ALPHA + (4 if gga else 1)], gga)
+            self._functional_is_gga = gga
+
+    def getGridMatrix(self):
+        """The grid matrix with the current rho (and grad rho) columns."""
+        gga = bool(self._functional_is_gga)
+        rho = self._engine.get_rho(gga)
+        return np.concatenate([self._grid[:, :5], rho], axis=1)
+
+    def calcXCIntegForFockAndEnergy(self, P_A, functional, F_A, P_B=None, F_B=None):
+        """Closed shell: F_A += Vxc(P_A); returns Exc. With xc-update = yes the
+        call after the first treats P_A as the density difference."""
+        if P_B is not None or F_B is not None:
+            raise NotImplementedError("open-shell overloads are not provided")
+        name = functional if isinstance(functional, str) else getattr(functional, "name")
+        name = name.upper()
+        if name not in FUNCTIONALS:
+            raise ValueError(f"unknown functional {name}")
+        gga = name in GGA
+        incremental = self.is_update_xc and self._iteration > 0 and self._functional_is_gga == gga
+        F = np.ascontiguousarray(F_A, dtype=np.float64)
+        exc, nel, F = self._engine.build_vxc(name, P_A, incremental=incremental, F=F)
+        if F is not F_A:
+            F_A[...] = F
+        self._functional_is_gga = gga
+        self._iteration += 1
+        self._nelec_alpha = nel
+        return exc
+
+    def getWholeDensity(self):
+        """(sum w rho_A, None) for the closed-shell case."""
+        return self._nelec_alpha, None
+
+    def close(self):
+        self._engine.close()

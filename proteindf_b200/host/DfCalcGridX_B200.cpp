@@ -1,0 +1,129 @@
+// DfCalcGridX_B200: see DfCalcGridX_B200.h.
+#include "DfCalcGridX_B200.h"
+
+#include <stdexcept>
+#include <string>
+
+#include "DfFunctional_B3LYP.h"
+#include "DfFunctional_B88LYP.h"
+#include "DfFunctional_Becke88.h"
+#include "DfFunctional_HFS.h"
+#include "DfFunctional_SVWN.h"
+
+namespace {
+
+void check(pdfxc_status st, pdfxc_ctx* ctx, const char* what) {
+    if (st != PDFXC_OK)
+        throw std::runtime_error(std::string(what) + " failed: " + (ctx ? pdfxc_last_error(ctx) : "no context"));
+}
+
+}  // namespace
+
+DfCalcGridX_B200::DfCalcGridX_B200(TlSerializeData* pPdfParam, int device, int precision)
+    : DfCalcGridX(pPdfParam) {
+    pdfxc_options opt;
+    pdfxc_default_options(&opt);
+    opt.precision = precision;
+    opt.rho_cutoff = this->inputtedDensityCutoffValue_;  // xc-density-threshold
+    check(pdfxc_create(&ctx_, device, &opt), nullptr, "pdfxc_create");
+
+    // shells from the reference's orbital table: a shell starts at its first
+    // component (basis type L*L); exponents and normalised coefficients are
+    // TlOrbitalInfo's own (src/libpdf/TlOrbitalInfoObject.cpp:38-99)
+    const TlOrbitalInfo& orb = this->m_tlOrbInfo;
+    const int natom = orb.getNumOfAtoms();
+    std::vector<double> xyz(3 * natom, 0.0);
+    std::vector<int> z(natom, 0);
+    std::vector<int> shAtom, shL, shNprim;
+    std::vector<double> pExp, pCoef;
+    const int nao = orb.getNumOfOrbitals();
+    for (int ao = 0; ao < nao; ++ao) {
+        const int a = orb.getAtomIndex(ao);
+        const TlPosition r = orb.getPosition(ao);
+        xyz[3 * a] = r.x(), xyz[3 * a + 1] = r.y(), xyz[3 * a + 2] = r.z();
+        z[a] = (int)orb.getAtomCharge(ao);
+        const int L = orb.getShellType(ao);
+        if (orb.getBasisType(ao) != L * L) continue;  // not the first component
+        shAtom.push_back(a);
+        shL.push_back(L);
+        const int np = orb.getCgtoContraction(ao);
+        shNprim.push_back(np);
+        for (int k = 0; k < np; ++k) {
+            pExp.push_back(orb.getExponent(ao, k));
+            pCoef.push_back(orb.getCoefficient(ao, k));
+        }
+    }
+    check(pdfxc_set_system(ctx_, natom, xyz.data(), z.data(), (int)shAtom.size(), shAtom.data(), shL.data(),
+                           shNprim.data(), pExp.data(), pCoef.data()),
+          ctx_, "pdfxc_set_system");
+}
+
+DfCalcGridX_B200::~DfCalcGridX_B200() { pdfxc_destroy(ctx_); }
+
+int DfCalcGridX_B200::functionalId(DfFunctional_LDA* f) {
+    if (dynamic_cast<DfFunctional_SVWN*>(f)) return PDFXC_SVWN;
+    if (dynamic_cast<DfFunctional_HFS*>(f)) return PDFXC_HFS;
+    throw std::runtime_error("DfCalcGridX_B200: unsupported LDA functional");
+}
+
+int DfCalcGridX_B200::functionalId(DfFunctional_GGA* f) {
+    if (dynamic_cast<DfFunctional_B3LYP*>(f)) return PDFXC_B3LYP;
+    if (dynamic_cast<DfFunctional_B88LYP*>(f)) return PDFXC_BLYP;
+    if (dynamic_cast<DfFunctional_Becke88*>(f)) return PDFXC_HFB;
+    throw std::runtime_error("DfCalcGridX_B200: unsupported GGA functional");
+}
+
+double DfCalcGridX_B200::calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                                     DfFunctional_LDA* pFunctional,
+                                                     TlDenseSymmetricMatrix_Lapack* pF_A) {
+    return this->build(P_A, functionalId(pFunctional), false, pF_A);
+}
+
+double DfCalcGridX_B200::calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                                     DfFunctional_GGA* pFunctional,
+                                                     TlDenseSymmetricMatrix_Lapack* pF_A) {
+    return this->build(P_A, functionalId(pFunctional), true, pF_A);
+}
+
+double DfCalcGridX_B200::build(const TlDenseSymmetricMatrix_Lapack& P_A, int fn, bool gga,
+                               TlDenseSymmetricMatrix_Lapack* pF_A) {
+    // the grid matrix of the previous iteration: points, weights and (for
+    // xc-update) the accumulated rho columns (DfCalcGridX.cpp:1816-1870)
+    TlDenseGeneralMatrix_Lapack gridMat =
+        DfObject::getGridMatrix<TlDenseGeneralMatrix_Lapack>(this->m_nIteration - 1);
+    const int64_t npts = gridMat.getNumOfRows();
+    const int nrho = gga ? 4 : 1;
+    if (!gridLoaded_) {
+        std::vector<double> xyzw(4 * npts);
+        std::vector<int> atom(npts);
+        for (int64_t i = 0; i < npts; ++i) {
+            for (int k = 0; k < 4; ++k) xyzw[4 * i + k] = gridMat.get(i, k);
+            atom[i] = (int)(gridMat.get(i, GM_ATOM_INDEX) + 0.5);
+        }
+        check(pdfxc_set_grid(ctx_, npts, xyzw.data(), atom.data()), ctx_, "pdfxc_set_grid");
+        gridLoaded_ = true;
+    }
+    const bool incremental = (this->m_nIteration > 1) && this->m_bIsUpdateXC;
+    if (incremental) {
+        std::vector<double> rho(nrho * npts);
+        for (int64_t i = 0; i < npts; ++i)
+            for (int k = 0; k < nrho; ++k) rho[nrho * i + k] = gridMat.get(i, GM_LDA_RHO_ALPHA + k);
+        check(pdfxc_set_rho(ctx_, gga ? 1 : 0, rho.data()), ctx_, "pdfxc_set_rho");
+    }
+    const int n = this->m_nNumOfAOs;
+    std::vector<double> P((size_t)n * n), F((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) P[(size_t)i * n + j] = P[(size_t)j * n + i] = P_A.get(i, j);
+    double exc = 0.0;
+    check(pdfxc_build_vxc(ctx_, fn, P.data(), incremental ? 1 : 0, F.data(), &exc, &nelecAlpha_), ctx_,
+          "pdfxc_build_vxc");
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) pF_A->add(i, j, F[(size_t)i * n + j]);
+    // write this iteration's grid matrix with the new rho columns
+    std::vector<double> rho(nrho * npts);
+    check(pdfxc_get_rho(ctx_, gga ? 1 : 0, rho.data()), ctx_, "pdfxc_get_rho");
+    for (int64_t i = 0; i < npts; ++i)
+        for (int k = 0; k < nrho; ++k) gridMat.set(i, GM_LDA_RHO_ALPHA + k, rho[nrho * i + k]);
+    DfObject::saveGridMatrix(this->m_nIteration, gridMat);
+    return exc;
+}

@@ -1,0 +1,58 @@
+// DfCalcGridX_B200: the drop-in for ProteinDF's DfCalcGridX on one B200.
+//
+// It derives from the reference class so that it keeps DfObject's parameter
+// and file plumbing (iteration number, xc-update, grid.mat) and the orbital
+// table, and it re-declares the closed-shell entry points the SCF driver
+// reaches through DfXCFunctional::getFxc<SymmetricMatrix, DfCalcGridClass>
+// (src/libpdf/DfXCFunctional.h:134-244):
+//
+//   double calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+//                                      DfFunctional_LDA* / DfFunctional_GGA*,
+//                                      TlDenseSymmetricMatrix_Lapack* F_A);
+//
+// (src/libpdf/DfCalcGridX.h:194-210). The computation runs in libpdfxc
+// (include/pdfxc.h). The side effects are the reference's: F_A is accumulated
+// into, the grid matrix of the previous iteration is read and the one of this
+// iteration is written with the new rho / grad rho columns
+// (src/libpdf/DfCalcGridX.cpp:1816-1860), so DfXCFunctional::checkGridAccuracy
+// and xc-update restarts keep working.
+//
+// Build: compile this file inside ProteinDF (it includes the reference's
+// headers) and link libpdfxc.so; see INTEGRATION.md.
+#ifndef DFCALCGRIDX_B200_H
+#define DFCALCGRIDX_B200_H
+
+#include <vector>
+
+#include "DfCalcGridX.h"
+#include "pdfxc.h"
+
+class DfCalcGridX_B200 : public DfCalcGridX {
+   public:
+    explicit DfCalcGridX_B200(TlSerializeData* pPdfParam, int device = 0,
+                              int precision = PDFXC_PRECISION_FP64);
+    virtual ~DfCalcGridX_B200();
+
+    double calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                       DfFunctional_LDA* pFunctional,
+                                       TlDenseSymmetricMatrix_Lapack* pF_A);
+    double calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                       DfFunctional_GGA* pFunctional,
+                                       TlDenseSymmetricMatrix_Lapack* pF_A);
+
+    // sum_i w_i rho_A(r_i) of the last build (DfCalcGridX::getWholeDensity)
+    double lastElectronCountAlpha() const { return nelecAlpha_; }
+
+   protected:
+    double build(const TlDenseSymmetricMatrix_Lapack& P_A, int functionalId, bool gga,
+                 TlDenseSymmetricMatrix_Lapack* pF_A);
+    static int functionalId(DfFunctional_LDA* f);
+    static int functionalId(DfFunctional_GGA* f);
+
+   private:
+    pdfxc_ctx* ctx_ = nullptr;
+    bool gridLoaded_ = false;
+    double nelecAlpha_ = 0.0;
+};
+
+#endif  // DFCALCGRIDX_B200_H

@@ -1,0 +1,28 @@
+"""The drop-in at the C++ class level: DfCalcGridX_B200 (proteindf_b200/host)
+beside the reference DfCalcGridX, both driven through the reference's own
+matrix classes, parameter set and grid-matrix files for two SCF iterations
+(the second with xc-update, so the rho columns written by the first are read
+back). Built as oracle/_ref/pdfxc_dropin from the reference sources."""
+import numpy as np
+import pytest
+
+from conftest import shell_table
+from oracle import refio
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.skipif(not refio.dropin_available(), reason="oracle/_ref/pdfxc_dropin not built")
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_dfcalcgridx_b200_matches_reference_class(tmp_path, water2, fn):
+    from proteindf_b200 import basis, systems
+    syms = [str(s) for s in water2["symbols"]]
+    g = water2["grid"][:3000]
+    r = refio.run_dropin(str(tmp_path), syms, systems.nuclear_charges(syms), water2["xyz"],
+                         basis.load_basis("cc-pVDZ"), fn, g, water2["PA"])
+    n = shell_table(water2).nao
+    for it in (1, 2):
+        e_ref, e_b = r[f"ref_exc{it}"][0], r[f"b200_exc{it}"][0]
+        v_ref, v_b = r[f"ref_vxc{it}"].reshape(n, n), r[f"b200_vxc{it}"].reshape(n, n)
+        assert abs(e_ref - e_b) <= 1e-8, (it, e_ref, e_b)
+        assert np.abs(v_ref - v_b).max() <= 1e-7, it

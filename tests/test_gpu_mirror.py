@@ -1,0 +1,30 @@
+"""proteindf_b200.dfcalcgridx.DfCalcGridX: the reference class's interface
+(accumulate into F_A, return Exc, xc-update across iterations, grid-matrix rho
+columns) on top of libpdfxc, against the reference fixtures."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def param(fx):
+    return {"coordinates": [(str(s), tuple(r)) for s, r in zip(fx["symbols"], fx["xyz"])],
+            "basis_set": "cc-pVDZ", "xc-update": "yes"}
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_mirror_two_iterations_with_xc_update(water2, fn):
+    from proteindf_b200.dfcalcgridx import DfCalcGridX
+    calc = DfCalcGridX(param(water2), grid_matrix=water2["grid"])
+    PA = water2["PA"]
+    F = np.zeros_like(PA)
+    calc.calcXCIntegForFockAndEnergy(0.5 * PA, fn, F)
+    F2 = np.zeros_like(PA)
+    exc = calc.calcXCIntegForFockAndEnergy(0.5 * PA, fn, F2)   # xc-update: rho(P/2) + rho(P/2)
+    assert abs(exc - water2[f"{fn}_exc"][0]) <= 1e-8
+    assert np.abs(F2 - water2[f"{fn}_vxc"]).max() <= 1e-7
+    g = calc.getGridMatrix()
+    assert np.abs(g[:, 5:] - water2[f"{fn}_rho"]).max() <= 1e-9
+    nel, _ = calc.getWholeDensity()
+    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-9
+    calc.close()

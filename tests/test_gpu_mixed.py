@@ -73,6 +73,32 @@ def test_mixed_vs_fp64_gpu_water8():
     assert abs(nelm - nel64) <= 2e-6 * abs(nel64)
 
 
+# INT8 fixed-point slices (split_terms = 10): exact integer accumulation, only
+# the unbiased slice truncation (~2^-28 of each row's largest entry) remains.
+OZ_TOL = (1e-9, 1e-8)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "HFB", "B3LYP"])
+def test_water2_int8_slices_vs_reference(water2, fn):
+    eng = engine(water2, precision="mixed", split_terms=10)
+    eng.set_grid(water2["grid"][:, :4])
+    exc, nel, V = eng.build_vxc(fn, water2["PA"])
+    dE = abs(exc - water2[f"{fn}_exc"][0])
+    dV = np.abs(V - water2[f"{fn}_vxc"]).max()
+    print(f"{fn} int8 slices: |dExc|={dE:.3e} max|dVxc|={dV:.3e}")
+    assert within(exc, water2[f"{fn}_exc"][0], V, water2[f"{fn}_vxc"], OZ_TOL)
+    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-9 * abs(nel)
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_chain12_int8_slices_vs_reference(chain12, fn):
+    eng = engine(chain12, precision="mixed", split_terms=10)
+    eng.set_grid(chain12["grid"][:, :4])
+    exc, nel, V = eng.build_vxc(fn, chain12["PA"])
+    print(f"chain12 {fn} int8 slices: |dExc|={abs(exc - chain12[f'{fn}_exc'][0]):.3e}")
+    assert within(exc, chain12[f"{fn}_exc"][0], V, chain12[f"{fn}_vxc"], OZ_TOL)
+
+
 def test_mixed_incremental(water2):
     eng = engine(water2, precision="mixed")
     eng.set_grid(water2["grid"][:, :4])
