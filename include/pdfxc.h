@@ -146,6 +146,27 @@ pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out);
 const char* pdfxc_last_error(const pdfxc_ctx* ctx);
 void pdfxc_destroy(pdfxc_ctx* ctx);
 
+/* FP64 XC build that allocates nothing. This entry point has no counterpart
+ * in the reference; it exists for callers that cannot call cudaMalloc (their
+ * device memory belongs to a pool or arena they do not control, or they run
+ * where allocation is forbidden). Every operand is a device pointer the caller
+ * owns: the shells as in pdfxc_set_system, npts grid rows (x, y, z, w), the
+ * n_ao x n_ao alpha density d_PA; d_V (n_ao x n_ao) is overwritten with Vxc
+ * and d_exc_nelec[0..1] with Exc and sum_i w_i rho_A(r_i). The intermediates
+ * live in a fixed 32 MiB __device__ array of the library, held by every GPU
+ * that loads it until the process exits. Limits: n_ao <= 256, nshell <= 256,
+ * else PDFXC_ERR_ARG. Every call shares that array (the accumulators are
+ * cleared at the start of a call), so calls that overlap on the GPU race; the
+ * call synchronises `stream` (a cudaStream_t, NULL = default stream) before it
+ * returns. Its first call on a device looks up the array's device address;
+ * make that first call before any stream capture. */
+pdfxc_status pdfxc_build_vxc_noalloc(int device, int functional, int natom, const double* d_atom_xyz,
+                                     int nshell, const int* d_shell_atom, const int* d_shell_l,
+                                     const int* d_shell_nprim, const double* d_prim_exp,
+                                     const double* d_prim_coef, int nao, int64_t npts,
+                                     const double* d_xyzw, const double* d_PA, double* d_V,
+                                     double* d_exc_nelec, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -19,7 +19,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 EXPORTS = [
     "pdfxc_default_options", "pdfxc_create", "pdfxc_set_system", "pdfxc_set_grid", "pdfxc_becke_weights",
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
-    "pdfxc_last_profile", "pdfxc_last_error", "pdfxc_destroy",
+    "pdfxc_last_profile", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
 ]
 
 
@@ -62,6 +62,8 @@ def load_library(path=LIB_PATH):
     L.pdfxc_last_error.restype = ctypes.c_char_p
     L.pdfxc_destroy.argtypes = [_vp]
     L.pdfxc_destroy.restype = None
+    L.pdfxc_build_vxc_noalloc.argtypes = [i32, i32, i32, _vp, i32, _vp, _vp, _vp, _vp, _vp, i32, i64, _vp, _vp, _vp,
+                                          _vp, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
             getattr(L, name).restype = i32
