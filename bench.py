@@ -37,6 +37,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--split-terms", type=int, default=10, choices=[3, 6, 10],
+                    help="mixed path: 3/6 split-BF16 products, 10 = INT8 fixed-point slices")
     ap.add_argument("--natoms", type=int, default=100)
     ap.add_argument("--functional", default="B3LYP")
     ap.add_argument("--grid", default="ULTRA_FINE")
@@ -73,6 +75,7 @@ def config(args, npts, nao, **extra):
     c = {"workload": f"{args.natoms}-atom peptide-like chain, cc-pVDZ, {args.functional}, {args.grid} grid",
          "atoms": args.natoms, "n_ao": nao, "grid_points": int(npts), "functional": args.functional,
          "grid": args.grid, "precision": args.precision, "nocc": args.nocc,
+         "split_terms": args.split_terms if args.precision == "mixed" else None,
          "l2": "flushed between timed steps (512 MiB write)"}
     c.update(extra)
     return c
@@ -217,7 +220,7 @@ def main():
     from proteindf_b200.xc import XcEngine
 
     syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed + rank)
-    eng = XcEngine(device=local, precision=args.precision)
+    eng = XcEngine(device=local, precision=args.precision, split_terms=args.split_terms)
     eng.set_system(sh)
     grid4, owner = final_grid(eng, P, W, A, brad)
     eng.set_grid(grid4, owner)

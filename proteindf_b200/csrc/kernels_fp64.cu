@@ -107,9 +107,18 @@ __global__ void __launch_bounds__(256) k_ao_eval(BasisView bas, GridView g, int 
     }
 }
 
-// X[m][p] = sum_k P[aos[m]][aos[k]] phi[k][p]; tile 64 rows x 128 points, K step 16.
-// 256 threads; thread (ty, tx) owns rows ty*4 + i and points tx + 16 j.
-constexpr int GX_BM = 64, GX_BK = 16;
+// FP64 tensor-core MMA: D(8x8) += A(8x4, row-major) B(4x8, col-major), FP64 in and out.
+// Per thread (g = lane / 4, t = lane % 4): a = A[g][t], b = B[t][g], d = {D[g][2t], D[g][2t+1]}.
+__device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+// X[m][p] = sum_k P[aos[m]][aos[k]] phi[k][p]: CTA tile 64 rows x 128 points, K step 16,
+// 8 warps as 2 x 4 warp tiles of 32 x 32 (4 x 4 DMMA tiles). The next K step's operands
+// are fetched into registers while the current one is multiplied.
+constexpr int GX_BM = 64, GX_BK = 16, GX_AS = GX_BK + 2, GX_BS = BLOCK_PTS + 4;
 __global__ void __launch_bounds__(256) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
                                                 int blk0, char* ws) {
     const int blk = blk0 + blockIdx.y;
@@ -122,52 +131,70 @@ __global__ void __launch_bounds__(256) k_gemm_x(GridView g, const double* __rest
     double* X = reinterpret_cast<double*>(ws + m.ws) + (size_t)nplanes * m.nbp * BLOCK_PTS;
     const int* aos = g.blk_aos + m.ao0;
 
-    __shared__ double As[GX_BK][GX_BM + 1];
-    __shared__ double Bs[GX_BK][BLOCK_PTS];
-    const int t = threadIdx.x, tx = t & 15, ty = t >> 4;
-    double acc[4][8];
+    __shared__ double As[GX_BM * GX_AS];   // [m][k]
+    __shared__ double Bs[GX_BK * GX_BS];   // [k][n]
+    __shared__ int s_row[GX_BM];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wm = warp >> 2, wn = warp & 3, gq = lane >> 2, tq = lane & 3;
+    for (int r = t; r < GX_BM; r += 256) s_row[r] = (m0 + r < m.nb) ? aos[m0 + r] : -1;
+    __syncthreads();
+
+    double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
 
+    double ra[4], rb[8];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {  // A: 64 x 16 gathered from P (L2-resident)
+            const int e = t + q * 256, r = e >> 4, c = e & 15, gc = k0 + c;
+            const int row = s_row[r];
+            ra[q] = (row >= 0 && gc < m.nb) ? __ldg(P + (size_t)row * nao + aos[gc]) : 0.0;
+        }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {  // B: 16 x 128 of phi, coalesced
+            const int e = t + q * 256, r = e >> 7, c = e & 127;
+            rb[q] = phi[(size_t)(k0 + r) * BLOCK_PTS + c];
+        }
+    };
+    fetch(0);
     for (int k0 = 0; k0 < m.nbp; k0 += GX_BK) {
-        // A tile: 64 x 16 gathered from P (4 per thread)
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
             const int e = t + q * 256;
-            const int r = e >> 4, c = e & 15;
-            const int gr = m0 + r, gc = k0 + c;
-            double v = 0.0;
-            if (gr < m.nb && gc < m.nb) v = P[(size_t)aos[gr] * nao + aos[gc]];
-            As[c][r] = v;
+            As[(e >> 4) * GX_AS + (e & 15)] = ra[q];
         }
-        // B tile: 16 x 128 of phi (8 per thread, coalesced)
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
             const int e = t + q * 256;
-            const int r = e >> 7, c = e & 127;
-            Bs[r][c] = phi[(size_t)(k0 + r) * BLOCK_PTS + c];
+            Bs[(e >> 7) * GX_BS + (e & 127)] = rb[q];
         }
         __syncthreads();
+        if (k0 + GX_BK < m.nbp) fetch(k0 + GX_BK);
 #pragma unroll
-        for (int kk = 0; kk < GX_BK; ++kk) {
-            double a[4], b[8];
+        for (int kk = 0; kk < GX_BK; kk += 4) {
+            double a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+            for (int i = 0; i < 4; ++i) a[i] = As[(wm * 32 + i * 8 + gq) * GX_AS + kk + tq];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) b[j] = Bs[kk][tx + 16 * j];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + tq) * GX_BS + wn * 32 + j * 8 + gq];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j) X[(size_t)(m0 + ty * 4 + i) * BLOCK_PTS + tx + 16 * j] = acc[i][j];
+        for (int j = 0; j < 4; ++j) {
+            double2* dst = reinterpret_cast<double2*>(X + (size_t)(m0 + wm * 32 + i * 8 + gq) * BLOCK_PTS + wn * 32 +
+                                                      j * 8 + 2 * tq);
+            *dst = make_double2(acc[i][j][0], acc[i][j][1]);
+        }
 }
 
 __device__ __forceinline__ double warp_sum(double v) {
@@ -234,10 +261,12 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int bl
     }
 }
 
-// Vacc[aos[m]][aos[n]] += sum_p phi[m][p] Z[n][p], tile 64 x 64, K = 128 points in steps of 16.
-constexpr int GV_B = 64, GV_BK = 16;
+// Vacc[aos[m]][aos[n]] += sum_p phi[m][p] Z[n][p]: CTA tile 64 x 64 AOs, K = 128 points in
+// steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles); Z is formed from
+// phi, grad phi and the per-point coefficients while the B tile is staged.
+constexpr int GV_B = 64, GV_BK = 16, GV_AS = GV_BK + 2, GV_BS = GV_B + 4;
 template <bool GGA>
-__global__ void __launch_bounds__(256) k_gemm_v(GridView g, int blk0, const double* __restrict__ coef,
+__global__ void __launch_bounds__(128) k_gemm_v(GridView g, int blk0, const double* __restrict__ coef,
                                                 char* ws, double* Vacc, int nao, int tiles) {
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
@@ -248,58 +277,59 @@ __global__ void __launch_bounds__(256) k_gemm_v(GridView g, int blk0, const doub
     const size_t plane = (size_t)m.nbp * BLOCK_PTS;
     const int* aos = g.blk_aos + m.ao0;
     __shared__ double cf[4][BLOCK_PTS];
-    __shared__ double As[GV_BK][GV_B + 1];
-    __shared__ double Bs[GV_BK][GV_B + 1];
-    const int t = threadIdx.x;
-    for (int e = t; e < 4 * BLOCK_PTS; e += 256) {
+    __shared__ double As[GV_B * GV_AS];  // [m][k]
+    __shared__ double Bs[GV_BK * GV_BS];  // [k][n]
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int wm = warp >> 1, wn = warp & 1, gq = lane >> 2, tq = lane & 3;
+    for (int e = t; e < 4 * BLOCK_PTS; e += 128) {
         const int pp = e >> 2, k = e & 3;
         cf[k][pp] = coef[((size_t)blk * BLOCK_PTS + pp) * 4 + k];
     }
-    const int tx = t & 15, ty = t >> 4;
-    double acc[4][4];
+    double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = 0.0;
+        for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
     __syncthreads();
     for (int k0 = 0; k0 < BLOCK_PTS; k0 += GV_BK) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const int e = t + q * 256;
+        for (int q = 0; q < 8; ++q) {
+            const int e = t + q * 128;
             const int r = e >> 4, c = e & 15;  // row within tile, point within K step
             const int pp = k0 + c;
-            As[c][r] = phi[(size_t)(m0 + r) * BLOCK_PTS + pp];
+            As[r * GV_AS + c] = phi[(size_t)(m0 + r) * BLOCK_PTS + pp];
             const size_t on = (size_t)(n0 + r) * BLOCK_PTS + pp;
             double z = cf[0][pp] * phi[on];
             if (GGA)
                 z += cf[1][pp] * phi[plane + on] + cf[2][pp] * phi[2 * plane + on] +
                      cf[3][pp] * phi[3 * plane + on];
-            Bs[c][r] = z;
+            Bs[c * GV_BS + r] = z;
         }
         __syncthreads();
 #pragma unroll
-        for (int kk = 0; kk < GV_BK; ++kk) {
+        for (int kk = 0; kk < GV_BK; kk += 4) {
             double a[4], b[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
+            for (int i = 0; i < 4; ++i) a[i] = As[(wm * 32 + i * 8 + gq) * GV_AS + kk + tq];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx + 16 * j];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + tq) * GV_BS + wn * 32 + j * 8 + gq];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+                for (int j = 0; j < 4; ++j) dmma(acc[i][j][0], acc[i][j][1], a[i], b[j]);
         }
         __syncthreads();
     }
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const int r = m0 + ty * 4 + i;
+        const int r = m0 + wm * 32 + i * 8 + gq;
         if (r >= m.nb) continue;
         const size_t rowoff = (size_t)aos[r] * nao;
 #pragma unroll
         for (int j = 0; j < 4; ++j) {
-            const int c = n0 + tx + 16 * j;
-            if (c < m.nb) atomicAdd(&Vacc[rowoff + aos[c]], acc[i][j]);
+            const int c = n0 + wn * 32 + j * 8 + 2 * tq;
+            if (c < m.nb) atomicAdd(&Vacc[rowoff + aos[c]], acc[i][j][0]);
+            if (c + 1 < m.nb) atomicAdd(&Vacc[rowoff + aos[c + 1]], acc[i][j][1]);
         }
     }
 }
@@ -355,9 +385,9 @@ void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga,
     const int tiles = (max_nbp + GV_B - 1) / GV_B;
     dim3 grid(tiles * tiles, nblk);
     if (gga)
-        k_gemm_v<true><<<grid, 256, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+        k_gemm_v<true><<<grid, 128, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
     else
-        k_gemm_v<false><<<grid, 256, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+        k_gemm_v<false><<<grid, 128, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
 }
 
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk, double* scalars,
