@@ -7,8 +7,13 @@ cc-pVDZ (5d; the 6-31G** stand-in, ~930 AOs), B3LYP, ULTRA_FINE 99x590 grid
 density P_A = C C^T from the QR of a seeded N(0,1) N x 380 matrix. One step is
 one closed-shell Vxc build (rho pass + Vxc pass) of the whole grid.
 
-  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision fp64|mixed]
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--precision both|fp64|mixed]
   python bench.py --impl reference ...   (the reference's CPU DfCalcGridX, sampled)
+
+With --precision both (default) the same grid is built with the FP64 drop-in and
+the mixed path (INT8 fixed-point slices on the tensor cores by default); the
+headline value is the mixed path, the line carries the FP64 numbers, the
+mixed-vs-FP64 speed-up and |dExc| / max|dVxc| between them.
 
 Under torchrun (N > 1) every rank builds its own chain (seed + rank): the units
 are independent molecules, no data-path collective; value = all ranks' points
@@ -36,7 +41,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="both", choices=["both", "fp64", "mixed"])
     ap.add_argument("--split-terms", type=int, default=10, choices=[3, 6, 10],
                     help="mixed path: 3/6 split-BF16 products, 10 = INT8 fixed-point slices")
     ap.add_argument("--natoms", type=int, default=100)
@@ -75,7 +80,7 @@ def config(args, npts, nao, **extra):
     c = {"workload": f"{args.natoms}-atom peptide-like chain, cc-pVDZ, {args.functional}, {args.grid} grid",
          "atoms": args.natoms, "n_ao": nao, "grid_points": int(npts), "functional": args.functional,
          "grid": args.grid, "precision": args.precision, "nocc": args.nocc,
-         "split_terms": args.split_terms if args.precision == "mixed" else None,
+         "split_terms": args.split_terms if args.precision != "fp64" else None,
          "l2": "flushed between timed steps (512 MiB write)"}
     c.update(extra)
     return c
@@ -220,50 +225,63 @@ def main():
     from proteindf_b200.xc import XcEngine
 
     syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed + rank)
-    eng = XcEngine(device=local, precision=args.precision, split_terms=args.split_terms)
-    eng.set_system(sh)
-    grid4, owner = final_grid(eng, P, W, A, brad)
-    eng.set_grid(grid4, owner)
-    stats = eng.grid_stats()
-    npts = len(grid4)
+    dev = f"cuda:{local}"
     nao = sh.nao
-    dP = torch.tensor(PA, device=f"cuda:{local}")
+    dP = torch.tensor(PA, device=dev)
     dV = torch.empty_like(dP)
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=f"cuda:{local}")
-
-    for _ in range(args.warmup):
-        eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
-    torch.cuda.synchronize()
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
 
     def barrier():
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
 
-    prof_sum = {}
-    dev_ms = 0.0
-    launches = 0
-    barrier()
-    with ClockSampler(local) as clk:
-        wall0 = time.perf_counter()
-        for _ in range(args.steps):
-            flush.zero_()
-            torch.cuda.synchronize()
-            exc, nel = eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
-            p = eng.last_profile()
-            dev_ms += p["total_ms"]
-            launches += p["launches"]
-            for k, v in p.items():
-                prof_sum[k] = prof_sum.get(k, 0.0) + v
-        barrier()
-        wall = time.perf_counter() - wall0
-    t_dev = torch.tensor([dev_ms], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(t_dev, op=torch.distributed.ReduceOp.MAX)
-    ms_per_step = float(t_dev.item()) / args.steps
-    value = world * npts / (ms_per_step * 1e-3)
+    def max_over_ranks(x):
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        if world > 1:
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
 
-    # end to end through the host API: P from pinned host memory in, Vxc out
+    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    engines = {p: XcEngine(device=local, precision=p, split_terms=args.split_terms) for p in precisions}
+    for e in engines.values():
+        e.set_system(sh)
+    grid4, owner = final_grid(next(iter(engines.values())), P, W, A, brad)
+    npts = len(grid4)
+    res = {}
+    clk_summary = None
+    for p, eng in engines.items():
+        eng.set_grid(grid4, owner)
+        for _ in range(args.warmup):
+            eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+        dev_ms, launches = 0.0, 0
+        barrier()
+        with ClockSampler(local) as clk:
+            for _ in range(args.steps):
+                flush.zero_()
+                torch.cuda.synchronize()
+                exc, nel = eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+                prof = eng.last_profile()
+                dev_ms += prof["total_ms"]
+                launches += prof["launches"]
+            barrier()
+        if p == precisions[-1]:
+            clk_summary = clk.summary()
+        V = dV.cpu().numpy()
+        # one build launched stage by stage for the per-stage times (same kernels, no graph)
+        eng.set_profiling(True)
+        flush.zero_()
+        torch.cuda.synchronize()
+        eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+        stage = eng.last_profile()
+        eng.set_profiling(False)
+        ms = max_over_ranks(dev_ms) / args.steps
+        res[p] = {"ms": ms, "value": world * npts / (ms * 1e-3), "exc": exc, "nel": nel, "V": V, "stage": stage,
+                  "launches": launches, "stats": eng.grid_stats()}
+
+    head = precisions[-1]
+    eng = engines[head]
+    # end to end through the host API: P from pinned host memory in, Vxc (F += Vxc) back
     pin_P = torch.empty((nao, nao), dtype=torch.float64, pin_memory=True)
     pin_P.copy_(torch.from_numpy(PA))
     pin_F = torch.zeros((nao, nao), dtype=torch.float64, pin_memory=True)
@@ -274,43 +292,63 @@ def main():
         t0 = time.perf_counter()
         eng.build_vxc(args.functional, pin_P.numpy(), F=pin_F.numpy())
         e2e_t.append(time.perf_counter() - t0)
-    t_e2e = torch.tensor([float(np.mean(e2e_t))], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        torch.distributed.all_reduce(t_e2e, op=torch.distributed.ReduceOp.MAX)
+    t_e2e = max_over_ranks(float(np.mean(e2e_t)))
 
     if rank == 0:
-        # roofline of the dominant contraction kernel
         peaks = measured_peaks()
-        flops = stats["contraction_flops"]  # sum over blocks of 4 nb^2 np: both contractions
-        per = {k: prof_sum[k] / args.steps for k in ("ao_ms", "gemm_x_ms", "rho_ms", "gemm_v_ms", "finish_ms")}
-        top = max(("gemm_x_ms", "gemm_v_ms"), key=lambda k: per[k])
-        achieved = 0.5 * flops / (per[top] * 1e-3) / 1e12
-        if args.precision == "fp64":
-            peak = fp64_gemm_peak(torch)
-            peak_note = "measured cuBLAS FP64 DGEMM 8192^3 on this GPU (burst)"
-        else:
-            peak = peaks.get("bf16_tflops", 1590.0)
-            peak_note = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1.59 PFLOP/s"
-        roof = {"bound": "tensor", "kernel": top.replace("_ms", ""), "achieved": achieved, "peak": peak,
-                "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "peak_source": peak_note,
-                "flops_per_build": 0.5 * flops, "stage_ms": per}
+        rooflines = {p: roofline(args, torch, peaks, res[p], p) for p in precisions}
         cpu = None
         if not args.no_cpu_baseline:
             grid5 = np.concatenate([grid4, owner[:, None].astype(np.float64)], axis=1)
             cpu = cpu_baseline(args, syms, xyz, grid5, PA, args.cpu_sample)
-        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
-                "vs_baseline": None, "dtype": "f64" if args.precision == "fp64" else "bf16x3/f32/f64",
+        h = res[head]
+        dtype = "f64" if head == "fp64" else ("int8 fixed-point slices/i32/f64" if args.split_terms == 10
+                                              else "bf16 split/f32/f64")
+        line = {"metric": METRIC, "value": h["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": h["ms"], "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": dtype,
                 "data": "synthetic (seeded chain and density, ProteinDF grid recipe)",
-                "config": config(args, npts, nao, blocks=stats["nblocks"], mean_screened_aos=stats["mean_nb"]),
-                "exc": exc, "nelec_alpha": nel, "wall_s": wall,
-                "e2e": {"value": world * npts / float(t_e2e.item()), "unit": UNIT,
+                "config": config(args, npts, nao, blocks=h["stats"]["nblocks"],
+                                 mean_screened_aos=h["stats"]["mean_nb"], headline=head),
+                "exc": h["exc"], "nelec_alpha": h["nel"],
+                "e2e": {"value": world * npts / t_e2e, "unit": UNIT,
                         "h2d_bytes_per_step": nao * nao * 8, "d2h_bytes_per_step": nao * nao * 8 + 16},
-                "roofline": roof, "cpu_baseline": cpu, "gpu_launches": launches, "clocks": clk.summary()}
+                "roofline": rooflines[head], "cpu_baseline": cpu, "gpu_launches": h["launches"],
+                "clocks": clk_summary}
+        if "fp64" in res and "mixed" in res:
+            f, m = res["fp64"], res["mixed"]
+            line["fp64"] = {"value": f["value"], "ms_per_step": f["ms"], "exc": f["exc"], "roofline": rooflines["fp64"]}
+            line["mixed_vs_fp64"] = {"speedup": f["ms"] / m["ms"], "abs_dexc": abs(m["exc"] - f["exc"]),
+                                     "max_abs_dvxc": float(np.abs(m["V"] - f["V"]).max()),
+                                     "abs_dnelec_alpha": abs(m["nel"] - f["nel"])}
         print(json.dumps(line), flush=True)
-    eng.close()
+    for e in engines.values():
+        e.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def roofline(args, torch, peaks, r, precision):
+    """Dominant contraction kernel of one build: algorithmic FLOPs (2 nb^2 np per block per
+    contraction) over its CUDA-event time, against the measured peak of the unit it runs on."""
+    per = {k: r["stage"][k] for k in ("ao_ms", "gemm_x_ms", "rho_ms", "gemm_v_ms", "finish_ms")}
+    top = max(("gemm_x_ms", "gemm_v_ms"), key=lambda k: per[k])
+    flops = 0.5 * r["stats"]["contraction_flops"]
+    achieved = flops / (per[top] * 1e-3) / 1e12 if per[top] > 0 else None
+    if precision == "fp64":
+        peak = fp64_gemm_peak(torch)
+        note = "measured cuBLAS FP64 DGEMM 8192^3 on this GPU (burst), FP64 tensor cores"
+    elif args.split_terms == 10:
+        bf = peaks.get("bf16_tflops", 1590.0)
+        peak = 2.0 * bf
+        note = ("2 x MEASURED_PEAKS.json bf16_tflops (dense INT8 rate is twice BF16 on B200); achieved counts "
+                "useful FP64-equivalent FLOPs, the tensor cores issue 10 slice products per useful product")
+    else:
+        peak = peaks.get("bf16_tflops", 1590.0)
+        note = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1.59 PFLOP/s"
+    return {"bound": "tensor", "kernel": top.replace("_ms", ""), "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "peak_source": note, "flops_per_launch_set": flops, "stage_ms": per}
 
 
 if __name__ == "__main__":

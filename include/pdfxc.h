@@ -143,6 +143,12 @@ typedef struct {
 
 pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out);
 
+/* Builds normally replay one captured CUDA graph per configuration, which
+ * times the build as a whole (total_ms). With profiling enabled the build is
+ * launched stage by stage instead, so that the per-stage times of
+ * pdfxc_last_profile are filled in. */
+pdfxc_status pdfxc_set_profiling(pdfxc_ctx* ctx, int enable);
+
 const char* pdfxc_last_error(const pdfxc_ctx* ctx);
 void pdfxc_destroy(pdfxc_ctx* ctx);
 

@@ -60,7 +60,85 @@ __global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atom_x
     }
 }
 
+// Pair constants: inv[m*n_atom + n] = 1/|R_m - R_n|, adj[m*n_atom + n] = a_mn (0 without size adjustment).
+__global__ void k_becke_pairs(const double* __restrict__ atom_xyz, const double* __restrict__ brad, int natom,
+                              int size_adjust, double* inv, double* adj) {
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < natom * natom; e += gridDim.x * blockDim.x) {
+        const int m = e / natom, n = e % natom;
+        if (m == n) {
+            inv[e] = adj[e] = 0.0;
+            continue;
+        }
+        const double dx = atom_xyz[3 * m] - atom_xyz[3 * n], dy = atom_xyz[3 * m + 1] - atom_xyz[3 * n + 1],
+                     dz = atom_xyz[3 * m + 2] - atom_xyz[3 * n + 2];
+        inv[e] = 1.0 / sqrt(dx * dx + dy * dy + dz * dz);
+        double a = 0.0;
+        if (size_adjust) {
+            const double au = (brad[m] - brad[n]) / (brad[m] + brad[n]);
+            a = au / (au * au - 1.0);
+            a = a < -0.5 ? -0.5 : (a > 0.5 ? 0.5 : a);
+        }
+        adj[e] = a;
+    }
+}
+
+// Same weights as k_becke, with each thread's point-atom distances kept in
+// shared memory ([atom][thread]) and the pair constants read from the table:
+// one multiply per pair instead of two square roots and a division.
+constexpr int BECKE_T = 64;
+__global__ void __launch_bounds__(BECKE_T) k_becke_tab(const double* __restrict__ atom_xyz, int natom,
+                                                       const double* __restrict__ inv, const double* __restrict__ adj,
+                                                       int64_t npts, const double* __restrict__ xyz,
+                                                       const int* __restrict__ owner,
+                                                       const double* __restrict__ w_single, double* __restrict__ w_out) {
+    extern __shared__ double rr[];  // [natom][BECKE_T]
+    const int t = threadIdx.x;
+    for (int64_t i0 = blockIdx.x * (int64_t)BECKE_T; i0 < npts; i0 += (int64_t)gridDim.x * BECKE_T) {
+        const int64_t i = i0 + t;
+        const bool live = i < npts;
+        const double rx = live ? xyz[3 * i] : 0.0, ry = live ? xyz[3 * i + 1] : 0.0, rz = live ? xyz[3 * i + 2] : 0.0;
+        for (int m = 0; m < natom; ++m) {
+            const double ax = atom_xyz[3 * m] - rx, ay = atom_xyz[3 * m + 1] - ry, az = atom_xyz[3 * m + 2] - rz;
+            rr[m * BECKE_T + t] = sqrt(ax * ax + ay * ay + az * az);
+        }
+        if (live) {
+            const int own = owner[i];
+            double tot = 0.0, pown = 0.0;
+            for (int m = 0; m < natom; ++m) {
+                const double rm = rr[m * BECKE_T + t];
+                const double* im = inv + (size_t)m * natom;
+                const double* am = adj + (size_t)m * natom;
+                double p = 1.0;
+                for (int n = 0; n < natom && p != 0.0; ++n) {
+                    if (n == m) continue;
+                    double u = (rm - rr[n * BECKE_T + t]) * __ldg(im + n);
+                    u = u + __ldg(am + n) * (1.0 - u * u);
+                    p *= becke_s(u);
+                }
+                tot += p;
+                if (m == own) pown = p;
+            }
+            w_out[i] = w_single[i] * (pown / tot);
+        }
+    }
+}
+
 }  // namespace
+
+void launch_becke_tab(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
+                      double* adj, int64_t npts, const double* xyz, const int* owner, const double* w_single,
+                      double* w_out, cudaStream_t s) {
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, natom, size_adjust, inv, adj);
+    int64_t blocks = (npts + BECKE_T - 1) / BECKE_T;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    const size_t smem = sizeof(double) * BECKE_T * natom;
+    cudaFuncSetAttribute(k_becke_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_becke_tab<<<(unsigned)blocks, BECKE_T, smem, s>>>(atom_xyz, natom, inv, adj, npts, xyz, owner, w_single,
+                                                        w_out);
+}
+
+size_t becke_tab_max_atoms() { return (200u * 1024u) / (sizeof(double) * BECKE_T); }
 
 void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust, int64_t npts,
                   const double* xyz, const int* owner, const double* w_single, double* w_out, cudaStream_t s) {

@@ -387,7 +387,7 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
                 return PDFXC_ERR_ARG;
             }
         cudaStream_t s = ctx->stream;
-        double *d_xyz = nullptr, *d_ws = nullptr, *d_wo = nullptr, *d_br = nullptr;
+        double *d_xyz = nullptr, *d_ws = nullptr, *d_wo = nullptr, *d_br = nullptr, *d_pair = nullptr;
         int* d_own = nullptr;
         try {
             dev_alloc(&d_xyz, 3 * (size_t)npts);
@@ -399,15 +399,21 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
             PDFXC_CUDA(cudaMemcpyAsync(d_ws, w_single, sizeof(double) * npts, cudaMemcpyHostToDevice, s));
             PDFXC_CUDA(cudaMemcpyAsync(d_br, becke_radius, sizeof(double) * ctx->natom, cudaMemcpyHostToDevice, s));
             PDFXC_CUDA(cudaMemcpyAsync(d_own, atom, sizeof(int) * npts, cudaMemcpyHostToDevice, s));
-            pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, npts, d_xyz, d_own, d_ws, d_wo, s);
+            if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
+                dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
+                pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, d_pair,
+                                        d_pair + (size_t)ctx->natom * ctx->natom, npts, d_xyz, d_own, d_ws, d_wo, s);
+            } else {
+                pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, npts, d_xyz, d_own, d_ws, d_wo, s);
+            }
             PDFXC_CUDA(cudaGetLastError());
             PDFXC_CUDA(cudaMemcpyAsync(w_out, d_wo, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
             PDFXC_CUDA(cudaStreamSynchronize(s));
         } catch (...) {
-            dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own);
+            dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own), dev_free(d_pair);
             throw;
         }
-        dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own);
+        dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own), dev_free(d_pair);
         return PDFXC_OK;
     });
 }
@@ -499,6 +505,7 @@ void collect_profile(pdfxc_ctx* ctx) {
         }
         return t;
     };
+    if (!ctx->last_staged) return;  // graph replay: only the total is timed
     for (size_t ci = 0; ci < ctx->chunks.size(); ++ci) {
         cudaEvent_t* e = &ctx->stage_ev[5 * ci];
         p.ao_ms += dt(e[0], e[1]);
@@ -513,7 +520,8 @@ void collect_profile(pdfxc_ctx* ctx) {
 // One build on ctx->stream. The sequence of launches is captured once into a
 // CUDA graph per (functional, incremental, density pointer) and replayed.
 void run_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental) {
-    if (!ctx->use_graph) {
+    ctx->last_staged = !ctx->use_graph || ctx->profiling;
+    if (ctx->last_staged) {
         PDFXC_CUDA(cudaEventRecord(ctx->ev[0], ctx->stream));
         enqueue_build(ctx, fn, d_PA, incremental);
         PDFXC_CUDA(cudaEventRecord(ctx->ev[1], ctx->stream));
@@ -669,6 +677,12 @@ pdfxc_status pdfxc_grid_stats(pdfxc_ctx* ctx, int64_t* nblocks, int64_t* npts_pa
     if (npts_padded) *npts_padded = (int64_t)ctx->nblk * BLOCK_PTS;
     if (contraction_flops) *contraction_flops = ctx->contraction_flops;
     if (mean_nb) *mean_nb = ctx->mean_nb;
+    return PDFXC_OK;
+}
+
+pdfxc_status pdfxc_set_profiling(pdfxc_ctx* ctx, int enable) {
+    if (!ctx) return PDFXC_ERR_ARG;
+    ctx->profiling = enable != 0;
     return PDFXC_OK;
 }
 

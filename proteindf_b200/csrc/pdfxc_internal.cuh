@@ -108,6 +108,8 @@ struct pdfxc_ctx {
 
     // one captured CUDA graph per build configuration (functional, incremental, density pointer)
     bool use_graph = true;
+    bool profiling = false;    // launch stage by stage so that stage events can be timed
+    bool last_staged = false;  // the last build ran stage by stage
     cudaGraphExec_t graph_exec = nullptr;
     int graph_fn = -1, graph_inc = -1;
     const double* graph_P = nullptr;
@@ -132,6 +134,11 @@ void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum
 void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust,
                   int64_t npts, const double* xyz, const int* owner, const double* w_single,
                   double* w_out, cudaStream_t s);
+// the table form (pair constants in inv/adj, n_atom^2 doubles each), for n_atom <= becke_tab_max_atoms()
+void launch_becke_tab(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
+                      double* adj, int64_t npts, const double* xyz, const int* owner, const double* w_single,
+                      double* w_out, cudaStream_t s);
+size_t becke_tab_max_atoms();
 
 // Intermediates of one block inside its chunk workspace (doubles):
 //   phi   [nbp][BLOCK_PTS]           AO values, row = local AO

@@ -19,7 +19,7 @@ PRECISION = {"fp64": 0, "mixed": 1}
 EXPORTS = [
     "pdfxc_default_options", "pdfxc_create", "pdfxc_set_system", "pdfxc_set_grid", "pdfxc_becke_weights",
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
-    "pdfxc_last_profile", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
+    "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
 ]
 
 
@@ -58,6 +58,7 @@ def load_library(path=LIB_PATH):
     L.pdfxc_set_rho.argtypes = [_vp, i32, _vp]
     L.pdfxc_grid_stats.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.pdfxc_last_profile.argtypes = [_vp, _vp]
+    L.pdfxc_set_profiling.argtypes = [_vp, i32]
     L.pdfxc_last_error.argtypes = [_vp]
     L.pdfxc_last_error.restype = ctypes.c_char_p
     L.pdfxc_destroy.argtypes = [_vp]
@@ -183,6 +184,10 @@ class XcEngine:
         self._check(self.L.pdfxc_grid_stats(self.h, ctypes.byref(nb), ctypes.byref(npad), ctypes.byref(fl),
                                             ctypes.byref(mnb)), "pdfxc_grid_stats")
         return {"nblocks": nb.value, "npts_padded": npad.value, "contraction_flops": fl.value, "mean_nb": mnb.value}
+
+    def set_profiling(self, enable):
+        """Stage-by-stage launches (per-stage times) instead of CUDA graph replay."""
+        self._check(self.L.pdfxc_set_profiling(self.h, int(enable)), "pdfxc_set_profiling")
 
     def last_profile(self):
         p = Profile()

@@ -75,7 +75,7 @@ def test_mixed_vs_fp64_gpu_water8():
 
 # INT8 fixed-point slices (split_terms = 10): exact integer accumulation, only
 # the unbiased slice truncation (~2^-28 of each row's largest entry) remains.
-OZ_TOL = (1e-9, 1e-8)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
+OZ_TOL = (1e-8, 1e-7)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
 
 
 @pytest.mark.parametrize("fn", ["SVWN", "HFB", "B3LYP"])
@@ -87,7 +87,7 @@ def test_water2_int8_slices_vs_reference(water2, fn):
     dV = np.abs(V - water2[f"{fn}_vxc"]).max()
     print(f"{fn} int8 slices: |dExc|={dE:.3e} max|dVxc|={dV:.3e}")
     assert within(exc, water2[f"{fn}_exc"][0], V, water2[f"{fn}_vxc"], OZ_TOL)
-    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-9 * abs(nel)
+    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-8 * abs(nel)
 
 
 @pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
