@@ -120,14 +120,13 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // are fetched into registers while the current one is multiplied.
 constexpr int GX_BM = 64, GX_BK = 16, GX_AS = GX_BK + 2, GX_BS = BLOCK_PTS + 4;
 __global__ void __launch_bounds__(256) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
-                                                int blk0, char* ws) {
+                                                int blk0, char* ws, int nplanes) {
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
     const int m0 = blockIdx.x * GX_BM;
     if (m0 >= m.nbp) return;
     const double* phi = reinterpret_cast<const double*>(ws + m.ws);
-    // X follows the phi planes (1 for LDA, 4 with gradients); gridDim.z carries that count.
-    const int nplanes = gridDim.z;
+    // X follows the phi planes (1 for LDA, 4 with gradients)
     double* X = reinterpret_cast<double*>(ws + m.ws) + (size_t)nplanes * m.nbp * BLOCK_PTS;
     const int* aos = g.blk_aos + m.ao0;
 
@@ -248,6 +247,14 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int bl
     }
     double* cf = coef + gp * 4;
     cf[0] = a, cf[1] = cx, cf[2] = cy, cf[3] = cz;
+    // Z[nu][p] = 0.5 w vrho phi + c . grad phi, written over X (no longer needed), all nbp rows
+    double* Z = const_cast<double*>(X);
+    for (int r = 0; r < m.nbp; ++r) {
+        const size_t o = (size_t)r * BLOCK_PTS + p;
+        double z = a * phi[o];
+        if (GGA) z += cx * phi[plane + o] + cy * phi[2 * plane + o] + cz * phi[3 * plane + o];
+        Z[o] = z;
+    }
     // block sums in FP64 (deterministic order)
     __shared__ double red[2][BLOCK_PTS / 32];
     double se = warp_sum(e), sn = warp_sum(w * rho);
@@ -262,57 +269,56 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int bl
 }
 
 // Vacc[aos[m]][aos[n]] += sum_p phi[m][p] Z[n][p]: CTA tile 64 x 64 AOs, K = 128 points in
-// steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles); Z is formed from
-// phi, grad phi and the per-point coefficients while the B tile is staged.
-constexpr int GV_B = 64, GV_BK = 16, GV_AS = GV_BK + 2, GV_BS = GV_B + 4;
+// steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles). Z was formed by
+// k_rho_functional in the place of X; both tiles are staged as [row][k] with 128-byte rows.
+constexpr int GV_B = 64, GV_BK = 16, GV_AS = GV_BK + 2;
 template <bool GGA>
 __global__ void __launch_bounds__(128) k_gemm_v(GridView g, int blk0, const double* __restrict__ coef,
                                                 char* ws, double* Vacc, int nao, int tiles) {
+    (void)coef;
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
     const int tm = blockIdx.x / tiles, tn = blockIdx.x % tiles;
     const int m0 = tm * GV_B, n0 = tn * GV_B;
     if (m0 >= m.nbp || n0 >= m.nbp) return;
     const double* phi = reinterpret_cast<const double*>(ws + m.ws);
-    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const double* Z = phi + (size_t)(GGA ? 4 : 1) * m.nbp * BLOCK_PTS;
     const int* aos = g.blk_aos + m.ao0;
-    __shared__ double cf[4][BLOCK_PTS];
     __shared__ double As[GV_B * GV_AS];  // [m][k]
-    __shared__ double Bs[GV_BK * GV_BS];  // [k][n]
+    __shared__ double Bs[GV_B * GV_AS];  // [n][k]
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int wm = warp >> 1, wn = warp & 1, gq = lane >> 2, tq = lane & 3;
-    for (int e = t; e < 4 * BLOCK_PTS; e += 128) {
-        const int pp = e >> 2, k = e & 3;
-        cf[k][pp] = coef[((size_t)blk * BLOCK_PTS + pp) * 4 + k];
-    }
     double acc[4][4][2];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
-    __syncthreads();
+    double ra[8], rb[8];
+    auto fetch = [&](int k0) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int e = t + q * 128, r = e >> 4, c = e & 15;  // row within tile, point within K step
+            ra[q] = phi[(size_t)(m0 + r) * BLOCK_PTS + k0 + c];
+            rb[q] = Z[(size_t)(n0 + r) * BLOCK_PTS + k0 + c];
+        }
+    };
+    fetch(0);
     for (int k0 = 0; k0 < BLOCK_PTS; k0 += GV_BK) {
 #pragma unroll
         for (int q = 0; q < 8; ++q) {
-            const int e = t + q * 128;
-            const int r = e >> 4, c = e & 15;  // row within tile, point within K step
-            const int pp = k0 + c;
-            As[r * GV_AS + c] = phi[(size_t)(m0 + r) * BLOCK_PTS + pp];
-            const size_t on = (size_t)(n0 + r) * BLOCK_PTS + pp;
-            double z = cf[0][pp] * phi[on];
-            if (GGA)
-                z += cf[1][pp] * phi[plane + on] + cf[2][pp] * phi[2 * plane + on] +
-                     cf[3][pp] * phi[3 * plane + on];
-            Bs[c * GV_BS + r] = z;
+            const int e = t + q * 128, r = e >> 4, c = e & 15;
+            As[r * GV_AS + c] = ra[q];
+            Bs[r * GV_AS + c] = rb[q];
         }
         __syncthreads();
+        if (k0 + GV_BK < BLOCK_PTS) fetch(k0 + GV_BK);
 #pragma unroll
         for (int kk = 0; kk < GV_BK; kk += 4) {
             double a[4], b[4];
 #pragma unroll
             for (int i = 0; i < 4; ++i) a[i] = As[(wm * 32 + i * 8 + gq) * GV_AS + kk + tq];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[(kk + tq) * GV_BS + wn * 32 + j * 8 + gq];
+            for (int j = 0; j < 4; ++j) b[j] = Bs[(wn * 32 + j * 8 + gq) * GV_AS + kk + tq];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -368,8 +374,8 @@ void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, b
 
 void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp,
                           int nplanes, char* ws, cudaStream_t s) {
-    dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk, nplanes);
-    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws);
+    dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk);
+    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, nplanes);
 }
 
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,

@@ -754,6 +754,22 @@ __global__ void __launch_bounds__(128, 1)
             const int ep = e_pt[row];
             double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
             for (int c0 = 0; c0 < 128; c0 += 16) {
+                // issue all operand loads of these 16 columns first (predicated), then use them
+                float f0[16], f1[16], f2[16], f3[16];
+                int ec[16];
+#pragma unroll
+                for (int c = 0; c < 16; ++c) {
+                    const int mu = nt * 128 + c0 + c;
+                    const bool live = mu < m.nb;
+                    const size_t o = (size_t)mu * BLOCK_PTS + row;
+                    f0[c] = live ? phi32[o] : 0.f;
+                    if (GGA) {
+                        f1[c] = live ? phi32[plane32 + o] : 0.f;
+                        f2[c] = live ? phi32[2 * plane32 + o] : 0.f;
+                        f3[c] = live ? phi32[3 * plane32 + o] : 0.f;
+                    }
+                    ec[c] = live ? e_p[mu] : 0;
+                }
                 uint32_t d2[16], d3[16], d4[16], d5[16];
                 umma::tmem_ld16_raw(taddr + c0, d2);
                 umma::tmem_ld16_raw(taddr + 128 + c0, d3);
@@ -762,17 +778,14 @@ __global__ void __launch_bounds__(128, 1)
                 umma::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
-                    const int mu = nt * 128 + c0 + c;
-                    if (mu >= m.nb) break;
                     const double s = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
                                      (double)(int)d5[c] * w5;
-                    const double x = ldexp(s, ep + e_p[mu]);
-                    const size_t o = (size_t)mu * BLOCK_PTS + row;
-                    r += (double)phi32[o] * x;
+                    const double x = ldexp(s, ep + ec[c]);
+                    r += (double)f0[c] * x;
                     if (GGA) {
-                        gx += (double)phi32[plane32 + o] * x;
-                        gy += (double)phi32[2 * plane32 + o] * x;
-                        gz += (double)phi32[3 * plane32 + o] * x;
+                        gx += (double)f1[c] * x;
+                        gy += (double)f2[c] * x;
+                        gz += (double)f3[c] * x;
                     }
                 }
             }
