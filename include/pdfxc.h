@@ -122,6 +122,25 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
 pdfxc_status pdfxc_get_rho(pdfxc_ctx* ctx, int gga, double* rho);
 pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho);
 
+/* XC nuclear gradient (closed shell, FP64) at a fixed density, on the grid of
+ * pdfxc_set_grid, which must have been given the owning atom of every point
+ * (each point moves with its atom). Replaces DfCalcGridX::energyGradient
+ * (src/libpdf/DfCalcGridX.cpp:1073-1099 LDA, :1209-1235 GGA) and its
+ * energyGradient_part (:1101-1207, :1237-1415).
+ * grad_orbital (host, n_atom x 3, overwritten): the AO-centre term, the
+ *   reference's Fxc_f after its closed-shell factor 2.
+ * w_single (host, npts in set_grid order, or NULL): single-centre weights of
+ *   the points; with it grad_weight (host, n_atom x 3, overwritten) receives
+ *   the grid-weight term, the derivative of the Becke partition (radii
+ *   becke_radius[n_atom], size_adjust as in pdfxc_becke_weights; at most 400
+ *   atoms). The reference's own weight term (Fxc_w, JGP_nablaB_omegaA,
+ *   src/libpdf/DfGenerateGrid.cpp:2259-2393) is identically zero, because its
+ *   JGP_t returns 0 for every |mu| <= 1; pass w_single = NULL for its output.
+ * exc (may be NULL): the XC energy on the grid. */
+pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
+                               const double* w_single, const double* becke_radius, int size_adjust,
+                               double* grad_orbital, double* grad_weight, double* exc);
+
 /* Statistics of the blocked grid: blocks, points (after padding), the sum of
  * 4 * nb^2 * np over blocks (the algorithmic contraction FLOPs of one build)
  * and the mean screened AO count per block. */

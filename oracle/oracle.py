@@ -107,3 +107,50 @@ def component(name, ra, rb, gaa, gab, gbb):
                                  ctypes.c_double(gaa), ctypes.c_double(gab), ctypes.c_double(gbb),
                                  o.ctypes.data_as(ctypes.c_void_p))
     return o
+
+
+def aos_d2(sh, xyz):
+    """AO values, first and second derivatives: (npts, 10, nao) in the order
+    phi, x, y, z, xx, xy, xz, yy, yz, zz."""
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    out = np.zeros((len(xyz), 10, sh.nao))
+    keep, args = _shell_args(sh)
+    lib().pdfxc_oracle_aos_d2(ctypes.c_int(sh.nshell), ctypes.c_int(sh.nao), *args, ctypes.c_long(len(xyz)),
+                              xyz.ctypes.data_as(ctypes.c_void_p), out.ctypes.data_as(ctypes.c_void_p))
+    return out
+
+
+def xc_grad(name, sh, xyzw, owner, PA, rho_cut=1e-16, threads=0):
+    """AO-centre term of the XC nuclear gradient (closed shell, doubled as the
+    reference's energyGradient does). Returns dict(grad (natom, 3), exc, f (npts,))."""
+    xyzw = np.ascontiguousarray(xyzw, dtype=np.float64).reshape(-1, 4)
+    owner = np.ascontiguousarray(owner, dtype=np.int32)
+    PA = np.ascontiguousarray(PA, dtype=np.float64)
+    natom = len(sh.atom_xyz)
+    grad = np.zeros((natom, 3))
+    f = np.zeros(len(xyzw))
+    exc = ctypes.c_double()
+    keep, args = _shell_args(sh)
+    lib().pdfxc_oracle_xc_grad(ctypes.c_int(FUNCTIONALS[name]), ctypes.c_int(sh.nshell), ctypes.c_int(sh.nao), *args,
+                               ctypes.c_int(natom), ctypes.c_long(len(xyzw)), xyzw.ctypes.data_as(ctypes.c_void_p),
+                               owner.ctypes.data_as(ctypes.c_void_p), PA.ctypes.data_as(ctypes.c_void_p),
+                               ctypes.c_double(rho_cut), grad.ctypes.data_as(ctypes.c_void_p), ctypes.byref(exc),
+                               f.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(threads))
+    return {"grad": grad, "exc": exc.value, "f": f}
+
+
+def becke_grad(atom_xyz, brad, xyz, owner, coef, size_adjust=True):
+    """Grid-weight term of the XC gradient: sum_g coef_g d omega_{A_g}(r_g) / dR, with
+    every point moving with its owner atom. coef = w_single * f."""
+    atom_xyz = np.ascontiguousarray(atom_xyz, dtype=np.float64)
+    brad = np.ascontiguousarray(brad, dtype=np.float64)
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    owner = np.ascontiguousarray(owner, dtype=np.int32)
+    coef = np.ascontiguousarray(coef, dtype=np.float64)
+    grad = np.zeros((len(atom_xyz), 3))
+    lib().pdfxc_oracle_becke_grad(ctypes.c_int(len(atom_xyz)), atom_xyz.ctypes.data_as(ctypes.c_void_p),
+                                  brad.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(int(size_adjust)),
+                                  ctypes.c_long(len(xyz)), xyz.ctypes.data_as(ctypes.c_void_p),
+                                  owner.ctypes.data_as(ctypes.c_void_p), coef.ctypes.data_as(ctypes.c_void_p),
+                                  grad.ctypes.data_as(ctypes.c_void_p))
+    return grad

@@ -517,3 +517,283 @@ int pdfxc_oracle_becke(int natom, const double* atom_xyz, const double* brad, in
     }
     return 0;
 }
+
+/* ---------------- XC nuclear gradient, AO-centre term:
+ * src/libpdf/DfCalcGridX.cpp:1073-1415 (energyGradient, energyGradient_part) with
+ * the AO second derivatives of :237-385 and :792-863.
+ * Per point g (owner atom A, weight w) with rho_A > rho_cut and per AO i on atom B:
+ *   X_i = sum_j P_ij phi_j,  Y_ki = sum_j P_ij d_k phi_j,
+ *   G_i = vrho grad phi_i X_i + sum_k c_k (grad d_k phi_i X_i + grad phi_i Y_ki)   (GGA terms)
+ *   c = 2 vgAA grad rho_A + vgAB grad rho_A,
+ *   grad[B] += -2 w G_i,  grad[A] -= -2 w G_i   (the grid moves with its atom),
+ * and the result is doubled for the closed shell (:1090, :1237).
+ * The AO second derivatives use d_k d_l (A e^{-a r^2}) =
+ *   (A_kl - 2a (x_l A_k + x_k A_l) - 2a delta_kl A + 4a^2 x_k x_l A) e^{-a r^2}
+ * for the angular polynomial A of each component, the same functions the
+ * reference expands term by term. ---------------------------------------------- */
+static void ang_poly(int t, double x, double y, double z, double* A, double* Ak, double* Akl) {
+    /* A, dA/d(x,y,z), d2A/(xx, xy, xz, yy, yz, zz) */
+    const double s3 = 1.0 / sqrt(3.0);
+    for (int k = 0; k < 3; ++k) Ak[k] = 0.0;
+    for (int k = 0; k < 6; ++k) Akl[k] = 0.0;
+    switch (t) {
+        case 0: *A = 1.0; break;
+        case 1: *A = x; Ak[0] = 1.0; break;
+        case 2: *A = y; Ak[1] = 1.0; break;
+        case 3: *A = z; Ak[2] = 1.0; break;
+        case 4: *A = x * y; Ak[0] = y; Ak[1] = x; Akl[1] = 1.0; break;
+        case 5: *A = z * x; Ak[0] = z; Ak[2] = x; Akl[2] = 1.0; break;
+        case 6: *A = y * z; Ak[1] = z; Ak[2] = y; Akl[4] = 1.0; break;
+        case 7: *A = 0.5 * (x * x - y * y); Ak[0] = x; Ak[1] = -y; Akl[0] = 1.0; Akl[3] = -1.0; break;
+        default:
+            *A = s3 * (z * z - 0.5 * (x * x + y * y));
+            Ak[0] = -s3 * x; Ak[1] = -s3 * y; Ak[2] = 2.0 * s3 * z;
+            Akl[0] = -s3; Akl[3] = -s3; Akl[5] = 2.0 * s3;
+    }
+}
+
+/* phi, d phi (3 x nao), d2 phi (6 x nao: xx xy xz yy yz zz) at one point */
+static void eval_aos_d2(const shells_t* S, const double* r, double* phi, double* d1, double* d2) {
+    const int N = S->nao;
+    static const int KL[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
+    for (int s = 0; s < S->nshell; ++s) {
+        const double* C = S->atom_xyz + 3 * S->sh_atom[s];
+        const double q[3] = {r[0] - C[0], r[1] - C[1], r[2] - C[2]};
+        const double d2r = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+        const int L = S->sh_l[s], n = 2 * L + 1;
+        for (int c = 0; c < n; ++c) {
+            const int t = L * L + c, mu = S->sh_ao0[s] + c;
+            double A, Ak[3], Akl[6];
+            ang_poly(t, q[0], q[1], q[2], &A, Ak, Akl);
+            double v = 0.0, g[3] = {0, 0, 0}, h[6] = {0, 0, 0, 0, 0, 0};
+            for (int k = 0; k < S->sh_nprim[s]; ++k) {
+                const double a = S->p_exp[S->sh_p0[s] + k];
+                if (a * d2r > 30.0) continue;
+                const double e = S->p_coef[S->sh_p0[s] + k] * exp(-a * d2r);
+                const double a2 = 2.0 * a;
+                v += A * e;
+                for (int m = 0; m < 3; ++m) g[m] += (Ak[m] - a2 * q[m] * A) * e;
+                for (int m = 0; m < 6; ++m) {
+                    const int kk = KL[m][0], ll = KL[m][1];
+                    double tv = Akl[m] - a2 * (q[ll] * Ak[kk] + q[kk] * Ak[ll]) + a2 * a2 * q[kk] * q[ll] * A;
+                    if (kk == ll) tv -= a2 * A;
+                    h[m] += tv * e;
+                }
+            }
+            phi[mu] = v;
+            for (int m = 0; m < 3; ++m) d1[m * N + mu] = g[m];
+            for (int m = 0; m < 6; ++m) d2[m * N + mu] = h[m];
+        }
+    }
+}
+
+int pdfxc_oracle_aos_d2(int nshell, int nao, const int* sh_atom, const int* sh_l, const int* sh_ao0,
+                        const int* sh_nprim, const int* sh_p0, const double* p_exp, const double* p_coef,
+                        const double* atom_xyz, long npts, const double* xyz, double* out /* npts x 10 x nao */) {
+    shells_t S = {nshell, nao, sh_atom, sh_l, sh_ao0, sh_nprim, sh_p0, p_exp, p_coef, atom_xyz};
+#pragma omp parallel for schedule(static)
+    for (long i = 0; i < npts; ++i) {
+        double* o = out + (size_t)i * 10 * nao;
+        eval_aos_d2(&S, xyz + 3 * i, o, o + nao, o + 4 * (size_t)nao);
+    }
+    return 0;
+}
+
+int pdfxc_oracle_xc_grad(int fn, int nshell, int nao, const int* sh_atom, const int* sh_l, const int* sh_ao0,
+                         const int* sh_nprim, const int* sh_p0, const double* p_exp, const double* p_coef,
+                         const double* atom_xyz, int natom, long npts, const double* xyzw, const int* owner,
+                         const double* PA, double rho_cut, double* grad /* natom x 3 */, double* exc,
+                         double* fdens /* npts, energy density f per point, or NULL */, int nthreads) {
+    shells_t S = {nshell, nao, sh_atom, sh_l, sh_ao0, sh_nprim, sh_p0, p_exp, p_coef, atom_xyz};
+    const int gga = pdfxc_oracle_is_gga(fn);
+    const size_t N = (size_t)nao;
+    int* ao_atom = (int*)malloc(sizeof(int) * N);
+    for (int s = 0; s < nshell; ++s)
+        for (int c = 0; c < 2 * sh_l[s] + 1; ++c) ao_atom[sh_ao0[s] + c] = sh_atom[s];
+    memset(grad, 0, sizeof(double) * 3 * (size_t)natom);
+    double E = 0.0;
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel reduction(+ : E)
+    {
+        double* phi = (double*)malloc(sizeof(double) * N * 14);
+        double *d1 = phi + N, *d2 = phi + 4 * N, *X = phi + 10 * N; /* X, Yx, Yy, Yz */
+        double* G = (double*)calloc(3 * (size_t)natom, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (long i = 0; i < npts; ++i) {
+            const double* r = xyzw + 4 * i;
+            const double w = r[3];
+            if (fdens) fdens[i] = 0.0;
+            eval_aos_d2(&S, r, phi, d1, d2);
+            for (size_t a = 0; a < N; ++a) {
+                const double* Pa = PA + a * N;
+                double s0 = 0, sx = 0, sy = 0, sz = 0;
+                for (size_t b = 0; b < N; ++b) {
+                    s0 += Pa[b] * phi[b];
+                    sx += Pa[b] * d1[b], sy += Pa[b] * d1[N + b], sz += Pa[b] * d1[2 * N + b];
+                }
+                X[a] = s0, X[N + a] = sx, X[2 * N + a] = sy, X[3 * N + a] = sz;
+            }
+            double rho = 0.0, gr[3] = {0, 0, 0};
+            for (size_t a = 0; a < N; ++a) {
+                rho += phi[a] * X[a];
+                for (int k = 0; k < 3; ++k) gr[k] += d1[k * N + a] * X[a];
+            }
+            for (int k = 0; k < 3; ++k) gr[k] *= 2.0;
+            if (!(rho > rho_cut)) continue;
+            const double gam = gga ? gr[0] * gr[0] + gr[1] * gr[1] + gr[2] * gr[2] : 0.0;
+            double o[6];
+            pdfxc_oracle_functional(fn, rho, rho, gam, gam, gam, o);
+            E += w * o[0];
+            if (fdens) fdens[i] = o[0];
+            double c[3] = {0, 0, 0};
+            if (gga)
+                for (int k = 0; k < 3; ++k) c[k] = (2.0 * o[3] + o[4]) * gr[k];
+            /* d2 index of (m, k): xx xy xz / xy yy yz / xz yz zz */
+            static const int H[3][3] = {{0, 1, 2}, {1, 3, 4}, {2, 4, 5}};
+            const int A = owner[i];
+            for (size_t a = 0; a < N; ++a) {
+                double gv[3];
+                for (int m = 0; m < 3; ++m) {
+                    double t = o[1] * d1[m * N + a] * X[a];
+                    if (gga)
+                        for (int k = 0; k < 3; ++k)
+                            t += c[k] * (d2[H[m][k] * N + a] * X[a] + d1[m * N + a] * X[(1 + k) * N + a]);
+                    gv[m] = -2.0 * w * t;
+                }
+                const int B = ao_atom[a];
+                for (int m = 0; m < 3; ++m) G[3 * B + m] += gv[m], G[3 * A + m] -= gv[m];
+            }
+        }
+#pragma omp critical
+        for (int k = 0; k < 3 * natom; ++k) grad[k] += 2.0 * G[k]; /* closed shell */
+        free(G);
+        free(phi);
+    }
+    free(ao_atom);
+    *exc = E;
+    return 0;
+}
+
+/* ---------------- XC nuclear gradient, grid-weight term: the derivative of the
+ * Becke partition of pdfxc_oracle_becke with respect to the nuclei (Johnson, Gill
+ * and Pople, J. Chem. Phys. 98, 5612 (1993), appendix B), written here from the
+ * partition function itself. For point r owned by atom A with coefficient
+ * c = w_single f(r):
+ *   omega_A = P_A / Z,  Z = sum_i P_i,  P_i = prod_{j != i} s(nu_ij),
+ *   grad_B omega_A = (grad_B P_A - omega_A grad_B Z) / Z        (B != A, point fixed),
+ *   grad_B P_i   = prod_{j != i, B} s_ij  s'(nu_iB) grad_B nu_iB         (i != B),
+ *   grad_B P_B   = sum_{j != B} prod_{k != B, j} s_Bk  s'(nu_Bj) grad_B nu_Bj,
+ *   grad_B mu_iB = -(u_B + mu_iB e_iB) / R_iB,  grad_B mu_Bj = (u_B - mu_Bj e_jB) / R_Bj,
+ *   u_B = (R_B - r)/|R_B - r|,  e_iB = (R_B - R_i)/R_iB,  d nu / d mu = 1 - 2 a mu,
+ *   s'(nu) = -(27/16) (1 - p2^2)(1 - p1^2)(1 - nu^2),  p1 = f1(nu), p2 = f1(p1);
+ *   grad[B] += c grad_B omega_A,  grad[A] -= c grad_B omega_A (the point moves with A).
+ * The reference's own weight term (JGP_nablaB_omegaA, src/libpdf/DfGenerateGrid.cpp:
+ * 2259-2393) evaluates to zero: its JGP_t returns 0 unless |mu| > 1. ----------- */
+int pdfxc_oracle_becke_grad(int natom, const double* atom_xyz, const double* brad, int size_adjust, long npts,
+                            const double* xyz, const int* owner, const double* coef, double* grad) {
+    const int n = natom;
+    memset(grad, 0, sizeof(double) * 3 * (size_t)n);
+#pragma omp parallel
+    {
+        double* rr = (double*)malloc(sizeof(double) * n);
+        double* s = (double*)malloc(sizeof(double) * (size_t)n * n);
+        double* ds = (double*)malloc(sizeof(double) * (size_t)n * n); /* d s / d mu, size adjustment folded in */
+        double* mu = (double*)malloc(sizeof(double) * (size_t)n * n);
+        double* P = (double*)malloc(sizeof(double) * n);
+        double* pre = (double*)malloc(sizeof(double) * (n + 1));
+        double* G = (double*)calloc(3 * (size_t)n, sizeof(double));
+#pragma omp for schedule(dynamic, 16)
+        for (long g = 0; g < npts; ++g) {
+            const double c = coef[g];
+            if (c == 0.0) continue;
+            const double* r = xyz + 3 * g;
+            const int A = owner[g];
+            for (int m = 0; m < n; ++m) {
+                const double* R = atom_xyz + 3 * m;
+                rr[m] = sqrt((r[0] - R[0]) * (r[0] - R[0]) + (r[1] - R[1]) * (r[1] - R[1]) + (r[2] - R[2]) * (r[2] - R[2]));
+            }
+            for (int i = 0; i < n; ++i)
+                for (int j = 0; j < n; ++j) {
+                    if (i == j) { s[i * n + j] = 1.0; ds[i * n + j] = 0.0; mu[i * n + j] = 0.0; continue; }
+                    const double* Ri = atom_xyz + 3 * i;
+                    const double* Rj = atom_xyz + 3 * j;
+                    const double Rij = sqrt((Ri[0] - Rj[0]) * (Ri[0] - Rj[0]) + (Ri[1] - Rj[1]) * (Ri[1] - Rj[1]) +
+                                            (Ri[2] - Rj[2]) * (Ri[2] - Rj[2]));
+                    const double m_ = (rr[i] - rr[j]) * (1.0 / Rij);
+                    double nu = m_, dnu = 1.0;
+                    if (size_adjust) {
+                        const double au = (brad[i] - brad[j]) / (brad[i] + brad[j]);
+                        double a = au / (au * au - 1.0);
+                        if (a < -0.5) a = -0.5;
+                        else if (a > 0.5) a = 0.5;
+                        nu = m_ + a * (1.0 - m_ * m_);
+                        dnu = 1.0 - 2.0 * a * m_;
+                    }
+                    const double p1 = 0.5 * nu * (3.0 - nu * nu), p2 = 0.5 * p1 * (3.0 - p1 * p1);
+                    s[i * n + j] = 0.5 * (1.0 - becke_f3(nu));
+                    ds[i * n + j] = -(27.0 / 16.0) * (1.0 - p2 * p2) * (1.0 - p1 * p1) * (1.0 - nu * nu) * dnu;
+                    mu[i * n + j] = m_;
+                }
+            double Z = 0.0;
+            for (int i = 0; i < n; ++i) {
+                double p = 1.0;
+                for (int j = 0; j < n; ++j) p *= s[i * n + j];
+                P[i] = p;
+                Z += p;
+            }
+            const double omega = P[A] / Z;
+            for (int B = 0; B < n; ++B) {
+                if (B == A) continue;
+                const double* RB = atom_xyz + 3 * B;
+                double uB[3];
+                for (int k = 0; k < 3; ++k) uB[k] = (RB[k] - r[k]) / rr[B];
+                double dZ[3] = {0, 0, 0}, dPA[3] = {0, 0, 0};
+                /* i != B: one factor s_iB differentiated */
+                for (int i = 0; i < n; ++i) {
+                    if (i == B) continue;
+                    double others = 1.0;
+                    for (int j = 0; j < n; ++j)
+                        if (j != B) others *= s[i * n + j];
+                    const double* Ri = atom_xyz + 3 * i;
+                    double e[3], RiB = 0.0;
+                    for (int k = 0; k < 3; ++k) e[k] = RB[k] - Ri[k], RiB += e[k] * e[k];
+                    RiB = sqrt(RiB);
+                    const double f = others * ds[i * n + B];
+                    for (int k = 0; k < 3; ++k) {
+                        const double gmu = -(uB[k] + mu[i * n + B] * e[k] / RiB) / RiB;
+                        dZ[k] += f * gmu;
+                        if (i == A) dPA[k] += f * gmu;
+                    }
+                }
+                /* i == B: every factor s_Bj in turn, prefix/suffix products of the rest */
+                pre[0] = 1.0;
+                for (int j = 0; j < n; ++j) pre[j + 1] = pre[j] * s[B * n + j];
+                double suf = 1.0;
+                for (int j = n - 1; j >= 0; --j) {
+                    if (j != B) {
+                        const double* Rj = atom_xyz + 3 * j;
+                        double e[3], RBj = 0.0;
+                        for (int k = 0; k < 3; ++k) e[k] = RB[k] - Rj[k], RBj += e[k] * e[k];
+                        RBj = sqrt(RBj);
+                        const double f = pre[j] * suf * ds[B * n + j];
+                        for (int k = 0; k < 3; ++k) dZ[k] += f * (uB[k] - mu[B * n + j] * e[k] / RBj) / RBj;
+                    }
+                    suf *= s[B * n + j];
+                }
+                for (int k = 0; k < 3; ++k) {
+                    const double d = c * (dPA[k] - omega * dZ[k]) / Z;
+                    G[3 * B + k] += d;
+                    G[3 * A + k] -= d;
+                }
+            }
+        }
+#pragma omp critical
+        for (int k = 0; k < 3 * n; ++k) grad[k] += G[k];
+        free(rr), free(s), free(ds), free(mu), free(P), free(pre), free(G);
+    }
+    return 0;
+}

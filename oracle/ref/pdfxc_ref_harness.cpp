@@ -12,6 +12,7 @@
 //   pdfxc_ref grid  <case.txt> <out.bin>   atom-centred grid + Becke weights
 //   pdfxc_ref func  <case.txt> <out.bin>   pointwise functional values
 //   pdfxc_ref lebedev - <out.bin>          unit-sphere Lebedev tables
+//   pdfxc_ref grad  <case.txt> <out.bin>   XC nuclear gradient + its SG-1 grid
 //
 // The XC mode follows DfCalcGridX::calcXCIntegForFockAndEnergy
 // (src/libpdf/DfCalcGridX.cpp:2280-2315): calcRho_{LDA,GGA}_part (:1862-1962)
@@ -220,6 +221,8 @@ class XcHarness : public DfCalcGridX {
     using DfCalcGridX::calcRho_LDA_part;
     using DfCalcGridX::getAOs;
     using DfCalcGridX::getDAOs;
+    using DfCalcGridX::getD2AOs;
+    using DfCalcGridX::energyGradient_part;
 };
 
 class GridHarness : public DfGenerateGrid {
@@ -382,6 +385,68 @@ int runGrid(const Case& c, const char* outPath) {
     return 0;
 }
 
+// XC nuclear gradient, DfCalcGridX::energyGradient (src/libpdf/DfCalcGridX.cpp:1073-1415):
+// energyGradient_part over all atoms gives the AO-centre term Fxc_f (then x2 for
+// RKS, as energyGradient does) and the grid-weight term Fxc_w separately. The
+// grid is the one energyGradient_part builds itself, DfGenerateGrid::getGrids
+// (SG-1, src/libpdf/DfGenerateGrid.cpp:2091-2257), recorded here atom by atom
+// so that other engines can be run on the same points.
+int runGrad(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    XcHarness h(&param);
+    const int natom = (int)c.atomSym.size();
+    const std::string fn = c.get("functional", "SVWN");
+    const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    TlDenseSymmetricMatrix_Lapack PA(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) PA.set(i, j, P[(size_t)i * N + j]);
+
+    TlDenseGeneralMatrix_Lapack Ff(natom, 3), Fw(natom, 3);
+    const auto t0 = std::chrono::steady_clock::now();
+    double exc = 0.0;
+    if (isGGA(fn)) {
+        DfFunctional_GGA* f = makeGGA(fn);
+        exc = h.energyGradient_part(PA, f, 0, natom, &Ff, &Fw);
+        delete f;
+    } else {
+        DfFunctional_LDA* f = makeLDA(fn);
+        exc = h.energyGradient_part(PA, f, 0, natom, &Ff, &Fw);
+        delete f;
+    }
+    const double tGrad = seconds_since(t0);
+    Ff *= 2.0;  // rks, as energyGradient does
+
+    DfGenerateGrid g(&param);
+    std::vector<double> pts, wsingle, wpart, atomIdx;
+    for (int a = 0; a < natom; ++a) {
+        std::vector<TlPosition> grids;
+        std::vector<double> ws, wp;
+        g.getGrids(a, &grids, &ws, &wp);
+        for (size_t k = 0; k < grids.size(); ++k) {
+            pts.insert(pts.end(), {grids[k].x(), grids[k].y(), grids[k].z()});
+            wsingle.push_back(ws[k]);
+            wpart.push_back(wp[k]);
+            atomIdx.push_back(a);
+        }
+    }
+    Out out(outPath);
+    std::vector<double> ff(3 * (size_t)natom), fw(3 * (size_t)natom);
+    for (int a = 0; a < natom; ++a)
+        for (int k = 0; k < 3; ++k) ff[3 * a + k] = Ff.get(a, k), fw[3 * a + k] = Fw.get(a, k);
+    out.put("grad_orbital", ff);
+    out.put("grad_weight", fw);
+    out.put("exc", exc);
+    out.put("t_grad", tGrad);
+    out.put("points", pts);
+    out.put("w_single", wsingle);
+    out.put("w_partition", wpart);
+    out.put("atom", atomIdx);
+    return 0;
+}
+
 // Pointwise functional values through the overloads buildVxc uses
 // (RKS: src/libpdf/DfCalcGridX.cpp:2076-2087, :2164-2185) and the
 // open-shell ones the reference unit tests use.
@@ -523,6 +588,7 @@ int main(int argc, char** argv) {
     if (mode == "xc") return runXc(c, argv[3]);
     if (mode == "grid") return runGrid(c, argv[3]);
     if (mode == "func") return runFunc(c, argv[3]);
+    if (mode == "grad") return runGrad(c, argv[3]);
 #ifdef PDFXC_DROPIN
     if (mode == "dropin") return runDropin(c, argv[3]);
 #endif

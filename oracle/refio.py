@@ -79,6 +79,18 @@ def run_grid(workdir, symbols, charges, xyz_bohr, basis, grid_kv):
     return run("grid", case, os.path.join(workdir, "grid_out.bin"))
 
 
+def run_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, timeout=None):
+    """Reference XC nuclear gradient (DfCalcGridX::energyGradient_part over all
+    atoms) and the SG-1 grid it integrates on. Returns the harness records:
+    grad_orbital (x2 for RKS), grad_weight, exc, points, w_single, w_partition, atom."""
+    os.makedirs(workdir, exist_ok=True)
+    ppath = os.path.join(workdir, "P.bin")
+    np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
+    case = os.path.join(workdir, "grad.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, {"functional": functional, "density_file": ppath})
+    return run("grad", case, os.path.join(workdir, "grad_out.bin"), timeout=timeout)
+
+
 def run_func(workdir, functional, inputs5):
     os.makedirs(workdir, exist_ok=True)
     ipath = os.path.join(workdir, "func_in.bin")

@@ -125,6 +125,11 @@ __global__ void __launch_bounds__(BECKE_T) k_becke_tab(const double* __restrict_
 
 }  // namespace
 
+void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
+                        double* adj, cudaStream_t s) {
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, natom, size_adjust, inv, adj);
+}
+
 void launch_becke_tab(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
                       double* adj, int64_t npts, const double* xyz, const int* owner, const double* w_single,
                       double* w_out, cudaStream_t s) {

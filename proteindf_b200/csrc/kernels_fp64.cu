@@ -117,17 +117,20 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 
 // X[m][p] = sum_k P[aos[m]][aos[k]] phi[k][p]: CTA tile 64 rows x 128 points, K step 16,
 // 8 warps as 2 x 4 warp tiles of 32 x 32 (4 x 4 DMMA tiles). The next K step's operands
-// are fetched into registers while the current one is multiplied.
+// are fetched into registers while the current one is multiplied. Planes are [nbp][128]
+// arrays of the block's workspace: source plane src0 + z, destination plane dst0 + z for
+// blockIdx.z = z (the build: one plane, phi -> X after the phi planes; the gradient:
+// phi and its three derivatives -> X and Y_x, Y_y, Y_z).
 constexpr int GX_BM = 64, GX_BK = 16, GX_AS = GX_BK + 2, GX_BS = BLOCK_PTS + 4;
 __global__ void __launch_bounds__(256) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
-                                                int blk0, char* ws, int nplanes) {
+                                                int blk0, char* ws, int src0, int dst0) {
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
     const int m0 = blockIdx.x * GX_BM;
     if (m0 >= m.nbp) return;
-    const double* phi = reinterpret_cast<const double*>(ws + m.ws);
-    // X follows the phi planes (1 for LDA, 4 with gradients)
-    double* X = reinterpret_cast<double*>(ws + m.ws) + (size_t)nplanes * m.nbp * BLOCK_PTS;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const double* phi = reinterpret_cast<const double*>(ws + m.ws) + (size_t)(src0 + blockIdx.z) * plane;
+    double* X = reinterpret_cast<double*>(ws + m.ws) + (size_t)(dst0 + blockIdx.z) * plane;
     const int* aos = g.blk_aos + m.ao0;
 
     __shared__ double As[GX_BM * GX_AS];   // [m][k]
@@ -375,7 +378,14 @@ void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, b
 void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp,
                           int nplanes, char* ws, cudaStream_t s) {
     dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk);
-    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, nplanes);
+    // X follows the phi planes (1 for LDA, 4 with gradients)
+    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, 0, nplanes);
+}
+
+void launch_gemm_x_planes(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp, int src0,
+                          int dst0, int nz, char* ws, cudaStream_t s) {
+    dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk, nz);
+    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, src0, dst0);
 }
 
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
@@ -394,6 +404,10 @@ void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga,
         k_gemm_v<true><<<grid, 128, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
     else
         k_gemm_v<false><<<grid, 128, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+}
+
+void launch_block_sums(const double* blk_sum, int nblk, double* scalars, cudaStream_t s) {
+    k_block_sums<<<1, 256, 0, s>>>(blk_sum, nblk, scalars);
 }
 
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk, double* scalars,

@@ -127,6 +127,14 @@ void free_grid(pdfxc_ctx* c) {
     dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum), dev_free(c->d_rho_acc);
     if (c->d_ws) cudaFree(c->d_ws);
     c->d_ws = nullptr;
+    c->h_owner.clear();
+    dev_free(c->d_owner), dev_free(c->d_ao_atom), dev_free(c->d_gmeta), dev_free(c->d_grad);
+    dev_free(c->d_fdens), dev_free(c->d_wslot), dev_free(c->d_brad), dev_free(c->d_pair);
+    if (c->d_gws) cudaFree(c->d_gws);
+    c->d_gws = nullptr;
+    c->gws_bytes = 0;
+    c->gmeta_gga = -1;
+    c->gchunks.clear();
     c->nblk = 0;
     c->npts = 0;
     c->rho_valid = false;
@@ -242,7 +250,13 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
             ctx->err = "pdfxc_set_grid: empty grid or null pointer";
             return PDFXC_ERR_ARG;
         }
-        (void)atom;  // the owning atom is not needed by the quadrature itself
+        // the owning atom is not needed by the quadrature itself; the gradient keeps it per point
+        if (atom)
+            for (int64_t i = 0; i < npts; ++i)
+                if (atom[i] < 0 || atom[i] >= ctx->natom) {
+                    ctx->err = "pdfxc_set_grid: owner atom index out of range";
+                    return PDFXC_ERR_ARG;
+                }
         free_grid(ctx);
         const int bp = ctx->opt.block_points;
         // 1. spatial order: Morton code over the grid's bounding box
@@ -261,6 +275,7 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
         const int nblk = (int)((npts + bp - 1) / bp);
         std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
         ctx->h_src.assign(px.size(), -1);
+        if (atom) ctx->h_owner.assign(px.size(), 0);
         std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
         ctx->h_meta.assign(nblk, BlockMeta{});
         for (int b = 0; b < nblk; ++b) {
@@ -277,9 +292,11 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
                     const double* r = xyzw + 4 * key[i].second;
                     px[slot] = r[0], py[slot] = r[1], pz[slot] = r[2], pw[slot] = r[3];
                     ctx->h_src[slot] = key[i].second;
+                    if (atom) ctx->h_owner[slot] = atom[key[i].second];
                     r2 = std::max(r2, (r[0] - c[0]) * (r[0] - c[0]) + (r[1] - c[1]) * (r[1] - c[1]) + (r[2] - c[2]) * (r[2] - c[2]));
                 } else {
                     px[slot] = c[0], py[slot] = c[1], pz[slot] = c[2], pw[slot] = 0.0;
+                    if (atom) ctx->h_owner[slot] = atom[key[i0].second];  // padding: weight 0
                 }
             }
             for (int k = 0; k < 3; ++k) cen[3 * b + k] = c[k];
@@ -666,6 +683,125 @@ pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho) {
         PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->rho_valid = true;
         ctx->rho_gga = gga ? 1 : 0;
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA, const double* w_single,
+                               const double* becke_radius, int size_adjust, double* grad_orbital, double* grad_weight,
+                               double* exc) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_xc_gradient: call pdfxc_set_system and pdfxc_set_grid first";
+            return PDFXC_ERR_STATE;
+        }
+        if (ctx->h_owner.empty()) {
+            ctx->err = "pdfxc_xc_gradient: the grid was set without owner atoms (pass atom to pdfxc_set_grid)";
+            return PDFXC_ERR_STATE;
+        }
+        if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP || !PA || !grad_orbital) {
+            ctx->err = "pdfxc_xc_gradient: unknown functional or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        if (w_single && (!becke_radius || !grad_weight)) {
+            ctx->err = "pdfxc_xc_gradient: the weight term needs becke_radius and grad_weight";
+            return PDFXC_ERR_ARG;
+        }
+        if (w_single && ctx->natom > pdfxc::grad_weight_max_atoms()) {
+            ctx->err = "pdfxc_xc_gradient: the weight term supports at most " +
+                       std::to_string(pdfxc::grad_weight_max_atoms()) + " atoms";
+            return PDFXC_ERR_UNSUPPORTED;
+        }
+        const bool gga = pdfxc::functional_is_gga(functional);
+        const int nao = ctx->nao, natom = ctx->natom;
+        cudaStream_t s = ctx->stream;
+        if (!ctx->d_ao_atom) {
+            std::vector<int> ao_atom(nao);
+            for (int sh = 0; sh < ctx->nshell; ++sh)
+                for (int c = 0; c < 2 * ctx->h_sh_l[sh] + 1; ++c) ao_atom[ctx->h_sh_ao0[sh] + c] = ctx->h_sh_atom[sh];
+            upload(&ctx->d_ao_atom, ao_atom, s);
+        }
+        if (!ctx->d_owner) upload(&ctx->d_owner, ctx->h_owner, s);
+        // gradient workspace: its own per-block offsets and chunks
+        if (ctx->gmeta_gga != (int)gga) {
+            std::vector<BlockMeta> gm = ctx->h_meta;
+            const size_t per_plane = sizeof(double) * BLOCK_PTS;
+            const int planes = pdfxc::grad_workspace_planes(gga);
+            ctx->gchunks.clear();
+            size_t off = 0, max_ws = 0;
+            Chunk cur{0, 0, 0, 0};
+            for (int b = 0; b < ctx->nblk; ++b) {
+                const size_t need = per_plane * (size_t)gm[b].nbp * planes;
+                if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
+                    cur.b1 = b;
+                    cur.ws_bytes = off;
+                    ctx->gchunks.push_back(cur);
+                    max_ws = std::max(max_ws, off);
+                    cur = Chunk{b, b, 0, 0};
+                    off = 0;
+                }
+                gm[b].ws = (int64_t)off;
+                off += need;
+                cur.max_nbp = std::max(cur.max_nbp, gm[b].nbp);
+            }
+            cur.b1 = ctx->nblk;
+            cur.ws_bytes = off;
+            ctx->gchunks.push_back(cur);
+            max_ws = std::max(max_ws, off);
+            upload(&ctx->d_gmeta, gm, s);
+            if (max_ws > ctx->gws_bytes) {
+                if (ctx->d_gws) cudaFree(ctx->d_gws);
+                ctx->d_gws = nullptr;
+                ctx->gws_bytes = 0;
+                if (cudaMalloc(&ctx->d_gws, max_ws) != cudaSuccess) {
+                    ctx->d_gws = nullptr;
+                    throw std::bad_alloc();
+                }
+                ctx->gws_bytes = max_ws;
+            }
+            ctx->gmeta_gga = (int)gga;
+        }
+        const size_t nslots = (size_t)ctx->nblk * BLOCK_PTS;
+        if (!ctx->d_grad) dev_alloc(&ctx->d_grad, 6 * (size_t)natom);
+        if (!ctx->d_fdens) dev_alloc(&ctx->d_fdens, nslots);
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * 6 * natom, s));
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, sizeof(double) * nao * nao, cudaMemcpyHostToDevice, s));
+        pdfxc::GridView gv = grid_view(ctx);
+        gv.meta = ctx->d_gmeta;
+        const pdfxc::BasisView bv = basis_view(ctx);
+        char* ws = static_cast<char*>(ctx->d_gws);
+        for (const Chunk& ch : ctx->gchunks) {
+            const int n = ch.b1 - ch.b0;
+            pdfxc::launch_ao_grad(bv, gv, ch.b0, n, gga, ws, s);
+            pdfxc::launch_grad_x(gv, ctx->d_P, nao, ch.b0, n, ch.max_nbp, gga, ws, s);
+            pdfxc::launch_grad_point(gv, ctx->d_ao_atom, ctx->d_owner, ch.b0, n, functional, ctx->opt.rho_cutoff, ws,
+                                     ctx->d_fdens, ctx->d_blk_sum, ctx->d_grad, s);
+            PDFXC_CUDA(cudaGetLastError());
+        }
+        pdfxc::launch_block_sums(ctx->d_blk_sum, ctx->nblk, ctx->d_scalars, s);
+        if (w_single) {
+            std::vector<double> wslot(nslots, 0.0);
+            for (size_t k = 0; k < nslots; ++k)
+                if (ctx->h_src[k] >= 0) wslot[k] = w_single[ctx->h_src[k]];
+            upload(&ctx->d_wslot, wslot, s);
+            std::vector<double> brad(becke_radius, becke_radius + natom);
+            upload(&ctx->d_brad, brad, s);
+            dev_alloc(&ctx->d_pair, 2 * (size_t)natom * natom);
+            double* inv = ctx->d_pair;
+            double* adj = ctx->d_pair + (size_t)natom * natom;
+            pdfxc::launch_becke_pairs(ctx->d_atom_xyz, ctx->d_brad, natom, size_adjust, inv, adj, s);
+            pdfxc::launch_grad_weight(ctx->d_atom_xyz, natom, inv, adj, (int64_t)nslots, ctx->d_px, ctx->d_py,
+                                      ctx->d_pz, ctx->d_owner, ctx->d_wslot, ctx->d_fdens, ctx->d_grad + 3 * natom, s);
+            PDFXC_CUDA(cudaGetLastError());
+        }
+        std::vector<double> g(6 * (size_t)natom);
+        double sc[2];
+        PDFXC_CUDA(cudaMemcpyAsync(g.data(), ctx->d_grad, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaStreamSynchronize(s));
+        std::copy(g.begin(), g.begin() + 3 * natom, grad_orbital);
+        if (w_single) std::copy(g.begin() + 3 * natom, g.end(), grad_weight);
+        if (exc) *exc = sc[0];
         return PDFXC_OK;
     });
 }

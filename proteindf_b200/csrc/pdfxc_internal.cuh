@@ -113,6 +113,21 @@ struct pdfxc_ctx {
     cudaGraphExec_t graph_exec = nullptr;
     int graph_fn = -1, graph_inc = -1;
     const double* graph_P = nullptr;
+
+    // XC nuclear gradient (pdfxc_xc_gradient); freed with the grid
+    std::vector<int> h_owner;              // owner atom per point slot (empty: set_grid had no atoms)
+    int* d_owner = nullptr;
+    int* d_ao_atom = nullptr;              // [n_ao]
+    pdfxc::BlockMeta* d_gmeta = nullptr;   // block metadata with gradient workspace offsets
+    int gmeta_gga = -1;
+    std::vector<pdfxc::Chunk> gchunks;
+    void* d_gws = nullptr;
+    size_t gws_bytes = 0;
+    double* d_grad = nullptr;   // [2 * natom * 3]: AO-centre term, grid-weight term
+    double* d_fdens = nullptr;  // [nblk * BLOCK_PTS] energy density per slot
+    double* d_wslot = nullptr;  // [nblk * BLOCK_PTS] single-centre weight per slot
+    double* d_brad = nullptr;   // [natom]
+    double* d_pair = nullptr;   // [2 * natom^2] Becke pair constants
 };
 
 namespace pdfxc {
@@ -122,6 +137,9 @@ void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, b
                     char* ws, int max_nsh, cudaStream_t s);
 void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp,
                    int nplanes, char* ws, cudaStream_t s);
+// the same contraction over nz planes: plane dst0 + z = P_sub * plane src0 + z
+void launch_gemm_x_planes(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp, int src0,
+                          int dst0, int nz, char* ws, cudaStream_t s);
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental,
                            double rho_cut, char* ws, double* rho, double* coef, double* blk_sum,
                            cudaStream_t s);
@@ -129,8 +147,23 @@ void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga,
                    char* ws, double* Vacc, int nao, cudaStream_t s);
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk,
                    double* scalars, cudaStream_t s);
+void launch_block_sums(const double* blk_sum, int nblk, double* scalars, cudaStream_t s);
+
+// gradient.cu: XC nuclear gradient (FP64)
+int grad_workspace_planes(bool gga);  // [nbp][BLOCK_PTS] double planes per block
+void launch_ao_grad(const BasisView& b, const GridView& g, int blk0, int nblk, bool gga, char* ws, cudaStream_t s);
+void launch_grad_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp, bool gga, char* ws,
+                   cudaStream_t s);
+void launch_grad_point(const GridView& g, const int* ao_atom, const int* owner, int blk0, int nblk, int fn,
+                       double rho_cut, const char* ws, double* fdens, double* blk_sum, double* grad, cudaStream_t s);
+int grad_weight_max_atoms();
+void launch_grad_weight(const double* atom_xyz, int natom, const double* inv, const double* adj, int64_t nslots,
+                        const double* px, const double* py, const double* pz, const int* owner, const double* wsingle,
+                        const double* fdens, double* grad, cudaStream_t s);
 
 // becke.cu
+void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
+                        double* adj, cudaStream_t s);
 void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust,
                   int64_t npts, const double* xyz, const int* owner, const double* w_single,
                   double* w_out, cudaStream_t s);

@@ -20,6 +20,7 @@ EXPORTS = [
     "pdfxc_default_options", "pdfxc_create", "pdfxc_set_system", "pdfxc_set_grid", "pdfxc_becke_weights",
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
+    "pdfxc_xc_gradient",
 ]
 
 
@@ -65,6 +66,7 @@ def load_library(path=LIB_PATH):
     L.pdfxc_destroy.restype = None
     L.pdfxc_build_vxc_noalloc.argtypes = [i32, i32, i32, _vp, i32, _vp, _vp, _vp, _vp, _vp, i32, i64, _vp, _vp, _vp,
                                           _vp, _vp]
+    L.pdfxc_xc_gradient.argtypes = [_vp, i32, _vp, _vp, _vp, i32, _vp, _vp, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
             getattr(L, name).restype = i32
@@ -131,11 +133,14 @@ class XcEngine:
         self._check(self.L.pdfxc_set_system(self.h, sh.natom, _ptr(k[0]), _ptr(k[1]), sh.nshell, _ptr(k[2]),
                                             _ptr(k[3]), _ptr(k[4]), _ptr(k[5]), _ptr(k[6])), "pdfxc_set_system")
         self.nao = sh.nao
+        self.natom = sh.natom
 
     def set_grid(self, xyzw, atom=None):
+        """xyzw: (npts, 4) points and weights; atom: owning atom per point (needed by xc_gradient)."""
         xyzw = np.ascontiguousarray(xyzw, dtype=np.float64).reshape(-1, 4)
-        atom = np.zeros(len(xyzw), np.int32) if atom is None else np.ascontiguousarray(atom, dtype=np.int32)
-        self._check(self.L.pdfxc_set_grid(self.h, len(xyzw), _ptr(xyzw), _ptr(atom)), "pdfxc_set_grid")
+        atom = None if atom is None else np.ascontiguousarray(atom, dtype=np.int32)
+        self._check(self.L.pdfxc_set_grid(self.h, len(xyzw), _ptr(xyzw), None if atom is None else _ptr(atom)),
+                    "pdfxc_set_grid")
         self.npts = len(xyzw)
 
     def becke_weights(self, xyz, atom, w_single, becke_radius, size_adjust=True):
@@ -168,6 +173,27 @@ class XcEngine:
                                                   _vp(d_V_ptr), ctypes.byref(exc), ctypes.byref(nel)),
                     "pdfxc_build_vxc_device")
         return exc.value, nel.value
+
+    def xc_gradient(self, functional, PA, w_single=None, becke_radius=None, size_adjust=True):
+        """XC nuclear gradient at fixed PA on the current grid (set with owner atoms).
+        Returns (grad_orbital (natom, 3), grad_weight (natom, 3) or None, exc). The
+        weight term needs the points' single-centre weights (set_grid order) and
+        the Becke radii; without them only the AO-centre term is formed."""
+        PA = np.ascontiguousarray(PA, dtype=np.float64)
+        natom = self.natom
+        go = np.zeros((natom, 3))
+        gw = None
+        args = [None, None, 0, None]
+        if w_single is not None:
+            ws = np.ascontiguousarray(w_single, dtype=np.float64)
+            br = np.ascontiguousarray(becke_radius, dtype=np.float64)
+            gw = np.zeros((natom, 3))
+            self._wkeep = (ws, br)
+            args = [_ptr(ws), _ptr(br), int(size_adjust), _ptr(gw)]
+        exc = ctypes.c_double()
+        self._check(self.L.pdfxc_xc_gradient(self.h, FUNCTIONALS[functional], _ptr(PA), args[0], args[1], args[2],
+                                             _ptr(go), args[3], ctypes.byref(exc)), "pdfxc_xc_gradient")
+        return go, gw, exc.value
 
     def get_rho(self, gga):
         out = np.zeros((self.npts, 4 if gga else 1))

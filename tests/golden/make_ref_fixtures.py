@@ -14,6 +14,10 @@ its inputs and outputs as compressed .npz files beside this script:
   ref_functionals.npz  functional values and first derivatives of all five
                    functionals on a seeded log-uniform (rho, gamma) set, both
                    the open-shell and the closed-shell overloads.
+  ref_grad_water.npz  one H2O, cc-pVDZ: the reference's XC nuclear gradient
+                   (DfCalcGridX::energyGradient_part, AO-centre and grid-weight
+                   terms apart) for SVWN and B3LYP, with the SG-1 grid it
+                   integrates on (points, single-centre and partition weights).
 
 usage (needs the reference tree): make -C oracle/ref && python tests/golden/make_ref_fixtures.py
 """
@@ -84,6 +88,26 @@ def functional_fixture():
     np.savez_compressed(os.path.join(HERE, "ref_functionals.npz"), **out)
 
 
+def grad_fixture():
+    b = basis.load_basis("cc-pVDZ")
+    syms, xyz = systems.water_cluster(1, seed=0)
+    q = systems.nuclear_charges(syms)
+    sh = basis.ShellTable(syms, xyz, b)
+    PA = 0.5 * systems.density_matrix(sh.nao, 5, seed=0)
+    out = {"symbols": np.array(syms), "xyz": xyz, "PA": PA}
+    with tempfile.TemporaryDirectory() as d:
+        for fn in ("SVWN", "B3LYP"):
+            r = refio.run_grad(d, syms, q, xyz, b, fn, PA)
+            out[f"{fn}_grad_orbital"] = r["grad_orbital"].reshape(-1, 3)
+            out[f"{fn}_grad_weight"] = r["grad_weight"].reshape(-1, 3)
+            out[f"{fn}_exc"] = r["exc"]
+    out["points"] = r["points"].reshape(-1, 3)
+    out["w_single"] = r["w_single"]
+    out["w_partition"] = r["w_partition"]
+    out["atom"] = r["atom"].astype(np.int8)
+    np.savez_compressed(os.path.join(HERE, "ref_grad_water.npz"), **out)
+
+
 def main():
     if not refio.ref_available():
         raise SystemExit("build the reference harness first: make -C oracle/ref")
@@ -92,6 +116,7 @@ def main():
     syms, xyz = systems.peptide_chain(12, seed=3)
     system_fixture("ref_chain12.npz", syms, xyz, 5000, ["SVWN", "B3LYP"], nocc=20, seed=3)
     functional_fixture()
+    grad_fixture()
 
 
 if __name__ == "__main__":
