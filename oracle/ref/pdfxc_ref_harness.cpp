@@ -572,6 +572,52 @@ int runDropin(const Case& c, const char* outPath) {
     }
     return 0;
 }
+
+// The XC nuclear gradient through both classes' energyGradient (each builds the
+// SG-1 gradient grid itself), then DfCalcGridX_B200 with the grid-weight term on.
+int runDropinGrad(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    const int natom = (int)c.atomSym.size();
+    const std::string fn = c.get("functional", "SVWN");
+    const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    TlDenseSymmetricMatrix_Lapack PA(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) PA.set(i, j, P[(size_t)i * N + j]);
+    Out out(outPath);
+    for (int engine = 0; engine < 3; ++engine) {
+        if (engine == 2) param["xc_gradient/weight_term"] = "yes";
+        TlDenseGeneralMatrix_Lapack G;
+        if (isGGA(fn)) {
+            DfFunctional_GGA* f = makeGGA(fn);
+            if (engine == 0) {
+                DfCalcGridX e(&param);
+                G = e.energyGradient(PA, f);
+            } else {
+                DfCalcGridX_B200 e(&param);
+                G = e.energyGradient(PA, f);
+            }
+            delete f;
+        } else {
+            DfFunctional_LDA* f = makeLDA(fn);
+            if (engine == 0) {
+                DfCalcGridX e(&param);
+                G = e.energyGradient(PA, f);
+            } else {
+                DfCalcGridX_B200 e(&param);
+                G = e.energyGradient(PA, f);
+            }
+            delete f;
+        }
+        std::vector<double> g(3 * (size_t)natom);
+        for (int a = 0; a < natom; ++a)
+            for (int k = 0; k < 3; ++k) g[3 * a + k] = G.get(a, k);
+        out.put(engine == 0 ? "ref_grad" : engine == 1 ? "b200_grad" : "b200_grad_weight_on", g);
+    }
+    return 0;
+}
 #endif
 
 }  // namespace
@@ -591,6 +637,7 @@ int main(int argc, char** argv) {
     if (mode == "grad") return runGrad(c, argv[3]);
 #ifdef PDFXC_DROPIN
     if (mode == "dropin") return runDropin(c, argv[3]);
+    if (mode == "dropin_grad") return runDropinGrad(c, argv[3]);
 #endif
     std::fprintf(stderr, "unknown mode %s\n", argv[1]);
     return 2;

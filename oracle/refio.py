@@ -124,3 +124,17 @@ def run_dropin(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA
     subprocess.run([DROPIN_BIN, "dropin", case, out], check=True, timeout=timeout, cwd=workdir,
                    stdout=subprocess.DEVNULL)
     return read_records(out)
+
+
+def run_dropin_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, timeout=None):
+    """energyGradient of the reference DfCalcGridX and of DfCalcGridX_B200 (without and
+    with the grid-weight term) on the same parameter set and density."""
+    os.makedirs(os.path.join(workdir, "fl_Work"), exist_ok=True)
+    ppath = os.path.join(workdir, "P.bin")
+    np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
+    case = os.path.join(workdir, "case.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, {"functional": functional, "density_file": ppath})
+    out = os.path.join(workdir, "dropin_grad.bin")
+    subprocess.run([DROPIN_BIN, "dropin_grad", case, out], check=True, timeout=timeout, cwd=workdir,
+                   stdout=subprocess.DEVNULL)
+    return read_records(out)

@@ -14,6 +14,13 @@ updated (and, with xc-update = yes, the next call adds rho(dP) to them), and
 getWholeDensity returns sum_i w_i rho_A(r_i) (:2502-2537). Functionals are
 named as the reference's xc-potential keyword (DfXCFunctional.cpp:70-104).
 
+energyGradient(P_A, functional) mirrors the XC nuclear gradient
+(src/libpdf/DfCalcGridX.cpp:1073-1415) on the current grid matrix (its atom
+column says which atom each point moves with). The reference integrates it on
+its own SG-1 grid; pass that grid's matrix here for the same result. With the
+points' single-centre weights and the Becke radii the grid-weight term is
+added, which the reference's own version evaluates to zero.
+
 Open-shell overloads are not provided (they raise NotImplementedError).
 """
 import numpy as np
@@ -83,6 +90,18 @@ class DfCalcGridX:
         self._iteration += 1
         self._nelec_alpha = nel
         return exc
+
+    def energyGradient(self, P_A, functional, w_single=None, becke_radius=None, size_adjust=True):
+        """XC nuclear gradient (natom, 3) at fixed P_A: the AO-centre term (the
+        reference's result), plus the grid-weight term when w_single is given."""
+        name = functional if isinstance(functional, str) else getattr(functional, "name")
+        name = name.upper()
+        if name not in FUNCTIONALS:
+            raise ValueError(f"unknown functional {name}")
+        go, gw, exc = self._engine.xc_gradient(name, P_A, w_single=w_single, becke_radius=becke_radius,
+                                               size_adjust=size_adjust)
+        self._gradient_exc = exc
+        return go if gw is None else go + gw
 
     def getWholeDensity(self):
         """(sum w rho_A, None) for the closed-shell case."""

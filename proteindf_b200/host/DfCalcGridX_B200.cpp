@@ -9,6 +9,9 @@
 #include "DfFunctional_Becke88.h"
 #include "DfFunctional_HFS.h"
 #include "DfFunctional_SVWN.h"
+#include "DfGenerateGrid.h"
+#include "TlPrdctbl.h"
+#include "TlUtils.h"
 
 namespace {
 
@@ -20,7 +23,7 @@ void check(pdfxc_status st, pdfxc_ctx* ctx, const char* what) {
 }  // namespace
 
 DfCalcGridX_B200::DfCalcGridX_B200(TlSerializeData* pPdfParam, int device, int precision)
-    : DfCalcGridX(pPdfParam) {
+    : DfCalcGridX(pPdfParam), device_(device) {
     pdfxc_options opt;
     pdfxc_default_options(&opt);
     opt.precision = precision;
@@ -56,9 +59,77 @@ DfCalcGridX_B200::DfCalcGridX_B200(TlSerializeData* pPdfParam, int device, int p
     check(pdfxc_set_system(ctx_, natom, xyz.data(), z.data(), (int)shAtom.size(), shAtom.data(), shL.data(),
                            shNprim.data(), pExp.data(), pCoef.data()),
           ctx_, "pdfxc_set_system");
+    sysXyz_ = xyz, sysZ_ = z, shAtom_ = shAtom, shL_ = shL, shNprim_ = shNprim, pExp_ = pExp, pCoef_ = pCoef;
 }
 
-DfCalcGridX_B200::~DfCalcGridX_B200() { pdfxc_destroy(ctx_); }
+DfCalcGridX_B200::~DfCalcGridX_B200() {
+    pdfxc_destroy(gradCtx_);
+    pdfxc_destroy(ctx_);
+}
+
+TlDenseGeneralMatrix_Lapack DfCalcGridX_B200::energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                                             DfFunctional_LDA* pFunctional) {
+    return this->gradient(P_A, functionalId(pFunctional));
+}
+
+TlDenseGeneralMatrix_Lapack DfCalcGridX_B200::energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                                             DfFunctional_GGA* pFunctional) {
+    return this->gradient(P_A, functionalId(pFunctional));
+}
+
+TlDenseGeneralMatrix_Lapack DfCalcGridX_B200::gradient(const TlDenseSymmetricMatrix_Lapack& P_A, int fn) {
+    TlSerializeData& param = *(this->pPdfParam_);
+    const int natom = (int)sysZ_.size();
+    if (!gradCtx_) {
+        pdfxc_options opt;
+        pdfxc_default_options(&opt);
+        opt.rho_cutoff = this->inputtedDensityCutoffValue_;
+        check(pdfxc_create(&gradCtx_, device_, &opt), nullptr, "pdfxc_create");
+        check(pdfxc_set_system(gradCtx_, natom, sysXyz_.data(), sysZ_.data(), (int)shAtom_.size(), shAtom_.data(),
+                               shL_.data(), shNprim_.data(), pExp_.data(), pCoef_.data()),
+              gradCtx_, "pdfxc_set_system");
+        // the grid energyGradient_part integrates on (src/libpdf/DfCalcGridX.cpp:1119-1121):
+        // per atom, single-centre weight times Becke partition weight
+        DfGenerateGrid gen(this->pPdfParam_);
+        std::vector<double> xyzw;
+        std::vector<int> atom;
+        gradWsingle_.clear();
+        for (int a = 0; a < natom; ++a) {
+            std::vector<TlPosition> pts;
+            std::vector<double> ws, wp;
+            gen.getGrids(a, &pts, &ws, &wp);
+            for (size_t k = 0; k < pts.size(); ++k) {
+                xyzw.insert(xyzw.end(), {pts[k].x(), pts[k].y(), pts[k].z(), ws[k] * wp[k]});
+                atom.push_back(a);
+                gradWsingle_.push_back(ws[k]);
+            }
+        }
+        check(pdfxc_set_grid(gradCtx_, (int64_t)atom.size(), xyzw.data(), atom.data()), gradCtx_, "pdfxc_set_grid");
+        // Becke radii and size adjustment as DfGenerateGrid sets them
+        // (src/libpdf/DfGenerateGrid.cpp:120-160, :1958-1968)
+        gradRadius_.assign(natom, 0.0);
+        for (int a = 0; a < natom; ++a)
+            gradRadius_[a] = sysZ_[a] == 1 ? 0.35 : TlPrdctbl::getBraggSlaterRadii(sysZ_[a]);
+        const std::string gt = TlUtils::toUpper(param["xc-potential/grid-type"].getStr());
+        gradSizeAdjust_ = !(gt == "SG-1" || gt == "SG1");
+        if (param["grid/atomic_size_adjustments"].getStr() != "")
+            gradSizeAdjust_ = param["grid/atomic_size_adjustments"].getBoolean();
+    }
+    const bool weightTerm = TlUtils::toUpper(param["xc_gradient/weight_term"].getStr()) == "YES";
+    const int n = this->m_nNumOfAOs;
+    std::vector<double> P((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) P[(size_t)i * n + j] = P[(size_t)j * n + i] = P_A.get(i, j);
+    std::vector<double> go(3 * (size_t)natom, 0.0), gw(3 * (size_t)natom, 0.0);
+    double exc = 0.0;
+    check(pdfxc_xc_gradient(gradCtx_, fn, P.data(), weightTerm ? gradWsingle_.data() : nullptr, gradRadius_.data(),
+                            gradSizeAdjust_ ? 1 : 0, go.data(), weightTerm ? gw.data() : nullptr, &exc),
+          gradCtx_, "pdfxc_xc_gradient");
+    TlDenseGeneralMatrix_Lapack G(natom, 3);
+    for (int a = 0; a < natom; ++a)
+        for (int k = 0; k < 3; ++k) G.set(a, k, go[3 * a + k] + gw[3 * a + k]);
+    return G;
+}
 
 int DfCalcGridX_B200::functionalId(DfFunctional_LDA* f) {
     if (dynamic_cast<DfFunctional_SVWN*>(f)) return PDFXC_SVWN;

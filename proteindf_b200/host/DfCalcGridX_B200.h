@@ -10,7 +10,13 @@
 //                                      DfFunctional_LDA* / DfFunctional_GGA*,
 //                                      TlDenseSymmetricMatrix_Lapack* F_A);
 //
-// (src/libpdf/DfCalcGridX.h:194-210). The computation runs in libpdfxc
+// (src/libpdf/DfCalcGridX.h:194-210), and the XC nuclear gradient the force
+// code reaches through DfForce::calcForceFromPureXC (src/libpdf/DfForce.cpp:366-410):
+//
+//   TlDenseGeneralMatrix_Lapack energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
+//                                              DfFunctional_LDA* / DfFunctional_GGA*);
+//
+// (src/libpdf/DfCalcGridX.h:81-88). The computation runs in libpdfxc
 // (include/pdfxc.h). The side effects are the reference's: F_A is accumulated
 // into, the grid matrix of the previous iteration is read and the one of this
 // iteration is written with the new rho / grad rho columns
@@ -40,6 +46,16 @@ class DfCalcGridX_B200 : public DfCalcGridX {
                                        DfFunctional_GGA* pFunctional,
                                        TlDenseSymmetricMatrix_Lapack* pF_A);
 
+    // XC nuclear gradient, natom x 3, on the reference's own gradient grid
+    // (DfGenerateGrid::getGrids, SG-1, built on the host as the reference builds
+    // it). The result is the reference's: the AO-centre term (its grid-weight
+    // term is identically zero, see pdfxc_xc_gradient). With the parameter
+    // "xc_gradient/weight_term" = "yes" the Becke grid-weight derivative is added.
+    TlDenseGeneralMatrix_Lapack energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                               DfFunctional_LDA* pFunctional);
+    TlDenseGeneralMatrix_Lapack energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                               DfFunctional_GGA* pFunctional);
+
     // sum_i w_i rho_A(r_i) of the last build (DfCalcGridX::getWholeDensity)
     double lastElectronCountAlpha() const { return nelecAlpha_; }
 
@@ -48,9 +64,16 @@ class DfCalcGridX_B200 : public DfCalcGridX {
                  TlDenseSymmetricMatrix_Lapack* pF_A);
     static int functionalId(DfFunctional_LDA* f);
     static int functionalId(DfFunctional_GGA* f);
+    TlDenseGeneralMatrix_Lapack gradient(const TlDenseSymmetricMatrix_Lapack& P_A, int functionalId);
 
    private:
     pdfxc_ctx* ctx_ = nullptr;
+    pdfxc_ctx* gradCtx_ = nullptr;  // the gradient's own grid
+    int device_ = 0;
+    // the system as given to libpdfxc, the gradient grid's single-centre weights and Becke radii
+    std::vector<double> sysXyz_, pExp_, pCoef_, gradWsingle_, gradRadius_;
+    std::vector<int> sysZ_, shAtom_, shL_, shNprim_;
+    bool gradSizeAdjust_ = true;
     bool gridLoaded_ = false;
     double nelecAlpha_ = 0.0;
 };

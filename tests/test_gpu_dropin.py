@@ -26,3 +26,21 @@ def test_dfcalcgridx_b200_matches_reference_class(tmp_path, water2, fn):
         v_ref, v_b = r[f"ref_vxc{it}"].reshape(n, n), r[f"b200_vxc{it}"].reshape(n, n)
         assert abs(e_ref - e_b) <= 1e-8, (it, e_ref, e_b)
         assert np.abs(v_ref - v_b).max() <= 1e-7, it
+
+
+@pytest.mark.skipif(not refio.dropin_available(), reason="oracle/_ref/pdfxc_dropin not built")
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_energy_gradient_matches_reference_class(tmp_path, fn):
+    """DfCalcGridX_B200::energyGradient against DfCalcGridX::energyGradient on one
+    H2O (each class builds the SG-1 gradient grid itself)."""
+    from proteindf_b200 import basis, systems
+    syms, xyz = systems.water_cluster(1, seed=0)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+    PA = 0.5 * systems.density_matrix(sh.nao, 5, seed=0)
+    r = refio.run_dropin_grad(str(tmp_path), syms, systems.nuclear_charges(syms), xyz,
+                              basis.load_basis("cc-pVDZ"), fn, PA)
+    ref, b200, won = r["ref_grad"], r["b200_grad"], r["b200_grad_weight_on"]
+    assert np.abs(ref - b200).max() < 1e-11 * np.abs(ref).max()
+    # the weight term moves the result, and the total stays translation invariant
+    assert np.abs(won - b200).max() > 1e-8
+    assert np.abs(won.reshape(-1, 3).sum(axis=0)).max() < 1e-10 * np.abs(ref).max()

@@ -28,3 +28,18 @@ def test_mirror_two_iterations_with_xc_update(water2, fn):
     nel, _ = calc.getWholeDensity()
     assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-9
     calc.close()
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_mirror_energy_gradient_on_reference_grid(fn):
+    """energyGradient on the reference's SG-1 gradient grid reproduces the reference's
+    result (its AO-centre term; its grid-weight term is zero)."""
+    from conftest import golden
+    from proteindf_b200.dfcalcgridx import DfCalcGridX
+    fx = golden("ref_grad_water.npz")
+    grid = np.c_[fx["points"], fx["w_single"] * fx["w_partition"], fx["atom"].astype(np.float64)]
+    calc = DfCalcGridX(param(fx), grid_matrix=grid)
+    g = calc.energyGradient(fx["PA"], fn)
+    ref = fx[f"{fn}_grad_orbital"] + fx[f"{fn}_grad_weight"]
+    assert np.abs(g - ref).max() < 1e-11 * np.abs(ref).max()
+    calc.close()
