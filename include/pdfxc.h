@@ -122,6 +122,27 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
 pdfxc_status pdfxc_get_rho(pdfxc_ctx* ctx, int gga, double* rho);
 pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho);
 
+/* Open-shell build (FP64 path only; a mixed-precision context returns
+ * PDFXC_ERR_UNSUPPORTED). Replaces the UKS overloads
+ * DfCalcGridX::calcXCIntegForFockAndEnergy(P_A, P_B, functional, F_A, F_B)
+ * (src/libpdf/DfCalcGridX.cpp:2292-2303 LDA, :2317-2328 GGA): calcRho_*_part
+ * on both spin densities (:1891-1922, :1963-2016) and buildVxc(gridMatrix,
+ * functional, F_A, F_B) (:2093-2135, :2195-2278). PA, PB: n_ao x n_ao (host).
+ * FA, FB: accumulated into. A point contributes when rho_A or rho_B exceeds
+ * the density cut-off. Per spin s the GGA coefficient is the reference's,
+ * w (2 vgamma_ss + vgamma_AB) grad rho_s (its build_XC_Matrix, :2455-2500, is
+ * given the spin's own gradient only). incremental: as pdfxc_build_vxc, for
+ * both spins. nelec_alpha, nelec_beta: sum_i w_i rho_s(r_i). */
+pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* PA, const double* PB,
+                                 int incremental, double* FA, double* FB, double* exc,
+                                 double* nelec_alpha, double* nelec_beta);
+
+/* Open-shell per-point densities in input point order, the grid-matrix
+ * columns of the open shell (src/libpdf/DfCalcGridX.h:35-54): npts x 2 (LDA:
+ * rho_A, rho_B) or npts x 8 (GGA: rho_A, grad rho_A, rho_B, grad rho_B). */
+pdfxc_status pdfxc_get_rho_uks(pdfxc_ctx* ctx, int gga, double* rho);
+pdfxc_status pdfxc_set_rho_uks(pdfxc_ctx* ctx, int gga, const double* rho);
+
 /* XC nuclear gradient (closed shell, FP64) at a fixed density, on the grid of
  * pdfxc_set_grid, which must have been given the owning atom of every point
  * (each point moves with its atom). Replaces DfCalcGridX::energyGradient

@@ -154,3 +154,23 @@ def becke_grad(atom_xyz, brad, xyz, owner, coef, size_adjust=True):
                                   owner.ctypes.data_as(ctypes.c_void_p), coef.ctypes.data_as(ctypes.c_void_p),
                                   grad.ctypes.data_as(ctypes.c_void_p))
     return grad
+
+
+def xc_uks(name, sh, xyzw, PA, PB, rho_cut=1e-16, threads=0):
+    """Open-shell quadrature. Returns dict(exc, nelec_alpha, nelec_beta, vxc_a, vxc_b, rho)."""
+    xyzw = np.ascontiguousarray(xyzw, dtype=np.float64).reshape(-1, 4)
+    PA = np.ascontiguousarray(PA, dtype=np.float64)
+    PB = np.ascontiguousarray(PB, dtype=np.float64)
+    n = len(xyzw)
+    gga = name in GGA
+    va, vb = np.zeros((sh.nao, sh.nao)), np.zeros((sh.nao, sh.nao))
+    rho = np.zeros((n, 8 if gga else 2))
+    exc, na, nb = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+    keep, args = _shell_args(sh)
+    lib().pdfxc_oracle_xc_uks(ctypes.c_int(FUNCTIONALS[name]), ctypes.c_int(sh.nshell), ctypes.c_int(sh.nao), *args,
+                              ctypes.c_long(n), xyzw.ctypes.data_as(ctypes.c_void_p),
+                              PA.ctypes.data_as(ctypes.c_void_p), PB.ctypes.data_as(ctypes.c_void_p),
+                              ctypes.c_double(rho_cut), ctypes.byref(exc), ctypes.byref(na), ctypes.byref(nb),
+                              va.ctypes.data_as(ctypes.c_void_p), vb.ctypes.data_as(ctypes.c_void_p),
+                              rho.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(threads))
+    return {"exc": exc.value, "nelec_alpha": na.value, "nelec_beta": nb.value, "vxc_a": va, "vxc_b": vb, "rho": rho}

@@ -797,3 +797,97 @@ int pdfxc_oracle_becke_grad(int natom, const double* atom_xyz, const double* bra
     }
     return 0;
 }
+
+/* ---------------- open shell: src/libpdf/DfCalcGridX.cpp:2292-2303, :2317-2328
+ * (calcXCIntegForFockAndEnergy(P_A, P_B, ...)), :1891-1922 and :1963-2016 (rho of
+ * both spins), :2093-2135 and :2195-2278 (buildVxc with F_A, F_B).
+ * A point contributes when rho_A > rho_cut or rho_B > rho_cut. For spin s,
+ * build_XC_Matrix (:2455-2500) is given vrho_s, vgamma_ss, vgamma_AB and the
+ * spin's own gradient, so c_s = w (2 vgamma_ss + vgamma_AB) grad rho_s.
+ * Outputs: exc, nelec_a/b = sum w rho_s, vxc_a/b (nao x nao, full),
+ * rho (npts x 2 LDA: rhoA rhoB; npts x 8 GGA: rhoA, grad A, rhoB, grad B). */
+int pdfxc_oracle_xc_uks(int fn, int nshell, int nao, const int* sh_atom, const int* sh_l, const int* sh_ao0,
+                        const int* sh_nprim, const int* sh_p0, const double* p_exp, const double* p_coef,
+                        const double* atom_xyz, long npts, const double* xyzw, const double* PA, const double* PB,
+                        double rho_cut, double* exc, double* nelec_a, double* nelec_b, double* vxc_a, double* vxc_b,
+                        double* rho_out, int nthreads) {
+    shells_t S = {nshell, nao, sh_atom, sh_l, sh_ao0, sh_nprim, sh_p0, p_exp, p_coef, atom_xyz};
+    const int gga = pdfxc_oracle_is_gga(fn);
+    const size_t N = (size_t)nao;
+    double E = 0.0, NA = 0.0, NB = 0.0;
+    memset(vxc_a, 0, sizeof(double) * N * N);
+    memset(vxc_b, 0, sizeof(double) * N * N);
+#ifdef _OPENMP
+    if (nthreads > 0) omp_set_num_threads(nthreads);
+#else
+    (void)nthreads;
+#endif
+#pragma omp parallel reduction(+ : E, NA, NB)
+    {
+        double* phi = (double*)malloc(sizeof(double) * N * 6);
+        double *gx = phi + N, *gy = phi + 2 * N, *gz = phi + 3 * N, *XA = phi + 4 * N, *XB = phi + 5 * N;
+        double* Va = (double*)calloc(N * N, sizeof(double));
+        double* Vb = (double*)calloc(N * N, sizeof(double));
+#pragma omp for schedule(dynamic, 64)
+        for (long i = 0; i < npts; ++i) {
+            const double* r = xyzw + 4 * i;
+            const double w = r[3];
+            eval_aos(&S, r, phi, gga ? gx : NULL, gy, gz);
+            for (size_t a = 0; a < N; ++a) {
+                double sa = 0.0, sb = 0.0;
+                for (size_t b = 0; b < N; ++b) sa += PA[a * N + b] * phi[b], sb += PB[a * N + b] * phi[b];
+                XA[a] = sa, XB[a] = sb;
+            }
+            double ra = 0.0, rb = 0.0, ga[3] = {0, 0, 0}, gb[3] = {0, 0, 0};
+            for (size_t a = 0; a < N; ++a) {
+                ra += phi[a] * XA[a], rb += phi[a] * XB[a];
+                if (gga) {
+                    ga[0] += gx[a] * XA[a], ga[1] += gy[a] * XA[a], ga[2] += gz[a] * XA[a];
+                    gb[0] += gx[a] * XB[a], gb[1] += gy[a] * XB[a], gb[2] += gz[a] * XB[a];
+                }
+            }
+            for (int k = 0; k < 3; ++k) ga[k] *= 2.0, gb[k] *= 2.0;
+            if (rho_out) {
+                double* ro = rho_out + (size_t)i * (gga ? 8 : 2);
+                if (gga) {
+                    ro[0] = ra, ro[1] = ga[0], ro[2] = ga[1], ro[3] = ga[2];
+                    ro[4] = rb, ro[5] = gb[0], ro[6] = gb[1], ro[7] = gb[2];
+                } else {
+                    ro[0] = ra, ro[1] = rb;
+                }
+            }
+            NA += w * ra, NB += w * rb;
+            if (!(ra > rho_cut || rb > rho_cut)) continue;
+            const double gaa = ga[0] * ga[0] + ga[1] * ga[1] + ga[2] * ga[2];
+            const double gbb = gb[0] * gb[0] + gb[1] * gb[1] + gb[2] * gb[2];
+            const double gab = ga[0] * gb[0] + ga[1] * gb[1] + ga[2] * gb[2];
+            double o[6];
+            pdfxc_oracle_functional(fn, ra, rb, gaa, gab, gbb, o);
+            E += w * o[0];
+            for (int spin = 0; spin < 2; ++spin) {
+                const double c1 = w * (spin ? o[2] : o[1]);
+                const double cc = w * (2.0 * (spin ? o[5] : o[3]) + o[4]);
+                const double* g = spin ? gb : ga;
+                const double cx = cc * g[0], cy = cc * g[1], cz = cc * g[2];
+                double* V = spin ? Vb : Va;
+                for (size_t a = 0; a < N; ++a) {
+                    const double ta = gga ? (cx * gx[a] + cy * gy[a] + cz * gz[a]) : 0.0;
+                    for (size_t b = 0; b <= a; ++b) {
+                        const double tb = gga ? (cx * gx[b] + cy * gy[b] + cz * gz[b]) : 0.0;
+                        V[a * N + b] += c1 * phi[a] * phi[b] + phi[a] * tb + phi[b] * ta;
+                    }
+                }
+            }
+        }
+#pragma omp critical
+        for (size_t a = 0; a < N; ++a)
+            for (size_t b = 0; b <= a; ++b) vxc_a[a * N + b] += Va[a * N + b], vxc_b[a * N + b] += Vb[a * N + b];
+        free(Va), free(Vb), free(phi);
+    }
+    for (size_t a = 0; a < N; ++a)
+        for (size_t b = 0; b < a; ++b) vxc_a[b * N + a] = vxc_a[a * N + b], vxc_b[b * N + a] = vxc_b[a * N + b];
+    *exc = E;
+    *nelec_a = NA;
+    *nelec_b = NB;
+    return 0;
+}

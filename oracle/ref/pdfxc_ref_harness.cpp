@@ -245,37 +245,43 @@ int runXc(const Case& c, const char* outPath) {
 
     const std::string fn = c.get("functional", "SVWN");
     const bool gga = isGGA(fn);
+    // open shell: a second density (density_file_b) and the P_A, P_B overloads
+    const bool uks = c.get("uks", "0") == "1";
     const long npts = std::atol(c.get("npts", "0").c_str());
-    const int ncol = gga ? 9 : 6;
+    const int ncol = uks ? (gga ? 13 : 7) : (gga ? 9 : 6);
     const std::vector<double> grid = readDoubles(c.get("grid_file"), (size_t)npts * 5);
     const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    const std::vector<double> Pb = uks ? readDoubles(c.get("density_file_b"), (size_t)N * N) : std::vector<double>();
     const int nthreads = std::atoi(c.get("threads", "1").c_str());
     omp_set_num_threads(nthreads > 0 ? nthreads : 1);
 
     TlDenseGeneralMatrix_Lapack gridMat(npts, ncol);
     for (long i = 0; i < npts; ++i)
         for (int k = 0; k < 5; ++k) gridMat.set(i, k, grid[5 * i + k]);
-    TlDenseSymmetricMatrix_Lapack PA(N);
+    TlDenseSymmetricMatrix_Lapack PA(N), PB(N);
     for (int i = 0; i < N; ++i)
-        for (int j = 0; j <= i; ++j) PA.set(i, j, P[(size_t)i * N + j]);
-    TlDenseSymmetricMatrix_Lapack F(N);
+        for (int j = 0; j <= i; ++j) {
+            PA.set(i, j, P[(size_t)i * N + j]);
+            if (uks) PB.set(i, j, Pb[(size_t)i * N + j]);
+        }
+    TlDenseSymmetricMatrix_Lapack F(N), FB(N);
 
     const auto t0 = std::chrono::steady_clock::now();
     if (gga) {
-        h.calcRho_GGA_part(PA, &gridMat);
+        uks ? h.calcRho_GGA_part(PA, PB, &gridMat) : h.calcRho_GGA_part(PA, &gridMat);
     } else {
-        h.calcRho_LDA_part(PA, &gridMat);
+        uks ? h.calcRho_LDA_part(PA, PB, &gridMat) : h.calcRho_LDA_part(PA, &gridMat);
     }
     const double tRho = seconds_since(t0);
     const auto t1 = std::chrono::steady_clock::now();
     double exc = 0.0;
     if (gga) {
         DfFunctional_GGA* f = makeGGA(fn);
-        exc = h.buildVxc(gridMat, f, &F);
+        exc = uks ? h.buildVxc(gridMat, f, &F, &FB) : h.buildVxc(gridMat, f, &F);
         delete f;
     } else {
         DfFunctional_LDA* f = makeLDA(fn);
-        exc = h.buildVxc(gridMat, f, &F);
+        exc = uks ? h.buildVxc(gridMat, f, &F, &FB) : h.buildVxc(gridMat, f, &F);
         delete f;
     }
     const double tVxc = seconds_since(t1);
@@ -285,18 +291,22 @@ int runXc(const Case& c, const char* outPath) {
     out.put("t_rho", tRho);
     out.put("t_vxc", tVxc);
     out.put("threads", (double)nthreads);
-    std::vector<double> vxc((size_t)N * N);
+    std::vector<double> vxc((size_t)N * N), vxcb((size_t)N * N);
     for (int i = 0; i < N; ++i)
-        for (int j = 0; j < N; ++j) vxc[(size_t)i * N + j] = F.get(i, j);
+        for (int j = 0; j < N; ++j) vxc[(size_t)i * N + j] = F.get(i, j), vxcb[(size_t)i * N + j] = FB.get(i, j);
     out.put("vxc", vxc);
+    if (uks) out.put("vxc_b", vxcb);
     std::vector<double> rho((size_t)npts * (ncol - 5));
-    double nel = 0.0;
+    double nel = 0.0, nelb = 0.0;
+    const int colB = gga ? DfCalcGridX::GM_GGA_RHO_BETA : DfCalcGridX::GM_LDA_RHO_BETA;
     for (long i = 0; i < npts; ++i) {
         for (int k = 5; k < ncol; ++k) rho[(size_t)i * (ncol - 5) + (k - 5)] = gridMat.get(i, k);
         nel += gridMat.get(i, DfCalcGridX::GM_WEIGHT) * gridMat.get(i, 5);
+        if (uks) nelb += gridMat.get(i, DfCalcGridX::GM_WEIGHT) * gridMat.get(i, colB);
     }
     out.put("rho", rho);
     out.put("nelec_alpha", nel);
+    if (uks) out.put("nelec_beta", nelb);
 
     // AO table as the reference normalises and orders it (TlOrbitalInfoObject).
     const TlOrbitalInfo& orb = h.orb();
@@ -573,6 +583,70 @@ int runDropin(const Case& c, const char* outPath) {
     return 0;
 }
 
+template <class Engine, class Functional>
+double runEngineUks(TlSerializeData& param, int iteration, const TlDenseSymmetricMatrix_Lapack& PA,
+                    const TlDenseSymmetricMatrix_Lapack& PB, Functional* f, TlDenseSymmetricMatrix_Lapack* FA,
+                    TlDenseSymmetricMatrix_Lapack* FB) {
+    param["num_of_iterations"] = iteration;
+    Engine e(&param);
+    return e.calcXCIntegForFockAndEnergy(PA, PB, f, FA, FB);
+}
+
+// Open-shell drop-in check: both classes' P_A, P_B overloads for two SCF iterations
+// (halves of P_A and P_B, the second with xc-update), through the grid-matrix files.
+int runDropinUks(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    param["method"] = "uks";
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    param["xc-update"] = "yes";
+    param["control"]["file_base_name"]["grid_matrix"] = "grid_%s.mat";
+    const std::string fn = c.get("functional", "SVWN");
+    const bool gga = isGGA(fn);
+    const long npts = std::atol(c.get("npts", "0").c_str());
+    const int ncol = gga ? 13 : 7;
+    const std::vector<double> grid = readDoubles(c.get("grid_file"), (size_t)npts * 5);
+    const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    const std::vector<double> Pb = readDoubles(c.get("density_file_b"), (size_t)N * N);
+    TlDenseGeneralMatrix_Lapack gridMat(npts, ncol);
+    for (long i = 0; i < npts; ++i)
+        for (int k = 0; k < 5; ++k) gridMat.set(i, k, grid[5 * i + k]);
+    TlDenseSymmetricMatrix_Lapack PA2(N), PB2(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) PA2.set(i, j, 0.5 * P[(size_t)i * N + j]), PB2.set(i, j, 0.5 * Pb[(size_t)i * N + j]);
+    Out out(outPath);
+    for (int engine = 0; engine < 2; ++engine) {
+        GridFileWriter(&param).save(0, gridMat);
+        double e[2] = {0, 0};
+        std::vector<TlDenseSymmetricMatrix_Lapack> FA(2, TlDenseSymmetricMatrix_Lapack(N)), FB(FA);
+        for (int it = 0; it < 2; ++it) {
+            if (gga) {
+                DfFunctional_GGA* f = makeGGA(fn);
+                e[it] = engine ? runEngineUks<DfCalcGridX_B200>(param, it + 1, PA2, PB2, f, &FA[it], &FB[it])
+                               : runEngineUks<DfCalcGridX>(param, it + 1, PA2, PB2, f, &FA[it], &FB[it]);
+                delete f;
+            } else {
+                DfFunctional_LDA* f = makeLDA(fn);
+                e[it] = engine ? runEngineUks<DfCalcGridX_B200>(param, it + 1, PA2, PB2, f, &FA[it], &FB[it])
+                               : runEngineUks<DfCalcGridX>(param, it + 1, PA2, PB2, f, &FA[it], &FB[it]);
+                delete f;
+            }
+        }
+        const char* tag = engine ? "b200" : "ref";
+        for (int it = 0; it < 2; ++it) {
+            std::vector<double> va((size_t)N * N), vb((size_t)N * N);
+            for (int i = 0; i < N; ++i)
+                for (int j = 0; j < N; ++j) va[(size_t)i * N + j] = FA[it].get(i, j), vb[(size_t)i * N + j] = FB[it].get(i, j);
+            char name[32];
+            std::snprintf(name, sizeof(name), "%s_exc%d", tag, it + 1), out.put(name, e[it]);
+            std::snprintf(name, sizeof(name), "%s_vxca%d", tag, it + 1), out.put(name, va);
+            std::snprintf(name, sizeof(name), "%s_vxcb%d", tag, it + 1), out.put(name, vb);
+        }
+    }
+    return 0;
+}
+
 // The XC nuclear gradient through both classes' energyGradient (each builds the
 // SG-1 gradient grid itself), then DfCalcGridX_B200 with the grid-weight term on.
 int runDropinGrad(const Case& c, const char* outPath) {
@@ -638,6 +712,7 @@ int main(int argc, char** argv) {
 #ifdef PDFXC_DROPIN
     if (mode == "dropin") return runDropin(c, argv[3]);
     if (mode == "dropin_grad") return runDropinGrad(c, argv[3]);
+    if (mode == "dropin_uks") return runDropinUks(c, argv[3]);
 #endif
     std::fprintf(stderr, "unknown mode %s\n", argv[1]);
     return 2;

@@ -70,6 +70,22 @@ def run_xc(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, ao
     return run("xc", case, os.path.join(workdir, "out.bin"), threads=threads, timeout=timeout)
 
 
+def run_xc_uks(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, PB, threads=1, timeout=None):
+    """Reference open-shell rho + Vxc pass (the P_A, P_B overloads)."""
+    os.makedirs(workdir, exist_ok=True)
+    gpath = os.path.join(workdir, "grid.bin")
+    ppath = os.path.join(workdir, "P.bin")
+    pbpath = os.path.join(workdir, "PB.bin")
+    np.ascontiguousarray(grid5, dtype=np.float64).tofile(gpath)
+    np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
+    np.ascontiguousarray(PB, dtype=np.float64).tofile(pbpath)
+    case = os.path.join(workdir, "case.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, {
+        "functional": functional, "npts": len(grid5), "grid_file": gpath, "density_file": ppath,
+        "density_file_b": pbpath, "uks": 1, "threads": threads})
+    return run("xc", case, os.path.join(workdir, "out.bin"), threads=threads, timeout=timeout)
+
+
 def run_grid(workdir, symbols, charges, xyz_bohr, basis, grid_kv):
     os.makedirs(workdir, exist_ok=True)
     case = os.path.join(workdir, "case.txt")
@@ -136,5 +152,25 @@ def run_dropin_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, 
     write_case(case, symbols, charges, xyz_bohr, basis, {"functional": functional, "density_file": ppath})
     out = os.path.join(workdir, "dropin_grad.bin")
     subprocess.run([DROPIN_BIN, "dropin_grad", case, out], check=True, timeout=timeout, cwd=workdir,
+                   stdout=subprocess.DEVNULL)
+    return read_records(out)
+
+
+def run_dropin_uks(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, PB, timeout=None):
+    """The open-shell overloads of the reference DfCalcGridX and of DfCalcGridX_B200, two
+    SCF iterations (PA/2, PB/2, then the same again with xc-update)."""
+    os.makedirs(os.path.join(workdir, "fl_Work"), exist_ok=True)
+    gpath = os.path.join(workdir, "grid.bin")
+    ppath = os.path.join(workdir, "P.bin")
+    pbpath = os.path.join(workdir, "PB.bin")
+    np.ascontiguousarray(grid5, dtype=np.float64).tofile(gpath)
+    np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
+    np.ascontiguousarray(PB, dtype=np.float64).tofile(pbpath)
+    case = os.path.join(workdir, "case.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, {
+        "functional": functional, "npts": len(grid5), "grid_file": gpath, "density_file": ppath,
+        "density_file_b": pbpath})
+    out = os.path.join(workdir, "dropin_uks.bin")
+    subprocess.run([DROPIN_BIN, "dropin_uks", case, out], check=True, timeout=timeout, cwd=workdir,
                    stdout=subprocess.DEVNULL)
     return read_records(out)

@@ -275,17 +275,15 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int bl
 // steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles). Z was formed by
 // k_rho_functional in the place of X; both tiles are staged as [row][k] with 128-byte rows.
 constexpr int GV_B = 64, GV_BK = 16, GV_AS = GV_BK + 2;
-template <bool GGA>
-__global__ void __launch_bounds__(128) k_gemm_v(GridView g, int blk0, const double* __restrict__ coef,
-                                                char* ws, double* Vacc, int nao, int tiles) {
-    (void)coef;
+__global__ void __launch_bounds__(128) k_gemm_v(GridView g, int blk0, char* ws, int zplane, double* Vacc, int nao,
+                                                int tiles) {
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
     const int tm = blockIdx.x / tiles, tn = blockIdx.x % tiles;
     const int m0 = tm * GV_B, n0 = tn * GV_B;
     if (m0 >= m.nbp || n0 >= m.nbp) return;
     const double* phi = reinterpret_cast<const double*>(ws + m.ws);
-    const double* Z = phi + (size_t)(GGA ? 4 : 1) * m.nbp * BLOCK_PTS;
+    const double* Z = phi + (size_t)zplane * m.nbp * BLOCK_PTS;
     const int* aos = g.blk_aos + m.ao0;
     __shared__ double As[GV_B * GV_AS];  // [m][k]
     __shared__ double Bs[GV_B * GV_AS];  // [n][k]
@@ -351,6 +349,84 @@ __global__ void k_symmetrize(const double* __restrict__ Vacc, double* V, int nao
     }
 }
 
+// Open shell (DfCalcGridX::calcRho_{LDA,GGA}_part(P_A, P_B, ...) :1891-1922, :1963-2016, and
+// buildVxc(gridMatrix, functional, F_A, F_B) :2093-2135, :2195-2278). One CTA per block,
+// one thread per point; X_A and X_B follow the phi planes. A point contributes when
+// rho_A or rho_B exceeds the cut-off. Per spin s the Vxc coefficients are the reference's:
+// 0.5 w vrho_s and c_s = w (2 vgamma_ss + vgamma_AB) grad rho_s (build_XC_Matrix,
+// :2455-2500, is called once per spin with that spin's gradient). Z_s replaces X_s.
+template <bool GGA>
+__global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional_uks(GridView g, int blk0, int fn, int incremental,
+                                                                  double rho_cut, char* ws, double* rho_a,
+                                                                  double* rho_b, double* blk_sum, double* blk_sum_b) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x;
+    const int nplanes = GGA ? 4 : 1;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const double* phi = reinterpret_cast<const double*>(ws + m.ws);
+    double* XA = const_cast<double*>(phi) + nplanes * plane;
+    double* XB = XA + plane;
+    double ra = 0.0, ax = 0.0, ay = 0.0, az = 0.0, rb = 0.0, bx = 0.0, by = 0.0, bz = 0.0;
+    for (int r = 0; r < m.nb; ++r) {
+        const size_t o = (size_t)r * BLOCK_PTS + p;
+        const double xa = XA[o], xb = XB[o];
+        ra = fma(phi[o], xa, ra);
+        rb = fma(phi[o], xb, rb);
+        if (GGA) {
+            const double dx = phi[plane + o], dy = phi[2 * plane + o], dz = phi[3 * plane + o];
+            ax = fma(dx, xa, ax), ay = fma(dy, xa, ay), az = fma(dz, xa, az);
+            bx = fma(dx, xb, bx), by = fma(dy, xb, by), bz = fma(dz, xb, bz);
+        }
+    }
+    ax *= 2.0, ay *= 2.0, az *= 2.0, bx *= 2.0, by *= 2.0, bz *= 2.0;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    double* sa = rho_a + gp * 4;
+    double* sb = rho_b + gp * 4;
+    if (incremental) {
+        ra += sa[0], ax += sa[1], ay += sa[2], az += sa[3];
+        rb += sb[0], bx += sb[1], by += sb[2], bz += sb[3];
+    }
+    sa[0] = ra, sa[1] = ax, sa[2] = ay, sa[3] = az;
+    sb[0] = rb, sb[1] = bx, sb[2] = by, sb[3] = bz;
+    const double w = g.pw[gp];
+    double e = 0.0, a_a = 0.0, a_b = 0.0, ca[3] = {0.0, 0.0, 0.0}, cb[3] = {0.0, 0.0, 0.0};
+    if (w != 0.0 && (ra > rho_cut || rb > rho_cut)) {
+        const double gaa = ax * ax + ay * ay + az * az, gbb = bx * bx + by * by + bz * bz;
+        const double gab = ax * bx + ay * by + az * bz;
+        const XcOut o = eval_functional(fn, ra, rb, gaa, gab, gbb);
+        e = w * o.f;
+        a_a = 0.5 * w * o.va, a_b = 0.5 * w * o.vb;
+        if (GGA) {
+            const double cca = w * (2.0 * o.vgaa + o.vgab), ccb = w * (2.0 * o.vgbb + o.vgab);
+            ca[0] = cca * ax, ca[1] = cca * ay, ca[2] = cca * az;
+            cb[0] = ccb * bx, cb[1] = ccb * by, cb[2] = ccb * bz;
+        }
+    }
+    for (int r = 0; r < m.nbp; ++r) {
+        const size_t o = (size_t)r * BLOCK_PTS + p;
+        double za = a_a * phi[o], zb = a_b * phi[o];
+        if (GGA) {
+            const double dx = phi[plane + o], dy = phi[2 * plane + o], dz = phi[3 * plane + o];
+            za += ca[0] * dx + ca[1] * dy + ca[2] * dz;
+            zb += cb[0] * dx + cb[1] * dy + cb[2] * dz;
+        }
+        XA[o] = za, XB[o] = zb;
+    }
+    __shared__ double red[3][BLOCK_PTS / 32];
+    const double se = warp_sum(e), sna = warp_sum(w * ra), snb = warp_sum(w * rb);
+    if ((p & 31) == 0) red[0][p >> 5] = se, red[1][p >> 5] = sna, red[2][p >> 5] = snb;
+    __syncthreads();
+    if (p == 0) {
+        double E = 0.0, NA = 0.0, NB = 0.0;
+        for (int i = 0; i < BLOCK_PTS / 32; ++i) E += red[0][i], NA += red[1][i], NB += red[2][i];
+        blk_sum[2 * blk] = E;
+        blk_sum[2 * blk + 1] = NA;
+        blk_sum_b[2 * blk] = NB;
+        blk_sum_b[2 * blk + 1] = 0.0;
+    }
+}
+
 // Deterministic FP64 sum of the per-block partials: one CTA, fixed order.
 __global__ void k_block_sums(const double* __restrict__ blk_sum, int nblk, double* out) {
     __shared__ double se[256], sn[256];
@@ -398,12 +474,26 @@ void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool i
 
 void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga, const double* coef, char* ws,
                    double* Vacc, int nao, cudaStream_t s) {
+    (void)coef;
+    launch_gemm_v_plane(g, blk0, nblk, max_nbp, gga ? 4 : 1, ws, Vacc, nao, s);
+}
+
+void launch_gemm_v_plane(const GridView& g, int blk0, int nblk, int max_nbp, int zplane, char* ws, double* Vacc,
+                         int nao, cudaStream_t s) {
     const int tiles = (max_nbp + GV_B - 1) / GV_B;
     dim3 grid(tiles * tiles, nblk);
-    if (gga)
-        k_gemm_v<true><<<grid, 128, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+    k_gemm_v<<<grid, 128, 0, s>>>(g, blk0, ws, zplane, Vacc, nao, tiles);
+}
+
+void launch_rho_functional_uks(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
+                               char* ws, double* rho_a, double* rho_b, double* blk_sum, double* blk_sum_b,
+                               cudaStream_t s) {
+    if (functional_is_gga(fn))
+        k_rho_functional_uks<true><<<nblk, BLOCK_PTS, 0, s>>>(g, blk0, fn, incremental, rho_cut, ws, rho_a, rho_b,
+                                                               blk_sum, blk_sum_b);
     else
-        k_gemm_v<false><<<grid, 128, 0, s>>>(g, blk0, coef, ws, Vacc, nao, tiles);
+        k_rho_functional_uks<false><<<nblk, BLOCK_PTS, 0, s>>>(g, blk0, fn, incremental, rho_cut, ws, rho_a, rho_b,
+                                                                blk_sum, blk_sum_b);
 }
 
 void launch_block_sums(const double* blk_sum, int nblk, double* scalars, cudaStream_t s) {

@@ -120,6 +120,57 @@ void drop_graph(pdfxc_ctx* c) {
     c->graph_P = nullptr;
 }
 
+void free_plan(pdfxc::Plan& p) {
+    dev_free(p.d_meta);
+    if (p.d_ws) cudaFree(p.d_ws);
+    p.d_ws = nullptr;
+    p.ws_bytes = 0;
+    p.planes = -1;
+    p.chunks.clear();
+}
+
+// Per-block workspace offsets and chunks for `planes` FP64 planes of nbp x BLOCK_PTS per
+// block, within the workspace budget; recomputed only when the plane count changes.
+void ensure_plan(pdfxc_ctx* ctx, pdfxc::Plan& p, int planes) {
+    if (p.planes == planes) return;
+    std::vector<BlockMeta> gm = ctx->h_meta;
+    const size_t per_plane = sizeof(double) * BLOCK_PTS;
+    p.chunks.clear();
+    size_t off = 0, max_ws = 0;
+    Chunk cur{0, 0, 0, 0};
+    for (int b = 0; b < ctx->nblk; ++b) {
+        const size_t need = per_plane * (size_t)gm[b].nbp * planes;
+        if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
+            cur.b1 = b;
+            cur.ws_bytes = off;
+            p.chunks.push_back(cur);
+            max_ws = std::max(max_ws, off);
+            cur = Chunk{b, b, 0, 0};
+            off = 0;
+        }
+        gm[b].ws = (int64_t)off;
+        off += need;
+        cur.max_nbp = std::max(cur.max_nbp, gm[b].nbp);
+    }
+    cur.b1 = ctx->nblk;
+    cur.ws_bytes = off;
+    p.chunks.push_back(cur);
+    max_ws = std::max(max_ws, off);
+    upload(&p.d_meta, gm, ctx->stream);
+    if (max_ws > p.ws_bytes) {
+        if (p.d_ws) cudaFree(p.d_ws);
+        p.d_ws = nullptr;
+        p.ws_bytes = 0;
+        if (cudaMalloc(&p.d_ws, max_ws) != cudaSuccess) {
+            p.d_ws = nullptr;
+            p.planes = -1;
+            throw std::bad_alloc();
+        }
+        p.ws_bytes = max_ws;
+    }
+    p.planes = planes;
+}
+
 void free_grid(pdfxc_ctx* c) {
     drop_graph(c);
     dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
@@ -128,13 +179,12 @@ void free_grid(pdfxc_ctx* c) {
     if (c->d_ws) cudaFree(c->d_ws);
     c->d_ws = nullptr;
     c->h_owner.clear();
-    dev_free(c->d_owner), dev_free(c->d_ao_atom), dev_free(c->d_gmeta), dev_free(c->d_grad);
+    dev_free(c->d_owner), dev_free(c->d_ao_atom), dev_free(c->d_grad);
     dev_free(c->d_fdens), dev_free(c->d_wslot), dev_free(c->d_brad), dev_free(c->d_pair);
-    if (c->d_gws) cudaFree(c->d_gws);
-    c->d_gws = nullptr;
-    c->gws_bytes = 0;
-    c->gmeta_gga = -1;
-    c->gchunks.clear();
+    free_plan(c->gplan);
+    free_plan(c->uplan);
+    dev_free(c->d_rho_b), dev_free(c->d_blk_sum_b);
+    c->rho_spin = 0;
     c->nblk = 0;
     c->npts = 0;
     c->rho_valid = false;
@@ -234,6 +284,7 @@ pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
         dev_alloc(&ctx->d_P, n2);
         dev_alloc(&ctx->d_V, n2);
         dev_alloc(&ctx->d_Vacc, n2);
+        dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b);  // open shell: sized on first use
         PDFXC_CUDA(cudaStreamSynchronize(s));
         free_grid(ctx);
         return PDFXC_OK;
@@ -575,8 +626,10 @@ pdfxc_status check_build(pdfxc_ctx* ctx, int functional, int incremental) {
         ctx->err = "pdfxc_build_vxc: unknown functional id " + std::to_string(functional);
         return PDFXC_ERR_ARG;
     }
-    if (incremental && (!ctx->rho_valid || ctx->rho_gga != (int)pdfxc::functional_is_gga(functional))) {
-        ctx->err = "pdfxc_build_vxc: incremental build needs a previous build (or pdfxc_set_rho) of the same functional type";
+    if (incremental && (!ctx->rho_valid || ctx->rho_spin != 1 ||
+                        ctx->rho_gga != (int)pdfxc::functional_is_gga(functional))) {
+        ctx->err = "pdfxc_build_vxc: incremental build needs a previous closed-shell build (or pdfxc_set_rho) of the "
+                   "same functional type";
         return PDFXC_ERR_STATE;
     }
     return PDFXC_OK;
@@ -610,6 +663,7 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
         if (nelec_alpha) *nelec_alpha = sc[1];
         ctx->rho_valid = true;
         ctx->rho_gga = pdfxc::functional_is_gga(functional);
+        ctx->rho_spin = 1;
         return PDFXC_OK;
     });
 }
@@ -641,6 +695,7 @@ pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, i
         if (nelec_alpha) *nelec_alpha = sc[1];
         ctx->rho_valid = true;
         ctx->rho_gga = pdfxc::functional_is_gga(functional);
+        ctx->rho_spin = 1;
         return PDFXC_OK;
     });
 }
@@ -683,6 +738,136 @@ pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho) {
         PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
         ctx->rho_valid = true;
         ctx->rho_gga = gga ? 1 : 0;
+        ctx->rho_spin = 1;
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* PA, const double* PB, int incremental,
+                                 double* FA, double* FB, double* exc, double* nelec_alpha, double* nelec_beta) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_build_vxc_uks: call pdfxc_set_system and pdfxc_set_grid first";
+            return PDFXC_ERR_STATE;
+        }
+        if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP || !PA || !PB || !FA || !FB) {
+            ctx->err = "pdfxc_build_vxc_uks: unknown functional or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        if (ctx->opt.precision != PDFXC_PRECISION_FP64) {
+            ctx->err = "pdfxc_build_vxc_uks: the open-shell build runs on the FP64 path only";
+            return PDFXC_ERR_UNSUPPORTED;
+        }
+        const bool gga = pdfxc::functional_is_gga(functional);
+        if (incremental && (!ctx->rho_valid || ctx->rho_spin != 2 || ctx->rho_gga != (int)gga)) {
+            ctx->err = "pdfxc_build_vxc_uks: incremental build needs a previous open-shell build (or "
+                       "pdfxc_set_rho_uks) of the same functional type";
+            return PDFXC_ERR_STATE;
+        }
+        const int nao = ctx->nao;
+        const size_t n2 = (size_t)nao * nao;
+        cudaStream_t s = ctx->stream;
+        if (!ctx->d_P_b) dev_alloc(&ctx->d_P_b, n2);
+        if (!ctx->d_V_b) dev_alloc(&ctx->d_V_b, n2);
+        if (!ctx->d_Vacc_b) dev_alloc(&ctx->d_Vacc_b, n2);
+        if (!ctx->d_scalars_b) dev_alloc(&ctx->d_scalars_b, 2);
+        if (!ctx->d_rho_b) {
+            dev_alloc(&ctx->d_rho_b, (size_t)ctx->nblk * BLOCK_PTS * 4);
+            PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho_b, 0, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s));
+        }
+        if (!ctx->d_blk_sum_b) dev_alloc(&ctx->d_blk_sum_b, (size_t)ctx->nblk * 2);
+        const int nphi = gga ? 4 : 1;
+        ensure_plan(ctx, ctx->uplan, nphi + 2);  // phi planes, X_A, X_B
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P_b, PB, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc, 0, n2 * sizeof(double), s));
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc_b, 0, n2 * sizeof(double), s));
+        pdfxc::GridView gv = grid_view(ctx);
+        gv.meta = ctx->uplan.d_meta;
+        const pdfxc::BasisView bv = basis_view(ctx);
+        char* ws = static_cast<char*>(ctx->uplan.d_ws);
+        PDFXC_CUDA(cudaEventRecord(ctx->ev[0], s));
+        for (const Chunk& c : ctx->uplan.chunks) {
+            const int nb = c.b1 - c.b0;
+            pdfxc::launch_ao_eval(bv, gv, c.b0, nb, gga, ws, 0, s);
+            pdfxc::launch_gemm_x_planes(gv, ctx->d_P, nao, c.b0, nb, c.max_nbp, 0, nphi, 1, ws, s);
+            pdfxc::launch_gemm_x_planes(gv, ctx->d_P_b, nao, c.b0, nb, c.max_nbp, 0, nphi + 1, 1, ws, s);
+            pdfxc::launch_rho_functional_uks(gv, c.b0, nb, functional, incremental != 0, ctx->opt.rho_cutoff, ws,
+                                             ctx->d_rho, ctx->d_rho_b, ctx->d_blk_sum, ctx->d_blk_sum_b, s);
+            pdfxc::launch_gemm_v_plane(gv, c.b0, nb, c.max_nbp, nphi, ws, ctx->d_Vacc, nao, s);
+            pdfxc::launch_gemm_v_plane(gv, c.b0, nb, c.max_nbp, nphi + 1, ws, ctx->d_Vacc_b, nao, s);
+            PDFXC_CUDA(cudaGetLastError());
+        }
+        pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum, ctx->nblk, ctx->d_scalars, s);
+        pdfxc::launch_finish(ctx->d_Vacc_b, ctx->d_V_b, nao, ctx->d_blk_sum_b, ctx->nblk, ctx->d_scalars_b, s);
+        PDFXC_CUDA(cudaEventRecord(ctx->ev[1], s));
+        PDFXC_CUDA(cudaGetLastError());
+        std::vector<double> Va(n2), Vb(n2);
+        double sa[2], sb[2];
+        PDFXC_CUDA(cudaMemcpyAsync(Va.data(), ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaMemcpyAsync(Vb.data(), ctx->d_V_b, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaMemcpyAsync(sa, ctx->d_scalars, sizeof(sa), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaMemcpyAsync(sb, ctx->d_scalars_b, sizeof(sb), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaStreamSynchronize(s));
+        pdfxc_profile& p = ctx->last_profile;
+        p = pdfxc_profile{};
+        PDFXC_CUDA(cudaEventElapsedTime(&p.total_ms, ctx->ev[0], ctx->ev[1]));
+        p.launches = 6 * (int64_t)ctx->uplan.chunks.size() + 4;
+        for (size_t i = 0; i < n2; ++i) FA[i] += Va[i], FB[i] += Vb[i];
+        if (exc) *exc = sa[0];
+        if (nelec_alpha) *nelec_alpha = sa[1];
+        if (nelec_beta) *nelec_beta = sb[0];
+        ctx->rho_valid = true;
+        ctx->rho_gga = gga;
+        ctx->rho_spin = 2;
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_get_rho_uks(pdfxc_ctx* ctx, int gga, double* rho) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!rho) return PDFXC_ERR_ARG;
+        if (ctx->nblk == 0 || !ctx->d_rho_b) {
+            ctx->err = "pdfxc_get_rho_uks: no open-shell densities (no grid or no open-shell build)";
+            return PDFXC_ERR_STATE;
+        }
+        const size_t ns = (size_t)ctx->nblk * BLOCK_PTS * 4;
+        std::vector<double> ra(ns), rb(ns);
+        PDFXC_CUDA(cudaMemcpyAsync(ra.data(), ctx->d_rho, ns * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaMemcpyAsync(rb.data(), ctx->d_rho_b, ns * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        const int nc = gga ? 4 : 1;
+        for (size_t slot = 0; slot < ctx->h_src.size(); ++slot) {
+            const int64_t i = ctx->h_src[slot];
+            if (i < 0) continue;
+            for (int k = 0; k < nc; ++k) rho[i * 2 * nc + k] = ra[slot * 4 + k], rho[i * 2 * nc + nc + k] = rb[slot * 4 + k];
+        }
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_set_rho_uks(pdfxc_ctx* ctx, int gga, const double* rho) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!rho) return PDFXC_ERR_ARG;
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_set_rho_uks: no grid";
+            return PDFXC_ERR_STATE;
+        }
+        const size_t ns = (size_t)ctx->nblk * BLOCK_PTS * 4;
+        std::vector<double> ra(ns, 0.0), rb(ns, 0.0);
+        const int nc = gga ? 4 : 1;
+        for (size_t slot = 0; slot < ctx->h_src.size(); ++slot) {
+            const int64_t i = ctx->h_src[slot];
+            if (i < 0) continue;
+            for (int k = 0; k < nc; ++k) ra[slot * 4 + k] = rho[i * 2 * nc + k], rb[slot * 4 + k] = rho[i * 2 * nc + nc + k];
+        }
+        if (!ctx->d_rho_b) dev_alloc(&ctx->d_rho_b, ns);
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_rho, ra.data(), ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        PDFXC_CUDA(cudaMemcpyAsync(ctx->d_rho_b, rb.data(), ns * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        ctx->rho_valid = true;
+        ctx->rho_gga = gga ? 1 : 0;
+        ctx->rho_spin = 2;
         return PDFXC_OK;
     });
 }
@@ -723,54 +908,17 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         }
         if (!ctx->d_owner) upload(&ctx->d_owner, ctx->h_owner, s);
         // gradient workspace: its own per-block offsets and chunks
-        if (ctx->gmeta_gga != (int)gga) {
-            std::vector<BlockMeta> gm = ctx->h_meta;
-            const size_t per_plane = sizeof(double) * BLOCK_PTS;
-            const int planes = pdfxc::grad_workspace_planes(gga);
-            ctx->gchunks.clear();
-            size_t off = 0, max_ws = 0;
-            Chunk cur{0, 0, 0, 0};
-            for (int b = 0; b < ctx->nblk; ++b) {
-                const size_t need = per_plane * (size_t)gm[b].nbp * planes;
-                if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
-                    cur.b1 = b;
-                    cur.ws_bytes = off;
-                    ctx->gchunks.push_back(cur);
-                    max_ws = std::max(max_ws, off);
-                    cur = Chunk{b, b, 0, 0};
-                    off = 0;
-                }
-                gm[b].ws = (int64_t)off;
-                off += need;
-                cur.max_nbp = std::max(cur.max_nbp, gm[b].nbp);
-            }
-            cur.b1 = ctx->nblk;
-            cur.ws_bytes = off;
-            ctx->gchunks.push_back(cur);
-            max_ws = std::max(max_ws, off);
-            upload(&ctx->d_gmeta, gm, s);
-            if (max_ws > ctx->gws_bytes) {
-                if (ctx->d_gws) cudaFree(ctx->d_gws);
-                ctx->d_gws = nullptr;
-                ctx->gws_bytes = 0;
-                if (cudaMalloc(&ctx->d_gws, max_ws) != cudaSuccess) {
-                    ctx->d_gws = nullptr;
-                    throw std::bad_alloc();
-                }
-                ctx->gws_bytes = max_ws;
-            }
-            ctx->gmeta_gga = (int)gga;
-        }
+        ensure_plan(ctx, ctx->gplan, pdfxc::grad_workspace_planes(gga));
         const size_t nslots = (size_t)ctx->nblk * BLOCK_PTS;
         if (!ctx->d_grad) dev_alloc(&ctx->d_grad, 6 * (size_t)natom);
         if (!ctx->d_fdens) dev_alloc(&ctx->d_fdens, nslots);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * 6 * natom, s));
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, sizeof(double) * nao * nao, cudaMemcpyHostToDevice, s));
         pdfxc::GridView gv = grid_view(ctx);
-        gv.meta = ctx->d_gmeta;
+        gv.meta = ctx->gplan.d_meta;
         const pdfxc::BasisView bv = basis_view(ctx);
-        char* ws = static_cast<char*>(ctx->d_gws);
-        for (const Chunk& ch : ctx->gchunks) {
+        char* ws = static_cast<char*>(ctx->gplan.d_ws);
+        for (const Chunk& ch : ctx->gplan.chunks) {
             const int n = ch.b1 - ch.b0;
             pdfxc::launch_ao_grad(bv, gv, ch.b0, n, gga, ws, s);
             pdfxc::launch_grad_x(gv, ctx->d_P, nao, ch.b0, n, ch.max_nbp, gga, ws, s);
@@ -838,6 +986,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     dev_free(ctx->d_atom_xyz), dev_free(ctx->d_p_exp), dev_free(ctx->d_p_coef);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
     dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
+    dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b), dev_free(ctx->d_scalars_b);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : ctx->stage_ev) cudaEventDestroy(e);

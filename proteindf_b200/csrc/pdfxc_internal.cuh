@@ -57,6 +57,16 @@ struct GridView {
     const int* blk_aos;        // global AO index of each local row
 };
 
+// A workspace layout for a build with its own number of [nbp][BLOCK_PTS] FP64 planes per
+// block (the XC gradient, the open-shell build): per-block offsets, chunks, workspace.
+struct Plan {
+    BlockMeta* d_meta = nullptr;
+    std::vector<Chunk> chunks;
+    void* d_ws = nullptr;
+    size_t ws_bytes = 0;
+    int planes = -1;
+};
+
 }  // namespace pdfxc
 
 struct pdfxc_ctx {
@@ -118,16 +128,20 @@ struct pdfxc_ctx {
     std::vector<int> h_owner;              // owner atom per point slot (empty: set_grid had no atoms)
     int* d_owner = nullptr;
     int* d_ao_atom = nullptr;              // [n_ao]
-    pdfxc::BlockMeta* d_gmeta = nullptr;   // block metadata with gradient workspace offsets
-    int gmeta_gga = -1;
-    std::vector<pdfxc::Chunk> gchunks;
-    void* d_gws = nullptr;
-    size_t gws_bytes = 0;
+    pdfxc::Plan gplan;                     // gradient workspace layout
     double* d_grad = nullptr;   // [2 * natom * 3]: AO-centre term, grid-weight term
     double* d_fdens = nullptr;  // [nblk * BLOCK_PTS] energy density per slot
     double* d_wslot = nullptr;  // [nblk * BLOCK_PTS] single-centre weight per slot
     double* d_brad = nullptr;   // [natom]
     double* d_pair = nullptr;   // [2 * natom^2] Becke pair constants
+
+    // open-shell build (pdfxc_build_vxc_uks): beta-spin buffers beside the alpha ones above
+    pdfxc::Plan uplan;
+    double* d_rho_b = nullptr;      // [nblk * BLOCK_PTS * 4]
+    double* d_blk_sum_b = nullptr;  // [nblk * 2]: N_beta, 0
+    double* d_scalars_b = nullptr;  // [2]
+    double *d_P_b = nullptr, *d_V_b = nullptr, *d_Vacc_b = nullptr;  // n_ao^2 each
+    int rho_spin = 0;               // the stored densities: 1 closed shell, 2 open shell
 };
 
 namespace pdfxc {
@@ -147,6 +161,14 @@ void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga,
                    char* ws, double* Vacc, int nao, cudaStream_t s);
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk,
                    double* scalars, cudaStream_t s);
+// Vacc += phi Z^T with Z in plane zplane of each block's workspace
+void launch_gemm_v_plane(const GridView& g, int blk0, int nblk, int max_nbp, int zplane, char* ws, double* Vacc,
+                         int nao, cudaStream_t s);
+// open shell: rho/grad rho of X_A, X_B (the two planes after phi), the functional, Z_A/Z_B over X_A/X_B;
+// blk_sum = (Exc, N_alpha) pairs, blk_sum_b = (N_beta, 0) pairs
+void launch_rho_functional_uks(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
+                               char* ws, double* rho_a, double* rho_b, double* blk_sum, double* blk_sum_b,
+                               cudaStream_t s);
 void launch_block_sums(const double* blk_sum, int nblk, double* scalars, cudaStream_t s);
 
 // gradient.cu: XC nuclear gradient (FP64)

@@ -21,7 +21,9 @@ its own SG-1 grid; pass that grid's matrix here for the same result. With the
 points' single-centre weights and the Becke radii the grid-weight term is
 added, which the reference's own version evaluates to zero.
 
-Open-shell overloads are not provided (they raise NotImplementedError).
+The open-shell overload calcXCIntegForFockAndEnergy(P_A, functional, F_A,
+P_B, F_B) mirrors (P_A, P_B, functional, F_A, F_B) of the reference
+(:2292-2303, :2317-2328); its grid matrix carries rho_A and rho_B columns.
 """
 import numpy as np
 
@@ -52,6 +54,7 @@ class DfCalcGridX:
         self._iteration = 0
         self._grid = None
         self._functional_is_gga = None
+        self._open_shell = False
         if grid_matrix is not None:
             self.setGridMatrix(grid_matrix)
 
@@ -60,33 +63,57 @@ class DfCalcGridX:
         g = np.ascontiguousarray(grid_matrix, dtype=np.float64)
         self._grid = g
         self._engine.set_grid(g[:, :4], g[:, GM_ATOM_INDEX].astype(np.int32))
-        if g.shape[1] > GM_RHO_ALPHA:
-            gga = g.shape[1] >= GM_RHO_ALPHA + 4
-            self._engine.set_rho(g[:, GM_RHO_ALPHA:GM_RHO_ALPHA + (4 if gga else 1)], gga)
-            self._functional_is_gga = gga
+        # rho columns by width (src/libpdf/DfCalcGridX.h:35-54): 6 LDA, 9 GGA closed shell;
+        # 7 LDA, 13 GGA open shell
+        ncol = g.shape[1]
+        if ncol in (6, 9):
+            gga = ncol == 9
+            self._engine.set_rho(g[:, GM_RHO_ALPHA:ncol], gga)
+            self._functional_is_gga, self._open_shell = gga, False
+        elif ncol in (7, 13):
+            gga = ncol == 13
+            self._engine.set_rho_uks(g[:, GM_RHO_ALPHA:ncol], gga)
+            self._functional_is_gga, self._open_shell = gga, True
 
     def getGridMatrix(self):
         """The grid matrix with the current rho (and grad rho) columns."""
         gga = bool(self._functional_is_gga)
-        rho = self._engine.get_rho(gga)
+        rho = self._engine.get_rho_uks(gga) if self._open_shell else self._engine.get_rho(gga)
         return np.concatenate([self._grid[:, :5], rho], axis=1)
 
     def calcXCIntegForFockAndEnergy(self, P_A, functional, F_A, P_B=None, F_B=None):
-        """Closed shell: F_A += Vxc(P_A); returns Exc. With xc-update = yes the
-        call after the first treats P_A as the density difference."""
-        if P_B is not None or F_B is not None:
-            raise NotImplementedError("open-shell overloads are not provided")
+        """Closed shell: F_A += Vxc(P_A); open shell (P_B and F_B given): F_A += Vxc_A,
+        F_B += Vxc_B. Returns Exc. With xc-update = yes the call after the first
+        treats the densities as differences."""
         name = functional if isinstance(functional, str) else getattr(functional, "name")
         name = name.upper()
         if name not in FUNCTIONALS:
             raise ValueError(f"unknown functional {name}")
         gga = name in GGA
-        incremental = self.is_update_xc and self._iteration > 0 and self._functional_is_gga == gga
+        open_shell = P_B is not None
+        if open_shell != (F_B is not None):
+            raise ValueError("the open-shell form needs both P_B and F_B")
+        incremental = (self.is_update_xc and self._iteration > 0 and self._functional_is_gga == gga
+                       and self._open_shell == open_shell)
+        if open_shell:
+            FA = np.ascontiguousarray(F_A, dtype=np.float64)
+            FB = np.ascontiguousarray(F_B, dtype=np.float64)
+            exc, na, nb, FA, FB = self._engine.build_vxc_uks(name, P_A, P_B, incremental=incremental, FA=FA, FB=FB)
+            if FA is not F_A:
+                F_A[...] = FA
+            if FB is not F_B:
+                F_B[...] = FB
+            self._functional_is_gga = gga
+            self._open_shell = True
+            self._iteration += 1
+            self._nelec_alpha, self._nelec_beta = na, nb
+            return exc
         F = np.ascontiguousarray(F_A, dtype=np.float64)
         exc, nel, F = self._engine.build_vxc(name, P_A, incremental=incremental, F=F)
         if F is not F_A:
             F_A[...] = F
         self._functional_is_gga = gga
+        self._open_shell = False
         self._iteration += 1
         self._nelec_alpha = nel
         return exc
@@ -104,8 +131,8 @@ class DfCalcGridX:
         return go if gw is None else go + gw
 
     def getWholeDensity(self):
-        """(sum w rho_A, None) for the closed-shell case."""
-        return self._nelec_alpha, None
+        """(sum w rho_A, sum w rho_B); the second is None after a closed-shell build."""
+        return self._nelec_alpha, (self._nelec_beta if self._open_shell else None)
 
     def close(self):
         self._engine.close()

@@ -156,6 +156,74 @@ double DfCalcGridX_B200::calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatri
     return this->build(P_A, functionalId(pFunctional), true, pF_A);
 }
 
+double DfCalcGridX_B200::calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                                     const TlDenseSymmetricMatrix_Lapack& P_B,
+                                                     DfFunctional_LDA* pFunctional,
+                                                     TlDenseSymmetricMatrix_Lapack* pF_A,
+                                                     TlDenseSymmetricMatrix_Lapack* pF_B) {
+    return this->buildOpenShell(P_A, P_B, functionalId(pFunctional), false, pF_A, pF_B);
+}
+
+double DfCalcGridX_B200::calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                                     const TlDenseSymmetricMatrix_Lapack& P_B,
+                                                     DfFunctional_GGA* pFunctional,
+                                                     TlDenseSymmetricMatrix_Lapack* pF_A,
+                                                     TlDenseSymmetricMatrix_Lapack* pF_B) {
+    return this->buildOpenShell(P_A, P_B, functionalId(pFunctional), true, pF_A, pF_B);
+}
+
+// points, weights and owner atoms of the grid matrix, once
+void DfCalcGridX_B200::loadGrid(const TlDenseGeneralMatrix_Lapack& gridMat) {
+    if (gridLoaded_) return;
+    const int64_t npts = gridMat.getNumOfRows();
+    std::vector<double> xyzw(4 * npts);
+    std::vector<int> atom(npts);
+    for (int64_t i = 0; i < npts; ++i) {
+        for (int k = 0; k < 4; ++k) xyzw[4 * i + k] = gridMat.get(i, k);
+        atom[i] = (int)(gridMat.get(i, GM_ATOM_INDEX) + 0.5);
+    }
+    check(pdfxc_set_grid(ctx_, npts, xyzw.data(), atom.data()), ctx_, "pdfxc_set_grid");
+    gridLoaded_ = true;
+}
+
+double DfCalcGridX_B200::buildOpenShell(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                        const TlDenseSymmetricMatrix_Lapack& P_B, int fn, bool gga,
+                                        TlDenseSymmetricMatrix_Lapack* pF_A, TlDenseSymmetricMatrix_Lapack* pF_B) {
+    // grid-matrix columns of the open shell: rho_A (grad rho_A) then rho_B (grad rho_B)
+    // from column GM_LDA_RHO_ALPHA = GM_GGA_RHO_ALPHA (src/libpdf/DfCalcGridX.h:35-54)
+    TlDenseGeneralMatrix_Lapack gridMat =
+        DfObject::getGridMatrix<TlDenseGeneralMatrix_Lapack>(this->m_nIteration - 1);
+    const int64_t npts = gridMat.getNumOfRows();
+    const int nc = gga ? 8 : 2;
+    this->loadGrid(gridMat);
+    const bool incremental = (this->m_nIteration > 1) && this->m_bIsUpdateXC;
+    if (incremental) {
+        std::vector<double> rho(nc * npts);
+        for (int64_t i = 0; i < npts; ++i)
+            for (int k = 0; k < nc; ++k) rho[nc * i + k] = gridMat.get(i, GM_LDA_RHO_ALPHA + k);
+        check(pdfxc_set_rho_uks(ctx_, gga ? 1 : 0, rho.data()), ctx_, "pdfxc_set_rho_uks");
+    }
+    const int n = this->m_nNumOfAOs;
+    std::vector<double> PA((size_t)n * n), PB((size_t)n * n), FA((size_t)n * n, 0.0), FB((size_t)n * n, 0.0);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) {
+            PA[(size_t)i * n + j] = PA[(size_t)j * n + i] = P_A.get(i, j);
+            PB[(size_t)i * n + j] = PB[(size_t)j * n + i] = P_B.get(i, j);
+        }
+    double exc = 0.0;
+    check(pdfxc_build_vxc_uks(ctx_, fn, PA.data(), PB.data(), incremental ? 1 : 0, FA.data(), FB.data(), &exc,
+                              &nelecAlpha_, &nelecBeta_),
+          ctx_, "pdfxc_build_vxc_uks");
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) pF_A->add(i, j, FA[(size_t)i * n + j]), pF_B->add(i, j, FB[(size_t)i * n + j]);
+    std::vector<double> rho(nc * npts);
+    check(pdfxc_get_rho_uks(ctx_, gga ? 1 : 0, rho.data()), ctx_, "pdfxc_get_rho_uks");
+    for (int64_t i = 0; i < npts; ++i)
+        for (int k = 0; k < nc; ++k) gridMat.set(i, GM_LDA_RHO_ALPHA + k, rho[nc * i + k]);
+    DfObject::saveGridMatrix(this->m_nIteration, gridMat);
+    return exc;
+}
+
 double DfCalcGridX_B200::build(const TlDenseSymmetricMatrix_Lapack& P_A, int fn, bool gga,
                                TlDenseSymmetricMatrix_Lapack* pF_A) {
     // the grid matrix of the previous iteration: points, weights and (for
@@ -164,16 +232,7 @@ double DfCalcGridX_B200::build(const TlDenseSymmetricMatrix_Lapack& P_A, int fn,
         DfObject::getGridMatrix<TlDenseGeneralMatrix_Lapack>(this->m_nIteration - 1);
     const int64_t npts = gridMat.getNumOfRows();
     const int nrho = gga ? 4 : 1;
-    if (!gridLoaded_) {
-        std::vector<double> xyzw(4 * npts);
-        std::vector<int> atom(npts);
-        for (int64_t i = 0; i < npts; ++i) {
-            for (int k = 0; k < 4; ++k) xyzw[4 * i + k] = gridMat.get(i, k);
-            atom[i] = (int)(gridMat.get(i, GM_ATOM_INDEX) + 0.5);
-        }
-        check(pdfxc_set_grid(ctx_, npts, xyzw.data(), atom.data()), ctx_, "pdfxc_set_grid");
-        gridLoaded_ = true;
-    }
+    this->loadGrid(gridMat);
     const bool incremental = (this->m_nIteration > 1) && this->m_bIsUpdateXC;
     if (incremental) {
         std::vector<double> rho(nrho * npts);

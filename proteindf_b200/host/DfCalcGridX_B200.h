@@ -45,6 +45,18 @@ class DfCalcGridX_B200 : public DfCalcGridX {
     double calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
                                        DfFunctional_GGA* pFunctional,
                                        TlDenseSymmetricMatrix_Lapack* pF_A);
+    // open shell (src/libpdf/DfCalcGridX.h:198-210): F_A, F_B accumulated into; the grid
+    // matrix carries rho_A and rho_B columns (LDA 7, GGA 13 columns)
+    double calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                       const TlDenseSymmetricMatrix_Lapack& P_B,
+                                       DfFunctional_LDA* pFunctional,
+                                       TlDenseSymmetricMatrix_Lapack* pF_A,
+                                       TlDenseSymmetricMatrix_Lapack* pF_B);
+    double calcXCIntegForFockAndEnergy(const TlDenseSymmetricMatrix_Lapack& P_A,
+                                       const TlDenseSymmetricMatrix_Lapack& P_B,
+                                       DfFunctional_GGA* pFunctional,
+                                       TlDenseSymmetricMatrix_Lapack* pF_A,
+                                       TlDenseSymmetricMatrix_Lapack* pF_B);
 
     // XC nuclear gradient, natom x 3, on the reference's own gradient grid
     // (DfGenerateGrid::getGrids, SG-1, built on the host as the reference builds
@@ -56,12 +68,17 @@ class DfCalcGridX_B200 : public DfCalcGridX {
     TlDenseGeneralMatrix_Lapack energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
                                                DfFunctional_GGA* pFunctional);
 
-    // sum_i w_i rho_A(r_i) of the last build (DfCalcGridX::getWholeDensity)
+    // sum_i w_i rho_s(r_i) of the last build (DfCalcGridX::getWholeDensity)
     double lastElectronCountAlpha() const { return nelecAlpha_; }
+    double lastElectronCountBeta() const { return nelecBeta_; }
 
    protected:
     double build(const TlDenseSymmetricMatrix_Lapack& P_A, int functionalId, bool gga,
                  TlDenseSymmetricMatrix_Lapack* pF_A);
+    double buildOpenShell(const TlDenseSymmetricMatrix_Lapack& P_A, const TlDenseSymmetricMatrix_Lapack& P_B,
+                          int functionalId, bool gga, TlDenseSymmetricMatrix_Lapack* pF_A,
+                          TlDenseSymmetricMatrix_Lapack* pF_B);
+    void loadGrid(const TlDenseGeneralMatrix_Lapack& gridMat);
     static int functionalId(DfFunctional_LDA* f);
     static int functionalId(DfFunctional_GGA* f);
     TlDenseGeneralMatrix_Lapack gradient(const TlDenseSymmetricMatrix_Lapack& P_A, int functionalId);
@@ -76,6 +93,7 @@ class DfCalcGridX_B200 : public DfCalcGridX {
     bool gradSizeAdjust_ = true;
     bool gridLoaded_ = false;
     double nelecAlpha_ = 0.0;
+    double nelecBeta_ = 0.0;
 };
 
 #endif  // DFCALCGRIDX_B200_H

@@ -20,7 +20,7 @@ EXPORTS = [
     "pdfxc_default_options", "pdfxc_create", "pdfxc_set_system", "pdfxc_set_grid", "pdfxc_becke_weights",
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
-    "pdfxc_xc_gradient",
+    "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks",
 ]
 
 
@@ -67,6 +67,9 @@ def load_library(path=LIB_PATH):
     L.pdfxc_build_vxc_noalloc.argtypes = [i32, i32, i32, _vp, i32, _vp, _vp, _vp, _vp, _vp, i32, i64, _vp, _vp, _vp,
                                           _vp, _vp]
     L.pdfxc_xc_gradient.argtypes = [_vp, i32, _vp, _vp, _vp, i32, _vp, _vp, _vp]
+    L.pdfxc_build_vxc_uks.argtypes = [_vp, i32, _vp, _vp, i32, _vp, _vp, _vp, _vp, _vp]
+    L.pdfxc_get_rho_uks.argtypes = [_vp, i32, _vp]
+    L.pdfxc_set_rho_uks.argtypes = [_vp, i32, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
             getattr(L, name).restype = i32
@@ -194,6 +197,28 @@ class XcEngine:
         self._check(self.L.pdfxc_xc_gradient(self.h, FUNCTIONALS[functional], _ptr(PA), args[0], args[1], args[2],
                                              _ptr(go), args[3], ctypes.byref(exc)), "pdfxc_xc_gradient")
         return go, gw, exc.value
+
+    def build_vxc_uks(self, functional, PA, PB, incremental=False, FA=None, FB=None):
+        """Open-shell host build. Returns (exc, nelec_alpha, nelec_beta, FA, FB), FA += Vxc_A, FB += Vxc_B."""
+        PA = np.ascontiguousarray(PA, dtype=np.float64)
+        PB = np.ascontiguousarray(PB, dtype=np.float64)
+        FA = np.zeros((self.nao, self.nao)) if FA is None else FA
+        FB = np.zeros((self.nao, self.nao)) if FB is None else FB
+        assert FA.flags.c_contiguous and FA.dtype == np.float64 and FB.flags.c_contiguous and FB.dtype == np.float64
+        exc, na, nb = ctypes.c_double(), ctypes.c_double(), ctypes.c_double()
+        self._check(self.L.pdfxc_build_vxc_uks(self.h, FUNCTIONALS[functional], _ptr(PA), _ptr(PB), int(incremental),
+                                               _ptr(FA), _ptr(FB), ctypes.byref(exc), ctypes.byref(na),
+                                               ctypes.byref(nb)), "pdfxc_build_vxc_uks")
+        return exc.value, na.value, nb.value, FA, FB
+
+    def get_rho_uks(self, gga):
+        out = np.zeros((self.npts, 8 if gga else 2))
+        self._check(self.L.pdfxc_get_rho_uks(self.h, int(gga), _ptr(out)), "pdfxc_get_rho_uks")
+        return out
+
+    def set_rho_uks(self, rho, gga):
+        rho = np.ascontiguousarray(rho, dtype=np.float64)
+        self._check(self.L.pdfxc_set_rho_uks(self.h, int(gga), _ptr(rho)), "pdfxc_set_rho_uks")
 
     def get_rho(self, gga):
         out = np.zeros((self.npts, 4 if gga else 1))

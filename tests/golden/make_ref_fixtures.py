@@ -14,6 +14,10 @@ its inputs and outputs as compressed .npz files beside this script:
   ref_functionals.npz  functional values and first derivatives of all five
                    functionals on a seeded log-uniform (rho, gamma) set, both
                    the open-shell and the closed-shell overloads.
+  ref_uks_water2.npz  the (H2O)2 grid sample of ref_water2.npz with two different
+                   spin densities (10 alpha, 9 beta occupied): the reference's
+                   open-shell Exc, Vxc_A, Vxc_B and electron counts for all five
+                   functionals, the rho columns for SVWN and B3LYP.
   ref_grad_water.npz  one H2O, cc-pVDZ: the reference's XC nuclear gradient
                    (DfCalcGridX::energyGradient_part, AO-centre and grid-weight
                    terms apart) for SVWN and B3LYP, with the SG-1 grid it
@@ -88,6 +92,29 @@ def functional_fixture():
     np.savez_compressed(os.path.join(HERE, "ref_functionals.npz"), **out)
 
 
+def uks_fixture():
+    w2 = dict(np.load(os.path.join(HERE, "ref_water2.npz")))
+    syms = [str(s) for s in w2["symbols"]]
+    xyz = w2["xyz"]
+    b = basis.load_basis("cc-pVDZ")
+    q = systems.nuclear_charges(syms)
+    sh = basis.ShellTable(syms, xyz, b)
+    PA = 0.5 * systems.density_matrix(sh.nao, 10, seed=20)
+    PB = 0.5 * systems.density_matrix(sh.nao, 9, seed=21)
+    out = {"PA": PA, "PB": PB}
+    with tempfile.TemporaryDirectory() as d:
+        for fn in FUNCS:
+            r = refio.run_xc_uks(d, syms, q, xyz, b, fn, w2["grid"], PA, PB)
+            out[f"{fn}_exc"] = r["exc"]
+            out[f"{fn}_vxc_a"] = r["vxc"].reshape(sh.nao, sh.nao)
+            out[f"{fn}_vxc_b"] = r["vxc_b"].reshape(sh.nao, sh.nao)
+            if fn in ("SVWN", "B3LYP"):  # the rho columns depend only on LDA / GGA
+                out[f"{fn}_rho"] = r["rho"].reshape(len(w2["grid"]), -1)
+            out[f"{fn}_nelec_alpha"] = r["nelec_alpha"]
+            out[f"{fn}_nelec_beta"] = r["nelec_beta"]
+    np.savez_compressed(os.path.join(HERE, "ref_uks_water2.npz"), **out)
+
+
 def grad_fixture():
     b = basis.load_basis("cc-pVDZ")
     syms, xyz = systems.water_cluster(1, seed=0)
@@ -116,6 +143,7 @@ def main():
     syms, xyz = systems.peptide_chain(12, seed=3)
     system_fixture("ref_chain12.npz", syms, xyz, 5000, ["SVWN", "B3LYP"], nocc=20, seed=3)
     functional_fixture()
+    uks_fixture()
     grad_fixture()
 
 

@@ -44,3 +44,24 @@ def test_energy_gradient_matches_reference_class(tmp_path, fn):
     # the weight term moves the result, and the total stays translation invariant
     assert np.abs(won - b200).max() > 1e-8
     assert np.abs(won.reshape(-1, 3).sum(axis=0)).max() < 1e-10 * np.abs(ref).max()
+
+
+@pytest.mark.skipif(not refio.dropin_available(), reason="oracle/_ref/pdfxc_dropin not built")
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_open_shell_overloads_match_reference_class(tmp_path, water2, fn):
+    """The P_A, P_B overloads of DfCalcGridX_B200 against the reference class, two SCF
+    iterations through the grid-matrix files (the second with xc-update)."""
+    from conftest import golden
+    from proteindf_b200 import basis, systems
+    uks = golden("ref_uks_water2.npz")
+    syms = [str(s) for s in water2["symbols"]]
+    g = water2["grid"][:3000]
+    r = refio.run_dropin_uks(str(tmp_path), syms, systems.nuclear_charges(syms), water2["xyz"],
+                             basis.load_basis("cc-pVDZ"), fn, g, uks["PA"], uks["PB"])
+    n = shell_table(water2).nao
+    for it in (1, 2):
+        e_ref, e_b = r[f"ref_exc{it}"][0], r[f"b200_exc{it}"][0]
+        assert abs(e_ref - e_b) <= 1e-10 * abs(e_ref), (it, e_ref, e_b)
+        for spin in ("a", "b"):
+            v_ref, v_b = r[f"ref_vxc{spin}{it}"].reshape(n, n), r[f"b200_vxc{spin}{it}"].reshape(n, n)
+            assert np.abs(v_ref - v_b).max() <= 1e-10, (it, spin)

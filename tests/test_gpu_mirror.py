@@ -43,3 +43,21 @@ def test_mirror_energy_gradient_on_reference_grid(fn):
     ref = fx[f"{fn}_grad_orbital"] + fx[f"{fn}_grad_weight"]
     assert np.abs(g - ref).max() < 1e-11 * np.abs(ref).max()
     calc.close()
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
+def test_mirror_open_shell(water2, fn):
+    from conftest import golden
+    from proteindf_b200.dfcalcgridx import DfCalcGridX
+    uks = golden("ref_uks_water2.npz")
+    calc = DfCalcGridX(param(water2), grid_matrix=water2["grid"])
+    FA, FB = np.zeros_like(uks["PA"]), np.zeros_like(uks["PA"])
+    exc = calc.calcXCIntegForFockAndEnergy(uks["PA"], fn, FA, P_B=uks["PB"], F_B=FB)
+    assert abs(exc - uks[f"{fn}_exc"][0]) < 1e-11 * abs(uks[f"{fn}_exc"][0])
+    assert np.abs(FA - uks[f"{fn}_vxc_a"]).max() < 1e-11
+    assert np.abs(FB - uks[f"{fn}_vxc_b"]).max() < 1e-11
+    na, nb = calc.getWholeDensity()
+    assert abs(na - uks[f"{fn}_nelec_alpha"][0]) < 1e-11 and abs(nb - uks[f"{fn}_nelec_beta"][0]) < 1e-11
+    g = calc.getGridMatrix()
+    assert g.shape[1] == (13 if fn == "B3LYP" else 7)
+    calc.close()

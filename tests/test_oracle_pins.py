@@ -116,3 +116,19 @@ def test_oracle_vs_live_reference_random_system(tmp_path):
     o = oracle.xc("B3LYP", sh, g[:, :4], PA)
     assert abs(r["exc"][0] - o["exc"]) < 1e-12
     assert np.abs(r["vxc"].reshape(sh.nao, -1) - o["vxc"]).max() < 1e-12
+
+
+@pytest.mark.parametrize("fn", ["SVWN", "HFS", "HFB", "BLYP", "B3LYP"])
+def test_oracle_open_shell_vs_reference(water2, fn):
+    """The P_A, P_B overloads (src/libpdf/DfCalcGridX.cpp:2292-2328) on the water-dimer
+    grid sample: Exc, Vxc_A, Vxc_B, electron counts and rho columns."""
+    fx = golden("ref_uks_water2.npz")
+    o = oracle.xc_uks(fn, shell_table(water2), water2["grid"][:, :4], fx["PA"], fx["PB"])
+    assert abs(o["exc"] - fx[f"{fn}_exc"][0]) < 1e-13 * abs(fx[f"{fn}_exc"][0])
+    assert np.abs(o["vxc_a"] - fx[f"{fn}_vxc_a"]).max() < 1e-14
+    assert np.abs(o["vxc_b"] - fx[f"{fn}_vxc_b"]).max() < 1e-14
+    assert abs(o["nelec_alpha"] - fx[f"{fn}_nelec_alpha"][0]) < 1e-13
+    assert abs(o["nelec_beta"] - fx[f"{fn}_nelec_beta"][0]) < 1e-13
+    if f"{fn}_rho" in fx:
+        ref = fx[f"{fn}_rho"]
+        assert np.all(np.abs(o["rho"] - ref) <= 1e-13 * np.maximum(1.0, np.abs(ref)))
