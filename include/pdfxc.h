@@ -43,7 +43,9 @@ enum {
     PDFXC_HFS = 1,   /* Slater (LDA) */
     PDFXC_HFB = 2,   /* Becke 88 (GGA) */
     PDFXC_BLYP = 3,  /* Becke 88 + LYP (GGA) */
-    PDFXC_B3LYP = 4  /* 0.80 Slater + 0.72 B88 + 0.19 VWN3 + 0.81 LYP (GGA) */
+    PDFXC_B3LYP = 4, /* 0.80 Slater + 0.72 B88 + 0.19 VWN3 + 0.81 LYP (GGA) */
+    PDFXC_PBE = 5    /* PBE exchange + PBE correlation (GGA); not in the reference, written from the
+                        published papers (Perdew, Burke, Ernzerhof 1996; Perdew, Wang 1992) */
 };
 
 enum {

@@ -11,8 +11,8 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libpdfxc_oracle.so")
 
-FUNCTIONALS = {"SVWN": 0, "HFS": 1, "HFB": 2, "BLYP": 3, "B88LYP": 3, "B3LYP": 4}
-GGA = {"HFB", "BLYP", "B88LYP", "B3LYP"}
+FUNCTIONALS = {"SVWN": 0, "HFS": 1, "HFB": 2, "BLYP": 3, "B88LYP": 3, "B3LYP": 4, "PBE": 5}
+GGA = {"HFB", "BLYP", "B88LYP", "B3LYP", "PBE"}
 
 _lib = None
 

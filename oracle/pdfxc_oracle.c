@@ -14,6 +14,7 @@
  * rhoB = rhoA and gAB = gBB = gAA, exactly as DfFunctional_{LDA,GGA}'s
  * closed-shell overloads do (src/libpdf/DfFunctional.h:98-126, :182-233).
  */
+#include <complex.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -22,7 +23,69 @@
 #include <omp.h>
 #endif
 
-enum { FN_SVWN = 0, FN_HFS = 1, FN_HFB = 2, FN_BLYP = 3, FN_B3LYP = 4 };
+enum { FN_SVWN = 0, FN_HFS = 1, FN_HFB = 2, FN_BLYP = 3, FN_B3LYP = 4, FN_PBE = 5 };
+
+/* ---------------- PBE (not in the reference): Perdew, Burke, Ernzerhof, Phys. Rev.
+ * Lett. 77, 3865 (1996) with the PW92 local correlation (Perdew, Wang, Phys. Rev. B
+ * 45, 13244 (1992)), restated from the papers in complex arithmetic so that the
+ * first derivatives follow by complex-step differentiation (Squire, Trapp 1998):
+ * df/dx = Im f(x + i h) / h, h = 1e-30, exact to rounding for this analytic f.
+ * Parity is unpinned (no reference implementation); the device's dual-number
+ * derivatives and this restatement are independent. */
+static double complex pbe_g(double complex rs, double A, double a1, double b1, double b2, double b3, double b4) {
+    const double complex srs = csqrt(rs);
+    const double complex den = 2.0 * A * (b1 * srs + b2 * rs + b3 * rs * srs + b4 * rs * rs);
+    return -2.0 * A * (1.0 + a1 * rs) * clog(1.0 + 1.0 / den);
+}
+
+static double complex pbe_x_spin(double complex r, double complex g) {
+    const double pi = M_PI, kappa = 0.804, mu = 0.06672455060314922 * M_PI * M_PI / 3.0;
+    const double complex n = 2.0 * r;
+    const double complex s2 = g / (cpow(3.0 * pi * pi * n, 2.0 / 3.0) * n * n);
+    const double complex fx = 1.0 + kappa - kappa / (1.0 + mu * s2 / kappa);
+    return 0.5 * (-0.75 * pow(3.0 / pi, 1.0 / 3.0)) * cpow(n, 4.0 / 3.0) * fx;
+}
+
+static double complex pbe_c(double complex ra, double complex rb, double complex gaa, double complex gab,
+                            double complex gbb) {
+    const double pi = M_PI, beta = 0.06672455060314922, gam = (1.0 - log(2.0)) / (pi * pi);
+    const double tiny = 1e-30, zmax = 1.0 - 1e-12;
+    const double fden = pow(2.0, 4.0 / 3.0) - 2.0, fzz = 8.0 / (9.0 * fden);
+    double complex f = 0.0;
+    if (creal(ra) > tiny) f += pbe_x_spin(ra, gaa);
+    if (creal(rb) > tiny) f += pbe_x_spin(rb, gbb);
+    const double complex rho = ra + rb;
+    if (creal(rho) <= tiny) return f;
+    double complex z = (ra - rb) / rho;
+    if (creal(z) > zmax) z = zmax;
+    if (creal(z) < -zmax) z = -zmax;
+    const double complex rs = cpow(3.0 / (4.0 * pi * rho), 1.0 / 3.0);
+    const double complex e0 = pbe_g(rs, 0.0310907, 0.21370, 7.5957, 3.5876, 1.6382, 0.49294);
+    const double complex e1 = pbe_g(rs, 0.01554535, 0.20548, 14.1189, 6.1977, 3.3662, 0.62517);
+    const double complex ac = -pbe_g(rs, 0.0168869, 0.11125, 10.357, 3.6231, 0.88026, 0.49671);
+    const double complex fz = (cpow(1.0 + z, 4.0 / 3.0) + cpow(1.0 - z, 4.0 / 3.0) - 2.0) / fden;
+    const double complex z4 = z * z * z * z;
+    const double complex ec = e0 + ac * fz * (1.0 - z4) / fzz + (e1 - e0) * fz * z4;
+    const double complex phi = 0.5 * (cpow(1.0 + z, 2.0 / 3.0) + cpow(1.0 - z, 2.0 / 3.0));
+    const double complex phi3 = phi * phi * phi;
+    const double complex ks2 = 4.0 * cpow(3.0 * pi * pi * rho, 1.0 / 3.0) / pi;
+    const double complex t2 = (gaa + 2.0 * gab + gbb) / (4.0 * phi * phi * ks2 * rho * rho);
+    const double complex A = (beta / gam) / (cexp(-ec / (gam * phi3)) - 1.0);
+    const double complex at2 = A * t2;
+    const double complex H = gam * phi3 * clog(1.0 + (beta / gam) * t2 * (1.0 + at2) / (1.0 + at2 + at2 * at2));
+    return f + rho * (ec + H);
+}
+
+static void pbe(double ra, double rb, double gaa, double gab, double gbb, double* o) {
+    const double h = 1e-30;
+    const double x[5] = {ra, rb, gaa, gab, gbb};
+    o[0] = creal(pbe_c(ra, rb, gaa, gab, gbb));
+    for (int k = 0; k < 5; ++k) {
+        double complex y[5];
+        for (int i = 0; i < 5; ++i) y[i] = x[i] + (i == k ? h * I : 0.0);
+        o[1 + k] = cimag(pbe_c(y[0], y[1], y[2], y[3], y[4])) / h;
+    }
+}
 
 /* ---------------- Slater exchange: src/libpdf/DfFunctional_Slater.cpp:25-85 ---- */
 static double slater_coef(void) { return -(9.0 / 4.0) * pow(3.0 / (4.0 * M_PI), 1.0 / 3.0) * (2.0 / 3.0); }
@@ -265,6 +328,9 @@ int pdfxc_oracle_functional(int fn, double ra, double rb, double gaa, double gab
             vgbb = 0.72 * gbb2 + 0.81 * glb;
             break;
         }
+        case FN_PBE:
+            pbe(ra, rb, gaa, gab, gbb, out);
+            return 0;
         default:
             return -1;
     }
@@ -272,7 +338,7 @@ int pdfxc_oracle_functional(int fn, double ra, double rb, double gaa, double gab
     return 0;
 }
 
-int pdfxc_oracle_is_gga(int fn) { return fn == FN_HFB || fn == FN_BLYP || fn == FN_B3LYP; }
+int pdfxc_oracle_is_gga(int fn) { return fn == FN_HFB || fn == FN_BLYP || fn == FN_B3LYP || fn == FN_PBE; }
 
 /* Single components, for the reference's per-class known-answer tests:
  * 0 Slater, 1 VWN5, 2 VWN3, 3 Becke88, 4 Becke88 except LDA, 5 LYP. */

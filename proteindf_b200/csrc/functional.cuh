@@ -11,8 +11,11 @@
 //   LYP          src/libpdf/DfFunctional_LYP.cpp:25-675
 //   composites   SVWN (DfFunctional_SVWN.cpp:25-41), B88LYP (DfFunctional_B88LYP.cpp),
 //                B3LYP 0.80/0.72/0.19/0.81 (DfFunctional_B3LYP.cpp:25-150)
+//   PBE          not in the reference: pbe.cuh (Perdew-Burke-Ernzerhof 1996, PW92 correlation)
 // Transcendentals are CUDA's own pow/exp/log/atan/sqrt.
 #pragma once
+
+#include "pbe.cuh"
 
 namespace pdfxc {
 
@@ -202,7 +205,7 @@ __device__ __forceinline__ void lyp_v(double ra, double rb, double gaa, double g
 
 }  // namespace fdetail
 
-__host__ __device__ constexpr bool functional_is_gga(int fn) { return fn == 2 || fn == 3 || fn == 4; }
+__host__ __device__ constexpr bool functional_is_gga(int fn) { return fn == 2 || fn == 3 || fn == 4 || fn == 5; }
 
 __device__ __forceinline__ XcOut eval_functional(int fn, double ra, double rb, double gaa, double gab,
                                                  double gbb) {
@@ -228,6 +231,11 @@ __device__ __forceinline__ XcOut eval_functional(int fn, double ra, double rb, d
             o.f = f1 + f2, o.va = a1 + a2, o.vb = b1 + b2;
             o.vgaa = g1 + g2, o.vgab = g4, o.vgbb = g3 + g5;
             break;
+        case 5: {  // PBE: value and the five first derivatives through dual numbers
+            const Dual5 f = pbe::pbe(dvar(ra, 0), dvar(rb, 1), dvar(gaa, 2), dvar(gab, 3), dvar(gbb, 4));
+            o.f = f.v, o.va = f.d[0], o.vb = f.d[1], o.vgaa = f.d[2], o.vgab = f.d[3], o.vgbb = f.d[4];
+            break;
+        }
         default: {  // B3LYP
             double fs, as, bs, fv, av, bv, fb, ab, bb, gba, gbb2, fl, al, bl, gla, glab, glb;
             slater(ra, rb, fs, as, bs);

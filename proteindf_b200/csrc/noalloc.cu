@@ -127,7 +127,7 @@ extern "C" pdfxc_status pdfxc_build_vxc_noalloc(int device, int functional, int 
                                                 const double* d_prim_coef, int nao, int64_t npts,
                                                 const double* d_xyzw, const double* d_PA, double* d_V,
                                                 double* d_exc_nelec, void* stream) {
-    if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP || natom <= 0 || nshell <= 0 || nao <= 0 || npts <= 0)
+    if (functional < PDFXC_SVWN || functional > PDFXC_PBE || natom <= 0 || nshell <= 0 || nao <= 0 || npts <= 0)
         return PDFXC_ERR_ARG;
     if (nao > PDFXC_NOALLOC_MAX_AO || nshell > PDFXC_NOALLOC_MAX_SHELL) return PDFXC_ERR_ARG;
     if (!d_atom_xyz || !d_shell_atom || !d_shell_l || !d_shell_nprim || !d_prim_exp || !d_prim_coef || !d_xyzw ||

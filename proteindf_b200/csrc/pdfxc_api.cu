@@ -622,7 +622,7 @@ pdfxc_status check_build(pdfxc_ctx* ctx, int functional, int incremental) {
         ctx->err = "pdfxc_build_vxc: call pdfxc_set_system and pdfxc_set_grid first";
         return PDFXC_ERR_STATE;
     }
-    if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP) {
+    if (functional < PDFXC_SVWN || functional > PDFXC_PBE) {
         ctx->err = "pdfxc_build_vxc: unknown functional id " + std::to_string(functional);
         return PDFXC_ERR_ARG;
     }
@@ -750,7 +750,7 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
             ctx->err = "pdfxc_build_vxc_uks: call pdfxc_set_system and pdfxc_set_grid first";
             return PDFXC_ERR_STATE;
         }
-        if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP || !PA || !PB || !FA || !FB) {
+        if (functional < PDFXC_SVWN || functional > PDFXC_PBE || !PA || !PB || !FA || !FB) {
             ctx->err = "pdfxc_build_vxc_uks: unknown functional or null pointer";
             return PDFXC_ERR_ARG;
         }
@@ -884,7 +884,7 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
             ctx->err = "pdfxc_xc_gradient: the grid was set without owner atoms (pass atom to pdfxc_set_grid)";
             return PDFXC_ERR_STATE;
         }
-        if (functional < PDFXC_SVWN || functional > PDFXC_B3LYP || !PA || !grad_orbital) {
+        if (functional < PDFXC_SVWN || functional > PDFXC_PBE || !PA || !grad_orbital) {
             ctx->err = "pdfxc_xc_gradient: unknown functional or null pointer";
             return PDFXC_ERR_ARG;
         }

@@ -11,8 +11,8 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libpdfxc.so")
 
-FUNCTIONALS = {"SVWN": 0, "HFS": 1, "HFB": 2, "BLYP": 3, "B88LYP": 3, "B3LYP": 4}
-GGA = {"HFB", "BLYP", "B88LYP", "B3LYP"}
+FUNCTIONALS = {"SVWN": 0, "HFS": 1, "HFB": 2, "BLYP": 3, "B88LYP": 3, "B3LYP": 4, "PBE": 5}
+GGA = {"HFB", "BLYP", "B88LYP", "B3LYP", "PBE"}
 PRECISION = {"fp64": 0, "mixed": 1}
 
 # Every entry point include/pdfxc.h declares.
