@@ -97,6 +97,15 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
                                  const int* atom, const double* w_single,
                                  const double* becke_radius, int size_adjust, double* w_out);
 
+/* Stratmann-Scuseria partition weights (DfGenerateGrid::calcMultiCenterWeight_SS,
+ * src/libpdf/DfGenerateGrid.cpp:1878-1956; grid/partitioning_method = SSWeight):
+ * w_out[i] = w_single[i] * P_owner(r_i) / sum_m P_m(r_i) with the SS cell function
+ * (a = 0.64, no size adjustment). Exact zeros of the cell function end each atom's
+ * product early, so large systems stay near O(N_atom) per point; at most 6000 atoms.
+ * Requires pdfxc_set_system. */
+pdfxc_status pdfxc_ss_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
+                              const double* w_single, double* w_out);
+
 /* One closed-shell XC build: rho pass + Vxc pass
  * (DfCalcGridX::calcXCIntegForFockAndEnergy, src/libpdf/DfCalcGridX.cpp:2280-2315).
  * PA: n_ao x n_ao alpha density (host). If incremental != 0 the density

@@ -174,3 +174,15 @@ def xc_uks(name, sh, xyzw, PA, PB, rho_cut=1e-16, threads=0):
                               va.ctypes.data_as(ctypes.c_void_p), vb.ctypes.data_as(ctypes.c_void_p),
                               rho.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(threads))
     return {"exc": exc.value, "nelec_alpha": na.value, "nelec_beta": nb.value, "vxc_a": va, "vxc_b": vb, "rho": rho}
+
+
+def ss(atom_xyz, xyz, owner):
+    """Stratmann-Scuseria partition factor of each point for its owner atom."""
+    atom_xyz = np.ascontiguousarray(atom_xyz, dtype=np.float64)
+    xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+    owner = np.ascontiguousarray(owner, dtype=np.int32)
+    fac = np.zeros(len(xyz))
+    lib().pdfxc_oracle_ss(ctypes.c_int(len(atom_xyz)), atom_xyz.ctypes.data_as(ctypes.c_void_p),
+                          ctypes.c_long(len(xyz)), xyz.ctypes.data_as(ctypes.c_void_p),
+                          owner.ctypes.data_as(ctypes.c_void_p), fac.ctypes.data_as(ctypes.c_void_p))
+    return fac

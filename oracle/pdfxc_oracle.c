@@ -957,3 +957,51 @@ int pdfxc_oracle_xc_uks(int fn, int nshell, int nao, const int* sh_atom, const i
     *nelec_b = NB;
     return 0;
 }
+
+/* ---------------- SS partition weights: src/libpdf/DfGenerateGrid.cpp:1878-1956
+ * (calcMultiCenterWeight_SS). For point r owned by atom A:
+ *   P_m(r) = prod_{n != m} s(mu_mn),  mu_mn = (|r-R_m| - |r-R_n|) / |R_m - R_n| (no size adjustment),
+ *   s = (1 - g)/2,  g = -1 (mu < -a), 1 (mu > a), else (35 z - 35 z^3 + 21 z^5 - 5 z^7)/16, z = mu/a,
+ *   a = 0.64;  factor = P_A / sum_m P_m. */
+int pdfxc_oracle_ss(int natom, const double* atom_xyz, long npts, const double* xyz, const int* owner,
+                    double* factor) {
+#pragma omp parallel
+    {
+        double* rr = (double*)malloc(sizeof(double) * (size_t)natom);
+#pragma omp for schedule(static)
+        for (long i = 0; i < npts; ++i) {
+            const double* r = xyz + 3 * i;
+            for (int m = 0; m < natom; ++m) {
+                const double* A = atom_xyz + 3 * m;
+                rr[m] = sqrt((r[0] - A[0]) * (r[0] - A[0]) + (r[1] - A[1]) * (r[1] - A[1]) +
+                             (r[2] - A[2]) * (r[2] - A[2]));
+            }
+            double tot = 0.0, pown = 0.0;
+            for (int m = 0; m < natom; ++m) {
+                double p = 1.0;
+                for (int n = 0; n < natom; ++n) {
+                    if (n == m) continue;
+                    const double* A = atom_xyz + 3 * m;
+                    const double* B = atom_xyz + 3 * n;
+                    const double Rmn = sqrt((A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) +
+                                            (A[2] - B[2]) * (A[2] - B[2]));
+                    const double u = (rr[m] - rr[n]) * (1.0 / Rmn);
+                    const double a = 0.64;
+                    double g;
+                    if (u < -a) g = -1.0;
+                    else if (u > a) g = 1.0;
+                    else {
+                        const double z = u / a, z2 = z * z, z3 = z2 * z, z5 = z2 * z3;
+                        g = (1.0 / 16.0) * (35.0 * z - 35.0 * z3 + 21.0 * z5 - 5.0 * z5 * z2);
+                    }
+                    p *= 0.5 * (1.0 - g);
+                }
+                tot += p;
+                if (m == owner[i]) pown = p;
+            }
+            factor[i] = pown / tot;
+        }
+        free(rr);
+    }
+    return 0;
+}

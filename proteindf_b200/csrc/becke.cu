@@ -123,7 +123,70 @@ __global__ void __launch_bounds__(BECKE_T) k_becke_tab(const double* __restrict_
     }
 }
 
+// Stratmann-Scuseria partition (DfGenerateGrid::calcMultiCenterWeight_SS,
+// src/libpdf/DfGenerateGrid.cpp:1878-1956): s = (1 - g(mu))/2 with g the
+// piecewise polynomial of a = 0.64, no size adjustment. s is exactly 0 for
+// mu > a and exactly 1 for mu < -a, so the product over n for atom m stops at
+// the first zero factor: for atoms m far from the point that happens within a
+// few factors, which keeps large systems near O(N_atom) per point. Atoms in
+// shared memory (x, y, z, unused), 1/R_mn from the pair table.
+__device__ __forceinline__ double ss_s(double u) {
+    constexpr double a = 0.64;
+    double g;
+    if (u < -a) {
+        g = -1.0;
+    } else if (u > a) {
+        g = 1.0;
+    } else {
+        const double z = u / a, z2 = z * z, z3 = z2 * z, z5 = z2 * z3;
+        g = (1.0 / 16.0) * (35.0 * z - 35.0 * z3 + 21.0 * z5 - 5.0 * z5 * z2);
+    }
+    return 0.5 * (1.0 - g);
+}
+
+__global__ void __launch_bounds__(128) k_ss(const double* __restrict__ atom_xyz, int natom,
+                                            const double* __restrict__ inv, int64_t npts,
+                                            const double* __restrict__ xyz, const int* __restrict__ owner,
+                                            const double* __restrict__ w_single, double* __restrict__ w_out) {
+    extern __shared__ double4 atoms[];
+    for (int a = threadIdx.x; a < natom; a += blockDim.x)
+        atoms[a] = make_double4(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2], 0.0);
+    __syncthreads();
+    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
+        const double rx = xyz[3 * i], ry = xyz[3 * i + 1], rz = xyz[3 * i + 2];
+        const int own = owner[i];
+        double tot = 0.0, pown = 0.0;
+        for (int m = 0; m < natom; ++m) {
+            const double4 A = atoms[m];
+            const double rm = sqrt((rx - A.x) * (rx - A.x) + (ry - A.y) * (ry - A.y) + (rz - A.z) * (rz - A.z));
+            const double* im = inv + (size_t)m * natom;
+            double p = 1.0;
+            for (int n = 0; n < natom && p != 0.0; ++n) {
+                if (n == m) continue;
+                const double4 B = atoms[n];
+                const double rn = sqrt((rx - B.x) * (rx - B.x) + (ry - B.y) * (ry - B.y) + (rz - B.z) * (rz - B.z));
+                p *= ss_s((rm - rn) * __ldg(im + n));
+            }
+            tot += p;
+            if (m == own) pown = p;
+        }
+        w_out[i] = w_single[i] * (pown / tot);
+    }
+}
+
 }  // namespace
+
+void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, int64_t npts, const double* xyz,
+               const int* owner, const double* w_single, double* w_out, cudaStream_t s) {
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, atom_xyz, natom, 0, inv, adj);
+    const int threads = 128;
+    int64_t blocks = (npts + threads - 1) / threads;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks < 1) blocks = 1;
+    const size_t smem = sizeof(double4) * natom;
+    cudaFuncSetAttribute(k_ss, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_ss<<<(unsigned)blocks, threads, smem, s>>>(atom_xyz, natom, inv, npts, xyz, owner, w_single, w_out);
+}
 
 void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
                         double* adj, cudaStream_t s) {

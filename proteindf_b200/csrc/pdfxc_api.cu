@@ -438,20 +438,30 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
     });
 }
 
-pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
-                                 const double* w_single, const double* becke_radius, int size_adjust, double* w_out) {
+}  // extern "C"
+
+namespace {
+
+// Partition weights on the device: Becke (ss = false) or Stratmann-Scuseria (ss = true).
+pdfxc_status partition_weights(pdfxc_ctx* ctx, bool ss, int64_t npts, const double* xyz, const int* atom,
+                               const double* w_single, const double* becke_radius, int size_adjust, double* w_out) {
+    const char* name = ss ? "pdfxc_ss_weights" : "pdfxc_becke_weights";
     return guarded(ctx, [&]() -> pdfxc_status {
         if (ctx->natom == 0) {
-            ctx->err = "pdfxc_becke_weights: call pdfxc_set_system first";
+            ctx->err = std::string(name) + ": call pdfxc_set_system first";
             return PDFXC_ERR_STATE;
         }
-        if (npts <= 0 || !xyz || !atom || !w_single || !becke_radius || !w_out) {
-            ctx->err = "pdfxc_becke_weights: empty input or null pointer";
+        if (npts <= 0 || !xyz || !atom || !w_single || !w_out || (!ss && !becke_radius)) {
+            ctx->err = std::string(name) + ": empty input or null pointer";
             return PDFXC_ERR_ARG;
+        }
+        if (ss && ctx->natom > 6000) {
+            ctx->err = "pdfxc_ss_weights: at most 6000 atoms (atoms are staged in shared memory)";
+            return PDFXC_ERR_UNSUPPORTED;
         }
         for (int64_t i = 0; i < npts; ++i)
             if (atom[i] < 0 || atom[i] >= ctx->natom) {
-                ctx->err = "pdfxc_becke_weights: owner atom index out of range";
+                ctx->err = std::string(name) + ": owner atom index out of range";
                 return PDFXC_ERR_ARG;
             }
         cudaStream_t s = ctx->stream;
@@ -465,9 +475,14 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
             dev_alloc(&d_own, (size_t)npts);
             PDFXC_CUDA(cudaMemcpyAsync(d_xyz, xyz, 3 * sizeof(double) * npts, cudaMemcpyHostToDevice, s));
             PDFXC_CUDA(cudaMemcpyAsync(d_ws, w_single, sizeof(double) * npts, cudaMemcpyHostToDevice, s));
-            PDFXC_CUDA(cudaMemcpyAsync(d_br, becke_radius, sizeof(double) * ctx->natom, cudaMemcpyHostToDevice, s));
+            if (!ss)
+                PDFXC_CUDA(cudaMemcpyAsync(d_br, becke_radius, sizeof(double) * ctx->natom, cudaMemcpyHostToDevice, s));
             PDFXC_CUDA(cudaMemcpyAsync(d_own, atom, sizeof(int) * npts, cudaMemcpyHostToDevice, s));
-            if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
+            if (ss) {
+                dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
+                pdfxc::launch_ss(ctx->d_atom_xyz, ctx->natom, d_pair, d_pair + (size_t)ctx->natom * ctx->natom, npts,
+                                 d_xyz, d_own, d_ws, d_wo, s);
+            } else if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
                 dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
                 pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, d_pair,
                                         d_pair + (size_t)ctx->natom * ctx->natom, npts, d_xyz, d_own, d_ws, d_wo, s);
@@ -484,6 +499,20 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
         dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own), dev_free(d_pair);
         return PDFXC_OK;
     });
+}
+
+}  // namespace
+
+extern "C" {
+
+pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
+                                 const double* w_single, const double* becke_radius, int size_adjust, double* w_out) {
+    return partition_weights(ctx, false, npts, xyz, atom, w_single, becke_radius, size_adjust, w_out);
+}
+
+pdfxc_status pdfxc_ss_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
+                              const double* w_single, double* w_out) {
+    return partition_weights(ctx, true, npts, xyz, atom, w_single, nullptr, 0, w_out);
 }
 
 }  // extern "C"

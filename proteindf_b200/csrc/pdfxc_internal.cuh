@@ -184,6 +184,9 @@ void launch_grad_weight(const double* atom_xyz, int natom, const double* inv, co
                         const double* fdens, double* grad, cudaStream_t s);
 
 // becke.cu
+// Stratmann-Scuseria weights (n_atom <= 6000: atoms in shared memory); inv/adj: n_atom^2 scratch each
+void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, int64_t npts, const double* xyz,
+               const int* owner, const double* w_single, double* w_out, cudaStream_t s);
 void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
                         double* adj, cudaStream_t s);
 void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust,

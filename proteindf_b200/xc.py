@@ -20,7 +20,7 @@ EXPORTS = [
     "pdfxc_default_options", "pdfxc_create", "pdfxc_set_system", "pdfxc_set_grid", "pdfxc_becke_weights",
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
-    "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks",
+    "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
 ]
 
 
@@ -69,6 +69,7 @@ def load_library(path=LIB_PATH):
     L.pdfxc_xc_gradient.argtypes = [_vp, i32, _vp, _vp, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_build_vxc_uks.argtypes = [_vp, i32, _vp, _vp, i32, _vp, _vp, _vp, _vp, _vp]
     L.pdfxc_get_rho_uks.argtypes = [_vp, i32, _vp]
+    L.pdfxc_ss_weights.argtypes = [_vp, i64, _vp, _vp, _vp, _vp]
     L.pdfxc_set_rho_uks.argtypes = [_vp, i32, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
@@ -154,6 +155,16 @@ class XcEngine:
         out = np.zeros(len(xyz))
         self._check(self.L.pdfxc_becke_weights(self.h, len(xyz), _ptr(xyz), _ptr(atom), _ptr(ws), _ptr(br),
                                                int(size_adjust), _ptr(out)), "pdfxc_becke_weights")
+        return out
+
+    def ss_weights(self, xyz, atom, w_single):
+        """Stratmann-Scuseria partition weights: w_single * P_owner / sum_m P_m."""
+        xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
+        atom = np.ascontiguousarray(atom, dtype=np.int32)
+        ws = np.ascontiguousarray(w_single, dtype=np.float64)
+        out = np.zeros(len(xyz))
+        self._check(self.L.pdfxc_ss_weights(self.h, len(xyz), _ptr(xyz), _ptr(atom), _ptr(ws), _ptr(out)),
+                    "pdfxc_ss_weights")
         return out
 
     def build_vxc(self, functional, PA, incremental=False, F=None):

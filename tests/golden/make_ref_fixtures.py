@@ -18,6 +18,9 @@ its inputs and outputs as compressed .npz files beside this script:
                    spin densities (10 alpha, 9 beta occupied): the reference's
                    open-shell Exc, Vxc_A, Vxc_B and electron counts for all five
                    functionals, the rho columns for SVWN and B3LYP.
+  ref_ss_water2.npz  the (H2O)2 USER 75x302 grid with the Stratmann-Scuseria
+                   partition (grid/partitioning_method = SSWeight): single-centre and
+                   final weights of a seeded point sample.
   ref_grad_water.npz  one H2O, cc-pVDZ: the reference's XC nuclear gradient
                    (DfCalcGridX::energyGradient_part, AO-centre and grid-weight
                    terms apart) for SVWN and B3LYP, with the SG-1 grid it
@@ -115,6 +118,21 @@ def uks_fixture():
     np.savez_compressed(os.path.join(HERE, "ref_uks_water2.npz"), **out)
 
 
+def ss_fixture():
+    w2 = dict(np.load(os.path.join(HERE, "ref_water2.npz")))
+    syms = [str(s) for s in w2["symbols"]]
+    kv = dict(GRID)
+    kv["partition"] = "SSWeight"
+    rng = np.random.default_rng(30)
+    with tempfile.TemporaryDirectory() as d:
+        g = refio.run_grid(d, syms, systems.nuclear_charges(syms), w2["xyz"], basis.load_basis("cc-pVDZ"), kv)
+    pts = g["points"].reshape(-1, 3)
+    sel = np.sort(rng.choice(len(pts), 4000, replace=False))
+    np.savez_compressed(os.path.join(HERE, "ref_ss_water2.npz"), points=pts[sel],
+                        atom=g["atom"][sel].astype(np.int32), w_single=g["w_single"][sel],
+                        w_final=g["w_final"][sel])
+
+
 def grad_fixture():
     b = basis.load_basis("cc-pVDZ")
     syms, xyz = systems.water_cluster(1, seed=0)
@@ -144,6 +162,7 @@ def main():
     system_fixture("ref_chain12.npz", syms, xyz, 5000, ["SVWN", "B3LYP"], nocc=20, seed=3)
     functional_fixture()
     uks_fixture()
+    ss_fixture()
     grad_fixture()
 
 

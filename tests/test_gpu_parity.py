@@ -166,3 +166,26 @@ def test_errors_are_status_codes(water2):
         eng.build_vxc("SVWN", water2["PA"], incremental=True)
     with pytest.raises(RuntimeError, match="owner atom"):
         eng.becke_weights(np.zeros((2, 3)), np.array([0, 99]), np.ones(2), np.ones(6))
+
+
+def test_ss_weights_vs_reference(water2):
+    """Device Stratmann-Scuseria weights on the reference's SSWeight grid sample, and
+    on a 30-atom chain against the oracle (relative 1e-13 per weight)."""
+    from oracle import oracle
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    fx = golden("ref_ss_water2.npz")
+    eng = XcEngine(device=0)
+    eng.set_system(shell_table(water2))
+    w = eng.ss_weights(fx["points"], fx["atom"], fx["w_single"])
+    assert np.all(np.abs(w - fx["w_final"]) <= 1e-13 * np.abs(fx["w_single"]))
+    eng.close()
+    syms, xyz = systems.peptide_chain(30, seed=5)
+    Z = [int(z) for z in systems.nuclear_charges(syms)]
+    P, W, A = grids.molecular_grid(xyz, Z, nrad=30, nang=110, radial="GC", mapping="TA", pruning=True)
+    eng = XcEngine(device=0)
+    eng.set_system(basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ")))
+    w = eng.ss_weights(P, A, W)
+    ref = W * oracle.ss(xyz, P, A)
+    assert np.all(np.abs(w - ref) <= 1e-13 * np.abs(W))
+    eng.close()

@@ -132,3 +132,11 @@ def test_oracle_open_shell_vs_reference(water2, fn):
     if f"{fn}_rho" in fx:
         ref = fx[f"{fn}_rho"]
         assert np.all(np.abs(o["rho"] - ref) <= 1e-13 * np.maximum(1.0, np.abs(ref)))
+
+
+def test_oracle_ss_weights_vs_reference(water2):
+    """Stratmann-Scuseria partition (src/libpdf/DfGenerateGrid.cpp:1878-1956) on the
+    reference's own SSWeight grid of the water dimer."""
+    fx = golden("ref_ss_water2.npz")
+    fac = oracle.ss(water2["xyz"], fx["points"], fx["atom"])
+    assert np.abs(fx["w_single"] * fac - fx["w_final"]).max() <= 1e-15 * np.abs(fx["w_single"]).max()
