@@ -173,6 +173,19 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
                                const double* w_single, const double* becke_radius, int size_adjust,
                                double* grad_orbital, double* grad_weight, double* exc);
 
+/* Sharding one molecule over several GPUs (the reference's MPI variant distributes
+ * grid rows and all-reduces F and E, src/libpdf/DfCalcGridX_Parallel.cpp:191-239).
+ * pdfxc_block_costs gives each block's contraction cost 4 nb^2 np (nblocks
+ * values, see pdfxc_grid_stats); pdfxc_partition_blocks (no context, no device)
+ * cuts blocks 0..nblk-1 into nparts contiguous ranges of near-equal cost,
+ * bounds[0..nparts]; pdfxc_set_block_range restricts every later build
+ * (closed shell, open shell, gradient) of the context to blocks [b_lo, b_hi), so
+ * that each rank's Vxc, Exc, electron count and gradient are partial sums whose
+ * all-reduce is the whole. The stored densities of xc-update stay per rank. */
+pdfxc_status pdfxc_block_costs(pdfxc_ctx* ctx, double* cost);
+pdfxc_status pdfxc_partition_blocks(int64_t nblk, const double* cost, int nparts, int64_t* bounds);
+pdfxc_status pdfxc_set_block_range(pdfxc_ctx* ctx, int64_t b_lo, int64_t b_hi);
+
 /* Statistics of the blocked grid: blocks, points (after padding), the sum of
  * 4 * nb^2 * np over blocks (the algorithmic contraction FLOPs of one build)
  * and the mean screened AO count per block. */

@@ -430,6 +430,7 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
         }
         ctx->ws_bytes = max_ws;
         ctx->nblk = nblk;
+        ctx->blk_lo = 0, ctx->blk_hi = nblk;
         ctx->npts = npts;
         ctx->contraction_flops = flops;
         ctx->mean_nb = sum_nb / nblk;
@@ -540,10 +541,21 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho_acc, 0, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s));
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
     }
+    // the context's block range (all blocks unless pdfxc_set_block_range narrowed it)
+    auto clip = [&](const Chunk& c, int& b0, int& n) {
+        b0 = std::max(c.b0, ctx->blk_lo);
+        n = std::min(c.b1, ctx->blk_hi) - b0;
+        return n > 0;
+    };
     for (size_t ci = 0; ci < ctx->chunks.size() && mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
         cudaEvent_t* e = &ctx->stage_ev[5 * ci];
-        pdfxc::MixedArgs a{bv, gv, c.b0, c.b1 - c.b0, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
+        int cb0, cn;
+        if (!clip(c, cb0, cn)) {
+            for (int k = 0; k < 5; ++k) PDFXC_CUDA(cudaEventRecord(e[k], s));
+            continue;
+        }
+        pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
                            ctx->d_Vacc, ctx->d_err};
         const bool oz = ctx->opt.split_terms == 10;
@@ -561,20 +573,25 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     for (size_t ci = 0; ci < ctx->chunks.size() && !mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
         cudaEvent_t* e = &ctx->stage_ev[5 * ci];
-        const int nb = c.b1 - c.b0;
+        int cb0, nb;
+        if (!clip(c, cb0, nb)) {
+            for (int k = 0; k < 5; ++k) PDFXC_CUDA(cudaEventRecord(e[k], s));
+            continue;
+        }
         PDFXC_CUDA(cudaEventRecord(e[0], s));
-        pdfxc::launch_ao_eval(bv, gv, c.b0, nb, gga, ws, 0, s);
+        pdfxc::launch_ao_eval(bv, gv, cb0, nb, gga, ws, 0, s);
         PDFXC_CUDA(cudaEventRecord(e[1], s));
-        pdfxc::launch_gemm_x(gv, d_PA, nao, c.b0, nb, c.max_nbp, gga ? 4 : 1, ws, s);
+        pdfxc::launch_gemm_x(gv, d_PA, nao, cb0, nb, c.max_nbp, gga ? 4 : 1, ws, s);
         PDFXC_CUDA(cudaEventRecord(e[2], s));
-        pdfxc::launch_rho_functional(gv, c.b0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho, ctx->d_coef,
+        pdfxc::launch_rho_functional(gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho, ctx->d_coef,
                                      ctx->d_blk_sum, s);
         PDFXC_CUDA(cudaEventRecord(e[3], s));
-        pdfxc::launch_gemm_v(gv, c.b0, nb, c.max_nbp, gga, ctx->d_coef, ws, ctx->d_Vacc, nao, s);
+        pdfxc::launch_gemm_v(gv, cb0, nb, c.max_nbp, gga, ctx->d_coef, ws, ctx->d_Vacc, nao, s);
         PDFXC_CUDA(cudaEventRecord(e[4], s));
         launches += 4;
     }
-    pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum, ctx->nblk, ctx->d_scalars, s);
+    pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum + 2 * (size_t)ctx->blk_lo,
+                         ctx->blk_hi - ctx->blk_lo, ctx->d_scalars, s);
     launches += 2;
     PDFXC_CUDA(cudaGetLastError());
     PDFXC_CUDA(cudaEventRecord(ctx->stage_ev[nev - 1], s));
@@ -817,18 +834,21 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
         char* ws = static_cast<char*>(ctx->uplan.d_ws);
         PDFXC_CUDA(cudaEventRecord(ctx->ev[0], s));
         for (const Chunk& c : ctx->uplan.chunks) {
-            const int nb = c.b1 - c.b0;
-            pdfxc::launch_ao_eval(bv, gv, c.b0, nb, gga, ws, 0, s);
-            pdfxc::launch_gemm_x_planes(gv, ctx->d_P, nao, c.b0, nb, c.max_nbp, 0, nphi, 1, ws, s);
-            pdfxc::launch_gemm_x_planes(gv, ctx->d_P_b, nao, c.b0, nb, c.max_nbp, 0, nphi + 1, 1, ws, s);
-            pdfxc::launch_rho_functional_uks(gv, c.b0, nb, functional, incremental != 0, ctx->opt.rho_cutoff, ws,
+            const int b0 = std::max(c.b0, ctx->blk_lo), nb = std::min(c.b1, ctx->blk_hi) - b0;
+            if (nb <= 0) continue;
+            pdfxc::launch_ao_eval(bv, gv, b0, nb, gga, ws, 0, s);
+            pdfxc::launch_gemm_x_planes(gv, ctx->d_P, nao, b0, nb, c.max_nbp, 0, nphi, 1, ws, s);
+            pdfxc::launch_gemm_x_planes(gv, ctx->d_P_b, nao, b0, nb, c.max_nbp, 0, nphi + 1, 1, ws, s);
+            pdfxc::launch_rho_functional_uks(gv, b0, nb, functional, incremental != 0, ctx->opt.rho_cutoff, ws,
                                              ctx->d_rho, ctx->d_rho_b, ctx->d_blk_sum, ctx->d_blk_sum_b, s);
-            pdfxc::launch_gemm_v_plane(gv, c.b0, nb, c.max_nbp, nphi, ws, ctx->d_Vacc, nao, s);
-            pdfxc::launch_gemm_v_plane(gv, c.b0, nb, c.max_nbp, nphi + 1, ws, ctx->d_Vacc_b, nao, s);
+            pdfxc::launch_gemm_v_plane(gv, b0, nb, c.max_nbp, nphi, ws, ctx->d_Vacc, nao, s);
+            pdfxc::launch_gemm_v_plane(gv, b0, nb, c.max_nbp, nphi + 1, ws, ctx->d_Vacc_b, nao, s);
             PDFXC_CUDA(cudaGetLastError());
         }
-        pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum, ctx->nblk, ctx->d_scalars, s);
-        pdfxc::launch_finish(ctx->d_Vacc_b, ctx->d_V_b, nao, ctx->d_blk_sum_b, ctx->nblk, ctx->d_scalars_b, s);
+        const size_t lo = ctx->blk_lo;
+        const int nr = ctx->blk_hi - ctx->blk_lo;
+        pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum + 2 * lo, nr, ctx->d_scalars, s);
+        pdfxc::launch_finish(ctx->d_Vacc_b, ctx->d_V_b, nao, ctx->d_blk_sum_b + 2 * lo, nr, ctx->d_scalars_b, s);
         PDFXC_CUDA(cudaEventRecord(ctx->ev[1], s));
         PDFXC_CUDA(cudaGetLastError());
         std::vector<double> Va(n2), Vb(n2);
@@ -948,14 +968,15 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         const pdfxc::BasisView bv = basis_view(ctx);
         char* ws = static_cast<char*>(ctx->gplan.d_ws);
         for (const Chunk& ch : ctx->gplan.chunks) {
-            const int n = ch.b1 - ch.b0;
-            pdfxc::launch_ao_grad(bv, gv, ch.b0, n, gga, ws, s);
-            pdfxc::launch_grad_x(gv, ctx->d_P, nao, ch.b0, n, ch.max_nbp, gga, ws, s);
-            pdfxc::launch_grad_point(gv, ctx->d_ao_atom, ctx->d_owner, ch.b0, n, functional, ctx->opt.rho_cutoff, ws,
+            const int b0 = std::max(ch.b0, ctx->blk_lo), n = std::min(ch.b1, ctx->blk_hi) - b0;
+            if (n <= 0) continue;
+            pdfxc::launch_ao_grad(bv, gv, b0, n, gga, ws, s);
+            pdfxc::launch_grad_x(gv, ctx->d_P, nao, b0, n, ch.max_nbp, gga, ws, s);
+            pdfxc::launch_grad_point(gv, ctx->d_ao_atom, ctx->d_owner, b0, n, functional, ctx->opt.rho_cutoff, ws,
                                      ctx->d_fdens, ctx->d_blk_sum, ctx->d_grad, s);
             PDFXC_CUDA(cudaGetLastError());
         }
-        pdfxc::launch_block_sums(ctx->d_blk_sum, ctx->nblk, ctx->d_scalars, s);
+        pdfxc::launch_block_sums(ctx->d_blk_sum + 2 * (size_t)ctx->blk_lo, ctx->blk_hi - ctx->blk_lo, ctx->d_scalars, s);
         if (w_single) {
             std::vector<double> wslot(nslots, 0.0);
             for (size_t k = 0; k < nslots; ++k)
@@ -967,8 +988,12 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
             double* inv = ctx->d_pair;
             double* adj = ctx->d_pair + (size_t)natom * natom;
             pdfxc::launch_becke_pairs(ctx->d_atom_xyz, ctx->d_brad, natom, size_adjust, inv, adj, s);
-            pdfxc::launch_grad_weight(ctx->d_atom_xyz, natom, inv, adj, (int64_t)nslots, ctx->d_px, ctx->d_py,
-                                      ctx->d_pz, ctx->d_owner, ctx->d_wslot, ctx->d_fdens, ctx->d_grad + 3 * natom, s);
+            // the slots of this context's block range
+            const size_t s0 = (size_t)ctx->blk_lo * BLOCK_PTS;
+            const int64_t ns = (int64_t)(ctx->blk_hi - ctx->blk_lo) * BLOCK_PTS;
+            pdfxc::launch_grad_weight(ctx->d_atom_xyz, natom, inv, adj, ns, ctx->d_px + s0, ctx->d_py + s0,
+                                      ctx->d_pz + s0, ctx->d_owner + s0, ctx->d_wslot + s0, ctx->d_fdens + s0,
+                                      ctx->d_grad + 3 * natom, s);
             PDFXC_CUDA(cudaGetLastError());
         }
         std::vector<double> g(6 * (size_t)natom);
@@ -981,6 +1006,56 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         if (exc) *exc = sc[0];
         return PDFXC_OK;
     });
+}
+
+pdfxc_status pdfxc_block_costs(pdfxc_ctx* ctx, double* cost) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!cost) return PDFXC_ERR_ARG;
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_block_costs: no grid";
+            return PDFXC_ERR_STATE;
+        }
+        for (int b = 0; b < ctx->nblk; ++b)
+            cost[b] = 4.0 * double(ctx->h_meta[b].nb) * ctx->h_meta[b].nb * ctx->h_meta[b].npts;
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_set_block_range(pdfxc_ctx* ctx, int64_t b_lo, int64_t b_hi) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_set_block_range: no grid";
+            return PDFXC_ERR_STATE;
+        }
+        if (b_lo < 0 || b_hi > ctx->nblk || b_lo > b_hi) {
+            ctx->err = "pdfxc_set_block_range: range outside [0, nblocks]";
+            return PDFXC_ERR_ARG;
+        }
+        drop_graph(ctx);
+        ctx->blk_lo = (int)b_lo, ctx->blk_hi = (int)b_hi;
+        ctx->rho_valid = false;  // stored densities outside the new range are not this context's
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_partition_blocks(int64_t nblk, const double* cost, int nparts, int64_t* bounds) {
+    if (nblk < 0 || nparts <= 0 || !bounds || (nblk > 0 && !cost)) return PDFXC_ERR_ARG;
+    double total = 0.0;
+    for (int64_t b = 0; b < nblk; ++b) {
+        if (!(cost[b] >= 0.0)) return PDFXC_ERR_ARG;
+        total += cost[b];
+    }
+    // contiguous ranges cut where the running cost crosses r / nparts of the total
+    bounds[0] = 0;
+    double run = 0.0;
+    int64_t b = 0;
+    for (int r = 1; r < nparts; ++r) {
+        const double target = total * r / nparts;
+        while (b < nblk && run + 0.5 * cost[b] < target) run += cost[b++];
+        bounds[r] = std::max(b, bounds[r - 1]);
+    }
+    bounds[nparts] = nblk;
+    return PDFXC_OK;
 }
 
 pdfxc_status pdfxc_grid_stats(pdfxc_ctx* ctx, int64_t* nblocks, int64_t* npts_padded, double* contraction_flops,

@@ -95,6 +95,7 @@ struct pdfxc_ctx {
     int *d_blk_shells = nullptr, *d_blk_shell_row = nullptr, *d_blk_aos = nullptr;
     double contraction_flops = 0.0;
     double mean_nb = 0.0;
+    int blk_lo = 0, blk_hi = 0;  // the blocks this context builds (pdfxc_set_block_range; default all)
 
     // per-build buffers
     void* d_ws = nullptr;

@@ -21,6 +21,7 @@ EXPORTS = [
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
     "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
+    "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range",
 ]
 
 
@@ -70,6 +71,9 @@ def load_library(path=LIB_PATH):
     L.pdfxc_build_vxc_uks.argtypes = [_vp, i32, _vp, _vp, i32, _vp, _vp, _vp, _vp, _vp]
     L.pdfxc_get_rho_uks.argtypes = [_vp, i32, _vp]
     L.pdfxc_ss_weights.argtypes = [_vp, i64, _vp, _vp, _vp, _vp]
+    L.pdfxc_block_costs.argtypes = [_vp, _vp]
+    L.pdfxc_partition_blocks.argtypes = [i64, _vp, i32, _vp]
+    L.pdfxc_set_block_range.argtypes = [_vp, i64, i64]
     L.pdfxc_set_rho_uks.argtypes = [_vp, i32, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
@@ -81,6 +85,17 @@ def load_library(path=LIB_PATH):
 
 def _ptr(a):
     return a.ctypes.data_as(_vp)
+
+
+def partition_blocks(cost, nparts):
+    """Contiguous block ranges of near-equal cost: bounds (nparts + 1,) int64. Host only."""
+    L = load_library()
+    cost = np.ascontiguousarray(cost, dtype=np.float64)
+    bounds = np.zeros(nparts + 1, dtype=np.int64)
+    st = L.pdfxc_partition_blocks(len(cost), _ptr(cost), int(nparts), _ptr(bounds))
+    if st != 0:
+        raise RuntimeError(f"pdfxc_partition_blocks: status {st}")
+    return bounds
 
 
 class XcEngine:
@@ -239,6 +254,15 @@ class XcEngine:
     def set_rho(self, rho, gga):
         rho = np.ascontiguousarray(rho, dtype=np.float64)
         self._check(self.L.pdfxc_set_rho(self.h, int(gga), _ptr(rho)), "pdfxc_set_rho")
+
+    def block_costs(self):
+        nb = self.grid_stats()["nblocks"]
+        out = np.zeros(nb)
+        self._check(self.L.pdfxc_block_costs(self.h, _ptr(out)), "pdfxc_block_costs")
+        return out
+
+    def set_block_range(self, b_lo, b_hi):
+        self._check(self.L.pdfxc_set_block_range(self.h, int(b_lo), int(b_hi)), "pdfxc_set_block_range")
 
     def grid_stats(self):
         nb, npad = ctypes.c_int64(), ctypes.c_int64()
