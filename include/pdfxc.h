@@ -173,6 +173,33 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
                                const double* w_single, const double* becke_radius, int size_adjust,
                                double* grad_orbital, double* grad_weight, double* exc);
 
+/* A batch of independent molecules in one context: every stage of a build runs
+ * once for all of them (one launch per stage over the blocks of every molecule,
+ * one captured CUDA graph per build). Each molecule's points are blocked and
+ * screened against its own shells only; the joint AO space is the molecules'
+ * AO spaces one after another, and P, Vxc are kept as one dense matrix of that
+ * size whose diagonal blocks are used. No counterpart in the reference (its
+ * DfCalcGridX holds one molecule). */
+typedef struct {
+    int natom;
+    const double* atom_xyz;   /* natom x 3, bohr */
+    const int* atom_z;        /* may be NULL */
+    int nshell;
+    const int* shell_atom;    /* 0..natom-1, this molecule's atoms */
+    const int* shell_l;
+    const int* shell_nprim;
+    const double* prim_exp;
+    const double* prim_coef;
+    int64_t npts;
+    const double* xyzw;       /* npts x 4 */
+    const int* atom;          /* owner atom per point (this molecule's numbering), or NULL */
+} pdfxc_mol;
+pdfxc_status pdfxc_set_batch(pdfxc_ctx* ctx, int nmol, const pdfxc_mol* mols);
+/* PA[m]: n_m x n_m alpha density of molecule m (host); F[m] += Vxc_m; exc[m],
+ * nelec_alpha[m] per molecule (either array may be NULL). */
+pdfxc_status pdfxc_build_vxc_batched(pdfxc_ctx* ctx, int functional, const double* const* PA, int incremental,
+                                     double* const* F, double* exc, double* nelec_alpha);
+
 /* Sharding one molecule over several GPUs (the reference's MPI variant distributes
  * grid rows and all-reduces F and E, src/libpdf/DfCalcGridX_Parallel.cpp:191-239).
  * pdfxc_block_costs gives each block's contraction cost 4 nb^2 np (nblocks

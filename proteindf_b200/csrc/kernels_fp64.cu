@@ -441,7 +441,27 @@ __global__ void k_block_sums(const double* __restrict__ blk_sum, int nblk, doubl
     if (threadIdx.x == 0) out[0] = se[0], out[1] = sn[0];
 }
 
+// Per-segment (per-molecule of a batch) FP64 sums of the block partials: one CTA per
+// segment, blocks [seg_blk[i], seg_blk[i+1]), the same fixed order as k_block_sums.
+__global__ void k_segment_sums(const double* __restrict__ blk_sum, const int* __restrict__ seg_blk, double* out) {
+    __shared__ double se[256], sn[256];
+    const int b0 = seg_blk[blockIdx.x], b1 = seg_blk[blockIdx.x + 1];
+    double e = 0.0, n = 0.0;
+    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x) e += blk_sum[2 * b], n += blk_sum[2 * b + 1];
+    se[threadIdx.x] = e, sn[threadIdx.x] = n;
+    __syncthreads();
+    for (int st = blockDim.x / 2; st > 0; st >>= 1) {
+        if (threadIdx.x < st) se[threadIdx.x] += se[threadIdx.x + st], sn[threadIdx.x] += sn[threadIdx.x + st];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) out[2 * blockIdx.x] = se[0], out[2 * blockIdx.x + 1] = sn[0];
+}
+
 }  // namespace
+
+void launch_segment_sums(const double* blk_sum, const int* seg_blk, int nseg, double* out, cudaStream_t s) {
+    k_segment_sums<<<nseg, 256, 0, s>>>(blk_sum, seg_blk, out);
+}
 
 void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, bool gga, char* ws,
                     int /*max_nsh*/, cudaStream_t s) {

@@ -175,6 +175,8 @@ void free_grid(pdfxc_ctx* c) {
     drop_graph(c);
     dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
     dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
+    dev_free(c->d_seg_blk), dev_free(c->d_mol_sums);
+    c->seg_blk.clear();
     dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum), dev_free(c->d_rho_acc);
     if (c->d_ws) cudaFree(c->d_ws);
     c->d_ws = nullptr;
@@ -291,46 +293,53 @@ pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
     });
 }
 
-pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom) {
-    return guarded(ctx, [&]() -> pdfxc_status {
-        if (ctx->nao == 0) {
-            ctx->err = "pdfxc_set_grid: call pdfxc_set_system first";
-            return PDFXC_ERR_STATE;
-        }
-        if (npts <= 0 || !xyzw) {
-            ctx->err = "pdfxc_set_grid: empty grid or null pointer";
-            return PDFXC_ERR_ARG;
-        }
-        // the owning atom is not needed by the quadrature itself; the gradient keeps it per point
-        if (atom)
-            for (int64_t i = 0; i < npts; ++i)
-                if (atom[i] < 0 || atom[i] >= ctx->natom) {
-                    ctx->err = "pdfxc_set_grid: owner atom index out of range";
-                    return PDFXC_ERR_ARG;
-                }
-        free_grid(ctx);
-        const int bp = ctx->opt.block_points;
-        // 1. spatial order: Morton code over the grid's bounding box
+}  // extern "C"
+
+namespace {
+
+// Points [p0, p1) of the grid whose blocks are screened against shells [sh0, sh1):
+// the whole grid for one molecule, one segment per molecule for a batch.
+struct GridSegment {
+    int64_t p0, p1;
+    int sh0, sh1;
+};
+
+// Spatial blocks and per-block basis screening, once per geometry: within each
+// segment the points are put in Morton order over the segment's bounding box and
+// cut into blocks of block_points; every block keeps the shells of its segment whose
+// value/gradient envelope reaches ao_cutoff at the block's nearest point.
+void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom,
+                const std::vector<GridSegment>& segs) {
+    free_grid(ctx);
+    const int bp = ctx->opt.block_points;
+    int nblk = 0;
+    for (const GridSegment& sg : segs) nblk += (int)((sg.p1 - sg.p0 + bp - 1) / bp);
+    std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
+    ctx->h_src.assign(px.size(), -1);
+    if (atom) ctx->h_owner.assign(px.size(), 0);
+    std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
+    std::vector<int> blk_seg(nblk);
+    ctx->h_meta.assign(nblk, BlockMeta{});
+    ctx->seg_blk.assign(1, 0);
+    int b = 0;
+    for (size_t si = 0; si < segs.size(); ++si) {
+        const GridSegment& sg = segs[si];
+        const int64_t n = sg.p1 - sg.p0;
+        // 1. spatial order: Morton code over the segment's bounding box
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int64_t i = 0; i < npts; ++i)
+        for (int64_t i = sg.p0; i < sg.p1; ++i)
             for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], xyzw[4 * i + k]), hi[k] = std::max(hi[k], xyzw[4 * i + k]);
-        double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-12});
-        std::vector<std::pair<uint64_t, int64_t>> key(npts);
-        for (int64_t i = 0; i < npts; ++i) {
+        const double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-12});
+        std::vector<std::pair<uint64_t, int64_t>> key(n);
+        for (int64_t i = 0; i < n; ++i) {
+            const double* r = xyzw + 4 * (sg.p0 + i);
             uint64_t q[3];
-            for (int k = 0; k < 3; ++k)
-                q[k] = (uint64_t)std::min(2097151.0, std::floor((xyzw[4 * i + k] - lo[k]) / span * 2097151.0));
-            key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, i};
+            for (int k = 0; k < 3; ++k) q[k] = (uint64_t)std::min(2097151.0, std::floor((r[k] - lo[k]) / span * 2097151.0));
+            key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, sg.p0 + i};
         }
         std::sort(key.begin(), key.end());
-        const int nblk = (int)((npts + bp - 1) / bp);
-        std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
-        ctx->h_src.assign(px.size(), -1);
-        if (atom) ctx->h_owner.assign(px.size(), 0);
-        std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
-        ctx->h_meta.assign(nblk, BlockMeta{});
-        for (int b = 0; b < nblk; ++b) {
-            const int64_t i0 = (int64_t)b * bp, i1 = std::min<int64_t>(npts, i0 + bp);
+        for (int64_t i0 = 0; i0 < n; i0 += bp, ++b) {
+            const int64_t i1 = std::min<int64_t>(n, i0 + bp);
             double c[3] = {0, 0, 0};
             for (int64_t i = i0; i < i1; ++i)
                 for (int k = 0; k < 3; ++k) c[k] += xyzw[4 * key[i].second + k];
@@ -353,88 +362,119 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
             for (int k = 0; k < 3; ++k) cen[3 * b + k] = c[k];
             rad[b] = std::sqrt(r2);
             ctx->h_meta[b].npts = (int)(i1 - i0);
+            blk_seg[b] = (int)si;
         }
-        // 2. per-shell screening radius, then the per-block shell lists
-        std::vector<double> Rs(ctx->nshell);
-        for (int s = 0; s < ctx->nshell; ++s)
-            Rs[s] = shell_cutoff_radius(ctx->h_sh_l[s], &ctx->h_p_exp[ctx->h_sh_p0[s]], &ctx->h_p_coef[ctx->h_sh_p0[s]],
-                                        ctx->h_sh_nprim[s], ctx->opt.ao_cutoff);
-        std::vector<int> shells, rows, aos;
-        const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
-        const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
-        double flops = 0.0, sum_nb = 0.0;
-        for (int b = 0; b < nblk; ++b) {
-            BlockMeta& m = ctx->h_meta[b];
-            m.sh0 = (int)shells.size();
-            m.ao0 = (int)aos.size();
-            int row = 0;
-            for (int s = 0; s < ctx->nshell; ++s) {
-                const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[s]];
-                const double d = std::sqrt((A[0] - cen[3 * b]) * (A[0] - cen[3 * b]) + (A[1] - cen[3 * b + 1]) * (A[1] - cen[3 * b + 1]) +
-                                           (A[2] - cen[3 * b + 2]) * (A[2] - cen[3 * b + 2]));
-                if (d - rad[b] > Rs[s]) continue;
-                shells.push_back(s);
-                rows.push_back(row);
-                const int n = 2 * ctx->h_sh_l[s] + 1;
-                for (int c = 0; c < n; ++c) aos.push_back(ctx->h_sh_ao0[s] + c);
-                row += n;
-            }
-            m.nsh = (int)shells.size() - m.sh0;
-            m.nb = row;
-            m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
-            flops += 4.0 * double(m.nb) * m.nb * m.npts;
-            sum_nb += m.nb;
+        ctx->seg_blk.push_back(b);
+    }
+    // 2. per-shell screening radius, then the per-block shell lists
+    std::vector<double> Rs(ctx->nshell);
+    for (int sh = 0; sh < ctx->nshell; ++sh)
+        Rs[sh] = shell_cutoff_radius(ctx->h_sh_l[sh], &ctx->h_p_exp[ctx->h_sh_p0[sh]], &ctx->h_p_coef[ctx->h_sh_p0[sh]],
+                                     ctx->h_sh_nprim[sh], ctx->opt.ao_cutoff);
+    std::vector<int> shells, rows, aos;
+    const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
+    const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
+    double flops = 0.0, sum_nb = 0.0;
+    for (int bb = 0; bb < nblk; ++bb) {
+        BlockMeta& m = ctx->h_meta[bb];
+        const GridSegment& sg = segs[blk_seg[bb]];
+        m.sh0 = (int)shells.size();
+        m.ao0 = (int)aos.size();
+        int row = 0;
+        for (int sh = sg.sh0; sh < sg.sh1; ++sh) {
+            const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[sh]];
+            const double d = std::sqrt((A[0] - cen[3 * bb]) * (A[0] - cen[3 * bb]) +
+                                       (A[1] - cen[3 * bb + 1]) * (A[1] - cen[3 * bb + 1]) +
+                                       (A[2] - cen[3 * bb + 2]) * (A[2] - cen[3 * bb + 2]));
+            if (d - rad[bb] > Rs[sh]) continue;
+            shells.push_back(sh);
+            rows.push_back(row);
+            const int nc = 2 * ctx->h_sh_l[sh] + 1;
+            for (int c = 0; c < nc; ++c) aos.push_back(ctx->h_sh_ao0[sh] + c);
+            row += nc;
         }
-        // 3. chunks of blocks whose intermediates fit the workspace budget
-        ctx->chunks.clear();
-        size_t off = 0, max_ws = 0;
-        Chunk cur{0, 0, 0, 0};
-        for (int b = 0; b < nblk; ++b) {
-            const size_t need = !mixed ? pdfxc::block_ws_doubles(ctx->h_meta[b].nbp, gga_ws) * sizeof(double)
-                                : ctx->opt.split_terms == 10 ? pdfxc::oz_layout(ctx->h_meta[b].nbp).total
-                                                             : pdfxc::mixed_layout(ctx->h_meta[b].nbp).total;
-            if (off + need > ctx->opt.workspace_bytes && b > cur.b0) {
-                cur.b1 = b;
-                cur.ws_bytes = off;
-                ctx->chunks.push_back(cur);
-                max_ws = std::max(max_ws, off);
-                cur = Chunk{b, b, 0, 0};
-                off = 0;
-            }
-            ctx->h_meta[b].ws = (int64_t)off;
-            off += need;
-            cur.max_nbp = std::max(cur.max_nbp, ctx->h_meta[b].nbp);
+        m.nsh = (int)shells.size() - m.sh0;
+        m.nb = row;
+        m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
+        flops += 4.0 * double(m.nb) * m.nb * m.npts;
+        sum_nb += m.nb;
+    }
+    // 3. chunks of blocks whose intermediates fit the workspace budget
+    ctx->chunks.clear();
+    size_t off = 0, max_ws = 0;
+    Chunk cur{0, 0, 0, 0};
+    for (int bb = 0; bb < nblk; ++bb) {
+        const size_t need = !mixed ? pdfxc::block_ws_doubles(ctx->h_meta[bb].nbp, gga_ws) * sizeof(double)
+                            : ctx->opt.split_terms == 10 ? pdfxc::oz_layout(ctx->h_meta[bb].nbp).total
+                                                         : pdfxc::mixed_layout(ctx->h_meta[bb].nbp).total;
+        if (off + need > ctx->opt.workspace_bytes && bb > cur.b0) {
+            cur.b1 = bb;
+            cur.ws_bytes = off;
+            ctx->chunks.push_back(cur);
+            max_ws = std::max(max_ws, off);
+            cur = Chunk{bb, bb, 0, 0};
+            off = 0;
         }
-        cur.b1 = nblk;
-        cur.ws_bytes = off;
-        ctx->chunks.push_back(cur);
-        max_ws = std::max(max_ws, off);
+        ctx->h_meta[bb].ws = (int64_t)off;
+        off += need;
+        cur.max_nbp = std::max(cur.max_nbp, ctx->h_meta[bb].nbp);
+    }
+    cur.b1 = nblk;
+    cur.ws_bytes = off;
+    ctx->chunks.push_back(cur);
+    max_ws = std::max(max_ws, off);
 
-        cudaStream_t s = ctx->stream;
-        upload(&ctx->d_px, px, s);
-        upload(&ctx->d_py, py, s);
-        upload(&ctx->d_pz, pz, s);
-        upload(&ctx->d_pw, pw, s);
-        upload(&ctx->d_meta, ctx->h_meta, s);
-        upload(&ctx->d_blk_shells, shells, s);
-        upload(&ctx->d_blk_shell_row, rows, s);
-        upload(&ctx->d_blk_aos, aos, s);
-        dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
-        dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
-        dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
-        if (mixed) dev_alloc(&ctx->d_rho_acc, (size_t)nblk * BLOCK_PTS * 4);
-        PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho, 0, sizeof(double) * (size_t)nblk * BLOCK_PTS * 4, s));
-        if (cudaMalloc(&ctx->d_ws, max_ws) != cudaSuccess) {
-            ctx->d_ws = nullptr;
-            throw std::bad_alloc();
+    cudaStream_t s = ctx->stream;
+    upload(&ctx->d_px, px, s);
+    upload(&ctx->d_py, py, s);
+    upload(&ctx->d_pz, pz, s);
+    upload(&ctx->d_pw, pw, s);
+    upload(&ctx->d_meta, ctx->h_meta, s);
+    upload(&ctx->d_blk_shells, shells, s);
+    upload(&ctx->d_blk_shell_row, rows, s);
+    upload(&ctx->d_blk_aos, aos, s);
+    upload(&ctx->d_seg_blk, ctx->seg_blk, s);
+    dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
+    dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
+    dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
+    if (mixed) dev_alloc(&ctx->d_rho_acc, (size_t)nblk * BLOCK_PTS * 4);
+    PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho, 0, sizeof(double) * (size_t)nblk * BLOCK_PTS * 4, s));
+    if (cudaMalloc(&ctx->d_ws, max_ws) != cudaSuccess) {
+        ctx->d_ws = nullptr;
+        throw std::bad_alloc();
+    }
+    ctx->ws_bytes = max_ws;
+    ctx->nblk = nblk;
+    ctx->blk_lo = 0, ctx->blk_hi = nblk;
+    ctx->npts = npts;
+    ctx->contraction_flops = flops;
+    ctx->mean_nb = sum_nb / nblk;
+    PDFXC_CUDA(cudaStreamSynchronize(s));
+}
+
+}  // namespace
+
+extern "C" {
+
+pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->nao == 0) {
+            ctx->err = "pdfxc_set_grid: call pdfxc_set_system first";
+            return PDFXC_ERR_STATE;
         }
-        ctx->ws_bytes = max_ws;
-        ctx->nblk = nblk;
-        ctx->blk_lo = 0, ctx->blk_hi = nblk;
-        ctx->npts = npts;
-        ctx->contraction_flops = flops;
-        ctx->mean_nb = sum_nb / nblk;
-        PDFXC_CUDA(cudaStreamSynchronize(s));
+        if (npts <= 0 || !xyzw) {
+            ctx->err = "pdfxc_set_grid: empty grid or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        // the owning atom is not needed by the quadrature itself; the gradient keeps it per point
+        if (atom)
+            for (int64_t i = 0; i < npts; ++i)
+                if (atom[i] < 0 || atom[i] >= ctx->natom) {
+                    ctx->err = "pdfxc_set_grid: owner atom index out of range";
+                    return PDFXC_ERR_ARG;
+                }
+        ctx->mol.clear();
+        build_grid(ctx, npts, xyzw, atom, {GridSegment{0, npts, 0, ctx->nshell}});
         return PDFXC_OK;
     });
 }
@@ -1004,6 +1044,125 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         std::copy(g.begin(), g.begin() + 3 * natom, grad_orbital);
         if (w_single) std::copy(g.begin() + 3 * natom, g.end(), grad_weight);
         if (exc) *exc = sc[0];
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_set_batch(pdfxc_ctx* ctx, int nmol, const pdfxc_mol* mols) {
+    if (!ctx) return PDFXC_ERR_ARG;
+    if (nmol <= 0 || !mols) {
+        ctx->err = "pdfxc_set_batch: no molecules";
+        return PDFXC_ERR_ARG;
+    }
+    std::vector<double> xyz, pexp, pcoef, xyzw;
+    std::vector<int> z, shatom, shl, shnp, owner;
+    std::vector<GridSegment> segs;
+    std::vector<int> aoff(1, 0);
+    int atom_off = 0, shell_off = 0;
+    int64_t pt_off = 0;
+    bool owners = true;
+    for (int m = 0; m < nmol; ++m) {
+        const pdfxc_mol& M = mols[m];
+        if (M.natom <= 0 || M.nshell <= 0 || M.npts <= 0 || !M.atom_xyz || !M.shell_atom || !M.shell_l ||
+            !M.shell_nprim || !M.prim_exp || !M.prim_coef || !M.xyzw) {
+            ctx->err = "pdfxc_set_batch: molecule " + std::to_string(m) + " is empty or has a null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        xyz.insert(xyz.end(), M.atom_xyz, M.atom_xyz + 3 * M.natom);
+        for (int a = 0; a < M.natom; ++a) z.push_back(M.atom_z ? M.atom_z[a] : 0);
+        int np = 0, nao_m = 0;
+        for (int sh = 0; sh < M.nshell; ++sh) {
+            if (M.shell_atom[sh] < 0 || M.shell_atom[sh] >= M.natom) {
+                ctx->err = "pdfxc_set_batch: molecule " + std::to_string(m) + ": shell atom out of range";
+                return PDFXC_ERR_ARG;
+            }
+            shatom.push_back(M.shell_atom[sh] + atom_off);
+            shl.push_back(M.shell_l[sh]);
+            shnp.push_back(M.shell_nprim[sh]);
+            np += M.shell_nprim[sh];
+            nao_m += 2 * M.shell_l[sh] + 1;
+        }
+        pexp.insert(pexp.end(), M.prim_exp, M.prim_exp + np);
+        pcoef.insert(pcoef.end(), M.prim_coef, M.prim_coef + np);
+        xyzw.insert(xyzw.end(), M.xyzw, M.xyzw + 4 * M.npts);
+        if (!M.atom) owners = false;
+        for (int64_t i = 0; owners && i < M.npts; ++i) {
+            if (M.atom[i] < 0 || M.atom[i] >= M.natom) {
+                ctx->err = "pdfxc_set_batch: molecule " + std::to_string(m) + ": owner atom out of range";
+                return PDFXC_ERR_ARG;
+            }
+            owner.push_back(M.atom[i] + atom_off);
+        }
+        segs.push_back(GridSegment{pt_off, pt_off + M.npts, shell_off, shell_off + M.nshell});
+        aoff.push_back(aoff.back() + nao_m);
+        atom_off += M.natom, shell_off += M.nshell, pt_off += M.npts;
+    }
+    pdfxc_status st = pdfxc_set_system(ctx, atom_off, xyz.data(), z.data(), shell_off, shatom.data(), shl.data(),
+                                       shnp.data(), pexp.data(), pcoef.data());
+    if (st != PDFXC_OK) return st;
+    return guarded(ctx, [&]() -> pdfxc_status {
+        build_grid(ctx, pt_off, xyzw.data(), owners ? owner.data() : nullptr, segs);
+        ctx->mol = aoff;
+        dev_alloc(&ctx->d_mol_sums, 2 * (size_t)nmol);
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_build_vxc_batched(pdfxc_ctx* ctx, int functional, const double* const* PA, int incremental,
+                                     double* const* F, double* exc, double* nelec_alpha) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->mol.size() < 2) {
+            ctx->err = "pdfxc_build_vxc_batched: call pdfxc_set_batch first";
+            return PDFXC_ERR_STATE;
+        }
+        pdfxc_status st = check_build(ctx, functional, incremental);
+        if (st) return st;
+        const int nmol = (int)ctx->mol.size() - 1;
+        if (!PA || !F) {
+            ctx->err = "pdfxc_build_vxc_batched: null pointer array";
+            return PDFXC_ERR_ARG;
+        }
+        for (int m = 0; m < nmol; ++m)
+            if (!PA[m] || !F[m]) {
+                ctx->err = "pdfxc_build_vxc_batched: null density or Fock pointer of molecule " + std::to_string(m);
+                return PDFXC_ERR_ARG;
+            }
+        cudaStream_t s = ctx->stream;
+        const size_t n = ctx->nao;
+        // each molecule's P_A into its diagonal block of the joint matrix; the blocks of the
+        // grid only touch their own molecule's AOs, so the off-diagonal blocks are never read
+        for (int m = 0; m < nmol; ++m) {
+            const size_t a0 = ctx->mol[m], nm = ctx->mol[m + 1] - ctx->mol[m];
+            PDFXC_CUDA(cudaMemcpy2DAsync(ctx->d_P + a0 * n + a0, n * sizeof(double), PA[m], nm * sizeof(double),
+                                         nm * sizeof(double), nm, cudaMemcpyHostToDevice, s));
+        }
+        run_build(ctx, functional, ctx->d_P, incremental != 0);
+        pdfxc::launch_segment_sums(ctx->d_blk_sum, ctx->d_seg_blk, nmol, ctx->d_mol_sums, s);
+        PDFXC_CUDA(cudaGetLastError());
+        std::vector<std::vector<double>> V(nmol);
+        std::vector<double> sums(2 * (size_t)nmol);
+        for (int m = 0; m < nmol; ++m) {
+            const size_t a0 = ctx->mol[m], nm = ctx->mol[m + 1] - ctx->mol[m];
+            V[m].resize(nm * nm);
+            PDFXC_CUDA(cudaMemcpy2DAsync(V[m].data(), nm * sizeof(double), ctx->d_V + a0 * n + a0, n * sizeof(double),
+                                         nm * sizeof(double), nm, cudaMemcpyDeviceToHost, s));
+        }
+        PDFXC_CUDA(cudaMemcpyAsync(sums.data(), ctx->d_mol_sums, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+        PDFXC_CUDA(cudaStreamSynchronize(s));
+        collect_profile(ctx);
+        if (int code = device_error(ctx)) {
+            ctx->err = "a bounded device wait expired in the tensor-core contraction (code " + std::to_string(code) + ")";
+            return PDFXC_ERR_TIMEOUT;
+        }
+        for (int m = 0; m < nmol; ++m) {
+            double* Fm = F[m];
+            for (size_t i = 0; i < V[m].size(); ++i) Fm[i] += V[m][i];
+            if (exc) exc[m] = sums[2 * m];
+            if (nelec_alpha) nelec_alpha[m] = sums[2 * m + 1];
+        }
+        ctx->rho_valid = true;
+        ctx->rho_gga = pdfxc::functional_is_gga(functional);
+        ctx->rho_spin = 1;
         return PDFXC_OK;
     });
 }

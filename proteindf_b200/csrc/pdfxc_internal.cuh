@@ -96,6 +96,11 @@ struct pdfxc_ctx {
     double contraction_flops = 0.0;
     double mean_nb = 0.0;
     int blk_lo = 0, blk_hi = 0;  // the blocks this context builds (pdfxc_set_block_range; default all)
+    std::vector<int> seg_blk;    // blocks of grid segment i (a molecule of a batch): [seg_blk[i], seg_blk[i+1])
+    int* d_seg_blk = nullptr;
+    // batch of molecules (pdfxc_set_batch): AO offset and count of each molecule in the joint system
+    std::vector<int> mol;        // AO offsets, size nmol + 1 (empty: a single molecule)
+    double* d_mol_sums = nullptr;  // [2 * nmol]: Exc, electron count per molecule
 
     // per-build buffers
     void* d_ws = nullptr;
@@ -171,6 +176,8 @@ void launch_rho_functional_uks(const GridView& g, int blk0, int nblk, int fn, bo
                                char* ws, double* rho_a, double* rho_b, double* blk_sum, double* blk_sum_b,
                                cudaStream_t s);
 void launch_block_sums(const double* blk_sum, int nblk, double* scalars, cudaStream_t s);
+// per grid segment: out[2 i], out[2 i + 1] = sums over blocks [seg_blk[i], seg_blk[i+1])
+void launch_segment_sums(const double* blk_sum, const int* seg_blk, int nseg, double* out, cudaStream_t s);
 
 // gradient.cu: XC nuclear gradient (FP64)
 int grad_workspace_planes(bool gga);  // [nbp][BLOCK_PTS] double planes per block

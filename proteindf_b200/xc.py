@@ -21,13 +21,22 @@ EXPORTS = [
     "pdfxc_build_vxc", "pdfxc_build_vxc_device", "pdfxc_get_rho", "pdfxc_set_rho", "pdfxc_grid_stats",
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
     "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
-    "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range",
+    "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
+    "pdfxc_build_vxc_batched",
 ]
 
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("block_points", ctypes.c_int), ("ao_cutoff", ctypes.c_double),
                 ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t), ("split_terms", ctypes.c_int)]
+
+
+class Mol(ctypes.Structure):
+    """pdfxc_mol: one molecule of a batch."""
+    _fields_ = [("natom", ctypes.c_int), ("atom_xyz", ctypes.c_void_p), ("atom_z", ctypes.c_void_p),
+                ("nshell", ctypes.c_int), ("shell_atom", ctypes.c_void_p), ("shell_l", ctypes.c_void_p),
+                ("shell_nprim", ctypes.c_void_p), ("prim_exp", ctypes.c_void_p), ("prim_coef", ctypes.c_void_p),
+                ("npts", ctypes.c_int64), ("xyzw", ctypes.c_void_p), ("atom", ctypes.c_void_p)]
 
 
 class Profile(ctypes.Structure):
@@ -74,6 +83,8 @@ def load_library(path=LIB_PATH):
     L.pdfxc_block_costs.argtypes = [_vp, _vp]
     L.pdfxc_partition_blocks.argtypes = [i64, _vp, i32, _vp]
     L.pdfxc_set_block_range.argtypes = [_vp, i64, i64]
+    L.pdfxc_set_batch.argtypes = [_vp, i32, _vp]
+    L.pdfxc_build_vxc_batched.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_set_rho_uks.argtypes = [_vp, i32, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
@@ -254,6 +265,37 @@ class XcEngine:
     def set_rho(self, rho, gga):
         rho = np.ascontiguousarray(rho, dtype=np.float64)
         self._check(self.L.pdfxc_set_rho(self.h, int(gga), _ptr(rho)), "pdfxc_set_rho")
+
+    def set_batch(self, mols):
+        """mols: list of (ShellTable, xyzw (npts, 4), atom (npts,) or None)."""
+        keep, structs = [], (Mol * len(mols))()
+        for k, (sh, xyzw, atom) in enumerate(mols):
+            arrs = [np.ascontiguousarray(a) for a in (
+                sh.atom_xyz.astype(np.float64), sh.atom_z.astype(np.int32), sh.shell_atom.astype(np.int32),
+                sh.shell_l.astype(np.int32), sh.shell_nprim.astype(np.int32), sh.prim_exp.astype(np.float64),
+                sh.prim_coef.astype(np.float64), np.asarray(xyzw, dtype=np.float64).reshape(-1, 4))]
+            at = None if atom is None else np.ascontiguousarray(atom, dtype=np.int32)
+            keep.append((arrs, at))
+            structs[k] = Mol(sh.natom, arrs[0].ctypes.data, arrs[1].ctypes.data, sh.nshell, arrs[2].ctypes.data,
+                             arrs[3].ctypes.data, arrs[4].ctypes.data, arrs[5].ctypes.data, arrs[6].ctypes.data,
+                             len(arrs[7]), arrs[7].ctypes.data, None if at is None else at.ctypes.data)
+        self._check(self.L.pdfxc_set_batch(self.h, len(mols), ctypes.byref(structs)), "pdfxc_set_batch")
+        self._batch_nao = [sh.nao for sh, _, _ in mols]
+        self.nao = sum(self._batch_nao)
+        self.natom = sum(sh.natom for sh, _, _ in mols)
+        self.npts = sum(len(np.asarray(x).reshape(-1, 4)) for _, x, _ in mols)
+
+    def build_vxc_batched(self, functional, PAs, incremental=False, Fs=None):
+        """One build of every molecule of the batch. Returns (exc (nmol,), nelec_alpha (nmol,), Fs)."""
+        nm = len(self._batch_nao)
+        PAs = [np.ascontiguousarray(P, dtype=np.float64) for P in PAs]
+        Fs = [np.zeros((n, n)) for n in self._batch_nao] if Fs is None else Fs
+        pa = (ctypes.c_void_p * nm)(*[P.ctypes.data for P in PAs])
+        fa = (ctypes.c_void_p * nm)(*[F.ctypes.data for F in Fs])
+        exc, nel = np.zeros(nm), np.zeros(nm)
+        self._check(self.L.pdfxc_build_vxc_batched(self.h, FUNCTIONALS[functional], pa, int(incremental), fa,
+                                                   _ptr(exc), _ptr(nel)), "pdfxc_build_vxc_batched")
+        return exc, nel, Fs
 
     def block_costs(self):
         nb = self.grid_stats()["nblocks"]
