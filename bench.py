@@ -18,6 +18,13 @@ mixed-vs-FP64 speed-up and |dExc| / max|dVxc| between them.
 Under torchrun (N > 1) every rank builds its own chain (seed + rank): the units
 are independent molecules, no data-path collective; value = all ranks' points
 / the slowest rank's time (weak scaling).
+
+Other workloads (not the headline line):
+  --workload batch64    64 independent chains of 10-120 atoms (seeded sizes), cc-pVDZ,
+                        B3LYP, USER 75x302 grid with Becke weights, one batched build
+                        (pdfxc_build_vxc_batched: one graph per build for all molecules)
+  --workload chain2000  one 2000-atom chain, cc-pVDZ (~18,600 AOs), B3LYP, USER 75x302
+                        grid with Stratmann-Scuseria weights, AO cut-off 1e-10
 """
 import argparse
 import json
@@ -51,6 +58,7 @@ def parse():
     ap.add_argument("--seed", type=int, default=1)
     ap.add_argument("--cpu-sample", type=int, default=4000, help="grid points for the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="chain", choices=["chain", "batch64", "chain2000"])
     return ap.parse_args()
 
 
@@ -215,6 +223,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload != "chain":
+        return run_large(args)
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -326,6 +336,95 @@ def main():
         e.close()
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_large(args):
+    """The many-molecule batch and the 2000-atom chain, FP64 and INT8 mixed, device time
+    per build (CUDA events of the library, L2 flushed between steps); one GPU."""
+    import torch
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    torch.cuda.set_device(0)
+    b = basis.load_basis("cc-pVDZ")
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    t0 = time.perf_counter()
+    if args.workload == "batch64":
+        rng = np.random.default_rng(args.seed)
+        sizes = rng.integers(10, 121, 64)
+        mols, PAs = [], []
+        tmp = XcEngine(device=0)
+        for k, n in enumerate(sizes):
+            syms, xyz = systems.peptide_chain(int(n), seed=args.seed + 1000 + k)
+            sh = basis.ShellTable(syms, xyz, b)
+            P, W, A = grids.molecular_grid(xyz, sh.atom_z, **grids.PRESETS["USER-75x302"])
+            brad = np.array([grids.BECKE_RADIUS[int(z)] for z in sh.atom_z])
+            tmp.set_system(sh)
+            w = tmp.becke_weights(P, A, W, brad)
+            P2, W2, A2 = grids.screen_by_weight(P, w, A)
+            mols.append((sh, np.c_[P2, W2], A2))
+            PAs.append(0.5 * systems.density_matrix(sh.nao, max(1, int(0.4 * sh.nao)), seed=args.seed + 2000 + k))
+        tmp.close()
+        npts = sum(len(g) for _, g, _ in mols)
+        nao = sum(sh.nao for sh, _, _ in mols)
+        desc = {"workload": "64 independent peptide-like chains of 10-120 atoms (seeded), cc-pVDZ, B3LYP, "
+                            "USER 75x302 grid, Becke weights, one batched build",
+                "molecules": 64, "atoms": int(sizes.sum()), "n_ao_total": int(nao), "grid_points": int(npts)}
+    else:
+        syms, xyz = systems.peptide_chain(2000, seed=args.seed)
+        sh = basis.ShellTable(syms, xyz, b)
+        P, W, A = grids.molecular_grid(xyz, sh.atom_z, **grids.PRESETS["USER-75x302"])
+        tmp = XcEngine(device=0)
+        tmp.set_system(sh)
+        w = tmp.ss_weights(P, A, W)
+        tmp.close()
+        P2, W2, A2 = grids.screen_by_weight(P, w, A)
+        grid4, owner = np.c_[P2, W2], A2
+        PA = 0.5 * systems.density_matrix(sh.nao, int(0.4 * sh.nao), seed=args.seed)
+        npts, nao = len(grid4), sh.nao
+        desc = {"workload": "2000-atom peptide-like chain, cc-pVDZ, B3LYP, USER 75x302 grid, "
+                            "Stratmann-Scuseria weights, AO cut-off 1e-10",
+                "atoms": 2000, "n_ao": int(nao), "grid_points": int(npts)}
+    t_setup = time.perf_counter() - t0
+    out = {}
+    for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
+        eng = XcEngine(device=0, precision=prec, split_terms=args.split_terms,
+                       ao_cutoff=1e-10 if args.workload == "chain2000" else 1e-14)
+        t1 = time.perf_counter()
+        if args.workload == "batch64":
+            eng.set_batch(mols)
+            build = lambda: eng.build_vxc_batched(args.functional, PAs)
+        else:
+            eng.set_system(sh)
+            eng.set_grid(grid4, owner)
+            dP = torch.tensor(PA, device="cuda:0")
+            dV = torch.empty_like(dP)
+            build = lambda: eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+        t_grid = time.perf_counter() - t1
+        for _ in range(args.warmup):
+            r = build()
+        ms = []
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            r = build()
+            ms.append(eng.last_profile()["total_ms"])
+        exc = float(np.sum(r[0])) if args.workload == "batch64" else float(r[0])
+        st = eng.grid_stats()
+        out[prec] = {"ms_per_step": float(np.mean(ms)), "value": npts / (np.mean(ms) * 1e-3), "exc": exc,
+                     "blocks": st["nblocks"], "mean_screened_aos": st["mean_nb"], "set_grid_s": t_grid}
+        eng.close()
+    head = out.get("mixed", out.get("fp64"))
+    line = {"metric": METRIC, "unit": UNIT, "value": head["value"], "ms_per_step": head["ms_per_step"],
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "dtype": "int8 fixed-point slices/i32/f64" if "mixed" in out else "f64",
+            "data": "synthetic (seeded chains and densities)",
+            "config": dict(desc, functional=args.functional, l2="flushed between timed steps (512 MiB write)",
+                           host_setup_s=t_setup)}
+    line.update(out)
+    if "fp64" in out and "mixed" in out:
+        line["mixed_vs_fp64"] = {"speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+                                 "abs_dexc": abs(out["mixed"]["exc"] - out["fp64"]["exc"])}
+    print(json.dumps(line), flush=True)
 
 
 def roofline(args, torch, peaks, r, precision):

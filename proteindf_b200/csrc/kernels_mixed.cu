@@ -836,11 +836,16 @@ __global__ void __launch_bounds__(128, 1)
 size_t oz_smem_bytes() { return (size_t)3 * 2 * OZ_SLICES * umma::I8_SLAB_BYTES + 7 * 8 + 16; }
 
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
+    // per-AO row maxima in dynamic shared memory: above 48 KiB (12,288 AOs in a block) the
+    // kernel has to be allowed more; the launch reports an error beyond the device's limit
     const size_t sm = sizeof(unsigned int) * a.max_nbp;
-    if (functional_is_gga(a.fn))
+    if (functional_is_gga(a.fn)) {
+        if (sm > 48 * 1024) cudaFuncSetAttribute(k_ao_oz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_ao_oz<true><<<a.nblk, 256, sm, s>>>(a.b, a.g, a.blk0, a.ws);
-    else
+    } else {
+        if (sm > 48 * 1024) cudaFuncSetAttribute(k_ao_oz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         k_ao_oz<false><<<a.nblk, 256, sm, s>>>(a.b, a.g, a.blk0, a.ws);
+    }
     k_slice_phi<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
     k_pack_p_oz<<<a.nblk, 256, 0, s>>>(a.g, a.P, a.nao, a.blk0, a.ws);
 }

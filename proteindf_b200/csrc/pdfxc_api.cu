@@ -27,6 +27,14 @@ struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
+// After a kernel launch: a launch that failed (configuration, resources) names itself in the
+// error, also while a graph is being captured. No synchronisation.
+#define PDFXC_LAUNCHED(what)                                                                        \
+    do {                                                                                            \
+        cudaError_t e_ = cudaPeekAtLastError();                                                     \
+        if (e_ != cudaSuccess) throw CudaError(std::string("launch of ") + (what) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
 #define PDFXC_CUDA(call)                                                                            \
     do {                                                                                            \
         cudaError_t e_ = (call);                                                                    \
@@ -50,6 +58,14 @@ template <class T>
 void upload(T** p, const std::vector<T>& v, cudaStream_t s) {
     dev_alloc(p, v.size());
     if (!v.empty()) PDFXC_CUDA(cudaMemcpyAsync(*p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
+// cudaMemsetAsync in pieces of at most 1 GiB (the 18,600-AO matrices are 2.8 GB)
+void memset_async(void* p, size_t bytes, cudaStream_t s) {
+    constexpr size_t piece = size_t(1) << 30;
+    char* c = static_cast<char*>(p);
+    for (size_t off = 0; off < bytes; off += piece)
+        PDFXC_CUDA(cudaMemsetAsync(c + off, 0, std::min(piece, bytes - off), s));
 }
 
 template <class T>
@@ -312,34 +328,57 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
                 const std::vector<GridSegment>& segs) {
     free_grid(ctx);
     const int bp = ctx->opt.block_points;
-    int nblk = 0;
-    for (const GridSegment& sg : segs) nblk += (int)((sg.p1 - sg.p0 + bp - 1) / bp);
-    std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
-    ctx->h_src.assign(px.size(), -1);
-    if (atom) ctx->h_owner.assign(px.size(), 0);
-    std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
-    std::vector<int> blk_seg(nblk);
-    ctx->h_meta.assign(nblk, BlockMeta{});
+    // 1. spatial order: Morton code over each segment's bounding box; a block takes up to
+    // block_points consecutive points and is closed early when its bounding-box diagonal would
+    // pass kMaxBlockExtent, so that a block never straddles two distant regions (on sparse outer
+    // grid shells a 128-point run of the Z curve can span 100 bohr and screen in thousands of AOs)
+    constexpr double kMaxBlockExtent = 12.0;  // bohr
+    std::vector<std::pair<uint64_t, int64_t>> key(npts);
+    std::vector<std::pair<int64_t, int64_t>> runs;  // [i0, i1) of key per block
+    std::vector<int> blk_seg;
     ctx->seg_blk.assign(1, 0);
-    int b = 0;
     for (size_t si = 0; si < segs.size(); ++si) {
         const GridSegment& sg = segs[si];
-        const int64_t n = sg.p1 - sg.p0;
-        // 1. spatial order: Morton code over the segment's bounding box
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
         for (int64_t i = sg.p0; i < sg.p1; ++i)
             for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], xyzw[4 * i + k]), hi[k] = std::max(hi[k], xyzw[4 * i + k]);
         const double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-12});
-        std::vector<std::pair<uint64_t, int64_t>> key(n);
-        for (int64_t i = 0; i < n; ++i) {
-            const double* r = xyzw + 4 * (sg.p0 + i);
+        for (int64_t i = sg.p0; i < sg.p1; ++i) {
+            const double* r = xyzw + 4 * i;
             uint64_t q[3];
             for (int k = 0; k < 3; ++k) q[k] = (uint64_t)std::min(2097151.0, std::floor((r[k] - lo[k]) / span * 2097151.0));
-            key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, sg.p0 + i};
+            key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, i};
         }
-        std::sort(key.begin(), key.end());
-        for (int64_t i0 = 0; i0 < n; i0 += bp, ++b) {
-            const int64_t i1 = std::min<int64_t>(n, i0 + bp);
+        std::sort(key.begin() + sg.p0, key.begin() + sg.p1);
+        for (int64_t i0 = sg.p0; i0 < sg.p1;) {
+            const double* r0 = xyzw + 4 * key[i0].second;
+            double blo[3] = {r0[0], r0[1], r0[2]}, bhi[3] = {r0[0], r0[1], r0[2]};
+            int64_t i1 = i0 + 1;
+            for (; i1 < sg.p1 && i1 - i0 < bp; ++i1) {
+                const double* r = xyzw + 4 * key[i1].second;
+                double d2 = 0.0;
+                for (int k = 0; k < 3; ++k) {
+                    const double l = std::min(blo[k], r[k]), h = std::max(bhi[k], r[k]);
+                    d2 += (h - l) * (h - l);
+                }
+                if (d2 > kMaxBlockExtent * kMaxBlockExtent) break;
+                for (int k = 0; k < 3; ++k) blo[k] = std::min(blo[k], r[k]), bhi[k] = std::max(bhi[k], r[k]);
+            }
+            runs.push_back({i0, i1});
+            blk_seg.push_back((int)si);
+            i0 = i1;
+        }
+        ctx->seg_blk.push_back((int)runs.size());
+    }
+    const int nblk = (int)runs.size();
+    std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
+    ctx->h_src.assign(px.size(), -1);
+    if (atom) ctx->h_owner.assign(px.size(), 0);
+    std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
+    ctx->h_meta.assign(nblk, BlockMeta{});
+    for (int b = 0; b < nblk; ++b) {
+        {
+            const int64_t i0 = runs[b].first, i1 = runs[b].second;
             double c[3] = {0, 0, 0};
             for (int64_t i = i0; i < i1; ++i)
                 for (int k = 0; k < 3; ++k) c[k] += xyzw[4 * key[i].second + k];
@@ -362,9 +401,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
             for (int k = 0; k < 3; ++k) cen[3 * b + k] = c[k];
             rad[b] = std::sqrt(r2);
             ctx->h_meta[b].npts = (int)(i1 - i0);
-            blk_seg[b] = (int)si;
         }
-        ctx->seg_blk.push_back(b);
     }
     // 2. per-shell screening radius, then the per-block shell lists
     std::vector<double> Rs(ctx->nshell);
@@ -574,11 +611,11 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         PDFXC_CUDA(cudaEventCreate(&e));
         ctx->stage_ev.push_back(e);
     }
-    PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc, 0, sizeof(double) * (size_t)nao * nao, s));
+    memset_async(ctx->d_Vacc, sizeof(double) * (size_t)nao * nao, s);
     int64_t launches = 0;
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
     if (mixed) {
-        PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho_acc, 0, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s));
+        memset_async(ctx->d_rho_acc, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
     }
     // the context's block range (all blocks unless pdfxc_set_block_range narrowed it)
@@ -601,12 +638,16 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         const bool oz = ctx->opt.split_terms == 10;
         PDFXC_CUDA(cudaEventRecord(e[0], s));
         oz ? pdfxc::oz_prepare(a, s) : pdfxc::mixed_prepare(a, s);
+        PDFXC_LAUNCHED("prepare (AO values, operand slices)");
         PDFXC_CUDA(cudaEventRecord(e[1], s));
         oz ? pdfxc::oz_rho(a, s) : pdfxc::mixed_rho(a, s);
+        PDFXC_LAUNCHED("rho contraction");
         PDFXC_CUDA(cudaEventRecord(e[2], s));
         oz ? pdfxc::oz_functional(a, s) : pdfxc::mixed_functional(a, s);
+        PDFXC_LAUNCHED("functional / Z");
         PDFXC_CUDA(cudaEventRecord(e[3], s));
         oz ? pdfxc::oz_vxc(a, s) : pdfxc::mixed_vxc(a, s);
+        PDFXC_LAUNCHED("Vxc contraction");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
         launches += oz ? 7 : 6;
     }
@@ -620,13 +661,17 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         }
         PDFXC_CUDA(cudaEventRecord(e[0], s));
         pdfxc::launch_ao_eval(bv, gv, cb0, nb, gga, ws, 0, s);
+        PDFXC_LAUNCHED("k_ao_eval");
         PDFXC_CUDA(cudaEventRecord(e[1], s));
         pdfxc::launch_gemm_x(gv, d_PA, nao, cb0, nb, c.max_nbp, gga ? 4 : 1, ws, s);
+        PDFXC_LAUNCHED("k_gemm_x");
         PDFXC_CUDA(cudaEventRecord(e[2], s));
         pdfxc::launch_rho_functional(gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho, ctx->d_coef,
                                      ctx->d_blk_sum, s);
+        PDFXC_LAUNCHED("k_rho_functional");
         PDFXC_CUDA(cudaEventRecord(e[3], s));
         pdfxc::launch_gemm_v(gv, cb0, nb, c.max_nbp, gga, ctx->d_coef, ws, ctx->d_Vacc, nao, s);
+        PDFXC_LAUNCHED("k_gemm_v");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
         launches += 4;
     }
@@ -866,8 +911,8 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
         ensure_plan(ctx, ctx->uplan, nphi + 2);  // phi planes, X_A, X_B
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P_b, PB, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
-        PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc, 0, n2 * sizeof(double), s));
-        PDFXC_CUDA(cudaMemsetAsync(ctx->d_Vacc_b, 0, n2 * sizeof(double), s));
+        memset_async(ctx->d_Vacc, n2 * sizeof(double), s);
+        memset_async(ctx->d_Vacc_b, n2 * sizeof(double), s);
         pdfxc::GridView gv = grid_view(ctx);
         gv.meta = ctx->uplan.d_meta;
         const pdfxc::BasisView bv = basis_view(ctx);
