@@ -425,26 +425,39 @@ __global__ void __launch_bounds__(128, 1)
 // ===========================================================================
 // Fixed-point slices on the INT8 tensor cores (the split-integer product of
 // Ozaki, Ogita, Oishi and Rump, 2012, on an integer unit). Each operand row
-// gets a power-of-two scale 2^e with |v| < 2^e and four signed 7-bit slices,
-// v = 2^e sum_{i=1..4} s_i 2^(-7 i) (slices rounded to nearest, the remainder
-// carried). A_i B_j^T is an exact integer product, accumulated exactly in
-// int32 TMEM; the products with i + j <= 5 are kept, one accumulator per
-// order k = i + j, and the epilogue forms 2^(eA + eB) sum_k 2^(-7 k) D_k in
-// FP64. The only rounding left is the slice truncation (~2^-28 of each row's
-// largest entry), which is unbiased; FP32 accumulation, whose rounding on the
-// tensor cores is toward zero, never occurs.
+// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits in
+// [-127, 127]: v = 2^e (s_1 / 127 + s_2 / (127 254) + s_3 / (127 254^2) +
+// s_4 / (127 254^3)), each digit rounded to nearest and the remainder (at most
+// half a unit) carried, so that |remainder| * 254 <= 127 keeps every digit in
+// range: about 31 bits per operand. A_i B_j^T is an exact integer product,
+// accumulated exactly in int32 TMEM; the products with i + j <= 5 are kept, one
+// accumulator per order k = i + j, and the epilogue forms
+// 2^(eA + eB) sum_k D_k / (127^2 254^(k-2)) in FP64. The operands are sliced
+// from the FP64 AO values of the FP64 path (an FP32 copy of phi would cost
+// ~3e-9 of Exc, the slices cost ~1e-11), and the rho epilogue multiplies by
+// the FP64 AO values. FP32 accumulation, whose rounding on the tensor cores is
+// toward zero, never occurs.
+constexpr double kOzD1 = 127.0, kOzD = 254.0;
+__device__ __forceinline__ double oz_weight(int k) {  // weight of order k = i + j
+    double w = 1.0 / (kOzD1 * kOzD1);
+    for (int i = 2; i < k; ++i) w /= kOzD;
+    return w;
+}
 
-__device__ __forceinline__ int oz_exponent(float m) { return m > 0.f ? ilogbf(m) + 1 : 0; }
+// exponent e with |v| < 2^e for every |v| <= m (0 for m = 0)
+__device__ __forceinline__ int oz_exponent(double m) {
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);
+    return e;
+}
 
 __device__ __forceinline__ void oz_slice(double v, int e, int8_t* s) {
-    double a = ldexp(v, -e);
+    double t = ldexp(v, -e) * kOzD1;  // |t| < 127
 #pragma unroll
     for (int i = 0; i < OZ_SLICES; ++i) {
-        a *= 128.0;
-        double q = rint(a);
-        q = fmin(fmax(q, -127.0), 127.0);
+        const double q = rint(t);
         s[i] = (int8_t)q;
-        a -= q;
+        t = (t - q) * kOzD;  // |t - q| <= 1/2
     }
 }
 
@@ -462,67 +475,28 @@ __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off,
     for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = *reinterpret_cast<uint4*>(s[i]);
 }
 
-// AO values (FP32 copy) and the row scales of phi^T (per point) and phi (per AO).
-template <bool GGA>
-__global__ void __launch_bounds__(256) k_ao_oz(BasisView bas, GridView g, int blk0, char* ws) {
-    extern __shared__ unsigned int s_rowmax[];  // [nbp], float bits of max |phi| per AO
-    __shared__ float s_ptmax[2][BLOCK_PTS];
+// Row scales of phi^T (per point, max over the block's AOs) and of phi (per AO row, max
+// over the points), from the FP64 AO values. One CTA per block: warps take AO rows
+// (lane = 4 points each), every thread also keeps the running maximum of its point.
+__global__ void __launch_bounds__(BLOCK_PTS) k_oz_scales(GridView g, int blk0, char* ws) {
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
     char* base = ws + m.ws;
-    float* phi32 = reinterpret_cast<float*>(base + L.phi32);
-    const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
-    for (int r = threadIdx.x; r < m.nbp; r += blockDim.x) s_rowmax[r] = 0u;
-    __syncthreads();
-    const int p = threadIdx.x & (BLOCK_PTS - 1);
-    const int half = threadIdx.x >> 7;
-    const int gp = blk * BLOCK_PTS + p;
-    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
-    float ptmax = 0.f;
-    for (int i = half; i < m.nsh; i += 2) {
-        const int s = g.blk_shells[m.sh0 + i];
-        const int row0 = g.blk_shell_row[m.sh0 + i];
-        const int a = bas.sh_atom[s];
-        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
-        const double d2 = x * x + y * y + z * z;
-        const int Lq = bas.sh_l[s], n = 2 * Lq + 1, np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
-        for (int c = 0; c < n; ++c) {
-            double v = 0, gx = 0, gy = 0, gz = 0;
-            for (int k = 0; k < np; ++k) {
-                const double al = bas.p_exp[p0 + k];
-                if (al * d2 <= 30.0) {
-                    const double e = bas.p_coef[p0 + k] * exp(-al * d2);
-                    double av, ax, ay, az;
-                    ang_factor_m(Lq * Lq + c, x, y, z, 2.0 * al, av, ax, ay, az);
-                    v += av * e;
-                    if (GGA) gx += ax * e, gy += ay * e, gz += az * e;
-                }
-            }
-            const int mu = row0 + c;
-            const size_t o = (size_t)mu * BLOCK_PTS + p;
-            const float f = (float)v;
-            phi32[o] = f;
-            if (GGA) {
-                phi32[plane32 + o] = (float)gx;
-                phi32[2 * plane32 + o] = (float)gy;
-                phi32[3 * plane32 + o] = (float)gz;
-            }
-            ptmax = fmaxf(ptmax, fabsf(f));
-            atomicMax(&s_rowmax[mu], __float_as_uint(fabsf(f)));
-        }
-    }
-    for (int mu = m.nb + half; mu < m.nbp; mu += 2) {
-        const size_t o = (size_t)mu * BLOCK_PTS + p;
-        phi32[o] = 0.f;
-        if (GGA) phi32[plane32 + o] = phi32[2 * plane32 + o] = phi32[3 * plane32 + o] = 0.f;
-    }
-    s_ptmax[half][p] = ptmax;
-    __syncthreads();
+    const double* phi = reinterpret_cast<const double*>(base + L.phi64);
     int* e_pt = reinterpret_cast<int*>(base + L.e_pt);
     int* e_phi = reinterpret_cast<int*>(base + L.e_phi);
-    if (threadIdx.x < BLOCK_PTS) e_pt[threadIdx.x] = oz_exponent(fmaxf(s_ptmax[0][threadIdx.x], s_ptmax[1][threadIdx.x]));
-    for (int r = threadIdx.x; r < m.nbp; r += blockDim.x) e_phi[r] = oz_exponent(__uint_as_float(s_rowmax[r]));
+    const int p = threadIdx.x, warp = p >> 5, lane = p & 31;
+    double pmax = 0.0;
+    for (int r = 0; r < m.nb; ++r) pmax = fmax(pmax, fabs(phi[(size_t)r * BLOCK_PTS + p]));
+    e_pt[p] = oz_exponent(pmax);
+    for (int r = warp; r < m.nbp; r += BLOCK_PTS / 32) {
+        double mx = 0.0;
+        if (r < m.nb)
+            for (int q = lane; q < BLOCK_PTS; q += 32) mx = fmax(mx, fabs(phi[(size_t)r * BLOCK_PTS + q]));
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (lane == 0) e_phi[r] = oz_exponent(mx);
+    }
 }
 
 // Slices of phi^T (rows = points) and phi (rows = AOs).
@@ -531,7 +505,7 @@ __global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* w
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
     char* base = ws + m.ws;
-    const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+    const double* phi = reinterpret_cast<const double*>(base + L.phi64);
     const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
     const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi);
     double v[16];
@@ -539,13 +513,13 @@ __global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* w
     for (int e = threadIdx.x; e < BLOCK_PTS * g1; e += blockDim.x) {  // phi^T: row p, 16 AOs
         const int p = e % BLOCK_PTS, mu0 = (e / BLOCK_PTS) * 16;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = phi32[(size_t)(mu0 + j) * BLOCK_PTS + p];
+        for (int j = 0; j < 16; ++j) v[j] = mu0 + j < m.nb ? phi[(size_t)(mu0 + j) * BLOCK_PTS + p] : 0.0;
         oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
     }
     for (int e = threadIdx.x; e < m.nbp * (BLOCK_PTS / 16); e += blockDim.x) {  // phi: row mu, 16 points
         const int mu = e / (BLOCK_PTS / 16), p0 = (e % (BLOCK_PTS / 16)) * 16;
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = phi32[(size_t)mu * BLOCK_PTS + p0 + j];
+        for (int j = 0; j < 16; ++j) v[j] = mu < m.nb ? phi[(size_t)mu * BLOCK_PTS + p0 + j] : 0.0;
         oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), v, e_phi[mu]);
     }
 }
@@ -574,7 +548,7 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
         if (live)
             for (int nu = lane; nu < m.nb; nu += 32) mx = fmax(mx, fabs(row[aos[nu]]));
         mx = warp_max_d(mx);
-        const int e = oz_exponent((float)mx * 1.0000001f);
+        const int e = oz_exponent(mx);
         if (lane == 0) e_p[mu] = e;
         for (int g0 = lane * 16; g0 < m.nbp; g0 += 32 * 16) {
 #pragma unroll
@@ -594,9 +568,9 @@ __global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, const d
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
     char* base = ws + m.ws;
-    const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+    const double* phi = reinterpret_cast<const double*>(base + L.phi64);
     int* e_z = reinterpret_cast<int*>(base + L.e_z);
-    const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
     __shared__ double cf[4][BLOCK_PTS];
     __shared__ double zrow[8][BLOCK_PTS];
     for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
@@ -609,15 +583,16 @@ __global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, const d
         for (int j = 0; j < 4; ++j) {
             const int p = lane + 32 * j;
             const size_t o = (size_t)nu * BLOCK_PTS + p;
-            double z = cf[0][p] * (double)phi32[o];
-            if (GGA)
-                z += cf[1][p] * (double)phi32[plane32 + o] + cf[2][p] * (double)phi32[2 * plane32 + o] +
-                     cf[3][p] * (double)phi32[3 * plane32 + o];
+            double z = 0.0;
+            if (nu < m.nb) {
+                z = cf[0][p] * phi[o];
+                if (GGA) z += cf[1][p] * phi[plane + o] + cf[2][p] * phi[2 * plane + o] + cf[3][p] * phi[3 * plane + o];
+            }
             zrow[warp][p] = z;
             mx = fmax(mx, fabs(z));
         }
         mx = warp_max_d(mx);
-        const int e = oz_exponent((float)mx * 1.0000001f);
+        const int e = oz_exponent(mx);
         if (lane == 0) e_z[nu] = e;
         __syncwarp();
         if (lane < BLOCK_PTS / 16)
@@ -745,28 +720,28 @@ __global__ void __launch_bounds__(128, 1)
     if (ready) {
         const int row = warp * 32 + lane;
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        const double w2 = 1.0 / 16384.0, w3 = w2 / 128.0, w4 = w3 / 128.0, w5 = w4 / 128.0;  // 2^-14 .. 2^-35
+        const double w2 = oz_weight(2), w3 = oz_weight(3), w4 = oz_weight(4), w5 = oz_weight(5);
         if (MODE == MODE_RHO) {
-            const float* phi32 = reinterpret_cast<const float*>(base + L.phi32);
+            const double* phi = reinterpret_cast<const double*>(base + L.phi64);
             const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
             const int* e_p = reinterpret_cast<const int*>(base + L.e_p);
-            const size_t plane32 = (size_t)m.nbp * BLOCK_PTS;
+            const size_t plane = (size_t)m.nbp * BLOCK_PTS;
             const int ep = e_pt[row];
             double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
             for (int c0 = 0; c0 < 128; c0 += 16) {
                 // issue all operand loads of these 16 columns first (predicated), then use them
-                float f0[16], f1[16], f2[16], f3[16];
+                double f0[16], f1[16], f2[16], f3[16];
                 int ec[16];
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
                     const int mu = nt * 128 + c0 + c;
                     const bool live = mu < m.nb;
                     const size_t o = (size_t)mu * BLOCK_PTS + row;
-                    f0[c] = live ? phi32[o] : 0.f;
+                    f0[c] = live ? phi[o] : 0.0;
                     if (GGA) {
-                        f1[c] = live ? phi32[plane32 + o] : 0.f;
-                        f2[c] = live ? phi32[2 * plane32 + o] : 0.f;
-                        f3[c] = live ? phi32[3 * plane32 + o] : 0.f;
+                        f1[c] = live ? phi[plane + o] : 0.0;
+                        f2[c] = live ? phi[2 * plane + o] : 0.0;
+                        f3[c] = live ? phi[3 * plane + o] : 0.0;
                     }
                     ec[c] = live ? e_p[mu] : 0;
                 }
@@ -781,11 +756,11 @@ __global__ void __launch_bounds__(128, 1)
                     const double s = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
                                      (double)(int)d5[c] * w5;
                     const double x = ldexp(s, ep + ec[c]);
-                    r += (double)f0[c] * x;
+                    r += f0[c] * x;
                     if (GGA) {
-                        gx += (double)f1[c] * x;
-                        gy += (double)f2[c] * x;
-                        gz += (double)f3[c] * x;
+                        gx += f1[c] * x;
+                        gy += f2[c] * x;
+                        gz += f3[c] * x;
                     }
                 }
             }
@@ -836,16 +811,9 @@ __global__ void __launch_bounds__(128, 1)
 size_t oz_smem_bytes() { return (size_t)3 * 2 * OZ_SLICES * umma::I8_SLAB_BYTES + 7 * 8 + 16; }
 
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
-    // per-AO row maxima in dynamic shared memory: above 48 KiB (12,288 AOs in a block) the
-    // kernel has to be allowed more; the launch reports an error beyond the device's limit
-    const size_t sm = sizeof(unsigned int) * a.max_nbp;
-    if (functional_is_gga(a.fn)) {
-        if (sm > 48 * 1024) cudaFuncSetAttribute(k_ao_oz<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_ao_oz<true><<<a.nblk, 256, sm, s>>>(a.b, a.g, a.blk0, a.ws);
-    } else {
-        if (sm > 48 * 1024) cudaFuncSetAttribute(k_ao_oz<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-        k_ao_oz<false><<<a.nblk, 256, sm, s>>>(a.b, a.g, a.blk0, a.ws);
-    }
+    // the FP64 path's AO values and gradients (the slices are cut from them), then the row scales
+    launch_ao_eval(a.b, a.g, a.blk0, a.nblk, functional_is_gga(a.fn), a.ws, 0, s);
+    k_oz_scales<<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.ws);
     k_slice_phi<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
     k_pack_p_oz<<<a.nblk, 256, 0, s>>>(a.g, a.P, a.nao, a.blk0, a.ws);
 }

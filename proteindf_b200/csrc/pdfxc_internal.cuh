@@ -251,7 +251,7 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 // v = 2^e * sum_i s_i 2^(-7 i); slice planes are packed K-major in 64-byte slabs.
 constexpr int OZ_SLICES = 4;
 struct OzLayout {
-    size_t phi32;               // FP32 phi and grad phi, [4][nbp][128]
+    size_t phi64;               // FP64 phi and grad phi, [4][nbp][128] (written by the FP64 AO kernel)
     size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs
     size_t phi2, phi2_plane;    // phi slices: rows = nbp AOs, K = 128 points
     size_t ppack, ppack_plane;  // P_sub slices: rows = nbp, K = nbp
@@ -264,8 +264,8 @@ __host__ __device__ inline OzLayout oz_layout(int nbp) {
     auto a256 = [](size_t x) { return (x + 255) & ~size_t(255); };
     OzLayout L;
     size_t o = 0;
-    L.phi32 = o;
-    o = a256(o + (size_t)4 * nbp * BLOCK_PTS * 4);
+    L.phi64 = o;  // offset 0: the layout of the FP64 path's phi planes
+    o = a256(o + (size_t)4 * nbp * BLOCK_PTS * 8);
     L.phi1 = o;
     L.phi1_plane = (size_t)BLOCK_PTS * nbp;
     o = a256(o + OZ_SLICES * L.phi1_plane);

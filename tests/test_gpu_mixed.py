@@ -73,9 +73,11 @@ def test_mixed_vs_fp64_gpu_water8():
     assert abs(nelm - nel64) <= 2e-6 * abs(nel64)
 
 
-# INT8 fixed-point slices (split_terms = 10): exact integer accumulation, only
-# the unbiased slice truncation (~2^-28 of each row's largest entry) remains.
-OZ_TOL = (1e-8, 1e-7)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
+# INT8 fixed-point slices (split_terms = 10): operands cut from the FP64 AO values
+# into four radix-254 digits (~31 bits), exact integer accumulation; only the
+# unbiased digit truncation remains (measured: 2e-11 of Exc on the 100-atom chain,
+# 5e-14 on the 2000-atom chain).
+OZ_TOL = (2e-10, 2e-9)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
 
 
 @pytest.mark.parametrize("fn", ["SVWN", "HFB", "B3LYP"])
@@ -87,7 +89,7 @@ def test_water2_int8_slices_vs_reference(water2, fn):
     dV = np.abs(V - water2[f"{fn}_vxc"]).max()
     print(f"{fn} int8 slices: |dExc|={dE:.3e} max|dVxc|={dV:.3e}")
     assert within(exc, water2[f"{fn}_exc"][0], V, water2[f"{fn}_vxc"], OZ_TOL)
-    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-8 * abs(nel)
+    assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-10 * abs(nel)
 
 
 @pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
