@@ -21,41 +21,31 @@ namespace pdfxc {
 
 namespace {
 
-__device__ __forceinline__ void ang_factor(int t, double x, double y, double z, double a2, double& v,
-                                           double& dx, double& dy, double& dz) {
-    // Angular prefactor and its derivative factor for basis type t
-    // (DfCalcGridX.cpp:103-235): phi = sum_k c_k v e^{-a r^2},
-    // d phi / dx = sum_k c_k dx e^{-a r^2}, with a2 = 2a.
+// Angular polynomial A of component t (the reference's prefactors, DfCalcGridX.cpp:103-141)
+// and its gradient.
+__device__ __forceinline__ void ang_poly1(int t, double x, double y, double z, double& A, double& Ax, double& Ay,
+                                          double& Az) {
     const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
     switch (t) {
-        case 0: v = 1.0; dx = -a2 * x; dy = -a2 * y; dz = -a2 * z; break;
-        case 1: v = x; dx = -a2 * x * x + 1.0; dy = -a2 * x * y; dz = -a2 * x * z; break;
-        case 2: v = y; dx = -a2 * y * x; dy = -a2 * y * y + 1.0; dz = -a2 * y * z; break;
-        case 3: v = z; dx = -a2 * z * x; dy = -a2 * z * y; dz = -a2 * z * z + 1.0; break;
-        case 4: v = x * y; dx = -a2 * x * y * x + y; dy = -a2 * x * y * y + x; dz = -a2 * x * y * z; break;
-        case 5: v = z * x; dx = -a2 * x * z * x + z; dy = -a2 * x * z * y; dz = -a2 * x * z * z + x; break;
-        case 6: v = y * z; dx = -a2 * y * z * x; dy = -a2 * y * z * y + z; dz = -a2 * y * z * z + y; break;
-        case 7: {
-            v = 0.5 * (x * x - y * y);
-            dx = 0.5 * ((-a2 * x * x * x + 2.0 * x) - (-a2 * y * y * x));
-            dy = 0.5 * ((-a2 * x * x * y) - (-a2 * y * y * y + 2.0 * y));
-            dz = 0.5 * ((-a2 * x * x * z) - (-a2 * y * y * z));
-            break;
-        }
-        default: {
-            v = s3 * (z * z - 0.5 * (x * x + y * y));
-            const double xxX = -a2 * x * x * x + 2.0 * x, xxY = -a2 * x * x * y, xxZ = -a2 * x * x * z;
-            const double yyX = -a2 * y * y * x, yyY = -a2 * y * y * y + 2.0 * y, yyZ = -a2 * y * y * z;
-            const double zzX = -a2 * z * z * x, zzY = -a2 * z * z * y, zzZ = -a2 * z * z * z + 2.0 * z;
-            dx = s3 * (zzX - 0.5 * (xxX + yyX));
-            dy = s3 * (zzY - 0.5 * (xxY + yyY));
-            dz = s3 * (zzZ - 0.5 * (xxZ + yyZ));
-        }
+        case 0: A = 1.0; Ax = Ay = Az = 0.0; break;
+        case 1: A = x; Ax = 1.0; Ay = Az = 0.0; break;
+        case 2: A = y; Ay = 1.0; Ax = Az = 0.0; break;
+        case 3: A = z; Az = 1.0; Ax = Ay = 0.0; break;
+        case 4: A = x * y; Ax = y; Ay = x; Az = 0.0; break;
+        case 5: A = z * x; Ax = z; Az = x; Ay = 0.0; break;
+        case 6: A = y * z; Ay = z; Az = y; Ax = 0.0; break;
+        case 7: A = 0.5 * (x * x - y * y); Ax = x; Ay = -y; Az = 0.0; break;
+        default: A = s3 * (z * z - 0.5 * (x * x + y * y)); Ax = -s3 * x; Ay = -s3 * y; Az = 2.0 * s3 * z;
     }
 }
 
 // One CTA per block, 256 threads: the point is threadIdx.x % 128, the two
 // halves of the CTA take alternate shells. Stores are coalesced along points.
+// Per shell the contraction is summed once, S0 = sum_k c_k e^{-a_k r^2} and
+// S1 = sum_k c_k a_k e^{-a_k r^2} (primitives with a r^2 > 30 skipped, :690);
+// each component is then phi = A S0 and grad phi = grad A S0 - 2 r A S1 for its
+// angular polynomial A: the reference's per-primitive prefactors
+// (getPrefactor / getPrefactorForDerivative, :103-235) summed in another order.
 template <bool GGA>
 __global__ void __launch_bounds__(256) k_ao_eval(BasisView bas, GridView g, int blk0, char* ws) {
     const int blk = blk0 + blockIdx.x;
@@ -75,27 +65,25 @@ __global__ void __launch_bounds__(256) k_ao_eval(BasisView bas, GridView g, int 
                      z = rz - bas.atom_xyz[3 * a + 2];
         const double d2 = x * x + y * y + z * z;
         const int L = bas.sh_l[s], n = 2 * L + 1, np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
-        double v[5] = {0, 0, 0, 0, 0}, gx[5] = {0, 0, 0, 0, 0}, gy[5] = {0, 0, 0, 0, 0},
-               gz[5] = {0, 0, 0, 0, 0};
+        double S0 = 0.0, S1 = 0.0;
         for (int k = 0; k < np; ++k) {
             const double al = bas.p_exp[p0 + k];
             if (al * d2 <= 30.0) {  // TOOBIG, DfCalcGridX.cpp:42, :690
                 const double e = bas.p_coef[p0 + k] * exp(-al * d2);
-                for (int c = 0; c < n; ++c) {
-                    double av, ax, ay, az;
-                    ang_factor(L * L + c, x, y, z, 2.0 * al, av, ax, ay, az);
-                    v[c] += av * e;
-                    if (GGA) gx[c] += ax * e, gy[c] += ay * e, gz[c] += az * e;
-                }
+                S0 += e;
+                if (GGA) S1 += al * e;
             }
         }
         for (int c = 0; c < n; ++c) {
+            double A, Ax, Ay, Az;
+            ang_poly1(L * L + c, x, y, z, A, Ax, Ay, Az);
             const size_t o = (size_t)(row0 + c) * BLOCK_PTS + p;
-            phi[o] = v[c];
+            phi[o] = A * S0;
             if (GGA) {
-                dphi[o] = gx[c];
-                dphi[plane + o] = gy[c];
-                dphi[2 * plane + o] = gz[c];
+                const double t = 2.0 * A * S1;
+                dphi[o] = Ax * S0 - x * t;
+                dphi[plane + o] = Ay * S0 - y * t;
+                dphi[2 * plane + o] = Az * S0 - z * t;
             }
         }
     }

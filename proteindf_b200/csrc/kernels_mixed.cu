@@ -516,8 +516,11 @@ __global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* w
         for (int j = 0; j < 16; ++j) v[j] = mu0 + j < m.nb ? phi[(size_t)(mu0 + j) * BLOCK_PTS + p] : 0.0;
         oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
     }
-    for (int e = threadIdx.x; e < m.nbp * (BLOCK_PTS / 16); e += blockDim.x) {  // phi: row mu, 16 points
-        const int mu = e / (BLOCK_PTS / 16), p0 = (e % (BLOCK_PTS / 16)) * 16;
+    // phi: a warp takes 8 rows x 64 points (lane = row r, K group kg), so each digit store
+    // instruction writes four whole 128-byte core matrices
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane & 7, kg = lane >> 3;
+    for (int t = warp; t < (m.nbp / 8) * 2; t += blockDim.x / 32) {
+        const int mu = (t >> 1) * 8 + r, p0 = (t & 1) * 64 + kg * 16;
 #pragma unroll
         for (int j = 0; j < 16; ++j) v[j] = mu < m.nb ? phi[(size_t)mu * BLOCK_PTS + p0 + j] : 0.0;
         oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), v, e_phi[mu]);
@@ -530,7 +533,9 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
-// P_sub slices, one warp per row mu: row scale first, then 16-column groups.
+// P_sub digits. Phase 1: the row exponents, a warp per row mu gathering P[aos[mu]][aos[nu]]
+// from the L2-resident P. Phase 2: a warp takes 8 rows x 64 columns (lane = row r, K group
+// kg: 16 columns), so each digit store instruction writes four whole 128-byte core matrices.
 __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __restrict__ P, int nao, int blk0,
                                                    char* ws) {
     const int blk = blk0 + blockIdx.x;
@@ -540,30 +545,38 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
     int* e_p = reinterpret_cast<int*>(base + L.e_p);
     const int* aos = g.blk_aos + m.ao0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double v[16];
     for (int mu = warp; mu < m.nbp; mu += blockDim.x / 32) {
-        const bool live = mu < m.nb;
-        const double* row = live ? P + (size_t)aos[mu] * nao : P;
         double mx = 0.0;
-        if (live)
-            for (int nu = lane; nu < m.nb; nu += 32) mx = fmax(mx, fabs(row[aos[nu]]));
-        mx = warp_max_d(mx);
-        const int e = oz_exponent(mx);
-        if (lane == 0) e_p[mu] = e;
-        for (int g0 = lane * 16; g0 < m.nbp; g0 += 32 * 16) {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int nu = g0 + j;
-                v[j] = (live && nu < m.nb) ? row[aos[nu]] : 0.0;
-            }
-            oz_store16(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, g0, m.nbp), v, e);
+        if (mu < m.nb) {
+            const double* row = P + (size_t)aos[mu] * nao;
+            for (int nu = lane; nu < m.nb; nu += 32) mx = fmax(mx, fabs(__ldg(row + aos[nu])));
         }
+        mx = warp_max_d(mx);
+        if (lane == 0) e_p[mu] = oz_exponent(mx);
+    }
+    __syncthreads();
+    const int r = lane & 7, kg = lane >> 3;
+    const int nk = m.nbp / 64;
+    double v[16];
+    for (int t = warp; t < (m.nbp / 8) * nk; t += blockDim.x / 32) {
+        const int mu = (t / nk) * 8 + r, k0 = (t % nk) * 64 + kg * 16;
+        const bool live = mu < m.nb;
+        const double* row = P + (size_t)(live ? aos[mu] : 0) * nao;
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const int nu = k0 + j;
+            v[j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0.0;
+        }
+        oz_store16(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, k0, m.nbp), v, live ? e_p[mu] : 0);
     }
 }
 
-// Z slices, one warp per row nu (Z[nu][p] = 0.5 w vrho phi + c . grad phi).
+// Z digits (Z[nu][p] = 0.5 w vrho phi + c . grad phi). A warp takes 8 rows: it forms their
+// Z values once (lanes along the points), takes each row's exponent, then cuts digits from a
+// shared-memory copy with lane = row r, K group kg, so each digit store instruction writes
+// four whole 128-byte core matrices.
 template <bool GGA>
-__global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
+__global__ void __launch_bounds__(128) k_pack_z_oz(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
@@ -572,32 +585,39 @@ __global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, const d
     int* e_z = reinterpret_cast<int*>(base + L.e_z);
     const size_t plane = (size_t)m.nbp * BLOCK_PTS;
     __shared__ double cf[4][BLOCK_PTS];
-    __shared__ double zrow[8][BLOCK_PTS];
+    __shared__ double zt[4][8][BLOCK_PTS + 2];  // per warp: 8 rows of Z
+    __shared__ int ez[4][8];
     for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
         cf[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int nu = warp; nu < m.nbp; nu += 8) {
-        double mx = 0.0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane & 7, kg = lane >> 3;
+    double v[16];
+    for (int nu0 = warp * 8; nu0 < m.nbp; nu0 += 32) {
+        for (int q = 0; q < 8; ++q) {
+            const int nu = nu0 + q;
+            double mx = 0.0;
 #pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int p = lane + 32 * j;
-            const size_t o = (size_t)nu * BLOCK_PTS + p;
-            double z = 0.0;
-            if (nu < m.nb) {
-                z = cf[0][p] * phi[o];
-                if (GGA) z += cf[1][p] * phi[plane + o] + cf[2][p] * phi[2 * plane + o] + cf[3][p] * phi[3 * plane + o];
+            for (int j = 0; j < 4; ++j) {
+                const int p = lane + 32 * j;
+                const size_t o = (size_t)nu * BLOCK_PTS + p;
+                double z = 0.0;
+                if (nu < m.nb) {
+                    z = cf[0][p] * phi[o];
+                    if (GGA) z += cf[1][p] * phi[plane + o] + cf[2][p] * phi[2 * plane + o] + cf[3][p] * phi[3 * plane + o];
+                }
+                zt[warp][q][p] = z;
+                mx = fmax(mx, fabs(z));
             }
-            zrow[warp][p] = z;
-            mx = fmax(mx, fabs(z));
+            mx = warp_max_d(mx);
+            if (lane == 0) ez[warp][q] = oz_exponent(mx), e_z[nu] = oz_exponent(mx);
         }
-        mx = warp_max_d(mx);
-        const int e = oz_exponent(mx);
-        if (lane == 0) e_z[nu] = e;
         __syncwarp();
-        if (lane < BLOCK_PTS / 16)
-            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu, lane * 16, BLOCK_PTS),
-                       &zrow[warp][lane * 16], e);
+        for (int slab = 0; slab < 2; ++slab) {
+            const int p0 = slab * 64 + kg * 16;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = zt[warp][r][p0 + j];
+            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, p0, BLOCK_PTS), v, ez[warp][r]);
+        }
         __syncwarp();
     }
 }
@@ -606,29 +626,44 @@ __global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, const d
 __constant__ int kOzA[10] = {1, 1, 2, 1, 2, 3, 1, 2, 3, 4};
 __constant__ int kOzB[10] = {1, 2, 1, 3, 2, 1, 4, 3, 2, 1};
 
+// One CTA per (block, 128-row M tile, 64-row N tile): RHO computes X^T = phi^T P_sub
+// (M = 128 points, N = 64 AOs mu, K = nbp AOs nu) with the rho / grad rho epilogue;
+// VXC computes V = phi Z^T (M = 128 AOs mu, N = 64 AOs nu, K = 128 points) with the
+// FP64 atomic epilogue. Four int32 accumulators of 64 columns (256 TMEM columns) and a
+// two-stage operand ring of 48 KiB let two CTAs share an SM, so one CTA's epilogue
+// overlaps the other's loads and MMAs. A stage holds the A tile's four digit planes
+// (128 rows x 64 K, canonical no-swizzle K-major layout, 8 KiB each) and the B tile's
+// four digit planes (64 rows x 64 K, 4 KiB each): the 64-row half of a packed 128-row
+// tile is four 1 KiB core-matrix groups, copied into a compact layout (LBO 1024 B).
+constexpr int OZ_NT = 64;
+constexpr int OZ_STAGES = 2;
+constexpr uint32_t OZ_A_BYTES = OZ_SLICES * umma::I8_SLAB_BYTES;   // 32 KiB
+constexpr uint32_t OZ_B_SLICE = OZ_NT * umma::I8_SLAB_K;          // 4 KiB
+constexpr uint32_t OZ_STAGE_BYTES = OZ_A_BYTES + OZ_SLICES * OZ_B_SLICE;  // 48 KiB
+constexpr uint32_t OZ_TMEM_COLS = 4 * OZ_NT;                      // one accumulator per order 2..5
+
 template <int MODE, bool GGA>
-__global__ void __launch_bounds__(128, 1)
+__global__ void __launch_bounds__(128, 2)
     k_oz(GridView g, int blk0, char* ws, int* err, int tiles_max, double* rho_acc, double* Vacc, int nao) {
     extern __shared__ __align__(1024) uint8_t smem[];
-    constexpr int S = 3;
-    constexpr uint32_t stage_bytes = 2 * OZ_SLICES * umma::I8_SLAB_BYTES;  // 64 KiB
+    constexpr int S = OZ_STAGES;
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
-    const int ntiles = m.nbp / umma::TILE_ROWS;
-    int mt, nt;
+    const int ntiles = m.nbp / umma::TILE_ROWS;  // 128-row tiles of this block
+    int mt, nt;                                   // nt counts 64-row tiles
     if (MODE == MODE_RHO) {
         mt = 0, nt = blockIdx.x;
-        if (nt >= ntiles) return;
+        if (nt >= 2 * ntiles) return;
     } else {
         mt = blockIdx.x / tiles_max, nt = blockIdx.x % tiles_max;
-        if (mt >= ntiles || nt >= ntiles) return;
+        if (mt >= ntiles || nt >= 2 * ntiles) return;
     }
     __shared__ int s_abort;
     if (threadIdx.x == 0) s_abort = *reinterpret_cast<const volatile int*>(err);
     __syncthreads();
     if (s_abort) return;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * stage_bytes);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * OZ_STAGE_BYTES);
     uint64_t* empty = full + S;
     uint64_t* done = empty + S;
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
@@ -640,21 +675,22 @@ __global__ void __launch_bounds__(128, 1)
     if (MODE == MODE_RHO) {
         Ab = base + L.phi1;
         Aplane = L.phi1_plane;
-        Bb = base + L.ppack + (size_t)nt * umma::TILE_ROWS * m.nbp;
+        Bb = base + L.ppack + (size_t)(nt / 2) * umma::TILE_ROWS * m.nbp;
         Bplane = L.ppack_plane;
         nslabs = m.nbp / (int)umma::I8_SLAB_K;
     } else {
         Ab = base + L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS;
         Aplane = L.phi2_plane;
-        Bb = base + L.zpack + (size_t)nt * umma::TILE_ROWS * BLOCK_PTS;
+        Bb = base + L.zpack + (size_t)(nt / 2) * umma::TILE_ROWS * BLOCK_PTS;
         Bplane = L.zpack_plane;
         nslabs = BLOCK_PTS / (int)umma::I8_SLAB_K;
     }
+    const size_t bhalf = (size_t)(nt & 1) * 8 * 128;  // row groups 8..15 of the 128-row tile
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == 0) umma::tmem_alloc(tslot, 512);
+    if (warp == 0) umma::tmem_alloc(tslot, OZ_TMEM_COLS);
     if (threadIdx.x == 32) {
-        for (int s = 0; s < S; ++s) umma::mbar_init(&full[s], 1), umma::mbar_init(&empty[s], 1);
+        for (int st = 0; st < S; ++st) umma::mbar_init(&full[st], 1), umma::mbar_init(&empty[st], 1);
         umma::mbar_init(done, 1);
         umma::mbar_init_fence();
     }
@@ -665,48 +701,49 @@ __global__ void __launch_bounds__(128, 1)
 
     if (warp == 0 && lane == 0) {  // producer
         for (int j = 0; j < nslabs; ++j) {
-            const int s = j % S;
-            if (j >= S && !umma::mbar_wait(&empty[s], ((j / S) - 1) & 1, err)) {
+            const int st = j % S;
+            if (j >= S && !umma::mbar_wait(&empty[st], ((j / S) - 1) & 1, err)) {
                 atomicExch(err, 1);
                 break;
             }
-            uint8_t* st = smem + s * stage_bytes;
-            umma::mbar_expect_tx(&full[s], stage_bytes);
+            uint8_t* sp = smem + st * OZ_STAGE_BYTES;
+            umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
+            const size_t js = (size_t)j * umma::I8_SLAB_BYTES;
             for (int a = 0; a < OZ_SLICES; ++a)
-                umma::bulk_g2s(st + a * umma::I8_SLAB_BYTES, Ab + a * Aplane + (size_t)j * umma::I8_SLAB_BYTES,
-                               umma::I8_SLAB_BYTES, &full[s]);
+                umma::bulk_g2s(sp + a * umma::I8_SLAB_BYTES, Ab + a * Aplane + js, umma::I8_SLAB_BYTES, &full[st]);
             for (int b = 0; b < OZ_SLICES; ++b)
-                umma::bulk_g2s(st + (OZ_SLICES + b) * umma::I8_SLAB_BYTES,
-                               Bb + b * Bplane + (size_t)j * umma::I8_SLAB_BYTES, umma::I8_SLAB_BYTES, &full[s]);
+                for (int kg = 0; kg < 4; ++kg)
+                    umma::bulk_g2s(sp + OZ_A_BYTES + b * OZ_B_SLICE + kg * 1024,
+                                   Bb + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
         }
     } else if (warp == 1 && lane == 0) {  // MMA issuer
-        const uint32_t idesc = umma::instr_desc_s8(128, 128);
+        const uint32_t idesc = umma::instr_desc_s8(128, OZ_NT);
         bool issued = false;
         for (int j = 0; j < nslabs; ++j) {
-            const int s = j % S;
-            if (!umma::mbar_wait(&full[s], (j / S) & 1, err)) {
+            const int st = j % S;
+            if (!umma::mbar_wait(&full[st], (j / S) & 1, err)) {
                 atomicExch(err, 2);
                 break;
             }
             umma::fence_after_sync();
-            const uint32_t st = umma::smem_u32(smem + s * stage_bytes);
+            const uint32_t sp = umma::smem_u32(smem + st * OZ_STAGE_BYTES);
 #pragma unroll
             for (int kk = 0; kk < 2; ++kk) {
 #pragma unroll
                 for (int t = 0; t < 10; ++t) {
                     const int i = kOzA[t], jj = kOzB[t];
-                    const uint32_t acc = tmem + (uint32_t)(i + jj - 2) * 128;
+                    const uint32_t acc = tmem + (uint32_t)(i + jj - 2) * OZ_NT;
                     const uint64_t ad =
-                        umma::smem_desc(st + (i - 1) * umma::I8_SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
-                    const uint64_t bd = umma::smem_desc(st + (OZ_SLICES + jj - 1) * umma::I8_SLAB_BYTES + kk * 4096,
-                                                        umma::LBO, umma::SBO);
+                        umma::smem_desc(sp + (i - 1) * umma::I8_SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
+                    const uint64_t bd =
+                        umma::smem_desc(sp + OZ_A_BYTES + (jj - 1) * OZ_B_SLICE + kk * 2048, 1024, umma::SBO);
                     // the first product of each order starts its accumulator
                     const bool first = (j == 0 && kk == 0 && (t == 0 || t == 1 || t == 3 || t == 6));
                     umma::mma_s8(acc, ad, bd, idesc, first ? 0u : 1u);
                 }
             }
             issued = true;
-            umma::mma_commit(&empty[s]);
+            umma::mma_commit(&empty[st]);
         }
         if (issued) umma::mma_commit(done);
         else umma::mbar_expect_tx(done, 0);
@@ -728,13 +765,13 @@ __global__ void __launch_bounds__(128, 1)
             const size_t plane = (size_t)m.nbp * BLOCK_PTS;
             const int ep = e_pt[row];
             double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-            for (int c0 = 0; c0 < 128; c0 += 16) {
+            for (int c0 = 0; c0 < OZ_NT; c0 += 16) {
                 // issue all operand loads of these 16 columns first (predicated), then use them
                 double f0[16], f1[16], f2[16], f3[16];
                 int ec[16];
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
-                    const int mu = nt * 128 + c0 + c;
+                    const int mu = nt * OZ_NT + c0 + c;
                     const bool live = mu < m.nb;
                     const size_t o = (size_t)mu * BLOCK_PTS + row;
                     f0[c] = live ? phi[o] : 0.0;
@@ -747,15 +784,15 @@ __global__ void __launch_bounds__(128, 1)
                 }
                 uint32_t d2[16], d3[16], d4[16], d5[16];
                 umma::tmem_ld16_raw(taddr + c0, d2);
-                umma::tmem_ld16_raw(taddr + 128 + c0, d3);
-                umma::tmem_ld16_raw(taddr + 256 + c0, d4);
-                umma::tmem_ld16_raw(taddr + 384 + c0, d5);
+                umma::tmem_ld16_raw(taddr + OZ_NT + c0, d3);
+                umma::tmem_ld16_raw(taddr + 2 * OZ_NT + c0, d4);
+                umma::tmem_ld16_raw(taddr + 3 * OZ_NT + c0, d5);
                 umma::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
-                    const double s = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
-                                     (double)(int)d5[c] * w5;
-                    const double x = ldexp(s, ep + ec[c]);
+                    const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
+                                      (double)(int)d5[c] * w5;
+                    const double x = ldexp(sx, ep + ec[c]);
                     r += f0[c] * x;
                     if (GGA) {
                         gx += f1[c] * x;
@@ -771,25 +808,25 @@ __global__ void __launch_bounds__(128, 1)
             const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi);
             const int* e_z = reinterpret_cast<const int*>(base + L.e_z);
             const int* aos = g.blk_aos + m.ao0;
-            double* tile = reinterpret_cast<double*>(smem);  // [128][17]
+            double* tile = reinterpret_cast<double*>(smem);  // [128][17], over the drained operand ring
             const int mu_r = mt * 128 + row;
             const int em = e_phi[mu_r];
-            for (int c0 = 0; c0 < 128; c0 += 16) {
+            for (int c0 = 0; c0 < OZ_NT; c0 += 16) {
                 uint32_t d2[16], d3[16], d4[16], d5[16];
                 umma::tmem_ld16_raw(taddr + c0, d2);
-                umma::tmem_ld16_raw(taddr + 128 + c0, d3);
-                umma::tmem_ld16_raw(taddr + 256 + c0, d4);
-                umma::tmem_ld16_raw(taddr + 384 + c0, d5);
+                umma::tmem_ld16_raw(taddr + OZ_NT + c0, d3);
+                umma::tmem_ld16_raw(taddr + 2 * OZ_NT + c0, d4);
+                umma::tmem_ld16_raw(taddr + 3 * OZ_NT + c0, d5);
                 umma::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
-                    const double s = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
-                                     (double)(int)d5[c] * w5;
-                    tile[row * 17 + c] = ldexp(s, em + e_z[nt * 128 + c0 + c]);
+                    const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
+                                      (double)(int)d5[c] * w5;
+                    tile[row * 17 + c] = ldexp(sx, em + e_z[nt * OZ_NT + c0 + c]);
                 }
                 __syncthreads();
                 const int c = threadIdx.x & 15;
-                const int nu = nt * 128 + c0 + c;
+                const int nu = nt * OZ_NT + c0 + c;
                 if (nu < m.nb) {
                     const int anu = aos[nu];
                     for (int rr = threadIdx.x >> 4; rr < 128; rr += 8) {
@@ -803,12 +840,12 @@ __global__ void __launch_bounds__(128, 1)
     }
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, 512);
+    if (warp == 0) umma::tmem_dealloc(tmem, OZ_TMEM_COLS);
 }
 
 }  // namespace
 
-size_t oz_smem_bytes() { return (size_t)3 * 2 * OZ_SLICES * umma::I8_SLAB_BYTES + 7 * 8 + 16; }
+size_t oz_smem_bytes() { return (size_t)OZ_STAGES * OZ_STAGE_BYTES + (2 * OZ_STAGES + 1) * 8 + 16; }
 
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
     // the FP64 path's AO values and gradients (the slices are cut from them), then the row scales
@@ -823,12 +860,12 @@ void oz_rho(const MixedArgs& a, cudaStream_t s) {
     const size_t smem = oz_smem_bytes();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<dim3(tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, tiles, a.rho_acc,
-                                                                   a.Vacc, a.nao);
+        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, 2 * tiles,
+                                                                       a.rho_acc, a.Vacc, a.nao);
     } else {
         cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<dim3(tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, tiles, a.rho_acc,
-                                                                    a.Vacc, a.nao);
+        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, 2 * tiles,
+                                                                        a.rho_acc, a.Vacc, a.nao);
     }
 }
 
@@ -836,11 +873,11 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
     if (functional_is_gga(a.fn)) {
         k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                               a.rho_store, a.coef, a.blk_sum);
-        k_pack_z_oz<true><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+        k_pack_z_oz<true><<<a.nblk, 128, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
     } else {
         k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                                a.rho_store, a.coef, a.blk_sum);
-        k_pack_z_oz<false><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+        k_pack_z_oz<false><<<a.nblk, 128, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
     }
 }
 
@@ -848,8 +885,9 @@ void oz_vxc(const MixedArgs& a, cudaStream_t s) {
     const int tiles = a.max_nbp / umma::TILE_ROWS;
     const size_t smem = oz_smem_bytes();
     cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_oz<MODE_VXC, false><<<dim3(tiles * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, tiles, a.rho_acc,
-                                                                        a.Vacc, a.nao);
+    // M tiles of 128 AOs x N tiles of 64 AOs
+    k_oz<MODE_VXC, false><<<dim3(tiles * 2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, 2 * tiles,
+                                                                            a.rho_acc, a.Vacc, a.nao);
 }
 
 size_t umma_smem_bytes(int nterms) {
