@@ -12,7 +12,8 @@ one closed-shell Vxc build (rho pass + Vxc pass) of the whole grid.
 
 With --precision both (default) the same grid is built with the FP64 drop-in and
 the mixed path (INT8 fixed-point slices on the tensor cores by default); the
-headline value is the mixed path, the line carries the FP64 numbers, the
+headline value is the FP64 drop-in (the plain FP64 path is the configuration the
+metric is quoted on), the line carries the mixed path's numbers, the
 mixed-vs-FP64 speed-up and |dExc| / max|dVxc| between them.
 
 Under torchrun (N > 1) every rank builds its own chain (seed + rank): the units
@@ -252,7 +253,7 @@ def main():
             torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         return float(t.item())
 
-    precisions = ["fp64", "mixed"] if args.precision == "both" else [args.precision]
+    precisions = ["mixed", "fp64"] if args.precision == "both" else [args.precision]
     engines = {p: XcEngine(device=local, precision=p, split_terms=args.split_terms) for p in precisions}
     for e in engines.values():
         e.set_system(sh)
@@ -327,7 +328,9 @@ def main():
                 "clocks": clk_summary}
         if "fp64" in res and "mixed" in res:
             f, m = res["fp64"], res["mixed"]
-            line["fp64"] = {"value": f["value"], "ms_per_step": f["ms"], "exc": f["exc"], "roofline": rooflines["fp64"]}
+            line["mixed"] = {"value": m["value"], "ms_per_step": m["ms"], "exc": m["exc"], "dtype": (
+                "int8 fixed-point slices/i32/f64" if args.split_terms == 10 else "bf16 split/f32/f64"),
+                "roofline": rooflines["mixed"]}
             line["mixed_vs_fp64"] = {"speedup": f["ms"] / m["ms"], "abs_dexc": abs(m["exc"] - f["exc"]),
                                      "max_abs_dvxc": float(np.abs(m["V"] - f["V"]).max()),
                                      "abs_dnelec_alpha": abs(m["nel"] - f["nel"])}
@@ -427,6 +430,18 @@ def run_large(args):
     print(json.dumps(line), flush=True)
 
 
+def measured_traffic(kernel):
+    """DRAM bytes per build of an FP64 contraction kernel from the committed ncu summary
+    (profiles/traffic_fp64_contractions_chain100_b3lyp_ultrafine.md), for the default workload."""
+    import re
+    try:
+        txt = open(os.path.join(ROOT, "profiles", "traffic_fp64_contractions_chain100_b3lyp_ultrafine.md")).read()
+    except OSError:
+        return None
+    mt = re.search(r"traffic_bytes_per_build k_" + kernel + r" = (\d+)", txt)
+    return int(mt.group(1)) if mt else None
+
+
 def roofline(args, torch, peaks, r, precision):
     """Dominant contraction kernel of one build: algorithmic FLOPs (2 nb^2 np per block per
     contraction) over its CUDA-event time, against the measured peak of the unit it runs on."""
@@ -445,8 +460,13 @@ def roofline(args, torch, peaks, r, precision):
     else:
         peak = peaks.get("bf16_tflops", 1590.0)
         note = "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1.59 PFLOP/s"
+    default = (args.natoms == 100 and args.grid == "ULTRA_FINE" and args.functional == "B3LYP" and args.nocc == 380
+               and args.seed == 1)
+    traffic = measured_traffic(top.replace("_ms", "")) if (precision == "fp64" and default) else None
     return {"bound": "tensor", "kernel": top.replace("_ms", ""), "achieved": achieved, "peak": peak,
-            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+            "unit": "TFLOP/s", "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+            "traffic_note": ("DRAM bytes of the kernel's launches in one build, one ncu capture "
+                             "(profiles/traffic_fp64_contractions_chain100_b3lyp_ultrafine.md)") if traffic else None,
             "peak_source": note, "flops_per_launch_set": flops, "stage_ms": per}
 
 
