@@ -110,7 +110,7 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // blockIdx.z = z (the build: one plane, phi -> X after the phi planes; the gradient:
 // phi and its three derivatives -> X and Y_x, Y_y, Y_z).
 constexpr int GX_BM = 64, GX_BK = 16, GX_AS = GX_BK + 2, GX_BS = BLOCK_PTS + 4;
-__global__ void __launch_bounds__(256) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
+__global__ void __launch_bounds__(256, 2) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
                                                 int blk0, char* ws, int src0, int dst0) {
     const int blk = blk0 + blockIdx.y;
     const BlockMeta m = g.meta[blk];
