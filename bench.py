@@ -413,8 +413,13 @@ def run_large(args):
             ms.append(eng.last_profile()["total_ms"])
         exc = float(np.sum(r[0])) if args.workload == "batch64" else float(r[0])
         st = eng.grid_stats()
+        eng.set_profiling(True)  # one more build, stage by stage, for the stage times (not timed above)
+        build()
+        prof = eng.last_profile()
+        eng.set_profiling(False)
         out[prec] = {"ms_per_step": float(np.mean(ms)), "value": npts / (np.mean(ms) * 1e-3), "exc": exc,
-                     "blocks": st["nblocks"], "mean_screened_aos": st["mean_nb"], "set_grid_s": t_grid}
+                     "blocks": st["nblocks"], "mean_screened_aos": st["mean_nb"], "set_grid_s": t_grid,
+                     "stage_ms": {k: prof[k] for k in ("ao_ms", "gemm_x_ms", "rho_ms", "gemm_v_ms", "finish_ms")}}
         eng.close()
     head = out.get("mixed", out.get("fp64"))
     line = {"metric": METRIC, "unit": UNIT, "value": head["value"], "ms_per_step": head["ms_per_step"],

@@ -59,7 +59,8 @@ typedef struct {
     double ao_cutoff;    /* drop a shell from a block when its value/gradient bound is below (default 1e-14) */
     double rho_cutoff;   /* xc-density-threshold: points with rho_A <= it are skipped (default 1e-16) */
     size_t workspace_bytes; /* device workspace budget for block intermediates (0 = default 4 GiB) */
-    int split_terms;     /* mixed path: 3 (hi*hi + hi*mid + mid*hi) or 6 (three-way split, default) */
+    int split_terms;     /* mixed path: INT8 digit products kept, 3, 6 or 10 (default 10: four radix-254
+                            digits per operand, every product i + j <= 5, about 31 bits) */
 } pdfxc_options;
 
 typedef struct pdfxc_ctx pdfxc_ctx;

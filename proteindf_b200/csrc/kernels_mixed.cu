@@ -444,9 +444,12 @@ __device__ __forceinline__ double oz_weight(int k) {  // weight of order k = i +
     return w;
 }
 
-// exponent e with |v| < 2^e for every |v| <= m (0 for m = 0)
+// exponent e with |v| < 2^e for every |v| <= m; an all-zero row gets kOzZeroExp, below every
+// double's exponent, so that a group maximum over row exponents ignores it (its digits are 0
+// and ldexp of a zero sum stays 0)
+constexpr int kOzZeroExp = -1100;
 __device__ __forceinline__ int oz_exponent(double m) {
-    int e = 0;
+    int e = kOzZeroExp;
     if (m > 0.0) frexp(m, &e);
     return e;
 }
@@ -475,6 +478,34 @@ __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off,
     for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = *reinterpret_cast<uint4*>(s[i]);
 }
 
+// Digits of the rows of an FP64 [nbp][128] plane of block `blk` with its group's row
+// exponents: the maximum over the group's blocks of their own row exponents (int array at
+// offset e_blk of each block's region); the group's first block also stores them at e_grp.
+// A warp takes 8 rows x 64 points (lane = row r, K group kg), so each digit store
+// instruction writes four whole 128-byte core matrices.
+__device__ void oz_slice_rows_group(const GridView& g, int blk, const BlockMeta& m, const OzLayout& L, char* ws,
+                                    size_t src, size_t e_blk, size_t e_grp, size_t dst) {
+    char* base = ws + m.ws;
+    const double* v = reinterpret_cast<const double*>(base + src);
+    auto group_exp = [&](int mu) {
+        int e = kOzZeroExp;
+        for (int i = 0; i < m.gn; ++i)
+            e = max(e, reinterpret_cast<const int*>(ws + g.meta[m.lead + i].ws + e_blk)[mu]);
+        return e;
+    };
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane & 7, kg = lane >> 3;
+    double x[16];
+    for (int t = warp; t < (m.nbp / 8) * 2; t += blockDim.x / 32) {
+        const int mu = (t >> 1) * 8 + r, p0 = (t & 1) * 64 + kg * 16;
+        const int e = group_exp(mu);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) x[j] = mu < m.nb ? v[(size_t)mu * BLOCK_PTS + p0 + j] : 0.0;
+        oz_store16(base + dst, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), x, e);
+    }
+    if (blk == m.lead)
+        for (int mu = threadIdx.x; mu < m.nbp; mu += blockDim.x) reinterpret_cast<int*>(base + e_grp)[mu] = group_exp(mu);
+}
+
 // Row scales of phi^T (per point, max over the block's AOs) and of phi (per AO row, max
 // over the points), from the FP64 AO values. One CTA per block: warps take AO rows
 // (lane = 4 points each), every thread also keeps the running maximum of its point.
@@ -499,7 +530,8 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_oz_scales(GridView g, int blk0, c
     }
 }
 
-// Slices of phi^T (rows = points) and phi (rows = AOs).
+// Slices of phi^T (rows = points, per-point exponents) and phi (rows = AOs, the group's
+// per-AO exponents: the Vxc contraction runs over the whole group's points).
 __global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* ws) {
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
@@ -507,7 +539,6 @@ __global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* w
     char* base = ws + m.ws;
     const double* phi = reinterpret_cast<const double*>(base + L.phi64);
     const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
-    const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi);
     double v[16];
     const int g1 = m.nbp / 16;
     for (int e = threadIdx.x; e < BLOCK_PTS * g1; e += blockDim.x) {  // phi^T: row p, 16 AOs
@@ -516,15 +547,7 @@ __global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* w
         for (int j = 0; j < 16; ++j) v[j] = mu0 + j < m.nb ? phi[(size_t)(mu0 + j) * BLOCK_PTS + p] : 0.0;
         oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
     }
-    // phi: a warp takes 8 rows x 64 points (lane = row r, K group kg), so each digit store
-    // instruction writes four whole 128-byte core matrices
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane & 7, kg = lane >> 3;
-    for (int t = warp; t < (m.nbp / 8) * 2; t += blockDim.x / 32) {
-        const int mu = (t >> 1) * 8 + r, p0 = (t & 1) * 64 + kg * 16;
-#pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = mu < m.nb ? phi[(size_t)mu * BLOCK_PTS + p0 + j] : 0.0;
-        oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), v, e_phi[mu]);
-    }
+    oz_slice_rows_group(g, blk, m, L, ws, L.phi64, L.e_phi, L.e_phi_g, L.phi2);
 }
 
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -533,12 +556,12 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
-// P_sub digits. Phase 1: the row exponents, a warp per row mu gathering P[aos[mu]][aos[nu]]
+// P_sub digits of a group. Phase 1: the row exponents, a warp per row mu gathering P[aos[mu]][aos[nu]]
 // from the L2-resident P. Phase 2: a warp takes 8 rows x 64 columns (lane = row r, K group
 // kg: 16 columns), so each digit store instruction writes four whole 128-byte core matrices.
-__global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __restrict__ P, int nao, int blk0,
-                                                   char* ws) {
-    const int blk = blk0 + blockIdx.x;
+__global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __restrict__ P, int nao,
+                                                   const int* __restrict__ grp, char* ws) {
+    const int blk = grp[blockIdx.x];  // one CTA per group: P_sub lives in the first block's region
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
     char* base = ws + m.ws;
@@ -571,65 +594,62 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
     }
 }
 
-// Z digits (Z[nu][p] = 0.5 w vrho phi + c . grad phi). A warp takes 8 rows: it forms their
-// Z values once (lanes along the points), takes each row's exponent, then cuts digits from a
-// shared-memory copy with lane = row r, K group kg, so each digit store instruction writes
-// four whole 128-byte core matrices.
+// Z[nu][p] = 0.5 w vrho phi + c . grad phi in FP64 over plane 0 of the block's AO planes
+// (phi is not read again after the rho contraction), and the block's row exponents of Z.
+// A warp per row, lanes along the points; each element is read and rewritten by one thread.
 template <bool GGA>
-__global__ void __launch_bounds__(128) k_pack_z_oz(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
+__global__ void __launch_bounds__(256) k_z_oz(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
     char* base = ws + m.ws;
-    const double* phi = reinterpret_cast<const double*>(base + L.phi64);
+    double* phi = reinterpret_cast<double*>(base + L.phi64);
     int* e_z = reinterpret_cast<int*>(base + L.e_z);
     const size_t plane = (size_t)m.nbp * BLOCK_PTS;
     __shared__ double cf[4][BLOCK_PTS];
-    __shared__ double zt[4][8][BLOCK_PTS + 2];  // per warp: 8 rows of Z
-    __shared__ int ez[4][8];
     for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
         cf[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
     __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane & 7, kg = lane >> 3;
-    double v[16];
-    for (int nu0 = warp * 8; nu0 < m.nbp; nu0 += 32) {
-        for (int q = 0; q < 8; ++q) {
-            const int nu = nu0 + q;
-            double mx = 0.0;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    for (int nu = warp; nu < m.nbp; nu += blockDim.x / 32) {
+        double mx = 0.0;
+        if (nu < m.nb) {
+            double z[4];
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 const int p = lane + 32 * j;
                 const size_t o = (size_t)nu * BLOCK_PTS + p;
-                double z = 0.0;
-                if (nu < m.nb) {
-                    z = cf[0][p] * phi[o];
-                    if (GGA) z += cf[1][p] * phi[plane + o] + cf[2][p] * phi[2 * plane + o] + cf[3][p] * phi[3 * plane + o];
-                }
-                zt[warp][q][p] = z;
-                mx = fmax(mx, fabs(z));
+                z[j] = cf[0][p] * phi[o];
+                if (GGA) z[j] += cf[1][p] * phi[plane + o] + cf[2][p] * phi[2 * plane + o] + cf[3][p] * phi[3 * plane + o];
             }
-            mx = warp_max_d(mx);
-            if (lane == 0) ez[warp][q] = oz_exponent(mx), e_z[nu] = oz_exponent(mx);
-        }
-        __syncwarp();
-        for (int slab = 0; slab < 2; ++slab) {
-            const int p0 = slab * 64 + kg * 16;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = zt[warp][r][p0 + j];
-            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, p0, BLOCK_PTS), v, ez[warp][r]);
+            for (int j = 0; j < 4; ++j) {
+                phi[(size_t)nu * BLOCK_PTS + lane + 32 * j] = z[j];
+                mx = fmax(mx, fabs(z[j]));
+            }
         }
-        __syncwarp();
+        mx = warp_max_d(mx);
+        if (lane == 0) e_z[nu] = oz_exponent(mx);
     }
+}
+
+// Z digits (rows = AOs, K = points) with the group's row exponents.
+__global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp);
+    oz_slice_rows_group(g, blk, m, L, ws, L.phi64, L.e_z, L.e_z_g, L.zpack);
 }
 
 // Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
 __constant__ int kOzA[10] = {1, 1, 2, 1, 2, 3, 1, 2, 3, 4};
 __constant__ int kOzB[10] = {1, 2, 1, 3, 2, 1, 4, 3, 2, 1};
 
-// One CTA per (block, 128-row M tile, 64-row N tile): RHO computes X^T = phi^T P_sub
-// (M = 128 points, N = 64 AOs mu, K = nbp AOs nu) with the rho / grad rho epilogue;
-// VXC computes V = phi Z^T (M = 128 AOs mu, N = 64 AOs nu, K = 128 points) with the
-// FP64 atomic epilogue. Four int32 accumulators of 64 columns (256 TMEM columns) and a
+// RHO: one CTA per (block, 64-row N tile) computes X^T = phi^T P_sub (M = 128 points,
+// N = 64 AOs mu, K = nbp AOs nu, P_sub of the block's group) with the rho / grad rho
+// epilogue. VXC: one CTA per (group, 128-row M tile, 64-row N tile) computes W = phi Z^T
+// (M = 128 AOs mu, N = 64 AOs nu, K = all points of the group's blocks, 128 per block)
+// with the FP64 atomic epilogue. Four int32 accumulators of 64 columns (256 TMEM columns) and a
 // two-stage operand ring of 48 KiB let two CTAs share an SM, so one CTA's epilogue
 // overlaps the other's loads and MMAs. A stage holds the A tile's four digit planes
 // (128 rows x 64 K, canonical no-swizzle K-major layout, 8 KiB each) and the B tile's
@@ -644,10 +664,11 @@ constexpr uint32_t OZ_TMEM_COLS = 4 * OZ_NT;                      // one accumul
 
 template <int MODE, bool GGA>
 __global__ void __launch_bounds__(128, 2)
-    k_oz(GridView g, int blk0, char* ws, int* err, int tiles_max, double* rho_acc, double* Vacc, int nao) {
+    k_oz(GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int tiles_max, double* rho_acc,
+         double* Vacc, int nao) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int S = OZ_STAGES;
-    const int blk = blk0 + blockIdx.y;
+    const int blk = MODE == MODE_RHO ? blk0 + (int)blockIdx.y : grp[blockIdx.y];  // VXC: the group's first block
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp);
     const int ntiles = m.nbp / umma::TILE_ROWS;  // 128-row tiles of this block
@@ -669,21 +690,24 @@ __global__ void __launch_bounds__(128, 2)
     uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
 
     const char* base = ws + m.ws;
-    const char *Ab, *Bb;
-    size_t Aplane, Bplane;
+    const char* lead = ws + g.meta[m.lead].ws;  // the group's first block: P_sub, group exponents
+    // operand tiles: byte offsets inside a block's region (RHO: A in this block's, B in the
+    // group's first block's; VXC: both in the region of the block that slab j belongs to)
+    size_t Ao, Bo, Aplane, Bplane;
     int nslabs;
+    constexpr int kBlockSlabs = BLOCK_PTS / (int)umma::I8_SLAB_K;  // VXC: K slabs per block
     if (MODE == MODE_RHO) {
-        Ab = base + L.phi1;
+        Ao = L.phi1;
         Aplane = L.phi1_plane;
-        Bb = base + L.ppack + (size_t)(nt / 2) * umma::TILE_ROWS * m.nbp;
+        Bo = L.ppack + (size_t)(nt / 2) * umma::TILE_ROWS * m.nbp;
         Bplane = L.ppack_plane;
         nslabs = m.nbp / (int)umma::I8_SLAB_K;
     } else {
-        Ab = base + L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS;
+        Ao = L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS;
         Aplane = L.phi2_plane;
-        Bb = base + L.zpack + (size_t)(nt / 2) * umma::TILE_ROWS * BLOCK_PTS;
+        Bo = L.zpack + (size_t)(nt / 2) * umma::TILE_ROWS * BLOCK_PTS;
         Bplane = L.zpack_plane;
-        nslabs = BLOCK_PTS / (int)umma::I8_SLAB_K;
+        nslabs = m.gn * kBlockSlabs;
     }
     const size_t bhalf = (size_t)(nt & 1) * 8 * 128;  // row groups 8..15 of the 128-row tile
 
@@ -708,13 +732,19 @@ __global__ void __launch_bounds__(128, 2)
             }
             uint8_t* sp = smem + st * OZ_STAGE_BYTES;
             umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
-            const size_t js = (size_t)j * umma::I8_SLAB_BYTES;
+            const char *As = base + Ao, *Bs = lead + Bo;
+            size_t js = (size_t)j * umma::I8_SLAB_BYTES;
+            if (MODE == MODE_VXC) {  // slab j: block lead + j / kBlockSlabs, its slab j % kBlockSlabs
+                const char* bj = ws + g.meta[m.lead + j / kBlockSlabs].ws;
+                As = bj + Ao, Bs = bj + Bo;
+                js = (size_t)(j % kBlockSlabs) * umma::I8_SLAB_BYTES;
+            }
             for (int a = 0; a < OZ_SLICES; ++a)
-                umma::bulk_g2s(sp + a * umma::I8_SLAB_BYTES, Ab + a * Aplane + js, umma::I8_SLAB_BYTES, &full[st]);
+                umma::bulk_g2s(sp + a * umma::I8_SLAB_BYTES, As + a * Aplane + js, umma::I8_SLAB_BYTES, &full[st]);
             for (int b = 0; b < OZ_SLICES; ++b)
                 for (int kg = 0; kg < 4; ++kg)
                     umma::bulk_g2s(sp + OZ_A_BYTES + b * OZ_B_SLICE + kg * 1024,
-                                   Bb + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
+                                   Bs + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
         }
     } else if (warp == 1 && lane == 0) {  // MMA issuer
         const uint32_t idesc = umma::instr_desc_s8(128, OZ_NT);
@@ -761,7 +791,7 @@ __global__ void __launch_bounds__(128, 2)
         if (MODE == MODE_RHO) {
             const double* phi = reinterpret_cast<const double*>(base + L.phi64);
             const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
-            const int* e_p = reinterpret_cast<const int*>(base + L.e_p);
+            const int* e_p = reinterpret_cast<const int*>(lead + L.e_p);
             const size_t plane = (size_t)m.nbp * BLOCK_PTS;
             const int ep = e_pt[row];
             double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
@@ -805,8 +835,8 @@ __global__ void __launch_bounds__(128, 2)
             atomicAdd(acc, r);
             if (GGA) atomicAdd(acc + 1, gx), atomicAdd(acc + 2, gy), atomicAdd(acc + 3, gz);
         } else {
-            const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi);
-            const int* e_z = reinterpret_cast<const int*>(base + L.e_z);
+            const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi_g);
+            const int* e_z = reinterpret_cast<const int*>(base + L.e_z_g);
             const int* aos = g.blk_aos + m.ao0;
             double* tile = reinterpret_cast<double*>(smem);  // [128][17], over the drained operand ring
             const int mu_r = mt * 128 + row;
@@ -852,7 +882,7 @@ void oz_prepare(const MixedArgs& a, cudaStream_t s) {
     launch_ao_eval(a.b, a.g, a.blk0, a.nblk, functional_is_gga(a.fn), a.ws, 0, s);
     k_oz_scales<<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.ws);
     k_slice_phi<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
-    k_pack_p_oz<<<a.nblk, 256, 0, s>>>(a.g, a.P, a.nao, a.blk0, a.ws);
+    k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.P, a.nao, a.grp, a.ws);
 }
 
 void oz_rho(const MixedArgs& a, cudaStream_t s) {
@@ -860,11 +890,11 @@ void oz_rho(const MixedArgs& a, cudaStream_t s) {
     const size_t smem = oz_smem_bytes();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, 2 * tiles,
+        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.grp, a.ws, a.err, 2 * tiles,
                                                                        a.rho_acc, a.Vacc, a.nao);
     } else {
         cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, 2 * tiles,
+        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.grp, a.ws, a.err, 2 * tiles,
                                                                         a.rho_acc, a.Vacc, a.nao);
     }
 }
@@ -873,11 +903,13 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
     if (functional_is_gga(a.fn)) {
         k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                               a.rho_store, a.coef, a.blk_sum);
-        k_pack_z_oz<true><<<a.nblk, 128, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+        k_z_oz<true><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+        k_pack_z_oz<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
     } else {
         k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                                a.rho_store, a.coef, a.blk_sum);
-        k_pack_z_oz<false><<<a.nblk, 128, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+        k_z_oz<false><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
+        k_pack_z_oz<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
     }
 }
 
@@ -885,8 +917,8 @@ void oz_vxc(const MixedArgs& a, cudaStream_t s) {
     const int tiles = a.max_nbp / umma::TILE_ROWS;
     const size_t smem = oz_smem_bytes();
     cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // M tiles of 128 AOs x N tiles of 64 AOs
-    k_oz<MODE_VXC, false><<<dim3(tiles * 2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.ws, a.err, 2 * tiles,
+    // per group: M tiles of 128 AOs x N tiles of 64 AOs
+    k_oz<MODE_VXC, false><<<dim3(tiles * 2 * tiles, a.ngrp), 128, smem, s>>>(a.g, a.blk0, a.grp, a.ws, a.err, 2 * tiles,
                                                                             a.rho_acc, a.Vacc, a.nao);
 }
 

@@ -97,7 +97,8 @@ __global__ void k_noalloc_chunk(const double* xyzw, int64_t npts, int64_t p0, in
         pw[e] = i < npts ? xyzw[4 * src + 3] : 0.0;
         if (j == 0) {
             const int64_t left = npts - first;
-            meta[b] = BlockMeta{0, nshell, 0, nao, nbp, (int)(left < BLOCK_PTS ? left : BLOCK_PTS), (int64_t)b * ws_block};
+            meta[b] = BlockMeta{0, nshell, 0, nao, nbp, (int)(left < BLOCK_PTS ? left : BLOCK_PTS), (int)b, 1,
+                                (int64_t)b * ws_block};
         }
     }
 }

@@ -191,8 +191,9 @@ void free_grid(pdfxc_ctx* c) {
     drop_graph(c);
     dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
     dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
-    dev_free(c->d_seg_blk), dev_free(c->d_mol_sums);
+    dev_free(c->d_seg_blk), dev_free(c->d_mol_sums), dev_free(c->d_grp);
     c->seg_blk.clear();
+    c->h_grp.clear();
     dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum), dev_free(c->d_rho_acc);
     if (c->d_ws) cudaFree(c->d_ws);
     c->d_ws = nullptr;
@@ -219,7 +220,7 @@ void pdfxc_default_options(pdfxc_options* opt) {
     opt->ao_cutoff = 1e-14;
     opt->rho_cutoff = 1e-16;
     opt->workspace_bytes = 0;
-    opt->split_terms = 6;
+    opt->split_terms = 10;
 }
 
 pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt) {
@@ -231,7 +232,7 @@ pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt)
     if (opt) c->opt = *opt;
     if (c->opt.block_points <= 0 || c->opt.block_points > BLOCK_PTS) c->opt.block_points = BLOCK_PTS;
     if (c->opt.workspace_bytes == 0) c->opt.workspace_bytes = size_t(4) << 30;
-    if (c->opt.split_terms != 3 && c->opt.split_terms != 6 && c->opt.split_terms != 10) c->opt.split_terms = 6;
+    if (c->opt.split_terms != 3 && c->opt.split_terms != 6 && c->opt.split_terms != 10) c->opt.split_terms = 10;
     if (c->opt.precision != PDFXC_PRECISION_FP64 && c->opt.precision != PDFXC_PRECISION_MIXED) {
         delete c;
         return PDFXC_ERR_ARG;
@@ -320,22 +321,35 @@ struct GridSegment {
     int sh0, sh1;
 };
 
-// Spatial blocks and per-block basis screening, once per geometry: within each
-// segment the points are put in Morton order over the segment's bounding box and
-// cut into blocks of block_points; every block keeps the shells of its segment whose
-// value/gradient envelope reaches ao_cutoff at the block's nearest point.
+// Blocks of one group on the INT8 path: the Vxc contraction of a group runs over all its
+// points before one epilogue, and the group's blocks share one screened basis. Shell
+// screening radii, not the point count, set a block's basis, so a group of four blocks
+// screens in about as many AOs as one block: on a 100-atom chain (cc-pVDZ, 99 x 590 grid)
+// groups of 4 x 128 points raise the contraction work by 18 % and cut the per-block
+// epilogue work (sum of nb^2) by 3.4x.
+int group_blocks(const pdfxc_ctx* ctx) {
+    return ctx->opt.precision == PDFXC_PRECISION_MIXED && ctx->opt.split_terms == 10 ? 4 : 1;
+}
+
+// Spatial blocks and basis screening, once per geometry: within each segment the points
+// are put in Morton order over the segment's bounding box and cut into groups of up to
+// group_blocks x block_points consecutive points, each group into blocks of block_points;
+// every group keeps the shells of its segment whose value/gradient envelope reaches
+// ao_cutoff at the group's nearest point.
 void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom,
                 const std::vector<GridSegment>& segs) {
     free_grid(ctx);
     const int bp = ctx->opt.block_points;
-    // 1. spatial order: Morton code over each segment's bounding box; a block takes up to
-    // block_points consecutive points and is closed early when its bounding-box diagonal would
-    // pass kMaxBlockExtent, so that a block never straddles two distant regions (on sparse outer
+    const int gb = group_blocks(ctx);
+    // 1. spatial order: Morton code over each segment's bounding box; a group takes up to
+    // gb * block_points consecutive points and is closed early when its bounding-box diagonal
+    // would pass kMaxBlockExtent, so that it never straddles two distant regions (on sparse outer
     // grid shells a 128-point run of the Z curve can span 100 bohr and screen in thousands of AOs)
     constexpr double kMaxBlockExtent = 12.0;  // bohr
     std::vector<std::pair<uint64_t, int64_t>> key(npts);
     std::vector<std::pair<int64_t, int64_t>> runs;  // [i0, i1) of key per block
     std::vector<int> blk_seg;
+    std::vector<int> grp_blk(1, 0);  // blocks of group k: [grp_blk[k], grp_blk[k+1])
     ctx->seg_blk.assign(1, 0);
     for (size_t si = 0; si < segs.size(); ++si) {
         const GridSegment& sg = segs[si];
@@ -354,7 +368,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
             const double* r0 = xyzw + 4 * key[i0].second;
             double blo[3] = {r0[0], r0[1], r0[2]}, bhi[3] = {r0[0], r0[1], r0[2]};
             int64_t i1 = i0 + 1;
-            for (; i1 < sg.p1 && i1 - i0 < bp; ++i1) {
+            for (; i1 < sg.p1 && i1 - i0 < (int64_t)gb * bp; ++i1) {
                 const double* r = xyzw + 4 * key[i1].second;
                 double d2 = 0.0;
                 for (int k = 0; k < 3; ++k) {
@@ -364,26 +378,45 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
                 if (d2 > kMaxBlockExtent * kMaxBlockExtent) break;
                 for (int k = 0; k < 3; ++k) blo[k] = std::min(blo[k], r[k]), bhi[k] = std::max(bhi[k], r[k]);
             }
-            runs.push_back({i0, i1});
-            blk_seg.push_back((int)si);
+            for (int64_t j0 = i0; j0 < i1; j0 += bp) {
+                runs.push_back({j0, std::min(i1, j0 + bp)});
+                blk_seg.push_back((int)si);
+            }
+            grp_blk.push_back((int)runs.size());
             i0 = i1;
         }
         ctx->seg_blk.push_back((int)runs.size());
     }
     const int nblk = (int)runs.size();
+    const int ngrp = (int)grp_blk.size() - 1;
     std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
     ctx->h_src.assign(px.size(), -1);
     if (atom) ctx->h_owner.assign(px.size(), 0);
-    std::vector<double> cen(3 * (size_t)nblk), rad(nblk);
+    std::vector<double> cen(3 * (size_t)ngrp), rad(ngrp);
     ctx->h_meta.assign(nblk, BlockMeta{});
-    for (int b = 0; b < nblk; ++b) {
-        {
+    for (int gi = 0; gi < ngrp; ++gi) {
+        // the group's centre and radius (screening)
+        const int64_t g0 = runs[grp_blk[gi]].first, g1 = runs[grp_blk[gi + 1] - 1].second;
+        double gc[3] = {0, 0, 0};
+        for (int64_t i = g0; i < g1; ++i)
+            for (int k = 0; k < 3; ++k) gc[k] += xyzw[4 * key[i].second + k];
+        for (int k = 0; k < 3; ++k) gc[k] /= double(g1 - g0);
+        double gr2 = 0.0;
+        for (int64_t i = g0; i < g1; ++i) {
+            const double* r = xyzw + 4 * key[i].second;
+            gr2 = std::max(gr2, (r[0] - gc[0]) * (r[0] - gc[0]) + (r[1] - gc[1]) * (r[1] - gc[1]) +
+                                    (r[2] - gc[2]) * (r[2] - gc[2]));
+        }
+        for (int k = 0; k < 3; ++k) cen[3 * gi + k] = gc[k];
+        rad[gi] = std::sqrt(gr2);
+    }
+    for (int gi = 0; gi < ngrp; ++gi)
+        for (int b = grp_blk[gi]; b < grp_blk[gi + 1]; ++b) {
             const int64_t i0 = runs[b].first, i1 = runs[b].second;
             double c[3] = {0, 0, 0};
             for (int64_t i = i0; i < i1; ++i)
                 for (int k = 0; k < 3; ++k) c[k] += xyzw[4 * key[i].second + k];
             for (int k = 0; k < 3; ++k) c[k] /= double(i1 - i0);
-            double r2 = 0.0;
             for (int j = 0; j < BLOCK_PTS; ++j) {
                 const size_t slot = (size_t)b * BLOCK_PTS + j;
                 const int64_t i = i0 + j;
@@ -392,17 +425,15 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
                     px[slot] = r[0], py[slot] = r[1], pz[slot] = r[2], pw[slot] = r[3];
                     ctx->h_src[slot] = key[i].second;
                     if (atom) ctx->h_owner[slot] = atom[key[i].second];
-                    r2 = std::max(r2, (r[0] - c[0]) * (r[0] - c[0]) + (r[1] - c[1]) * (r[1] - c[1]) + (r[2] - c[2]) * (r[2] - c[2]));
                 } else {
                     px[slot] = c[0], py[slot] = c[1], pz[slot] = c[2], pw[slot] = 0.0;
                     if (atom) ctx->h_owner[slot] = atom[key[i0].second];  // padding: weight 0
                 }
             }
-            for (int k = 0; k < 3; ++k) cen[3 * b + k] = c[k];
-            rad[b] = std::sqrt(r2);
             ctx->h_meta[b].npts = (int)(i1 - i0);
+            ctx->h_meta[b].lead = grp_blk[gi];
+            ctx->h_meta[b].gn = grp_blk[gi + 1] - grp_blk[gi];
         }
-    }
     // 2. per-shell screening radius, then the per-block shell lists
     std::vector<double> Rs(ctx->nshell);
     for (int sh = 0; sh < ctx->nshell; ++sh)
@@ -412,49 +443,59 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
     double flops = 0.0, sum_nb = 0.0;
-    for (int bb = 0; bb < nblk; ++bb) {
-        BlockMeta& m = ctx->h_meta[bb];
-        const GridSegment& sg = segs[blk_seg[bb]];
-        m.sh0 = (int)shells.size();
-        m.ao0 = (int)aos.size();
+    for (int gi = 0; gi < ngrp; ++gi) {
+        const GridSegment& sg = segs[blk_seg[grp_blk[gi]]];
+        const int sh0 = (int)shells.size(), ao0 = (int)aos.size();
         int row = 0;
         for (int sh = sg.sh0; sh < sg.sh1; ++sh) {
             const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[sh]];
-            const double d = std::sqrt((A[0] - cen[3 * bb]) * (A[0] - cen[3 * bb]) +
-                                       (A[1] - cen[3 * bb + 1]) * (A[1] - cen[3 * bb + 1]) +
-                                       (A[2] - cen[3 * bb + 2]) * (A[2] - cen[3 * bb + 2]));
-            if (d - rad[bb] > Rs[sh]) continue;
+            const double d = std::sqrt((A[0] - cen[3 * gi]) * (A[0] - cen[3 * gi]) +
+                                       (A[1] - cen[3 * gi + 1]) * (A[1] - cen[3 * gi + 1]) +
+                                       (A[2] - cen[3 * gi + 2]) * (A[2] - cen[3 * gi + 2]));
+            if (d - rad[gi] > Rs[sh]) continue;
             shells.push_back(sh);
             rows.push_back(row);
             const int nc = 2 * ctx->h_sh_l[sh] + 1;
             for (int c = 0; c < nc; ++c) aos.push_back(ctx->h_sh_ao0[sh] + c);
             row += nc;
         }
-        m.nsh = (int)shells.size() - m.sh0;
-        m.nb = row;
-        m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
-        flops += 4.0 * double(m.nb) * m.nb * m.npts;
-        sum_nb += m.nb;
+        for (int bb = grp_blk[gi]; bb < grp_blk[gi + 1]; ++bb) {
+            BlockMeta& m = ctx->h_meta[bb];
+            m.sh0 = sh0, m.ao0 = ao0;
+            m.nsh = (int)shells.size() - sh0;
+            m.nb = row;
+            m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
+            flops += 4.0 * double(m.nb) * m.nb * m.npts;
+            sum_nb += m.nb;
+        }
     }
-    // 3. chunks of blocks whose intermediates fit the workspace budget
+    // 3. chunks of whole groups whose intermediates fit the workspace budget
     ctx->chunks.clear();
     size_t off = 0, max_ws = 0;
     Chunk cur{0, 0, 0, 0};
-    for (int bb = 0; bb < nblk; ++bb) {
-        const size_t need = !mixed ? pdfxc::block_ws_doubles(ctx->h_meta[bb].nbp, gga_ws) * sizeof(double)
-                            : ctx->opt.split_terms == 10 ? pdfxc::oz_layout(ctx->h_meta[bb].nbp).total
-                                                         : pdfxc::mixed_layout(ctx->h_meta[bb].nbp).total;
-        if (off + need > ctx->opt.workspace_bytes && bb > cur.b0) {
-            cur.b1 = bb;
+    auto block_need = [&](int bb) -> size_t {
+        const BlockMeta& m = ctx->h_meta[bb];
+        if (!mixed) return pdfxc::block_ws_doubles(m.nbp, gga_ws) * sizeof(double);
+        if (ctx->opt.split_terms != 10) return pdfxc::mixed_layout(m.nbp).total;
+        const pdfxc::OzLayout L = pdfxc::oz_layout(m.nbp);
+        return m.lead == bb ? L.total_lead : L.total;
+    };
+    for (int gi = 0; gi < ngrp; ++gi) {
+        size_t need = 0;
+        for (int bb = grp_blk[gi]; bb < grp_blk[gi + 1]; ++bb) need += block_need(bb);
+        if (off + need > ctx->opt.workspace_bytes && grp_blk[gi] > cur.b0) {
+            cur.b1 = grp_blk[gi];
             cur.ws_bytes = off;
             ctx->chunks.push_back(cur);
             max_ws = std::max(max_ws, off);
-            cur = Chunk{bb, bb, 0, 0};
+            cur = Chunk{grp_blk[gi], grp_blk[gi], 0, 0};
             off = 0;
         }
-        ctx->h_meta[bb].ws = (int64_t)off;
-        off += need;
-        cur.max_nbp = std::max(cur.max_nbp, ctx->h_meta[bb].nbp);
+        for (int bb = grp_blk[gi]; bb < grp_blk[gi + 1]; ++bb) {
+            ctx->h_meta[bb].ws = (int64_t)off;
+            off += block_need(bb);
+            cur.max_nbp = std::max(cur.max_nbp, ctx->h_meta[bb].nbp);
+        }
     }
     cur.b1 = nblk;
     cur.ws_bytes = off;
@@ -471,6 +512,8 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     upload(&ctx->d_blk_shell_row, rows, s);
     upload(&ctx->d_blk_aos, aos, s);
     upload(&ctx->d_seg_blk, ctx->seg_blk, s);
+    ctx->h_grp.assign(grp_blk.begin(), grp_blk.end() - 1);
+    upload(&ctx->d_grp, ctx->h_grp, s);
     dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
     dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
     dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
@@ -632,9 +675,11 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
             for (int k = 0; k < 5; ++k) PDFXC_CUDA(cudaEventRecord(e[k], s));
             continue;
         }
+        const int g_lo = (int)(std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), cb0) - ctx->h_grp.begin());
+        const int g_hi = (int)(std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), cb0 + cn) - ctx->h_grp.begin());
         pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
-                           ctx->d_Vacc, ctx->d_err};
+                           ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo};
         const bool oz = ctx->opt.split_terms == 10;
         PDFXC_CUDA(cudaEventRecord(e[0], s));
         oz ? pdfxc::oz_prepare(a, s) : pdfxc::mixed_prepare(a, s);
@@ -649,7 +694,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         oz ? pdfxc::oz_vxc(a, s) : pdfxc::mixed_vxc(a, s);
         PDFXC_LAUNCHED("Vxc contraction");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
-        launches += oz ? 7 : 6;
+        launches += oz ? 9 : 6;
     }
     for (size_t ci = 0; ci < ctx->chunks.size() && !mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
@@ -1236,7 +1281,13 @@ pdfxc_status pdfxc_set_block_range(pdfxc_ctx* ctx, int64_t b_lo, int64_t b_hi) {
             return PDFXC_ERR_ARG;
         }
         drop_graph(ctx);
-        ctx->blk_lo = (int)b_lo, ctx->blk_hi = (int)b_hi;
+        // a group is built whole, by the range that holds its first block: both ends move
+        // up to the next group start (no move when every block is its own group)
+        auto snap = [&](int64_t b) {
+            const auto it = std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), (int)b);
+            return it == ctx->h_grp.end() ? ctx->nblk : *it;
+        };
+        ctx->blk_lo = snap(b_lo), ctx->blk_hi = snap(b_hi);
         ctx->rho_valid = false;  // stored densities outside the new range are not this context's
         return PDFXC_OK;
     });

@@ -23,6 +23,8 @@ struct BlockMeta {
     int nb;        // screened AOs
     int nbp;       // nb rounded up to the contraction tile
     int npts;      // real points in the block (<= BLOCK_PTS)
+    int lead;      // first block of this block's group (the block itself when ungrouped)
+    int gn;        // blocks in the group; a group's blocks are consecutive and share one screened basis
     int64_t ws;    // byte offset of this block's intermediates inside its chunk's workspace
 };
 
@@ -98,6 +100,8 @@ struct pdfxc_ctx {
     int blk_lo = 0, blk_hi = 0;  // the blocks this context builds (pdfxc_set_block_range; default all)
     std::vector<int> seg_blk;    // blocks of grid segment i (a molecule of a batch): [seg_blk[i], seg_blk[i+1])
     int* d_seg_blk = nullptr;
+    std::vector<int> h_grp;      // first block of every group, ascending (groups: consecutive blocks, one basis)
+    int* d_grp = nullptr;
     // batch of molecules (pdfxc_set_batch): AO offset and count of each molecule in the joint system
     std::vector<int> mol;        // AO offsets, size nmol + 1 (empty: a single molecule)
     double* d_mol_sums = nullptr;  // [2 * nmol]: Exc, electron count per molecule
@@ -247,17 +251,24 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 }
 
 // Intermediates of one block on the fixed-point (INT8 slice) path. Operands are
-// split into OZ_SLICES signed 7-bit slices with a power-of-two scale per row:
-// v = 2^e * sum_i s_i 2^(-7 i); slice planes are packed K-major in 64-byte slabs.
+// cut into OZ_SLICES signed digits in [-127, 127] with a power-of-two scale per row:
+// v = 2^e (s_1/127 + s_2/(127 254) + s_3/(127 254^2) + s_4/(127 254^3)); digit planes
+// are packed K-major in 64-byte slabs. The Vxc contraction runs over all points of a
+// group, so the scales of its operands (phi and Z rows) are group maxima: every block
+// keeps its own row exponents (e_phi, e_z) and the group's (e_phi_g, e_z_g, written by
+// the group's first block). P_sub is shared by the group and lives only in the first
+// block's region, after `total` (`total_lead` bytes in all).
 constexpr int OZ_SLICES = 4;
 struct OzLayout {
-    size_t phi64;               // FP64 phi and grad phi, [4][nbp][128] (written by the FP64 AO kernel)
+    size_t phi64;               // FP64 phi and grad phi, [4][nbp][128] (written by the FP64 AO kernel);
+                                // plane 0 holds Z after the rho contraction
     size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs
     size_t phi2, phi2_plane;    // phi slices: rows = nbp AOs, K = 128 points
-    size_t ppack, ppack_plane;  // P_sub slices: rows = nbp, K = nbp
     size_t zpack, zpack_plane;  // Z slices: rows = nbp, K = 128 points
-    size_t e_pt, e_phi, e_p, e_z;  // int exponents: per point (phi^T rows), per AO row of phi, P_sub, Z
+    size_t e_pt, e_phi, e_z, e_phi_g, e_z_g, e_p;  // int exponents: per point, per AO row (block, group), P_sub
     size_t total;
+    size_t ppack, ppack_plane;  // P_sub slices of the group: rows = nbp, K = nbp (first block only)
+    size_t total_lead;
 };
 
 __host__ __device__ inline OzLayout oz_layout(int nbp) {
@@ -272,21 +283,21 @@ __host__ __device__ inline OzLayout oz_layout(int nbp) {
     L.phi2 = o;
     L.phi2_plane = (size_t)nbp * BLOCK_PTS;
     o = a256(o + OZ_SLICES * L.phi2_plane);
-    L.ppack = o;
-    L.ppack_plane = (size_t)nbp * nbp;
-    o = a256(o + OZ_SLICES * L.ppack_plane);
     L.zpack = o;
     L.zpack_plane = (size_t)nbp * BLOCK_PTS;
     o = a256(o + OZ_SLICES * L.zpack_plane);
     L.e_pt = o;
     o = a256(o + sizeof(int) * BLOCK_PTS);
-    L.e_phi = o;
-    o = a256(o + sizeof(int) * nbp);
-    L.e_p = o;
-    o = a256(o + sizeof(int) * nbp);
-    L.e_z = o;
-    o = a256(o + sizeof(int) * nbp);
+    size_t* e[5] = {&L.e_phi, &L.e_z, &L.e_phi_g, &L.e_z_g, &L.e_p};
+    for (size_t* f : e) {
+        *f = o;
+        o = a256(o + sizeof(int) * nbp);
+    }
     L.total = o;
+    L.ppack = o;
+    L.ppack_plane = (size_t)nbp * nbp;
+    o = a256(o + OZ_SLICES * L.ppack_plane);
+    L.total_lead = o;
     return L;
 }
 
@@ -300,6 +311,8 @@ struct MixedArgs {
     char* ws;
     double *rho_acc, *rho_store, *coef, *blk_sum, *Vacc;
     int* err;
+    const int* grp;  // first blocks of the chunk's groups (INT8 path)
+    int ngrp;
 };
 void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
 void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue

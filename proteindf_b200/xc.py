@@ -119,7 +119,7 @@ class XcEngine:
     """
 
     def __init__(self, device=0, precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16,
-                 workspace_bytes=0, split_terms=6):
+                 workspace_bytes=0, split_terms=10):
         self.L = load_library()
         opt = Options()
         self.L.pdfxc_default_options(ctypes.byref(opt))

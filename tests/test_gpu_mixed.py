@@ -39,7 +39,7 @@ def test_water2_mixed_vs_reference(water2, fn, terms):
 
 @pytest.mark.parametrize("fn", ["SVWN", "B3LYP"])
 def test_chain12_mixed_vs_reference(chain12, fn):
-    eng = engine(chain12, precision="mixed")
+    eng = engine(chain12, precision="mixed", split_terms=6)
     eng.set_grid(chain12["grid"][:, :4])
     exc, nel, V = eng.build_vxc(fn, chain12["PA"])
     dE = abs(exc - chain12[f"{fn}_exc"][0])
@@ -64,7 +64,7 @@ def test_mixed_vs_fp64_gpu_water8():
     PA = 0.5 * systems.density_matrix(sh.nao, 40, seed=0)
     e64.set_grid(xyzw, A)
     exc64, nel64, V64 = e64.build_vxc("B3LYP", PA)
-    em = XcEngine(precision="mixed")
+    em = XcEngine(precision="mixed", split_terms=6)
     em.set_system(sh)
     em.set_grid(xyzw, A)
     excm, nelm, Vm = em.build_vxc("B3LYP", PA)
@@ -75,9 +75,13 @@ def test_mixed_vs_fp64_gpu_water8():
 
 # INT8 fixed-point slices (split_terms = 10): operands cut from the FP64 AO values
 # into four radix-254 digits (~31 bits), exact integer accumulation; only the
-# unbiased digit truncation remains (measured: 2e-11 of Exc on the 100-atom chain,
-# 5e-14 on the 2000-atom chain).
-OZ_TOL = (2e-10, 2e-9)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
+# unbiased digit truncation and the dropped digit products of order >= 6 remain
+# (measured: 2e-11 of Exc on the 100-atom chain, 5e-14 on the 2000-atom chain). The
+# Vxc contraction accumulates a group of up to 4 blocks (512 points) under one scale
+# per AO row; measured max|dVxc|/max|Vxc|: 1.0e-9 to 1.3e-9 on (H2O)2 and 2.0e-9 to
+# 3.4e-9 on the 12-atom chain (a CPU emulation of the digit arithmetic gives 3.0e-9 for
+# 128-point and 3.2e-9 for 512-point accumulation on the chain).
+OZ_TOL = (2e-10, 5e-9)  # (|dExc|/|Exc|, max|dVxc|/max|Vxc|)
 
 
 @pytest.mark.parametrize("fn", ["SVWN", "HFB", "B3LYP"])
@@ -87,7 +91,7 @@ def test_water2_int8_slices_vs_reference(water2, fn):
     exc, nel, V = eng.build_vxc(fn, water2["PA"])
     dE = abs(exc - water2[f"{fn}_exc"][0])
     dV = np.abs(V - water2[f"{fn}_vxc"]).max()
-    print(f"{fn} int8 slices: |dExc|={dE:.3e} max|dVxc|={dV:.3e}")
+    print(f"{fn} int8 slices: |dExc|={dE:.3e} max|dVxc|={dV:.3e} rel {dV / np.abs(water2[f'{fn}_vxc']).max():.3e}")
     assert within(exc, water2[f"{fn}_exc"][0], V, water2[f"{fn}_vxc"], OZ_TOL)
     assert abs(nel - water2[f"{fn}_nelec_alpha"][0]) <= 1e-10 * abs(nel)
 
@@ -97,12 +101,14 @@ def test_chain12_int8_slices_vs_reference(chain12, fn):
     eng = engine(chain12, precision="mixed", split_terms=10)
     eng.set_grid(chain12["grid"][:, :4])
     exc, nel, V = eng.build_vxc(fn, chain12["PA"])
-    print(f"chain12 {fn} int8 slices: |dExc|={abs(exc - chain12[f'{fn}_exc'][0]):.3e}")
+    dV = np.abs(V - chain12[f"{fn}_vxc"]).max() / np.abs(chain12[f"{fn}_vxc"]).max()
+    print(f"chain12 {fn} int8 slices: |dExc|={abs(exc - chain12[f'{fn}_exc'][0]):.3e} max|dVxc|/max|Vxc|={dV:.3e}")
     assert within(exc, chain12[f"{fn}_exc"][0], V, chain12[f"{fn}_vxc"], OZ_TOL)
 
 
-def test_mixed_incremental(water2):
-    eng = engine(water2, precision="mixed")
+@pytest.mark.parametrize("terms", [6, 10])
+def test_mixed_incremental(water2, terms):
+    eng = engine(water2, precision="mixed", split_terms=terms)
     eng.set_grid(water2["grid"][:, :4])
     PA = water2["PA"]
     eng.build_vxc("B3LYP", 0.5 * PA)
