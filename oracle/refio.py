@@ -104,7 +104,8 @@ def run_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, timeout
     np.ascontiguousarray(PA, dtype=np.float64).tofile(ppath)
     case = os.path.join(workdir, "grad.txt")
     write_case(case, symbols, charges, xyz_bohr, basis, {"functional": functional, "density_file": ppath})
-    return run("grad", case, os.path.join(workdir, "grad_out.bin"), timeout=timeout)
+    # one thread: the SG-1 grid generator of the reference races with several (see _dropin_env)
+    return run("grad", case, os.path.join(workdir, "grad_out.bin"), threads=1, timeout=timeout)
 
 
 def run_func(workdir, functional, inputs5):
@@ -125,6 +126,16 @@ def dropin_available():
     return os.path.exists(DROPIN_BIN)
 
 
+def _dropin_env():
+    """One OpenMP thread for the harness that links the reference classes: the reference's
+    DfGenerateGrid::getGrids builds its orientation matrix in an OpenMP loop that adds into
+    one shared matrix without a reduction (src/libpdf/DfGenerateGrid.cpp:1768-1795), so with
+    several threads the SG-1 gradient grid of either class can come out rotated."""
+    env = dict(os.environ)
+    env["OMP_NUM_THREADS"] = "1"
+    return env
+
+
 def run_dropin(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, timeout=None):
     """Reference DfCalcGridX and DfCalcGridX_B200 on the same inputs, two SCF
     iterations (P_A/2, then the difference P_A/2 with xc-update)."""
@@ -138,7 +149,7 @@ def run_dropin(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA
         "functional": functional, "npts": len(grid5), "grid_file": gpath, "density_file": ppath})
     out = os.path.join(workdir, "dropin.bin")
     subprocess.run([DROPIN_BIN, "dropin", case, out], check=True, timeout=timeout, cwd=workdir,
-                   stdout=subprocess.DEVNULL)
+                   stdout=subprocess.DEVNULL, env=_dropin_env())
     return read_records(out)
 
 
@@ -152,7 +163,7 @@ def run_dropin_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, 
     write_case(case, symbols, charges, xyz_bohr, basis, {"functional": functional, "density_file": ppath})
     out = os.path.join(workdir, "dropin_grad.bin")
     subprocess.run([DROPIN_BIN, "dropin_grad", case, out], check=True, timeout=timeout, cwd=workdir,
-                   stdout=subprocess.DEVNULL)
+                   stdout=subprocess.DEVNULL, env=_dropin_env())
     return read_records(out)
 
 
@@ -172,5 +183,5 @@ def run_dropin_uks(workdir, symbols, charges, xyz_bohr, basis, functional, grid5
         "density_file_b": pbpath})
     out = os.path.join(workdir, "dropin_uks.bin")
     subprocess.run([DROPIN_BIN, "dropin_uks", case, out], check=True, timeout=timeout, cwd=workdir,
-                   stdout=subprocess.DEVNULL)
+                   stdout=subprocess.DEVNULL, env=_dropin_env())
     return read_records(out)

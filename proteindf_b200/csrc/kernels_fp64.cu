@@ -14,6 +14,7 @@
 // V_ij += w vrho phi_i phi_j + phi_i (c . grad phi_j) + phi_j (c . grad phi_i).
 #include <cuda_runtime.h>
 
+#include "ao.cuh"
 #include "functional.cuh"
 #include "pdfxc_internal.cuh"
 
@@ -21,31 +22,10 @@ namespace pdfxc {
 
 namespace {
 
-// Angular polynomial A of component t (the reference's prefactors, DfCalcGridX.cpp:103-141)
-// and its gradient.
-__device__ __forceinline__ void ang_poly1(int t, double x, double y, double z, double& A, double& Ax, double& Ay,
-                                          double& Az) {
-    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
-    switch (t) {
-        case 0: A = 1.0; Ax = Ay = Az = 0.0; break;
-        case 1: A = x; Ax = 1.0; Ay = Az = 0.0; break;
-        case 2: A = y; Ay = 1.0; Ax = Az = 0.0; break;
-        case 3: A = z; Az = 1.0; Ax = Ay = 0.0; break;
-        case 4: A = x * y; Ax = y; Ay = x; Az = 0.0; break;
-        case 5: A = z * x; Ax = z; Az = x; Ay = 0.0; break;
-        case 6: A = y * z; Ay = z; Az = y; Ax = 0.0; break;
-        case 7: A = 0.5 * (x * x - y * y); Ax = x; Ay = -y; Az = 0.0; break;
-        default: A = s3 * (z * z - 0.5 * (x * x + y * y)); Ax = -s3 * x; Ay = -s3 * y; Az = 2.0 * s3 * z;
-    }
-}
-
 // One CTA per block, 256 threads: the point is threadIdx.x % 128, the two
 // halves of the CTA take alternate shells. Stores are coalesced along points.
-// Per shell the contraction is summed once, S0 = sum_k c_k e^{-a_k r^2} and
-// S1 = sum_k c_k a_k e^{-a_k r^2} (primitives with a r^2 > 30 skipped, :690);
-// each component is then phi = A S0 and grad phi = grad A S0 - 2 r A S1 for its
-// angular polynomial A: the reference's per-primitive prefactors
-// (getPrefactor / getPrefactorForDerivative, :103-235) summed in another order.
+// Per shell the contraction is summed once (shell_radial), then every component
+// is formed from the radial sums (ao_from_radial).
 template <bool GGA>
 __global__ void __launch_bounds__(256) k_ao_eval(BasisView bas, GridView g, int blk0, char* ws) {
     const int blk = blk0 + blockIdx.x;
@@ -63,27 +43,18 @@ __global__ void __launch_bounds__(256) k_ao_eval(BasisView bas, GridView g, int 
         const int a = bas.sh_atom[s];
         const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1],
                      z = rz - bas.atom_xyz[3 * a + 2];
-        const double d2 = x * x + y * y + z * z;
-        const int L = bas.sh_l[s], n = 2 * L + 1, np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
-        double S0 = 0.0, S1 = 0.0;
-        for (int k = 0; k < np; ++k) {
-            const double al = bas.p_exp[p0 + k];
-            if (al * d2 <= 30.0) {  // TOOBIG, DfCalcGridX.cpp:42, :690
-                const double e = bas.p_coef[p0 + k] * exp(-al * d2);
-                S0 += e;
-                if (GGA) S1 += al * e;
-            }
-        }
+        const int L = bas.sh_l[s], n = 2 * L + 1;
+        double S0, S1;
+        shell_radial<GGA>(bas, s, x * x + y * y + z * z, S0, S1);
         for (int c = 0; c < n; ++c) {
-            double A, Ax, Ay, Az;
-            ang_poly1(L * L + c, x, y, z, A, Ax, Ay, Az);
+            double v, gx, gy, gz;
+            ao_from_radial<GGA>(L * L + c, x, y, z, S0, S1, v, gx, gy, gz);
             const size_t o = (size_t)(row0 + c) * BLOCK_PTS + p;
-            phi[o] = A * S0;
+            phi[o] = v;
             if (GGA) {
-                const double t = 2.0 * A * S1;
-                dphi[o] = Ax * S0 - x * t;
-                dphi[plane + o] = Ay * S0 - y * t;
-                dphi[2 * plane + o] = Az * S0 - z * t;
+                dphi[o] = gx;
+                dphi[plane + o] = gy;
+                dphi[2 * plane + o] = gz;
             }
         }
     }

@@ -20,6 +20,7 @@
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include "ao.cuh"
 #include "functional.cuh"
 #include "pdfxc_internal.cuh"
 #include "umma.cuh"
@@ -433,10 +434,13 @@ __global__ void __launch_bounds__(128, 1)
 // accumulated exactly in int32 TMEM; the products with i + j <= 5 are kept, one
 // accumulator per order k = i + j, and the epilogue forms
 // 2^(eA + eB) sum_k D_k / (127^2 254^(k-2)) in FP64. The operands are sliced
-// from the FP64 AO values of the FP64 path (an FP32 copy of phi would cost
-// ~3e-9 of Exc, the slices cost ~1e-11), and the rho epilogue multiplies by
-// the FP64 AO values. FP32 accumulation, whose rounding on the tensor cores is
-// toward zero, never occurs.
+// from FP64 AO values (an FP32 copy of phi would cost ~3e-9 of Exc, the slices
+// cost ~1e-11), and the rho epilogue multiplies by FP64 AO values. FP32
+// accumulation, whose rounding on the tensor cores is toward zero, never occurs.
+//
+// AO values are never stored: the AO kernel keeps each shell's radial sums S0, S1
+// per point (16 bytes per shell and point instead of 32 per AO and point for phi
+// and its gradient) and every consumer forms the components from them.
 constexpr double kOzD1 = 127.0, kOzD = 254.0;
 __device__ __forceinline__ double oz_weight(int k) {  // weight of order k = i + j
     double w = 1.0 / (kOzD1 * kOzD1);
@@ -454,23 +458,37 @@ __device__ __forceinline__ int oz_exponent(double m) {
     return e;
 }
 
-__device__ __forceinline__ void oz_slice(double v, int e, int8_t* s) {
-    double t = ldexp(v, -e) * kOzD1;  // |t| < 127
+// 2^e (0 below the normal range, where only kOzZeroExp sums lie, and those sums are 0)
+__device__ __forceinline__ double oz_pow2(int e) {
+    return e < -1022 ? 0.0 : __longlong_as_double((long long)(e + 1023) << 52);
+}
+
+// The digits of v at row scale 2^e, sc = 127 254^3 2^-e (0 for an all-zero row): the whole
+// expansion q = rint(v sc) fits an int32 (|q| <= 127 254^3 < 2^31); balanced remainders
+// modulo 254 from the last digit up give s_4, s_3, s_2 in [-127, 127] and leave the first,
+// |s_1| <= 127 + 1/2. Integer arithmetic after one FP64 multiply and one rounding.
+constexpr double kOzFull = 127.0 * 254.0 * 254.0 * 254.0;
+__device__ __forceinline__ double oz_digit_scale(int e) { return e <= kOzZeroExp ? 0.0 : ldexp(kOzFull, -e); }
+__device__ __forceinline__ void oz_slice(double v, double sc, int8_t* s) {
+    int q = __double2int_rn(v * sc);
 #pragma unroll
-    for (int i = 0; i < OZ_SLICES; ++i) {
-        const double q = rint(t);
-        s[i] = (int8_t)q;
-        t = (t - q) * kOzD;  // |t - q| <= 1/2
+    for (int i = OZ_SLICES - 1; i > 0; --i) {
+        int r = q % 254;
+        r = r > 127 ? r - 254 : (r < -127 ? r + 254 : r);
+        s[i] = (int8_t)r;
+        q = (q - r) / 254;
     }
+    s[0] = (int8_t)q;
 }
 
 // 16 consecutive K values of one row -> four 16-byte slice stores.
 __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
     __align__(16) int8_t s[OZ_SLICES][16];
+    const double sc = oz_digit_scale(e);
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
         int8_t t[OZ_SLICES];
-        oz_slice(v[j], e, t);
+        oz_slice(v[j], sc, t);
 #pragma unroll
         for (int i = 0; i < OZ_SLICES; ++i) s[i][j] = t[i];
     }
@@ -478,15 +496,116 @@ __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off,
     for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = *reinterpret_cast<uint4*>(s[i]);
 }
 
-// Digits of the rows of an FP64 [nbp][128] plane of block `blk` with its group's row
-// exponents: the maximum over the group's blocks of their own row exponents (int array at
-// offset e_blk of each block's region); the group's first block also stores them at e_grp.
-// A warp takes 8 rows x 64 points (lane = row r, K group kg), so each digit store
-// instruction writes four whole 128-byte core matrices.
-__device__ void oz_slice_rows_group(const GridView& g, int blk, const BlockMeta& m, const OzLayout& L, char* ws,
-                                    size_t src, size_t e_blk, size_t e_grp, size_t dst) {
+__device__ __forceinline__ double warp_max_d(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// One AO row of a block: its component, its shell's atom and radial sums.
+struct OzRow {
+    int t;                  // L^2 + component
+    double ax, ay, az;      // the shell's atom
+    const double* S0;       // radial sums of the shell at the block's points
+    const double* S1;
+};
+
+__device__ __forceinline__ OzRow oz_row(const GridView& g, const BlockMeta& m, const double* rad, int mu) {
+    const RowGeom q = g.blk_row_geom[m.ao0 + mu];
+    const int slot = q.info >> 4;
+    OzRow r;
+    r.t = q.info & 15;
+    r.ax = q.ax, r.ay = q.ay, r.az = q.az;
+    r.S0 = rad + (size_t)slot * BLOCK_PTS;
+    r.S1 = rad + (size_t)(m.nsh + slot) * BLOCK_PTS;
+    return r;
+}
+
+// Point coordinates of a block (and, for Z, the per-point Vxc coefficients) in shared memory.
+struct OzPoints {
+    double x[BLOCK_PTS], y[BLOCK_PTS], z[BLOCK_PTS];
+    double c[4][BLOCK_PTS];  // 0.5 w vrho, c_x, c_y, c_z
+};
+
+__device__ __forceinline__ void oz_load_points(const GridView& g, int blk, const double* coef, OzPoints& P) {
+    for (int p = threadIdx.x; p < BLOCK_PTS; p += blockDim.x) {
+        const size_t gp = (size_t)blk * BLOCK_PTS + p;
+        P.x[p] = g.px[gp], P.y[p] = g.py[gp], P.z[p] = g.pz[gp];
+    }
+    if (coef)
+        for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
+            P.c[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
+}
+
+// phi (Z = false) or Z = 0.5 w vrho phi + c . grad phi (Z = true) of row r at point p.
+template <bool Z, bool GGA>
+__device__ __forceinline__ double oz_value(const OzRow& r, const OzPoints& P, int p) {
+    const double x = P.x[p] - r.ax, y = P.y[p] - r.ay, z = P.z[p] - r.az;
+    double v, gx, gy, gz;
+    ao_from_radial<Z && GGA>(r.t, x, y, z, r.S0[p], (Z && GGA) ? r.S1[p] : 0.0, v, gx, gy, gz);
+    if (!Z) return v;
+    double w = P.c[0][p] * v;
+    if (GGA) w += P.c[1][p] * gx + P.c[2][p] * gy + P.c[3][p] * gz;
+    return w;
+}
+
+// AO stage of a block: radial sums of its shells at its points, the per-point exponents of
+// phi^T rows (max over the AOs) and the block's per-AO exponents of phi rows (max over the
+// points). 256 threads: the point is threadIdx.x % 128, the two halves take alternate
+// shells; a row's maximum is reduced over a warp's 32 points by shuffles and over the
+// half's four warps by an integer atomic max on the row's exponent (the exponent of a
+// maximum is the maximum of the exponents).
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_ao_oz(BasisView bas, GridView g, int blk0, char* ws) {
+    __shared__ double hmax[BLOCK_PTS];
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const OzLayout L = oz_layout(m.nbp, m.nsh);
     char* base = ws + m.ws;
-    const double* v = reinterpret_cast<const double*>(base + src);
+    double* S0p = reinterpret_cast<double*>(base + L.rad);
+    double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
+    int* e_phi = reinterpret_cast<int*>(base + L.e_phi);
+    for (int r = threadIdx.x; r < m.nbp; r += blockDim.x) e_phi[r] = kOzZeroExp;
+    __syncthreads();
+    const int p = threadIdx.x & (BLOCK_PTS - 1), half = threadIdx.x >> 7, lane = threadIdx.x & 31;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
+    double pm = 0.0;
+    for (int i = half; i < m.nsh; i += 2) {
+        const int s = g.blk_shells[m.sh0 + i];
+        const int row0 = g.blk_shell_row[m.sh0 + i];
+        const int a = bas.sh_atom[s];
+        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
+        const int Lq = bas.sh_l[s];
+        double S0, S1;
+        shell_radial<GGA>(bas, s, x * x + y * y + z * z, S0, S1);
+        S0p[(size_t)i * BLOCK_PTS + p] = S0;
+        if (GGA) S1p[(size_t)i * BLOCK_PTS + p] = S1;
+        for (int c = 0; c < 2 * Lq + 1; ++c) {
+            double v, gx, gy, gz;
+            ao_from_radial<false>(Lq * Lq + c, x, y, z, S0, 0.0, v, gx, gy, gz);
+            v = fabs(v);
+            pm = fmax(pm, v);
+            const double wm = warp_max_d(v);
+            if (lane == 0 && wm > 0.0) atomicMax(&e_phi[row0 + c], oz_exponent(wm));
+        }
+    }
+    if (half) hmax[p] = pm;
+    __syncthreads();
+    if (!half) reinterpret_cast<int*>(base + L.e_pt)[p] = oz_exponent(fmax(pm, hmax[p]));
+}
+
+// Digits of the rows (phi, or Z) of block `blk` with its group's row exponents: the maximum
+// over the group's blocks of their own row exponents (int array at offset e_blk of each
+// block's region); the group's first block also stores them at e_grp. A warp takes 8 rows x
+// 64 points (lane = row r, K group kg), so each digit store instruction writes four whole
+// 128-byte core matrices. The caller has loaded the block's points into P.
+template <bool Z, bool GGA>
+__device__ void oz_slice_rows_group(const BasisView& bas, const GridView& g, int blk, const BlockMeta& m,
+                                    const OzLayout& L, char* ws, const OzPoints& P, size_t e_blk, size_t e_grp,
+                                    size_t dst) {
+    char* base = ws + m.ws;
+    const double* rad = reinterpret_cast<const double*>(base + L.rad);
     auto group_exp = [&](int mu) {
         int e = kOzZeroExp;
         for (int i = 0; i < m.gn; ++i)
@@ -498,62 +617,67 @@ __device__ void oz_slice_rows_group(const GridView& g, int blk, const BlockMeta&
     for (int t = warp; t < (m.nbp / 8) * 2; t += blockDim.x / 32) {
         const int mu = (t >> 1) * 8 + r, p0 = (t & 1) * 64 + kg * 16;
         const int e = group_exp(mu);
+        if (mu < m.nb) {
+            const OzRow row = oz_row(g, m, rad, mu);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) x[j] = mu < m.nb ? v[(size_t)mu * BLOCK_PTS + p0 + j] : 0.0;
+            for (int j = 0; j < 16; ++j) x[j] = oz_value<Z, GGA>(row, P, p0 + j);
+        } else {
+#pragma unroll
+            for (int j = 0; j < 16; ++j) x[j] = 0.0;
+        }
+        // zpack_plane == phi2_plane: both are [nbp][128]
         oz_store16(base + dst, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), x, e);
     }
     if (blk == m.lead)
         for (int mu = threadIdx.x; mu < m.nbp; mu += blockDim.x) reinterpret_cast<int*>(base + e_grp)[mu] = group_exp(mu);
 }
 
-// Row scales of phi^T (per point, max over the block's AOs) and of phi (per AO row, max
-// over the points), from the FP64 AO values. One CTA per block: warps take AO rows
-// (lane = 4 points each), every thread also keeps the running maximum of its point.
-__global__ void __launch_bounds__(BLOCK_PTS) k_oz_scales(GridView g, int blk0, char* ws) {
-    const int blk = blk0 + blockIdx.x;
-    const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp);
-    char* base = ws + m.ws;
-    const double* phi = reinterpret_cast<const double*>(base + L.phi64);
-    int* e_pt = reinterpret_cast<int*>(base + L.e_pt);
-    int* e_phi = reinterpret_cast<int*>(base + L.e_phi);
-    const int p = threadIdx.x, warp = p >> 5, lane = p & 31;
-    double pmax = 0.0;
-    for (int r = 0; r < m.nb; ++r) pmax = fmax(pmax, fabs(phi[(size_t)r * BLOCK_PTS + p]));
-    e_pt[p] = oz_exponent(pmax);
-    for (int r = warp; r < m.nbp; r += BLOCK_PTS / 32) {
-        double mx = 0.0;
-        if (r < m.nb)
-            for (int q = lane; q < BLOCK_PTS; q += 32) mx = fmax(mx, fabs(phi[(size_t)r * BLOCK_PTS + q]));
-        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
-        if (lane == 0) e_phi[r] = oz_exponent(mx);
-    }
-}
-
 // Slices of phi^T (rows = points, per-point exponents) and phi (rows = AOs, the group's
-// per-AO exponents: the Vxc contraction runs over the whole group's points).
-__global__ void __launch_bounds__(256) k_slice_phi(GridView g, int blk0, char* ws) {
+// per-AO exponents: the Vxc contraction runs over the whole group's points). Per tile of
+// 16 AO rows the CTA forms phi once in shared memory (a thread per point and half-tile);
+// then the first half cuts the phi^T digits (a thread per point: 16 AOs, one 16-byte store
+// per digit plane) and the second half the phi digits (a thread per row and 16 points; 8
+// consecutive rows with the same points fill whole 128-byte core matrices).
+__global__ void __launch_bounds__(256) k_slice_phi(BasisView bas, GridView g, int blk0, char* ws) {
+    __shared__ OzPoints P;
+    __shared__ double vt[16][BLOCK_PTS + 1];
+    __shared__ int eg[16];
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp);
+    const OzLayout L = oz_layout(m.nbp, m.nsh);
     char* base = ws + m.ws;
-    const double* phi = reinterpret_cast<const double*>(base + L.phi64);
+    const double* rad = reinterpret_cast<const double*>(base + L.rad);
     const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
-    double v[16];
-    const int g1 = m.nbp / 16;
-    for (int e = threadIdx.x; e < BLOCK_PTS * g1; e += blockDim.x) {  // phi^T: row p, 16 AOs
-        const int p = e % BLOCK_PTS, mu0 = (e / BLOCK_PTS) * 16;
+    int* e_phi_g = reinterpret_cast<int*>(base + L.e_phi_g);
+    oz_load_points(g, blk, nullptr, P);
+    const int p = threadIdx.x & (BLOCK_PTS - 1), half = threadIdx.x >> 7;
+    for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
+        __syncthreads();  // the previous tile's digits are cut (and P is loaded)
+#pragma unroll 4
+        for (int j = 0; j < 8; ++j) {
+            const int r = half * 8 + j, mu = mu0 + r;
+            vt[r][p] = mu < m.nb ? oz_value<false, false>(oz_row(g, m, rad, mu), P, p) : 0.0;
+        }
+        if (threadIdx.x < 16) {  // the group's exponent of each row: the max over its blocks
+            int e = kOzZeroExp;
+            for (int i = 0; i < m.gn; ++i)
+                e = max(e, reinterpret_cast<const int*>(ws + g.meta[m.lead + i].ws + L.e_phi)[mu0 + threadIdx.x]);
+            eg[threadIdx.x] = e;
+            if (blk == m.lead) e_phi_g[mu0 + threadIdx.x] = e;
+        }
+        __syncthreads();
+        double v[16];
+        if (half == 0) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) v[j] = mu0 + j < m.nb ? phi[(size_t)(mu0 + j) * BLOCK_PTS + p] : 0.0;
-        oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
+            for (int j = 0; j < 16; ++j) v[j] = vt[j][p];
+            oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
+        } else {
+            const int u = threadIdx.x - BLOCK_PTS, r = (u & 7) + 8 * (u >> 6), kg = (u >> 3) & 7;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = vt[r][kg * 16 + j];
+            oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu0 + r, kg * 16, BLOCK_PTS), v, eg[r]);
+        }
     }
-    oz_slice_rows_group(g, blk, m, L, ws, L.phi64, L.e_phi, L.e_phi_g, L.phi2);
-}
-
-__device__ __forceinline__ double warp_max_d(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
-    return v;
 }
 
 // P_sub digits of a group. Phase 1: the row exponents, a warp per row mu gathering P[aos[mu]][aos[nu]]
@@ -563,7 +687,7 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
                                                    const int* __restrict__ grp, char* ws) {
     const int blk = grp[blockIdx.x];  // one CTA per group: P_sub lives in the first block's region
     const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp);
+    const OzLayout L = oz_layout(m.nbp, m.nsh);
     char* base = ws + m.ws;
     int* e_p = reinterpret_cast<int*>(base + L.e_p);
     const int* aos = g.blk_aos + m.ao0;
@@ -594,39 +718,27 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
     }
 }
 
-// Z[nu][p] = 0.5 w vrho phi + c . grad phi in FP64 over plane 0 of the block's AO planes
-// (phi is not read again after the rho contraction), and the block's row exponents of Z.
-// A warp per row, lanes along the points; each element is read and rewritten by one thread.
+// The block's row exponents of Z[nu][p] = 0.5 w vrho phi + c . grad phi (formed from the
+// radial sums; Z is not stored). A warp per row, lanes along the points.
 template <bool GGA>
-__global__ void __launch_bounds__(256) k_z_oz(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
+__global__ void __launch_bounds__(256) k_z_oz(BasisView bas, GridView g, int blk0, const double* __restrict__ coef,
+                                              char* ws) {
+    __shared__ OzPoints P;
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp);
+    const OzLayout L = oz_layout(m.nbp, m.nsh);
     char* base = ws + m.ws;
-    double* phi = reinterpret_cast<double*>(base + L.phi64);
+    const double* rad = reinterpret_cast<const double*>(base + L.rad);
     int* e_z = reinterpret_cast<int*>(base + L.e_z);
-    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
-    __shared__ double cf[4][BLOCK_PTS];
-    for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
-        cf[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
+    oz_load_points(g, blk, coef, P);
     __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     for (int nu = warp; nu < m.nbp; nu += blockDim.x / 32) {
         double mx = 0.0;
         if (nu < m.nb) {
-            double z[4];
+            const OzRow row = oz_row(g, m, rad, nu);
 #pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const int p = lane + 32 * j;
-                const size_t o = (size_t)nu * BLOCK_PTS + p;
-                z[j] = cf[0][p] * phi[o];
-                if (GGA) z[j] += cf[1][p] * phi[plane + o] + cf[2][p] * phi[2 * plane + o] + cf[3][p] * phi[3 * plane + o];
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                phi[(size_t)nu * BLOCK_PTS + lane + 32 * j] = z[j];
-                mx = fmax(mx, fabs(z[j]));
-            }
+            for (int j = 0; j < 4; ++j) mx = fmax(mx, fabs(oz_value<true, GGA>(row, P, lane + 32 * j)));
         }
         mx = warp_max_d(mx);
         if (lane == 0) e_z[nu] = oz_exponent(mx);
@@ -634,11 +746,16 @@ __global__ void __launch_bounds__(256) k_z_oz(GridView g, int blk0, const double
 }
 
 // Z digits (rows = AOs, K = points) with the group's row exponents.
-__global__ void __launch_bounds__(256) k_pack_z_oz(GridView g, int blk0, char* ws) {
+template <bool GGA>
+__global__ void __launch_bounds__(256) k_pack_z_oz(BasisView bas, GridView g, int blk0,
+                                                   const double* __restrict__ coef, char* ws) {
+    __shared__ OzPoints P;
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp);
-    oz_slice_rows_group(g, blk, m, L, ws, L.phi64, L.e_z, L.e_z_g, L.zpack);
+    const OzLayout L = oz_layout(m.nbp, m.nsh);
+    oz_load_points(g, blk, coef, P);
+    __syncthreads();
+    oz_slice_rows_group<true, GGA>(bas, g, blk, m, L, ws, P, L.e_z, L.e_z_g, L.zpack);
 }
 
 // Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
@@ -664,13 +781,13 @@ constexpr uint32_t OZ_TMEM_COLS = 4 * OZ_NT;                      // one accumul
 
 template <int MODE, bool GGA>
 __global__ void __launch_bounds__(128, 2)
-    k_oz(GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int tiles_max, double* rho_acc,
-         double* Vacc, int nao) {
+    k_oz(BasisView bas, GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int tiles_max,
+         double* rho_acc, double* Vacc, int nao) {
     extern __shared__ __align__(1024) uint8_t smem[];
     constexpr int S = OZ_STAGES;
     const int blk = MODE == MODE_RHO ? blk0 + (int)blockIdx.y : grp[blockIdx.y];  // VXC: the group's first block
     const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp);
+    const OzLayout L = oz_layout(m.nbp, m.nsh);
     const int ntiles = m.nbp / umma::TILE_ROWS;  // 128-row tiles of this block
     int mt, nt;                                   // nt counts 64-row tiles
     if (MODE == MODE_RHO) {
@@ -789,29 +906,32 @@ __global__ void __launch_bounds__(128, 2)
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
         const double w2 = oz_weight(2), w3 = oz_weight(3), w4 = oz_weight(4), w5 = oz_weight(5);
         if (MODE == MODE_RHO) {
-            const double* phi = reinterpret_cast<const double*>(base + L.phi64);
+            // per 16 columns: X^T[p][mu] from TMEM to FP64, then phi and grad phi of each column's
+            // AO at this thread's point from the row's geometry and its shell's radial sums
             const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
             const int* e_p = reinterpret_cast<const int*>(lead + L.e_p);
-            const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+            const double* rad = reinterpret_cast<const double*>(base + L.rad);
             const int ep = e_pt[row];
+            const size_t gp = (size_t)blk * BLOCK_PTS + row;
+            const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
             double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-            for (int c0 = 0; c0 < OZ_NT; c0 += 16) {
-                // issue all operand loads of these 16 columns first (predicated), then use them
-                double f0[16], f1[16], f2[16], f3[16];
-                int ec[16];
-#pragma unroll
-                for (int c = 0; c < 16; ++c) {
-                    const int mu = nt * OZ_NT + c0 + c;
-                    const bool live = mu < m.nb;
-                    const size_t o = (size_t)mu * BLOCK_PTS + row;
-                    f0[c] = live ? phi[o] : 0.0;
-                    if (GGA) {
-                        f1[c] = live ? phi[plane + o] : 0.0;
-                        f2[c] = live ? phi[2 * plane + o] : 0.0;
-                        f3[c] = live ? phi[3 * plane + o] : 0.0;
-                    }
-                    ec[c] = live ? e_p[mu] : 0;
+            // this thread's radial sums of the tile's shells, fetched up front (independent loads)
+            // into its own slots of the drained operand ring; shells beyond its capacity are read
+            // from global memory in the column loop
+            const int col0 = nt * OZ_NT, colN = min(col0 + OZ_NT, m.nb);
+            constexpr int kCap = OZ_STAGES * OZ_STAGE_BYTES / (2 * 8 * BLOCK_PTS);
+            double* rs = reinterpret_cast<double*>(smem);
+            int slot0 = 0, ns = 0;
+            if (col0 < colN) {
+                slot0 = g.blk_row_geom[m.ao0 + col0].info >> 4;
+                ns = min((g.blk_row_geom[m.ao0 + colN - 1].info >> 4) - slot0 + 1, kCap);
+#pragma unroll 4
+                for (int k = 0; k < ns; ++k) {
+                    rs[(2 * k) * BLOCK_PTS + row] = rad[(size_t)(slot0 + k) * BLOCK_PTS + row];
+                    if (GGA) rs[(2 * k + 1) * BLOCK_PTS + row] = rad[(size_t)(m.nsh + slot0 + k) * BLOCK_PTS + row];
                 }
+            }
+            for (int c0 = 0; c0 < OZ_NT && col0 + c0 < m.nb; c0 += 16) {
                 uint32_t d2[16], d3[16], d4[16], d5[16];
                 umma::tmem_ld16_raw(taddr + c0, d2);
                 umma::tmem_ld16_raw(taddr + OZ_NT + c0, d3);
@@ -820,14 +940,26 @@ __global__ void __launch_bounds__(128, 2)
                 umma::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
-                    const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
-                                      (double)(int)d5[c] * w5;
-                    const double x = ldexp(sx, ep + ec[c]);
-                    r += f0[c] * x;
-                    if (GGA) {
-                        gx += f1[c] * x;
-                        gy += f2[c] * x;
-                        gz += f3[c] * x;
+                    const int mu = nt * OZ_NT + c0 + c;
+                    if (mu < m.nb) {
+                        const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 +
+                                          (double)(int)d4[c] * w4 + (double)(int)d5[c] * w5;
+                        const double X = sx * oz_pow2(ep + e_p[mu]);
+                        const RowGeom q = g.blk_row_geom[m.ao0 + mu];
+                        const int slot = q.info >> 4, k = slot - slot0;
+                        const double S0 = k < ns ? rs[(2 * k) * BLOCK_PTS + row] : rad[(size_t)slot * BLOCK_PTS + row];
+                        double S1 = 0.0;
+                        if (GGA)
+                            S1 = k < ns ? rs[(2 * k + 1) * BLOCK_PTS + row]
+                                        : rad[(size_t)(m.nsh + slot) * BLOCK_PTS + row];
+                        double v, ax, ay, az;
+                        ao_from_radial<GGA>(q.info & 15, px - q.ax, py - q.ay, pz - q.az, S0, S1, v, ax, ay, az);
+                        r += v * X;
+                        if (GGA) {
+                            gx += ax * X;
+                            gy += ay * X;
+                            gz += az * X;
+                        }
                     }
                 }
             }
@@ -852,7 +984,7 @@ __global__ void __launch_bounds__(128, 2)
                 for (int c = 0; c < 16; ++c) {
                     const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
                                       (double)(int)d5[c] * w5;
-                    tile[row * 17 + c] = ldexp(sx, em + e_z[nt * OZ_NT + c0 + c]);
+                    tile[row * 17 + c] = sx * oz_pow2(em + e_z[nt * OZ_NT + c0 + c]);
                 }
                 __syncthreads();
                 const int c = threadIdx.x & 15;
@@ -878,10 +1010,12 @@ __global__ void __launch_bounds__(128, 2)
 size_t oz_smem_bytes() { return (size_t)OZ_STAGES * OZ_STAGE_BYTES + (2 * OZ_STAGES + 1) * 8 + 16; }
 
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
-    // the FP64 path's AO values and gradients (the slices are cut from them), then the row scales
-    launch_ao_eval(a.b, a.g, a.blk0, a.nblk, functional_is_gga(a.fn), a.ws, 0, s);
-    k_oz_scales<<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.ws);
-    k_slice_phi<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
+    // radial sums and row scales, then the phi digits of both layouts, then P_sub per group
+    if (functional_is_gga(a.fn))
+        k_ao_oz<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
+    else
+        k_ao_oz<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
+    k_slice_phi<<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
     k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.P, a.nao, a.grp, a.ws);
 }
 
@@ -890,12 +1024,12 @@ void oz_rho(const MixedArgs& a, cudaStream_t s) {
     const size_t smem = oz_smem_bytes();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.grp, a.ws, a.err, 2 * tiles,
-                                                                       a.rho_acc, a.Vacc, a.nao);
+        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
+                                                                       2 * tiles, a.rho_acc, a.Vacc, a.nao);
     } else {
         cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.g, a.blk0, a.grp, a.ws, a.err, 2 * tiles,
-                                                                        a.rho_acc, a.Vacc, a.nao);
+        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
+                                                                        2 * tiles, a.rho_acc, a.Vacc, a.nao);
     }
 }
 
@@ -903,13 +1037,13 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
     if (functional_is_gga(a.fn)) {
         k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                               a.rho_store, a.coef, a.blk_sum);
-        k_z_oz<true><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
-        k_pack_z_oz<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
+        k_z_oz<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
+        k_pack_z_oz<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
     } else {
         k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                                a.rho_store, a.coef, a.blk_sum);
-        k_z_oz<false><<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.coef, a.ws);
-        k_pack_z_oz<<<a.nblk, 256, 0, s>>>(a.g, a.blk0, a.ws);
+        k_z_oz<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
+        k_pack_z_oz<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
     }
 }
 
@@ -918,8 +1052,8 @@ void oz_vxc(const MixedArgs& a, cudaStream_t s) {
     const size_t smem = oz_smem_bytes();
     cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     // per group: M tiles of 128 AOs x N tiles of 64 AOs
-    k_oz<MODE_VXC, false><<<dim3(tiles * 2 * tiles, a.ngrp), 128, smem, s>>>(a.g, a.blk0, a.grp, a.ws, a.err, 2 * tiles,
-                                                                            a.rho_acc, a.Vacc, a.nao);
+    k_oz<MODE_VXC, false><<<dim3(tiles * 2 * tiles, a.ngrp), 128, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
+                                                                            2 * tiles, a.rho_acc, a.Vacc, a.nao);
 }
 
 size_t umma_smem_bytes(int nterms) {

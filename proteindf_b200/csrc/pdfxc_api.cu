@@ -126,7 +126,8 @@ pdfxc::BasisView basis_view(const pdfxc_ctx* c) {
 }
 
 pdfxc::GridView grid_view(const pdfxc_ctx* c) {
-    return {c->d_px, c->d_py, c->d_pz, c->d_pw, c->d_meta, c->d_blk_shells, c->d_blk_shell_row, c->d_blk_aos};
+    return {c->d_px,         c->d_py,         c->d_pz,          c->d_pw,         c->d_meta,
+            c->d_blk_shells, c->d_blk_shell_row, c->d_blk_aos, c->d_blk_row_info, c->d_blk_row_geom};
 }
 
 void drop_graph(pdfxc_ctx* c) {
@@ -191,6 +192,7 @@ void free_grid(pdfxc_ctx* c) {
     drop_graph(c);
     dev_free(c->d_px), dev_free(c->d_py), dev_free(c->d_pz), dev_free(c->d_pw);
     dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
+    dev_free(c->d_blk_row_info), dev_free(c->d_blk_row_geom);
     dev_free(c->d_seg_blk), dev_free(c->d_mol_sums), dev_free(c->d_grp);
     c->seg_blk.clear();
     c->h_grp.clear();
@@ -439,7 +441,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     for (int sh = 0; sh < ctx->nshell; ++sh)
         Rs[sh] = shell_cutoff_radius(ctx->h_sh_l[sh], &ctx->h_p_exp[ctx->h_sh_p0[sh]], &ctx->h_p_coef[ctx->h_sh_p0[sh]],
                                      ctx->h_sh_nprim[sh], ctx->opt.ao_cutoff);
-    std::vector<int> shells, rows, aos;
+    std::vector<int> shells, rows, aos, row_info;
     const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
     double flops = 0.0, sum_nb = 0.0;
@@ -455,8 +457,11 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
             if (d - rad[gi] > Rs[sh]) continue;
             shells.push_back(sh);
             rows.push_back(row);
-            const int nc = 2 * ctx->h_sh_l[sh] + 1;
-            for (int c = 0; c < nc; ++c) aos.push_back(ctx->h_sh_ao0[sh] + c);
+            const int L = ctx->h_sh_l[sh], nc = 2 * L + 1;
+            for (int c = 0; c < nc; ++c) {
+                aos.push_back(ctx->h_sh_ao0[sh] + c);
+                row_info.push_back(16 * ((int)shells.size() - 1 - sh0) + L * L + c);
+            }
             row += nc;
         }
         for (int bb = grp_blk[gi]; bb < grp_blk[gi + 1]; ++bb) {
@@ -477,7 +482,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
         const BlockMeta& m = ctx->h_meta[bb];
         if (!mixed) return pdfxc::block_ws_doubles(m.nbp, gga_ws) * sizeof(double);
         if (ctx->opt.split_terms != 10) return pdfxc::mixed_layout(m.nbp).total;
-        const pdfxc::OzLayout L = pdfxc::oz_layout(m.nbp);
+        const pdfxc::OzLayout L = pdfxc::oz_layout(m.nbp, m.nsh);
         return m.lead == bb ? L.total_lead : L.total;
     };
     for (int gi = 0; gi < ngrp; ++gi) {
@@ -511,6 +516,19 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     upload(&ctx->d_blk_shells, shells, s);
     upload(&ctx->d_blk_shell_row, rows, s);
     upload(&ctx->d_blk_aos, aos, s);
+    upload(&ctx->d_blk_row_info, row_info, s);
+    if (mixed) {
+        std::vector<pdfxc::RowGeom> geom(row_info.size());
+        for (int gi = 0; gi < ngrp; ++gi) {
+            const BlockMeta& m = ctx->h_meta[grp_blk[gi]];
+            for (int r = 0; r < m.nb; ++r) {
+                const int info = row_info[m.ao0 + r];
+                const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[shells[m.sh0 + (info >> 4)]]];
+                geom[m.ao0 + r] = pdfxc::RowGeom{A[0], A[1], A[2], info, 0};
+            }
+        }
+        upload(&ctx->d_blk_row_geom, geom, s);
+    }
     upload(&ctx->d_seg_blk, ctx->seg_blk, s);
     ctx->h_grp.assign(grp_blk.begin(), grp_blk.end() - 1);
     upload(&ctx->d_grp, ctx->h_grp, s);

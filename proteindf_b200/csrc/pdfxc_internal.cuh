@@ -57,6 +57,15 @@ struct GridView {
     const int* blk_shells;     // shell id
     const int* blk_shell_row;  // local AO row of the shell's first component
     const int* blk_aos;        // global AO index of each local row
+    const int* blk_row_info;   // per local row: 16 * (shell slot in the block's list) + L^2 + component
+    const struct RowGeom* blk_row_geom;  // per local row: its shell's atom and blk_row_info (INT8 path)
+};
+
+// One AO row of a block's screened basis: the atom of its shell and its blk_row_info entry.
+struct __align__(16) RowGeom {
+    double ax, ay, az;
+    int info;
+    int pad;
 };
 
 // A workspace layout for a build with its own number of [nbp][BLOCK_PTS] FP64 planes per
@@ -94,7 +103,8 @@ struct pdfxc_ctx {
     std::vector<int64_t> h_src;  // original index of each padded point slot (-1 = padding)
     double *d_px = nullptr, *d_py = nullptr, *d_pz = nullptr, *d_pw = nullptr;
     pdfxc::BlockMeta* d_meta = nullptr;
-    int *d_blk_shells = nullptr, *d_blk_shell_row = nullptr, *d_blk_aos = nullptr;
+    int *d_blk_shells = nullptr, *d_blk_shell_row = nullptr, *d_blk_aos = nullptr, *d_blk_row_info = nullptr;
+    pdfxc::RowGeom* d_blk_row_geom = nullptr;
     double contraction_flops = 0.0;
     double mean_nb = 0.0;
     int blk_lo = 0, blk_hi = 0;  // the blocks this context builds (pdfxc_set_block_range; default all)
@@ -253,15 +263,16 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 // Intermediates of one block on the fixed-point (INT8 slice) path. Operands are
 // cut into OZ_SLICES signed digits in [-127, 127] with a power-of-two scale per row:
 // v = 2^e (s_1/127 + s_2/(127 254) + s_3/(127 254^2) + s_4/(127 254^3)); digit planes
-// are packed K-major in 64-byte slabs. The Vxc contraction runs over all points of a
-// group, so the scales of its operands (phi and Z rows) are group maxima: every block
-// keeps its own row exponents (e_phi, e_z) and the group's (e_phi_g, e_z_g, written by
-// the group's first block). P_sub is shared by the group and lives only in the first
-// block's region, after `total` (`total_lead` bytes in all).
+// are packed K-major in 64-byte slabs. AO values are not stored: the block keeps each
+// shell's radial sums S0, S1 at its points ([2][nsh][128] FP64) and every consumer forms
+// phi = A S0, grad phi = grad A S0 - 2 r A S1 from them. The Vxc contraction runs over
+// all points of a group, so the scales of its operands (phi and Z rows) are group
+// maxima: every block keeps its own row exponents (e_phi, e_z) and the group's
+// (e_phi_g, e_z_g, written by the group's first block). P_sub is shared by the group
+// and lives only in the first block's region, after `total` (`total_lead` bytes in all).
 constexpr int OZ_SLICES = 4;
 struct OzLayout {
-    size_t phi64;               // FP64 phi and grad phi, [4][nbp][128] (written by the FP64 AO kernel);
-                                // plane 0 holds Z after the rho contraction
+    size_t rad;                 // radial sums: S0 [nsh][128], then S1 [nsh][128]
     size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs
     size_t phi2, phi2_plane;    // phi slices: rows = nbp AOs, K = 128 points
     size_t zpack, zpack_plane;  // Z slices: rows = nbp, K = 128 points
@@ -271,12 +282,12 @@ struct OzLayout {
     size_t total_lead;
 };
 
-__host__ __device__ inline OzLayout oz_layout(int nbp) {
+__host__ __device__ inline OzLayout oz_layout(int nbp, int nsh) {
     auto a256 = [](size_t x) { return (x + 255) & ~size_t(255); };
     OzLayout L;
     size_t o = 0;
-    L.phi64 = o;  // offset 0: the layout of the FP64 path's phi planes
-    o = a256(o + (size_t)4 * nbp * BLOCK_PTS * 8);
+    L.rad = o;
+    o = a256(o + (size_t)2 * nsh * BLOCK_PTS * 8);
     L.phi1 = o;
     L.phi1_plane = (size_t)BLOCK_PTS * nbp;
     o = a256(o + OZ_SLICES * L.phi1_plane);
