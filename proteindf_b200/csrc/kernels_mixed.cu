@@ -426,14 +426,14 @@ __global__ void __launch_bounds__(128, 1)
 // ===========================================================================
 // Fixed-point slices on the INT8 tensor cores (the split-integer product of
 // Ozaki, Ogita, Oishi and Rump, 2012, on an integer unit). Each operand row
-// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits in
-// [-127, 127]: v = 2^e (s_1 / 127 + s_2 / (127 254) + s_3 / (127 254^2) +
-// s_4 / (127 254^3)), each digit rounded to nearest and the remainder (at most
-// half a unit) carried, so that |remainder| * 254 <= 127 keeps every digit in
-// range: about 31 bits per operand. A_i B_j^T is an exact integer product,
-// accumulated exactly in int32 TMEM; the products with i + j <= 5 are kept, one
-// accumulator per order k = i + j, and the epilogue forms
-// 2^(eA + eB) sum_k D_k / (127^2 254^(k-2)) in FP64. The operands are sliced
+// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits:
+// v = 2^e (s_1 + s_2 / 2^8 + s_3 / 2^16 + s_4 / 2^24) / 127 with |s_1| <= 127 and
+// s_2..s_4 in [-128, 127], the balanced base-256 expansion of v rounded to
+// 127 2^24 units of 2^e: about 31 bits per operand. A_i B_j^T is an exact integer
+// product (|s_i s_j| <= 2^14, so K up to 2^15 stays inside int32), accumulated
+// exactly in int32 TMEM; the products with i + j <= 5 are kept, one accumulator
+// per order k = i + j, and the epilogue forms
+// 2^(eA + eB) sum_k D_k / (127^2 2^(8 (k-2))) in FP64. The operands are sliced
 // from FP64 AO values (an FP32 copy of phi would cost ~3e-9 of Exc, the slices
 // cost ~1e-11), and the rho epilogue multiplies by FP64 AO values. FP32
 // accumulation, whose rounding on the tensor cores is toward zero, never occurs.
@@ -441,7 +441,7 @@ __global__ void __launch_bounds__(128, 1)
 // AO values are never stored: the AO kernel keeps each shell's radial sums S0, S1
 // per point (16 bytes per shell and point instead of 32 per AO and point for phi
 // and its gradient) and every consumer forms the components from them.
-constexpr double kOzD1 = 127.0, kOzD = 254.0;
+constexpr double kOzD1 = 127.0, kOzD = 256.0;
 __device__ __forceinline__ double oz_weight(int k) {  // weight of order k = i + j
     double w = 1.0 / (kOzD1 * kOzD1);
     for (int i = 2; i < k; ++i) w /= kOzD;
@@ -463,37 +463,36 @@ __device__ __forceinline__ double oz_pow2(int e) {
     return e < -1022 ? 0.0 : __longlong_as_double((long long)(e + 1023) << 52);
 }
 
-// The digits of v at row scale 2^e, sc = 127 254^3 2^-e (0 for an all-zero row): the whole
-// expansion q = rint(v sc) fits an int32 (|q| <= 127 254^3 < 2^31); balanced remainders
-// modulo 254 from the last digit up give s_4, s_3, s_2 in [-127, 127] and leave the first,
-// |s_1| <= 127 + 1/2. Integer arithmetic after one FP64 multiply and one rounding.
-constexpr double kOzFull = 127.0 * 254.0 * 254.0 * 254.0;
+// The digits of 16 values of one row at row scale 2^e, stored as four 16-byte digit-plane
+// pieces (plane i holds s_{i+1}): q = rint(v 127 2^24 2^-e) fits an int32 (|q| <= 127 2^24)
+// and is q = s_1 2^24 + s_2 2^16 + s_3 2^8 + s_4 with balanced digits in [-128, 127]; adding
+// 0x80808080 (128 in every byte) makes every byte s_i + 128 without carries, so the XOR with
+// 0x80808080 leaves the four digits as the bytes of one word (|s_1| <= 127 + 1/2 since the
+// lower digits add at most 128 (2^16 + 2^8 + 1) < 2^23). A 4 x 4 byte transpose per four
+// values then gathers each digit plane. One FP64 multiply, one rounding and a few integer
+// operations per value; sc = 0 for an all-zero row.
+constexpr double kOzFull = 127.0 * 16777216.0;
 __device__ __forceinline__ double oz_digit_scale(int e) { return e <= kOzZeroExp ? 0.0 : ldexp(kOzFull, -e); }
-__device__ __forceinline__ void oz_slice(double v, double sc, int8_t* s) {
-    int q = __double2int_rn(v * sc);
-#pragma unroll
-    for (int i = OZ_SLICES - 1; i > 0; --i) {
-        int r = q % 254;
-        r = r > 127 ? r - 254 : (r < -127 ? r + 254 : r);
-        s[i] = (int8_t)r;
-        q = (q - r) / 254;
-    }
-    s[0] = (int8_t)q;
+__device__ __forceinline__ uint32_t oz_word(double v, double sc) {
+    return ((uint32_t)__double2int_rn(v * sc) + 0x80808080u) ^ 0x80808080u;
 }
-
-// 16 consecutive K values of one row -> four 16-byte slice stores.
 __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
-    __align__(16) int8_t s[OZ_SLICES][16];
     const double sc = oz_digit_scale(e);
+    uint4 d[OZ_SLICES];
+    uint32_t* dw = reinterpret_cast<uint32_t*>(d);
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        int8_t t[OZ_SLICES];
-        oz_slice(v[j], sc, t);
-#pragma unroll
-        for (int i = 0; i < OZ_SLICES; ++i) s[i][j] = t[i];
+    for (int g = 0; g < 4; ++g) {
+        const uint32_t a = oz_word(v[4 * g], sc), b = oz_word(v[4 * g + 1], sc), c = oz_word(v[4 * g + 2], sc),
+                       w = oz_word(v[4 * g + 3], sc);
+        const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
+        const uint32_t t2 = __byte_perm(c, w, 0x5140), t3 = __byte_perm(c, w, 0x7362);
+        dw[3 * 4 + g] = __byte_perm(t0, t2, 0x5410);  // byte 0: s_4
+        dw[2 * 4 + g] = __byte_perm(t0, t2, 0x7632);  // byte 1: s_3
+        dw[1 * 4 + g] = __byte_perm(t1, t3, 0x5410);  // byte 2: s_2
+        dw[0 * 4 + g] = __byte_perm(t1, t3, 0x7632);  // byte 3: s_1
     }
 #pragma unroll
-    for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = *reinterpret_cast<uint4*>(s[i]);
+    for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = d[i];
 }
 
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -593,43 +592,6 @@ __global__ void __launch_bounds__(256) k_ao_oz(BasisView bas, GridView g, int bl
     if (half) hmax[p] = pm;
     __syncthreads();
     if (!half) reinterpret_cast<int*>(base + L.e_pt)[p] = oz_exponent(fmax(pm, hmax[p]));
-}
-
-// Digits of the rows (phi, or Z) of block `blk` with its group's row exponents: the maximum
-// over the group's blocks of their own row exponents (int array at offset e_blk of each
-// block's region); the group's first block also stores them at e_grp. A warp takes 8 rows x
-// 64 points (lane = row r, K group kg), so each digit store instruction writes four whole
-// 128-byte core matrices. The caller has loaded the block's points into P.
-template <bool Z, bool GGA>
-__device__ void oz_slice_rows_group(const BasisView& bas, const GridView& g, int blk, const BlockMeta& m,
-                                    const OzLayout& L, char* ws, const OzPoints& P, size_t e_blk, size_t e_grp,
-                                    size_t dst) {
-    char* base = ws + m.ws;
-    const double* rad = reinterpret_cast<const double*>(base + L.rad);
-    auto group_exp = [&](int mu) {
-        int e = kOzZeroExp;
-        for (int i = 0; i < m.gn; ++i)
-            e = max(e, reinterpret_cast<const int*>(ws + g.meta[m.lead + i].ws + e_blk)[mu]);
-        return e;
-    };
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, r = lane & 7, kg = lane >> 3;
-    double x[16];
-    for (int t = warp; t < (m.nbp / 8) * 2; t += blockDim.x / 32) {
-        const int mu = (t >> 1) * 8 + r, p0 = (t & 1) * 64 + kg * 16;
-        const int e = group_exp(mu);
-        if (mu < m.nb) {
-            const OzRow row = oz_row(g, m, rad, mu);
-#pragma unroll
-            for (int j = 0; j < 16; ++j) x[j] = oz_value<Z, GGA>(row, P, p0 + j);
-        } else {
-#pragma unroll
-            for (int j = 0; j < 16; ++j) x[j] = 0.0;
-        }
-        // zpack_plane == phi2_plane: both are [nbp][128]
-        oz_store16(base + dst, L.phi2_plane, umma::packed_offset_i8(mu, p0, BLOCK_PTS), x, e);
-    }
-    if (blk == m.lead)
-        for (int mu = threadIdx.x; mu < m.nbp; mu += blockDim.x) reinterpret_cast<int*>(base + e_grp)[mu] = group_exp(mu);
 }
 
 // Slices of phi^T (rows = points, per-point exponents) and phi (rows = AOs, the group's
@@ -745,17 +707,48 @@ __global__ void __launch_bounds__(256) k_z_oz(BasisView bas, GridView g, int blk
     }
 }
 
-// Z digits (rows = AOs, K = points) with the group's row exponents.
+// Z digits (rows = AOs, K = points) with the group's row exponents. Per tile of 16 rows
+// the CTA forms Z once in shared memory (a thread per point and half-tile, so the rows and
+// their angular type are uniform across a warp), then 128 threads cut the digits (a thread
+// per row and 16 points; 8 consecutive rows with the same points fill whole 128-byte core
+// matrices).
 template <bool GGA>
 __global__ void __launch_bounds__(256) k_pack_z_oz(BasisView bas, GridView g, int blk0,
                                                    const double* __restrict__ coef, char* ws) {
     __shared__ OzPoints P;
+    __shared__ double vt[16][BLOCK_PTS + 1];
+    __shared__ int eg[16];
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp, m.nsh);
+    char* base = ws + m.ws;
+    const double* rad = reinterpret_cast<const double*>(base + L.rad);
+    int* e_z_g = reinterpret_cast<int*>(base + L.e_z_g);
     oz_load_points(g, blk, coef, P);
-    __syncthreads();
-    oz_slice_rows_group<true, GGA>(bas, g, blk, m, L, ws, P, L.e_z, L.e_z_g, L.zpack);
+    const int p = threadIdx.x & (BLOCK_PTS - 1), half = threadIdx.x >> 7;
+    for (int nu0 = 0; nu0 < m.nbp; nu0 += 16) {
+        __syncthreads();  // the previous tile's digits are cut (and P is loaded)
+#pragma unroll 4
+        for (int j = 0; j < 8; ++j) {
+            const int r = half * 8 + j, nu = nu0 + r;
+            vt[r][p] = nu < m.nb ? oz_value<true, GGA>(oz_row(g, m, rad, nu), P, p) : 0.0;
+        }
+        if (threadIdx.x < 16) {  // the group's exponent of each row: the max over its blocks
+            int e = kOzZeroExp;
+            for (int i = 0; i < m.gn; ++i)
+                e = max(e, reinterpret_cast<const int*>(ws + g.meta[m.lead + i].ws + L.e_z)[nu0 + threadIdx.x]);
+            eg[threadIdx.x] = e;
+            if (blk == m.lead) e_z_g[nu0 + threadIdx.x] = e;
+        }
+        __syncthreads();
+        if (half == 1) {
+            const int u = threadIdx.x - BLOCK_PTS, r = (u & 7) + 8 * (u >> 6), kg = (u >> 3) & 7;
+            double v[16];
+#pragma unroll
+            for (int j = 0; j < 16; ++j) v[j] = vt[r][kg * 16 + j];
+            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, kg * 16, BLOCK_PTS), v, eg[r]);
+        }
+    }
 }
 
 // Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
