@@ -772,11 +772,20 @@ constexpr uint32_t OZ_B_SLICE = OZ_NT * umma::I8_SLAB_K;          // 4 KiB
 constexpr uint32_t OZ_STAGE_BYTES = OZ_A_BYTES + OZ_SLICES * OZ_B_SLICE;  // 48 KiB
 constexpr uint32_t OZ_TMEM_COLS = 4 * OZ_NT;                      // one accumulator per order 2..5
 
+// RHO runs 8 warps: the MMA pipeline uses warps 0 and 1 as in VXC, and the epilogue splits
+// the tile's 64 columns between warps w and w + 4, which read the same TMEM lane quarter.
+template <int MODE>
+constexpr int oz_threads() {
+    return MODE == MODE_RHO ? 256 : 128;
+}
+
 template <int MODE, bool GGA>
-__global__ void __launch_bounds__(128, 2)
+__global__ void __launch_bounds__(oz_threads<MODE>(), 2)
     k_oz(BasisView bas, GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int tiles_max,
          double* rho_acc, double* Vacc, int nao) {
     extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ RowGeom s_geom[OZ_NT];  // RHO: the tile's columns
+    __shared__ int s_ep[OZ_NT];
     constexpr int S = OZ_STAGES;
     const int blk = MODE == MODE_RHO ? blk0 + (int)blockIdx.y : grp[blockIdx.y];  // VXC: the group's first block
     const BlockMeta m = g.meta[blk];
@@ -899,52 +908,60 @@ __global__ void __launch_bounds__(128, 2)
         const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
         const double w2 = oz_weight(2), w3 = oz_weight(3), w4 = oz_weight(4), w5 = oz_weight(5);
         if (MODE == MODE_RHO) {
-            // per 16 columns: X^T[p][mu] from TMEM to FP64, then phi and grad phi of each column's
-            // AO at this thread's point from the row's geometry and its shell's radial sums
-            const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
+            // The tile's column data (row geometry, P_sub exponent) once per CTA in shared memory;
+            // then each thread (point = lane quarter of its warp, columns = half of the tile)
+            // fetches its radial sums of the half's shells up front (independent loads) into its
+            // own slots of the drained operand ring, and per 16 columns converts X^T[p][mu] from
+            // TMEM to FP64 and forms phi and grad phi of the column's AO at its point.
+            const int col0 = nt * OZ_NT;
             const int* e_p = reinterpret_cast<const int*>(lead + L.e_p);
+            if (threadIdx.x < OZ_NT && col0 + (int)threadIdx.x < m.nb) {
+                s_geom[threadIdx.x] = g.blk_row_geom[m.ao0 + col0 + threadIdx.x];
+                s_ep[threadIdx.x] = e_p[col0 + threadIdx.x];
+            }
+            __syncthreads();
+            const int quarter = warp & 3, chalf = warp >> 2;
+            const int pt = quarter * 32 + lane;
+            const uint32_t tq = tmem + ((uint32_t)(quarter * 32) << 16);
             const double* rad = reinterpret_cast<const double*>(base + L.rad);
-            const int ep = e_pt[row];
-            const size_t gp = (size_t)blk * BLOCK_PTS + row;
+            const int ep = reinterpret_cast<const int*>(base + L.e_pt)[pt];
+            const size_t gp = (size_t)blk * BLOCK_PTS + pt;
             const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
-            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-            // this thread's radial sums of the tile's shells, fetched up front (independent loads)
-            // into its own slots of the drained operand ring; shells beyond its capacity are read
-            // from global memory in the column loop
-            const int col0 = nt * OZ_NT, colN = min(col0 + OZ_NT, m.nb);
-            constexpr int kCap = OZ_STAGES * OZ_STAGE_BYTES / (2 * 8 * BLOCK_PTS);
-            double* rs = reinterpret_cast<double*>(smem);
+            constexpr int kHalf = OZ_NT / 2;
+            constexpr int kCap = OZ_STAGES * OZ_STAGE_BYTES / 2 / (2 * 8 * BLOCK_PTS);  // shells per half
+            double* rs = reinterpret_cast<double*>(smem + (size_t)chalf * (OZ_STAGES * OZ_STAGE_BYTES / 2));
+            const int ca = chalf * kHalf, cb = min(ca + kHalf, m.nb - col0);  // this half's columns [ca, cb)
             int slot0 = 0, ns = 0;
-            if (col0 < colN) {
-                slot0 = g.blk_row_geom[m.ao0 + col0].info >> 4;
-                ns = min((g.blk_row_geom[m.ao0 + colN - 1].info >> 4) - slot0 + 1, kCap);
+            if (ca < cb) {
+                slot0 = s_geom[ca].info >> 4;
+                ns = min((s_geom[cb - 1].info >> 4) - slot0 + 1, kCap);
 #pragma unroll 4
                 for (int k = 0; k < ns; ++k) {
-                    rs[(2 * k) * BLOCK_PTS + row] = rad[(size_t)(slot0 + k) * BLOCK_PTS + row];
-                    if (GGA) rs[(2 * k + 1) * BLOCK_PTS + row] = rad[(size_t)(m.nsh + slot0 + k) * BLOCK_PTS + row];
+                    rs[(2 * k) * BLOCK_PTS + pt] = rad[(size_t)(slot0 + k) * BLOCK_PTS + pt];
+                    if (GGA) rs[(2 * k + 1) * BLOCK_PTS + pt] = rad[(size_t)(m.nsh + slot0 + k) * BLOCK_PTS + pt];
                 }
             }
-            for (int c0 = 0; c0 < OZ_NT && col0 + c0 < m.nb; c0 += 16) {
+            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+            for (int c0 = ca; c0 < cb; c0 += 16) {
                 uint32_t d2[16], d3[16], d4[16], d5[16];
-                umma::tmem_ld16_raw(taddr + c0, d2);
-                umma::tmem_ld16_raw(taddr + OZ_NT + c0, d3);
-                umma::tmem_ld16_raw(taddr + 2 * OZ_NT + c0, d4);
-                umma::tmem_ld16_raw(taddr + 3 * OZ_NT + c0, d5);
+                umma::tmem_ld16_raw(tq + c0, d2);
+                umma::tmem_ld16_raw(tq + OZ_NT + c0, d3);
+                umma::tmem_ld16_raw(tq + 2 * OZ_NT + c0, d4);
+                umma::tmem_ld16_raw(tq + 3 * OZ_NT + c0, d5);
                 umma::tmem_wait_ld();
 #pragma unroll
                 for (int c = 0; c < 16; ++c) {
-                    const int mu = nt * OZ_NT + c0 + c;
-                    if (mu < m.nb) {
+                    if (c0 + c < cb) {
                         const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 +
                                           (double)(int)d4[c] * w4 + (double)(int)d5[c] * w5;
-                        const double X = sx * oz_pow2(ep + e_p[mu]);
-                        const RowGeom q = g.blk_row_geom[m.ao0 + mu];
+                        const double X = sx * oz_pow2(ep + s_ep[c0 + c]);
+                        const RowGeom q = s_geom[c0 + c];
                         const int slot = q.info >> 4, k = slot - slot0;
-                        const double S0 = k < ns ? rs[(2 * k) * BLOCK_PTS + row] : rad[(size_t)slot * BLOCK_PTS + row];
+                        const double S0 = k < ns ? rs[(2 * k) * BLOCK_PTS + pt] : rad[(size_t)slot * BLOCK_PTS + pt];
                         double S1 = 0.0;
                         if (GGA)
-                            S1 = k < ns ? rs[(2 * k + 1) * BLOCK_PTS + row]
-                                        : rad[(size_t)(m.nsh + slot) * BLOCK_PTS + row];
+                            S1 = k < ns ? rs[(2 * k + 1) * BLOCK_PTS + pt]
+                                        : rad[(size_t)(m.nsh + slot) * BLOCK_PTS + pt];
                         double v, ax, ay, az;
                         ao_from_radial<GGA>(q.info & 15, px - q.ax, py - q.ay, pz - q.az, S0, S1, v, ax, ay, az);
                         r += v * X;
@@ -956,7 +973,7 @@ __global__ void __launch_bounds__(128, 2)
                     }
                 }
             }
-            double* acc = rho_acc + ((size_t)blk * BLOCK_PTS + row) * 4;
+            double* acc = rho_acc + ((size_t)blk * BLOCK_PTS + pt) * 4;
             atomicAdd(acc, r);
             if (GGA) atomicAdd(acc + 1, gx), atomicAdd(acc + 2, gy), atomicAdd(acc + 3, gz);
         } else {
@@ -1017,11 +1034,11 @@ void oz_rho(const MixedArgs& a, cudaStream_t s) {
     const size_t smem = oz_smem_bytes();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
+        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), oz_threads<MODE_RHO>(), smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
                                                                        2 * tiles, a.rho_acc, a.Vacc, a.nao);
     } else {
         cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), 128, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
+        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), oz_threads<MODE_RHO>(), smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
                                                                         2 * tiles, a.rho_acc, a.Vacc, a.nao);
     }
 }
