@@ -426,14 +426,16 @@ __global__ void __launch_bounds__(128, 1)
 // ===========================================================================
 // Fixed-point slices on the INT8 tensor cores (the split-integer product of
 // Ozaki, Ogita, Oishi and Rump, 2012, on an integer unit). Each operand row
-// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits:
-// v = 2^e (s_1 + s_2 / 2^8 + s_3 / 2^16 + s_4 / 2^24) / 127 with |s_1| <= 127 and
-// s_2..s_4 in [-128, 127], the balanced base-256 expansion of v rounded to
-// 127 2^24 units of 2^e: about 31 bits per operand. A_i B_j^T is an exact integer
-// product (|s_i s_j| <= 2^14, so K up to 2^15 stays inside int32), accumulated
-// exactly in int32 TMEM; the products with i + j <= 5 are kept, one accumulator
-// per order k = i + j, and the epilogue forms
-// 2^(eA + eB) sum_k D_k / (127^2 2^(8 (k-2))) in FP64. The operands are sliced
+// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits in [-127, 127]:
+// v = 2^e (s_1 + s_2 / 255 + s_3 / 255^2 + s_4 / 255^3) / 127, the balanced base-255
+// expansion of v rounded to 127 255^3 units of 2^e: about 31 bits per operand. The
+// digit set is symmetric (digits(-v) = -digits(v)), so the dropped low-order products
+// have zero mean; a base-256 expansion, whose lower digits lie in [-128, 127], would
+// not. A_i B_j^T is an
+// exact integer product (|s_i s_j| <= 127^2, so K up to 2^15 stays inside int32),
+// accumulated exactly in int32 TMEM; the products with i + j <= 5 are kept, one
+// accumulator per order k = i + j, and the epilogue forms
+// 2^(eA + eB) sum_k D_k / (127^2 255^(k-2)) in FP64. The operands are sliced
 // from FP64 AO values (an FP32 copy of phi would cost ~3e-9 of Exc, the slices
 // cost ~1e-11), and the rho epilogue multiplies by FP64 AO values. FP32
 // accumulation, whose rounding on the tensor cores is toward zero, never occurs.
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(128, 1)
 // AO values are never stored: the AO kernel keeps each shell's radial sums S0, S1
 // per point (16 bytes per shell and point instead of 32 per AO and point for phi
 // and its gradient) and every consumer forms the components from them.
-constexpr double kOzD1 = 127.0, kOzD = 256.0;
+constexpr double kOzD1 = 127.0, kOzD = 255.0;
 __device__ __forceinline__ double oz_weight(int k) {  // weight of order k = i + j
     double w = 1.0 / (kOzD1 * kOzD1);
     for (int i = 2; i < k; ++i) w /= kOzD;
@@ -464,17 +466,19 @@ __device__ __forceinline__ double oz_pow2(int e) {
 }
 
 // The digits of 16 values of one row at row scale 2^e, stored as four 16-byte digit-plane
-// pieces (plane i holds s_{i+1}): q = rint(v 127 2^24 2^-e) fits an int32 (|q| <= 127 2^24)
-// and is q = s_1 2^24 + s_2 2^16 + s_3 2^8 + s_4 with balanced digits in [-128, 127]; adding
-// 0x80808080 (128 in every byte) makes every byte s_i + 128 without carries, so the XOR with
-// 0x80808080 leaves the four digits as the bytes of one word (|s_1| <= 127 + 1/2 since the
-// lower digits add at most 128 (2^16 + 2^8 + 1) < 2^23). A 4 x 4 byte transpose per four
-// values then gathers each digit plane. One FP64 multiply, one rounding and a few integer
-// operations per value; sc = 0 for an all-zero row.
-constexpr double kOzFull = 127.0 * 16777216.0;
+// pieces (plane i holds s_{i+1}): q = rint(v 127 255^3 2^-e) fits an int32 (|q| <= 127 255^3);
+// u = q + 127 (255^3 + 255^2 + 255 + 1) lies in [0, 255^4), and its base-255 digits d_i
+// (three unsigned divisions by 255) are s_i + 127. Adding 129 to every byte (mod 256, no
+// carries between bytes) turns d_i into the int8 s_i; a 4 x 4 byte transpose per four values
+// then gathers each digit plane. sc = 0 for an all-zero row.
+constexpr double kOzFull = 127.0 * 255.0 * 255.0 * 255.0;
+constexpr uint32_t kOzOff = 127u * (255u * 255u * 255u + 255u * 255u + 255u + 1u);
 __device__ __forceinline__ double oz_digit_scale(int e) { return e <= kOzZeroExp ? 0.0 : ldexp(kOzFull, -e); }
 __device__ __forceinline__ uint32_t oz_word(double v, double sc) {
-    return ((uint32_t)__double2int_rn(v * sc) + 0x80808080u) ^ 0x80808080u;
+    const uint32_t u = (uint32_t)__double2int_rn(v * sc) + kOzOff;
+    const uint32_t u1 = u / 255u, u2 = u1 / 255u, u3 = u2 / 255u;
+    const uint32_t x = (u3 << 24) | ((u2 - 255u * u3) << 16) | ((u1 - 255u * u2) << 8) | (u - 255u * u1);
+    return ((x & 0x7F7F7F7Fu) + 0x01010101u) ^ ((x ^ 0x81818181u) & 0x80808080u);
 }
 __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
     const double sc = oz_digit_scale(e);
