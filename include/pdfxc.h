@@ -50,7 +50,8 @@ enum {
 
 enum {
     PDFXC_PRECISION_FP64 = 0,  /* the drop-in: every product in FP64 */
-    PDFXC_PRECISION_MIXED = 1  /* tensor-core split-BF16 contractions, FP64 sums */
+    PDFXC_PRECISION_MIXED = 1  /* the two contractions on tensor cores with split operands (INT8 digits by
+                                  default, see split_terms), FP64 AO values, functional and sums */
 };
 
 typedef struct {
@@ -59,8 +60,10 @@ typedef struct {
     double ao_cutoff;    /* drop a shell from a block when its value/gradient bound is below (default 1e-14) */
     double rho_cutoff;   /* xc-density-threshold: points with rho_A <= it are skipped (default 1e-16) */
     size_t workspace_bytes; /* device workspace budget for block intermediates (0 = default 4 GiB) */
-    int split_terms;     /* mixed path: INT8 digit products kept, 3, 6 or 10 (default 10: four radix-254
-                            digits per operand, every product i + j <= 5, about 31 bits) */
+    int split_terms;     /* mixed path operand split: 10 (default) = four balanced base-255 INT8 digits
+                            per operand (about 31 bits), the 10 digit products of order i + j <= 5 on
+                            the integer tensor cores; 3 or 6 = BF16 hi/mid(/lo) split with FP32
+                            accumulation (about 1e-6 relative, for comparison only) */
 } pdfxc_options;
 
 typedef struct pdfxc_ctx pdfxc_ctx;
@@ -133,6 +136,15 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
  * them (restart with xc-update = yes). */
 pdfxc_status pdfxc_get_rho(pdfxc_ctx* ctx, int gga, double* rho);
 pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho);
+
+/* Density at arbitrary points: rho[i] = sum_jk P[j][k] phi_j(r_i) phi_k(r_i) for the
+ * row-major n_ao x n_ao host matrix P and the points xyz (npts x 3, bohr). Replaces
+ * DfCalcGridX::gridDensity (src/libpdf/DfCalcGridX.cpp:1038-1044, AO values of every
+ * basis function then getRhoAtGridPoint, :865-881), which TlDensField::makeDensFld
+ * (src/tools/TlDensField.cpp:35-53) calls once per point of a density-field grid. Needs
+ * pdfxc_set_system; runs on the FP64 path of a private grid, so the context's own grid,
+ * stored densities and build graphs are untouched. No weights, no functional. */
+pdfxc_status pdfxc_density(pdfxc_ctx* ctx, const double* P, int64_t npts, const double* xyz, double* rho);
 
 /* Open-shell build (FP64 path only; a mixed-precision context returns
  * PDFXC_ERR_UNSUPPORTED). Replaces the UKS overloads

@@ -13,6 +13,7 @@
 //   pdfxc_ref func  <case.txt> <out.bin>   pointwise functional values
 //   pdfxc_ref lebedev - <out.bin>          unit-sphere Lebedev tables
 //   pdfxc_ref grad  <case.txt> <out.bin>   XC nuclear gradient + its SG-1 grid
+//   pdfxc_ref density <case.txt> <out.bin> DfCalcGridX::gridDensity at listed points
 //
 // The XC mode follows DfCalcGridX::calcXCIntegForFockAndEnergy
 // (src/libpdf/DfCalcGridX.cpp:2280-2315): calcRho_{LDA,GGA}_part (:1862-1962)
@@ -23,6 +24,7 @@
 // recorded separately.
 #include <omp.h>
 
+#include <algorithm>
 #include <chrono>
 #include <cstdio>
 #include <cstdlib>
@@ -492,6 +494,37 @@ int runFunc(const Case& c, const char* outPath) {
 
 // Unit-sphere Lebedev tables for every order the reference supports
 // (src/libpdftl/TlLebedevGrid.cpp), as used by getSphericalGrids.
+// rho(r) = phi(r)^T P phi(r) at the points of points_file (npts x 3) through the
+// reference's DfCalcGridX::gridDensity (src/libpdf/DfCalcGridX.cpp:1038-1044), one
+// call per point as TlDensField::makeDensFld makes them (src/tools/TlDensField.cpp:35-53).
+std::vector<double> referenceDensities(TlSerializeData* param, const TlDenseSymmetricMatrix_Lapack& P,
+                                       const std::vector<double>& xyz) {
+    DfCalcGridX e(param);
+    std::vector<double> rho(xyz.size() / 3, 0.0);
+    for (size_t k = 0; k < rho.size(); ++k) e.gridDensity(P, TlPosition(xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2]), &rho[k]);
+    return rho;
+}
+
+TlDenseSymmetricMatrix_Lapack readSymmetric(const Case& c, int N) {
+    const std::vector<double> P = readDoubles(c.get("density_file"), (size_t)N * N);
+    TlDenseSymmetricMatrix_Lapack PA(N);
+    for (int i = 0; i < N; ++i)
+        for (int j = 0; j <= i; ++j) PA.set(i, j, P[(size_t)i * N + j]);
+    return PA;
+}
+
+int runDensity(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    const int npts = std::atoi(c.get("npts").c_str());
+    const std::vector<double> xyz = readDoubles(c.get("points_file"), (size_t)npts * 3);
+    Out out(outPath);
+    out.put("rho", referenceDensities(&param, readSymmetric(c, N), xyz));
+    return 0;
+}
+
 int runLebedev(const char* outPath) {
     TlLebedevGrid leb;
     const std::vector<int> orders = leb.getSupportedGridNumber();
@@ -649,6 +682,29 @@ int runDropinUks(const Case& c, const char* outPath) {
 
 // The XC nuclear gradient through both classes' energyGradient (each builds the
 // SG-1 gradient grid itself), then DfCalcGridX_B200 with the grid-weight term on.
+// gridDensity through both classes; the B200 class also through its batched form.
+int runDropinDensity(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    const int N = orbProbe.getNumOfOrbitals();
+    param["num_of_AOs"] = N;
+    const int npts = std::atoi(c.get("npts").c_str());
+    const std::vector<double> xyz = readDoubles(c.get("points_file"), (size_t)npts * 3);
+    const TlDenseSymmetricMatrix_Lapack P = readSymmetric(c, N);
+    Out out(outPath);
+    out.put("ref_rho", referenceDensities(&param, P, xyz));
+    DfCalcGridX_B200 b(&param);
+    std::vector<TlPosition> pts;
+    std::vector<double> one(npts, 0.0);
+    for (int k = 0; k < npts; ++k) {
+        pts.emplace_back(xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2]);
+        if (k < 8) b.gridDensity(P, pts.back(), &one[k]);
+    }
+    out.put("b200_rho", b.gridDensities(P, pts));
+    out.put("b200_rho_single", std::vector<double>(one.begin(), one.begin() + std::min(npts, 8)));
+    return 0;
+}
+
 int runDropinGrad(const Case& c, const char* outPath) {
     TlSerializeData param = makeParam(c);
     const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
@@ -709,7 +765,9 @@ int main(int argc, char** argv) {
     if (mode == "grid") return runGrid(c, argv[3]);
     if (mode == "func") return runFunc(c, argv[3]);
     if (mode == "grad") return runGrad(c, argv[3]);
+    if (mode == "density") return runDensity(c, argv[3]);
 #ifdef PDFXC_DROPIN
+    if (mode == "dropin_density") return runDropinDensity(c, argv[3]);
     if (mode == "dropin") return runDropin(c, argv[3]);
     if (mode == "dropin_grad") return runDropinGrad(c, argv[3]);
     if (mode == "dropin_uks") return runDropinUks(c, argv[3]);

@@ -108,6 +108,23 @@ def run_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, timeout
     return run("grad", case, os.path.join(workdir, "grad_out.bin"), threads=1, timeout=timeout)
 
 
+def _density_case(workdir, symbols, charges, xyz_bohr, basis, P, points):
+    os.makedirs(os.path.join(workdir, "fl_Work"), exist_ok=True)
+    ppath, xpath = os.path.join(workdir, "P.bin"), os.path.join(workdir, "points.bin")
+    np.ascontiguousarray(P, dtype=np.float64).tofile(ppath)
+    np.ascontiguousarray(points, dtype=np.float64).reshape(-1, 3).tofile(xpath)
+    case = os.path.join(workdir, "density.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis,
+               {"density_file": ppath, "points_file": xpath, "npts": len(np.reshape(points, (-1, 3)))})
+    return case
+
+
+def run_density(workdir, symbols, charges, xyz_bohr, basis, P, points, timeout=None):
+    """rho(r) = phi^T P phi at the points through the reference's DfCalcGridX::gridDensity."""
+    case = _density_case(workdir, symbols, charges, xyz_bohr, basis, P, points)
+    return run("density", case, os.path.join(workdir, "density_out.bin"), timeout=timeout)["rho"]
+
+
 def run_func(workdir, functional, inputs5):
     os.makedirs(workdir, exist_ok=True)
     ipath = os.path.join(workdir, "func_in.bin")
@@ -163,6 +180,16 @@ def run_dropin_grad(workdir, symbols, charges, xyz_bohr, basis, functional, PA, 
     write_case(case, symbols, charges, xyz_bohr, basis, {"functional": functional, "density_file": ppath})
     out = os.path.join(workdir, "dropin_grad.bin")
     subprocess.run([DROPIN_BIN, "dropin_grad", case, out], check=True, timeout=timeout, cwd=workdir,
+                   stdout=subprocess.DEVNULL, env=_dropin_env())
+    return read_records(out)
+
+
+def run_dropin_density(workdir, symbols, charges, xyz_bohr, basis, P, points, timeout=None):
+    """gridDensity of the reference DfCalcGridX and of DfCalcGridX_B200 (per point for the first
+    8 points, and batched) on the same points: records ref_rho, b200_rho, b200_rho_single."""
+    case = _density_case(workdir, symbols, charges, xyz_bohr, basis, P, points)
+    out = os.path.join(workdir, "dropin_density.bin")
+    subprocess.run([DROPIN_BIN, "dropin_density", case, out], check=True, timeout=timeout, cwd=workdir,
                    stdout=subprocess.DEVNULL, env=_dropin_env())
     return read_records(out)
 

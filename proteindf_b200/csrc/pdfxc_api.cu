@@ -914,6 +914,57 @@ pdfxc_status pdfxc_get_rho(pdfxc_ctx* ctx, int gga, double* rho) {
     });
 }
 
+pdfxc_status pdfxc_density(pdfxc_ctx* ctx, const double* P, int64_t npts, const double* xyz, double* rho) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->natom == 0) {
+            ctx->err = "pdfxc_density: call pdfxc_set_system first";
+            return PDFXC_ERR_STATE;
+        }
+        if (npts < 0 || (npts > 0 && (!P || !xyz || !rho))) {
+            ctx->err = "pdfxc_density: negative count or null pointer";
+            return PDFXC_ERR_ARG;
+        }
+        if (npts == 0) return PDFXC_OK;
+        auto sub_check = [&](pdfxc_status st, const char* what) {
+            if (st != PDFXC_OK) throw std::runtime_error(std::string("pdfxc_density: ") + what + ": " + ctx->dens->err);
+        };
+        if (!ctx->dens) {
+            pdfxc_options o;
+            pdfxc_default_options(&o);
+            o.ao_cutoff = ctx->opt.ao_cutoff;
+            o.workspace_bytes = ctx->opt.workspace_bytes;
+            if (pdfxc_create(&ctx->dens, ctx->device, &o) != PDFXC_OK) throw std::runtime_error("pdfxc_density: create");
+            sub_check(pdfxc_set_system(ctx->dens, ctx->natom, ctx->h_atom_xyz.data(), ctx->h_atom_z.data(), ctx->nshell,
+                                       ctx->h_sh_atom.data(), ctx->h_sh_l.data(), ctx->h_sh_nprim.data(),
+                                       ctx->h_p_exp.data(), ctx->h_p_coef.data()),
+                      "set_system");
+        }
+        pdfxc_ctx* d = ctx->dens;
+        // the points as a grid of zero weights: the FP64 rho kernel stores rho at every
+        // point and evaluates the functional only where the weight is non-zero
+        std::vector<double> xyzw(4 * (size_t)npts);
+        for (int64_t i = 0; i < npts; ++i)
+            xyzw[4 * i] = xyz[3 * i], xyzw[4 * i + 1] = xyz[3 * i + 1], xyzw[4 * i + 2] = xyz[3 * i + 2], xyzw[4 * i + 3] = 0.0;
+        sub_check(pdfxc_set_grid(d, npts, xyzw.data(), nullptr), "set_grid");
+        cudaStream_t s = d->stream;
+        const int nao = d->nao;
+        PDFXC_CUDA(cudaMemcpyAsync(d->d_P, P, sizeof(double) * nao * nao, cudaMemcpyHostToDevice, s));
+        const pdfxc::BasisView bv = basis_view(d);
+        const pdfxc::GridView gv = grid_view(d);
+        char* ws = static_cast<char*>(d->d_ws);
+        for (const Chunk& c : d->chunks) {
+            const int nb = c.b1 - c.b0;
+            pdfxc::launch_ao_eval(bv, gv, c.b0, nb, false, ws, 0, s);
+            pdfxc::launch_gemm_x(gv, d->d_P, nao, c.b0, nb, c.max_nbp, 1, ws, s);
+            pdfxc::launch_rho_functional(gv, c.b0, nb, PDFXC_SVWN, false, d->opt.rho_cutoff, ws, d->d_rho, d->d_coef,
+                                         d->d_blk_sum, s);
+            PDFXC_LAUNCHED("density (AO values, X, rho)");
+        }
+        sub_check(pdfxc_get_rho(d, 0, rho), "get_rho");
+        return PDFXC_OK;
+    });
+}
+
 pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho) {
     return guarded(ctx, [&]() -> pdfxc_status {
         if (!rho) return PDFXC_ERR_ARG;
@@ -1357,6 +1408,7 @@ const char* pdfxc_last_error(const pdfxc_ctx* ctx) { return ctx ? ctx->err.c_str
 
 void pdfxc_destroy(pdfxc_ctx* ctx) {
     if (!ctx) return;
+    if (ctx->dens) pdfxc_destroy(ctx->dens);
     cudaSetDevice(ctx->device);
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_grid(ctx);

@@ -129,6 +129,7 @@ struct pdfxc_ctx {
     double* d_V = nullptr;        // n_ao^2
     double* d_Vacc = nullptr;     // n_ao^2 non-symmetric accumulator
     bool rho_valid = false;
+    pdfxc_ctx* dens = nullptr;  // pdfxc_density: FP64 context over the requested points (same system)
     int rho_gga = 0;
 
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -134,5 +134,15 @@ class DfCalcGridX:
         """(sum w rho_A, sum w rho_B); the second is None after a closed-shell build."""
         return self._nelec_alpha, (self._nelec_beta if self._open_shell else None)
 
+    def gridDensity(self, P, position):
+        """rho(r) = phi(r)^T P phi(r) at one point (DfCalcGridX::gridDensity,
+        src/libpdf/DfCalcGridX.cpp:1038-1044). gridDensities takes many points in one call."""
+        return float(self.gridDensities(P, np.asarray(position, dtype=np.float64).reshape(1, 3))[0])
+
+    def gridDensities(self, P, positions):
+        """rho at every point of positions (n, 3), bohr: the loop of TlDensField::makeDensFld
+        (src/tools/TlDensField.cpp:35-53) as one device call."""
+        return self._engine.density(P, positions)
+
     def close(self):
         self._engine.close()

@@ -67,6 +67,24 @@ DfCalcGridX_B200::~DfCalcGridX_B200() {
     pdfxc_destroy(ctx_);
 }
 
+std::vector<double> DfCalcGridX_B200::gridDensities(const TlDenseSymmetricMatrix_Lapack& P,
+                                                    const std::vector<TlPosition>& grids) {
+    const int n = this->m_nNumOfAOs;
+    std::vector<double> full((size_t)n * n);
+    for (int i = 0; i < n; ++i)
+        for (int j = 0; j <= i; ++j) full[(size_t)i * n + j] = full[(size_t)j * n + i] = P.get(i, j);
+    std::vector<double> xyz(3 * grids.size()), rho(grids.size(), 0.0);
+    for (size_t k = 0; k < grids.size(); ++k)
+        xyz[3 * k] = grids[k].x(), xyz[3 * k + 1] = grids[k].y(), xyz[3 * k + 2] = grids[k].z();
+    check(pdfxc_density(ctx_, full.data(), (int64_t)grids.size(), xyz.data(), rho.data()), ctx_, "pdfxc_density");
+    return rho;
+}
+
+void DfCalcGridX_B200::gridDensity(const TlDenseSymmetricMatrix_Lapack& P, const TlPosition& gridPosition,
+                                   double* pRho) {
+    *pRho = this->gridDensities(P, std::vector<TlPosition>(1, gridPosition))[0];
+}
+
 TlDenseGeneralMatrix_Lapack DfCalcGridX_B200::energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
                                                              DfFunctional_LDA* pFunctional) {
     return this->gradient(P_A, functionalId(pFunctional));

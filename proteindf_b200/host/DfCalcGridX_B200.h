@@ -68,6 +68,12 @@ class DfCalcGridX_B200 : public DfCalcGridX {
     TlDenseGeneralMatrix_Lapack energyGradient(const TlDenseSymmetricMatrix_Lapack& P_A,
                                                DfFunctional_GGA* pFunctional);
 
+    // rho(r) = phi(r)^T P phi(r) at one point (DfCalcGridX::gridDensity, src/libpdf/DfCalcGridX.cpp:1038-1044)
+    // and at many points in one device call, the loop of TlDensField::makeDensFld
+    // (src/tools/TlDensField.cpp:35-53); the build grid and its stored densities are untouched
+    void gridDensity(const TlDenseSymmetricMatrix_Lapack& P, const TlPosition& gridPosition, double* pRho);
+    std::vector<double> gridDensities(const TlDenseSymmetricMatrix_Lapack& P, const std::vector<TlPosition>& grids);
+
     // sum_i w_i rho_s(r_i) of the last build (DfCalcGridX::getWholeDensity)
     double lastElectronCountAlpha() const { return nelecAlpha_; }
     double lastElectronCountBeta() const { return nelecBeta_; }

@@ -22,7 +22,7 @@ EXPORTS = [
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
     "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
     "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
-    "pdfxc_build_vxc_batched",
+    "pdfxc_build_vxc_batched", "pdfxc_density",
 ]
 
 
@@ -66,6 +66,7 @@ def load_library(path=LIB_PATH):
     L.pdfxc_build_vxc.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_build_vxc_device.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_get_rho.argtypes = [_vp, i32, _vp]
+    L.pdfxc_density.argtypes = [_vp, _vp, i64, _vp, _vp]
     L.pdfxc_set_rho.argtypes = [_vp, i32, _vp]
     L.pdfxc_grid_stats.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.pdfxc_last_profile.argtypes = [_vp, _vp]
@@ -265,6 +266,14 @@ class XcEngine:
     def set_rho(self, rho, gga):
         rho = np.ascontiguousarray(rho, dtype=np.float64)
         self._check(self.L.pdfxc_set_rho(self.h, int(gga), _ptr(rho)), "pdfxc_set_rho")
+
+    def density(self, P, xyz):
+        """rho(r) = phi(r)^T P phi(r) at the points xyz (n, 3), bohr (DfCalcGridX::gridDensity)."""
+        P = np.ascontiguousarray(P, dtype=np.float64)
+        xyz = np.ascontiguousarray(np.asarray(xyz, dtype=np.float64).reshape(-1, 3))
+        out = np.zeros(len(xyz))
+        self._check(self.L.pdfxc_density(self.h, _ptr(P), len(xyz), _ptr(xyz), _ptr(out)), "pdfxc_density")
+        return out
 
     def set_batch(self, mols):
         """mols: list of (ShellTable, xyzw (npts, 4), atom (npts,) or None)."""

@@ -25,8 +25,13 @@ its inputs and outputs as compressed .npz files beside this script:
                    (DfCalcGridX::energyGradient_part, AO-centre and grid-weight
                    terms apart) for SVWN and B3LYP, with the SG-1 grid it
                    integrates on (points, single-centre and partition weights).
+  ref_density_water2.npz  (H2O)2 with the alpha density of ref_water2.npz: the
+                   reference's DfCalcGridX::gridDensity at a seeded set of points
+                   (a box around the molecules, points near and on the nuclei, far
+                   points where rho vanishes).
 
-usage (needs the reference tree): make -C oracle/ref && python tests/golden/make_ref_fixtures.py
+usage (needs the reference tree): make -C oracle/ref && python tests/golden/make_ref_fixtures.py [name ...]
+(names: system functional uks ss grad density; none = all)
 """
 import os
 import sys
@@ -153,18 +158,38 @@ def grad_fixture():
     np.savez_compressed(os.path.join(HERE, "ref_grad_water.npz"), **out)
 
 
-def main():
+def density_fixture():
+    w2 = dict(np.load(os.path.join(HERE, "ref_water2.npz")))
+    syms = [str(s) for s in w2["symbols"]]
+    xyz = w2["xyz"]
+    rng = np.random.default_rng(40)
+    lo, hi = xyz.min(0) - 6.0, xyz.max(0) + 6.0
+    box = lo + (hi - lo) * rng.random((400, 3))
+    near = xyz[rng.integers(0, len(xyz), 60)] + rng.normal(scale=0.05, size=(60, 3))
+    d = rng.normal(size=(20, 3))
+    far = xyz.mean(0) + (25.0 + 15.0 * rng.random((20, 1))) * d / np.linalg.norm(d, axis=1, keepdims=True)
+    pts = np.concatenate([box, near, xyz, far])
+    with tempfile.TemporaryDirectory() as dd:
+        rho = refio.run_density(dd, syms, systems.nuclear_charges(syms), xyz, basis.load_basis("cc-pVDZ"),
+                                w2["PA"], pts)
+    np.savez_compressed(os.path.join(HERE, "ref_density_water2.npz"), symbols=np.array(syms), xyz=xyz,
+                        P=w2["PA"], points=pts, rho=rho)
+
+
+def main(names):
     if not refio.ref_available():
         raise SystemExit("build the reference harness first: make -C oracle/ref")
-    syms, xyz = systems.water_cluster(2, seed=0)
-    system_fixture("ref_water2.npz", syms, xyz, 6000, FUNCS, nocc=10, seed=0)
-    syms, xyz = systems.peptide_chain(12, seed=3)
-    system_fixture("ref_chain12.npz", syms, xyz, 5000, ["SVWN", "B3LYP"], nocc=20, seed=3)
-    functional_fixture()
-    uks_fixture()
-    ss_fixture()
-    grad_fixture()
+    if not names or "system" in names:
+        syms, xyz = systems.water_cluster(2, seed=0)
+        system_fixture("ref_water2.npz", syms, xyz, 6000, FUNCS, nocc=10, seed=0)
+        syms, xyz = systems.peptide_chain(12, seed=3)
+        system_fixture("ref_chain12.npz", syms, xyz, 5000, ["SVWN", "B3LYP"], nocc=20, seed=3)
+    steps = {"functional": functional_fixture, "uks": uks_fixture, "ss": ss_fixture, "grad": grad_fixture,
+             "density": density_fixture}
+    for name, f in steps.items():
+        if not names or name in names:
+            f()
 
 
 if __name__ == "__main__":
-    main()
+    main(sys.argv[1:])

@@ -140,3 +140,13 @@ def test_oracle_ss_weights_vs_reference(water2):
     fx = golden("ref_ss_water2.npz")
     fac = oracle.ss(water2["xyz"], fx["points"], fx["atom"])
     assert np.abs(fx["w_single"] * fac - fx["w_final"]).max() <= 1e-15 * np.abs(fx["w_single"]).max()
+
+
+def test_oracle_density_at_points_vs_reference():
+    """rho = phi^T P phi at arbitrary points (DfCalcGridX::gridDensity) from the oracle's AO
+    values against the reference's gridDensity on the committed point set."""
+    fx = golden("ref_density_water2.npz")
+    phi, _ = oracle.aos(shell_table(fx), fx["points"])
+    rho = np.einsum("pi,ij,pj->p", phi, fx["P"], phi)
+    assert np.all(np.abs(rho - fx["rho"]) <= 1e-12 * np.maximum(1.0, np.abs(fx["rho"])))
+    assert np.all(fx["rho"][-20:] == 0.0)  # far points: every primitive beyond the a r^2 > 30 cut
