@@ -110,6 +110,46 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
 pdfxc_status pdfxc_ss_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
                               const double* w_single, double* w_out);
 
+/* Grid generation on the device (DfGenerateGrid::generateGrid_atom,
+ * src/libpdf/DfGenerateGrid.cpp:934-1091): per atom and radial shell i = 1..nrad an
+ * abscissa r_i and weight w_i (Gauss-Chebyshev of the second kind with a Becke, Treutler-
+ * Ahlrichs or Knowles-Kaltenborn map, :1612-1655, or Euler-Maclaurin, :1597-1610) scaled
+ * by the atom's radius; shells with r_i > 30 bohr are dropped (:1005-1007); the angular
+ * order is nang, or pruned (Murray-Handy-Laming with K = 5, rounded down to a tabulated
+ * order, :1658-1688; or the SG-1 regions by atomic number, :1690-1713 and :960-982); the
+ * points are the unit grid of that order rotated by `orientation`, scaled by r_i about
+ * the atom, with weights w_unit * w_i (getSphericalGrids, :1715-1734); then the
+ * partition weights (Becke with optional size adjustment, or Stratmann-Scuseria) and the
+ * weight screen |w| > weight_cutoff (screeningGridsByWeight0, :1979-2004). The result
+ * becomes the context's grid, as after pdfxc_set_grid with owner atoms, in the
+ * reference's point order (atom, shell, angular point); *npts receives its size. The
+ * unit grids are input data (the caller's Lebedev tables). */
+enum { PDFXC_RADIAL_GC = 0, PDFXC_RADIAL_EM = 1 };
+enum { PDFXC_MAP_BECKE = 0, PDFXC_MAP_TA = 1, PDFXC_MAP_KK = 2 };
+enum { PDFXC_PRUNE_NONE = 0, PDFXC_PRUNE_MHL = 1, PDFXC_PRUNE_SG1 = 2 };
+enum { PDFXC_PARTITION_BECKE = 0, PDFXC_PARTITION_SS = 1 };
+typedef struct {
+    int nrad;                   /* radial shells per atom (before the 30 bohr cut) */
+    int nang;                   /* angular order without pruning; the MHL cap */
+    int radial;                 /* PDFXC_RADIAL_* */
+    int mapping;                /* PDFXC_MAP_* (Gauss-Chebyshev only) */
+    int pruning;                /* PDFXC_PRUNE_* */
+    int partition;              /* PDFXC_PARTITION_* */
+    int size_adjust;            /* Becke atomic-size adjustment (Becke partition only) */
+    double weight_cutoff;       /* points with |w| <= weight_cutoff are dropped (the reference: 1e-16) */
+    const double* atom_radius;  /* natom: radial scale and pruning radius (Bragg-Slater; the SG-1 radii for SG-1) */
+    const double* becke_radius; /* natom: size-adjustment radii (Becke partition only) */
+    int n_orders;               /* unit-sphere grids: n_orders orders in ascending order, */
+    const int* orders;          /* and their points, x y z w per row, order after order */
+    const double* unit_grids;
+    const double* orientation;  /* 3 x 3 row-major rotation of the unit grids; NULL = identity */
+} pdfxc_grid_params;
+pdfxc_status pdfxc_generate_grid(pdfxc_ctx* ctx, const pdfxc_grid_params* prm, int64_t* npts);
+
+/* The context's grid in input order: xyzw (npts x 4, final weights) and, when the grid
+ * has owner atoms, atom (npts; may be NULL) -- the grid matrix's first five columns. */
+pdfxc_status pdfxc_get_grid(pdfxc_ctx* ctx, double* xyzw, int* atom);
+
 /* One closed-shell XC build: rho pass + Vxc pass
  * (DfCalcGridX::calcXCIntegForFockAndEnergy, src/libpdf/DfCalcGridX.cpp:2280-2315).
  * PA: n_ao x n_ao alpha density (host). If incremental != 0 the density

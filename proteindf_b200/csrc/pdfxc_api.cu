@@ -582,6 +582,33 @@ pdfxc_status pdfxc_set_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, co
 namespace {
 
 // Partition weights on the device: Becke (ss = false) or Stratmann-Scuseria (ss = true).
+// Partition weights of device-resident points: d_wo = d_ws * P_owner / sum_m P_m (Becke or
+// Stratmann-Scuseria), enqueued on the context's stream; d_br (natom Becke radii) only for Becke.
+void partition_weights_device(pdfxc_ctx* ctx, bool ss, int64_t npts, const double* d_xyz, const int* d_own,
+                              const double* d_ws, const double* d_br, int size_adjust, double* d_wo) {
+    cudaStream_t s = ctx->stream;
+    double* d_pair = nullptr;
+    try {
+        if (ss) {
+            dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
+            pdfxc::launch_ss(ctx->d_atom_xyz, ctx->natom, d_pair, d_pair + (size_t)ctx->natom * ctx->natom, npts,
+                             d_xyz, d_own, d_ws, d_wo, s);
+        } else if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
+            dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
+            pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, d_pair,
+                                    d_pair + (size_t)ctx->natom * ctx->natom, npts, d_xyz, d_own, d_ws, d_wo, s);
+        } else {
+            pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, npts, d_xyz, d_own, d_ws, d_wo, s);
+        }
+        PDFXC_CUDA(cudaGetLastError());
+        PDFXC_CUDA(cudaStreamSynchronize(s));
+    } catch (...) {
+        dev_free(d_pair);
+        throw;
+    }
+    dev_free(d_pair);
+}
+
 pdfxc_status partition_weights(pdfxc_ctx* ctx, bool ss, int64_t npts, const double* xyz, const int* atom,
                                const double* w_single, const double* becke_radius, int size_adjust, double* w_out) {
     const char* name = ss ? "pdfxc_ss_weights" : "pdfxc_becke_weights";
@@ -604,7 +631,7 @@ pdfxc_status partition_weights(pdfxc_ctx* ctx, bool ss, int64_t npts, const doub
                 return PDFXC_ERR_ARG;
             }
         cudaStream_t s = ctx->stream;
-        double *d_xyz = nullptr, *d_ws = nullptr, *d_wo = nullptr, *d_br = nullptr, *d_pair = nullptr;
+        double *d_xyz = nullptr, *d_ws = nullptr, *d_wo = nullptr, *d_br = nullptr;
         int* d_own = nullptr;
         try {
             dev_alloc(&d_xyz, 3 * (size_t)npts);
@@ -617,25 +644,14 @@ pdfxc_status partition_weights(pdfxc_ctx* ctx, bool ss, int64_t npts, const doub
             if (!ss)
                 PDFXC_CUDA(cudaMemcpyAsync(d_br, becke_radius, sizeof(double) * ctx->natom, cudaMemcpyHostToDevice, s));
             PDFXC_CUDA(cudaMemcpyAsync(d_own, atom, sizeof(int) * npts, cudaMemcpyHostToDevice, s));
-            if (ss) {
-                dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
-                pdfxc::launch_ss(ctx->d_atom_xyz, ctx->natom, d_pair, d_pair + (size_t)ctx->natom * ctx->natom, npts,
-                                 d_xyz, d_own, d_ws, d_wo, s);
-            } else if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
-                dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
-                pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, d_pair,
-                                        d_pair + (size_t)ctx->natom * ctx->natom, npts, d_xyz, d_own, d_ws, d_wo, s);
-            } else {
-                pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, npts, d_xyz, d_own, d_ws, d_wo, s);
-            }
-            PDFXC_CUDA(cudaGetLastError());
+            partition_weights_device(ctx, ss, npts, d_xyz, d_own, d_ws, d_br, size_adjust, d_wo);
             PDFXC_CUDA(cudaMemcpyAsync(w_out, d_wo, sizeof(double) * npts, cudaMemcpyDeviceToHost, s));
             PDFXC_CUDA(cudaStreamSynchronize(s));
         } catch (...) {
-            dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own), dev_free(d_pair);
+            dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own);
             throw;
         }
-        dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own), dev_free(d_pair);
+        dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo), dev_free(d_br), dev_free(d_own);
         return PDFXC_OK;
     });
 }
@@ -652,6 +668,198 @@ pdfxc_status pdfxc_becke_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz
 pdfxc_status pdfxc_ss_weights(pdfxc_ctx* ctx, int64_t npts, const double* xyz, const int* atom,
                               const double* w_single, double* w_out) {
     return partition_weights(ctx, true, npts, xyz, atom, w_single, nullptr, 0, w_out);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Radial abscissa and weight of shell i (1-based) of nr: Gauss-Chebyshev of the second kind
+// with the Becke, Treutler-Ahlrichs or Knowles-Kaltenborn map
+// (DfGenerateGrid::getRadialAbscissaAndWeight_GaussChebyshev, src/libpdf/DfGenerateGrid.cpp:1612-1655).
+void radial_gc(double R, int nr, int i, int mapping, double* r, double* w) {
+    const double pi = 3.14159265358979323846;
+    const double n1 = nr + 1.0;
+    const double t = i * pi / n1;
+    const double sn = std::sin(t), cs = std::cos(t);
+    const double ss = sn * sn;
+    const double x = (n1 - 2.0 * i) / n1 + (2.0 / pi) * (1.0 + (2.0 / 3.0) * ss) * cs * sn;
+    const double inv_x1 = 1.0 / (x - 1.0);
+    const double inv_ln2 = 1.0 / std::log(2.0);
+    double jac;
+    if (mapping == PDFXC_MAP_BECKE) {
+        *r = R * (1.0 + x) / (1.0 - x);
+        jac = R * ((x + 1.0) * inv_x1 * inv_x1 - inv_x1);
+    } else if (mapping == PDFXC_MAP_TA) {
+        *r = inv_ln2 * std::log(2.0 * (-inv_x1)) * R;
+        jac = R * inv_ln2 / (1.0 - x);
+    } else {
+        *r = inv_ln2 * std::log(2.0 * (-inv_x1));
+        jac = inv_ln2 / (1.0 - x);
+    }
+    *w = (16.0 / (3.0 * n1)) * ss * ss * jac * *r * *r * 4.0 * pi;
+}
+
+// Euler-Maclaurin (DfGenerateGrid::getRadialAbscissaAndWeight_EulerMaclaurin, :1597-1610).
+void radial_em(double R, int nr, int i, double* r, double* w) {
+    const double pi = 3.14159265358979323846;
+    const double inv = 1.0 / double(nr + 1 - i);
+    *r = R * double(i * i) * inv * inv;
+    const double i5 = double((long long)i * i * i * i * i);
+    *w = 2.0 * std::pow(R, 3) * double(nr + 1) * i5 * std::pow(inv, 7) * 4.0 * pi;
+}
+
+// Angular order of a shell at r_i: nang without pruning; Murray-Handy-Laming with K = 5
+// (min(int(5 r / R * nang), nang), rounded down to a tabulated order or the smallest,
+// :1658-1688); SG-1 regions of r / R by atomic number (:1690-1713, parameters :960-982).
+int angular_order(int pruning, double r, double R, int nang, int Z, const std::vector<int>& orders) {
+    if (pruning == PDFXC_PRUNE_SG1) {
+        double a[4] = {0.0, 0.0, 0.0, 10000.0};
+        if (Z == 1 || Z == 2) a[0] = 0.25, a[1] = 0.5, a[2] = 1.0, a[3] = 4.5;
+        else if (Z >= 3 && Z <= 10) a[0] = 0.1667, a[1] = 0.5, a[2] = 0.9, a[3] = 3.5;
+        else if (Z >= 11 && Z <= 18) a[0] = 0.1, a[1] = 0.4, a[2] = 0.8, a[3] = 2.5;
+        const double q = r * (1.0 / R);
+        if (q < a[1]) return q < a[0] ? 6 : 38;
+        if (q < a[2]) return 86;
+        return q < a[3] ? 194 : 86;
+    }
+    int n = nang;
+    if (pruning == PDFXC_PRUNE_MHL) n = std::min<int>((5.0 * r / R) * nang, nang);
+    const auto it = std::upper_bound(orders.begin(), orders.end(), n);
+    return it == orders.begin() ? orders[0] : *(it - 1);
+}
+
+}  // namespace
+
+extern "C" {
+
+pdfxc_status pdfxc_generate_grid(pdfxc_ctx* ctx, const pdfxc_grid_params* prm, int64_t* npts_out) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (ctx->natom == 0) {
+            ctx->err = "pdfxc_generate_grid: call pdfxc_set_system first";
+            return PDFXC_ERR_STATE;
+        }
+        if (!prm || prm->nrad <= 0 || prm->n_orders <= 0 || !prm->orders || !prm->unit_grids || !prm->atom_radius ||
+            prm->radial < PDFXC_RADIAL_GC || prm->radial > PDFXC_RADIAL_EM || prm->mapping < PDFXC_MAP_BECKE ||
+            prm->mapping > PDFXC_MAP_KK || prm->pruning < PDFXC_PRUNE_NONE || prm->pruning > PDFXC_PRUNE_SG1 ||
+            (prm->partition != PDFXC_PARTITION_BECKE && prm->partition != PDFXC_PARTITION_SS) ||
+            (prm->partition == PDFXC_PARTITION_BECKE && !prm->becke_radius)) {
+            ctx->err = "pdfxc_generate_grid: missing table or parameter out of range";
+            return PDFXC_ERR_ARG;
+        }
+        const int natom = ctx->natom;
+        std::vector<int> orders(prm->orders, prm->orders + prm->n_orders);
+        std::vector<int64_t> urow(orders.size());
+        int64_t nrows = 0;
+        for (size_t k = 0; k < orders.size(); ++k) {
+            if (orders[k] <= 0 || (k > 0 && orders[k] <= orders[k - 1])) {
+                ctx->err = "pdfxc_generate_grid: unit-grid orders must be positive and ascending";
+                return PDFXC_ERR_ARG;
+            }
+            urow[k] = nrows;
+            nrows += orders[k];
+        }
+        for (int a = 0; a < natom; ++a)
+            if (!(prm->atom_radius[a] > 0.0) || (prm->pruning == PDFXC_PRUNE_SG1 && ctx->h_atom_z[a] <= 0)) {
+                ctx->err = "pdfxc_generate_grid: atom radius not positive (or SG-1 without atomic numbers)";
+                return PDFXC_ERR_ARG;
+            }
+        // shells (host: O(natom nrad)), then the points and weights on the device
+        std::vector<pdfxc::GridShell> shells;
+        int64_t np = 0;
+        for (int a = 0; a < natom; ++a) {
+            const double R = prm->atom_radius[a];
+            for (int i = 1; i <= prm->nrad; ++i) {
+                double r, wr;
+                if (prm->radial == PDFXC_RADIAL_GC) radial_gc(R, prm->nrad, i, prm->mapping, &r, &wr);
+                else radial_em(R, prm->nrad, i, &r, &wr);
+                if (r > 30.0) continue;
+                const int n = angular_order(prm->pruning, r, R, prm->nang, ctx->h_atom_z[a], orders);
+                const auto it = std::lower_bound(orders.begin(), orders.end(), n);
+                if (it == orders.end() || *it != n) {
+                    ctx->err = "pdfxc_generate_grid: angular order " + std::to_string(n) + " is not tabulated";
+                    return PDFXC_ERR_ARG;
+                }
+                shells.push_back(pdfxc::GridShell{a, n, urow[it - orders.begin()], np, r, wr});
+                np += n;
+            }
+        }
+        cudaStream_t s = ctx->stream;
+        const double ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+        std::vector<double> O(prm->orientation ? prm->orientation : ident, (prm->orientation ? prm->orientation : ident) + 9);
+        pdfxc::GridShell* d_sh = nullptr;
+        double *d_unit = nullptr, *d_O = nullptr, *d_xyz = nullptr, *d_ws = nullptr, *d_wo = nullptr, *d_br = nullptr;
+        int* d_own = nullptr;
+        std::vector<double> xyz(3 * (size_t)np), w((size_t)np);
+        std::vector<int> own((size_t)np);
+        try {
+            upload(&d_sh, shells, s);
+            upload(&d_unit, std::vector<double>(prm->unit_grids, prm->unit_grids + 4 * nrows), s);
+            upload(&d_O, O, s);
+            dev_alloc(&d_xyz, 3 * (size_t)np);
+            dev_alloc(&d_ws, (size_t)np);
+            dev_alloc(&d_wo, (size_t)np);
+            dev_alloc(&d_own, (size_t)np);
+            pdfxc::launch_grid_points(d_sh, (int)shells.size(), d_unit, d_O, ctx->d_atom_xyz, d_xyz, d_ws, d_own, s);
+            PDFXC_LAUNCHED("k_grid_points");
+            if (prm->partition == PDFXC_PARTITION_BECKE)
+                upload(&d_br, std::vector<double>(prm->becke_radius, prm->becke_radius + natom), s);
+            partition_weights_device(ctx, prm->partition == PDFXC_PARTITION_SS, np, d_xyz, d_own, d_ws, d_br,
+                                     prm->size_adjust, d_wo);
+            PDFXC_CUDA(cudaMemcpyAsync(xyz.data(), d_xyz, sizeof(double) * xyz.size(), cudaMemcpyDeviceToHost, s));
+            PDFXC_CUDA(cudaMemcpyAsync(w.data(), d_wo, sizeof(double) * w.size(), cudaMemcpyDeviceToHost, s));
+            PDFXC_CUDA(cudaMemcpyAsync(own.data(), d_own, sizeof(int) * own.size(), cudaMemcpyDeviceToHost, s));
+            PDFXC_CUDA(cudaStreamSynchronize(s));
+        } catch (...) {
+            dev_free(d_sh), dev_free(d_unit), dev_free(d_O), dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo);
+            dev_free(d_br), dev_free(d_own);
+            throw;
+        }
+        dev_free(d_sh), dev_free(d_unit), dev_free(d_O), dev_free(d_xyz), dev_free(d_ws), dev_free(d_wo);
+        dev_free(d_br), dev_free(d_own);
+        // the weight screen, in point order
+        std::vector<double> xyzw;
+        std::vector<int> atom;
+        xyzw.reserve(4 * (size_t)np);
+        atom.reserve((size_t)np);
+        for (int64_t i = 0; i < np; ++i)
+            if (std::fabs(w[i]) > prm->weight_cutoff) {
+                xyzw.insert(xyzw.end(), {xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2], w[i]});
+                atom.push_back(own[i]);
+            }
+        const int64_t n = (int64_t)atom.size();
+        if (n == 0) {
+            ctx->err = "pdfxc_generate_grid: every point was screened out";
+            return PDFXC_ERR_ARG;
+        }
+        const pdfxc_status st = pdfxc_set_grid(ctx, n, xyzw.data(), atom.data());
+        if (st == PDFXC_OK && npts_out) *npts_out = n;
+        return st;
+    });
+}
+
+pdfxc_status pdfxc_get_grid(pdfxc_ctx* ctx, double* xyzw, int* atom) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!xyzw) return PDFXC_ERR_ARG;
+        if (ctx->nblk == 0) {
+            ctx->err = "pdfxc_get_grid: no grid";
+            return PDFXC_ERR_STATE;
+        }
+        const size_t nslot = (size_t)ctx->nblk * BLOCK_PTS;
+        std::vector<double> c[4] = {std::vector<double>(nslot), std::vector<double>(nslot), std::vector<double>(nslot),
+                                    std::vector<double>(nslot)};
+        const double* src[4] = {ctx->d_px, ctx->d_py, ctx->d_pz, ctx->d_pw};
+        for (int k = 0; k < 4; ++k)
+            PDFXC_CUDA(cudaMemcpyAsync(c[k].data(), src[k], sizeof(double) * nslot, cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        for (size_t slot = 0; slot < nslot; ++slot) {
+            const int64_t i = ctx->h_src[slot];
+            if (i < 0) continue;
+            for (int k = 0; k < 4; ++k) xyzw[4 * i + k] = c[k][slot];
+            if (atom && !ctx->h_owner.empty()) atom[i] = ctx->h_owner[slot];
+        }
+        return PDFXC_OK;
+    });
 }
 
 }  // extern "C"

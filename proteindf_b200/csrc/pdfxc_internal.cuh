@@ -68,6 +68,14 @@ struct __align__(16) RowGeom {
     int pad;
 };
 
+// One radial shell of an atom-centred grid: n points from the unit grid rows [u0, u0 + n),
+// abscissa r and radial weight wr, written to points [p0, p0 + n).
+struct GridShell {
+    int atom, n;
+    int64_t u0, p0;
+    double r, wr;
+};
+
 // A workspace layout for a build with its own number of [nbp][BLOCK_PTS] FP64 planes per
 // block (the XC gradient, the open-shell build): per-block offsets, chunks, workspace.
 struct Plan {
@@ -166,6 +174,10 @@ struct pdfxc_ctx {
 };
 
 namespace pdfxc {
+
+// gridgen.cu: the points and single-centre weights of the shells
+void launch_grid_points(const GridShell* shells, int nshell, const double* unit, const double* O,
+                        const double* atom_xyz, double* xyz, double* w, int* owner, cudaStream_t s);
 
 // kernels_fp64.cu
 void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, bool gga,

@@ -32,6 +32,9 @@ _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 # (src/libpdf/DfGenerateGrid.cpp:1958-1968).
 BRAGG_SLATER = {1: 0.25, 6: 0.70, 7: 0.65, 8: 0.60}
 BECKE_RADIUS = {1: 0.35, 6: 0.70, 7: 0.65, 8: 0.60}
+# Radial scales of the SG-1 grid (and of USER grids' gradient grid), as the reference
+# sets them for those grid types (src/libpdf/DfGenerateGrid.cpp:409-418).
+SG1_RADIUS = {1: 1.0000, 6: 1.2308, 7: 1.0256, 8: 0.8791}
 
 _LEB = None
 

@@ -22,13 +22,28 @@ EXPORTS = [
     "pdfxc_last_profile", "pdfxc_set_profiling", "pdfxc_last_error", "pdfxc_destroy", "pdfxc_build_vxc_noalloc",
     "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
     "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
-    "pdfxc_build_vxc_batched", "pdfxc_density",
+    "pdfxc_build_vxc_batched", "pdfxc_density", "pdfxc_generate_grid", "pdfxc_get_grid",
 ]
 
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("block_points", ctypes.c_int), ("ao_cutoff", ctypes.c_double),
                 ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t), ("split_terms", ctypes.c_int)]
+
+
+class GridParams(ctypes.Structure):
+    """pdfxc_grid_params: device grid generation."""
+    _fields_ = [("nrad", ctypes.c_int), ("nang", ctypes.c_int), ("radial", ctypes.c_int), ("mapping", ctypes.c_int),
+                ("pruning", ctypes.c_int), ("partition", ctypes.c_int), ("size_adjust", ctypes.c_int),
+                ("weight_cutoff", ctypes.c_double), ("atom_radius", ctypes.c_void_p), ("becke_radius", ctypes.c_void_p),
+                ("n_orders", ctypes.c_int), ("orders", ctypes.c_void_p), ("unit_grids", ctypes.c_void_p),
+                ("orientation", ctypes.c_void_p)]
+
+
+RADIAL = {"GC": 0, "EM": 1}
+MAPPING = {"BECKE": 0, "TA": 1, "KK": 2}
+PRUNING = {False: 0, True: 1, "MHL": 1, "SG1": 2}
+PARTITION = {"Becke": 0, "SSWeight": 1}
 
 
 class Mol(ctypes.Structure):
@@ -67,6 +82,8 @@ def load_library(path=LIB_PATH):
     L.pdfxc_build_vxc_device.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_get_rho.argtypes = [_vp, i32, _vp]
     L.pdfxc_density.argtypes = [_vp, _vp, i64, _vp, _vp]
+    L.pdfxc_generate_grid.argtypes = [_vp, ctypes.POINTER(GridParams), _vp]
+    L.pdfxc_get_grid.argtypes = [_vp, _vp, _vp]
     L.pdfxc_set_rho.argtypes = [_vp, i32, _vp]
     L.pdfxc_grid_stats.argtypes = [_vp, _vp, _vp, _vp, _vp]
     L.pdfxc_last_profile.argtypes = [_vp, _vp]
@@ -173,6 +190,35 @@ class XcEngine:
         self._check(self.L.pdfxc_set_grid(self.h, len(xyzw), _ptr(xyzw), None if atom is None else _ptr(atom)),
                     "pdfxc_set_grid")
         self.npts = len(xyzw)
+
+    def generate_grid(self, atom_radius, nrad=75, nang=302, radial="GC", mapping="TA", pruning=True,
+                      partition="Becke", becke_radius=None, size_adjust=True, weight_cutoff=1e-16,
+                      orientation=None, unit_grids=None):
+        """Build the grid on the device (DfGenerateGrid::generateGrid_atom) and make it the
+        context's grid. atom_radius: per atom radial scale (Bragg-Slater; the SG-1 radii with
+        pruning="SG1"); unit_grids: {order: (n, 4) x y z w} (default: the package's Lebedev
+        tables). Returns the number of points."""
+        from . import grids
+        tabs = grids.lebedev_table() if unit_grids is None else unit_grids
+        orders = np.array(sorted(tabs), dtype=np.int32)
+        unit = np.ascontiguousarray(np.concatenate([np.asarray(tabs[int(n)], dtype=np.float64) for n in orders]))
+        ar = np.ascontiguousarray(atom_radius, dtype=np.float64)
+        br = None if becke_radius is None else np.ascontiguousarray(becke_radius, dtype=np.float64)
+        O = None if orientation is None else np.ascontiguousarray(orientation, dtype=np.float64).reshape(3, 3)
+        prm = GridParams(nrad, nang, RADIAL[radial], MAPPING[mapping], PRUNING[pruning], PARTITION[partition],
+                         int(size_adjust), weight_cutoff, _ptr(ar), None if br is None else _ptr(br), len(orders),
+                         _ptr(orders), _ptr(unit), None if O is None else _ptr(O))
+        n = ctypes.c_int64(0)
+        self._check(self.L.pdfxc_generate_grid(self.h, ctypes.byref(prm), ctypes.byref(n)), "pdfxc_generate_grid")
+        self.npts = n.value
+        return n.value
+
+    def get_grid(self):
+        """The context's grid in input order: (xyzw (n, 4), atom (n,))."""
+        xyzw = np.zeros((self.npts, 4))
+        atom = np.full(self.npts, -1, dtype=np.int32)
+        self._check(self.L.pdfxc_get_grid(self.h, _ptr(xyzw), _ptr(atom)), "pdfxc_get_grid")
+        return xyzw, atom
 
     def becke_weights(self, xyz, atom, w_single, becke_radius, size_adjust=True):
         xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
