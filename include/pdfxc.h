@@ -137,7 +137,8 @@ typedef struct {
     int partition;              /* PDFXC_PARTITION_* */
     int size_adjust;            /* Becke atomic-size adjustment (Becke partition only) */
     double weight_cutoff;       /* points with |w| <= weight_cutoff are dropped (the reference: 1e-16) */
-    const double* atom_radius;  /* natom: radial scale and pruning radius (Bragg-Slater; the SG-1 radii for SG-1) */
+    const double* atom_radius;  /* natom: radial scale and pruning radius (Bragg-Slater; the SG-1 radii for SG-1);
+                                   0 = no grid on that atom (the reference skips dummy atoms) */
     const double* becke_radius; /* natom: size-adjustment radii (Becke partition only) */
     int n_orders;               /* unit-sphere grids: n_orders orders in ascending order, */
     const int* orders;          /* and their points, x y z w per row, order after order */

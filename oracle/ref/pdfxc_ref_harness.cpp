@@ -551,6 +551,7 @@ int runLebedev(const char* outPath) {
 // rho columns of the first are read back from the grid-matrix file).
 }  // namespace
 #include "DfCalcGridX_B200.h"
+#include "DfGenerateGrid_B200.h"
 namespace {
 
 class GridFileWriter : public DfObject {
@@ -682,6 +683,43 @@ int runDropinUks(const Case& c, const char* outPath) {
 
 // The XC nuclear gradient through both classes' energyGradient (each builds the
 // SG-1 gradient grid itself), then DfCalcGridX_B200 with the grid-weight term on.
+// The grid matrix of iteration 0 (DfObject keeps its loader protected).
+struct GridMatrixReader : public DfObject {
+    explicit GridMatrixReader(TlSerializeData* p) : DfObject(p) {}
+    TlDenseGeneralMatrix_Lapack read() { return this->getGridMatrix<TlDenseGeneralMatrix_Lapack>(0); }
+};
+
+std::vector<double> rowMajor(const TlDenseGeneralMatrix_Lapack& G) {
+    std::vector<double> v;
+    for (TlMatrixObject::index_type i = 0; i < G.getNumOfRows(); ++i)
+        for (TlMatrixObject::index_type j = 0; j < G.getNumOfCols(); ++j) v.push_back(G.get(i, j));
+    return v;
+}
+
+// The grid producer: the reference's DfGenerateGrid::dfGrdMain, then DfGenerateGrid_B200's,
+// each writing the grid matrix of iteration 0 (read back after each).
+int runDropinGenGrid(const Case& c, const char* outPath) {
+    TlSerializeData param = makeParam(c);
+    const TlOrbitalInfo orbProbe(param["coordinates"], param["basis_set"]);
+    param["num_of_AOs"] = orbProbe.getNumOfOrbitals();
+    Out out(outPath);
+    {
+        DfGenerateGrid g(&param);
+        g.dfGrdMain();
+        const TlDenseGeneralMatrix_Lapack G = GridMatrixReader(&param).read();
+        out.put("ref_grid", rowMajor(G));
+        out.put("ref_ncol", (double)G.getNumOfCols());
+    }
+    {
+        DfGenerateGrid_B200 g(&param);
+        g.dfGrdMain();
+        const TlDenseGeneralMatrix_Lapack G = GridMatrixReader(&param).read();
+        out.put("b200_grid", rowMajor(G));
+        out.put("b200_ncol", (double)G.getNumOfCols());
+    }
+    return 0;
+}
+
 // gridDensity through both classes; the B200 class also through its batched form.
 int runDropinDensity(const Case& c, const char* outPath) {
     TlSerializeData param = makeParam(c);
@@ -768,6 +806,7 @@ int main(int argc, char** argv) {
     if (mode == "density") return runDensity(c, argv[3]);
 #ifdef PDFXC_DROPIN
     if (mode == "dropin_density") return runDropinDensity(c, argv[3]);
+    if (mode == "dropin_gengrid") return runDropinGenGrid(c, argv[3]);
     if (mode == "dropin") return runDropin(c, argv[3]);
     if (mode == "dropin_grad") return runDropinGrad(c, argv[3]);
     if (mode == "dropin_uks") return runDropinUks(c, argv[3]);

@@ -194,6 +194,20 @@ def run_dropin_density(workdir, symbols, charges, xyz_bohr, basis, P, points, ti
     return read_records(out)
 
 
+def run_dropin_gengrid(workdir, symbols, charges, xyz_bohr, basis, grid_kv, timeout=None):
+    """The grid producer: DfGenerateGrid::dfGrdMain of the reference, then DfGenerateGrid_B200's,
+    on the same parameter set (grid_kv: grid_type, nrad, nang, radial, gc_mapping, partition,
+    pruning). Returns (ref_grid, b200_grid) as (rows, ncol) arrays of the grid matrix."""
+    os.makedirs(os.path.join(workdir, "fl_Work"), exist_ok=True)
+    case = os.path.join(workdir, "gengrid.txt")
+    write_case(case, symbols, charges, xyz_bohr, basis, dict(grid_kv, functional="SVWN"))
+    out = os.path.join(workdir, "dropin_gengrid.bin")
+    subprocess.run([DROPIN_BIN, "dropin_gengrid", case, out], check=True, timeout=timeout, cwd=workdir,
+                   stdout=subprocess.DEVNULL, env=_dropin_env())
+    r = read_records(out)
+    return (r["ref_grid"].reshape(-1, int(r["ref_ncol"][0])), r["b200_grid"].reshape(-1, int(r["b200_ncol"][0])))
+
+
 def run_dropin_uks(workdir, symbols, charges, xyz_bohr, basis, functional, grid5, PA, PB, timeout=None):
     """The open-shell overloads of the reference DfCalcGridX and of DfCalcGridX_B200, two
     SCF iterations (PA/2, PB/2, then the same again with xc-update)."""

@@ -760,8 +760,9 @@ pdfxc_status pdfxc_generate_grid(pdfxc_ctx* ctx, const pdfxc_grid_params* prm, i
             nrows += orders[k];
         }
         for (int a = 0; a < natom; ++a)
-            if (!(prm->atom_radius[a] > 0.0) || (prm->pruning == PDFXC_PRUNE_SG1 && ctx->h_atom_z[a] <= 0)) {
-                ctx->err = "pdfxc_generate_grid: atom radius not positive (or SG-1 without atomic numbers)";
+            if (!(prm->atom_radius[a] >= 0.0) ||
+                (prm->atom_radius[a] > 0.0 && prm->pruning == PDFXC_PRUNE_SG1 && ctx->h_atom_z[a] <= 0)) {
+                ctx->err = "pdfxc_generate_grid: atom radius negative (or SG-1 without atomic numbers)";
                 return PDFXC_ERR_ARG;
             }
         // shells (host: O(natom nrad)), then the points and weights on the device
@@ -769,6 +770,7 @@ pdfxc_status pdfxc_generate_grid(pdfxc_ctx* ctx, const pdfxc_grid_params* prm, i
         int64_t np = 0;
         for (int a = 0; a < natom; ++a) {
             const double R = prm->atom_radius[a];
+            if (R == 0.0) continue;  // no grid on this atom (a dummy atom of the reference)
             for (int i = 1; i <= prm->nrad; ++i) {
                 double r, wr;
                 if (prm->radial == PDFXC_RADIAL_GC) radial_gc(R, prm->nrad, i, prm->mapping, &r, &wr);
@@ -783,6 +785,10 @@ pdfxc_status pdfxc_generate_grid(pdfxc_ctx* ctx, const pdfxc_grid_params* prm, i
                 shells.push_back(pdfxc::GridShell{a, n, urow[it - orders.begin()], np, r, wr});
                 np += n;
             }
+        }
+        if (np == 0) {
+            ctx->err = "pdfxc_generate_grid: every point was screened out (no atom has a grid)";
+            return PDFXC_ERR_ARG;
         }
         cudaStream_t s = ctx->stream;
         const double ident[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};

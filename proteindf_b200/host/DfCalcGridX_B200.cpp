@@ -12,6 +12,7 @@
 #include "DfGenerateGrid.h"
 #include "TlPrdctbl.h"
 #include "TlUtils.h"
+#include "pdfxc_system.h"
 
 namespace {
 
@@ -30,36 +31,10 @@ DfCalcGridX_B200::DfCalcGridX_B200(TlSerializeData* pPdfParam, int device, int p
     opt.rho_cutoff = this->inputtedDensityCutoffValue_;  // xc-density-threshold
     check(pdfxc_create(&ctx_, device, &opt), nullptr, "pdfxc_create");
 
-    // shells from the reference's orbital table: a shell starts at its first
-    // component (basis type L*L); exponents and normalised coefficients are
-    // TlOrbitalInfo's own (src/libpdf/TlOrbitalInfoObject.cpp:38-99)
-    const TlOrbitalInfo& orb = this->m_tlOrbInfo;
-    const int natom = orb.getNumOfAtoms();
-    std::vector<double> xyz(3 * natom, 0.0);
-    std::vector<int> z(natom, 0);
-    std::vector<int> shAtom, shL, shNprim;
-    std::vector<double> pExp, pCoef;
-    const int nao = orb.getNumOfOrbitals();
-    for (int ao = 0; ao < nao; ++ao) {
-        const int a = orb.getAtomIndex(ao);
-        const TlPosition r = orb.getPosition(ao);
-        xyz[3 * a] = r.x(), xyz[3 * a + 1] = r.y(), xyz[3 * a + 2] = r.z();
-        z[a] = (int)orb.getAtomCharge(ao);
-        const int L = orb.getShellType(ao);
-        if (orb.getBasisType(ao) != L * L) continue;  // not the first component
-        shAtom.push_back(a);
-        shL.push_back(L);
-        const int np = orb.getCgtoContraction(ao);
-        shNprim.push_back(np);
-        for (int k = 0; k < np; ++k) {
-            pExp.push_back(orb.getExponent(ao, k));
-            pCoef.push_back(orb.getCoefficient(ao, k));
-        }
-    }
-    check(pdfxc_set_system(ctx_, natom, xyz.data(), z.data(), (int)shAtom.size(), shAtom.data(), shL.data(),
-                           shNprim.data(), pExp.data(), pCoef.data()),
-          ctx_, "pdfxc_set_system");
-    sysXyz_ = xyz, sysZ_ = z, shAtom_ = shAtom, shL_ = shL, shNprim_ = shNprim, pExp_ = pExp, pCoef_ = pCoef;
+    const PdfxcSystem sys(this->m_tlOrbInfo);
+    check(sys.setOn(ctx_), ctx_, "pdfxc_set_system");
+    sysXyz_ = sys.xyz, sysZ_ = sys.z, shAtom_ = sys.shAtom, shL_ = sys.shL, shNprim_ = sys.shNprim;
+    pExp_ = sys.pExp, pCoef_ = sys.pCoef;
 }
 
 DfCalcGridX_B200::~DfCalcGridX_B200() {

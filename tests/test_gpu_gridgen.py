@@ -6,6 +6,7 @@ import numpy as np
 import pytest
 
 from conftest import golden, shell_table
+from oracle import refio
 
 pytestmark = pytest.mark.gpu
 
@@ -117,5 +118,45 @@ def test_generate_grid_errors(water2):
         e.generate_grid([grids.SG1_RADIUS[z] for z in Z], partition="SSWeight", nrad=50, radial="EM",
                         pruning="SG1", unit_grids={6: grids.lebedev_table()[6], 590: grids.lebedev_table()[590]})
     with pytest.raises(RuntimeError, match="radius"):
+        e.generate_grid([-1.0] * len(Z), partition="SSWeight")
+    with pytest.raises(RuntimeError, match="screened out"):  # radius 0: no grid on any atom
         e.generate_grid([0.0] * len(Z), partition="SSWeight")
     e.close()
+
+
+def _match_grids(ref, b200):
+    """Rows of the two grid matrices matched by position (the weight screens may differ on a
+    point whose weight sits at the cut); returns (ref rows, b200 rows, unmatched weights)."""
+    from scipy.spatial import cKDTree
+    d, idx = cKDTree(b200[:, :3]).query(ref[:, :3])
+    hit = d <= 1e-9
+    lost = np.concatenate([ref[~hit, 3], np.delete(b200[:, 3], idx[hit])])
+    return ref[hit], b200[idx[hit]], lost
+
+
+@pytest.mark.skipif(not refio.dropin_available(), reason="oracle/_ref/pdfxc_dropin not built")
+@pytest.mark.parametrize("kv", [
+    dict(grid_type="USER", nrad=75, nang=302, radial="GC", gc_mapping="TA", partition="Becke", pruning="yes"),
+    dict(grid_type="USER", nrad=40, nang=194, radial="GC", gc_mapping="BECKE", partition="SSWeight", pruning="no"),
+    dict(grid_type="FINE"),
+    dict(grid_type="SG-1"),
+], ids=["user-becke-ta", "user-ss-becke-map", "fine", "sg1"])
+def test_dfgenerategrid_b200_matches_reference_producer(tmp_path, water2, kv):
+    """DfGenerateGrid_B200::dfGrdMain beside the reference's DfGenerateGrid::dfGrdMain: the
+    same parameter set, orientation matrix and Lebedev tables, the same grid matrix file
+    (x, y, z, weight, atom, zeroed density columns)."""
+    from proteindf_b200 import basis, systems
+    syms = [str(s) for s in water2["symbols"]]
+    ref, b200 = refio.run_dropin_gengrid(str(tmp_path), syms, systems.nuclear_charges(syms), water2["xyz"],
+                                         basis.load_basis("cc-pVDZ"), kv)
+    assert ref.shape[1] == b200.shape[1] and abs(len(ref) - len(b200)) <= 4
+    r, b, lost = _match_grids(ref, b200)
+    # a point deep in another atom's cell has a partition product of ~1e-17 relative, which
+    # neither side computes to relative accuracy: the screens may differ there, at weights
+    # below 1e-12 (the largest weights are ~1e3)
+    assert np.all(np.abs(lost) <= 1e-12)
+    assert len(r) >= len(ref) - 4
+    assert np.array_equal(r[:, 4], b[:, 4])  # owner atoms
+    assert np.all(r[:, 5:] == 0.0) and np.all(b[:, 5:] == 0.0)
+    assert np.abs(r[:, :3] - b[:, :3]).max() <= 1e-13
+    assert np.all(np.abs(r[:, 3] - b[:, 3]) <= 1e-10 * np.abs(r[:, 3]) + 1e-13 * np.abs(r[:, 3]).max())
