@@ -126,10 +126,8 @@ __global__ void __launch_bounds__(BECKE_T) k_becke_tab(const double* __restrict_
 // Stratmann-Scuseria partition (DfGenerateGrid::calcMultiCenterWeight_SS,
 // src/libpdf/DfGenerateGrid.cpp:1878-1956): s = (1 - g(mu))/2 with g the
 // piecewise polynomial of a = 0.64, no size adjustment. s is exactly 0 for
-// mu > a and exactly 1 for mu < -a, so the product over n for atom m stops at
-// the first zero factor: for atoms m far from the point that happens within a
-// few factors, which keeps large systems near O(N_atom) per point. Atoms in
-// shared memory (x, y, z, unused), 1/R_mn from the pair table.
+// mu >= a and exactly 1 for mu <= -a (the polynomial is -1 / +1 at z = -1 / +1),
+// which bounds the atoms that matter at a point (k_ss); 1/R_mn from the pair table.
 __device__ __forceinline__ double ss_s(double u) {
     constexpr double a = 0.64;
     double g;
@@ -144,28 +142,46 @@ __device__ __forceinline__ double ss_s(double u) {
     return 0.5 * (1.0 - g);
 }
 
+// One thread per point. For a point r owned by atom A at distance d, an atom m can have
+// P_m = prod_n s(mu_mn) != 0 only if |A - m| < 2 d / (1 - a) (otherwise mu_mA >= a, s = 0), and
+// a factor s(mu_mn) can differ from 1 only if |m - n| < 2 |r - m| / (1 - a) (otherwise
+// mu_mn <= -a, s = 1): both bounds from |r - n| >= |m - n| - |r - m|, and s is exactly 0 / 1 at
+// +-a. So the candidates m are A and A's neighbours up to 2 d / (1 - a), and the factors of P_m
+// come from m's neighbours up to 2 |r - m| / (1 - a), each list sorted by distance; the
+// skipped factors are exactly 1 and the skipped terms exactly 0. Points deep inside their
+// owner's cell see no candidate and no factor (w = w_single). nbr_idx / nbr_dist: per atom the
+// other atoms in ascending distance (natom - 1 entries).
 __global__ void __launch_bounds__(128) k_ss(const double* __restrict__ atom_xyz, int natom,
-                                            const double* __restrict__ inv, int64_t npts,
+                                            const double* __restrict__ inv, const int* __restrict__ nbr_idx,
+                                            const double* __restrict__ nbr_dist, int64_t npts,
                                             const double* __restrict__ xyz, const int* __restrict__ owner,
                                             const double* __restrict__ w_single, double* __restrict__ w_out) {
-    extern __shared__ double4 atoms[];
-    for (int a = threadIdx.x; a < natom; a += blockDim.x)
-        atoms[a] = make_double4(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2], 0.0);
-    __syncthreads();
+    constexpr double kReach = 2.0 / (1.0 - 0.64);
+    const int nn = natom - 1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
         const double rx = xyz[3 * i], ry = xyz[3 * i + 1], rz = xyz[3 * i + 2];
         const int own = owner[i];
+        auto dist = [&](int a) {
+            const double dx = rx - atom_xyz[3 * a], dy = ry - atom_xyz[3 * a + 1], dz = rz - atom_xyz[3 * a + 2];
+            return sqrt(dx * dx + dy * dy + dz * dz);
+        };
+        const double lim_own = kReach * dist(own);
         double tot = 0.0, pown = 0.0;
-        for (int m = 0; m < natom; ++m) {
-            const double4 A = atoms[m];
-            const double rm = sqrt((rx - A.x) * (rx - A.x) + (ry - A.y) * (ry - A.y) + (rz - A.z) * (rz - A.z));
+        for (int k = -1; k < nn; ++k) {
+            int m = own;
+            if (k >= 0) {
+                if (nbr_dist[(size_t)own * nn + k] >= lim_own) break;
+                m = nbr_idx[(size_t)own * nn + k];
+            }
+            const double rm = dist(m), lim_m = kReach * rm;
             const double* im = inv + (size_t)m * natom;
+            const int* ni = nbr_idx + (size_t)m * nn;
+            const double* nd = nbr_dist + (size_t)m * nn;
             double p = 1.0;
-            for (int n = 0; n < natom && p != 0.0; ++n) {
-                if (n == m) continue;
-                const double4 B = atoms[n];
-                const double rn = sqrt((rx - B.x) * (rx - B.x) + (ry - B.y) * (ry - B.y) + (rz - B.z) * (rz - B.z));
-                p *= ss_s((rm - rn) * __ldg(im + n));
+            for (int j = 0; j < nn && p != 0.0; ++j) {
+                if (nd[j] >= lim_m) break;
+                const int n = ni[j];
+                p *= ss_s((rm - dist(n)) * __ldg(im + n));
             }
             tot += p;
             if (m == own) pown = p;
@@ -176,16 +192,16 @@ __global__ void __launch_bounds__(128) k_ss(const double* __restrict__ atom_xyz,
 
 }  // namespace
 
-void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, int64_t npts, const double* xyz,
-               const int* owner, const double* w_single, double* w_out, cudaStream_t s) {
+void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, const int* nbr_idx,
+               const double* nbr_dist, int64_t npts, const double* xyz, const int* owner, const double* w_single,
+               double* w_out, cudaStream_t s) {
     k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, atom_xyz, natom, 0, inv, adj);
     const int threads = 128;
     int64_t blocks = (npts + threads - 1) / threads;
     if (blocks > 148 * 64) blocks = 148 * 64;
     if (blocks < 1) blocks = 1;
-    const size_t smem = sizeof(double4) * natom;
-    cudaFuncSetAttribute(k_ss, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_ss<<<(unsigned)blocks, threads, smem, s>>>(atom_xyz, natom, inv, npts, xyz, owner, w_single, w_out);
+    k_ss<<<(unsigned)blocks, threads, 0, s>>>(atom_xyz, natom, inv, nbr_idx, nbr_dist, npts, xyz, owner, w_single,
+                                              w_out);
 }
 
 void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,

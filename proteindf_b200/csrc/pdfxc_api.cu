@@ -268,6 +268,7 @@ pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
             ctx->err = "pdfxc_set_system: empty system or null pointer";
             return PDFXC_ERR_ARG;
         }
+        dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);  // neighbour lists of the old geometry
         ctx->natom = natom;
         ctx->nshell = nshell;
         ctx->h_atom_xyz.assign(atom_xyz, atom_xyz + 3 * natom);
@@ -590,9 +591,30 @@ void partition_weights_device(pdfxc_ctx* ctx, bool ss, int64_t npts, const doubl
     double* d_pair = nullptr;
     try {
         if (ss) {
+            const int na = ctx->natom, nn = na - 1;
+            if (!ctx->d_nbr_idx && nn > 0) {  // once per system: neighbour lists by distance
+                std::vector<int> idx((size_t)na * nn);
+                std::vector<double> dst((size_t)na * nn);
+                std::vector<std::pair<double, int>> row(nn);
+                for (int m = 0; m < na; ++m) {
+                    const double* A = &ctx->h_atom_xyz[3 * m];
+                    int k = 0;
+                    for (int n = 0; n < na; ++n) {
+                        if (n == m) continue;
+                        const double* B = &ctx->h_atom_xyz[3 * n];
+                        row[k++] = {std::sqrt((A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) +
+                                              (A[2] - B[2]) * (A[2] - B[2])),
+                                    n};
+                    }
+                    std::sort(row.begin(), row.end());
+                    for (int j = 0; j < nn; ++j) idx[(size_t)m * nn + j] = row[j].second, dst[(size_t)m * nn + j] = row[j].first;
+                }
+                upload(&ctx->d_nbr_idx, idx, s);
+                upload(&ctx->d_nbr_dist, dst, s);
+            }
             dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
-            pdfxc::launch_ss(ctx->d_atom_xyz, ctx->natom, d_pair, d_pair + (size_t)ctx->natom * ctx->natom, npts,
-                             d_xyz, d_own, d_ws, d_wo, s);
+            pdfxc::launch_ss(ctx->d_atom_xyz, ctx->natom, d_pair, d_pair + (size_t)ctx->natom * ctx->natom,
+                             ctx->d_nbr_idx, ctx->d_nbr_dist, npts, d_xyz, d_own, d_ws, d_wo, s);
         } else if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
             dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
             pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, d_pair,
@@ -1627,6 +1649,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_grid(ctx);
     dev_free(ctx->d_atom_xyz), dev_free(ctx->d_p_exp), dev_free(ctx->d_p_coef);
+    dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
     dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
     dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b), dev_free(ctx->d_scalars_b);

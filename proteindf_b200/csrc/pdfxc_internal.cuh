@@ -138,6 +138,8 @@ struct pdfxc_ctx {
     double* d_Vacc = nullptr;     // n_ao^2 non-symmetric accumulator
     bool rho_valid = false;
     pdfxc_ctx* dens = nullptr;  // pdfxc_density: FP64 context over the requested points (same system)
+    int* d_nbr_idx = nullptr;     // Stratmann-Scuseria weights: per atom the other atoms by distance
+    double* d_nbr_dist = nullptr;
     int rho_gga = 0;
 
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -220,8 +222,10 @@ void launch_grad_weight(const double* atom_xyz, int natom, const double* inv, co
 
 // becke.cu
 // Stratmann-Scuseria weights (n_atom <= 6000: atoms in shared memory); inv/adj: n_atom^2 scratch each
-void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, int64_t npts, const double* xyz,
-               const int* owner, const double* w_single, double* w_out, cudaStream_t s);
+// nbr_idx / nbr_dist: per atom the other atoms in ascending distance, natom x (natom - 1)
+void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, const int* nbr_idx,
+               const double* nbr_dist, int64_t npts, const double* xyz, const int* owner, const double* w_single,
+               double* w_out, cudaStream_t s);
 void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
                         double* adj, cudaStream_t s);
 void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust,
