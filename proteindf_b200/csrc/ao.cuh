@@ -59,4 +59,42 @@ __device__ __forceinline__ void ao_from_radial(int t, double x, double y, double
     }
 }
 
+// All components of a shell of angular momentum L at once (L = 0, 1, 2; the component order
+// and prefactors of ang_poly1): v[c] = A_c S0 and g[c] = grad A_c S0 - 2 r A_c S1, c < 2L + 1.
+// One branch per shell instead of one per component.
+__device__ __forceinline__ void shell_components(int L, double x, double y, double z, double S0, double S1,
+                                                 double v[5], double gx[5], double gy[5], double gz[5]) {
+    const double u = 2.0 * S1;
+    if (L == 0) {
+        v[0] = S0;
+        gx[0] = -x * u, gy[0] = -y * u, gz[0] = -z * u;
+        return;
+    }
+    if (L == 1) {
+        const double r[3] = {x, y, z};
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double t = r[c] * u;
+            v[c] = r[c] * S0;
+            gx[c] = (c == 0 ? S0 : 0.0) - x * t;
+            gy[c] = (c == 1 ? S0 : 0.0) - y * t;
+            gz[c] = (c == 2 ? S0 : 0.0) - z * t;
+        }
+        return;
+    }
+    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+    const double A[5] = {x * y, z * x, y * z, 0.5 * (x * x - y * y), s3 * (z * z - 0.5 * (x * x + y * y))};
+    const double Ax[5] = {y, z, 0.0, x, -s3 * x};
+    const double Ay[5] = {x, 0.0, z, -y, -s3 * y};
+    const double Az[5] = {0.0, x, y, 0.0, 2.0 * s3 * z};
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        const double t = A[c] * u;
+        v[c] = A[c] * S0;
+        gx[c] = Ax[c] * S0 - x * t;
+        gy[c] = Ay[c] * S0 - y * t;
+        gz[c] = Az[c] * S0 - z * t;
+    }
+}
+
 }  // namespace pdfxc

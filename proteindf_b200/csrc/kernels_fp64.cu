@@ -230,6 +230,149 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int bl
     }
 }
 
+// GGA closed-shell build without stored AO gradients. Layout of a block (doubles):
+// phi [nbp][128], X then Z [nbp][128], then the radial sums S0 [nsh][128] and S1 [nsh][128]
+// (block_ws_doubles_rad). k_ao_eval_rad writes phi and the radial sums; k_rho_functional_rad
+// forms phi and grad phi of every component from the radial sums (ao_from_radial, the
+// formulas of k_ao_eval) in row order, so rho and grad rho are summed as from stored planes,
+// and reads 2 nsh + nb rows per point instead of 5 nbp (and 2 nsh + nbp instead of 4 nbp for Z).
+// The shells' rows, angular momenta and atoms are staged in shared memory, 128 at a time.
+__global__ void __launch_bounds__(256) k_ao_eval_rad(BasisView bas, GridView g, int blk0, char* ws) {
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x & (BLOCK_PTS - 1);
+    const int half = threadIdx.x >> 7;
+    double* phi = reinterpret_cast<double*>(ws + m.ws);
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    double* S0p = phi + 2 * plane;
+    double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
+    const int gp = blk * BLOCK_PTS + p;
+    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
+    for (int i = half; i < m.nsh; i += 2) {
+        const int s = g.blk_shells[m.sh0 + i];
+        const int row0 = g.blk_shell_row[m.sh0 + i];
+        const int a = bas.sh_atom[s];
+        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
+        const int L = bas.sh_l[s], n = 2 * L + 1;
+        double S0, S1;
+        shell_radial<true>(bas, s, x * x + y * y + z * z, S0, S1);
+        S0p[(size_t)i * BLOCK_PTS + p] = S0;
+        S1p[(size_t)i * BLOCK_PTS + p] = S1;
+        for (int c = 0; c < n; ++c) {
+            double v, gx, gy, gz;
+            ao_from_radial<false>(L * L + c, x, y, z, S0, S1, v, gx, gy, gz);
+            phi[(size_t)(row0 + c) * BLOCK_PTS + p] = v;
+        }
+    }
+    for (int r = m.nb + half; r < m.nbp; r += 2) phi[(size_t)r * BLOCK_PTS + p] = 0.0;
+}
+
+struct ShellStage {
+    double ax[128], ay[128], az[128];
+    int row0[128], lq[128];
+};
+
+__device__ __forceinline__ void stage_shells(const BasisView& bas, const GridView& g, const BlockMeta& m, int i0,
+                                             ShellStage& st) {
+    for (int k = threadIdx.x; k < 128 && i0 + k < m.nsh; k += blockDim.x) {
+        const int s = g.blk_shells[m.sh0 + i0 + k];
+        const int a = bas.sh_atom[s];
+        st.ax[k] = bas.atom_xyz[3 * a], st.ay[k] = bas.atom_xyz[3 * a + 1], st.az[k] = bas.atom_xyz[3 * a + 2];
+        st.row0[k] = g.blk_shell_row[m.sh0 + i0 + k];
+        st.lq[k] = bas.sh_l[s];
+    }
+}
+
+__global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional_rad(BasisView bas, GridView g, int blk0, int fn,
+                                                                  int incremental, double rho_cut, char* ws,
+                                                                  double* rho_store, double* coef, double* blk_sum) {
+    __shared__ ShellStage st;
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    double* X = reinterpret_cast<double*>(ws + m.ws) + plane;
+    const double* S0p = X + plane;
+    const double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    double v[5], ax[5], ay[5], az[5];
+    for (int i0 = 0; i0 < m.nsh; i0 += 128) {
+        __syncthreads();
+        stage_shells(bas, g, m, i0, st);
+        __syncthreads();
+        const int kn = min(128, m.nsh - i0);
+        double S0n = S0p[(size_t)i0 * BLOCK_PTS + p], S1n = S1p[(size_t)i0 * BLOCK_PTS + p];
+        for (int k = 0; k < kn; ++k) {
+            const int i = i0 + k;
+            const double S0 = S0n, S1 = S1n;
+            if (k + 1 < kn) S0n = S0p[(size_t)(i + 1) * BLOCK_PTS + p], S1n = S1p[(size_t)(i + 1) * BLOCK_PTS + p];
+            const int L = st.lq[k], row0 = st.row0[k];
+            shell_components(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0, S1, v, ax, ay, az);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                if (c < 2 * L + 1) {
+                    const double xv = X[(size_t)(row0 + c) * BLOCK_PTS + p];
+                    rho = fma(v[c], xv, rho);
+                    gx = fma(ax[c], xv, gx);
+                    gy = fma(ay[c], xv, gy);
+                    gz = fma(az[c], xv, gz);
+                }
+            }
+        }
+    }
+    gx *= 2.0, gy *= 2.0, gz *= 2.0;
+    double* rs = rho_store + gp * 4;
+    if (incremental) {
+        rho += rs[0];
+        gx += rs[1], gy += rs[2], gz += rs[3];
+    }
+    rs[0] = rho, rs[1] = gx, rs[2] = gy, rs[3] = gz;
+    const double w = g.pw[gp];
+    double e = 0.0, a = 0.0, cx = 0.0, cy = 0.0, cz = 0.0;
+    if (w != 0.0 && rho > rho_cut) {
+        const double gam = gx * gx + gy * gy + gz * gz;
+        const XcOut o = eval_functional(fn, rho, rho, gam, gam, gam);
+        e = w * o.f;
+        a = 0.5 * w * o.va;
+        const double cc = w * (2.0 * o.vgaa + o.vgab);
+        cx = cc * gx, cy = cc * gy, cz = cc * gz;
+    }
+    double* cf = coef + gp * 4;
+    cf[0] = a, cf[1] = cx, cf[2] = cy, cf[3] = cz;
+    // Z[nu][p] = 0.5 w vrho phi + c . grad phi over X (every row of X has been read by this thread)
+    for (int i0 = 0; i0 < m.nsh; i0 += 128) {
+        __syncthreads();
+        stage_shells(bas, g, m, i0, st);
+        __syncthreads();
+        const int kn = min(128, m.nsh - i0);
+        double S0n = S0p[(size_t)i0 * BLOCK_PTS + p], S1n = S1p[(size_t)i0 * BLOCK_PTS + p];
+        for (int k = 0; k < kn; ++k) {
+            const int i = i0 + k;
+            const double S0 = S0n, S1 = S1n;
+            if (k + 1 < kn) S0n = S0p[(size_t)(i + 1) * BLOCK_PTS + p], S1n = S1p[(size_t)(i + 1) * BLOCK_PTS + p];
+            const int L = st.lq[k], row0 = st.row0[k];
+            shell_components(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0, S1, v, ax, ay, az);
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                if (c < 2 * L + 1) X[(size_t)(row0 + c) * BLOCK_PTS + p] = a * v[c] + cx * ax[c] + cy * ay[c] + cz * az[c];
+        }
+    }
+    for (int r = m.nb; r < m.nbp; ++r) X[(size_t)r * BLOCK_PTS + p] = 0.0;
+    // block sums in FP64 (deterministic order)
+    __shared__ double red[2][BLOCK_PTS / 32];
+    double se = warp_sum(e), sn = warp_sum(w * rho);
+    if ((p & 31) == 0) red[0][p >> 5] = se, red[1][p >> 5] = sn;
+    __syncthreads();
+    if (p == 0) {
+        double E = 0.0, N = 0.0;
+        for (int q = 0; q < BLOCK_PTS / 32; ++q) E += red[0][q], N += red[1][q];
+        blk_sum[2 * blk] = E;
+        blk_sum[2 * blk + 1] = N;
+    }
+}
+
 // Vacc[aos[m]][aos[n]] += sum_p phi[m][p] Z[n][p]: CTA tile 64 x 64 AOs, K = 128 points in
 // steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles). Z was formed by
 // k_rho_functional in the place of X; both tiles are staged as [row][k] with 128-byte rows.
@@ -441,6 +584,15 @@ void launch_gemm_x_planes(const GridView& g, const double* P, int nao, int blk0,
                           int dst0, int nz, char* ws, cudaStream_t s) {
     dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk, nz);
     k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, src0, dst0);
+}
+
+void launch_ao_eval_rad(const BasisView& b, const GridView& g, int blk0, int nblk, char* ws, cudaStream_t s) {
+    k_ao_eval_rad<<<nblk, 256, 0, s>>>(b, g, blk0, ws);
+}
+
+void launch_rho_functional_rad(const BasisView& b, const GridView& g, int blk0, int nblk, int fn, bool incremental,
+                               double rho_cut, char* ws, double* rho, double* coef, double* blk_sum, cudaStream_t s) {
+    k_rho_functional_rad<<<nblk, BLOCK_PTS, 0, s>>>(b, g, blk0, fn, incremental, rho_cut, ws, rho, coef, blk_sum);
 }
 
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,

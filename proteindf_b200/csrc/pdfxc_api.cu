@@ -443,7 +443,6 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
         Rs[sh] = shell_cutoff_radius(ctx->h_sh_l[sh], &ctx->h_p_exp[ctx->h_sh_p0[sh]], &ctx->h_p_coef[ctx->h_sh_p0[sh]],
                                      ctx->h_sh_nprim[sh], ctx->opt.ao_cutoff);
     std::vector<int> shells, rows, aos, row_info;
-    const bool gga_ws = true;  // size the workspace for gradients (GGA); LDA uses a prefix of it
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
     double flops = 0.0, sum_nb = 0.0;
     for (int gi = 0; gi < ngrp; ++gi) {
@@ -481,7 +480,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     Chunk cur{0, 0, 0, 0};
     auto block_need = [&](int bb) -> size_t {
         const BlockMeta& m = ctx->h_meta[bb];
-        if (!mixed) return pdfxc::block_ws_doubles(m.nbp, gga_ws) * sizeof(double);
+        if (!mixed) return pdfxc::block_ws_doubles_rad(m.nbp, m.nsh) * sizeof(double);
         if (ctx->opt.split_terms != 10) return pdfxc::mixed_layout(m.nbp).total;
         const pdfxc::OzLayout L = pdfxc::oz_layout(m.nbp, m.nsh);
         return m.lead == bb ? L.total_lead : L.total;
@@ -958,18 +957,24 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
             for (int k = 0; k < 5; ++k) PDFXC_CUDA(cudaEventRecord(e[k], s));
             continue;
         }
+        // per block: phi, X (then Z), and for GGA the shells' radial sums (block_ws_doubles_rad)
         PDFXC_CUDA(cudaEventRecord(e[0], s));
-        pdfxc::launch_ao_eval(bv, gv, cb0, nb, gga, ws, 0, s);
+        if (gga) pdfxc::launch_ao_eval_rad(bv, gv, cb0, nb, ws, s);
+        else pdfxc::launch_ao_eval(bv, gv, cb0, nb, false, ws, 0, s);
         PDFXC_LAUNCHED("k_ao_eval");
         PDFXC_CUDA(cudaEventRecord(e[1], s));
-        pdfxc::launch_gemm_x(gv, d_PA, nao, cb0, nb, c.max_nbp, gga ? 4 : 1, ws, s);
+        pdfxc::launch_gemm_x(gv, d_PA, nao, cb0, nb, c.max_nbp, 1, ws, s);
         PDFXC_LAUNCHED("k_gemm_x");
         PDFXC_CUDA(cudaEventRecord(e[2], s));
-        pdfxc::launch_rho_functional(gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho, ctx->d_coef,
-                                     ctx->d_blk_sum, s);
+        if (gga)
+            pdfxc::launch_rho_functional_rad(bv, gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho,
+                                             ctx->d_coef, ctx->d_blk_sum, s);
+        else
+            pdfxc::launch_rho_functional(gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho,
+                                         ctx->d_coef, ctx->d_blk_sum, s);
         PDFXC_LAUNCHED("k_rho_functional");
         PDFXC_CUDA(cudaEventRecord(e[3], s));
-        pdfxc::launch_gemm_v(gv, cb0, nb, c.max_nbp, gga, ctx->d_coef, ws, ctx->d_Vacc, nao, s);
+        pdfxc::launch_gemm_v_plane(gv, cb0, nb, c.max_nbp, 1, ws, ctx->d_Vacc, nao, s);
         PDFXC_LAUNCHED("k_gemm_v");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
         launches += 4;

@@ -189,6 +189,10 @@ void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nb
 // the same contraction over nz planes: plane dst0 + z = P_sub * plane src0 + z
 void launch_gemm_x_planes(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp, int src0,
                           int dst0, int nz, char* ws, cudaStream_t s);
+// the GGA closed-shell build from radial sums (layout block_ws_doubles_rad)
+void launch_ao_eval_rad(const BasisView& b, const GridView& g, int blk0, int nblk, char* ws, cudaStream_t s);
+void launch_rho_functional_rad(const BasisView& b, const GridView& g, int blk0, int nblk, int fn, bool incremental,
+                               double rho_cut, char* ws, double* rho, double* coef, double* blk_sum, cudaStream_t s);
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental,
                            double rho_cut, char* ws, double* rho, double* coef, double* blk_sum,
                            cudaStream_t s);
@@ -243,6 +247,12 @@ size_t becke_tab_max_atoms();
 //   X     [nbp][BLOCK_PTS]           P_sub * phi
 __host__ __device__ inline size_t block_ws_doubles(int nbp, bool gga) {
     return (size_t)nbp * BLOCK_PTS * (gga ? 5 : 2);
+}
+
+// The closed-shell FP64 build: phi and X (then Z) planes, then the shells' radial sums S0, S1
+// (the GGA form; the LDA form uses the two planes only).
+__host__ __device__ inline size_t block_ws_doubles_rad(int nbp, int nsh) {
+    return (size_t)BLOCK_PTS * (2 * (size_t)nbp + 2 * (size_t)nsh);
 }
 
 // Intermediates of one block on the mixed path (byte offsets; nbp % 128 == 0).
