@@ -373,6 +373,85 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional_rad(BasisView bas,
     }
 }
 
+// The same build in three light kernels: rho and sum grad phi X per point (k_rho_rad, into
+// rho_acc), the functional (launch_functional_points), then Z over X (k_z_rad). Each loop over
+// the AO components holds few registers, so that enough warps hide the loads of X and of the
+// radial sums; k_rho_functional_rad keeps all three in one kernel of 138 registers.
+__global__ void __launch_bounds__(BLOCK_PTS, 6) k_rho_rad(BasisView bas, GridView g, int blk0, const char* ws,
+                                                       double* rho_acc) {
+    __shared__ ShellStage st;
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    const double* X = reinterpret_cast<const double*>(ws + m.ws) + plane;
+    const double* S0p = X + plane;
+    const double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
+    double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+    double v[5], ax[5], ay[5], az[5];
+    for (int i0 = 0; i0 < m.nsh; i0 += 128) {
+        __syncthreads();
+        stage_shells(bas, g, m, i0, st);
+        __syncthreads();
+        const int kn = min(128, m.nsh - i0);
+        for (int k = 0; k < kn; ++k) {
+            const int i = i0 + k;
+            const int L = st.lq[k], row0 = st.row0[k];
+            double xv[5];
+#pragma unroll
+            for (int c = 0; c < 5; ++c) xv[c] = c < 2 * L + 1 ? X[(size_t)(row0 + c) * BLOCK_PTS + p] : 0.0;
+            shell_components(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0p[(size_t)i * BLOCK_PTS + p],
+                             S1p[(size_t)i * BLOCK_PTS + p], v, ax, ay, az);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                if (c < 2 * L + 1) {
+                    rho = fma(v[c], xv[c], rho);
+                    gx = fma(ax[c], xv[c], gx);
+                    gy = fma(ay[c], xv[c], gy);
+                    gz = fma(az[c], xv[c], gz);
+                }
+            }
+        }
+    }
+    double* ra = rho_acc + gp * 4;
+    ra[0] = rho, ra[1] = gx, ra[2] = gy, ra[3] = gz;
+}
+
+__global__ void __launch_bounds__(BLOCK_PTS, 6) k_z_rad(BasisView bas, GridView g, int blk0, const double* coef,
+                                                     char* ws) {
+    __shared__ ShellStage st;
+    const int blk = blk0 + blockIdx.x;
+    const BlockMeta m = g.meta[blk];
+    const int p = threadIdx.x;
+    const size_t plane = (size_t)m.nbp * BLOCK_PTS;
+    double* Z = reinterpret_cast<double*>(ws + m.ws) + plane;
+    const double* S0p = Z + plane;
+    const double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
+    const double* cf = coef + gp * 4;
+    const double a = cf[0], cx = cf[1], cy = cf[2], cz = cf[3];
+    double v[5], ax[5], ay[5], az[5];
+    for (int i0 = 0; i0 < m.nsh; i0 += 128) {
+        __syncthreads();
+        stage_shells(bas, g, m, i0, st);
+        __syncthreads();
+        const int kn = min(128, m.nsh - i0);
+        for (int k = 0; k < kn; ++k) {
+            const int i = i0 + k;
+            const int L = st.lq[k], row0 = st.row0[k];
+            shell_components(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0p[(size_t)i * BLOCK_PTS + p],
+                             S1p[(size_t)i * BLOCK_PTS + p], v, ax, ay, az);
+#pragma unroll
+            for (int c = 0; c < 5; ++c)
+                if (c < 2 * L + 1) Z[(size_t)(row0 + c) * BLOCK_PTS + p] = a * v[c] + cx * ax[c] + cy * ay[c] + cz * az[c];
+        }
+    }
+    for (int r = m.nb; r < m.nbp; ++r) Z[(size_t)r * BLOCK_PTS + p] = 0.0;
+}
+
 // Vacc[aos[m]][aos[n]] += sum_p phi[m][p] Z[n][p]: CTA tile 64 x 64 AOs, K = 128 points in
 // steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles). Z was formed by
 // k_rho_functional in the place of X; both tiles are staged as [row][k] with 128-byte rows.
@@ -593,6 +672,16 @@ void launch_ao_eval_rad(const BasisView& b, const GridView& g, int blk0, int nbl
 void launch_rho_functional_rad(const BasisView& b, const GridView& g, int blk0, int nblk, int fn, bool incremental,
                                double rho_cut, char* ws, double* rho, double* coef, double* blk_sum, cudaStream_t s) {
     k_rho_functional_rad<<<nblk, BLOCK_PTS, 0, s>>>(b, g, blk0, fn, incremental, rho_cut, ws, rho, coef, blk_sum);
+}
+
+void launch_rho_rad(const BasisView& b, const GridView& g, int blk0, int nblk, const char* ws, double* rho_acc,
+                    cudaStream_t s) {
+    k_rho_rad<<<nblk, BLOCK_PTS, 0, s>>>(b, g, blk0, ws, rho_acc);
+}
+
+void launch_z_rad(const BasisView& b, const GridView& g, int blk0, int nblk, const double* coef, char* ws,
+                  cudaStream_t s) {
+    k_z_rad<<<nblk, BLOCK_PTS, 0, s>>>(b, g, blk0, coef, ws);
 }
 
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,

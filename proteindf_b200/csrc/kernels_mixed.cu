@@ -1023,6 +1023,17 @@ __global__ void __launch_bounds__(oz_threads<MODE>(), 2)
 
 size_t oz_smem_bytes() { return (size_t)OZ_STAGES * OZ_STAGE_BYTES + (2 * OZ_STAGES + 1) * 8 + 16; }
 
+void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
+                              const double* rho_acc, double* rho_store, double* coef, double* blk_sum,
+                              cudaStream_t s) {
+    if (functional_is_gga(fn))
+        k_functional_mixed<true><<<nblk, BLOCK_PTS, 0, s>>>(g, blk0, fn, incremental, rho_cut, rho_acc, rho_store,
+                                                            coef, blk_sum);
+    else
+        k_functional_mixed<false><<<nblk, BLOCK_PTS, 0, s>>>(g, blk0, fn, incremental, rho_cut, rho_acc, rho_store,
+                                                             coef, blk_sum);
+}
+
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
     // radial sums and row scales, then the phi digits of both layouts, then P_sub per group
     if (functional_is_gga(a.fn))

@@ -535,7 +535,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
     dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
     dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
-    if (mixed) dev_alloc(&ctx->d_rho_acc, (size_t)nblk * BLOCK_PTS * 4);
+    dev_alloc(&ctx->d_rho_acc, (size_t)nblk * BLOCK_PTS * 4);  // per-point sums of the rho pass
     PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho, 0, sizeof(double) * (size_t)nblk * BLOCK_PTS * 4, s));
     if (cudaMalloc(&ctx->d_ws, max_ws) != cudaSuccess) {
         ctx->d_ws = nullptr;
@@ -966,10 +966,12 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         pdfxc::launch_gemm_x(gv, d_PA, nao, cb0, nb, c.max_nbp, 1, ws, s);
         PDFXC_LAUNCHED("k_gemm_x");
         PDFXC_CUDA(cudaEventRecord(e[2], s));
-        if (gga)
-            pdfxc::launch_rho_functional_rad(bv, gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho,
-                                             ctx->d_coef, ctx->d_blk_sum, s);
-        else
+        if (gga) {
+            pdfxc::launch_rho_rad(bv, gv, cb0, nb, ws, ctx->d_rho_acc, s);
+            pdfxc::launch_functional_points(gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ctx->d_rho_acc,
+                                            ctx->d_rho, ctx->d_coef, ctx->d_blk_sum, s);
+            pdfxc::launch_z_rad(bv, gv, cb0, nb, ctx->d_coef, ws, s);
+        } else
             pdfxc::launch_rho_functional(gv, cb0, nb, fn, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho,
                                          ctx->d_coef, ctx->d_blk_sum, s);
         PDFXC_LAUNCHED("k_rho_functional");
@@ -977,7 +979,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         pdfxc::launch_gemm_v_plane(gv, cb0, nb, c.max_nbp, 1, ws, ctx->d_Vacc, nao, s);
         PDFXC_LAUNCHED("k_gemm_v");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
-        launches += 4;
+        launches += gga ? 6 : 4;
     }
     pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum + 2 * (size_t)ctx->blk_lo,
                          ctx->blk_hi - ctx->blk_lo, ctx->d_scalars, s);

@@ -193,6 +193,15 @@ void launch_gemm_x_planes(const GridView& g, const double* P, int nao, int blk0,
 void launch_ao_eval_rad(const BasisView& b, const GridView& g, int blk0, int nblk, char* ws, cudaStream_t s);
 void launch_rho_functional_rad(const BasisView& b, const GridView& g, int blk0, int nblk, int fn, bool incremental,
                                double rho_cut, char* ws, double* rho, double* coef, double* blk_sum, cudaStream_t s);
+void launch_rho_rad(const BasisView& b, const GridView& g, int blk0, int nblk, const char* ws, double* rho_acc,
+                    cudaStream_t s);
+void launch_z_rad(const BasisView& b, const GridView& g, int blk0, int nblk, const double* coef, char* ws,
+                  cudaStream_t s);
+// per point: rho = rho_acc (+ stored, incremental), grad rho = 2 rho_acc[1..3] (+ stored), the
+// functional, the Vxc coefficients and the block sums (kernels_mixed.cu)
+void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
+                              const double* rho_acc, double* rho_store, double* coef, double* blk_sum,
+                              cudaStream_t s);
 void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool incremental,
                            double rho_cut, char* ws, double* rho, double* coef, double* blk_sum,
                            cudaStream_t s);
