@@ -684,73 +684,79 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
     }
 }
 
-// The block's row exponents of Z[nu][p] = 0.5 w vrho phi + c . grad phi (formed from the
-// radial sums; Z is not stored). A warp per row, lanes along the points.
-template <bool GGA>
-__global__ void __launch_bounds__(256) k_z_oz(BasisView bas, GridView g, int blk0, const double* __restrict__ coef,
-                                              char* ws) {
-    __shared__ OzPoints P;
-    const int blk = blk0 + blockIdx.x;
-    const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp, m.nsh);
-    char* base = ws + m.ws;
-    const double* rad = reinterpret_cast<const double*>(base + L.rad);
-    int* e_z = reinterpret_cast<int*>(base + L.e_z);
-    oz_load_points(g, blk, coef, P);
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int nu = warp; nu < m.nbp; nu += blockDim.x / 32) {
-        double mx = 0.0;
-        if (nu < m.nb) {
-            const OzRow row = oz_row(g, m, rad, nu);
-#pragma unroll
-            for (int j = 0; j < 4; ++j) mx = fmax(mx, fabs(oz_value<true, GGA>(row, P, lane + 32 * j)));
-        }
-        mx = warp_max_d(mx);
-        if (lane == 0) e_z[nu] = oz_exponent(mx);
-    }
-}
+// Z digits of a whole group in one CTA (512 threads, one per point of its up to four blocks):
+// per tile of 16 rows the CTA forms Z once in shared memory, takes each row's maximum over the
+// group's points (the group's row scale, stored by the first block for the Vxc epilogue), and
+// cuts the digits of every block from the same tile. One Z evaluation per value instead of two
+// (row exponents per block, then digits with the group maximum).
+constexpr int kGroupPts = 4 * BLOCK_PTS;
+struct OzGroupTile {
+    double x[kGroupPts], y[kGroupPts], z[kGroupPts];
+    double c[4][kGroupPts];
+    double vt[16][kGroupPts + 1];
+    int eg[16];
+};
+constexpr size_t kGroupTileBytes = sizeof(OzGroupTile);
 
-// Z digits (rows = AOs, K = points) with the group's row exponents. Per tile of 16 rows
-// the CTA forms Z once in shared memory (a thread per point and half-tile, so the rows and
-// their angular type are uniform across a warp), then 128 threads cut the digits (a thread
-// per row and 16 points; 8 consecutive rows with the same points fill whole 128-byte core
-// matrices).
 template <bool GGA>
-__global__ void __launch_bounds__(256) k_pack_z_oz(BasisView bas, GridView g, int blk0,
-                                                   const double* __restrict__ coef, char* ws) {
-    __shared__ OzPoints P;
-    __shared__ double vt[16][BLOCK_PTS + 1];
-    __shared__ int eg[16];
-    const int blk = blk0 + blockIdx.x;
-    const BlockMeta m = g.meta[blk];
+__global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const int* __restrict__ grp,
+                                                                 const double* __restrict__ coef, char* ws) {
+    extern __shared__ __align__(16) uint8_t zsm[];
+    OzGroupTile& T = *reinterpret_cast<OzGroupTile*>(zsm);
+    const int lead = grp[blockIdx.x];
+    const BlockMeta m = g.meta[lead];
     const OzLayout L = oz_layout(m.nbp, m.nsh);
-    char* base = ws + m.ws;
+    const int tid = threadIdx.x, b = tid / BLOCK_PTS, q = tid % BLOCK_PTS;
+    const bool live = b < m.gn;
+    const int blk = lead + (live ? b : 0);
+    char* base = ws + g.meta[blk].ws;
     const double* rad = reinterpret_cast<const double*>(base + L.rad);
-    int* e_z_g = reinterpret_cast<int*>(base + L.e_z_g);
-    oz_load_points(g, blk, coef, P);
-    const int p = threadIdx.x & (BLOCK_PTS - 1), half = threadIdx.x >> 7;
+    if (live) {
+        const size_t gp = (size_t)blk * BLOCK_PTS + q;
+        T.x[tid] = g.px[gp], T.y[tid] = g.py[gp], T.z[tid] = g.pz[gp];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) T.c[k][tid] = coef[gp * 4 + k];
+    }
+    const int warp = tid >> 5, lane = tid & 31;
     for (int nu0 = 0; nu0 < m.nbp; nu0 += 16) {
-        __syncthreads();  // the previous tile's digits are cut (and P is loaded)
+        __syncthreads();  // the previous tile's digits are cut (and the points are loaded)
+        if (live) {
 #pragma unroll 4
-        for (int j = 0; j < 8; ++j) {
-            const int r = half * 8 + j, nu = nu0 + r;
-            vt[r][p] = nu < m.nb ? oz_value<true, GGA>(oz_row(g, m, rad, nu), P, p) : 0.0;
-        }
-        if (threadIdx.x < 16) {  // the group's exponent of each row: the max over its blocks
-            int e = kOzZeroExp;
-            for (int i = 0; i < m.gn; ++i)
-                e = max(e, reinterpret_cast<const int*>(ws + g.meta[m.lead + i].ws + L.e_z)[nu0 + threadIdx.x]);
-            eg[threadIdx.x] = e;
-            if (blk == m.lead) e_z_g[nu0 + threadIdx.x] = e;
+            for (int r = 0; r < 16; ++r) {
+                const int nu = nu0 + r;
+                double zv = 0.0;
+                if (nu < m.nb) {
+                    const OzRow row = oz_row(g, m, rad, nu);
+                    const double dx = T.x[tid] - row.ax, dy = T.y[tid] - row.ay, dz = T.z[tid] - row.az;
+                    double v, gx, gy, gz;
+                    ao_from_radial<GGA>(row.t, dx, dy, dz, row.S0[q], GGA ? row.S1[q] : 0.0, v, gx, gy, gz);
+                    zv = T.c[0][tid] * v;
+                    if (GGA) zv += T.c[1][tid] * gx + T.c[2][tid] * gy + T.c[3][tid] * gz;
+                }
+                T.vt[r][tid] = zv;
+            }
+        } else {
+            for (int r = 0; r < 16; ++r) T.vt[r][tid] = 0.0;
         }
         __syncthreads();
-        if (half == 1) {
-            const int u = threadIdx.x - BLOCK_PTS, r = (u & 7) + 8 * (u >> 6), kg = (u >> 3) & 7;
+        {  // warp r: the row's maximum over the group's points
+            const int r = warp;  // 16 warps, 16 rows
+            double mx = 0.0;
+            for (int p = lane; p < kGroupPts; p += 32) mx = fmax(mx, fabs(T.vt[r][p]));
+            mx = warp_max_d(mx);
+            if (lane == 0) {
+                const int e = oz_exponent(mx);
+                T.eg[r] = e;
+                reinterpret_cast<int*>(ws + m.ws + L.e_z_g)[nu0 + r] = e;
+            }
+        }
+        __syncthreads();
+        if (live) {  // thread = (block b, row r, 16 points kg) of the tile
+            const int r = (q & 7) + 8 * (q >> 6), kg = (q >> 3) & 7;
             double v[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = vt[r][kg * 16 + j];
-            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, kg * 16, BLOCK_PTS), v, eg[r]);
+            for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
+            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
     }
 }
@@ -1062,13 +1068,13 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
     if (functional_is_gga(a.fn)) {
         k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                               a.rho_store, a.coef, a.blk_sum);
-        k_z_oz<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
-        k_pack_z_oz<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
+        cudaFuncSetAttribute(k_pack_z_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGroupTileBytes);
+        k_pack_z_group<true><<<a.ngrp, kGroupPts, kGroupTileBytes, s>>>(a.g, a.grp, a.coef, a.ws);
     } else {
         k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                                a.rho_store, a.coef, a.blk_sum);
-        k_z_oz<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
-        k_pack_z_oz<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.coef, a.ws);
+        cudaFuncSetAttribute(k_pack_z_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGroupTileBytes);
+        k_pack_z_group<false><<<a.ngrp, kGroupPts, kGroupTileBytes, s>>>(a.g, a.grp, a.coef, a.ws);
     }
 }
 

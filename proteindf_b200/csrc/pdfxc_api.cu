@@ -947,7 +947,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         oz ? pdfxc::oz_vxc(a, s) : pdfxc::mixed_vxc(a, s);
         PDFXC_LAUNCHED("Vxc contraction");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
-        launches += oz ? 9 : 6;
+        launches += oz ? 8 : 6;
     }
     for (size_t ci = 0; ci < ctx->chunks.size() && !mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
