@@ -524,133 +524,130 @@ __device__ __forceinline__ OzRow oz_row(const GridView& g, const BlockMeta& m, c
     return r;
 }
 
-// Point coordinates of a block (and, for Z, the per-point Vxc coefficients) in shared memory.
-struct OzPoints {
-    double x[BLOCK_PTS], y[BLOCK_PTS], z[BLOCK_PTS];
-    double c[4][BLOCK_PTS];  // 0.5 w vrho, c_x, c_y, c_z
+// AO stage and phi digits of a whole group in one CTA (512 threads, one per point of its up
+// to four blocks). Pass 1: the radial sums S0, S1 of every shell of the group's basis at the
+// thread's point (stored for the later stages) and the point's exponent of phi^T rows (the
+// max over the AOs: max_c |A_c S0| = |S0| max_c |A_c|, the rounding being monotone). Pass 2,
+// per tile of 16 AO rows: phi formed once in shared memory, each row's maximum over the
+// group's points (the group's scale of phi rows, taken in shared memory, stored by the first
+// block), then every thread cuts the phi^T digits of its point (16 AOs, one 16-byte store per
+// digit plane) and a (row, 16 points) piece of the phi digits (8 consecutive rows with the
+// same points fill whole 128-byte core matrices).
+constexpr int kGroupPts = 4 * BLOCK_PTS;
+struct OzPhiTile {
+    double x[kGroupPts], y[kGroupPts], z[kGroupPts];
+    double vt[16][kGroupPts + 1];
+    int eg[16];
 };
+constexpr size_t kPhiTileBytes = sizeof(OzPhiTile);
 
-__device__ __forceinline__ void oz_load_points(const GridView& g, int blk, const double* coef, OzPoints& P) {
-    for (int p = threadIdx.x; p < BLOCK_PTS; p += blockDim.x) {
-        const size_t gp = (size_t)blk * BLOCK_PTS + p;
-        P.x[p] = g.px[gp], P.y[p] = g.py[gp], P.z[p] = g.pz[gp];
+__device__ __forceinline__ double ang_max_abs(int L, double x, double y, double z) {
+    if (L == 0) return 1.0;
+    if (L == 1) return fmax(fabs(x), fmax(fabs(y), fabs(z)));
+    double A, Ax, Ay, Az, mx = 0.0;
+#pragma unroll
+    for (int c = 0; c < 5; ++c) {
+        ang_poly1(4 + c, x, y, z, A, Ax, Ay, Az);
+        mx = fmax(mx, fabs(A));
     }
-    if (coef)
-        for (int e = threadIdx.x; e < 4 * BLOCK_PTS; e += blockDim.x)
-            P.c[e & 3][e >> 2] = coef[((size_t)blk * BLOCK_PTS + (e >> 2)) * 4 + (e & 3)];
+    return mx;
 }
 
-// phi (Z = false) or Z = 0.5 w vrho phi + c . grad phi (Z = true) of row r at point p.
-template <bool Z, bool GGA>
-__device__ __forceinline__ double oz_value(const OzRow& r, const OzPoints& P, int p) {
-    const double x = P.x[p] - r.ax, y = P.y[p] - r.ay, z = P.z[p] - r.az;
-    double v, gx, gy, gz;
-    ao_from_radial<Z && GGA>(r.t, x, y, z, r.S0[p], (Z && GGA) ? r.S1[p] : 0.0, v, gx, gy, gz);
-    if (!Z) return v;
-    double w = P.c[0][p] * v;
-    if (GGA) w += P.c[1][p] * gx + P.c[2][p] * gy + P.c[3][p] * gz;
-    return w;
-}
-
-// AO stage of a block: radial sums of its shells at its points, the per-point exponents of
-// phi^T rows (max over the AOs) and the block's per-AO exponents of phi rows (max over the
-// points). 256 threads: the point is threadIdx.x % 128, the two halves take alternate
-// shells; a row's maximum is reduced over a warp's 32 points by shuffles and over the
-// half's four warps by an integer atomic max on the row's exponent (the exponent of a
-// maximum is the maximum of the exponents).
 template <bool GGA>
-__global__ void __launch_bounds__(256) k_ao_oz(BasisView bas, GridView g, int blk0, char* ws) {
-    __shared__ double hmax[BLOCK_PTS];
-    const int blk = blk0 + blockIdx.x;
-    const BlockMeta m = g.meta[blk];
+__global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridView g, const int* __restrict__ grp,
+                                                              char* ws) {
+    extern __shared__ __align__(16) uint8_t psm[];
+    OzPhiTile& T = *reinterpret_cast<OzPhiTile*>(psm);
+    const int lead = grp[blockIdx.x];
+    const BlockMeta m = g.meta[lead];
     const OzLayout L = oz_layout(m.nbp, m.nsh);
-    char* base = ws + m.ws;
-    double* S0p = reinterpret_cast<double*>(base + L.rad);
-    double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
-    int* e_phi = reinterpret_cast<int*>(base + L.e_phi);
-    for (int r = threadIdx.x; r < m.nbp; r += blockDim.x) e_phi[r] = kOzZeroExp;
-    __syncthreads();
-    const int p = threadIdx.x & (BLOCK_PTS - 1), half = threadIdx.x >> 7, lane = threadIdx.x & 31;
-    const size_t gp = (size_t)blk * BLOCK_PTS + p;
-    const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
-    double pm = 0.0;
-    for (int i = half; i < m.nsh; i += 2) {
-        const int s = g.blk_shells[m.sh0 + i];
-        const int row0 = g.blk_shell_row[m.sh0 + i];
-        const int a = bas.sh_atom[s];
-        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
-        const int Lq = bas.sh_l[s];
-        double S0, S1;
-        shell_radial<GGA>(bas, s, x * x + y * y + z * z, S0, S1);
-        S0p[(size_t)i * BLOCK_PTS + p] = S0;
-        if (GGA) S1p[(size_t)i * BLOCK_PTS + p] = S1;
-        for (int c = 0; c < 2 * Lq + 1; ++c) {
-            double v, gx, gy, gz;
-            ao_from_radial<false>(Lq * Lq + c, x, y, z, S0, 0.0, v, gx, gy, gz);
-            v = fabs(v);
-            pm = fmax(pm, v);
-            const double wm = warp_max_d(v);
-            if (lane == 0 && wm > 0.0) atomicMax(&e_phi[row0 + c], oz_exponent(wm));
+    const int tid = threadIdx.x, b = tid / BLOCK_PTS, q = tid % BLOCK_PTS;
+    const bool live = b < m.gn;
+    char* base = ws + g.meta[lead + (live ? b : 0)].ws;
+    double* rad = reinterpret_cast<double*>(base + L.rad);
+    int ept = kOzZeroExp;
+    if (live) {
+        const size_t gp = (size_t)(lead + b) * BLOCK_PTS + q;
+        const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
+        T.x[tid] = rx, T.y[tid] = ry, T.z[tid] = rz;
+        double pm = 0.0;
+        for (int i = 0; i < m.nsh; ++i) {
+            const int sh = g.blk_shells[m.sh0 + i];
+            const int a = bas.sh_atom[sh];
+            const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
+            double S0, S1;
+            shell_radial<GGA>(bas, sh, x * x + y * y + z * z, S0, S1);
+            rad[(size_t)i * BLOCK_PTS + q] = S0;
+            if (GGA) rad[(size_t)(m.nsh + i) * BLOCK_PTS + q] = S1;
+            pm = fmax(pm, ang_max_abs(bas.sh_l[sh], x, y, z) * fabs(S0));
         }
+        ept = oz_exponent(pm);
+        reinterpret_cast<int*>(base + L.e_pt)[q] = ept;
     }
-    if (half) hmax[p] = pm;
-    __syncthreads();
-    if (!half) reinterpret_cast<int*>(base + L.e_pt)[p] = oz_exponent(fmax(pm, hmax[p]));
-}
-
-// Slices of phi^T (rows = points, per-point exponents) and phi (rows = AOs, the group's
-// per-AO exponents: the Vxc contraction runs over the whole group's points). Per tile of
-// 16 AO rows the CTA forms phi once in shared memory (a thread per point and half-tile);
-// then the first half cuts the phi^T digits (a thread per point: 16 AOs, one 16-byte store
-// per digit plane) and the second half the phi digits (a thread per row and 16 points; 8
-// consecutive rows with the same points fill whole 128-byte core matrices).
-__global__ void __launch_bounds__(256) k_slice_phi(BasisView bas, GridView g, int blk0, char* ws) {
-    __shared__ OzPoints P;
-    __shared__ double vt[16][BLOCK_PTS + 1];
-    __shared__ int eg[16];
-    const int blk = blk0 + blockIdx.x;
-    const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp, m.nsh);
-    char* base = ws + m.ws;
-    const double* rad = reinterpret_cast<const double*>(base + L.rad);
-    const int* e_pt = reinterpret_cast<const int*>(base + L.e_pt);
-    int* e_phi_g = reinterpret_cast<int*>(base + L.e_phi_g);
-    oz_load_points(g, blk, nullptr, P);
-    const int p = threadIdx.x & (BLOCK_PTS - 1), half = threadIdx.x >> 7;
+    const int warp = tid >> 5, lane = tid & 31;
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
-        __syncthreads();  // the previous tile's digits are cut (and P is loaded)
+        __syncthreads();  // the previous tile's digits are cut (and the points are stored)
+        if (live) {
 #pragma unroll 4
-        for (int j = 0; j < 8; ++j) {
-            const int r = half * 8 + j, mu = mu0 + r;
-            vt[r][p] = mu < m.nb ? oz_value<false, false>(oz_row(g, m, rad, mu), P, p) : 0.0;
-        }
-        if (threadIdx.x < 16) {  // the group's exponent of each row: the max over its blocks
-            int e = kOzZeroExp;
-            for (int i = 0; i < m.gn; ++i)
-                e = max(e, reinterpret_cast<const int*>(ws + g.meta[m.lead + i].ws + L.e_phi)[mu0 + threadIdx.x]);
-            eg[threadIdx.x] = e;
-            if (blk == m.lead) e_phi_g[mu0 + threadIdx.x] = e;
+            for (int r = 0; r < 16; ++r) {
+                const int mu = mu0 + r;
+                double v = 0.0;
+                if (mu < m.nb) {
+                    const OzRow row = oz_row(g, m, rad, mu);
+                    double gx, gy, gz;
+                    ao_from_radial<false>(row.t, T.x[tid] - row.ax, T.y[tid] - row.ay, T.z[tid] - row.az, row.S0[q],
+                                          0.0, v, gx, gy, gz);
+                }
+                T.vt[r][tid] = v;
+            }
+        } else {
+            for (int r = 0; r < 16; ++r) T.vt[r][tid] = 0.0;
         }
         __syncthreads();
-        double v[16];
-        if (half == 0) {
+        {  // warp r: the row's maximum over the group's points
+            double mx = 0.0;
+            for (int p = lane; p < kGroupPts; p += 32) mx = fmax(mx, fabs(T.vt[warp][p]));
+            mx = warp_max_d(mx);
+            if (lane == 0) {
+                const int e = oz_exponent(mx);
+                T.eg[warp] = e;
+                reinterpret_cast<int*>(ws + m.ws + L.e_phi_g)[mu0 + warp] = e;
+            }
+        }
+        __syncthreads();
+        if (live) {
+            double v[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = vt[j][p];
-            oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(p, mu0, m.nbp), v, e_pt[p]);
-        } else {
-            const int u = threadIdx.x - BLOCK_PTS, r = (u & 7) + 8 * (u >> 6), kg = (u >> 3) & 7;
+            for (int j = 0; j < 16; ++j) v[j] = T.vt[j][tid];
+            oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(q, mu0, m.nbp), v, ept);
+            const int r = (q & 7) + 8 * (q >> 6), kg = (q >> 3) & 7;
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = vt[r][kg * 16 + j];
-            oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu0 + r, kg * 16, BLOCK_PTS), v, eg[r]);
+            for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
+            oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
     }
 }
 
-// P_sub digits of a group. Phase 1: the row exponents, a warp per row mu gathering P[aos[mu]][aos[nu]]
-// from the L2-resident P. Phase 2: a warp takes 8 rows x 64 columns (lane = row r, K group
+// Exponents of the rows of P (a warp per row): the scale of a row of every group's P_sub.
+// The maximum over the whole row bounds the maximum over a group's columns, so the digits
+// stay in range; a row's largest elements (near its diagonal) are in every group that
+// holds the row, so the scale is, almost always, the sub-row's own.
+__global__ void __launch_bounds__(256) k_p_rowexp(const double* __restrict__ P, int nao, int* __restrict__ e) {
+    const int row = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= nao) return;
+    const double* r = P + (size_t)row * nao;
+    double mx = 0.0;
+    for (int c = lane; c < nao; c += 32) mx = fmax(mx, fabs(__ldg(r + c)));
+    mx = warp_max_d(mx);
+    if (lane == 0) e[row] = oz_exponent(mx);
+}
+
+// P_sub digits of a group, one gather of P[aos[mu]][aos[nu]] (L2-resident for a few thousand
+// AOs) with the rows' exponents of P. A warp takes 8 rows x 64 columns (lane = row r, K group
 // kg: 16 columns), so each digit store instruction writes four whole 128-byte core matrices.
 __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __restrict__ P, int nao,
-                                                   const int* __restrict__ grp, char* ws) {
+                                                   const int* __restrict__ grp, const int* __restrict__ p_rowexp,
+                                                   char* ws) {
     const int blk = grp[blockIdx.x];  // one CTA per group: P_sub lives in the first block's region
     const BlockMeta m = g.meta[blk];
     const OzLayout L = oz_layout(m.nbp, m.nsh);
@@ -658,29 +655,22 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
     int* e_p = reinterpret_cast<int*>(base + L.e_p);
     const int* aos = g.blk_aos + m.ao0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    for (int mu = warp; mu < m.nbp; mu += blockDim.x / 32) {
-        double mx = 0.0;
-        if (mu < m.nb) {
-            const double* row = P + (size_t)aos[mu] * nao;
-            for (int nu = lane; nu < m.nb; nu += 32) mx = fmax(mx, fabs(__ldg(row + aos[nu])));
-        }
-        mx = warp_max_d(mx);
-        if (lane == 0) e_p[mu] = oz_exponent(mx);
-    }
-    __syncthreads();
     const int r = lane & 7, kg = lane >> 3;
     const int nk = m.nbp / 64;
     double v[16];
     for (int t = warp; t < (m.nbp / 8) * nk; t += blockDim.x / 32) {
         const int mu = (t / nk) * 8 + r, k0 = (t % nk) * 64 + kg * 16;
         const bool live = mu < m.nb;
-        const double* row = P + (size_t)(live ? aos[mu] : 0) * nao;
+        const int amu = live ? aos[mu] : 0;
+        const int e = live ? __ldg(p_rowexp + amu) : kOzZeroExp;
+        if (kg == 0 && k0 == 0) e_p[mu] = e;
+        const double* row = P + (size_t)amu * nao;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int nu = k0 + j;
             v[j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0.0;
         }
-        oz_store16(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, k0, m.nbp), v, live ? e_p[mu] : 0);
+        oz_store16(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, k0, m.nbp), v, e);
     }
 }
 
@@ -689,7 +679,6 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
 // group's points (the group's row scale, stored by the first block for the Vxc epilogue), and
 // cuts the digits of every block from the same tile. One Z evaluation per value instead of two
 // (row exponents per block, then digits with the group maximum).
-constexpr int kGroupPts = 4 * BLOCK_PTS;
 struct OzGroupTile {
     double x[kGroupPts], y[kGroupPts], z[kGroupPts];
     double c[4][kGroupPts];
@@ -761,273 +750,392 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
     }
 }
 
-// Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
-__constant__ int kOzA[10] = {1, 1, 2, 1, 2, 3, 1, 2, 3, 4};
-__constant__ int kOzB[10] = {1, 2, 1, 3, 2, 1, 4, 3, 2, 1};
-
-// RHO: one CTA per (block, 64-row N tile) computes X^T = phi^T P_sub (M = 128 points,
-// N = 64 AOs mu, K = nbp AOs nu, P_sub of the block's group) with the rho / grad rho
-// epilogue. VXC: one CTA per (group, 128-row M tile, 64-row N tile) computes W = phi Z^T
-// (M = 128 AOs mu, N = 64 AOs nu, K = all points of the group's blocks, 128 per block)
-// with the FP64 atomic epilogue. Four int32 accumulators of 64 columns (256 TMEM columns) and a
-// two-stage operand ring of 48 KiB let two CTAs share an SM, so one CTA's epilogue
-// overlaps the other's loads and MMAs. A stage holds the A tile's four digit planes
-// (128 rows x 64 K, canonical no-swizzle K-major layout, 8 KiB each) and the B tile's
-// four digit planes (64 rows x 64 K, 4 KiB each): the 64-row half of a packed 128-row
-// tile is four 1 KiB core-matrix groups, copied into a compact layout (LBO 1024 B).
+// RHO items: (block, 64-row N tile): X^T = phi^T P_sub (M = 128 points, N = 64 AOs mu,
+// K = nbp AOs nu, P_sub of the block's group) with the rho / grad rho epilogue. VXC items:
+// (group, 128-row M tile, 64-row N tile): W = phi Z^T (M = 128 AOs mu, N = 64 AOs nu, K = all
+// points of the group's blocks, 128 per block) with the FP64 atomic epilogue.
+//
+// One persistent CTA per SM walks the items (item = blockIdx.x + k gridDim.x) with three
+// roles: warp 0 copies operand slabs into a two-stage ring (cp.async.bulk, mbarriers full /
+// empty), warp 1 issues the MMAs of an item into one of two TMEM accumulator sets (each four
+// int32 accumulators of 64 columns, one per order i + j = 2..5; 512 columns in all) and
+// commits it to tfull[set], and warps 2..9 run the epilogue of the item before, reading set
+// and releasing it through tempty[set]. So one item's epilogue runs under the next item's
+// copies and MMAs. A stage holds the A tile's four digit planes (128 rows x 64 K, canonical
+// no-swizzle K-major layout, 8 KiB each) and the B tile's four digit planes (64 rows x 64 K,
+// 4 KiB each): the 64-row half of a packed 128-row tile is four 1 KiB core-matrix groups,
+// copied into a compact layout (LBO 1024 B).
 constexpr int OZ_NT = 64;
 constexpr int OZ_STAGES = 2;
 constexpr uint32_t OZ_A_BYTES = OZ_SLICES * umma::I8_SLAB_BYTES;   // 32 KiB
 constexpr uint32_t OZ_B_SLICE = OZ_NT * umma::I8_SLAB_K;          // 4 KiB
 constexpr uint32_t OZ_STAGE_BYTES = OZ_A_BYTES + OZ_SLICES * OZ_B_SLICE;  // 48 KiB
-constexpr uint32_t OZ_TMEM_COLS = 4 * OZ_NT;                      // one accumulator per order 2..5
+constexpr uint32_t OZ_TMEM_COLS = 4 * OZ_NT;                      // one accumulator set
+constexpr int OZ_EPI_WARPS = 16;  // two groups of 4 lane quarters x 2 column halves
+constexpr int OZ_THREADS = 64 + 32 * OZ_EPI_WARPS;  // copies, MMAs, epilogue
+// Epilogue region after the ring, a quarter per (group, column half). RHO: the radial sums of
+// up to kOzRsCap shells of the half's columns, staged per thread. VXC: the half's [128][17]
+// FP64 transpose tile.
+constexpr int kOzRsCap = 12;
+constexpr uint32_t OZ_EPI_BYTES = 4u * kOzRsCap * 2 * BLOCK_PTS * 8;  // 96 KiB
+static_assert(4u * 128 * 17 * 8 <= OZ_EPI_BYTES, "transpose tiles fit the epilogue region");
+constexpr uint32_t OZ_BAR_OFF = OZ_STAGES * OZ_STAGE_BYTES + OZ_EPI_BYTES;
 
-// RHO runs 8 warps: the MMA pipeline uses warps 0 and 1 as in VXC, and the epilogue splits
-// the tile's 64 columns between warps w and w + 4, which read the same TMEM lane quarter.
-template <int MODE>
-constexpr int oz_threads() {
-    return MODE == MODE_RHO ? 256 : 128;
+// An item's int32 accumulators of orders 2..5 as one exact integer: with weights
+// w_k = 255^(5-k) w_5, sum_k d_k w_k = n w_5 with n = ((d2 255 + d3) 255 + d4) 255 + d5, whose
+// partial sums are integers below 2^53, so FP64 forms n exactly.
+__device__ __forceinline__ double oz_combine(uint32_t d2, uint32_t d3, uint32_t d4, uint32_t d5) {
+    return fma(fma(fma((double)(int)d2, 255.0, (double)(int)d3), 255.0, (double)(int)d4), 255.0, (double)(int)d5);
 }
 
-template <int MODE, bool GGA>
-__global__ void __launch_bounds__(oz_threads<MODE>(), 2)
-    k_oz(BasisView bas, GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int tiles_max,
-         double* rho_acc, double* Vacc, int nao) {
-    extern __shared__ __align__(1024) uint8_t smem[];
-    __shared__ RowGeom s_geom[OZ_NT];  // RHO: the tile's columns
-    __shared__ int s_ep[OZ_NT];
-    constexpr int S = OZ_STAGES;
-    const int blk = MODE == MODE_RHO ? blk0 + (int)blockIdx.y : grp[blockIdx.y];  // VXC: the group's first block
-    const BlockMeta m = g.meta[blk];
-    const OzLayout L = oz_layout(m.nbp, m.nsh);
-    const int ntiles = m.nbp / umma::TILE_ROWS;  // 128-row tiles of this block
-    int mt, nt;                                   // nt counts 64-row tiles
+// The item's block (RHO) or group's first block (VXC) and tiles; false for an empty slot.
+template <int MODE>
+__device__ __forceinline__ bool oz_item(const GridView& g, int blk0, const int* grp, int it, int tiles_max, int& blk,
+                                        int& mt, int& nt) {
     if (MODE == MODE_RHO) {
-        mt = 0, nt = blockIdx.x;
-        if (nt >= 2 * ntiles) return;
-    } else {
-        mt = blockIdx.x / tiles_max, nt = blockIdx.x % tiles_max;
-        if (mt >= ntiles || nt >= 2 * ntiles) return;
+        const int tn = 2 * tiles_max;
+        blk = blk0 + it / tn, mt = 0, nt = it % tn;
+        return nt < 2 * (g.meta[blk].nbp / umma::TILE_ROWS);
     }
+    const int per = tiles_max * 2 * tiles_max;
+    blk = grp[it / per];
+    const int r = it % per;
+    mt = r / (2 * tiles_max), nt = r % (2 * tiles_max);
+    const int ntiles = g.meta[blk].nbp / umma::TILE_ROWS;
+    return mt < ntiles && nt < 2 * ntiles;
+}
+
+// Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
+__constant__ int kOzA[10] = {1, 1, 2, 1, 2, 3, 1, 2, 3, 4};
+__constant__ int kOzB[10] = {1, 2, 1, 3, 2, 1, 4, 3, 2, 1};
+
+template <int MODE, bool GGA>
+__global__ void __launch_bounds__(OZ_THREADS, 1)
+    k_oz(BasisView bas, GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int nitems,
+         int tiles_max, double* rho_acc, double* Vacc, int nao) {
+    extern __shared__ __align__(1024) uint8_t smem[];
+    // per epilogue group and alternate item of the group (a group writes one buffer while its
+    // slower warps may still read the other): RHO the item's columns (row geometry, scale); VXC
+    // the AO indices of the item's columns and rows and the columns' Z exponents
+    __shared__ RowGeom s_geom[MODE == MODE_RHO ? 4 : 1][OZ_NT];
+    __shared__ double s_cs[MODE == MODE_RHO ? 4 : 1][OZ_NT];
+    __shared__ int s_acol[MODE == MODE_VXC ? 4 : 1][OZ_NT], s_ez[MODE == MODE_VXC ? 4 : 1][OZ_NT];
+    __shared__ int s_arow[MODE == MODE_VXC ? 4 : 1][128];
+    constexpr int S = OZ_STAGES;
     __shared__ int s_abort;
     if (threadIdx.x == 0) s_abort = *reinterpret_cast<const volatile int*>(err);
     __syncthreads();
     if (s_abort) return;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + S * OZ_STAGE_BYTES);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OZ_BAR_OFF);
     uint64_t* empty = full + S;
-    uint64_t* done = empty + S;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(done + 1);
-
-    const char* base = ws + m.ws;
-    const char* lead = ws + g.meta[m.lead].ws;  // the group's first block: P_sub, group exponents
-    // operand tiles: byte offsets inside a block's region (RHO: A in this block's, B in the
-    // group's first block's; VXC: both in the region of the block that slab j belongs to)
-    size_t Ao, Bo, Aplane, Bplane;
-    int nslabs;
-    constexpr int kBlockSlabs = BLOCK_PTS / (int)umma::I8_SLAB_K;  // VXC: K slabs per block
-    if (MODE == MODE_RHO) {
-        Ao = L.phi1;
-        Aplane = L.phi1_plane;
-        Bo = L.ppack + (size_t)(nt / 2) * umma::TILE_ROWS * m.nbp;
-        Bplane = L.ppack_plane;
-        nslabs = m.nbp / (int)umma::I8_SLAB_K;
-    } else {
-        Ao = L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS;
-        Aplane = L.phi2_plane;
-        Bo = L.zpack + (size_t)(nt / 2) * umma::TILE_ROWS * BLOCK_PTS;
-        Bplane = L.zpack_plane;
-        nslabs = m.gn * kBlockSlabs;
-    }
-    const size_t bhalf = (size_t)(nt & 1) * 8 * 128;  // row groups 8..15 of the 128-row tile
-
+    uint64_t* tfull = empty + S;
+    uint64_t* tempty = tfull + 2;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (warp == 0) umma::tmem_alloc(tslot, OZ_TMEM_COLS);
+    if (warp == 0) umma::tmem_alloc(tslot, 2 * OZ_TMEM_COLS);
     if (threadIdx.x == 32) {
         for (int st = 0; st < S; ++st) umma::mbar_init(&full[st], 1), umma::mbar_init(&empty[st], 1);
-        umma::mbar_init(done, 1);
+        for (int k = 0; k < 2; ++k) umma::mbar_init(&tfull[k], 1), umma::mbar_init(&tempty[k], OZ_EPI_WARPS / 2);
         umma::mbar_init_fence();
     }
     umma::fence_before_sync();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = *tslot;
+    constexpr int kBlockSlabs = BLOCK_PTS / (int)umma::I8_SLAB_K;  // VXC: K slabs per block
 
-    if (warp == 0 && lane == 0) {  // producer
-        for (int j = 0; j < nslabs; ++j) {
-            const int st = j % S;
-            if (j >= S && !umma::mbar_wait(&empty[st], ((j / S) - 1) & 1, err)) {
-                atomicExch(err, 1);
-                break;
-            }
-            uint8_t* sp = smem + st * OZ_STAGE_BYTES;
-            umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
-            const char *As = base + Ao, *Bs = lead + Bo;
-            size_t js = (size_t)j * umma::I8_SLAB_BYTES;
-            if (MODE == MODE_VXC) {  // slab j: block lead + j / kBlockSlabs, its slab j % kBlockSlabs
-                const char* bj = ws + g.meta[m.lead + j / kBlockSlabs].ws;
-                As = bj + Ao, Bs = bj + Bo;
-                js = (size_t)(j % kBlockSlabs) * umma::I8_SLAB_BYTES;
-            }
-            for (int a = 0; a < OZ_SLICES; ++a)
-                umma::bulk_g2s(sp + a * umma::I8_SLAB_BYTES, As + a * Aplane + js, umma::I8_SLAB_BYTES, &full[st]);
-            for (int b = 0; b < OZ_SLICES; ++b)
-                for (int kg = 0; kg < 4; ++kg)
-                    umma::bulk_g2s(sp + OZ_A_BYTES + b * OZ_B_SLICE + kg * 1024,
-                                   Bs + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
-        }
-    } else if (warp == 1 && lane == 0) {  // MMA issuer
-        const uint32_t idesc = umma::instr_desc_s8(128, OZ_NT);
-        bool issued = false;
-        for (int j = 0; j < nslabs; ++j) {
-            const int st = j % S;
-            if (!umma::mbar_wait(&full[st], (j / S) & 1, err)) {
-                atomicExch(err, 2);
-                break;
-            }
-            umma::fence_after_sync();
-            const uint32_t sp = umma::smem_u32(smem + st * OZ_STAGE_BYTES);
-#pragma unroll
-            for (int kk = 0; kk < 2; ++kk) {
-#pragma unroll
-                for (int t = 0; t < 10; ++t) {
-                    const int i = kOzA[t], jj = kOzB[t];
-                    const uint32_t acc = tmem + (uint32_t)(i + jj - 2) * OZ_NT;
-                    const uint64_t ad =
-                        umma::smem_desc(sp + (i - 1) * umma::I8_SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
-                    const uint64_t bd =
-                        umma::smem_desc(sp + OZ_A_BYTES + (jj - 1) * OZ_B_SLICE + kk * 2048, 1024, umma::SBO);
-                    // the first product of each order starts its accumulator
-                    const bool first = (j == 0 && kk == 0 && (t == 0 || t == 1 || t == 3 || t == 6));
-                    umma::mma_s8(acc, ad, bd, idesc, first ? 0u : 1u);
+    if (warp == 0) {
+        if (lane == 0) {  // copies
+            uint32_t gj = 0;
+            bool ok = true;
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                int blk, mt, nt;
+                if (!oz_item<MODE>(g, blk0, grp, it, tiles_max, blk, mt, nt)) continue;
+                const BlockMeta m = g.meta[blk];
+                const OzLayout L = oz_layout(m.nbp, m.nsh);
+                const char* base = ws + m.ws;
+                const char* lead = ws + g.meta[m.lead].ws;
+                size_t Ao, Bo, Aplane, Bplane;
+                int nslabs;
+                if (MODE == MODE_RHO) {
+                    Ao = L.phi1, Aplane = L.phi1_plane;
+                    Bo = L.ppack + (size_t)(nt / 2) * umma::TILE_ROWS * m.nbp, Bplane = L.ppack_plane;
+                    nslabs = m.nbp / (int)umma::I8_SLAB_K;
+                } else {
+                    Ao = L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS, Aplane = L.phi2_plane;
+                    Bo = L.zpack + (size_t)(nt / 2) * umma::TILE_ROWS * BLOCK_PTS, Bplane = L.zpack_plane;
+                    nslabs = m.gn * kBlockSlabs;
+                }
+                const size_t bhalf = (size_t)(nt & 1) * 8 * 128;  // row groups 8..15 of the 128-row tile
+                for (int j = 0; j < nslabs; ++j, ++gj) {
+                    const int st = gj % S;
+                    if (gj >= S && !umma::mbar_wait(&empty[st], ((gj / S) - 1) & 1, err)) {
+                        atomicExch(err, 1);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t* sp = smem + st * OZ_STAGE_BYTES;
+                    umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
+                    const char *As = base + Ao, *Bs = lead + Bo;
+                    size_t js = (size_t)j * umma::I8_SLAB_BYTES;
+                    if (MODE == MODE_VXC) {  // slab j: block lead + j / kBlockSlabs, its slab j % kBlockSlabs
+                        const char* bj = ws + g.meta[m.lead + j / kBlockSlabs].ws;
+                        As = bj + Ao, Bs = bj + Bo;
+                        js = (size_t)(j % kBlockSlabs) * umma::I8_SLAB_BYTES;
+                    }
+                    for (int a = 0; a < OZ_SLICES; ++a)
+                        umma::bulk_g2s(sp + a * umma::I8_SLAB_BYTES, As + a * Aplane + js, umma::I8_SLAB_BYTES,
+                                       &full[st]);
+                    for (int b = 0; b < OZ_SLICES; ++b)
+                        for (int kg = 0; kg < 4; ++kg)
+                            umma::bulk_g2s(sp + OZ_A_BYTES + b * OZ_B_SLICE + kg * 1024,
+                                           Bs + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
                 }
             }
-            issued = true;
-            umma::mma_commit(&empty[st]);
         }
-        if (issued) umma::mma_commit(done);
-        else umma::mbar_expect_tx(done, 0);
-    }
-    __syncwarp();
-    bool waited = umma::mbar_wait(done, 0, err);
-    if (!waited) atomicExch(err, 3);
-    const bool ready = __syncthreads_and(waited) != 0;
-    umma::fence_after_sync();
-
-    if (ready) {
-        const int row = warp * 32 + lane;
-        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-        const double w2 = oz_weight(2), w3 = oz_weight(3), w4 = oz_weight(4), w5 = oz_weight(5);
-        if (MODE == MODE_RHO) {
-            // The tile's column data (row geometry, P_sub exponent) once per CTA in shared memory;
-            // then each thread (point = lane quarter of its warp, columns = half of the tile)
-            // fetches its radial sums of the half's shells up front (independent loads) into its
-            // own slots of the drained operand ring, and per 16 columns converts X^T[p][mu] from
-            // TMEM to FP64 and forms phi and grad phi of the column's AO at its point.
-            const int col0 = nt * OZ_NT;
-            const int* e_p = reinterpret_cast<const int*>(lead + L.e_p);
-            if (threadIdx.x < OZ_NT && col0 + (int)threadIdx.x < m.nb) {
-                s_geom[threadIdx.x] = g.blk_row_geom[m.ao0 + col0 + threadIdx.x];
-                s_ep[threadIdx.x] = e_p[col0 + threadIdx.x];
-            }
-            __syncthreads();
-            const int quarter = warp & 3, chalf = warp >> 2;
-            const int pt = quarter * 32 + lane;
-            const uint32_t tq = tmem + ((uint32_t)(quarter * 32) << 16);
-            const double* rad = reinterpret_cast<const double*>(base + L.rad);
-            const int ep = reinterpret_cast<const int*>(base + L.e_pt)[pt];
-            const size_t gp = (size_t)blk * BLOCK_PTS + pt;
-            const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
-            constexpr int kHalf = OZ_NT / 2;
-            constexpr int kCap = OZ_STAGES * OZ_STAGE_BYTES / 2 / (2 * 8 * BLOCK_PTS);  // shells per half
-            double* rs = reinterpret_cast<double*>(smem + (size_t)chalf * (OZ_STAGES * OZ_STAGE_BYTES / 2));
-            const int ca = chalf * kHalf, cb = min(ca + kHalf, m.nb - col0);  // this half's columns [ca, cb)
-            int slot0 = 0, ns = 0;
-            if (ca < cb) {
-                slot0 = s_geom[ca].info >> 4;
-                ns = min((s_geom[cb - 1].info >> 4) - slot0 + 1, kCap);
-#pragma unroll 4
-                for (int k = 0; k < ns; ++k) {
-                    rs[(2 * k) * BLOCK_PTS + pt] = rad[(size_t)(slot0 + k) * BLOCK_PTS + pt];
-                    if (GGA) rs[(2 * k + 1) * BLOCK_PTS + pt] = rad[(size_t)(m.nsh + slot0 + k) * BLOCK_PTS + pt];
+        __syncwarp();
+    } else if (warp == 1) {
+        if (lane == 0) {  // MMAs
+            const uint32_t idesc = umma::instr_desc_s8(128, OZ_NT);
+            uint32_t gj = 0;
+            int li = 0;
+            bool ok = true;
+            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+                int blk, mt, nt;
+                if (!oz_item<MODE>(g, blk0, grp, it, tiles_max, blk, mt, nt)) continue;
+                const BlockMeta m = g.meta[blk];
+                const int nslabs = MODE == MODE_RHO ? m.nbp / (int)umma::I8_SLAB_K : m.gn * kBlockSlabs;
+                const int set = li & 1;
+                if (li >= 2 && !umma::mbar_wait(&tempty[set], ((li >> 1) - 1) & 1, err)) {
+                    atomicExch(err, 4);
+                    break;
                 }
-            }
-            double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-            for (int c0 = ca; c0 < cb; c0 += 16) {
-                uint32_t d2[16], d3[16], d4[16], d5[16];
-                umma::tmem_ld16_raw(tq + c0, d2);
-                umma::tmem_ld16_raw(tq + OZ_NT + c0, d3);
-                umma::tmem_ld16_raw(tq + 2 * OZ_NT + c0, d4);
-                umma::tmem_ld16_raw(tq + 3 * OZ_NT + c0, d5);
-                umma::tmem_wait_ld();
+                umma::fence_after_sync();
+                const uint32_t tacc = tmem + (uint32_t)set * OZ_TMEM_COLS;
+                for (int j = 0; j < nslabs; ++j, ++gj) {
+                    const int st = gj % S;
+                    if (!umma::mbar_wait(&full[st], (gj / S) & 1, err)) {
+                        atomicExch(err, 2);
+                        ok = false;
+                        break;
+                    }
+                    umma::fence_after_sync();
+                    const uint32_t sp = umma::smem_u32(smem + st * OZ_STAGE_BYTES);
 #pragma unroll
-                for (int c = 0; c < 16; ++c) {
-                    if (c0 + c < cb) {
-                        const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 +
-                                          (double)(int)d4[c] * w4 + (double)(int)d5[c] * w5;
-                        const double X = sx * oz_pow2(ep + s_ep[c0 + c]);
-                        const RowGeom q = s_geom[c0 + c];
-                        const int slot = q.info >> 4, k = slot - slot0;
-                        const double S0 = k < ns ? rs[(2 * k) * BLOCK_PTS + pt] : rad[(size_t)slot * BLOCK_PTS + pt];
-                        double S1 = 0.0;
-                        if (GGA)
-                            S1 = k < ns ? rs[(2 * k + 1) * BLOCK_PTS + pt]
-                                        : rad[(size_t)(m.nsh + slot) * BLOCK_PTS + pt];
-                        double v, ax, ay, az;
-                        ao_from_radial<GGA>(q.info & 15, px - q.ax, py - q.ay, pz - q.az, S0, S1, v, ax, ay, az);
-                        r += v * X;
-                        if (GGA) {
-                            gx += ax * X;
-                            gy += ay * X;
-                            gz += az * X;
+                    for (int kk = 0; kk < 2; ++kk) {
+#pragma unroll
+                        for (int t = 0; t < 10; ++t) {
+                            const int i = kOzA[t], jj = kOzB[t];
+                            const uint32_t acc = tacc + (uint32_t)(i + jj - 2) * OZ_NT;
+                            const uint64_t ad =
+                                umma::smem_desc(sp + (i - 1) * umma::I8_SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
+                            const uint64_t bd =
+                                umma::smem_desc(sp + OZ_A_BYTES + (jj - 1) * OZ_B_SLICE + kk * 2048, 1024, umma::SBO);
+                            // the first product of each order starts its accumulator
+                            const bool first = (j == 0 && kk == 0 && (t == 0 || t == 1 || t == 3 || t == 6));
+                            umma::mma_s8(acc, ad, bd, idesc, first ? 0u : 1u);
                         }
                     }
+                    umma::mma_commit(&empty[st]);
                 }
+                if (!ok) break;
+                umma::mma_commit(&tfull[set]);
+                ++li;
             }
-            double* acc = rho_acc + ((size_t)blk * BLOCK_PTS + pt) * 4;
-            atomicAdd(acc, r);
-            if (GGA) atomicAdd(acc + 1, gx), atomicAdd(acc + 2, gy), atomicAdd(acc + 3, gz);
-        } else {
-            const int* e_phi = reinterpret_cast<const int*>(base + L.e_phi_g);
-            const int* e_z = reinterpret_cast<const int*>(base + L.e_z_g);
-            const int* aos = g.blk_aos + m.ao0;
-            double* tile = reinterpret_cast<double*>(smem);  // [128][17], over the drained operand ring
-            const int mu_r = mt * 128 + row;
-            const int em = e_phi[mu_r];
-            for (int c0 = 0; c0 < OZ_NT; c0 += 16) {
-                uint32_t d2[16], d3[16], d4[16], d5[16];
-                umma::tmem_ld16_raw(taddr + c0, d2);
-                umma::tmem_ld16_raw(taddr + OZ_NT + c0, d3);
-                umma::tmem_ld16_raw(taddr + 2 * OZ_NT + c0, d4);
-                umma::tmem_ld16_raw(taddr + 3 * OZ_NT + c0, d5);
-                umma::tmem_wait_ld();
-#pragma unroll
-                for (int c = 0; c < 16; ++c) {
-                    const double sx = (double)(int)d2[c] * w2 + (double)(int)d3[c] * w3 + (double)(int)d4[c] * w4 +
-                                      (double)(int)d5[c] * w5;
-                    tile[row * 17 + c] = sx * oz_pow2(em + e_z[nt * OZ_NT + c0 + c]);
+        }
+        __syncwarp();
+    } else {  // epilogue: two groups of 8 warps (2..9 and 10..17) take alternate items
+        // Group h takes the items with li % 2 == h and so always reads TMEM set h; while one
+        // group waits on its loads the other computes. Warp w reads TMEM lanes 32 (w % 4) .. + 31.
+        const int h = (warp - 2) >> 3;
+        const int quarter = warp & 3, chalf = ((warp - 2) >> 2) & 1;  // lane quarter, column half
+        const int gt = (threadIdx.x - 64) & 255;                        // thread index in the group
+        const int gbar = 1 + h;                                          // the group's named barrier
+        const int ca = chalf * 32;                                       // this thread's columns [ca, ca + 32)
+        const double w5 = oz_weight(5);
+        uint8_t* epi = smem + OZ_STAGES * OZ_STAGE_BYTES;
+        const uint32_t tq = tmem + (uint32_t)h * OZ_TMEM_COLS + ((uint32_t)(quarter * 32) << 16);
+        int li = 0;
+        for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
+            int blk, mt, nt;
+            if (!oz_item<MODE>(g, blk0, grp, it, tiles_max, blk, mt, nt)) continue;
+            if ((li & 1) != h) {
+                ++li;
+                continue;
+            }
+            ++li;
+            const int ph = ((li - 1) >> 1) & 1;  // tfull[h] parity of this item
+            const int sb = 2 * h + ph;            // the item's shared-memory buffer
+            const BlockMeta m = g.meta[blk];
+            const OzLayout L = oz_layout(m.nbp, m.nsh);
+            const char* base = ws + m.ws;
+            const char* lead = ws + g.meta[m.lead].ws;
+            if (MODE == MODE_RHO) {
+                // Per item: the columns' row geometry and scales w5 2^e_p in shared memory; each
+                // thread (point = its lane, 32 columns) stages the radial sums of its columns'
+                // shells (independent loads) while the MMAs run; then, shell by shell, it reads the
+                // shell's accumulator columns from TMEM, forms X and phi, grad phi of the shell's
+                // components at its point and accumulates rho and grad rho.
+                const int col0 = nt * OZ_NT;
+                if (gt < OZ_NT) {
+                    const bool live = col0 + gt < m.nb;
+                    s_geom[sb][gt] = live ? g.blk_row_geom[m.ao0 + col0 + gt] : RowGeom{0.0, 0.0, 0.0, 0, 0};
+                    s_cs[sb][gt] = live ? w5 * oz_pow2(reinterpret_cast<const int*>(lead + L.e_p)[col0 + gt]) : 0.0;
                 }
-                __syncthreads();
-                const int c = threadIdx.x & 15;
-                const int nu = nt * OZ_NT + c0 + c;
-                if (nu < m.nb) {
-                    const int anu = aos[nu];
-                    for (int rr = threadIdx.x >> 4; rr < 128; rr += 8) {
-                        const int mu = mt * 128 + rr;
-                        if (mu < m.nb) atomicAdd(&Vacc[(size_t)aos[mu] * nao + anu], tile[rr * 17 + c]);
+                umma::named_sync(gbar, 256);
+                const int pt = quarter * 32 + lane;
+                const double* rad = reinterpret_cast<const double*>(base + L.rad);
+                const int cb = min(ca + 32, m.nb - col0);
+                double* rs = reinterpret_cast<double*>(epi) + (size_t)(2 * h + chalf) * kOzRsCap * 2 * BLOCK_PTS;
+                int slot0 = 0, ns = 0;
+                if (ca < cb) {
+                    slot0 = s_geom[sb][ca].info >> 4;
+                    ns = min((s_geom[sb][cb - 1].info >> 4) - slot0 + 1, kOzRsCap);
+                    for (int k = 0; k < ns; ++k) {
+                        rs[(2 * k) * BLOCK_PTS + pt] = rad[(size_t)(slot0 + k) * BLOCK_PTS + pt];
+                        if (GGA) rs[(2 * k + 1) * BLOCK_PTS + pt] = rad[(size_t)(m.nsh + slot0 + k) * BLOCK_PTS + pt];
                     }
                 }
-                __syncthreads();
+                const int ep = reinterpret_cast<const int*>(base + L.e_pt)[pt];
+                const size_t gp = (size_t)blk * BLOCK_PTS + pt;
+                const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
+                bool ok = umma::mbar_wait(&tfull[h], ph, err);
+                __syncwarp();
+                ok = umma::named_and(gbar, 256, ok);
+                if (!ok) {
+                    if (gt == 0) atomicExch(err, 3);
+                    break;
+                }
+                umma::fence_after_sync();
+                double r = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
+                for (int c = ca; c < cb;) {
+                    const RowGeom q = s_geom[sb][c];
+                    const int t = q.info & 15, slot = q.info >> 4, k = slot - slot0;
+                    const int Lq = t == 0 ? 0 : (t < 4 ? 1 : 2);
+                    const int cs0 = c - (t - Lq * Lq);  // column of the shell's first component
+                    const int ce = cs0 + 2 * Lq + 1;
+                    // the shell's accumulator columns in [ca, cb) (a uniform branch per column)
+                    uint32_t d[5][4];
+#pragma unroll
+                    for (int u = 0; u < 5; ++u) {
+                        const int cc = cs0 + u;
+                        if (cc < ce && cc >= ca && cc < cb) {
+#pragma unroll
+                            for (int o = 0; o < 4; ++o) umma::tmem_ld1_raw(tq + o * OZ_NT + cc, d[u][o]);
+                        }
+                    }
+                    const bool staged = (unsigned)k < (unsigned)ns;
+                    const double S0 = staged ? rs[(2 * k) * BLOCK_PTS + pt] : rad[(size_t)slot * BLOCK_PTS + pt];
+                    double S1 = 0.0;
+                    if (GGA)
+                        S1 = staged ? rs[(2 * k + 1) * BLOCK_PTS + pt] : rad[(size_t)(m.nsh + slot) * BLOCK_PTS + pt];
+                    const double x = px - q.ax, y = py - q.ay, z = pz - q.az;
+                    umma::tmem_wait_ld();
+                    // the shell's components, each added as soon as it is formed
+                    auto add = [&](int u, double A, double Ax, double Ay, double Az) {
+                        const int cc = cs0 + u;
+                        if (cc >= ca && cc < cb) {
+                            const double X = oz_combine(d[u][0], d[u][1], d[u][2], d[u][3]) * s_cs[sb][cc];
+                            r = fma(A * S0, X, r);
+                            if (GGA) {
+                                const double w = 2.0 * A * S1;
+                                gx = fma(Ax * S0 - x * w, X, gx);
+                                gy = fma(Ay * S0 - y * w, X, gy);
+                                gz = fma(Az * S0 - z * w, X, gz);
+                            }
+                        }
+                    };
+                    if (Lq == 0) {
+                        add(0, 1.0, 0.0, 0.0, 0.0);
+                    } else if (Lq == 1) {
+                        add(0, x, 1.0, 0.0, 0.0);
+                        add(1, y, 0.0, 1.0, 0.0);
+                        add(2, z, 0.0, 0.0, 1.0);
+                    } else {
+                        const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+                        add(0, x * y, y, x, 0.0);
+                        add(1, z * x, z, 0.0, x);
+                        add(2, y * z, 0.0, z, y);
+                        add(3, 0.5 * (x * x - y * y), x, -y, 0.0);
+                        add(4, s3 * (z * z - 0.5 * (x * x + y * y)), -s3 * x, -s3 * y, 2.0 * s3 * z);
+                    }
+                    c = ce;
+                }
+                umma::fence_before_sync();
+                __syncwarp();
+                if (lane == 0) umma::mbar_arrive(&tempty[h]);
+                if (ca < cb) {
+                    const double sc = oz_pow2(ep);
+                    double* acc = rho_acc + ((size_t)blk * BLOCK_PTS + pt) * 4;
+                    atomicAdd(acc, r * sc);
+                    if (GGA) atomicAdd(acc + 1, gx * sc), atomicAdd(acc + 2, gy * sc), atomicAdd(acc + 3, gz * sc);
+                }
+            } else {
+                // Per item: the columns' AO indices and Z exponents and the rows' AO indices in
+                // shared memory; per 16 columns each thread converts its row's accumulators to FP64
+                // W in its column half's transpose tile, then the half's 128 threads add the tile
+                // to Vacc (16 consecutive columns of two rows per warp instruction).
+                const int* aos = g.blk_aos + m.ao0;
+                if (gt < OZ_NT) {
+                    const int nu = nt * OZ_NT + gt;
+                    s_acol[sb][gt] = nu < m.nb ? aos[nu] : -1;
+                    s_ez[sb][gt] = reinterpret_cast<const int*>(base + L.e_z_g)[nu];
+                }
+                if (gt < 128) {
+                    const int mu = mt * 128 + gt;
+                    s_arow[sb][gt] = mu < m.nb ? aos[mu] : -1;
+                }
+                const int row = quarter * 32 + lane;
+                const int em = reinterpret_cast<const int*>(base + L.e_phi_g)[mt * 128 + row];
+                umma::named_sync(gbar, 256);
+                bool ok = umma::mbar_wait(&tfull[h], ph, err);
+                __syncwarp();
+                ok = umma::named_and(gbar, 256, ok);
+                if (!ok) {
+                    if (gt == 0) atomicExch(err, 3);
+                    break;
+                }
+                umma::fence_after_sync();
+                double* tile = reinterpret_cast<double*>(epi) + (size_t)(2 * h + chalf) * 128 * 17;
+                const int tbar = 3 + 2 * h + chalf;  // the column half's named barrier
+                for (int c0 = ca; c0 < ca + 32; c0 += 16) {
+                    uint32_t d2[16], d3[16], d4[16], d5[16];
+                    umma::tmem_ld16_raw(tq + c0, d2);
+                    umma::tmem_ld16_raw(tq + OZ_NT + c0, d3);
+                    umma::tmem_ld16_raw(tq + 2 * OZ_NT + c0, d4);
+                    umma::tmem_ld16_raw(tq + 3 * OZ_NT + c0, d5);
+                    umma::tmem_wait_ld();
+                    if (c0 == ca + 16) {  // the set is read: hand it back to the MMAs
+                        umma::fence_before_sync();
+                        __syncwarp();
+                        if (lane == 0) umma::mbar_arrive(&tempty[h]);
+                    }
+#pragma unroll
+                    for (int c = 0; c < 16; ++c)
+                        tile[row * 17 + c] =
+                            oz_combine(d2[c], d3[c], d4[c], d5[c]) * (w5 * oz_pow2(em + s_ez[sb][c0 + c]));
+                    umma::named_sync(tbar, 128);
+                    const int c = row & 15;
+                    const int anu = s_acol[sb][c0 + c];
+                    if (anu >= 0) {
+                        for (int rr = row >> 4; rr < 128; rr += 8) {
+                            const int amu = s_arow[sb][rr];
+                            if (amu >= 0) atomicAdd(&Vacc[(size_t)amu * nao + anu], tile[rr * 17 + c]);
+                        }
+                    }
+                    umma::named_sync(tbar, 128);
+                }
             }
         }
     }
     umma::fence_before_sync();
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, OZ_TMEM_COLS);
+    if (warp == 0) umma::tmem_dealloc(tmem, 2 * OZ_TMEM_COLS);
 }
 
 }  // namespace
 
-size_t oz_smem_bytes() { return (size_t)OZ_STAGES * OZ_STAGE_BYTES + (2 * OZ_STAGES + 1) * 8 + 16; }
+size_t oz_smem_bytes() { return (size_t)OZ_BAR_OFF + (2 * OZ_STAGES + 4) * 8 + 16; }
 
 void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
                               const double* rho_acc, double* rho_store, double* coef, double* blk_sum,
@@ -1040,27 +1148,42 @@ void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, boo
                                                              coef, blk_sum);
 }
 
+void oz_p_rowexp(const double* P, int nao, int* e, cudaStream_t s) {
+    k_p_rowexp<<<(nao + 7) / 8, 256, 0, s>>>(P, nao, e);
+}
+
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
-    // radial sums and row scales, then the phi digits of both layouts, then P_sub per group
-    if (functional_is_gga(a.fn))
-        k_ao_oz<true><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
-    else
-        k_ao_oz<false><<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
-    k_slice_phi<<<a.nblk, 256, 0, s>>>(a.b, a.g, a.blk0, a.ws);
-    k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.P, a.nao, a.grp, a.ws);
+    // per group: radial sums, row scales and the phi digits of both layouts; then P_sub
+    if (functional_is_gga(a.fn)) {
+        cudaFuncSetAttribute(k_phi_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiTileBytes);
+        k_phi_group<true><<<a.ngrp, kGroupPts, kPhiTileBytes, s>>>(a.b, a.g, a.grp, a.ws);
+    } else {
+        cudaFuncSetAttribute(k_phi_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiTileBytes);
+        k_phi_group<false><<<a.ngrp, kGroupPts, kPhiTileBytes, s>>>(a.b, a.g, a.grp, a.ws);
+    }
+    k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.P, a.nao, a.grp, a.p_rowexp, a.ws);
+}
+
+// Persistent contraction grid: one CTA per SM (its shared memory and all 512 TMEM columns
+// keep a second CTA off the SM), no more than there are items.
+static int oz_grid(int nitems) {
+    int dev = 0, nsm = 148;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    return std::max(1, std::min(nitems, nsm));
 }
 
 void oz_rho(const MixedArgs& a, cudaStream_t s) {
     const int tiles = a.max_nbp / umma::TILE_ROWS;
+    const int nitems = a.nblk * 2 * tiles;
     const size_t smem = oz_smem_bytes();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<dim3(2 * tiles, a.nblk), oz_threads<MODE_RHO>(), smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
-                                                                       2 * tiles, a.rho_acc, a.Vacc, a.nao);
+        k_oz<MODE_RHO, true><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
+                                                                       tiles, a.rho_acc, a.Vacc, a.nao);
     } else {
         cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<dim3(2 * tiles, a.nblk), oz_threads<MODE_RHO>(), smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
-                                                                        2 * tiles, a.rho_acc, a.Vacc, a.nao);
+        k_oz<MODE_RHO, false><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
+                                                                        tiles, a.rho_acc, a.Vacc, a.nao);
     }
 }
 
@@ -1080,11 +1203,11 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
 
 void oz_vxc(const MixedArgs& a, cudaStream_t s) {
     const int tiles = a.max_nbp / umma::TILE_ROWS;
+    const int nitems = a.ngrp * tiles * 2 * tiles;  // per group: M tiles of 128 AOs x N tiles of 64 AOs
     const size_t smem = oz_smem_bytes();
     cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    // per group: M tiles of 128 AOs x N tiles of 64 AOs
-    k_oz<MODE_VXC, false><<<dim3(tiles * 2 * tiles, a.ngrp), 128, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err,
-                                                                            2 * tiles, a.rho_acc, a.Vacc, a.nao);
+    k_oz<MODE_VXC, false><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
+                                                                    tiles, a.rho_acc, a.Vacc, a.nao);
 }
 
 size_t umma_smem_bytes(int nterms) {

@@ -306,6 +306,7 @@ pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
         dev_alloc(&ctx->d_P, n2);
         dev_alloc(&ctx->d_V, n2);
         dev_alloc(&ctx->d_Vacc, n2);
+        dev_alloc(&ctx->d_p_rowexp, (size_t)ao);
         dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b);  // open shell: sized on first use
         PDFXC_CUDA(cudaStreamSynchronize(s));
         free_grid(ctx);
@@ -913,6 +914,10 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     if (mixed) {
         memset_async(ctx->d_rho_acc, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+        if (ctx->opt.split_terms == 10) {
+            pdfxc::oz_p_rowexp(d_PA, nao, ctx->d_p_rowexp, s);
+            ++launches;
+        }
     }
     // the context's block range (all blocks unless pdfxc_set_block_range narrowed it)
     auto clip = [&](const Chunk& c, int& b0, int& n) {
@@ -932,7 +937,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         const int g_hi = (int)(std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), cb0 + cn) - ctx->h_grp.begin());
         pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
-                           ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo};
+                           ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp};
         const bool oz = ctx->opt.split_terms == 10;
         PDFXC_CUDA(cudaEventRecord(e[0], s));
         oz ? pdfxc::oz_prepare(a, s) : pdfxc::mixed_prepare(a, s);
@@ -947,7 +952,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         oz ? pdfxc::oz_vxc(a, s) : pdfxc::mixed_vxc(a, s);
         PDFXC_LAUNCHED("Vxc contraction");
         PDFXC_CUDA(cudaEventRecord(e[4], s));
-        launches += oz ? 8 : 6;
+        launches += oz ? 7 : 6;
     }
     for (size_t ci = 0; ci < ctx->chunks.size() && !mixed; ++ci) {
         const Chunk& c = ctx->chunks[ci];
@@ -1659,6 +1664,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
     dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
+    dev_free(ctx->d_p_rowexp);
     dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b), dev_free(ctx->d_scalars_b);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);

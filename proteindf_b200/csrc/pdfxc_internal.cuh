@@ -136,6 +136,7 @@ struct pdfxc_ctx {
     double* d_P = nullptr;        // n_ao^2 staging for host-pointer builds
     double* d_V = nullptr;        // n_ao^2
     double* d_Vacc = nullptr;     // n_ao^2 non-symmetric accumulator
+    int* d_p_rowexp = nullptr;    // n_ao: exponents of the rows of P (INT8 path)
     bool rho_valid = false;
     pdfxc_ctx* dens = nullptr;  // pdfxc_density: FP64 context over the requested points (same system)
     int* d_nbr_idx = nullptr;     // Stratmann-Scuseria weights: per atom the other atoms by distance
@@ -303,8 +304,7 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 // shell's radial sums S0, S1 at its points ([2][nsh][128] FP64) and every consumer forms
 // phi = A S0, grad phi = grad A S0 - 2 r A S1 from them. The Vxc contraction runs over
 // all points of a group, so the scales of its operands (phi and Z rows) are group
-// maxima: every block keeps its own phi row exponents (e_phi) and the group's (e_phi_g,
-// e_z_g, written by the group's first block). P_sub is shared by the group
+// maxima (e_phi_g, e_z_g, written by the group's first block). P_sub is shared by the group
 // and lives only in the first block's region, after `total` (`total_lead` bytes in all).
 constexpr int OZ_SLICES = 4;
 struct OzLayout {
@@ -312,7 +312,7 @@ struct OzLayout {
     size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs
     size_t phi2, phi2_plane;    // phi slices: rows = nbp AOs, K = 128 points
     size_t zpack, zpack_plane;  // Z slices: rows = nbp, K = 128 points
-    size_t e_pt, e_phi, e_phi_g, e_z_g, e_p;  // int exponents: per point, per AO row (block, group), P_sub
+    size_t e_pt, e_phi_g, e_z_g, e_p;  // int exponents: per point, per AO row of the group, P_sub
     size_t total;
     size_t ppack, ppack_plane;  // P_sub slices of the group: rows = nbp, K = nbp (first block only)
     size_t total_lead;
@@ -335,7 +335,7 @@ __host__ __device__ inline OzLayout oz_layout(int nbp, int nsh) {
     o = a256(o + OZ_SLICES * L.zpack_plane);
     L.e_pt = o;
     o = a256(o + sizeof(int) * BLOCK_PTS);
-    size_t* e[4] = {&L.e_phi, &L.e_phi_g, &L.e_z_g, &L.e_p};
+    size_t* e[3] = {&L.e_phi_g, &L.e_z_g, &L.e_p};
     for (size_t* f : e) {
         *f = o;
         o = a256(o + sizeof(int) * nbp);
@@ -360,6 +360,7 @@ struct MixedArgs {
     int* err;
     const int* grp;  // first blocks of the chunk's groups (INT8 path)
     int ngrp;
+    const int* p_rowexp;  // exponents of the rows of P (INT8 path)
 };
 void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
 void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue
@@ -367,6 +368,7 @@ void mixed_functional(const MixedArgs& a, cudaStream_t s);  // functional, Z pac
 void mixed_vxc(const MixedArgs& a, cudaStream_t s);         // Vacc += phi Z^T
 size_t umma_smem_bytes(int nterms);
 // the same four stages with INT8 fixed-point slices (split_terms == 10)
+void oz_p_rowexp(const double* P, int nao, int* e, cudaStream_t s);  // once per build
 void oz_prepare(const MixedArgs& a, cudaStream_t s);
 void oz_rho(const MixedArgs& a, cudaStream_t s);
 void oz_functional(const MixedArgs& a, cudaStream_t s);
