@@ -541,16 +541,13 @@ struct OzPhiTile {
 };
 constexpr size_t kPhiTileBytes = sizeof(OzPhiTile);
 
+// max_c |A_c| over a shell's components (the expressions of ang_poly1, without its branch per component)
 __device__ __forceinline__ double ang_max_abs(int L, double x, double y, double z) {
     if (L == 0) return 1.0;
     if (L == 1) return fmax(fabs(x), fmax(fabs(y), fabs(z)));
-    double A, Ax, Ay, Az, mx = 0.0;
-#pragma unroll
-    for (int c = 0; c < 5; ++c) {
-        ang_poly1(4 + c, x, y, z, A, Ax, Ay, Az);
-        mx = fmax(mx, fabs(A));
-    }
-    return mx;
+    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+    const double a = fmax(fabs(x * y), fmax(fabs(z * x), fabs(y * z)));
+    return fmax(a, fmax(fabs(0.5 * (x * x - y * y)), fabs(s3 * (z * z - 0.5 * (x * x + y * y)))));
 }
 
 template <bool GGA>
@@ -805,9 +802,10 @@ __device__ __forceinline__ bool oz_item(const GridView& g, int blk0, const int* 
     return mt < ntiles && nt < 2 * ntiles;
 }
 
-// Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j.
-__constant__ int kOzA[10] = {1, 1, 2, 1, 2, 3, 1, 2, 3, 4};
-__constant__ int kOzB[10] = {1, 2, 1, 3, 2, 1, 4, 3, 2, 1};
+// Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j: pair t is nibble t of
+// these constants (i: 1 1 2 1 2 3 1 2 3 4, j: 1 2 1 3 2 1 4 3 2 1), so unrolled loops fold them.
+__device__ __forceinline__ constexpr int oz_pair_a(int t) { return (int)((0x4321321211ull >> (4 * t)) & 15); }
+__device__ __forceinline__ constexpr int oz_pair_b(int t) { return (int)((0x1234123121ull >> (4 * t)) & 15); }
 
 template <int MODE, bool GGA>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
@@ -920,17 +918,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         break;
                     }
                     umma::fence_after_sync();
+                    // the stage's base descriptors; an operand's descriptor adds its byte offset / 16
+                    // to the start-address field (addresses stay below 256 KiB, so it cannot carry)
                     const uint32_t sp = umma::smem_u32(smem + st * OZ_STAGE_BYTES);
+                    const uint64_t ad0 = umma::smem_desc(sp, umma::LBO, umma::SBO);
+                    const uint64_t bd0 = umma::smem_desc(sp + OZ_A_BYTES, 1024, umma::SBO);
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
 #pragma unroll
                         for (int t = 0; t < 10; ++t) {
-                            const int i = kOzA[t], jj = kOzB[t];
+                            const int i = oz_pair_a(t), jj = oz_pair_b(t);
                             const uint32_t acc = tacc + (uint32_t)(i + jj - 2) * OZ_NT;
-                            const uint64_t ad =
-                                umma::smem_desc(sp + (i - 1) * umma::I8_SLAB_BYTES + kk * 4096, umma::LBO, umma::SBO);
-                            const uint64_t bd =
-                                umma::smem_desc(sp + OZ_A_BYTES + (jj - 1) * OZ_B_SLICE + kk * 2048, 1024, umma::SBO);
+                            const uint64_t ad = ad0 + (uint64_t)(((i - 1) * umma::I8_SLAB_BYTES + kk * 4096) >> 4);
+                            const uint64_t bd = bd0 + (uint64_t)(((jj - 1) * OZ_B_SLICE + kk * 2048) >> 4);
                             // the first product of each order starts its accumulator
                             const bool first = (j == 0 && kk == 0 && (t == 0 || t == 1 || t == 3 || t == 6));
                             umma::mma_s8(acc, ad, bd, idesc, first ? 0u : 1u);
