@@ -171,6 +171,18 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
                                     int incremental, double* d_V, double* exc,
                                     double* nelec_alpha);
 
+/* The XC part of the Fock update kept on the device: replaces the host round trip of
+ * DfFockMatrix::setXC_DIRECT (src/libpdf/DfFockMatrix.h:711-721), which loads Fxc of this
+ * iteration and, from the second iteration on, subtracts Fxc of the previous one. Builds Vxc of
+ * SCF iteration `iteration` (>= 1) from d_PA as pdfxc_build_vxc_device does, keeps it in the
+ * context, and writes d_dV = Vxc(iteration) - Vxc(iteration - 1) for iteration >= 2, d_dV =
+ * Vxc(1) for iteration 1 (device n_ao*n_ao FP64, overwritten). d_V (optional, NULL to skip)
+ * receives Vxc(iteration). For iteration >= 2 the context's previous call of this function must
+ * have been iteration - 1 (else PDFXC_ERR_STATE; pdfxc_set_system clears the history). */
+pdfxc_status pdfxc_build_vxc_delta_device(pdfxc_ctx* ctx, int functional, const double* d_PA,
+                                          int incremental, int iteration, double* d_V,
+                                          double* d_dV, double* exc, double* nelec_alpha);
+
 /* Per-point densities of the last build in input point order: npts x 1
  * (LDA: rho_A) or npts x 4 (GGA: rho_A, d/dx, d/dy, d/dz) -- the rho columns
  * of the grid matrix (src/libpdf/DfCalcGridX.h:35-54). pdfxc_set_rho seeds

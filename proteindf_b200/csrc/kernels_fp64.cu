@@ -720,6 +720,21 @@ void launch_block_sums(const double* blk_sum, int nblk, double* scalars, cudaStr
     k_block_sums<<<1, 256, 0, s>>>(blk_sum, nblk, scalars);
 }
 
+// dV = V - Vprev (or V with no previous iteration), then Vprev = V: the XC part of
+// DfFockMatrix::setXC_DIRECT (src/libpdf/DfFockMatrix.h:711-721) on the device.
+__global__ void k_fock_delta(const double* __restrict__ V, double* Vprev, double* __restrict__ dV, size_t n,
+                             int has_prev) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const double v = V[i];
+        dV[i] = has_prev ? v - Vprev[i] : v;
+        Vprev[i] = v;
+    }
+}
+
+void launch_fock_delta(const double* V, double* Vprev, double* dV, size_t n, bool has_prev, cudaStream_t s) {
+    k_fock_delta<<<148 * 8, 256, 0, s>>>(V, Vprev, dV, n, has_prev ? 1 : 0);
+}
+
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk, double* scalars,
                    cudaStream_t s) {
     k_symmetrize<<<148 * 8, 256, 0, s>>>(Vacc, V, nao);

@@ -306,6 +306,8 @@ pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
         dev_alloc(&ctx->d_P, n2);
         dev_alloc(&ctx->d_V, n2);
         dev_alloc(&ctx->d_Vacc, n2);
+        dev_free(ctx->d_Vprev);  // the delta history belongs to the old system
+        ctx->vprev_iter = 0;
         dev_alloc(&ctx->d_p_rowexp, (size_t)ao);
         dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b);  // open shell: sized on first use
         PDFXC_CUDA(cudaStreamSynchronize(s));
@@ -1110,6 +1112,49 @@ pdfxc_status pdfxc_build_vxc_device(pdfxc_ctx* ctx, int functional, const double
     });
 }
 
+pdfxc_status pdfxc_build_vxc_delta_device(pdfxc_ctx* ctx, int functional, const double* d_PA, int incremental,
+                                          int iteration, double* d_V, double* d_dV, double* exc, double* nelec_alpha) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        pdfxc_status st = check_build(ctx, functional, incremental);
+        if (st) return st;
+        if (!d_PA || !d_dV) {
+            ctx->err = "pdfxc_build_vxc_delta_device: null device pointer";
+            return PDFXC_ERR_ARG;
+        }
+        if (iteration < 1) {
+            ctx->err = "pdfxc_build_vxc_delta_device: iteration must be >= 1";
+            return PDFXC_ERR_ARG;
+        }
+        if (iteration >= 2 && ctx->vprev_iter != iteration - 1) {
+            ctx->err = "pdfxc_build_vxc_delta_device: the context holds no Vxc of iteration " +
+                       std::to_string(iteration - 1);
+            return PDFXC_ERR_STATE;
+        }
+        const size_t n2 = (size_t)ctx->nao * ctx->nao;
+        if (!ctx->d_Vprev) dev_alloc(&ctx->d_Vprev, n2);
+        run_build(ctx, functional, d_PA, incremental != 0);
+        if (d_V) PDFXC_CUDA(cudaMemcpyAsync(d_V, ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
+        pdfxc::launch_fock_delta(ctx->d_V, ctx->d_Vprev, d_dV, n2, iteration >= 2, ctx->stream);
+        PDFXC_LAUNCHED("fock delta");
+        double sc[2];
+        PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        collect_profile(ctx);
+        if (int code = device_error(ctx)) {
+            ctx->vprev_iter = 0;
+            ctx->err = "a bounded device wait expired in the tensor-core contraction (code " + std::to_string(code) + ")";
+            return PDFXC_ERR_TIMEOUT;
+        }
+        ctx->vprev_iter = iteration;
+        if (exc) *exc = sc[0];
+        if (nelec_alpha) *nelec_alpha = sc[1];
+        ctx->rho_valid = true;
+        ctx->rho_gga = pdfxc::functional_is_gga(functional);
+        ctx->rho_spin = 1;
+        return PDFXC_OK;
+    });
+}
+
 pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, int incremental, double* F, double* exc,
                              double* nelec_alpha) {
     return guarded(ctx, [&]() -> pdfxc_status {
@@ -1664,7 +1709,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
     dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
-    dev_free(ctx->d_p_rowexp);
+    dev_free(ctx->d_p_rowexp); dev_free(ctx->d_Vprev);
     dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b), dev_free(ctx->d_scalars_b);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);

@@ -135,6 +135,8 @@ struct pdfxc_ctx {
     double* d_scalars = nullptr;  // [2]
     double* d_P = nullptr;        // n_ao^2 staging for host-pointer builds
     double* d_V = nullptr;        // n_ao^2
+    double* d_Vprev = nullptr;    // n_ao^2: Vxc of the last delta build (pdfxc_build_vxc_delta_device)
+    int vprev_iter = 0;           // its SCF iteration, 0 = none
     double* d_Vacc = nullptr;     // n_ao^2 non-symmetric accumulator
     int* d_p_rowexp = nullptr;    // n_ao: exponents of the rows of P (INT8 path)
     bool rho_valid = false;
@@ -208,6 +210,7 @@ void launch_rho_functional(const GridView& g, int blk0, int nblk, int fn, bool i
                            cudaStream_t s);
 void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga, const double* coef,
                    char* ws, double* Vacc, int nao, cudaStream_t s);
+void launch_fock_delta(const double* V, double* Vprev, double* dV, size_t n, bool has_prev, cudaStream_t s);
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk,
                    double* scalars, cudaStream_t s);
 // Vacc += phi Z^T with Z in plane zplane of each block's workspace

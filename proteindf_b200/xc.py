@@ -23,6 +23,7 @@ EXPORTS = [
     "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
     "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
     "pdfxc_build_vxc_batched", "pdfxc_density", "pdfxc_generate_grid", "pdfxc_get_grid",
+    "pdfxc_build_vxc_delta_device",
 ]
 
 
@@ -80,6 +81,7 @@ def load_library(path=LIB_PATH):
     L.pdfxc_becke_weights.argtypes = [_vp, i64, _vp, _vp, _vp, _vp, i32, _vp]
     L.pdfxc_build_vxc.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_build_vxc_device.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
+    L.pdfxc_build_vxc_delta_device.argtypes = [_vp, i32, _vp, i32, i32, _vp, _vp, _vp, _vp]
     L.pdfxc_get_rho.argtypes = [_vp, i32, _vp]
     L.pdfxc_density.argtypes = [_vp, _vp, i64, _vp, _vp]
     L.pdfxc_generate_grid.argtypes = [_vp, ctypes.POINTER(GridParams), _vp]
@@ -259,6 +261,18 @@ class XcEngine:
         self._check(self.L.pdfxc_build_vxc_device(self.h, FUNCTIONALS[functional], _vp(d_PA_ptr), int(incremental),
                                                   _vp(d_V_ptr), ctypes.byref(exc), ctypes.byref(nel)),
                     "pdfxc_build_vxc_device")
+        return exc.value, nel.value
+
+    def build_vxc_delta_device(self, functional, iteration, d_PA_ptr, d_dV_ptr, d_V_ptr=None, incremental=False):
+        """Fxc(iteration) - Fxc(iteration - 1) into d_dV (Fxc(1) at iteration 1), kept on the device
+        (DfFockMatrix::setXC_DIRECT, src/libpdf/DfFockMatrix.h:711-721); d_V optionally receives
+        Fxc(iteration). Returns (exc, nelec_alpha)."""
+        exc = ctypes.c_double()
+        nel = ctypes.c_double()
+        self._check(self.L.pdfxc_build_vxc_delta_device(self.h, FUNCTIONALS[functional], _vp(d_PA_ptr),
+                                                        int(incremental), int(iteration), _vp(d_V_ptr or 0),
+                                                        _vp(d_dV_ptr), ctypes.byref(exc), ctypes.byref(nel)),
+                    "pdfxc_build_vxc_delta_device")
         return exc.value, nel.value
 
     def xc_gradient(self, functional, PA, w_single=None, becke_radius=None, size_adjust=True):
