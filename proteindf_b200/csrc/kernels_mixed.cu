@@ -513,8 +513,7 @@ struct OzRow {
     const double* S1;
 };
 
-__device__ __forceinline__ OzRow oz_row(const GridView& g, const BlockMeta& m, const double* rad, int mu) {
-    const RowGeom q = g.blk_row_geom[m.ao0 + mu];
+__device__ __forceinline__ OzRow oz_row_of(const RowGeom& q, const BlockMeta& m, const double* rad) {
     const int slot = q.info >> 4;
     OzRow r;
     r.t = q.info & 15;
@@ -537,8 +536,15 @@ constexpr int kGroupPts = 4 * BLOCK_PTS;
 struct OzPhiTile {
     double x[kGroupPts], y[kGroupPts], z[kGroupPts];
     double vt[16][kGroupPts + 1];
+    RowGeom rg[16];  // the tile's row geometry, staged during the previous tile's digit cut
     int eg[16];
 };
+
+// Row geometry of rows r0 .. r0 + 15 into rg by the CTA's last 16 threads (zero past the last row).
+__device__ __forceinline__ void oz_stage_rows(const GridView& g, const BlockMeta& m, int r0, RowGeom* rg) {
+    const int k = (int)threadIdx.x - ((int)blockDim.x - 16);
+    if (k >= 0) rg[k] = r0 + k < m.nb ? g.blk_row_geom[m.ao0 + r0 + k] : RowGeom{0.0, 0.0, 0.0, 0, 0};
+}
 constexpr size_t kPhiTileBytes = sizeof(OzPhiTile);
 
 // max_c |A_c| over a shell's components (the expressions of ang_poly1, without its branch per component)
@@ -582,15 +588,16 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
         reinterpret_cast<int*>(base + L.e_pt)[q] = ept;
     }
     const int warp = tid >> 5, lane = tid & 31;
+    oz_stage_rows(g, m, 0, T.rg);
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
-        __syncthreads();  // the previous tile's digits are cut (and the points are stored)
+        __syncthreads();  // the previous tile's digits are cut (and the points and rows are stored)
         if (live) {
 #pragma unroll 4
             for (int r = 0; r < 16; ++r) {
                 const int mu = mu0 + r;
                 double v = 0.0;
                 if (mu < m.nb) {
-                    const OzRow row = oz_row(g, m, rad, mu);
+                    const OzRow row = oz_row_of(T.rg[r], m, rad);
                     double gx, gy, gz;
                     ao_from_radial<false>(row.t, T.x[tid] - row.ax, T.y[tid] - row.ay, T.z[tid] - row.az, row.S0[q],
                                           0.0, v, gx, gy, gz);
@@ -622,6 +629,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
             oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
+        oz_stage_rows(g, m, mu0 + 16, T.rg);  // every thread has formed this tile's values
     }
 }
 
@@ -680,6 +688,7 @@ struct OzGroupTile {
     double x[kGroupPts], y[kGroupPts], z[kGroupPts];
     double c[4][kGroupPts];
     double vt[16][kGroupPts + 1];
+    RowGeom rg[16];  // the tile's row geometry, staged during the previous tile's digit cut
     int eg[16];
 };
 constexpr size_t kGroupTileBytes = sizeof(OzGroupTile);
@@ -704,15 +713,16 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
         for (int k = 0; k < 4; ++k) T.c[k][tid] = coef[gp * 4 + k];
     }
     const int warp = tid >> 5, lane = tid & 31;
+    oz_stage_rows(g, m, 0, T.rg);
     for (int nu0 = 0; nu0 < m.nbp; nu0 += 16) {
-        __syncthreads();  // the previous tile's digits are cut (and the points are loaded)
+        __syncthreads();  // the previous tile's digits are cut (and the points and rows are loaded)
         if (live) {
 #pragma unroll 4
             for (int r = 0; r < 16; ++r) {
                 const int nu = nu0 + r;
                 double zv = 0.0;
                 if (nu < m.nb) {
-                    const OzRow row = oz_row(g, m, rad, nu);
+                    const OzRow row = oz_row_of(T.rg[r], m, rad);
                     const double dx = T.x[tid] - row.ax, dy = T.y[tid] - row.ay, dz = T.z[tid] - row.az;
                     double v, gx, gy, gz;
                     ao_from_radial<GGA>(row.t, dx, dy, dz, row.S0[q], GGA ? row.S1[q] : 0.0, v, gx, gy, gz);
@@ -744,6 +754,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
             oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
+        oz_stage_rows(g, m, nu0 + 16, T.rg);  // every thread has formed this tile's values
     }
 }
 

@@ -115,3 +115,27 @@ def test_mixed_incremental(water2, terms):
     exc_i, _, V_i = eng.build_vxc("B3LYP", 0.5 * PA, incremental=True)
     exc_f, _, V_f = eng.build_vxc("B3LYP", PA)
     assert within(exc_i, exc_f, V_i, V_f, TOL[6])
+
+
+def test_int8_accuracy_target_chain300():
+    """The accuracy target of the INT8 path, |dExc| <= 1e-6 Eh against the FP64 path, on a 300-atom
+    chain with the settings of the 2000-atom benchmark (device grid producer, USER 75x302, SS
+    weights, AO cut-off 1e-10); also Vxc and the electron count."""
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    syms, xyz = systems.peptide_chain(300, seed=11)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+    PA = 0.5 * systems.density_matrix(sh.nao, int(0.4 * sh.nao), seed=11)
+    radius = [grids.BRAGG_SLATER[int(z)] for z in sh.atom_z]
+    res = {}
+    for precision in ("fp64", "mixed"):
+        e = XcEngine(device=0, precision=precision, ao_cutoff=1e-10)
+        e.set_system(sh)
+        npts = e.generate_grid(radius, partition="SSWeight", **grids.PRESETS["USER-75x302"])
+        assert npts > 3_000_000
+        res[precision] = e.build_vxc("B3LYP", PA)
+        e.close()
+    (xf, nf, Vf), (xm, nm, Vm) = res["fp64"], res["mixed"]
+    assert abs(xm - xf) <= 1e-6
+    assert np.abs(Vm - Vf).max() <= OZ_TOL[1] * np.abs(Vf).max()
+    assert abs(nm - nf) <= 1e-6
