@@ -44,6 +44,44 @@ __device__ __forceinline__ void shell_radial(const BasisView& bas, int s, double
     }
 }
 
+// A shell as the AO kernels read it from shared memory (every thread of a CTA walks the same
+// shells, so broadcasts replace chains of dependent global loads): its atom, L and primitives.
+constexpr int kStagedPrims = 10;
+struct ShellRec {
+    double ax, ay, az;
+    int lq, np;  // np < 0: more than kStagedPrims primitives, read from the global tables
+    int sh, row0;
+    double alpha[kStagedPrims], coef[kStagedPrims];
+};
+
+__device__ __forceinline__ void stage_shell(const BasisView& bas, int sh, int row0, ShellRec& r) {
+    const int a = bas.sh_atom[sh], np = bas.sh_nprim[sh], p0 = bas.sh_p0[sh];
+    r.ax = bas.atom_xyz[3 * a], r.ay = bas.atom_xyz[3 * a + 1], r.az = bas.atom_xyz[3 * a + 2];
+    r.lq = bas.sh_l[sh], r.sh = sh, r.row0 = row0;
+    r.np = np <= kStagedPrims ? np : -1;
+    if (np <= kStagedPrims)
+        for (int k = 0; k < np; ++k) r.alpha[k] = bas.p_exp[p0 + k], r.coef[k] = bas.p_coef[p0 + k];
+}
+
+// shell_radial on a staged shell (the same operations in the same order)
+template <bool GGA>
+__device__ __forceinline__ void shell_radial_staged(const BasisView& bas, const ShellRec& r, double d2, double& S0,
+                                                    double& S1) {
+    if (r.np < 0) {
+        shell_radial<GGA>(bas, r.sh, d2, S0, S1);
+        return;
+    }
+    S0 = 0.0, S1 = 0.0;
+    for (int k = 0; k < r.np; ++k) {
+        const double al = r.alpha[k];
+        if (al * d2 <= 30.0) {
+            const double e = r.coef[k] * exp(-al * d2);
+            S0 += e;
+            if (GGA) S1 += al * e;
+        }
+    }
+}
+
 // Value and (GGA) gradient of component t at displacement (x, y, z) from the shell's atom.
 template <bool GGA>
 __device__ __forceinline__ void ao_from_radial(int t, double x, double y, double z, double S0, double S1, double& v,

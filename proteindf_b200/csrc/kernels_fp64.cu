@@ -236,7 +236,7 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_rho_functional(GridView g, int bl
 // forms phi and grad phi of every component from the radial sums (ao_from_radial, the
 // formulas of k_ao_eval) in row order, so rho and grad rho are summed as from stored planes,
 // and reads 2 nsh + nb rows per point instead of 5 nbp (and 2 nsh + nbp instead of 4 nbp for Z).
-// The shells' rows, angular momenta and atoms are staged in shared memory, 128 at a time.
+// The shells (rows, angular momenta, atoms, primitives) are staged in shared memory, 64 at a time.
 __global__ void __launch_bounds__(256) k_ao_eval_rad(BasisView bas, GridView g, int blk0, char* ws) {
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
@@ -248,20 +248,25 @@ __global__ void __launch_bounds__(256) k_ao_eval_rad(BasisView bas, GridView g, 
     double* S1p = S0p + (size_t)m.nsh * BLOCK_PTS;
     const int gp = blk * BLOCK_PTS + p;
     const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
-    for (int i = half; i < m.nsh; i += 2) {
-        const int s = g.blk_shells[m.sh0 + i];
-        const int row0 = g.blk_shell_row[m.sh0 + i];
-        const int a = bas.sh_atom[s];
-        const double x = rx - bas.atom_xyz[3 * a], y = ry - bas.atom_xyz[3 * a + 1], z = rz - bas.atom_xyz[3 * a + 2];
-        const int L = bas.sh_l[s], n = 2 * L + 1;
-        double S0, S1;
-        shell_radial<true>(bas, s, x * x + y * y + z * z, S0, S1);
-        S0p[(size_t)i * BLOCK_PTS + p] = S0;
-        S1p[(size_t)i * BLOCK_PTS + p] = S1;
-        for (int c = 0; c < n; ++c) {
-            double v, gx, gy, gz;
-            ao_from_radial<false>(L * L + c, x, y, z, S0, S1, v, gx, gy, gz);
-            phi[(size_t)(row0 + c) * BLOCK_PTS + p] = v;
+    __shared__ ShellRec recs[64];  // the block's shells, 64 at a time
+    for (int i0 = 0; i0 < m.nsh; i0 += 64) {
+        __syncthreads();
+        for (int k = threadIdx.x; k < 64 && i0 + k < m.nsh; k += blockDim.x)
+            stage_shell(bas, g.blk_shells[m.sh0 + i0 + k], g.blk_shell_row[m.sh0 + i0 + k], recs[k]);
+        __syncthreads();
+        for (int i = i0 + half; i < min(i0 + 64, m.nsh); i += 2) {
+            const ShellRec& r = recs[i - i0];
+            const double x = rx - r.ax, y = ry - r.ay, z = rz - r.az;
+            const int L = r.lq, n = 2 * L + 1;
+            double S0, S1;
+            shell_radial_staged<true>(bas, r, x * x + y * y + z * z, S0, S1);
+            S0p[(size_t)i * BLOCK_PTS + p] = S0;
+            S1p[(size_t)i * BLOCK_PTS + p] = S1;
+            for (int c = 0; c < n; ++c) {
+                double v, gx, gy, gz;
+                ao_from_radial<false>(L * L + c, x, y, z, S0, S1, v, gx, gy, gz);
+                phi[(size_t)(r.row0 + c) * BLOCK_PTS + p] = v;
+            }
         }
     }
     for (int r = m.nb + half; r < m.nbp; r += 2) phi[(size_t)r * BLOCK_PTS + p] = 0.0;

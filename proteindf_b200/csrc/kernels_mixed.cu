@@ -547,14 +547,6 @@ __device__ __forceinline__ void oz_stage_rows(const GridView& g, const BlockMeta
 }
 constexpr size_t kPhiTileBytes = sizeof(OzPhiTile);
 
-// A shell of a group's basis as pass 1 of k_phi_group reads it from shared memory.
-constexpr int kOzStagedPrims = 10;
-struct OzShellRec {
-    double ax, ay, az;
-    int lq, np;
-    double alpha[kOzStagedPrims], coef[kOzStagedPrims];
-};
-
 // max_c |A_c| over a shell's components (the expressions of ang_poly1, without its branch per component)
 __device__ __forceinline__ double ang_max_abs(int L, double x, double y, double z) {
     if (L == 0) return 1.0;
@@ -577,29 +569,13 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
     char* base = ws + g.meta[lead + (live ? b : 0)].ws;
     double* rad = reinterpret_cast<double*>(base + L.rad);
     int ept = kOzZeroExp;
-    // The group's shell table (atom position, L, primitives) in the tile buffer, which pass 1
-    // does not use: every thread reads every shell, so shared-memory broadcasts replace chains of
-    // dependent global loads. A group whose table does not fit, or with a shell of more than
-    // kOzStagedPrims primitives, reads the global tables (the flag is uniform over the CTA).
-    OzShellRec* recs = reinterpret_cast<OzShellRec*>(&T.vt[0][0]);
-    __shared__ int s_global;
-    if (tid == 0) s_global = (size_t)m.nsh * sizeof(OzShellRec) > sizeof(T.vt);
+    // The group's shell table in the tile buffer, which pass 1 does not use (a group whose table
+    // does not fit reads the global tables; m.nsh is uniform over the CTA).
+    ShellRec* recs = reinterpret_cast<ShellRec*>(&T.vt[0][0]);
+    const bool staged = (size_t)m.nsh * sizeof(ShellRec) <= sizeof(T.vt);
+    if (staged)
+        for (int i = tid; i < m.nsh; i += blockDim.x) stage_shell(bas, g.blk_shells[m.sh0 + i], 0, recs[i]);
     __syncthreads();
-    if (!s_global)
-        for (int i = tid; i < m.nsh; i += blockDim.x) {
-            const int sh = g.blk_shells[m.sh0 + i];
-            const int a = bas.sh_atom[sh], np = bas.sh_nprim[sh], p0 = bas.sh_p0[sh];
-            if (np > kOzStagedPrims) {
-                s_global = 1;  // any writer sets the same value
-                continue;
-            }
-            OzShellRec& r = recs[i];
-            r.ax = bas.atom_xyz[3 * a], r.ay = bas.atom_xyz[3 * a + 1], r.az = bas.atom_xyz[3 * a + 2];
-            r.lq = bas.sh_l[sh], r.np = np;
-            for (int k = 0; k < np; ++k) r.alpha[k] = bas.p_exp[p0 + k], r.coef[k] = bas.p_coef[p0 + k];
-        }
-    __syncthreads();
-    const bool staged = !s_global;
     if (live) {
         const size_t gp = (size_t)(lead + b) * BLOCK_PTS + q;
         const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
@@ -608,20 +584,11 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
         for (int i = 0; i < m.nsh; ++i) {
             double x, y, z, S0, S1;
             int Lq;
-            if (staged) {  // the operations of shell_radial, on the staged table
-                const OzShellRec& r = recs[i];
+            if (staged) {
+                const ShellRec& r = recs[i];
                 x = rx - r.ax, y = ry - r.ay, z = rz - r.az;
                 Lq = r.lq;
-                const double d2 = x * x + y * y + z * z;
-                S0 = 0.0, S1 = 0.0;
-                for (int k = 0; k < r.np; ++k) {
-                    const double al = r.alpha[k];
-                    if (al * d2 <= 30.0) {
-                        const double e = r.coef[k] * exp(-al * d2);
-                        S0 += e;
-                        if (GGA) S1 += al * e;
-                    }
-                }
+                shell_radial_staged<GGA>(bas, r, x * x + y * y + z * z, S0, S1);
             } else {
                 const int sh = g.blk_shells[m.sh0 + i];
                 const int a = bas.sh_atom[sh];
