@@ -480,14 +480,13 @@ __device__ __forceinline__ uint32_t oz_word(double v, double sc) {
     const uint32_t x = (u3 << 24) | ((u2 - 255u * u3) << 16) | ((u1 - 255u * u2) << 8) | (u - 255u * u1);
     return ((x & 0x7F7F7F7Fu) + 0x01010101u) ^ ((x ^ 0x81818181u) & 0x80808080u);
 }
-__device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
-    const double sc = oz_digit_scale(e);
+// 16 values' digit words (byte i of a word = digit s_{4-i}) to the four digit planes
+__device__ __forceinline__ void oz_store16_words(char* base, size_t plane, size_t off, const uint32_t* wd) {
     uint4 d[OZ_SLICES];
     uint32_t* dw = reinterpret_cast<uint32_t*>(d);
 #pragma unroll
     for (int g = 0; g < 4; ++g) {
-        const uint32_t a = oz_word(v[4 * g], sc), b = oz_word(v[4 * g + 1], sc), c = oz_word(v[4 * g + 2], sc),
-                       w = oz_word(v[4 * g + 3], sc);
+        const uint32_t a = wd[4 * g], b = wd[4 * g + 1], c = wd[4 * g + 2], w = wd[4 * g + 3];
         const uint32_t t0 = __byte_perm(a, b, 0x5140), t1 = __byte_perm(a, b, 0x7362);
         const uint32_t t2 = __byte_perm(c, w, 0x5140), t3 = __byte_perm(c, w, 0x7362);
         dw[3 * 4 + g] = __byte_perm(t0, t2, 0x5410);  // byte 0: s_4
@@ -497,6 +496,13 @@ __device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off,
     }
 #pragma unroll
     for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = d[i];
+}
+__device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
+    const double sc = oz_digit_scale(e);
+    uint32_t w[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) w[j] = oz_word(v[j], sc);
+    oz_store16_words(base, plane, off, w);
 }
 
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -649,24 +655,32 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
     }
 }
 
-// Exponents of the rows of P (a warp per row): the scale of a row of every group's P_sub.
-// The maximum over the whole row bounds the maximum over a group's columns, so the digits
-// stay in range; a row's largest elements (near its diagonal) are in every group that
-// holds the row, so the scale is, almost always, the sub-row's own.
-__global__ void __launch_bounds__(256) k_p_rowexp(const double* __restrict__ P, int nao, int* __restrict__ e) {
+// The digits of P, once per build (a warp per row): the row's exponent (the scale of that row in
+// every group's P_sub; the maximum over the whole row bounds the maximum over a group's
+// columns, so the digits stay in range, and a row's largest elements, near its diagonal, lie in
+// every group that holds the row, so the scale is almost always the sub-row's own), then each
+// element's four digits as one word. The groups' P_sub packing then gathers 4-byte words
+// instead of 8-byte values and cuts nothing.
+__global__ void __launch_bounds__(256) k_p_digits(const double* __restrict__ P, int nao, const int* __restrict__ row_cols,
+                                                  int* __restrict__ e, uint32_t* __restrict__ words) {
     const int row = blockIdx.x * 8 + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (row >= nao) return;
+    const int c0 = row_cols ? row_cols[2 * row] : 0, c1 = row_cols ? row_cols[2 * row + 1] : nao;
     const double* r = P + (size_t)row * nao;
     double mx = 0.0;
-    for (int c = lane; c < nao; c += 32) mx = fmax(mx, fabs(__ldg(r + c)));
+    for (int c = c0 + lane; c < c1; c += 32) mx = fmax(mx, fabs(__ldg(r + c)));
     mx = warp_max_d(mx);
-    if (lane == 0) e[row] = oz_exponent(mx);
+    const int er = oz_exponent(mx);
+    if (lane == 0) e[row] = er;
+    const double sc = oz_digit_scale(er);
+    uint32_t* w = words + (size_t)row * nao;
+    for (int c = c0 + lane; c < c1; c += 32) w[c] = oz_word(__ldg(r + c), sc);
 }
 
-// P_sub digits of a group, one gather of P[aos[mu]][aos[nu]] (L2-resident for a few thousand
-// AOs) with the rows' exponents of P. A warp takes 8 rows x 64 columns (lane = row r, K group
-// kg: 16 columns), so each digit store instruction writes four whole 128-byte core matrices.
-__global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __restrict__ P, int nao,
+// P_sub digits of a group: a gather of the words of P[aos[mu]][aos[nu]] (the digit words of a
+// zero are 0). A warp takes 8 rows x 64 columns (lane = row r, K group kg: 16 columns), so each
+// digit store instruction writes four whole 128-byte core matrices.
+__global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* __restrict__ words, int nao,
                                                    const int* __restrict__ grp, const int* __restrict__ p_rowexp,
                                                    char* ws) {
     const int blk = grp[blockIdx.x];  // one CTA per group: P_sub lives in the first block's region
@@ -678,20 +692,19 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const double* __r
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = lane & 7, kg = lane >> 3;
     const int nk = m.nbp / 64;
-    double v[16];
+    uint32_t w[16];
     for (int t = warp; t < (m.nbp / 8) * nk; t += blockDim.x / 32) {
         const int mu = (t / nk) * 8 + r, k0 = (t % nk) * 64 + kg * 16;
         const bool live = mu < m.nb;
         const int amu = live ? aos[mu] : 0;
-        const int e = live ? __ldg(p_rowexp + amu) : kOzZeroExp;
-        if (kg == 0 && k0 == 0) e_p[mu] = e;
-        const double* row = P + (size_t)amu * nao;
+        if (kg == 0 && k0 == 0) e_p[mu] = live ? __ldg(p_rowexp + amu) : kOzZeroExp;
+        const uint32_t* row = words + (size_t)amu * nao;
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
             const int nu = k0 + j;
-            v[j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0.0;
+            w[j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0u;
         }
-        oz_store16(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, k0, m.nbp), v, e);
+        oz_store16_words(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, k0, m.nbp), w);
     }
 }
 
@@ -1175,8 +1188,8 @@ void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, boo
                                                              coef, blk_sum);
 }
 
-void oz_p_rowexp(const double* P, int nao, int* e, cudaStream_t s) {
-    k_p_rowexp<<<(nao + 7) / 8, 256, 0, s>>>(P, nao, e);
+void oz_p_digits(const double* P, int nao, const int* row_cols, int* e, uint32_t* words, cudaStream_t s) {
+    k_p_digits<<<(nao + 7) / 8, 256, 0, s>>>(P, nao, row_cols, e, words);
 }
 
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
@@ -1188,7 +1201,7 @@ void oz_prepare(const MixedArgs& a, cudaStream_t s) {
         cudaFuncSetAttribute(k_phi_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiTileBytes);
         k_phi_group<false><<<a.ngrp, kGroupPts, kPhiTileBytes, s>>>(a.b, a.g, a.grp, a.ws);
     }
-    k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.P, a.nao, a.grp, a.p_rowexp, a.ws);
+    k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.p_words, a.nao, a.grp, a.p_rowexp, a.ws);
 }
 
 // Persistent contraction grid: one CTA per SM (its shared memory and all 512 TMEM columns

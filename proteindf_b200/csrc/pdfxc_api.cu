@@ -309,6 +309,9 @@ pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz,
         dev_free(ctx->d_Vprev);  // the delta history belongs to the old system
         ctx->vprev_iter = 0;
         dev_alloc(&ctx->d_p_rowexp, (size_t)ao);
+        dev_free(ctx->d_p_words);
+        dev_free(ctx->d_row_cols);  // a batch sets it after this call
+        if (ctx->opt.precision == PDFXC_PRECISION_MIXED && ctx->opt.split_terms == 10) dev_alloc(&ctx->d_p_words, n2);
         dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b);  // open shell: sized on first use
         PDFXC_CUDA(cudaStreamSynchronize(s));
         free_grid(ctx);
@@ -917,7 +920,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         memset_async(ctx->d_rho_acc, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
         if (ctx->opt.split_terms == 10) {
-            pdfxc::oz_p_rowexp(d_PA, nao, ctx->d_p_rowexp, s);
+            pdfxc::oz_p_digits(d_PA, nao, ctx->d_row_cols, ctx->d_p_rowexp, ctx->d_p_words, s);
             ++launches;
         }
     }
@@ -939,7 +942,8 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         const int g_hi = (int)(std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), cb0 + cn) - ctx->h_grp.begin());
         pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
-                           ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp};
+                           ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp,
+                           ctx->d_p_words};
         const bool oz = ctx->opt.split_terms == 10;
         PDFXC_CUDA(cudaEventRecord(e[0], s));
         oz ? pdfxc::oz_prepare(a, s) : pdfxc::mixed_prepare(a, s);
@@ -1556,6 +1560,13 @@ pdfxc_status pdfxc_set_batch(pdfxc_ctx* ctx, int nmol, const pdfxc_mol* mols) {
         build_grid(ctx, pt_off, xyzw.data(), owners ? owner.data() : nullptr, segs);
         ctx->mol = aoff;
         dev_alloc(&ctx->d_mol_sums, 2 * (size_t)nmol);
+        // the joint P holds each molecule's P_A in its diagonal block and nothing else: rows
+        // read only their own molecule's columns
+        std::vector<int> cols(2 * (size_t)aoff.back());
+        for (int m = 0; m < nmol; ++m)
+            for (int r = aoff[m]; r < aoff[m + 1]; ++r) cols[2 * r] = aoff[m], cols[2 * r + 1] = aoff[m + 1];
+        upload(&ctx->d_row_cols, cols, ctx->stream);
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
         return PDFXC_OK;
     });
 }
@@ -1709,7 +1720,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
     dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
-    dev_free(ctx->d_p_rowexp); dev_free(ctx->d_Vprev);
+    dev_free(ctx->d_p_rowexp); dev_free(ctx->d_Vprev); dev_free(ctx->d_p_words); dev_free(ctx->d_row_cols);
     dev_free(ctx->d_P_b), dev_free(ctx->d_V_b), dev_free(ctx->d_Vacc_b), dev_free(ctx->d_scalars_b);
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);

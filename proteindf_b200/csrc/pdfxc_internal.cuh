@@ -139,6 +139,8 @@ struct pdfxc_ctx {
     int vprev_iter = 0;           // its SCF iteration, 0 = none
     double* d_Vacc = nullptr;     // n_ao^2 non-symmetric accumulator
     int* d_p_rowexp = nullptr;    // n_ao: exponents of the rows of P (INT8 path)
+    uint32_t* d_p_words = nullptr;  // n_ao^2: the four digits of each element of P (INT8 path)
+    int* d_row_cols = nullptr;      // batch: per AO row its molecule's columns [c0, c1) (2 ints)
     bool rho_valid = false;
     pdfxc_ctx* dens = nullptr;  // pdfxc_density: FP64 context over the requested points (same system)
     int* d_nbr_idx = nullptr;     // Stratmann-Scuseria weights: per atom the other atoms by distance
@@ -363,7 +365,8 @@ struct MixedArgs {
     int* err;
     const int* grp;  // first blocks of the chunk's groups (INT8 path)
     int ngrp;
-    const int* p_rowexp;  // exponents of the rows of P (INT8 path)
+    const int* p_rowexp;      // exponents of the rows of P (INT8 path)
+    const uint32_t* p_words;  // the four digits of each element of P (INT8 path)
 };
 void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
 void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue
@@ -371,7 +374,8 @@ void mixed_functional(const MixedArgs& a, cudaStream_t s);  // functional, Z pac
 void mixed_vxc(const MixedArgs& a, cudaStream_t s);         // Vacc += phi Z^T
 size_t umma_smem_bytes(int nterms);
 // the same four stages with INT8 fixed-point slices (split_terms == 10)
-void oz_p_rowexp(const double* P, int nao, int* e, cudaStream_t s);  // once per build
+// once per build; row_cols (batch, may be null): each row's molecule's columns, the only ones read
+void oz_p_digits(const double* P, int nao, const int* row_cols, int* e, uint32_t* words, cudaStream_t s);
 void oz_prepare(const MixedArgs& a, cudaStream_t s);
 void oz_rho(const MixedArgs& a, cudaStream_t s);
 void oz_functional(const MixedArgs& a, cudaStream_t s);
