@@ -542,9 +542,29 @@ constexpr int kGroupPts = 4 * BLOCK_PTS;
 struct OzPhiTile {
     double x[kGroupPts], y[kGroupPts], z[kGroupPts];
     double vt[16][kGroupPts + 1];
-    RowGeom rg[16];  // the tile's row geometry, staged during the previous tile's digit cut
+    RowGeom rg[2][16];  // row geometry of this tile and the next (staged during this tile's row maxima)
     int eg[16];
 };
+
+// Prefetch into L1 of the line holding p (no wait, no register).
+__device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
+
+// L1 prefetches of this thread's radial sums (S0, and S1 for a GGA) of the shells of 16 rows.
+template <bool S1>
+__device__ __forceinline__ void oz_prefetch_rows(const RowGeom* rg, int r0, const BlockMeta& m, const double* rad,
+                                                 int q) {
+    int prev = -1;
+#pragma unroll 4
+    for (int r = 0; r < 16; ++r) {
+        if (r0 + r >= m.nb) break;
+        const int slot = rg[r].info >> 4;
+        if (slot != prev) {
+            prefetch_l1(rad + (size_t)slot * BLOCK_PTS + q);
+            if (S1) prefetch_l1(rad + (size_t)(m.nsh + slot) * BLOCK_PTS + q);
+            prev = slot;
+        }
+    }
+}
 
 // Row geometry of rows r0 .. r0 + 15 into rg by the CTA's last 16 threads (zero past the last row).
 __device__ __forceinline__ void oz_stage_rows(const GridView& g, const BlockMeta& m, int r0, RowGeom* rg) {
@@ -610,8 +630,9 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
         reinterpret_cast<int*>(base + L.e_pt)[q] = ept;
     }
     const int warp = tid >> 5, lane = tid & 31;
-    oz_stage_rows(g, m, 0, T.rg);
+    oz_stage_rows(g, m, 0, T.rg[0]);
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
+        const int cur = (mu0 >> 4) & 1;
         __syncthreads();  // the previous tile's digits are cut (and the points and rows are stored)
         if (live) {
 #pragma unroll 4
@@ -619,7 +640,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
                 const int mu = mu0 + r;
                 double v = 0.0;
                 if (mu < m.nb) {
-                    const OzRow row = oz_row_of(T.rg[r], m, rad);
+                    const OzRow row = oz_row_of(T.rg[cur][r], m, rad);
                     double gx, gy, gz;
                     ao_from_radial<false>(row.t, T.x[tid] - row.ax, T.y[tid] - row.ay, T.z[tid] - row.az, row.S0[q],
                                           0.0, v, gx, gy, gz);
@@ -640,8 +661,10 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
                 reinterpret_cast<int*>(ws + m.ws + L.e_phi_g)[mu0 + warp] = e;
             }
         }
+        oz_stage_rows(g, m, mu0 + 16, T.rg[cur ^ 1]);  // every thread has formed this tile's values
         __syncthreads();
         if (live) {
+            oz_prefetch_rows<false>(T.rg[cur ^ 1], mu0 + 16, m, rad, q);  // the next tile's S0, under the cut
             double v[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = T.vt[j][tid];
@@ -651,7 +674,6 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
             oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
-        oz_stage_rows(g, m, mu0 + 16, T.rg);  // every thread has formed this tile's values
     }
 }
 
@@ -717,7 +739,7 @@ struct OzGroupTile {
     double x[kGroupPts], y[kGroupPts], z[kGroupPts];
     double c[4][kGroupPts];
     double vt[16][kGroupPts + 1];
-    RowGeom rg[16];  // the tile's row geometry, staged during the previous tile's digit cut
+    RowGeom rg[2][16];  // row geometry of this tile and the next (staged during this tile's row maxima)
     int eg[16];
 };
 constexpr size_t kGroupTileBytes = sizeof(OzGroupTile);
@@ -742,8 +764,9 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
         for (int k = 0; k < 4; ++k) T.c[k][tid] = coef[gp * 4 + k];
     }
     const int warp = tid >> 5, lane = tid & 31;
-    oz_stage_rows(g, m, 0, T.rg);
+    oz_stage_rows(g, m, 0, T.rg[0]);
     for (int nu0 = 0; nu0 < m.nbp; nu0 += 16) {
+        const int cur = (nu0 >> 4) & 1;
         __syncthreads();  // the previous tile's digits are cut (and the points and rows are loaded)
         if (live) {
 #pragma unroll 4
@@ -751,7 +774,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
                 const int nu = nu0 + r;
                 double zv = 0.0;
                 if (nu < m.nb) {
-                    const OzRow row = oz_row_of(T.rg[r], m, rad);
+                    const OzRow row = oz_row_of(T.rg[cur][r], m, rad);
                     const double dx = T.x[tid] - row.ax, dy = T.y[tid] - row.ay, dz = T.z[tid] - row.az;
                     double v, gx, gy, gz;
                     ao_from_radial<GGA>(row.t, dx, dy, dz, row.S0[q], GGA ? row.S1[q] : 0.0, v, gx, gy, gz);
@@ -775,7 +798,9 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
                 reinterpret_cast<int*>(ws + m.ws + L.e_z_g)[nu0 + r] = e;
             }
         }
+        oz_stage_rows(g, m, nu0 + 16, T.rg[cur ^ 1]);  // every thread has formed this tile's values
         __syncthreads();
+        if (live) oz_prefetch_rows<GGA>(T.rg[cur ^ 1], nu0 + 16, m, rad, q);  // the next tile's sums, under the cut
         if (live) {  // thread = (block b, row r, 16 points kg) of the tile
             const int r = (q & 7) + 8 * (q >> 6), kg = (q >> 3) & 7;
             double v[16];
@@ -783,7 +808,6 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
             oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
-        oz_stage_rows(g, m, nu0 + 16, T.rg);  // every thread has formed this tile's values
     }
 }
 
