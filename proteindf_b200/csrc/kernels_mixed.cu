@@ -823,9 +823,10 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
 // commits it to tfull[set], and warps 2..9 run the epilogue of the item before, reading set
 // and releasing it through tempty[set]. So one item's epilogue runs under the next item's
 // copies and MMAs. A stage holds the A tile's four digit planes (128 rows x 64 K, canonical
-// no-swizzle K-major layout, 8 KiB each) and the B tile's four digit planes (64 rows x 64 K,
-// 4 KiB each): the 64-row half of a packed 128-row tile is four 1 KiB core-matrix groups,
-// copied into a compact layout (LBO 1024 B).
+// no-swizzle K-major layout, 8 KiB each) and the B tile's four digit planes (64 rows x 64 K) as
+// two stacked pairs [B_1; B_2], [B_3; B_4] of 128 rows in the A tiles' layout (8 KiB each): the
+// 64-row half of a packed 128-row tile is four 1 KiB core-matrix groups, and plane b's group kg
+// goes to pair b / 2, rows 64 (b % 2) onward, of the pair's k16 group kg.
 constexpr int OZ_NT = 64;
 constexpr int OZ_STAGES = 2;
 constexpr uint32_t OZ_A_BYTES = OZ_SLICES * umma::I8_SLAB_BYTES;   // 32 KiB
@@ -866,10 +867,25 @@ __device__ __forceinline__ bool oz_item(const GridView& g, int blk0, const int* 
     return mt < ntiles && nt < 2 * ntiles;
 }
 
-// Slice pairs (i, j), 1-based, with i + j <= 5, grouped by order i + j: pair t is nibble t of
-// these constants (i: 1 1 2 1 2 3 1 2 3 4, j: 1 2 1 3 2 1 4 3 2 1), so unrolled loops fold them.
-__device__ __forceinline__ constexpr int oz_pair_a(int t) { return (int)((0x4321321211ull >> (4 * t)) & 15); }
-__device__ __forceinline__ constexpr int oz_pair_b(int t) { return (int)((0x1234123121ull >> (4 * t)) & 15); }
+// The 10 slice products A_i B_j^T with i + j <= 5 as six MMAs per K step. Product (i, j) goes to
+// the accumulator of order i + j, at TMEM columns 64 (i + j - 2); for one A plane the products
+// with consecutive j land in adjacent 64-column ranges, so the stage stores the B planes as two
+// stacked pairs [B_1; B_2] and [B_3; B_4] (128 rows each, the layout of a 128-row A tile) and
+// one N = 128 MMA computes two products:
+//   t  A plane  B pair  N    columns  orders
+//   0  1        0       128  0..127   2, 3
+//   1  1        1       128  128..255 4, 5
+//   2  2        0       128  64..191  3, 4
+//   3  2        1 (B_3) 64   192..255 5
+//   4  3        0       128  128..255 4, 5
+//   5  4        0 (B_1) 64   192..255 5
+// (nibble t of each constant; unrolled loops fold them). The per-instruction cost of the
+// tensor core is nearly the same for N = 64 and N = 128, so six MMAs take about 60 % of the time
+// of ten.
+__device__ __forceinline__ constexpr int oz_mma_a(int t) { return (int)((0x432211u >> (4 * t)) & 15); }
+__device__ __forceinline__ constexpr int oz_mma_pair(int t) { return (int)((0x001010u >> (4 * t)) & 15); }
+__device__ __forceinline__ constexpr int oz_mma_wide(int t) { return (int)((0x010111u >> (4 * t)) & 15); }
+__device__ __forceinline__ constexpr int oz_mma_col(int t) { return (int)((0x323120u >> (4 * t)) & 15); }
 
 template <int MODE, bool GGA>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
@@ -950,7 +966,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                                        &full[st]);
                     for (int b = 0; b < OZ_SLICES; ++b)
                         for (int kg = 0; kg < 4; ++kg)
-                            umma::bulk_g2s(sp + OZ_A_BYTES + b * OZ_B_SLICE + kg * 1024,
+                            umma::bulk_g2s(sp + OZ_A_BYTES + (b >> 1) * 8192 + kg * 2048 + (b & 1) * 1024,
                                            Bs + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
                 }
             }
@@ -958,7 +974,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {  // MMAs
-            const uint32_t idesc = umma::instr_desc_s8(128, OZ_NT);
+            const uint32_t idesc128 = umma::instr_desc_s8(128, 2 * OZ_NT), idesc64 = umma::instr_desc_s8(128, OZ_NT);
             uint32_t gj = 0;
             int li = 0;
             bool ok = true;
@@ -986,18 +1002,18 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     // to the start-address field (addresses stay below 256 KiB, so it cannot carry)
                     const uint32_t sp = umma::smem_u32(smem + st * OZ_STAGE_BYTES);
                     const uint64_t ad0 = umma::smem_desc(sp, umma::LBO, umma::SBO);
-                    const uint64_t bd0 = umma::smem_desc(sp + OZ_A_BYTES, 1024, umma::SBO);
+                    const uint64_t bd0 = umma::smem_desc(sp + OZ_A_BYTES, umma::LBO, umma::SBO);
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
 #pragma unroll
-                        for (int t = 0; t < 10; ++t) {
-                            const int i = oz_pair_a(t), jj = oz_pair_b(t);
-                            const uint32_t acc = tacc + (uint32_t)(i + jj - 2) * OZ_NT;
+                        for (int t = 0; t < 6; ++t) {
+                            const int i = oz_mma_a(t);
                             const uint64_t ad = ad0 + (uint64_t)(((i - 1) * umma::I8_SLAB_BYTES + kk * 4096) >> 4);
-                            const uint64_t bd = bd0 + (uint64_t)(((jj - 1) * OZ_B_SLICE + kk * 2048) >> 4);
-                            // the first product of each order starts its accumulator
-                            const bool first = (j == 0 && kk == 0 && (t == 0 || t == 1 || t == 3 || t == 6));
-                            umma::mma_s8(acc, ad, bd, idesc, first ? 0u : 1u);
+                            const uint64_t bd = bd0 + (uint64_t)((oz_mma_pair(t) * 8192 + kk * 4096) >> 4);
+                            // the two MMAs of A_1 start all four accumulators
+                            const bool first = (j == 0 && kk == 0 && t < 2);
+                            umma::mma_s8(tacc + (uint32_t)oz_mma_col(t) * OZ_NT, ad, bd,
+                                         oz_mma_wide(t) ? idesc128 : idesc64, first ? 0u : 1u);
                         }
                     }
                     umma::mma_commit(&empty[st]);
