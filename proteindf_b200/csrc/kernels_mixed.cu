@@ -480,8 +480,29 @@ __device__ __forceinline__ uint32_t oz_word(double v, double sc) {
     const uint32_t x = (u3 << 24) | ((u2 - 255u * u3) << 16) | ((u1 - 255u * u2) << 8) | (u - 255u * u1);
     return ((x & 0x7F7F7F7Fu) + 0x01010101u) ^ ((x ^ 0x81818181u) & 0x80808080u);
 }
+// Digit-plane layouts in HBM, in the order the contraction stages need them, so that a stage is
+// two bulk copies. Within a 64-K slab the canonical no-swizzle K-major core-matrix order of a
+// 128-row tile, [k16 group][8-row group][8 rows x 16 bytes].
+// * A operands (128-row tiles: phi^T for rho, phi for Vxc): per (tile, slab) the four planes'
+//   8 KiB slabs one after another (32 KiB); plane i at + 8192 i.
+// * B operands (64-row tiles: P_sub for rho, Z for Vxc): per (64-row tile, slab) two 8 KiB pairs
+//   [B_1; B_2], [B_3; B_4] in the layout of a 128-row slab, plane i at rows 64 (i % 2) of pair
+//   i / 2 (16 KiB); plane i at + 8192 (i / 2) + 1024 (i % 2).
+struct OzPlanes {
+    uint32_t pair, half;  // plane i lies (i / 2) pair + (i % 2) half bytes after plane 0
+};
+constexpr OzPlanes kOzPlanesA{16384, 8192}, kOzPlanesB{8192, 1024};
+__host__ __device__ inline size_t oz_off_a(int r, int k, int K) {
+    return ((size_t)(r / 128) * (K / 64) + k / 64) * 32768 + (size_t)((((k % 64) / 16) * 16 + (r % 128) / 8) * 128) +
+           (r % 8) * 16 + (k % 16);
+}
+__host__ __device__ inline size_t oz_off_b(int r, int k, int K) {
+    return ((size_t)(r / 64) * (K / 64) + k / 64) * 16384 + (size_t)(((k % 64) / 16) * 2048 + ((r % 64) / 8) * 128) +
+           (r % 8) * 16 + (k % 16);
+}
+
 // 16 values' digit words (byte i of a word = digit s_{4-i}) to the four digit planes
-__device__ __forceinline__ void oz_store16_words(char* base, size_t plane, size_t off, const uint32_t* wd) {
+__device__ __forceinline__ void oz_store16_words(char* base, OzPlanes pl, size_t off, const uint32_t* wd) {
     uint4 d[OZ_SLICES];
     uint32_t* dw = reinterpret_cast<uint32_t*>(d);
 #pragma unroll
@@ -495,14 +516,15 @@ __device__ __forceinline__ void oz_store16_words(char* base, size_t plane, size_
         dw[0 * 4 + g] = __byte_perm(t1, t3, 0x7632);  // byte 3: s_1
     }
 #pragma unroll
-    for (int i = 0; i < OZ_SLICES; ++i) *reinterpret_cast<uint4*>(base + i * plane + off) = d[i];
+    for (int i = 0; i < OZ_SLICES; ++i)
+        *reinterpret_cast<uint4*>(base + off + (i >> 1) * pl.pair + (i & 1) * pl.half) = d[i];
 }
-__device__ __forceinline__ void oz_store16(char* base, size_t plane, size_t off, const double* v, int e) {
+__device__ __forceinline__ void oz_store16(char* base, OzPlanes pl, size_t off, const double* v, int e) {
     const double sc = oz_digit_scale(e);
     uint32_t w[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) w[j] = oz_word(v[j], sc);
-    oz_store16_words(base, plane, off, w);
+    oz_store16_words(base, pl, off, w);
 }
 
 __device__ __forceinline__ double warp_max_d(double v) {
@@ -668,11 +690,11 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
             double v[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = T.vt[j][tid];
-            oz_store16(base + L.phi1, L.phi1_plane, umma::packed_offset_i8(q, mu0, m.nbp), v, ept);
+            oz_store16(base + L.phi1, kOzPlanesA, oz_off_a(q, mu0, m.nbp), v, ept);
             const int r = (q & 7) + 8 * (q >> 6), kg = (q >> 3) & 7;
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
-            oz_store16(base + L.phi2, L.phi2_plane, umma::packed_offset_i8(mu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
+            oz_store16(base + L.phi2, kOzPlanesA, oz_off_a(mu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
     }
 }
@@ -726,7 +748,7 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* _
             const int nu = k0 + j;
             w[j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0u;
         }
-        oz_store16_words(base + L.ppack, L.ppack_plane, umma::packed_offset_i8(mu, k0, m.nbp), w);
+        oz_store16_words(base + L.ppack, kOzPlanesB, oz_off_b(mu, k0, m.nbp), w);
     }
 }
 
@@ -806,7 +828,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
             double v[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
-            oz_store16(base + L.zpack, L.zpack_plane, umma::packed_offset_i8(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
+            oz_store16(base + L.zpack, kOzPlanesB, oz_off_b(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
     }
 }
@@ -933,18 +955,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 const OzLayout L = oz_layout(m.nbp, m.nsh);
                 const char* base = ws + m.ws;
                 const char* lead = ws + g.meta[m.lead].ws;
-                size_t Ao, Bo, Aplane, Bplane;
-                int nslabs;
+                // per slab one 32 KiB A copy and one 16 KiB B copy (the layouts of oz_off_a, oz_off_b)
+                size_t Ao, Bo;
+                int nslabs, kslabs;  // slabs of the item; slabs per block of the K extent
                 if (MODE == MODE_RHO) {
-                    Ao = L.phi1, Aplane = L.phi1_plane;
-                    Bo = L.ppack + (size_t)(nt / 2) * umma::TILE_ROWS * m.nbp, Bplane = L.ppack_plane;
-                    nslabs = m.nbp / (int)umma::I8_SLAB_K;
+                    nslabs = kslabs = m.nbp / (int)umma::I8_SLAB_K;
+                    Ao = L.phi1;
+                    Bo = L.ppack + (size_t)nt * kslabs * 16384;
                 } else {
-                    Ao = L.phi2 + (size_t)mt * umma::TILE_ROWS * BLOCK_PTS, Aplane = L.phi2_plane;
-                    Bo = L.zpack + (size_t)(nt / 2) * umma::TILE_ROWS * BLOCK_PTS, Bplane = L.zpack_plane;
+                    kslabs = kBlockSlabs;
                     nslabs = m.gn * kBlockSlabs;
+                    Ao = L.phi2 + (size_t)mt * kslabs * 32768;
+                    Bo = L.zpack + (size_t)nt * kslabs * 16384;
                 }
-                const size_t bhalf = (size_t)(nt & 1) * 8 * 128;  // row groups 8..15 of the 128-row tile
                 for (int j = 0; j < nslabs; ++j, ++gj) {
                     const int st = gj % S;
                     if (gj >= S && !umma::mbar_wait(&empty[st], ((gj / S) - 1) & 1, err)) {
@@ -955,19 +978,14 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     uint8_t* sp = smem + st * OZ_STAGE_BYTES;
                     umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
                     const char *As = base + Ao, *Bs = lead + Bo;
-                    size_t js = (size_t)j * umma::I8_SLAB_BYTES;
+                    int js = j;
                     if (MODE == MODE_VXC) {  // slab j: block lead + j / kBlockSlabs, its slab j % kBlockSlabs
                         const char* bj = ws + g.meta[m.lead + j / kBlockSlabs].ws;
                         As = bj + Ao, Bs = bj + Bo;
-                        js = (size_t)(j % kBlockSlabs) * umma::I8_SLAB_BYTES;
+                        js = j % kBlockSlabs;
                     }
-                    for (int a = 0; a < OZ_SLICES; ++a)
-                        umma::bulk_g2s(sp + a * umma::I8_SLAB_BYTES, As + a * Aplane + js, umma::I8_SLAB_BYTES,
-                                       &full[st]);
-                    for (int b = 0; b < OZ_SLICES; ++b)
-                        for (int kg = 0; kg < 4; ++kg)
-                            umma::bulk_g2s(sp + OZ_A_BYTES + (b >> 1) * 8192 + kg * 2048 + (b & 1) * 1024,
-                                           Bs + b * Bplane + js + (size_t)kg * 2048 + bhalf, 1024, &full[st]);
+                    umma::bulk_g2s(sp, As + (size_t)js * 32768, OZ_A_BYTES, &full[st]);
+                    umma::bulk_g2s(sp + OZ_A_BYTES, Bs + (size_t)js * 16384, OZ_STAGE_BYTES - OZ_A_BYTES, &full[st]);
                 }
             }
         }
