@@ -850,7 +850,12 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
 // 64-row half of a packed 128-row tile is four 1 KiB core-matrix groups, and plane b's group kg
 // goes to pair b / 2, rows 64 (b % 2) onward, of the pair's k16 group kg.
 constexpr int OZ_NT = 64;
-constexpr int OZ_STAGES = 2;
+// operand ring stages: the Vxc contraction (K = a group's 512 points, eight slabs per item) keeps
+// three in flight, the rho contraction (K = nbp) two beside its larger radial-sum staging
+template <int MODE>
+constexpr int oz_stages() {
+    return MODE == MODE_VXC ? 3 : 2;
+}
 constexpr uint32_t OZ_A_BYTES = OZ_SLICES * umma::I8_SLAB_BYTES;   // 32 KiB
 constexpr uint32_t OZ_B_SLICE = OZ_NT * umma::I8_SLAB_K;          // 4 KiB
 constexpr uint32_t OZ_STAGE_BYTES = OZ_A_BYTES + OZ_SLICES * OZ_B_SLICE;  // 48 KiB
@@ -861,9 +866,14 @@ constexpr int OZ_THREADS = 64 + 32 * OZ_EPI_WARPS;  // copies, MMAs, epilogue
 // up to kOzRsCap shells of the half's columns, staged per thread. VXC: the half's [128][17]
 // FP64 transpose tile.
 constexpr int kOzRsCap = 12;
-constexpr uint32_t OZ_EPI_BYTES = 4u * kOzRsCap * 2 * BLOCK_PTS * 8;  // 96 KiB
-static_assert(4u * 128 * 17 * 8 <= OZ_EPI_BYTES, "transpose tiles fit the epilogue region");
-constexpr uint32_t OZ_BAR_OFF = OZ_STAGES * OZ_STAGE_BYTES + OZ_EPI_BYTES;
+template <int MODE>
+constexpr uint32_t oz_epi_bytes() {  // rho: 96 KiB of staged radial sums; Vxc: four 17 KiB tiles
+    return MODE == MODE_RHO ? 4u * kOzRsCap * 2 * BLOCK_PTS * 8 : 4u * 128 * 17 * 8;
+}
+template <int MODE>
+constexpr uint32_t oz_bar_off() {
+    return oz_stages<MODE>() * OZ_STAGE_BYTES + oz_epi_bytes<MODE>();
+}
 
 // An item's int32 accumulators of orders 2..5 as one exact integer: with weights
 // w_k = 255^(5-k) w_5, sum_k d_k w_k = n w_5 with n = ((d2 255 + d3) 255 + d4) 255 + d5, whose
@@ -921,12 +931,12 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     __shared__ double s_cs[MODE == MODE_RHO ? 4 : 1][OZ_NT];
     __shared__ int s_acol[MODE == MODE_VXC ? 4 : 1][OZ_NT], s_ez[MODE == MODE_VXC ? 4 : 1][OZ_NT];
     __shared__ int s_arow[MODE == MODE_VXC ? 4 : 1][128];
-    constexpr int S = OZ_STAGES;
+    constexpr int S = oz_stages<MODE>();
     __shared__ int s_abort;
     if (threadIdx.x == 0) s_abort = *reinterpret_cast<const volatile int*>(err);
     __syncthreads();
     if (s_abort) return;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + OZ_BAR_OFF);
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + oz_bar_off<MODE>());
     uint64_t* empty = full + S;
     uint64_t* tfull = empty + S;
     uint64_t* tempty = tfull + 2;
@@ -1051,7 +1061,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const int gbar = 1 + h;                                          // the group's named barrier
         const int ca = chalf * 32;                                       // this thread's columns [ca, ca + 32)
         const double w5 = oz_weight(5);
-        uint8_t* epi = smem + OZ_STAGES * OZ_STAGE_BYTES;
+        uint8_t* epi = smem + S * OZ_STAGE_BYTES;
         const uint32_t tq = tmem + (uint32_t)h * OZ_TMEM_COLS + ((uint32_t)(quarter * 32) << 16);
         int li = 0;
         for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
@@ -1233,7 +1243,10 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
 }  // namespace
 
-size_t oz_smem_bytes() { return (size_t)OZ_BAR_OFF + (2 * OZ_STAGES + 4) * 8 + 16; }
+template <int MODE>
+size_t oz_smem_bytes() {
+    return (size_t)oz_bar_off<MODE>() + (2 * oz_stages<MODE>() + 4) * 8 + 16;
+}
 
 void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
                               const double* rho_acc, double* rho_store, double* coef, double* blk_sum,
@@ -1273,7 +1286,7 @@ static int oz_grid(int nitems) {
 void oz_rho(const MixedArgs& a, cudaStream_t s) {
     const int tiles = a.max_nbp / umma::TILE_ROWS;
     const int nitems = a.nblk * 2 * tiles;
-    const size_t smem = oz_smem_bytes();
+    const size_t smem = oz_smem_bytes<MODE_RHO>();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         k_oz<MODE_RHO, true><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
@@ -1302,7 +1315,7 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
 void oz_vxc(const MixedArgs& a, cudaStream_t s) {
     const int tiles = a.max_nbp / umma::TILE_ROWS;
     const int nitems = a.ngrp * tiles * 2 * tiles;  // per group: M tiles of 128 AOs x N tiles of 64 AOs
-    const size_t smem = oz_smem_bytes();
+    const size_t smem = oz_smem_bytes<MODE_VXC>();
     cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_oz<MODE_VXC, false><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
                                                                     tiles, a.rho_acc, a.Vacc, a.nao);
