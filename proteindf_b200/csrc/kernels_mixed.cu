@@ -533,23 +533,6 @@ __device__ __forceinline__ double warp_max_d(double v) {
     return v;
 }
 
-// One AO row of a block: its component, its shell's atom and radial sums.
-struct OzRow {
-    int t;                  // L^2 + component
-    double ax, ay, az;      // the shell's atom
-    const double* S0;       // radial sums of the shell at the block's points
-    const double* S1;
-};
-
-__device__ __forceinline__ OzRow oz_row_of(const RowGeom& q, const BlockMeta& m, const double* rad) {
-    const int slot = q.info >> 4;
-    OzRow r;
-    r.t = q.info & 15;
-    r.ax = q.ax, r.ay = q.ay, r.az = q.az;
-    r.S0 = rad + (size_t)slot * BLOCK_PTS;
-    r.S1 = rad + (size_t)(m.nsh + slot) * BLOCK_PTS;
-    return r;
-}
 
 // AO stage and phi digits of a whole group in one CTA (512 threads, one per point of its up
 // to four blocks). Pass 1: the radial sums S0, S1 of every shell of the group's basis at the
@@ -656,18 +639,35 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
         const int cur = (mu0 >> 4) & 1;
         __syncthreads();  // the previous tile's digits are cut (and the points and rows are stored)
-        if (live) {
-#pragma unroll 4
-            for (int r = 0; r < 16; ++r) {
-                const int mu = mu0 + r;
-                double v = 0.0;
-                if (mu < m.nb) {
-                    const OzRow row = oz_row_of(T.rg[cur][r], m, rad);
-                    double gx, gy, gz;
-                    ao_from_radial<false>(row.t, T.x[tid] - row.ax, T.y[tid] - row.ay, T.z[tid] - row.az, row.S0[q],
-                                          0.0, v, gx, gy, gz);
+        if (live) {  // shell by shell over the tile's rows (uniform over the CTA), phi = A S0
+            int r = 0;
+            while (r < 16) {
+                if (mu0 + r >= m.nb) {
+                    T.vt[r][tid] = 0.0;
+                    ++r;
+                    continue;
                 }
-                T.vt[r][tid] = v;
+                const RowGeom& gq = T.rg[cur][r];
+                const int t = gq.info & 15, slot = gq.info >> 4;
+                const int Lq = t == 0 ? 0 : (t < 4 ? 1 : 2);
+                const int u0 = t - Lq * Lq;                 // the component of row r
+                const int n = min(2 * Lq + 1 - u0, 16 - r);  // the shell's rows in this tile from r
+                const double S0 = rad[(size_t)slot * BLOCK_PTS + q];
+                const double x = T.x[tid] - gq.ax, y = T.y[tid] - gq.ay, z = T.z[tid] - gq.az;
+                double pc[5];
+                if (Lq == 0) {
+                    pc[0] = S0;
+                } else if (Lq == 1) {
+                    pc[0] = x * S0, pc[1] = y * S0, pc[2] = z * S0;
+                } else {  // the products of ang_poly1
+                    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+                    pc[0] = (x * y) * S0, pc[1] = (z * x) * S0, pc[2] = (y * z) * S0;
+                    pc[3] = (0.5 * (x * x - y * y)) * S0, pc[4] = (s3 * (z * z - 0.5 * (x * x + y * y))) * S0;
+                }
+#pragma unroll
+                for (int k = 0; k < 5; ++k)
+                    if (k >= u0 && k < u0 + n) T.vt[r + k - u0][tid] = pc[k];
+                r += n;
             }
         } else {
             for (int r = 0; r < 16; ++r) T.vt[r][tid] = 0.0;
