@@ -732,23 +732,39 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* _
     const OzLayout L = oz_layout(m.nbp, m.nsh);
     char* base = ws + m.ws;
     int* e_p = reinterpret_cast<int*>(base + L.e_p);
-    const int* aos = g.blk_aos + m.ao0;
+    // the group's AO list in shared memory (a group with more screened AOs reads it from global)
+    constexpr int kAosCap = 1024;
+    __shared__ int s_aos[kAosCap];
+    const bool staged = m.nb <= kAosCap;
+    if (staged)
+        for (int i = threadIdx.x; i < m.nb; i += blockDim.x) s_aos[i] = g.blk_aos[m.ao0 + i];
+    __syncthreads();
+    const int* aos = staged ? s_aos : g.blk_aos + m.ao0;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int r = lane & 7, kg = lane >> 3;
-    const int nk = m.nbp / 64;
-    uint32_t w[16];
-    for (int t = warp; t < (m.nbp / 8) * nk; t += blockDim.x / 32) {
-        const int mu = (t / nk) * 8 + r, k0 = (t % nk) * 64 + kg * 16;
-        const bool live = mu < m.nb;
-        const int amu = live ? aos[mu] : 0;
-        if (kg == 0 && k0 == 0) e_p[mu] = live ? __ldg(p_rowexp + amu) : kOzZeroExp;
-        const uint32_t* row = words + (size_t)amu * nao;
+    const int nk = m.nbp / 64, ntile = (m.nbp / 8) * nk;
+    constexpr int kWarps = 8;  // 256 threads
+    // two warp tiles per iteration: 32 independent gathers in flight per lane
+    for (int t0 = warp; t0 < ntile; t0 += 2 * kWarps) {
+        uint32_t w[2][16];
+        int mu[2], k0[2];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const int nu = k0 + j;
-            w[j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0u;
+        for (int h = 0; h < 2; ++h) {
+            const int t = t0 + h * kWarps;
+            mu[h] = (t / nk) * 8 + r, k0[h] = (t % nk) * 64 + kg * 16;
+            const bool live = t < ntile && mu[h] < m.nb;
+            const int amu = live ? aos[mu[h]] : 0;
+            if (t < ntile && kg == 0 && k0[h] == 0) e_p[mu[h]] = live ? __ldg(p_rowexp + amu) : kOzZeroExp;
+            const uint32_t* row = words + (size_t)amu * nao;
+#pragma unroll
+            for (int j = 0; j < 16; ++j) {
+                const int nu = k0[h] + j;
+                w[h][j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0u;
+            }
         }
-        oz_store16_words(base + L.ppack, kOzPlanesB, oz_off_b(mu, k0, m.nbp), w);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (t0 + h * kWarps < ntile) oz_store16_words(base + L.ppack, kOzPlanesB, oz_off_b(mu[h], k0[h], m.nbp), w[h]);
     }
 }
 
