@@ -135,4 +135,26 @@ __device__ __forceinline__ void shell_components(int L, double x, double y, doub
     }
 }
 
+// The Vxc operand Z = a phi + c . grad phi of every component of a shell (a = 0.5 w v_rho, c the
+// gradient coefficients; zero c for an LDA). With phi = A S0 and grad phi = grad A S0 - 2 r A S1,
+// Z = A alpha + S0 (c . grad A) with alpha = a S0 - 2 S1 (c . r) once per shell and point.
+__device__ __forceinline__ void shell_z(int L, double x, double y, double z, double S0, double S1, double a,
+                                        double cx, double cy, double cz, double zc[5]) {
+    const double alpha = a * S0 - 2.0 * S1 * (cx * x + cy * y + cz * z);
+    if (L == 0) {
+        zc[0] = alpha;
+    } else if (L == 1) {
+        zc[0] = x * alpha + S0 * cx;
+        zc[1] = y * alpha + S0 * cy;
+        zc[2] = z * alpha + S0 * cz;
+    } else {
+        const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+        zc[0] = x * y * alpha + S0 * (cx * y + cy * x);
+        zc[1] = z * x * alpha + S0 * (cx * z + cz * x);
+        zc[2] = y * z * alpha + S0 * (cy * z + cz * y);
+        zc[3] = 0.5 * (x * x - y * y) * alpha + S0 * (cx * x - cy * y);
+        zc[4] = s3 * (z * z - 0.5 * (x * x + y * y)) * alpha + S0 * s3 * (2.0 * cz * z - cx * x - cy * y);
+    }
+}
+
 }  // namespace pdfxc

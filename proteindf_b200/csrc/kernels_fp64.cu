@@ -438,7 +438,7 @@ __global__ void __launch_bounds__(BLOCK_PTS, 6) k_z_rad(BasisView bas, GridView 
     const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
     const double* cf = coef + gp * 4;
     const double a = cf[0], cx = cf[1], cy = cf[2], cz = cf[3];
-    double v[5], ax[5], ay[5], az[5];
+    double zc[5];
     for (int i0 = 0; i0 < m.nsh; i0 += 128) {
         __syncthreads();
         stage_shells(bas, g, m, i0, st);
@@ -447,11 +447,11 @@ __global__ void __launch_bounds__(BLOCK_PTS, 6) k_z_rad(BasisView bas, GridView 
         for (int k = 0; k < kn; ++k) {
             const int i = i0 + k;
             const int L = st.lq[k], row0 = st.row0[k];
-            shell_components(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0p[(size_t)i * BLOCK_PTS + p],
-                             S1p[(size_t)i * BLOCK_PTS + p], v, ax, ay, az);
+            shell_z(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0p[(size_t)i * BLOCK_PTS + p],
+                    S1p[(size_t)i * BLOCK_PTS + p], a, cx, cy, cz, zc);
 #pragma unroll
             for (int c = 0; c < 5; ++c)
-                if (c < 2 * L + 1) Z[(size_t)(row0 + c) * BLOCK_PTS + p] = a * v[c] + cx * ax[c] + cy * ay[c] + cz * az[c];
+                if (c < 2 * L + 1) Z[(size_t)(row0 + c) * BLOCK_PTS + p] = zc[c];
         }
     }
     for (int r = m.nb; r < m.nbp; ++r) Z[(size_t)r * BLOCK_PTS + p] = 0.0;

@@ -808,9 +808,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
         __syncthreads();  // the previous tile's digits are cut (and the points and rows are loaded)
         if (live) {
             // Shell by shell over the tile's rows (a run of rows of one shell is uniform over the
-            // CTA): with phi = A S0 and grad phi = grad A S0 - 2 r A S1,
-            // Z = c0 phi + c . grad phi = A alpha + S0 (c . grad A), alpha = c0 S0 - 2 S1 (c . r),
-            // so a component costs a few FMAs once alpha is formed for the shell.
+            // CTA), with the shell's Z from shell_z: a few FMAs per component.
             const double c0 = T.c[0][tid], c1 = GGA ? T.c[1][tid] : 0.0, c2 = GGA ? T.c[2][tid] : 0.0,
                          c3 = GGA ? T.c[3][tid] : 0.0;
             int r = 0;
@@ -826,24 +824,9 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
                 const int u0 = t - Lq * Lq;                 // the component of row r
                 const int n = min(2 * Lq + 1 - u0, 16 - r);  // the shell's rows in this tile from r
                 const double S0 = rad[(size_t)slot * BLOCK_PTS + q];
-                const double x = T.x[tid] - gq.ax, y = T.y[tid] - gq.ay, z = T.z[tid] - gq.az;
-                double alpha = c0 * S0;
-                if (GGA) alpha -= 2.0 * rad[(size_t)(m.nsh + slot) * BLOCK_PTS + q] * (c1 * x + c2 * y + c3 * z);
+                const double S1 = GGA ? rad[(size_t)(m.nsh + slot) * BLOCK_PTS + q] : 0.0;
                 double zc[5];
-                if (Lq == 0) {
-                    zc[0] = alpha;
-                } else if (Lq == 1) {
-                    zc[0] = x * alpha + S0 * c1;
-                    zc[1] = y * alpha + S0 * c2;
-                    zc[2] = z * alpha + S0 * c3;
-                } else {
-                    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
-                    zc[0] = x * y * alpha + S0 * (c1 * y + c2 * x);
-                    zc[1] = z * x * alpha + S0 * (c1 * z + c3 * x);
-                    zc[2] = y * z * alpha + S0 * (c2 * z + c3 * y);
-                    zc[3] = 0.5 * (x * x - y * y) * alpha + S0 * (c1 * x - c2 * y);
-                    zc[4] = s3 * (z * z - 0.5 * (x * x + y * y)) * alpha + S0 * s3 * (2.0 * c3 * z - c1 * x - c2 * y);
-                }
+                shell_z(Lq, T.x[tid] - gq.ax, T.y[tid] - gq.ay, T.z[tid] - gq.az, S0, S1, c0, c1, c2, c3, zc);
 #pragma unroll
                 for (int k = 0; k < 5; ++k)
                     if (k >= u0 && k < u0 + n) T.vt[r + k - u0][tid] = zc[k];
