@@ -157,4 +157,36 @@ __device__ __forceinline__ void shell_z(int L, double x, double y, double z, dou
     }
 }
 
+// rho and grad rho contributions of a shell's components with coefficients X[c] (c < 2L + 1; zero
+// for a component that is not added): with phi = A S0 and grad phi = grad A S0 - 2 r A S1,
+// sum_c X_c phi_c = S0 PA and sum_c X_c grad phi_c = S0 PG - 2 r S1 PA, with PA = sum_c X_c A_c and
+// PG = sum_c X_c grad A_c, so a component costs a few FMAs.
+template <bool GGA>
+__device__ __forceinline__ void shell_rho(int L, double x, double y, double z, double S0, double S1, const double X[5],
+                                          double& r, double& gx, double& gy, double& gz) {
+    double PA, Px = 0.0, Py = 0.0, Pz = 0.0;
+    if (L == 0) {
+        PA = X[0];
+    } else if (L == 1) {
+        PA = x * X[0] + y * X[1] + z * X[2];
+        Px = X[0], Py = X[1], Pz = X[2];
+    } else {
+        const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+        PA = X[0] * (x * y) + X[1] * (z * x) + X[2] * (y * z) + X[3] * (0.5 * (x * x - y * y)) +
+             X[4] * (s3 * (z * z - 0.5 * (x * x + y * y)));
+        if (GGA) {
+            Px = X[0] * y + X[1] * z + (X[3] - s3 * X[4]) * x;
+            Py = X[0] * x + X[2] * z - (X[3] + s3 * X[4]) * y;
+            Pz = X[1] * x + X[2] * y + 2.0 * s3 * X[4] * z;
+        }
+    }
+    r = fma(S0, PA, r);
+    if (GGA) {
+        const double w = 2.0 * S1 * PA;
+        gx += S0 * Px - x * w;
+        gy += S0 * Py - y * w;
+        gz += S0 * Pz - z * w;
+    }
+}
+
 }  // namespace pdfxc

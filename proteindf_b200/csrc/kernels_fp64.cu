@@ -395,7 +395,6 @@ __global__ void __launch_bounds__(BLOCK_PTS, 6) k_rho_rad(BasisView bas, GridVie
     const size_t gp = (size_t)blk * BLOCK_PTS + p;
     const double px = g.px[gp], py = g.py[gp], pz = g.pz[gp];
     double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
-    double v[5], ax[5], ay[5], az[5];
     for (int i0 = 0; i0 < m.nsh; i0 += 128) {
         __syncthreads();
         stage_shells(bas, g, m, i0, st);
@@ -407,17 +406,8 @@ __global__ void __launch_bounds__(BLOCK_PTS, 6) k_rho_rad(BasisView bas, GridVie
             double xv[5];
 #pragma unroll
             for (int c = 0; c < 5; ++c) xv[c] = c < 2 * L + 1 ? X[(size_t)(row0 + c) * BLOCK_PTS + p] : 0.0;
-            shell_components(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0p[(size_t)i * BLOCK_PTS + p],
-                             S1p[(size_t)i * BLOCK_PTS + p], v, ax, ay, az);
-#pragma unroll
-            for (int c = 0; c < 5; ++c) {
-                if (c < 2 * L + 1) {
-                    rho = fma(v[c], xv[c], rho);
-                    gx = fma(ax[c], xv[c], gx);
-                    gy = fma(ay[c], xv[c], gy);
-                    gz = fma(az[c], xv[c], gz);
-                }
-            }
+            shell_rho<true>(L, px - st.ax[k], py - st.ay[k], pz - st.az[k], S0p[(size_t)i * BLOCK_PTS + p],
+                            S1p[(size_t)i * BLOCK_PTS + p], xv, rho, gx, gy, gz);
         }
     }
     double* ra = rho_acc + gp * 4;

@@ -1166,34 +1166,16 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                         S1 = staged ? rs[(2 * k + 1) * BLOCK_PTS + pt] : rad[(size_t)(m.nsh + slot) * BLOCK_PTS + pt];
                     const double x = px - q.ax, y = py - q.ay, z = pz - q.az;
                     umma::tmem_wait_ld();
-                    // the shell's components, each added as soon as it is formed
-                    auto add = [&](int u, double A, double Ax, double Ay, double Az) {
+                    // the shell's X (zero for its components outside [ca, cb)), then its rho terms
+                    double xv[5];
+#pragma unroll
+                    for (int u = 0; u < 5; ++u) {
                         const int cc = cs0 + u;
-                        if (cc >= ca && cc < cb) {
-                            const double X = oz_combine(d[u][0], d[u][1], d[u][2], d[u][3]) * s_cs[sb][cc];
-                            r = fma(A * S0, X, r);
-                            if (GGA) {
-                                const double w = 2.0 * A * S1;
-                                gx = fma(Ax * S0 - x * w, X, gx);
-                                gy = fma(Ay * S0 - y * w, X, gy);
-                                gz = fma(Az * S0 - z * w, X, gz);
-                            }
-                        }
-                    };
-                    if (Lq == 0) {
-                        add(0, 1.0, 0.0, 0.0, 0.0);
-                    } else if (Lq == 1) {
-                        add(0, x, 1.0, 0.0, 0.0);
-                        add(1, y, 0.0, 1.0, 0.0);
-                        add(2, z, 0.0, 0.0, 1.0);
-                    } else {
-                        const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
-                        add(0, x * y, y, x, 0.0);
-                        add(1, z * x, z, 0.0, x);
-                        add(2, y * z, 0.0, z, y);
-                        add(3, 0.5 * (x * x - y * y), x, -y, 0.0);
-                        add(4, s3 * (z * z - 0.5 * (x * x + y * y)), -s3 * x, -s3 * y, 2.0 * s3 * z);
+                        xv[u] = (cc < ce && cc >= ca && cc < cb)
+                                    ? oz_combine(d[u][0], d[u][1], d[u][2], d[u][3]) * s_cs[sb][cc]
+                                    : 0.0;
                     }
+                    shell_rho<GGA>(Lq, x, y, z, S0, S1, xv, r, gx, gy, gz);
                     c = ce;
                 }
                 umma::fence_before_sync();
