@@ -451,11 +451,91 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     std::vector<int> shells, rows, aos, row_info;
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
     double flops = 0.0, sum_nb = 0.0;
+    // Candidate shells of a group from a uniform grid of the segment's atoms (cell edge = the
+    // largest screening radius): only atoms whose cell overlaps the cube of half-edge
+    // rad + max Rs around the group's centre can pass the test below, and walking the candidates
+    // in atom order visits their shells in shell order when each atom's shells are contiguous and
+    // atoms ascend with the shell index (otherwise every shell of the segment is tested).
+    struct AtomCells {
+        bool ok = false;
+        double lo[3], edge, reach;
+        int dim[3];
+        std::vector<int> start, atoms;    // CSR: the atoms of each cell, ascending
+        std::vector<int> sh_first, sh_end;  // per atom of the segment: its shells
+        int a0 = 0;
+    };
+    std::vector<AtomCells> cells(segs.size());
+    auto build_cells = [&](size_t si) {
+        AtomCells& C = cells[si];
+        const GridSegment& sg = segs[si];
+        if (sg.sh1 <= sg.sh0) return;
+        const int a0 = ctx->h_sh_atom[sg.sh0], a1 = ctx->h_sh_atom[sg.sh1 - 1] + 1;
+        for (int sh = sg.sh0 + 1; sh < sg.sh1; ++sh)
+            if (ctx->h_sh_atom[sh] < ctx->h_sh_atom[sh - 1]) return;  // not in atom order
+        C.a0 = a0;
+        C.sh_first.assign(a1 - a0, 0), C.sh_end.assign(a1 - a0, 0);
+        for (int sh = sg.sh1 - 1; sh >= sg.sh0; --sh) C.sh_first[ctx->h_sh_atom[sh] - a0] = sh;
+        for (int sh = sg.sh0; sh < sg.sh1; ++sh) C.sh_end[ctx->h_sh_atom[sh] - a0] = sh + 1;
+        double rmax = 0.0, hi[3];
+        for (int sh = sg.sh0; sh < sg.sh1; ++sh) rmax = std::max(rmax, Rs[sh]);
+        C.edge = std::max(rmax, 1.0), C.reach = rmax;
+        for (int k = 0; k < 3; ++k) C.lo[k] = 1e300, hi[k] = -1e300;
+        for (int a = a0; a < a1; ++a)
+            for (int k = 0; k < 3; ++k)
+                C.lo[k] = std::min(C.lo[k], ctx->h_atom_xyz[3 * a + k]), hi[k] = std::max(hi[k], ctx->h_atom_xyz[3 * a + k]);
+        size_t ncell = 1;
+        for (int k = 0; k < 3; ++k) C.dim[k] = (int)((hi[k] - C.lo[k]) / C.edge) + 1, ncell *= (size_t)C.dim[k];
+        if (ncell > (size_t)1 << 22) return;  // too fine a grid: test every shell
+        auto cell_of = [&](int a) {
+            size_t c = 0;
+            for (int k = 0; k < 3; ++k)
+                c = c * C.dim[k] + std::min(C.dim[k] - 1, (int)((ctx->h_atom_xyz[3 * a + k] - C.lo[k]) / C.edge));
+            return c;
+        };
+        C.start.assign(ncell + 1, 0);
+        for (int a = a0; a < a1; ++a) ++C.start[cell_of(a) + 1];
+        for (size_t c = 0; c < ncell; ++c) C.start[c + 1] += C.start[c];
+        C.atoms.resize(a1 - a0);
+        std::vector<int> fill(C.start.begin(), C.start.end() - 1);
+        for (int a = a0; a < a1; ++a) C.atoms[fill[cell_of(a)]++] = a;  // ascending within a cell
+        C.ok = true;
+    };
+    for (size_t si = 0; si < segs.size(); ++si) build_cells(si);
+    std::vector<int> cand_sh;
+    auto candidates = [&](size_t si, int gi) {  // the shells to test for group gi, in shell order
+        const AtomCells& C = cells[si];
+        const GridSegment& sg = segs[si];
+        cand_sh.clear();
+        if (!C.ok) {
+            for (int sh = sg.sh0; sh < sg.sh1; ++sh) cand_sh.push_back(sh);
+            return;
+        }
+        const double r = rad[gi] + C.reach;
+        int c0[3], c1[3];
+        for (int k = 0; k < 3; ++k) {
+            c0[k] = std::max(0, (int)std::floor((cen[3 * gi + k] - r - C.lo[k]) / C.edge));
+            c1[k] = std::min(C.dim[k] - 1, (int)std::floor((cen[3 * gi + k] + r - C.lo[k]) / C.edge));
+        }
+        static thread_local std::vector<int> ats;
+        ats.clear();
+        for (int x = c0[0]; x <= c1[0]; ++x)
+            for (int y = c0[1]; y <= c1[1]; ++y)
+                for (int z = c0[2]; z <= c1[2]; ++z) {
+                    const size_t c = ((size_t)x * C.dim[1] + y) * C.dim[2] + z;
+                    ats.insert(ats.end(), C.atoms.begin() + C.start[c], C.atoms.begin() + C.start[c + 1]);
+                }
+        std::sort(ats.begin(), ats.end());
+        for (int a : ats)
+            for (int sh = C.sh_first[a - C.a0]; sh < C.sh_end[a - C.a0]; ++sh) cand_sh.push_back(sh);
+    };
     for (int gi = 0; gi < ngrp; ++gi) {
-        const GridSegment& sg = segs[blk_seg[grp_blk[gi]]];
+        const size_t si = blk_seg[grp_blk[gi]];
+        const GridSegment& sg = segs[si];
+        (void)sg;
         const int sh0 = (int)shells.size(), ao0 = (int)aos.size();
         int row = 0;
-        for (int sh = sg.sh0; sh < sg.sh1; ++sh) {
+        candidates(si, gi);
+        for (int sh : cand_sh) {
             const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[sh]];
             const double d = std::sqrt((A[0] - cen[3 * gi]) * (A[0] - cen[3 * gi]) +
                                        (A[1] - cen[3 * gi + 1]) * (A[1] - cen[3 * gi + 1]) +
