@@ -20,12 +20,19 @@ Under torchrun (N > 1) every rank builds its own chain (seed + rank): the units
 are independent molecules, no data-path collective; value = all ranks' points
 / the slowest rank's time (weak scaling).
 
-Other workloads (not the headline line):
-  --workload batch64    64 independent chains of 10-120 atoms (seeded sizes), cc-pVDZ,
-                        B3LYP, USER 75x302 grid with Becke weights, one batched build
-                        (pdfxc_build_vxc_batched: one graph per build for all molecules)
-  --workload chain2000  one 2000-atom chain, cc-pVDZ (~18,600 AOs), B3LYP, USER 75x302
-                        grid with Stratmann-Scuseria weights, AO cut-off 1e-10
+The same line (N = 1, unless --no-large) carries the two large configurations,
+each built with the FP64 drop-in and the INT8 path, their speed-up and |dExc|:
+  chain2000  one 2000-atom chain, cc-pVDZ (~18,600 AOs), B3LYP, USER 75x302 grid with
+             Stratmann-Scuseria weights, AO cut-off 1e-10
+  batch64    64 independent chains of 10-120 atoms (seeded sizes), cc-pVDZ, B3LYP,
+             USER 75x302 grid with Becke weights, one batched build per step
+             (pdfxc_build_vxc_batched: one graph per build for all molecules)
+--workload chain2000 / batch64 runs one of them alone.
+
+cpu_baseline: the reference's own DfCalcGridX (oracle/_ref/pdfxc_ref, built from its
+sources) on seeded samples of the grid's rows, all host cores (two sample sizes, whose
+rates must agree) and one thread; its Exc and Vxc on the first sample are compared
+with the GPU builds on the same rows (vs_reference_parity).
 """
 import argparse
 import json
@@ -60,6 +67,7 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4000, help="grid points for the CPU baseline sample")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="chain", choices=["chain", "batch64", "chain2000"])
+    ap.add_argument("--no-large", action="store_true", help="leave the 2000-atom chain and the batch out")
     return ap.parse_args()
 
 
@@ -163,59 +171,119 @@ def fp64_gemm_peak(torch):
     return 2.0 * n ** 3 / (best * 1e-3) / 1e12
 
 
-def cpu_baseline(args, syms, xyz, grid5, PA, sample, reference_kind=True):
-    """Reference DfCalcGridX (oracle/_ref/pdfxc_ref) on a seeded sample of grid rows,
-    all host cores; per-point cost is position-independent in the reference (it
-    evaluates every AO at every point), so points/s extrapolates linearly."""
+def cpu_model():
+    try:
+        for line in open("/proc/cpuinfo"):
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def sample_rows(n_total, n, seed):
+    rng = np.random.default_rng(seed)
+    return np.sort(rng.choice(n_total, min(n, n_total), replace=False))
+
+
+def reference_on_rows(args, syms, xyz, grid5, PA, rows, threads):
+    """The reference engine (or, without it, the CPU restatement) on the given grid rows:
+    (seconds, kind, exc, vxc)."""
     import tempfile
     from oracle import refio
     from proteindf_b200 import basis, systems
-    cores = os.cpu_count() or 1
-    rng = np.random.default_rng(0)
-    sel = np.sort(rng.choice(len(grid5), min(sample, len(grid5)), replace=False))
-    g = grid5[sel]
-    if reference_kind and refio.ref_available():
+    g = grid5[rows]
+    if refio.ref_available():
         with tempfile.TemporaryDirectory() as d:
             r = refio.run_xc(d, syms, systems.nuclear_charges(syms), xyz, basis.load_basis("cc-pVDZ"),
-                             args.functional, g, PA, threads=cores)
-        t = float(r["t_rho"][0] + r["t_vxc"][0])
-        kind = "reference"
-    else:
-        from oracle import oracle
-        sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
-        t0 = time.perf_counter()
-        oracle.xc(args.functional, sh, g[:, :4], PA, threads=cores)
-        t = time.perf_counter() - t0
-        kind = "port"
-    return {"value": len(g) / t, "unit": UNIT, "cores": cores, "kind": kind,
-            "sample": f"{len(g)} of {len(grid5)} grid points (seed 0), rho pass + Vxc pass, {t:.1f} s"}
+                             args.functional, g, PA, threads=threads)
+        n = int(round(np.sqrt(r["vxc"].size)))
+        return float(r["t_rho"][0] + r["t_vxc"][0]), "reference", float(r["exc"][0]), r["vxc"].reshape(n, n)
+    from oracle import oracle
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+    t0 = time.perf_counter()
+    r = oracle.xc(args.functional, sh, g[:, :4], PA, threads=threads)
+    return time.perf_counter() - t0, "port", r["exc"], r["vxc"]
+
+
+def cpu_baseline(args, syms, xyz, grid5, PA, sample):
+    """Reference DfCalcGridX (oracle/_ref/pdfxc_ref) on seeded samples of grid rows. Its
+    per-point cost is position-independent (it evaluates every AO at every point), so
+    points/s extrapolates linearly: two samples (sample/2 rows, seed 0; sample rows, seed 1)
+    on all host cores, whose rates must agree, and one sample on one thread (seed 2). The
+    seed-0 sample's Exc and Vxc are returned for the parity check."""
+    cores = os.cpu_count() or 1
+    runs = []
+    keep = None
+    for n, seed, threads in ((sample // 2, 0, cores), (sample, 1, cores), (max(100, sample // 16), 2, 1)):
+        rows = sample_rows(len(grid5), n, seed)
+        t, kind, exc, vxc = reference_on_rows(args, syms, xyz, grid5, PA, rows, threads)
+        runs.append({"points": int(len(rows)), "seed": seed, "threads": threads, "seconds": t,
+                     "points_per_s": len(rows) / t})
+        if seed == 0:
+            keep = {"rows": rows, "exc": exc, "vxc": vxc}
+    full = runs[:2]
+    value = sum(r["points"] for r in full) / sum(r["seconds"] for r in full)
+    spread = abs(full[0]["points_per_s"] - full[1]["points_per_s"]) / value
+    out = {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+           "sample": (f"{full[0]['points']} + {full[1]['points']} of {len(grid5)} grid points (seeds 0, 1), "
+                      f"rho pass + Vxc pass on {cores} threads, {sum(r['seconds'] for r in full):.1f} s; "
+                      "extrapolated (cost per point is position-independent)"),
+           "samples": runs, "sample_rate_spread": spread,
+           "one_thread": {"value": runs[2]["points_per_s"], "unit": UNIT, "points": runs[2]["points"]}}
+    return out, keep
+
+
+def parity_vs_reference(args, sh, grid4, owner, keep, precisions):
+    """The GPU builds on the reference's seed-0 sample rows: |dExc| and max|dVxc| per path."""
+    from proteindf_b200.xc import XcEngine
+    rows = keep["rows"]
+    out = {"points": int(len(rows)), "functional": args.functional}
+    for p in precisions:
+        eng = XcEngine(device=0, precision=p, split_terms=args.split_terms)
+        eng.set_system(sh)
+        eng.set_grid(grid4[rows], owner[rows])
+        exc, _, V = eng.build_vxc(args.functional, keep["PA"])
+        eng.close()
+        out[p] = {"abs_dexc": abs(exc - keep["exc"]), "max_abs_dvxc": float(np.abs(V - keep["vxc"]).max()),
+                  "reference_exc_on_sample": keep["exc"]}
+    return out
 
 
 def run_reference(args):
     rank, world, _ = dist_env()
     if rank != 0:
         return
-    from proteindf_b200 import grids, systems
-    from oracle import oracle, refio
+    from proteindf_b200 import grids
+    from oracle import oracle
     syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed)
-    # Becke weights on the CPU oracle for the reference arm (no GPU on its path)
+    # Becke weights from the CPU restatement: bit for bit the device's (same IEEE operations in
+    # the same order), so the weight screen keeps the same points as the GPU arm's grid
     fac = oracle.becke(xyz, brad, P, A)
     P2, W2, A2 = grids.screen_by_weight(P, W * fac, A)
     grid5 = np.concatenate([P2, W2[:, None], A2[:, None]], axis=1)
-    per_step = max(200, args.cpu_sample // 4)
-    vals = []
+    per_step = max(200, args.cpu_sample // 2)
+    cores = os.cpu_count() or 1
+    vals, kind = [], "reference"
+    first = None
     for i in range(args.warmup + args.steps):
-        cb = cpu_baseline(args, syms, xyz, grid5, PA, per_step)
+        rows = sample_rows(len(grid5), per_step, i)
+        t, kind, exc, vxc = reference_on_rows(args, syms, xyz, grid5, PA, rows, cores)
+        if i == 0:
+            first = {"points": int(len(rows)), "seed": 0, "exc": exc, "vxc_trace": float(np.trace(vxc)),
+                     "vxc_sum": float(vxc.sum())}
         if i >= args.warmup:
-            vals.append(cb["value"])
+            vals.append(len(rows) / t)
     v = float(np.mean(vals))
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": len(grid5) / v * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic (seeded chain, reference-generated grid recipe)",
+            "data": "synthetic (seeded chain and density, ProteinDF grid recipe)",
             "config": config(args, len(grid5), sh.nao),
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cb["cores"], "kind": cb["kind"],
-                             "sample": f"{per_step} grid points per step, extrapolated to {len(grid5)}"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "cpu_model": cpu_model(),
+                             "sample": f"{per_step} grid points per step (seed = step), extrapolated to "
+                                       f"{len(grid5)}"},
+            "reference_on_sample": first,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -308,10 +376,12 @@ def main():
     if rank == 0:
         peaks = measured_peaks()
         rooflines = {p: roofline(args, torch, peaks, res[p], p) for p in precisions}
-        cpu = None
+        cpu, parity = None, None
         if not args.no_cpu_baseline:
             grid5 = np.concatenate([grid4, owner[:, None].astype(np.float64)], axis=1)
-            cpu = cpu_baseline(args, syms, xyz, grid5, PA, args.cpu_sample)
+            cpu, keep = cpu_baseline(args, syms, xyz, grid5, PA, args.cpu_sample)
+            keep["PA"] = PA
+            parity = parity_vs_reference(args, sh, grid4, owner, keep, precisions)
         h = res[head]
         dtype = "f64" if head == "fp64" else ("int8 fixed-point slices/i32/f64" if args.split_terms == 10
                                               else "bf16 split/f32/f64")
@@ -325,7 +395,7 @@ def main():
                 "e2e": {"value": world * npts / t_e2e, "unit": UNIT,
                         "h2d_bytes_per_step": nao * nao * 8, "d2h_bytes_per_step": nao * nao * 8 + 16},
                 "roofline": rooflines[head], "cpu_baseline": cpu, "gpu_launches": h["launches"],
-                "clocks": clk_summary}
+                "clocks": clk_summary, "vs_reference_parity": parity}
         if "fp64" in res and "mixed" in res:
             f, m = res["fp64"], res["mixed"]
             line["mixed"] = {"value": m["value"], "ms_per_step": m["ms"], "exc": m["exc"], "dtype": (
@@ -334,24 +404,29 @@ def main():
             line["mixed_vs_fp64"] = {"speedup": f["ms"] / m["ms"], "abs_dexc": abs(m["exc"] - f["exc"]),
                                      "max_abs_dvxc": float(np.abs(m["V"] - f["V"]).max()),
                                      "abs_dnelec_alpha": abs(m["nel"] - f["nel"])}
-        print(json.dumps(line), flush=True)
     for e in engines.values():
         e.close()
+    if rank == 0 and world == 1 and not args.no_large:
+        del dP, dV
+        torch.cuda.empty_cache()
+        for name in ("chain2000", "batch64"):
+            line[name] = large_workload(args, name, flush)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
 
 
-def run_large(args):
-    """The many-molecule batch and the 2000-atom chain, FP64 and INT8 mixed, device time
-    per build (CUDA events of the library, L2 flushed between steps); one GPU."""
+def large_workload(args, name, flush):
+    """The 64-molecule batch or the 2000-atom chain, FP64 drop-in and INT8 path, device time
+    per build (CUDA events of the library on its stream, L2 flushed between steps); one GPU."""
     import torch
     from proteindf_b200 import basis, grids, systems
     from proteindf_b200.xc import XcEngine
-    torch.cuda.set_device(0)
     b = basis.load_basis("cc-pVDZ")
-    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
     t0 = time.perf_counter()
-    if args.workload == "batch64":
+    dP = dV = None
+    if name == "batch64":
         rng = np.random.default_rng(args.seed)
         sizes = rng.integers(10, 121, 64)
         mols, PAs = [], []
@@ -378,26 +453,26 @@ def run_large(args):
         syms, xyz = systems.peptide_chain(2000, seed=args.seed)
         sh = basis.ShellTable(syms, xyz, b)
         radius = [grids.BRAGG_SLATER[int(z)] for z in sh.atom_z]
-        PA = 0.5 * systems.density_matrix(sh.nao, int(0.4 * sh.nao), seed=args.seed)
+        dP = 0.5 * systems.density_matrix_device(sh.nao, int(0.4 * sh.nao), seed=args.seed, device="cuda:0")
+        dV = torch.empty_like(dP)
         npts, nao = None, sh.nao
         desc = {"workload": "2000-atom peptide-like chain, cc-pVDZ, B3LYP, USER 75x302 grid, "
                             "Stratmann-Scuseria weights, AO cut-off 1e-10",
                 "atoms": 2000, "n_ao": int(nao)}
     t_setup = time.perf_counter() - t0
     out = {}
+    Vs = {}
     for prec in (["fp64", "mixed"] if args.precision == "both" else [args.precision]):
         eng = XcEngine(device=0, precision=prec, split_terms=args.split_terms,
-                       ao_cutoff=1e-10 if args.workload == "chain2000" else 1e-14)
+                       ao_cutoff=1e-10 if name == "chain2000" else 1e-14)
         t1 = time.perf_counter()
-        if args.workload == "batch64":
+        if name == "batch64":
             eng.set_batch(mols)
             build = lambda: eng.build_vxc_batched(args.functional, PAs)
         else:
             eng.set_system(sh)
             npts = eng.generate_grid(radius, partition="SSWeight", **grids.PRESETS["USER-75x302"])
             desc["grid_points"] = int(npts)
-            dP = torch.tensor(PA, device="cuda:0")
-            dV = torch.empty_like(dP)
             build = lambda: eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
         t_grid = time.perf_counter() - t1
         for _ in range(args.warmup):
@@ -408,7 +483,12 @@ def run_large(args):
             torch.cuda.synchronize()
             r = build()
             ms.append(eng.last_profile()["total_ms"])
-        exc = float(np.sum(r[0])) if args.workload == "batch64" else float(r[0])
+        if name == "batch64":
+            exc = float(np.sum(r[0]))
+            Vs[prec] = r[2]
+        else:
+            exc = float(r[0])
+            Vs[prec] = dV.clone()
         st = eng.grid_stats()
         eng.set_profiling(True)  # one more build, stage by stage, for the stage times (not timed above)
         build()
@@ -416,20 +496,37 @@ def run_large(args):
         eng.set_profiling(False)
         out[prec] = {"ms_per_step": float(np.mean(ms)), "value": npts / (np.mean(ms) * 1e-3), "exc": exc,
                      "blocks": st["nblocks"], "mean_screened_aos": st["mean_nb"],
-                     ("grid_generation_s" if args.workload == "chain2000" else "set_grid_s"): t_grid,
+                     ("grid_generation_s" if name == "chain2000" else "set_grid_s"): t_grid,
                      "stage_ms": {k: prof[k] for k in ("ao_ms", "gemm_x_ms", "rho_ms", "gemm_v_ms", "finish_ms")}}
         eng.close()
-    head = out.get("mixed", out.get("fp64"))
+    res = {"metric": METRIC, "unit": UNIT, "steps": args.steps, "warmup": args.warmup,
+           "config": dict(desc, functional=args.functional, l2="flushed between timed steps (512 MiB write)",
+                          host_setup_s=t_setup)}
+    res.update(out)
+    if "fp64" in out and "mixed" in out:
+        if name == "batch64":
+            dv = max(float(np.abs(a - b).max()) for a, b in zip(Vs["fp64"], Vs["mixed"]))
+        else:
+            dv = float((Vs["fp64"] - Vs["mixed"]).abs().max())
+        res["mixed_vs_fp64"] = {"speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
+                                "abs_dexc": abs(out["mixed"]["exc"] - out["fp64"]["exc"]), "max_abs_dvxc": dv}
+    del Vs, dP, dV
+    torch.cuda.empty_cache()
+    return res
+
+
+def run_large(args):
+    """One large configuration alone (--workload chain2000 | batch64)."""
+    import torch
+    torch.cuda.set_device(0)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda:0")
+    res = large_workload(args, args.workload, flush)
+    head = res.get("mixed", res.get("fp64"))
     line = {"metric": METRIC, "unit": UNIT, "value": head["value"], "ms_per_step": head["ms_per_step"],
             "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "dtype": "int8 fixed-point slices/i32/f64" if "mixed" in out else "f64",
-            "data": "synthetic (seeded chains and densities)",
-            "config": dict(desc, functional=args.functional, l2="flushed between timed steps (512 MiB write)",
-                           host_setup_s=t_setup)}
-    line.update(out)
-    if "fp64" in out and "mixed" in out:
-        line["mixed_vs_fp64"] = {"speedup": out["fp64"]["ms_per_step"] / out["mixed"]["ms_per_step"],
-                                 "abs_dexc": abs(out["mixed"]["exc"] - out["fp64"]["exc"])}
+            "dtype": "int8 fixed-point slices/i32/f64" if "mixed" in res else "f64",
+            "data": "synthetic (seeded chains and densities)"}
+    line.update(res)
     print(json.dumps(line), flush=True)
 
 

@@ -279,6 +279,36 @@ pdfxc_status pdfxc_block_costs(pdfxc_ctx* ctx, double* cost);
 pdfxc_status pdfxc_partition_blocks(int64_t nblk, const double* cost, int nparts, int64_t* bounds);
 pdfxc_status pdfxc_set_block_range(pdfxc_ctx* ctx, int64_t b_lo, int64_t b_hi);
 
+/* The blocking and screening of a grid, planned on the host without a device or
+ * context: what pdfxc_set_grid would build for these options, system and points
+ * (same blocks, groups, screened shells and workspace chunks). Returns
+ * PDFXC_ERR_UNSUPPORTED where pdfxc_set_grid would: a mixed-precision (INT8)
+ * context takes at most 33,280 screened AOs per group, the bound up to which its
+ * int32 accumulation is exact. No counterpart in the reference (it does not
+ * screen, src/libpdf/DfCalcGridX.cpp:655-665); tile and group shapes can be
+ * compared with it before a context is made. */
+typedef struct {
+    int64_t nblocks, ngroups, npts_padded;
+    int max_nb;               /* largest screened AO count of a block */
+    double contraction_flops; /* sum over blocks of 4 nb^2 np */
+    double mean_nb;
+    size_t workspace_bytes;   /* the largest workspace chunk */
+    int nchunks;
+} pdfxc_grid_plan;
+pdfxc_status pdfxc_plan_grid(const pdfxc_options* opt, int natom, const double* atom_xyz, int nshell,
+                             const int* shell_atom, const int* shell_l, const int* shell_nprim,
+                             const double* prim_exp, const double* prim_coef, int64_t npts, const double* xyzw,
+                             pdfxc_grid_plan* out);
+
+/* The exchange step of a sharded build (the reference all-reduces F,
+ * src/libpdf/DfCalcGridX_Parallel.cpp:191-239): a symmetric n x n device
+ * matrix's upper triangle (j >= i) packed row by row into n (n + 1) / 2
+ * doubles, so that one all-reduce moves half the matrix, and the inverse, which
+ * writes both triangles. Device pointers; enqueued on `stream` (a cudaStream_t,
+ * NULL = the default stream) without synchronising. */
+pdfxc_status pdfxc_pack_upper(const double* d_V, int n, double* d_packed, void* stream);
+pdfxc_status pdfxc_unpack_upper(const double* d_packed, int n, double* d_V, void* stream);
+
 /* Statistics of the blocked grid: blocks, points (after padding), the sum of
  * 4 * nb^2 * np over blocks (the algorithmic contraction FLOPs of one build)
  * and the mean screened AO count per block. */

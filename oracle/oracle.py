@@ -84,7 +84,10 @@ def xc(name, sh, xyzw, PA, rho_cut=1e-16, threads=0):
     return {"exc": exc.value, "nelec_alpha": nel.value, "vxc": vxc, "rho": rho}
 
 
-def becke(atom_xyz, brad, xyz, owner, size_adjust=True):
+def becke(atom_xyz, brad, xyz, owner, size_adjust=True, ghost=None):
+    """Becke partition factor of each point for its owner atom; ghost (natom bools, optional):
+    dummy atoms, left out as partners."""
+    g = None if ghost is None else np.ascontiguousarray(ghost, dtype=np.int32)
     atom_xyz = np.ascontiguousarray(atom_xyz, dtype=np.float64)
     brad = np.ascontiguousarray(brad, dtype=np.float64)
     xyz = np.ascontiguousarray(xyz, dtype=np.float64).reshape(-1, 3)
@@ -93,7 +96,9 @@ def becke(atom_xyz, brad, xyz, owner, size_adjust=True):
     lib().pdfxc_oracle_becke(ctypes.c_int(len(atom_xyz)), atom_xyz.ctypes.data_as(ctypes.c_void_p),
                              brad.ctypes.data_as(ctypes.c_void_p), ctypes.c_int(int(size_adjust)),
                              ctypes.c_long(len(xyz)), xyz.ctypes.data_as(ctypes.c_void_p),
-                             owner.ctypes.data_as(ctypes.c_void_p), fac.ctypes.data_as(ctypes.c_void_p))
+                             owner.ctypes.data_as(ctypes.c_void_p),
+                             None if g is None else g.ctypes.data_as(ctypes.c_void_p),
+                             fac.ctypes.data_as(ctypes.c_void_p))
     return fac
 
 

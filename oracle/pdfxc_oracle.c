@@ -541,7 +541,7 @@ static double becke_f3(double x) {
 }
 
 int pdfxc_oracle_becke(int natom, const double* atom_xyz, const double* brad, int size_adjust,
-                       long npts, const double* xyz, const int* owner, double* factor) {
+                       long npts, const double* xyz, const int* owner, const int* ghost, double* factor) {
 #pragma omp parallel
     {
         double* P = (double*)malloc(sizeof(double) * (size_t)natom);
@@ -558,7 +558,8 @@ int pdfxc_oracle_becke(int natom, const double* atom_xyz, const double* brad, in
             for (int m = 0; m < natom; ++m) {
                 double p = 1.0;
                 for (int n = 0; n < natom; ++n) {
-                    if (n == m) continue;
+                    /* partners with atomic number <= 0 (dummy atoms) are left out (:2056) */
+                    if (n == m || (ghost && ghost[n])) continue;
                     const double* A = atom_xyz + 3 * m;
                     const double* B = atom_xyz + 3 * n;
                     const double Rmn = sqrt((A[0] - B[0]) * (A[0] - B[0]) + (A[1] - B[1]) * (A[1] - B[1]) +

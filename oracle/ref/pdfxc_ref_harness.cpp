@@ -358,7 +358,8 @@ int runGrid(const Case& c, const char* outPath) {
         const double rM = TlPrdctbl::getBraggSlaterRadii(Z);
         radii.push_back(rM);
         radii.push_back(g.getCovalentRadiiForBecke(Z));
-        for (int i = 1; i <= g.nrgrid; ++i) {
+        // a dummy atom has no grid of its own (generateGrid_atom skips atomic number 0)
+        for (int i = 1; i <= g.nrgrid && Z != 0; ++i) {
             double ri = 0.0, wr = 0.0;
             if (g.radialGridType_ == DfGenerateGrid::RG_GaussChebyshev) {
                 g.getRadialAbscissaAndWeight_GaussChebyshev(rM, g.nrgrid, i, &ri, &wr);

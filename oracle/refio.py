@@ -38,7 +38,7 @@ def write_case(path, symbols, charges, xyz_bohr, basis, kv):
         for s, q, r in zip(symbols, charges, np.asarray(xyz_bohr).reshape(-1, 3)):
             f.write(f"atom {s} {q:.1f} {r[0]:.17g} {r[1]:.17g} {r[2]:.17g}\n")
         for el in sorted(set(symbols), key=list(symbols).index):
-            for sh in basis[el]:
+            for sh in basis.get(el, []) if el == "X" else basis[el]:  # X: a dummy atom, no basis
                 f.write(f"cgto {el} {sh['shell']} {len(sh['prims'])}\n")
                 for e, c in sh["prims"]:
                     f.write(f"{e:.17g} {c:.17g}\n")

@@ -21,7 +21,9 @@ import numpy as np
 
 _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 SHELL_L = {"s": 0, "p": 1, "d": 2}
-ELEMENT_Z = {"H": 1, "He": 2, "C": 6, "N": 7, "O": 8}
+# "X" is the reference's dummy atom: atomic number 0, no basis functions, no grid
+# (src/libpdf/Fl_Geometry.cpp:326-333, src/libpdf/DfGenerateGrid.cpp:950)
+ELEMENT_Z = {"X": 0, "H": 1, "He": 2, "C": 6, "N": 7, "O": 8}
 
 
 def load_basis(name="cc-pVDZ"):
@@ -76,7 +78,7 @@ class ShellTable:
         sa, sl, s0, sn, sp, pe, pc = [], [], [], [], [], [], []
         ao = 0
         for ia, el in enumerate(self.symbols):
-            for sh in basis[el]:
+            for sh in basis.get(el, []) if el == "X" else basis[el]:
                 e, c = normalised_contraction(sh["shell"], sh["prims"])
                 L = SHELL_L[sh["shell"]]
                 sa.append(ia)

@@ -7,8 +7,13 @@
 //   nu_mn  = mu_mn + a_mn (1 - mu_mn^2), a = u / (u^2 - 1), u = (R_m - R_n)/(R_m + R_n),
 //            a clamped to [-1/2, 1/2] (atomic size adjustment, Becke radii)
 //   w(r)   = w_single(r) * P_A(r) / sum_m P_m(r).
+// Partner atoms n with atomic number <= 0 (dummy atoms, `ghost`) are left out of
+// every product, as Ps_uij does (:2056); a dummy atom m still has its own P_m.
 // One thread per point; the atoms (coordinates and radius) are staged in
-// shared memory once per CTA. All arithmetic is FP64.
+// shared memory once per CTA. All arithmetic is FP64, and this file is compiled
+// without fused multiply-adds, so that every operation rounds once in the order
+// written: the weights then equal the CPU restatement's (plain IEEE operations in
+// the same order) bit for bit, and the weight screen keeps the same points.
 #include <cuda_runtime.h>
 
 #include "pdfxc_internal.cuh"
@@ -24,12 +29,14 @@ __device__ __forceinline__ double becke_s(double nu) {
 }
 
 __global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atom_xyz, const double* __restrict__ brad,
-                                               int natom, int size_adjust, int64_t npts,
-                                               const double* __restrict__ xyz, const int* __restrict__ owner,
-                                               const double* __restrict__ w_single, double* __restrict__ w_out) {
-    extern __shared__ double4 atoms[];  // x, y, z, radius
+                                               const int* __restrict__ ghost, int natom, int size_adjust,
+                                               int64_t npts, const double* __restrict__ xyz,
+                                               const int* __restrict__ owner, const double* __restrict__ w_single,
+                                               double* __restrict__ w_out) {
+    extern __shared__ double4 atoms[];  // x, y, z, radius (negative: a dummy partner, left out)
     for (int a = threadIdx.x; a < natom; a += blockDim.x)
-        atoms[a] = make_double4(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2], brad[a]);
+        atoms[a] = make_double4(atom_xyz[3 * a], atom_xyz[3 * a + 1], atom_xyz[3 * a + 2],
+                                ghost && ghost[a] ? -1.0 : brad[a]);
     __syncthreads();
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < npts; i += (int64_t)gridDim.x * blockDim.x) {
         const double rx = xyz[3 * i], ry = xyz[3 * i + 1], rz = xyz[3 * i + 2];
@@ -42,11 +49,13 @@ __global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atom_x
             for (int n = 0; n < natom && p != 0.0; ++n) {
                 if (n == m) continue;
                 const double4 B = atoms[n];
+                if (B.w < 0.0) continue;
+                const double Am = A.w < 0.0 ? brad[m] : A.w;
                 const double rn = sqrt((rx - B.x) * (rx - B.x) + (ry - B.y) * (ry - B.y) + (rz - B.z) * (rz - B.z));
                 const double Rmn = sqrt((A.x - B.x) * (A.x - B.x) + (A.y - B.y) * (A.y - B.y) + (A.z - B.z) * (A.z - B.z));
                 double u = (rm - rn) * (1.0 / Rmn);
                 if (size_adjust) {
-                    const double au = (A.w - B.w) / (A.w + B.w);
+                    const double au = (Am - B.w) / (Am + B.w);
                     double a = au / (au * au - 1.0);
                     a = a < -0.5 ? -0.5 : (a > 0.5 ? 0.5 : a);
                     u = u + a * (1.0 - u * u);
@@ -61,12 +70,18 @@ __global__ void __launch_bounds__(128) k_becke(const double* __restrict__ atom_x
 }
 
 // Pair constants: inv[m*n_atom + n] = 1/|R_m - R_n|, adj[m*n_atom + n] = a_mn (0 without size adjustment).
-__global__ void k_becke_pairs(const double* __restrict__ atom_xyz, const double* __restrict__ brad, int natom,
-                              int size_adjust, double* inv, double* adj) {
+// A dummy partner n (ghost[n] != 0) gets inv = 0 and adj = -1: then nu = -1 and its factor
+// s = (1 - f3(-1)) / 2 is exactly 1 (f(-1) = -1 in IEEE arithmetic), the same as leaving it out.
+__global__ void k_becke_pairs(const double* __restrict__ atom_xyz, const double* __restrict__ brad,
+                              const int* __restrict__ ghost, int natom, int size_adjust, double* inv, double* adj) {
     for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < natom * natom; e += gridDim.x * blockDim.x) {
         const int m = e / natom, n = e % natom;
         if (m == n) {
             inv[e] = adj[e] = 0.0;
+            continue;
+        }
+        if (ghost && ghost[n]) {
+            inv[e] = 0.0, adj[e] = -1.0;
             continue;
         }
         const double dx = atom_xyz[3 * m] - atom_xyz[3 * n], dy = atom_xyz[3 * m + 1] - atom_xyz[3 * n + 1],
@@ -195,7 +210,7 @@ __global__ void __launch_bounds__(128) k_ss(const double* __restrict__ atom_xyz,
 void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, const int* nbr_idx,
                const double* nbr_dist, int64_t npts, const double* xyz, const int* owner, const double* w_single,
                double* w_out, cudaStream_t s) {
-    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, atom_xyz, natom, 0, inv, adj);
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, atom_xyz, nullptr, natom, 0, inv, adj);
     const int threads = 128;
     int64_t blocks = (npts + threads - 1) / threads;
     if (blocks > 148 * 64) blocks = 148 * 64;
@@ -206,13 +221,13 @@ void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, cons
 
 void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
                         double* adj, cudaStream_t s) {
-    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, natom, size_adjust, inv, adj);
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, nullptr, natom, size_adjust, inv, adj);
 }
 
-void launch_becke_tab(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
-                      double* adj, int64_t npts, const double* xyz, const int* owner, const double* w_single,
-                      double* w_out, cudaStream_t s) {
-    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, natom, size_adjust, inv, adj);
+void launch_becke_tab(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
+                      double* inv, double* adj, int64_t npts, const double* xyz, const int* owner,
+                      const double* w_single, double* w_out, cudaStream_t s) {
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, ghost, natom, size_adjust, inv, adj);
     int64_t blocks = (npts + BECKE_T - 1) / BECKE_T;
     if (blocks > 148 * 32) blocks = 148 * 32;
     if (blocks < 1) blocks = 1;
@@ -224,14 +239,19 @@ void launch_becke_tab(const double* atom_xyz, const double* brad, int natom, int
 
 size_t becke_tab_max_atoms() { return (200u * 1024u) / (sizeof(double) * BECKE_T); }
 
-void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust, int64_t npts,
-                  const double* xyz, const int* owner, const double* w_single, double* w_out, cudaStream_t s) {
+void launch_becke(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
+                  int64_t npts, const double* xyz, const int* owner, const double* w_single, double* w_out,
+                  cudaStream_t s) {
     const int threads = 128;
     int64_t blocks = (npts + threads - 1) / threads;
     if (blocks > 148 * 64) blocks = 148 * 64;
     if (blocks < 1) blocks = 1;
-    k_becke<<<(unsigned)blocks, threads, sizeof(double4) * natom, s>>>(atom_xyz, brad, natom, size_adjust, npts, xyz,
-                                                                       owner, w_single, w_out);
+    const size_t smem = sizeof(double4) * natom;
+    cudaFuncSetAttribute(k_becke, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_becke<<<(unsigned)blocks, threads, smem, s>>>(atom_xyz, brad, ghost, natom, size_adjust, npts, xyz, owner,
+                                                    w_single, w_out);
 }
+
+size_t becke_max_atoms() { return (220u * 1024u) / sizeof(double4); }
 
 }  // namespace pdfxc

@@ -730,6 +730,56 @@ void launch_fock_delta(const double* V, double* Vprev, double* dV, size_t n, boo
     k_fock_delta<<<148 * 8, 256, 0, s>>>(V, Vprev, dV, n, has_prev ? 1 : 0);
 }
 
+// The upper triangle of a symmetric n x n matrix packed row by row: (i, j >= i) at
+// i n - i (i - 1) / 2 + (j - i). One CTA per row; the reads and writes along j are coalesced.
+__global__ void k_pack_upper(const double* __restrict__ V, int n, double* __restrict__ packed) {
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const int64_t o = (int64_t)i * n - (int64_t)i * (i - 1) / 2 - i;
+        for (int j = i + threadIdx.x; j < n; j += blockDim.x) packed[o + j] = V[(int64_t)i * n + j];
+    }
+}
+
+// Both triangles from the packed upper triangle, in 32 x 32 tiles: a tile on or above the
+// diagonal copies packed rows; a tile below it reads its mirror tile's packed rows (coalesced)
+// into shared memory and writes the transpose.
+__global__ void k_unpack_upper(const double* __restrict__ packed, int n, double* __restrict__ V) {
+    __shared__ double t[32][33];
+    const int nt = (n + 31) / 32;
+    for (int64_t tile = blockIdx.x; tile < (int64_t)nt * nt; tile += gridDim.x) {
+        const int ti = (int)(tile / nt), tj = (int)(tile % nt);
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 32 x 8 threads
+        if (ti <= tj) {
+            for (int r = ty; r < 32; r += 8) {
+                const int i = ti * 32 + r, j = tj * 32 + tx;
+                if (i < n && j < n) {
+                    const int a = min(i, j), b = max(i, j);
+                    V[(int64_t)i * n + j] = packed[(int64_t)a * n - (int64_t)a * (a - 1) / 2 + (b - a)];
+                }
+            }
+        } else {
+            // rows tj*32.. of the mirror tile (row index < column index: the packed upper part)
+            for (int r = ty; r < 32; r += 8) {
+                const int a = tj * 32 + r, b = ti * 32 + tx;
+                if (a < n && b < n) t[r][tx] = packed[(int64_t)a * n - (int64_t)a * (a - 1) / 2 + (b - a)];
+            }
+            __syncthreads();
+            for (int r = ty; r < 32; r += 8) {
+                const int i = ti * 32 + r, j = tj * 32 + tx;
+                if (i < n && j < n) V[(int64_t)i * n + j] = t[tx][r];
+            }
+            __syncthreads();
+        }
+    }
+}
+
+void launch_pack_upper(const double* V, int n, double* packed, cudaStream_t s) {
+    k_pack_upper<<<148 * 8, 256, 0, s>>>(V, n, packed);
+}
+
+void launch_unpack_upper(const double* packed, int n, double* V, cudaStream_t s) {
+    k_unpack_upper<<<148 * 8, 256, 0, s>>>(packed, n, V);
+}
+
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk, double* scalars,
                    cudaStream_t s) {
     k_symmetrize<<<148 * 8, 256, 0, s>>>(Vacc, V, nao);

@@ -141,9 +141,11 @@ extern "C" pdfxc_status pdfxc_build_vxc_noalloc(int device, int functional, int 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     pdfxc_status st = PDFXC_OK;
     do {
-        // the AO count implied by the shells must match n_ao (a small device -> host copy, no allocation)
+        // the AO count implied by the shells must match n_ao: a small device -> host copy (no
+        // allocation) ordered on the caller's stream, after the caller's writes of the shell table
         int h_l[PDFXC_NOALLOC_MAX_SHELL];
-        if (cudaMemcpy(h_l, d_shell_l, sizeof(int) * nshell, cudaMemcpyDeviceToHost) != cudaSuccess) {
+        if (cudaMemcpyAsync(h_l, d_shell_l, sizeof(int) * nshell, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
             st = PDFXC_ERR_CUDA;
             break;
         }
@@ -163,42 +165,59 @@ extern "C" pdfxc_status pdfxc_build_vxc_noalloc(int device, int functional, int 
         }
         const bool gga = pdfxc::functional_is_gga(functional);
         const int nbp = nao > 64 ? (nao + 63) / 64 * 64 : 64;
-        // fixed part of the scratch
-        size_t off = 0;
-        auto take = [&](size_t bytes) {
-            unsigned char* p = base + off;
-            off = align256(off + bytes);
-            return p;
-        };
-        double* Vacc = reinterpret_cast<double*>(take(sizeof(double) * nao * nao));
-        double* totals = reinterpret_cast<double*>(take(sizeof(double) * 2));
-        int* sh_p0 = reinterpret_cast<int*>(take(sizeof(int) * nshell));
-        int* sh_ao0 = reinterpret_cast<int*>(take(sizeof(int) * nshell));
-        int* blk_shells = reinterpret_cast<int*>(take(sizeof(int) * nshell));
-        int* blk_shell_row = reinterpret_cast<int*>(take(sizeof(int) * nshell));
-        int* blk_aos = reinterpret_cast<int*>(take(sizeof(int) * nao));
-        // per-block part
         const size_t ws_block = pdfxc::block_ws_doubles(nbp, true) * sizeof(double);
-        const size_t per_block = ws_block + sizeof(BlockMeta) + sizeof(double) * BLOCK_PTS * (4 + 4 + 4) + 2 * sizeof(double);
-        const size_t avail = PDFXC_NOALLOC_SCRATCH_BYTES - off - 8 * 256;
-        const int chunk = (int)(avail / per_block);
+        // the carve-outs of the array for `chunk` blocks per pass; each starts on a 256-byte boundary
+        struct Layout {
+            double *Vacc, *totals, *px, *py, *pz, *pw, *rho, *coef, *blk_sum;
+            int *sh_p0, *sh_ao0, *blk_shells, *blk_shell_row, *blk_aos;
+            BlockMeta* meta;
+            char* ws;
+            size_t end;
+        };
+        auto layout = [&](int chunk) {
+            Layout L;
+            size_t off = 0;
+            auto take = [&](size_t bytes) {
+                unsigned char* p = base + off;
+                off = align256(off + bytes);
+                return p;
+            };
+            L.Vacc = reinterpret_cast<double*>(take(sizeof(double) * nao * nao));
+            L.totals = reinterpret_cast<double*>(take(sizeof(double) * 2));
+            L.sh_p0 = reinterpret_cast<int*>(take(sizeof(int) * nshell));
+            L.sh_ao0 = reinterpret_cast<int*>(take(sizeof(int) * nshell));
+            L.blk_shells = reinterpret_cast<int*>(take(sizeof(int) * nshell));
+            L.blk_shell_row = reinterpret_cast<int*>(take(sizeof(int) * nshell));
+            L.blk_aos = reinterpret_cast<int*>(take(sizeof(int) * nao));
+            L.meta = reinterpret_cast<BlockMeta*>(take(sizeof(BlockMeta) * chunk));
+            L.px = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
+            L.py = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
+            L.pz = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
+            L.pw = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
+            L.rho = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * 4 * chunk));
+            L.coef = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * 4 * chunk));
+            L.blk_sum = reinterpret_cast<double*>(take(sizeof(double) * 2 * chunk));
+            L.ws = reinterpret_cast<char*>(take(ws_block * chunk));
+            L.end = off;
+            return L;
+        };
+        // the largest block count per pass whose layout fits the array (padding included)
+        const size_t per_block = ws_block + sizeof(BlockMeta) + sizeof(double) * BLOCK_PTS * (4 + 4 + 4) +
+                                 2 * sizeof(double);
+        int chunk = (int)(PDFXC_NOALLOC_SCRATCH_BYTES / per_block);
+        while (chunk > 0 && layout(chunk).end > PDFXC_NOALLOC_SCRATCH_BYTES) --chunk;
         if (chunk < 1) {
             st = PDFXC_ERR_ARG;
             break;
         }
-        BlockMeta* meta = reinterpret_cast<BlockMeta*>(take(sizeof(BlockMeta) * chunk));
-        double* px = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
-        double* py = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
-        double* pz = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
-        double* pw = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * chunk));
-        double* rho = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * 4 * chunk));
-        double* coef = reinterpret_cast<double*>(take(sizeof(double) * BLOCK_PTS * 4 * chunk));
-        double* blk_sum = reinterpret_cast<double*>(take(sizeof(double) * 2 * chunk));
-        char* ws = reinterpret_cast<char*>(take(ws_block * chunk));
-        if (off > PDFXC_NOALLOC_SCRATCH_BYTES) {
-            st = PDFXC_ERR_ARG;
-            break;
-        }
+        const Layout L = layout(chunk);
+        double* Vacc = L.Vacc;
+        double* totals = L.totals;
+        int *sh_p0 = L.sh_p0, *sh_ao0 = L.sh_ao0, *blk_shells = L.blk_shells, *blk_shell_row = L.blk_shell_row;
+        int* blk_aos = L.blk_aos;
+        BlockMeta* meta = L.meta;
+        double *px = L.px, *py = L.py, *pz = L.pz, *pw = L.pw, *rho = L.rho, *coef = L.coef, *blk_sum = L.blk_sum;
+        char* ws = L.ws;
         // clear what must start at zero: the Vxc accumulator and the totals
         if (cudaMemsetAsync(Vacc, 0, sizeof(double) * nao * nao, s) != cudaSuccess ||
             cudaMemsetAsync(totals, 0, sizeof(double) * 2, s) != cudaSuccess) {
@@ -207,6 +226,10 @@ extern "C" pdfxc_status pdfxc_build_vxc_noalloc(int device, int functional, int 
         }
         k_noalloc_basis<<<1, 256, 0, s>>>(nshell, d_shell_l, d_shell_nprim, sh_p0, sh_ao0, blk_shells, blk_shell_row,
                                           blk_aos, nao);
+        if (cudaPeekAtLastError() != cudaSuccess) {
+            st = PDFXC_ERR_CUDA;
+            break;
+        }
         const pdfxc::BasisView bv{d_atom_xyz, d_shell_atom, d_shell_l, d_shell_nprim, sh_p0, sh_ao0, d_prim_exp,
                                   d_prim_coef};
         const pdfxc::GridView gv{px, py, pz, pw, meta, blk_shells, blk_shell_row, blk_aos};
@@ -220,10 +243,16 @@ extern "C" pdfxc_status pdfxc_build_vxc_noalloc(int device, int functional, int 
             pdfxc::launch_rho_functional(gv, 0, nb, functional, false, 1e-16, ws, rho, coef, blk_sum, s);
             pdfxc::launch_gemm_v(gv, 0, nb, nbp, gga, coef, ws, Vacc, nao, s);
             k_noalloc_sums<<<1, 32, 0, s>>>(blk_sum, nb, totals);
+            if (cudaPeekAtLastError() != cudaSuccess) {  // this pass's launches (configuration, resources)
+                st = PDFXC_ERR_CUDA;
+                break;
+            }
         }
+        if (st != PDFXC_OK) break;
         k_noalloc_symmetrize<<<148 * 4, 256, 0, s>>>(Vacc, d_V, nao);
-        if (cudaMemcpyAsync(d_exc_nelec, totals, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
-            cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(s) != cudaSuccess) {
+        if (cudaPeekAtLastError() != cudaSuccess ||
+            cudaMemcpyAsync(d_exc_nelec, totals, 2 * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess ||
+            cudaStreamSynchronize(s) != cudaSuccess) {
             st = PDFXC_ERR_CUDA;
             break;
         }

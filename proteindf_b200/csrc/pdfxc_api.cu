@@ -27,6 +27,11 @@ struct CudaError : std::runtime_error {
     using std::runtime_error::runtime_error;
 };
 
+// An input the library cannot take (status PDFXC_ERR_UNSUPPORTED).
+struct Unsupported : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+
 // After a kernel launch: a launch that failed (configuration, resources) names itself in the
 // error, also while a graph is being captured. No synchronisation.
 #define PDFXC_LAUNCHED(what)                                                                        \
@@ -86,6 +91,9 @@ pdfxc_status guarded(pdfxc_ctx* ctx, F&& f) {
     } catch (const CudaError& e) {
         ctx->err = e.what();
         return PDFXC_ERR_CUDA;
+    } catch (const Unsupported& e) {
+        ctx->err = e.what();
+        return PDFXC_ERR_UNSUPPORTED;
     } catch (const std::exception& e) {
         ctx->err = e.what();
         return PDFXC_ERR_ARG;
@@ -260,39 +268,67 @@ pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt)
     return PDFXC_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// The host copy of a system (atoms, shells, primitives) with its AO offsets; no device work.
+pdfxc_status set_host_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz, const int* atom_z, int nshell,
+                             const int* shell_atom, const int* shell_l, const int* shell_nprim,
+                             const double* prim_exp, const double* prim_coef) {
+    if (natom <= 0 || nshell <= 0 || !atom_xyz || !shell_atom || !shell_l || !shell_nprim || !prim_exp || !prim_coef) {
+        ctx->err = "pdfxc_set_system: empty system or null pointer";
+        return PDFXC_ERR_ARG;
+    }
+    for (int s = 0; s < nshell; ++s)
+        if (shell_l[s] < 0 || shell_l[s] > 2 || shell_nprim[s] <= 0 || shell_atom[s] < 0 || shell_atom[s] >= natom) {
+            ctx->err = "pdfxc_set_system: shell " + std::to_string(s) + " out of range (only s, p, d shells)";
+            return PDFXC_ERR_ARG;
+        }
+    ctx->natom = natom;
+    ctx->nshell = nshell;
+    ctx->h_atom_xyz.assign(atom_xyz, atom_xyz + 3 * natom);
+    ctx->h_atom_z.assign(natom, 0);
+    if (atom_z) ctx->h_atom_z.assign(atom_z, atom_z + natom);
+    ctx->h_sh_atom.assign(shell_atom, shell_atom + nshell);
+    ctx->h_sh_l.assign(shell_l, shell_l + nshell);
+    ctx->h_sh_nprim.assign(shell_nprim, shell_nprim + nshell);
+    ctx->h_sh_p0.resize(nshell);
+    ctx->h_sh_ao0.resize(nshell);
+    int np = 0, ao = 0;
+    for (int s = 0; s < nshell; ++s) {
+        ctx->h_sh_p0[s] = np;
+        ctx->h_sh_ao0[s] = ao;
+        np += shell_nprim[s];
+        ao += 2 * shell_l[s] + 1;
+    }
+    ctx->nao = ao;
+    ctx->h_p_exp.assign(prim_exp, prim_exp + np);
+    ctx->h_p_coef.assign(prim_coef, prim_coef + np);
+    return PDFXC_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 pdfxc_status pdfxc_set_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz, const int* atom_z, int nshell,
                               const int* shell_atom, const int* shell_l, const int* shell_nprim,
                               const double* prim_exp, const double* prim_coef) {
     return guarded(ctx, [&]() -> pdfxc_status {
-        if (natom <= 0 || nshell <= 0 || !atom_xyz || !shell_atom || !shell_l || !shell_nprim || !prim_exp || !prim_coef) {
-            ctx->err = "pdfxc_set_system: empty system or null pointer";
-            return PDFXC_ERR_ARG;
-        }
+        if (const pdfxc_status st = set_host_system(ctx, natom, atom_xyz, atom_z, nshell, shell_atom, shell_l,
+                                                    shell_nprim, prim_exp, prim_coef))
+            return st;
         dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);  // neighbour lists of the old geometry
-        ctx->natom = natom;
-        ctx->nshell = nshell;
-        ctx->h_atom_xyz.assign(atom_xyz, atom_xyz + 3 * natom);
-        ctx->h_atom_z.assign(natom, 0);
-        if (atom_z) ctx->h_atom_z.assign(atom_z, atom_z + natom);
-        ctx->h_sh_atom.assign(shell_atom, shell_atom + nshell);
-        ctx->h_sh_l.assign(shell_l, shell_l + nshell);
-        ctx->h_sh_nprim.assign(shell_nprim, shell_nprim + nshell);
-        ctx->h_sh_p0.resize(nshell);
-        ctx->h_sh_ao0.resize(nshell);
-        int np = 0, ao = 0;
-        for (int s = 0; s < nshell; ++s) {
-            if (shell_l[s] < 0 || shell_l[s] > 2 || shell_nprim[s] <= 0 || shell_atom[s] < 0 || shell_atom[s] >= natom) {
-                ctx->err = "pdfxc_set_system: shell " + std::to_string(s) + " out of range (only s, p, d shells)";
-                return PDFXC_ERR_ARG;
-            }
-            ctx->h_sh_p0[s] = np;
-            ctx->h_sh_ao0[s] = ao;
-            np += shell_nprim[s];
-            ao += 2 * shell_l[s] + 1;
+        const int ao = ctx->nao;
+        // dummy atoms (atomic number <= 0; only when atomic numbers are given): the Becke partition
+        // leaves them out as partners (DfGenerateGrid::Ps_uij, src/libpdf/DfGenerateGrid.cpp:2056)
+        dev_free(ctx->d_ghost);
+        if (atom_z && std::any_of(atom_z, atom_z + natom, [](int z) { return z <= 0; })) {
+            std::vector<int> ghost(natom);
+            for (int a = 0; a < natom; ++a) ghost[a] = atom_z[a] <= 0 ? 1 : 0;
+            upload(&ctx->d_ghost, ghost, ctx->stream);
         }
-        ctx->nao = ao;
-        ctx->h_p_exp.assign(prim_exp, prim_exp + np);
-        ctx->h_p_coef.assign(prim_coef, prim_coef + np);
         cudaStream_t s = ctx->stream;
         upload(&ctx->d_atom_xyz, ctx->h_atom_xyz, s);
         upload(&ctx->d_sh_atom, ctx->h_sh_atom, s);
@@ -345,9 +381,19 @@ int group_blocks(const pdfxc_ctx* ctx) {
 // group_blocks x block_points consecutive points, each group into blocks of block_points;
 // every group keeps the shells of its segment whose value/gradient envelope reaches
 // ao_cutoff at the group's nearest point.
-void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom,
-                const std::vector<GridSegment>& segs) {
-    free_grid(ctx);
+// The host side of a blocked grid (plan_grid), before it is uploaded.
+struct HostGrid {
+    std::vector<double> px, py, pz, pw;
+    std::vector<int> shells, rows, aos, row_info, grp_blk;
+    int nblk = 0, ngrp = 0, max_nb = 0;
+    double flops = 0.0, sum_nb = 0.0;
+    size_t max_ws = 0;
+    bool mixed = false;
+};
+
+void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom,
+               const std::vector<GridSegment>& segs, HostGrid& G) {
+    ctx->h_owner.clear();
     const int bp = ctx->opt.block_points;
     const int gb = group_blocks(ctx);
     // 1. spatial order: Morton code over each segment's bounding box; a group takes up to
@@ -358,7 +404,8 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     std::vector<std::pair<uint64_t, int64_t>> key(npts);
     std::vector<std::pair<int64_t, int64_t>> runs;  // [i0, i1) of key per block
     std::vector<int> blk_seg;
-    std::vector<int> grp_blk(1, 0);  // blocks of group k: [grp_blk[k], grp_blk[k+1])
+    std::vector<int>& grp_blk = G.grp_blk;  // blocks of group k: [grp_blk[k], grp_blk[k+1])
+    grp_blk.assign(1, 0);
     ctx->seg_blk.assign(1, 0);
     for (size_t si = 0; si < segs.size(); ++si) {
         const GridSegment& sg = segs[si];
@@ -398,7 +445,9 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     }
     const int nblk = (int)runs.size();
     const int ngrp = (int)grp_blk.size() - 1;
-    std::vector<double> px((size_t)nblk * BLOCK_PTS), py(px.size()), pz(px.size()), pw(px.size(), 0.0);
+    std::vector<double>&px = G.px, &py = G.py, &pz = G.pz, &pw = G.pw;
+    px.assign((size_t)nblk * BLOCK_PTS, 0.0), py.assign(px.size(), 0.0), pz.assign(px.size(), 0.0),
+        pw.assign(px.size(), 0.0);
     ctx->h_src.assign(px.size(), -1);
     if (atom) ctx->h_owner.assign(px.size(), 0);
     std::vector<double> cen(3 * (size_t)ngrp), rad(ngrp);
@@ -448,7 +497,8 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     for (int sh = 0; sh < ctx->nshell; ++sh)
         Rs[sh] = shell_cutoff_radius(ctx->h_sh_l[sh], &ctx->h_p_exp[ctx->h_sh_p0[sh]], &ctx->h_p_coef[ctx->h_sh_p0[sh]],
                                      ctx->h_sh_nprim[sh], ctx->opt.ao_cutoff);
-    std::vector<int> shells, rows, aos, row_info;
+    std::vector<int>&shells = G.shells, &rows = G.rows, &aos = G.aos, &row_info = G.row_info;
+    shells.clear(), rows.clear(), aos.clear(), row_info.clear();
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
     double flops = 0.0, sum_nb = 0.0;
     // Candidate shells of a group from a uniform grid of the segment's atoms (cell edge = the
@@ -558,7 +608,19 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
             m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
             flops += 4.0 * double(m.nb) * m.nb * m.npts;
             sum_nb += m.nb;
+            G.max_nb = std::max(G.max_nb, m.nb);
         }
+    }
+    // The INT8 rho contraction runs over K = nbp screened AOs and accumulates exactly in int32:
+    // its order-5 accumulator sums four digit products of at most 127^2 per K index
+    // (kernels_mixed.cu), exact while 4 * 127^2 * K < 2^31.
+    if (mixed && ctx->opt.split_terms == 10) {
+        for (int bb = 0; bb < nblk; ++bb)
+            if (ctx->h_meta[bb].nbp > pdfxc::OZ_MAX_K)
+                throw Unsupported("grid: a group of points screens in " + std::to_string(ctx->h_meta[bb].nb) +
+                                  " AOs; the INT8 tensor-core contraction is exact up to " +
+                                  std::to_string(pdfxc::OZ_MAX_K) +
+                                  " AOs per group (use the FP64 path or a larger ao_cutoff)");
     }
     // 3. chunks of whole groups whose intermediates fit the workspace budget
     ctx->chunks.clear();
@@ -593,6 +655,21 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     ctx->chunks.push_back(cur);
     max_ws = std::max(max_ws, off);
 
+    G.nblk = nblk, G.ngrp = ngrp, G.flops = flops, G.sum_nb = sum_nb, G.max_ws = max_ws, G.mixed = mixed;
+}
+
+void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom,
+                const std::vector<GridSegment>& segs) {
+    free_grid(ctx);
+    HostGrid G;
+    plan_grid(ctx, npts, xyzw, atom, segs, G);
+    const int nblk = G.nblk, ngrp = G.ngrp;
+    const size_t max_ws = G.max_ws;
+    const bool mixed = G.mixed;
+    const std::vector<double>&px = G.px, &py = G.py, &pz = G.pz, &pw = G.pw;
+    const std::vector<int>&shells = G.shells, &rows = G.rows, &aos = G.aos, &row_info = G.row_info;
+    const std::vector<int>& grp_blk = G.grp_blk;
+    const double flops = G.flops, sum_nb = G.sum_nb;
     cudaStream_t s = ctx->stream;
     upload(&ctx->d_px, px, s);
     upload(&ctx->d_py, py, s);
@@ -702,10 +779,14 @@ void partition_weights_device(pdfxc_ctx* ctx, bool ss, int64_t npts, const doubl
                              ctx->d_nbr_idx, ctx->d_nbr_dist, npts, d_xyz, d_own, d_ws, d_wo, s);
         } else if ((size_t)ctx->natom <= pdfxc::becke_tab_max_atoms()) {
             dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
-            pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, d_pair,
+            pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->d_ghost, ctx->natom, size_adjust, d_pair,
                                     d_pair + (size_t)ctx->natom * ctx->natom, npts, d_xyz, d_own, d_ws, d_wo, s);
+        } else if ((size_t)ctx->natom <= pdfxc::becke_max_atoms()) {
+            pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->d_ghost, ctx->natom, size_adjust, npts, d_xyz, d_own,
+                                d_ws, d_wo, s);
         } else {
-            pdfxc::launch_becke(ctx->d_atom_xyz, d_br, ctx->natom, size_adjust, npts, d_xyz, d_own, d_ws, d_wo, s);
+            throw std::runtime_error("Becke partition: at most " + std::to_string(pdfxc::becke_max_atoms()) +
+                                     " atoms (use the Stratmann-Scuseria partition)");
         }
         PDFXC_CUDA(cudaGetLastError());
         PDFXC_CUDA(cudaStreamSynchronize(s));
@@ -1216,6 +1297,9 @@ pdfxc_status pdfxc_build_vxc_delta_device(pdfxc_ctx* ctx, int functional, const 
         }
         const size_t n2 = (size_t)ctx->nao * ctx->nao;
         if (!ctx->d_Vprev) dev_alloc(&ctx->d_Vprev, n2);
+        // the difference kernel overwrites d_Vprev: until this call has completed, the context
+        // holds no usable previous iteration
+        ctx->vprev_iter = 0;
         run_build(ctx, functional, d_PA, incremental != 0);
         if (d_V) PDFXC_CUDA(cudaMemcpyAsync(d_V, ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToDevice, ctx->stream));
         pdfxc::launch_fock_delta(ctx->d_V, ctx->d_Vprev, d_dV, n2, iteration >= 2, ctx->stream);
@@ -1766,6 +1850,54 @@ pdfxc_status pdfxc_partition_blocks(int64_t nblk, const double* cost, int nparts
     return PDFXC_OK;
 }
 
+pdfxc_status pdfxc_plan_grid(const pdfxc_options* opt, int natom, const double* atom_xyz, int nshell,
+                              const int* shell_atom, const int* shell_l, const int* shell_nprim,
+                              const double* prim_exp, const double* prim_coef, int64_t npts, const double* xyzw,
+                              pdfxc_grid_plan* out) {
+    if (!out || npts <= 0 || !xyzw) return PDFXC_ERR_ARG;
+    pdfxc_ctx c;  // host fields only: nothing here touches a device
+    pdfxc_default_options(&c.opt);
+    if (opt) c.opt = *opt;
+    if (c.opt.block_points <= 0 || c.opt.block_points > BLOCK_PTS) c.opt.block_points = BLOCK_PTS;
+    if (c.opt.workspace_bytes == 0) c.opt.workspace_bytes = size_t(4) << 30;
+    if (c.opt.split_terms != 3 && c.opt.split_terms != 6 && c.opt.split_terms != 10) c.opt.split_terms = 10;
+    if (c.opt.precision != PDFXC_PRECISION_FP64 && c.opt.precision != PDFXC_PRECISION_MIXED) return PDFXC_ERR_ARG;
+    try {
+        if (const pdfxc_status st = set_host_system(&c, natom, atom_xyz, nullptr, nshell, shell_atom, shell_l,
+                                                    shell_nprim, prim_exp, prim_coef))
+            return st;
+        HostGrid G;
+        plan_grid(&c, npts, xyzw, nullptr, {GridSegment{0, npts, 0, c.nshell}}, G);
+        out->nblocks = G.nblk;
+        out->ngroups = G.ngrp;
+        out->npts_padded = (int64_t)G.nblk * BLOCK_PTS;
+        out->max_nb = G.max_nb;
+        out->contraction_flops = G.flops;
+        out->mean_nb = G.nblk ? G.sum_nb / G.nblk : 0.0;
+        out->workspace_bytes = G.max_ws;
+        out->nchunks = (int)c.chunks.size();
+    } catch (const Unsupported&) {
+        return PDFXC_ERR_UNSUPPORTED;
+    } catch (const std::bad_alloc&) {
+        return PDFXC_ERR_NOMEM;
+    } catch (const std::exception&) {
+        return PDFXC_ERR_ARG;
+    }
+    return PDFXC_OK;
+}
+
+pdfxc_status pdfxc_pack_upper(const double* d_V, int n, double* d_packed, void* stream) {
+    if (n <= 0 || !d_V || !d_packed) return PDFXC_ERR_ARG;
+    pdfxc::launch_pack_upper(d_V, n, d_packed, static_cast<cudaStream_t>(stream));
+    return cudaPeekAtLastError() == cudaSuccess ? PDFXC_OK : PDFXC_ERR_CUDA;
+}
+
+pdfxc_status pdfxc_unpack_upper(const double* d_packed, int n, double* d_V, void* stream) {
+    if (n <= 0 || !d_V || !d_packed) return PDFXC_ERR_ARG;
+    pdfxc::launch_unpack_upper(d_packed, n, d_V, static_cast<cudaStream_t>(stream));
+    return cudaPeekAtLastError() == cudaSuccess ? PDFXC_OK : PDFXC_ERR_CUDA;
+}
+
 pdfxc_status pdfxc_grid_stats(pdfxc_ctx* ctx, int64_t* nblocks, int64_t* npts_padded, double* contraction_flops,
                               double* mean_nb) {
     if (!ctx) return PDFXC_ERR_ARG;
@@ -1797,7 +1929,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     if (ctx->stream) cudaStreamSynchronize(ctx->stream);
     free_grid(ctx);
     dev_free(ctx->d_atom_xyz), dev_free(ctx->d_p_exp), dev_free(ctx->d_p_coef);
-    dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist);
+    dev_free(ctx->d_nbr_idx), dev_free(ctx->d_nbr_dist), dev_free(ctx->d_ghost);
     dev_free(ctx->d_sh_atom), dev_free(ctx->d_sh_l), dev_free(ctx->d_sh_nprim), dev_free(ctx->d_sh_p0), dev_free(ctx->d_sh_ao0);
     dev_free(ctx->d_P), dev_free(ctx->d_V), dev_free(ctx->d_Vacc), dev_free(ctx->d_scalars), dev_free(ctx->d_err);
     dev_free(ctx->d_p_rowexp); dev_free(ctx->d_Vprev); dev_free(ctx->d_p_words); dev_free(ctx->d_row_cols);

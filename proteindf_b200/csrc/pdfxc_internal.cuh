@@ -143,6 +143,7 @@ struct pdfxc_ctx {
     int* d_row_cols = nullptr;      // batch: per AO row its molecule's columns [c0, c1) (2 ints)
     bool rho_valid = false;
     pdfxc_ctx* dens = nullptr;  // pdfxc_density: FP64 context over the requested points (same system)
+    int* d_ghost = nullptr;       // [natom] dummy atoms (atomic number <= 0 given to set_system), or null
     int* d_nbr_idx = nullptr;     // Stratmann-Scuseria weights: per atom the other atoms by distance
     double* d_nbr_dist = nullptr;
     int rho_gga = 0;
@@ -215,6 +216,9 @@ void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga,
 void launch_fock_delta(const double* V, double* Vprev, double* dV, size_t n, bool has_prev, cudaStream_t s);
 void launch_finish(const double* Vacc, double* V, int nao, const double* blk_sum, int nblk,
                    double* scalars, cudaStream_t s);
+// the upper triangle (j >= i) of a symmetric n x n matrix packed row by row, and back (both triangles)
+void launch_pack_upper(const double* V, int n, double* packed, cudaStream_t s);
+void launch_unpack_upper(const double* packed, int n, double* V, cudaStream_t s);
 // Vacc += phi Z^T with Z in plane zplane of each block's workspace
 void launch_gemm_v_plane(const GridView& g, int blk0, int nblk, int max_nbp, int zplane, char* ws, double* Vacc,
                          int nao, cudaStream_t s);
@@ -247,13 +251,15 @@ void launch_ss(const double* atom_xyz, int natom, double* inv, double* adj, cons
                double* w_out, cudaStream_t s);
 void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
                         double* adj, cudaStream_t s);
-void launch_becke(const double* atom_xyz, const double* brad, int natom, int size_adjust,
+// ghost (n_atom ints, may be null): partner atoms left out of every product (atomic number <= 0)
+void launch_becke(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
                   int64_t npts, const double* xyz, const int* owner, const double* w_single,
                   double* w_out, cudaStream_t s);
+size_t becke_max_atoms();
 // the table form (pair constants in inv/adj, n_atom^2 doubles each), for n_atom <= becke_tab_max_atoms()
-void launch_becke_tab(const double* atom_xyz, const double* brad, int natom, int size_adjust, double* inv,
-                      double* adj, int64_t npts, const double* xyz, const int* owner, const double* w_single,
-                      double* w_out, cudaStream_t s);
+void launch_becke_tab(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
+                      double* inv, double* adj, int64_t npts, const double* xyz, const int* owner,
+                      const double* w_single, double* w_out, cudaStream_t s);
 size_t becke_tab_max_atoms();
 
 // Intermediates of one block inside its chunk workspace (doubles):
@@ -312,6 +318,10 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 // maxima (e_phi_g, e_z_g, written by the group's first block). P_sub is shared by the group
 // and lives only in the first block's region, after `total` (`total_lead` bytes in all).
 constexpr int OZ_SLICES = 4;
+// Largest K (screened AOs of a group, padded to 128) of the INT8 rho contraction: its order-5
+// int32 accumulator sums four digit products of at most 127^2 per K index, exact while
+// 4 * 127^2 * K <= 2^31 - 1 (K <= 33285).
+constexpr int OZ_MAX_K = 33280;
 struct OzLayout {
     size_t rad;                 // radial sums: S0 [nsh][128], then S1 [nsh][128]
     size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs

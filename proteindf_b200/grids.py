@@ -30,8 +30,9 @@ _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 # used for the radial mapping and the pruning; the Becke size adjustment uses
 # 0.35 for hydrogen and the Bragg-Slater radius otherwise
 # (src/libpdf/DfGenerateGrid.cpp:1958-1968).
-BRAGG_SLATER = {1: 0.25, 6: 0.70, 7: 0.65, 8: 0.60}
-BECKE_RADIUS = {1: 0.35, 6: 0.70, 7: 0.65, 8: 0.60}
+# A dummy atom (atomic number 0) has radius 0 in both tables and no grid of its own.
+BRAGG_SLATER = {0: 0.0, 1: 0.25, 6: 0.70, 7: 0.65, 8: 0.60}
+BECKE_RADIUS = {0: 0.0, 1: 0.35, 6: 0.70, 7: 0.65, 8: 0.60}
 # Radial scales of the SG-1 grid (and of USER grids' gradient grid), as the reference
 # sets them for those grid types (src/libpdf/DfGenerateGrid.cpp:409-418).
 SG1_RADIUS = {1: 1.0000, 6: 1.2308, 7: 1.0256, 8: 0.8791}
@@ -105,6 +106,8 @@ def molecular_grid(atom_xyz, atom_z, **kw):
     """Single-centre grid for every atom: (points (n,3), w_single (n,), atom (n,))."""
     P, W, A = [], [], []
     for a, (c, z) in enumerate(zip(np.asarray(atom_xyz), atom_z)):
+        if int(z) == 0:  # dummy atom: no grid (DfGenerateGrid::generateGrid_atom, :950)
+            continue
         p, w = atom_grid(np.asarray(c, dtype=np.float64), int(z), **kw)
         P.append(p)
         W.append(w)

@@ -90,6 +90,19 @@ def density_matrix(nao, nocc, seed=0):
     return 2.0 * q @ q.T
 
 
+def density_matrix_device(nao, nocc, seed=0, device="cuda"):
+    """The same matrix as density_matrix (the same seeded N(0,1) draw), with the QR and the
+    product formed on a CUDA device as a torch FP64 tensor: for the ~18,600-AO inputs whose
+    host QR takes minutes. Equal to density_matrix up to rounding (P is invariant to the
+    signs of Q's columns)."""
+    import torch
+    rng = np.random.default_rng(seed)
+    a = torch.from_numpy(rng.standard_normal((nao, nocc))).to(device)
+    q, _ = torch.linalg.qr(a)
+    del a
+    return 2.0 * (q @ q.T)
+
+
 def nuclear_charges(symbols):
-    z = {"H": 1, "C": 6, "N": 7, "O": 8}
+    z = {"X": 0, "H": 1, "C": 6, "N": 7, "O": 8}
     return [float(z[s]) for s in symbols]

@@ -23,7 +23,7 @@ EXPORTS = [
     "pdfxc_xc_gradient", "pdfxc_build_vxc_uks", "pdfxc_get_rho_uks", "pdfxc_set_rho_uks", "pdfxc_ss_weights",
     "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
     "pdfxc_build_vxc_batched", "pdfxc_density", "pdfxc_generate_grid", "pdfxc_get_grid",
-    "pdfxc_build_vxc_delta_device",
+    "pdfxc_build_vxc_delta_device", "pdfxc_pack_upper", "pdfxc_unpack_upper", "pdfxc_plan_grid",
 ]
 
 
@@ -53,6 +53,13 @@ class Mol(ctypes.Structure):
                 ("nshell", ctypes.c_int), ("shell_atom", ctypes.c_void_p), ("shell_l", ctypes.c_void_p),
                 ("shell_nprim", ctypes.c_void_p), ("prim_exp", ctypes.c_void_p), ("prim_coef", ctypes.c_void_p),
                 ("npts", ctypes.c_int64), ("xyzw", ctypes.c_void_p), ("atom", ctypes.c_void_p)]
+
+
+class GridPlan(ctypes.Structure):
+    """pdfxc_grid_plan: the host plan of a blocked, screened grid."""
+    _fields_ = [("nblocks", ctypes.c_int64), ("ngroups", ctypes.c_int64), ("npts_padded", ctypes.c_int64),
+                ("max_nb", ctypes.c_int), ("contraction_flops", ctypes.c_double), ("mean_nb", ctypes.c_double),
+                ("workspace_bytes", ctypes.c_size_t), ("nchunks", ctypes.c_int)]
 
 
 class Profile(ctypes.Structure):
@@ -106,6 +113,10 @@ def load_library(path=LIB_PATH):
     L.pdfxc_set_batch.argtypes = [_vp, i32, _vp]
     L.pdfxc_build_vxc_batched.argtypes = [_vp, i32, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_set_rho_uks.argtypes = [_vp, i32, _vp]
+    L.pdfxc_plan_grid.argtypes = [ctypes.POINTER(Options), i32, _vp, i32, _vp, _vp, _vp, _vp, _vp, i64, _vp,
+                                  ctypes.POINTER(GridPlan)]
+    L.pdfxc_pack_upper.argtypes = [_vp, i32, _vp, _vp]
+    L.pdfxc_unpack_upper.argtypes = [_vp, i32, _vp, _vp]
     for name in EXPORTS:
         if name not in ("pdfxc_last_error", "pdfxc_destroy", "pdfxc_default_options"):
             getattr(L, name).restype = i32
@@ -129,6 +140,38 @@ def partition_blocks(cost, nparts):
     return bounds
 
 
+def make_options(precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16, workspace_bytes=0,
+                 split_terms=10):
+    L = load_library()
+    opt = Options()
+    L.pdfxc_default_options(ctypes.byref(opt))
+    opt.precision = PRECISION[precision]
+    opt.block_points = block_points
+    opt.ao_cutoff = ao_cutoff
+    opt.rho_cutoff = rho_cutoff
+    opt.workspace_bytes = workspace_bytes
+    opt.split_terms = split_terms
+    return opt
+
+
+def plan_grid(sh, xyzw, **options):
+    """The blocking and screening pdfxc_set_grid would do, planned on the host (no device):
+    returns a dict of pdfxc_grid_plan's fields, or raises RuntimeError with the status
+    (6 = unsupported: an INT8 group beyond its exact accumulation bound)."""
+    L = load_library()
+    opt = make_options(**options)
+    k = [np.ascontiguousarray(a) for a in (
+        sh.atom_xyz.astype(np.float64), sh.shell_atom.astype(np.int32), sh.shell_l.astype(np.int32),
+        sh.shell_nprim.astype(np.int32), sh.prim_exp.astype(np.float64), sh.prim_coef.astype(np.float64))]
+    xyzw = np.ascontiguousarray(xyzw, dtype=np.float64).reshape(-1, 4)
+    out = GridPlan()
+    st = L.pdfxc_plan_grid(ctypes.byref(opt), sh.natom, _ptr(k[0]), sh.nshell, _ptr(k[1]), _ptr(k[2]), _ptr(k[3]),
+                           _ptr(k[4]), _ptr(k[5]), len(xyzw), _ptr(xyzw), ctypes.byref(out))
+    if st != 0:
+        raise RuntimeError(f"pdfxc_plan_grid: status {st}")
+    return {name: getattr(out, name) for name, _ in GridPlan._fields_}
+
+
 class XcEngine:
     """One libpdfxc context on one GPU.
 
@@ -141,19 +184,13 @@ class XcEngine:
     def __init__(self, device=0, precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16,
                  workspace_bytes=0, split_terms=10):
         self.L = load_library()
-        opt = Options()
-        self.L.pdfxc_default_options(ctypes.byref(opt))
-        opt.precision = PRECISION[precision]
-        opt.block_points = block_points
-        opt.ao_cutoff = ao_cutoff
-        opt.rho_cutoff = rho_cutoff
-        opt.workspace_bytes = workspace_bytes
-        opt.split_terms = split_terms
+        opt = make_options(precision, block_points, ao_cutoff, rho_cutoff, workspace_bytes, split_terms)
         h = _vp()
         st = self.L.pdfxc_create(ctypes.byref(h), device, ctypes.byref(opt))
         if st != 0:
             raise RuntimeError(f"pdfxc_create failed with status {st}")
         self.h = h
+        self.device = device
         self.nao = 0
         self.npts = 0
 

@@ -87,6 +87,45 @@ def test_becke_vs_reference(water2):
     assert np.all(np.abs(w - water2["becke_w_final"]) <= 1e-13 * np.abs(water2["becke_w_single"]))
 
 
+def test_becke_equals_oracle_bit_for_bit():
+    """The device's Becke weights (compiled without fused multiply-adds) equal the CPU
+    restatement's bit for bit, so both sides keep the same points under the 1e-16 weight screen;
+    a 30-atom chain on a USER 40 x 110 grid, table form."""
+    from oracle import oracle
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    syms, xyz = systems.peptide_chain(30, seed=5)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+    P, W, A = grids.molecular_grid(xyz, sh.atom_z, nrad=40, nang=110, radial="GC", mapping="TA", pruning=True)
+    brad = np.array([grids.BECKE_RADIUS[int(z)] for z in sh.atom_z])
+    eng = XcEngine()
+    eng.set_system(sh)
+    w = eng.becke_weights(P, A, W, brad)
+    ref = W * oracle.becke(xyz, brad, P, A)
+    assert np.array_equal(w, ref), np.abs(w - ref).max()
+    eng.close()
+
+
+def test_becke_dummy_atom_vs_reference():
+    """A dummy atom (atomic number 0) is left out of the partition products, as the reference's
+    Ps_uij does (src/libpdf/DfGenerateGrid.cpp:2056); equal to the oracle bit for bit."""
+    from oracle import oracle
+    from proteindf_b200 import basis
+    from proteindf_b200.xc import XcEngine
+    fx = golden("ref_becke_ghost_water2.npz")
+    syms = [str(s) for s in fx["symbols"]]
+    sh = basis.ShellTable(syms, fx["xyz"], basis.load_basis("cc-pVDZ"))
+    assert sh.atom_z[-1] == 0
+    eng = XcEngine()
+    eng.set_system(sh)
+    brad = fx["radii"][:, 1]
+    w = eng.becke_weights(fx["points"], fx["atom"], fx["w_single"], brad)
+    assert np.all(np.abs(w - fx["w_final"]) <= 1e-13 * np.abs(fx["w_single"]))
+    ref = fx["w_single"] * oracle.becke(fx["xyz"], brad, fx["points"], fx["atom"], ghost=sh.atom_z == 0)
+    assert np.array_equal(w, ref)
+    eng.close()
+
+
 def test_incremental_density_update(water2):
     """xc-update = yes: a build on dP adds rho(dP) to the stored rho(P_prev)."""
     eng = engine(water2)

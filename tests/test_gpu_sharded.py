@@ -89,6 +89,17 @@ def test_nccl_front_end_world_one(water2):
         exc, nel = sh.build_vxc_device("B3LYP", PA, V)
         assert abs(exc - water2["B3LYP_exc"][0]) < 1e-8
         assert (V.cpu().numpy() - water2["B3LYP_vxc"]).__abs__().max() < 1e-7
+        # the host-array builds reduce through a CUDA tensor on the NCCL group
+        exc, nel, Vh = sh.build_vxc("B3LYP", water2["PA"])
+        assert abs(exc - water2["B3LYP_exc"][0]) < 1e-8
+        assert np.abs(Vh - water2["B3LYP_vxc"]).max() < 1e-7
+        uks = golden("ref_uks_water2.npz")
+        eu, na, nb, FA, FB = sh.build_vxc_uks("BLYP", uks["PA"], uks["PB"])
+        assert abs(eu - uks["BLYP_exc"][0]) < 1e-8
+        assert np.abs(FA - uks["BLYP_vxc_a"]).max() < 1e-7 and np.abs(FB - uks["BLYP_vxc_b"]).max() < 1e-7
+        go, gw, eg = sh.xc_gradient("SVWN", water2["PA"])
+        go1, _, eg1 = eng.xc_gradient("SVWN", water2["PA"])
+        assert gw is None and np.array_equal(go, go1) and eg == eg1
         eng.close()
     finally:
         dist.destroy_process_group()

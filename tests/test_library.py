@@ -47,3 +47,46 @@ def test_create_reports_missing_device():
     L = xc.load_library()
     h = ctypes.c_void_p()
     assert L.pdfxc_create(ctypes.byref(h), 0, None) == 2  # PDFXC_ERR_CUDA
+
+
+def test_plan_grid_matches_between_precisions_on_host():
+    """The host planner (no device): blocks of 128 points on the FP64 path, groups of up to
+    four blocks on the INT8 path, the same screened-basis statistics the contexts report."""
+    from conftest import golden, shell_table
+    fx = golden("ref_water2.npz")
+    sh = shell_table(fx)
+    g = fx["grid"][:, :4]
+    f = xc.plan_grid(sh, g, precision="fp64")
+    m = xc.plan_grid(sh, g, precision="mixed", split_terms=10)
+    assert f["nblocks"] == f["ngroups"] and f["npts_padded"] == 128 * f["nblocks"]
+    assert m["ngroups"] <= m["nblocks"] and m["nblocks"] >= len(g) // 128
+    assert 0 < f["max_nb"] <= sh.nao and 0 < m["max_nb"] <= sh.nao
+    assert f["contraction_flops"] > 0 and f["workspace_bytes"] > 0
+
+
+def test_plan_grid_refuses_int8_group_beyond_exact_bound():
+    """A group that screens in more AOs than the INT8 contraction accumulates exactly
+    (33,280: four digit products of 127^2 per K index within int32) is refused with
+    PDFXC_ERR_UNSUPPORTED on the mixed path and accepted on the FP64 path."""
+    import numpy as np
+
+    class Synthetic:  # 6,700 d shells on one atom: 33,500 AOs, every one of them screened in
+        natom, nshell = 1, 6700
+        atom_xyz = np.zeros((1, 3))
+        shell_atom = np.zeros(6700, np.int32)
+        shell_l = np.full(6700, 2, np.int32)
+        shell_nprim = np.ones(6700, np.int32)
+        prim_exp = np.full(6700, 0.5)
+        prim_coef = np.ones(6700)
+    xyzw = np.zeros((16, 4))
+    xyzw[:, 0] = np.linspace(0.1, 0.5, 16)
+    xyzw[:, 3] = 1.0
+    f = xc.plan_grid(Synthetic, xyzw, precision="fp64")
+    assert f["max_nb"] == 33500
+    with pytest.raises(RuntimeError, match="status 6"):
+        xc.plan_grid(Synthetic, xyzw, precision="mixed", split_terms=10)
+    # just inside the bound: 6,656 shells = 33,280 AOs
+    Synthetic.nshell = 6656
+    for k in ("shell_atom", "shell_l", "shell_nprim", "prim_exp", "prim_coef"):
+        setattr(Synthetic, k, getattr(Synthetic, k)[:6656])
+    assert xc.plan_grid(Synthetic, xyzw, precision="mixed", split_terms=10)["max_nb"] == 33280

@@ -60,6 +60,101 @@ def test_block_sharded_build_allreduce(tmp_path):
     assert abs(s[n * n + 1] - fx["B3LYP_nelec_alpha"][0]) < 1e-10
 
 
+class _OracleRankEngine:
+    """The XcEngine interface that ShardedXcEngine drives, with the CPU oracle standing in for
+    the rank's GPU build: blocks of 128 rows in input order, each rank builds its block range."""
+
+    def __init__(self, sh):
+        self.sh = sh
+
+    def set_system(self, sh):
+        self.sh = sh
+
+    def set_grid(self, xyzw, atom=None):
+        self.g, self.atom = np.asarray(xyzw)[:, :4], atom
+        self.blocks = np.array_split(np.arange(len(self.g)), (len(self.g) + 127) // 128)
+        self.rows = np.arange(len(self.g))
+
+    def block_costs(self):
+        return np.array([4.0 * self.sh.nao ** 2 * len(b) for b in self.blocks])
+
+    def set_block_range(self, lo, hi):
+        self.rows = np.concatenate(self.blocks[lo:hi])
+
+    def build_vxc(self, fn, PA, incremental=False):
+        from oracle import oracle
+        r = oracle.xc(fn, self.sh, self.g[self.rows], PA)
+        return r["exc"], r["nelec_alpha"], r["vxc"]
+
+    def build_vxc_uks(self, fn, PA, PB, incremental=False):
+        from oracle import oracle
+        r = oracle.xc_uks(fn, self.sh, self.g[self.rows], PA, PB)
+        return r["exc"], r["nelec_alpha"], r["nelec_beta"], r["vxc_a"], r["vxc_b"]
+
+    def xc_gradient(self, fn, PA, w_single=None, becke_radius=None, size_adjust=True):
+        from oracle import oracle
+        r = oracle.xc_grad(fn, self.sh, self.g[self.rows], self.atom[self.rows], PA)
+        return r["grad"], None, r["exc"]
+
+
+def _sharded_worker(rank, world, port, out_path):
+    import sys
+    sys.path.insert(0, os.path.abspath(os.path.join(os.path.dirname(__file__), "..")))
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import torch.distributed as dist
+    from conftest import golden, shell_table
+    from proteindf_b200.sharded import ShardedXcEngine
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    fx, uks = golden("ref_water2.npz"), golden("ref_uks_water2.npz")
+    sh = shell_table(fx)
+    eng = ShardedXcEngine(_OracleRankEngine(sh))
+    eng.set_grid(fx["grid"][:, :4], fx["grid"][:, 4].astype(np.int32))
+    e, n, V = eng.build_vxc("B3LYP", fx["PA"])
+    eu, na, nb, FA, FB = eng.build_vxc_uks("BLYP", uks["PA"], uks["PB"])
+    g, gw, eg = eng.xc_gradient("SVWN", fx["PA"])
+    assert gw is None
+    if rank == 0:
+        np.savez(out_path, e=e, n=n, V=V, eu=eu, na=na, nb=nb, FA=FA, FB=FB, g=g, eg=eg)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_engine_host_builds_two_ranks(tmp_path):
+    """ShardedXcEngine over two gloo ranks: the closed-shell build, the open-shell build and
+    the XC gradient on host arrays (the packed upper triangles and the scalars in one
+    all-reduce per build) equal the one-rank result."""
+    import torch.multiprocessing as mp
+    from conftest import golden, shell_table
+    from oracle import oracle
+    out = str(tmp_path / "sharded.npz")
+    mp.start_processes(_sharded_worker, args=(2, _free_port(), out), nprocs=2, join=True, start_method="spawn")
+    r = dict(np.load(out))
+    fx, uks = golden("ref_water2.npz"), golden("ref_uks_water2.npz")
+    sh = shell_table(fx)
+    g = fx["grid"]
+    assert abs(r["e"] - fx["B3LYP_exc"][0]) < 1e-12
+    assert abs(r["n"] - fx["B3LYP_nelec_alpha"][0]) < 1e-10
+    assert np.abs(r["V"] - fx["B3LYP_vxc"]).max() < 1e-12
+    assert abs(r["eu"] - uks["BLYP_exc"][0]) < 1e-12
+    assert abs(r["na"] - uks["BLYP_nelec_alpha"][0]) < 1e-10 and abs(r["nb"] - uks["BLYP_nelec_beta"][0]) < 1e-10
+    assert np.abs(r["FA"] - uks["BLYP_vxc_a"]).max() < 1e-12 and np.abs(r["FB"] - uks["BLYP_vxc_b"]).max() < 1e-12
+    full = oracle.xc_grad("SVWN", sh, g[:, :4], g[:, 4].astype(np.int32), fx["PA"])
+    assert np.abs(r["g"] - full["grad"]).max() < 1e-11
+    assert abs(r["eg"] - full["exc"]) < 1e-12
+
+
+def test_packed_upper_host_round_trip():
+    from proteindf_b200.sharded import _pack_host, _unpack_host
+    rng = np.random.default_rng(3)
+    for n in (1, 2, 7, 33):
+        A = rng.normal(size=(n, n))
+        S = A + A.T
+        p = _pack_host(S)
+        assert p.shape == (n * (n + 1) // 2,)
+        assert np.array_equal(_unpack_host(p, n), S)
+
+
 def test_partition_blocks_properties():
     from proteindf_b200.xc import partition_blocks
     rng = np.random.default_rng(0)

@@ -150,3 +150,32 @@ def test_oracle_density_at_points_vs_reference():
     rho = np.einsum("pi,ij,pj->p", phi, fx["P"], phi)
     assert np.all(np.abs(rho - fx["rho"]) <= 1e-12 * np.maximum(1.0, np.abs(fx["rho"])))
     assert np.all(fx["rho"][-20:] == 0.0)  # far points: every primitive beyond the a r^2 > 30 cut
+
+
+def test_oracle_becke_leaves_dummy_atoms_out():
+    """The reference's Becke product skips partner atoms of atomic number <= 0 (dummy atoms X,
+    src/libpdf/DfGenerateGrid.cpp:2056); a dummy atom between two waters changes the weights
+    by up to 0.47 if it is counted."""
+    fx = golden("ref_becke_ghost_water2.npz")
+    syms = [str(s) for s in fx["symbols"]]
+    ghost = np.array([s == "X" for s in syms])
+    brad = fx["radii"][:, 1]
+    ref = fx["w_final"] / fx["w_single"]
+    f = oracle.becke(fx["xyz"], brad, fx["points"], fx["atom"], ghost=ghost)
+    assert np.all(np.abs(f - ref) <= 1e-14 * np.maximum(np.abs(ref), 1e-300) + 1e-300)
+    f_all = oracle.becke(fx["xyz"], brad, fx["points"], fx["atom"])
+    assert np.abs(f_all - ref).max() > 0.1
+
+
+def test_host_grid_recipe_reproduces_water8_reference_grid():
+    """The (H2O)8 configuration's whole USER 75 x 302 Becke grid: the host recipe
+    (proteindf_b200.grids) with the oracle's Becke weights and the 1e-16 weight screen gives
+    the reference's point count and weight sum."""
+    from proteindf_b200 import basis, grids
+    fx = golden("ref_water8_user75x302.npz")
+    sh = basis.ShellTable([str(s) for s in fx["symbols"]], fx["xyz"], basis.load_basis("cc-pVDZ"))
+    P, W, A = grids.molecular_grid(fx["xyz"], sh.atom_z, **grids.PRESETS["USER-75x302"])
+    w = W * oracle.becke(fx["xyz"], fx["radii"][:, 1], P, A)
+    keep = np.abs(w) > 1e-16
+    assert abs(int(keep.sum()) - int(fx["grid_npts"])) <= 5
+    assert abs(w[keep].sum() - float(fx["grid_wsum"])) <= 1e-12 * float(fx["grid_wsum"])
