@@ -239,6 +239,27 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
                                const double* w_single, const double* becke_radius, int size_adjust,
                                double* grad_orbital, double* grad_weight, double* exc);
 
+/* The adjoint of the closed-shell XC energy, Exc(P, R), on the grid of pdfxc_set_grid (owner
+ * atoms required), FP64. dexc is the cotangent of Exc (the upstream derivative dL/dExc; 1 for
+ * the derivatives themselves); every output is scaled by it. Per workspace chunk the AO values,
+ * gradients and second derivatives are recomputed (none is kept from a build), X = P_sub phi,
+ * the functional's derivatives at every point, then
+ *   dexc_dP (host, n_ao x n_ao, overwritten): dL/dP for the total density P = 2 PA, each
+ *     element taken as independent -- sum over points of phi Z^T + Z phi^T with the density
+ *     adjoint Z = 0.5 w vrho phi + w (2 vgAA + vgAB) grad rho . grad phi, which is the
+ *     build's Vxc (SCF codes such as the reference feed Vxc = dExc/dP into F); dL/dPA is
+ *     2 dexc_dP;
+ *   grad_orbital, grad_weight (host, n_atom x 3, as pdfxc_xc_gradient): dL/dR, the AO-centre
+ *     term with the points moving with their atoms, and, with w_single, the derivative of the
+ *     Becke partition (at most 400 atoms; NULL w_single leaves the weight term out);
+ *   exc (may be NULL): Exc itself.
+ * Replaces the derivative side of DfCalcGridX (energyGradient / energyGradient_part,
+ * src/libpdf/DfCalcGridX.cpp:1073-1415); the dExc/dP output has no separate routine in the
+ * reference, whose calcXCIntegForFockAndEnergy returns the same matrix from the forward pass. */
+pdfxc_status pdfxc_xc_backward(pdfxc_ctx* ctx, int functional, const double* PA, double dexc,
+                               const double* w_single, const double* becke_radius, int size_adjust,
+                               double* dexc_dP, double* grad_orbital, double* grad_weight, double* exc);
+
 /* A batch of independent molecules in one context: every stage of a build runs
  * once for all of them (one launch per stage over the blocks of every molecule,
  * one captured CUDA graph per build). Each molecule's points are blocked and
@@ -335,6 +356,14 @@ pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out);
  * launched stage by stage instead, so that the per-stage times of
  * pdfxc_last_profile are filled in. */
 pdfxc_status pdfxc_set_profiling(pdfxc_ctx* ctx, int enable);
+
+/* The failure path of the library's bounded device waits, exercised without a fault: a kernel
+ * waits on an mbarrier that nothing completes, through the same bounded wait as the tensor-core
+ * contraction kernels, gives up after limit_seconds (0 < limit <= 10) and records its code in the
+ * context's device error word; the host reads it as the builds do and returns
+ * PDFXC_ERR_TIMEOUT, the expected result. The error word is cleared again, so the context stays
+ * usable. No counterpart in the reference (its waits are MPI and OpenMP barriers). */
+pdfxc_status pdfxc_selftest_wait(pdfxc_ctx* ctx, double limit_seconds);
 
 const char* pdfxc_last_error(const pdfxc_ctx* ctx);
 void pdfxc_destroy(pdfxc_ctx* ctx);

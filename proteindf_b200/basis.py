@@ -27,8 +27,16 @@ ELEMENT_Z = {"X": 0, "H": 1, "He": 2, "C": 6, "N": 7, "O": 8}
 
 
 def load_basis(name="cc-pVDZ"):
+    """A basis set of the reference's library (data/basis2, dumped to basis_sets.json).
+    "cc-pVDZ-noHp" is cc-pVDZ with the hydrogen p shell left out (3s2p1d on C/N/O, 2s on H):
+    the shell structure of 6-31G*, which the reference's library does not have."""
+    derived = name == "cc-pVDZ-noHp"
     with open(os.path.join(_DATA, "basis_sets.json")) as f:
-        return json.load(f)[name]
+        b = json.load(f)["cc-pVDZ" if derived else name]
+    if derived:
+        b = dict(b)
+        b["H"] = [sh for sh in b["H"] if sh["shell"] != "p"]
+    return b
 
 
 def _dfact(n):

@@ -166,18 +166,22 @@ __device__ __forceinline__ void warp_add3_by_owner(double* grad, int own, double
 
 // One CTA (128 threads, one per point) per block. fdens receives the energy density
 // f(rho) per point slot (0 below the density cut-off, for the weight term), blk_sum the
-// block's Exc and electron-count partials, grad the AO-centre term (natom x 3).
+// block's Exc and electron-count partials, grad the AO-centre term (natom x 3). Every
+// derivative is scaled by `seed`, the cotangent of Exc (1 for the plain gradient). With
+// want_z the adjoint of the density with respect to P replaces X in place:
+// Z_i = 0.5 a phi_i + c . grad phi_i (a = seed w vrho, c = seed w (2 vgAA + vgAB) grad rho),
+// so that phi Z^T + Z phi^T summed over the blocks is seed dExc/dP.
 template <bool GGA>
 __global__ void __launch_bounds__(BLOCK_PTS) k_grad_point(GridView g, const int* __restrict__ ao_atom,
                                                           const int* __restrict__ owner, int blk0, int fn,
-                                                          double rho_cut, const char* ws, double* fdens,
-                                                          double* blk_sum, double* grad) {
+                                                          double rho_cut, char* ws, double seed, int want_z,
+                                                          double* fdens, double* blk_sum, double* grad) {
     const int blk = blk0 + blockIdx.x;
     const BlockMeta m = g.meta[blk];
     const int p = threadIdx.x;
     const size_t plane = (size_t)m.nbp * BLOCK_PTS;
     const double* phi = reinterpret_cast<const double*>(ws + m.ws);
-    const double* X = phi + grad_phi_planes(GGA) * plane;
+    double* X = reinterpret_cast<double*>(ws + m.ws) + grad_phi_planes(GGA) * plane;
     double rho = 0.0, gx = 0.0, gy = 0.0, gz = 0.0;
     for (int r = 0; r < m.nb; ++r) {
         const size_t o = (size_t)r * BLOCK_PTS + p;
@@ -197,13 +201,13 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_grad_point(GridView g, const int*
         const double gam = GGA ? gx * gx + gy * gy + gz * gz : 0.0;
         const XcOut o = eval_functional(fn, rho, rho, gam, gam, gam);
         f = o.f;
-        a = w * o.va;
+        a = seed * w * o.va;
         if (GGA) {
-            const double cc = w * (2.0 * o.vgaa + o.vgab);
+            const double cc = seed * w * (2.0 * o.vgaa + o.vgab);
             cx = cc * gx, cy = cc * gy, cz = cc * gz;
         }
     }
-    fdens[gp] = f;
+    fdens[gp] = seed * f;
 
     // AO-centre term: the block's AO list is in shell order, so each atom's AOs form runs
     const int* aos = g.blk_aos + m.ao0;
@@ -230,6 +234,7 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_grad_point(GridView g, const int*
         }
         ax += Gx, ay += Gy, az += Gz;
         tx += Gx, ty += Gy, tz += Gz;
+        if (want_z) X[o] = 0.5 * a * phi[o] + (GGA ? cx * d1x + cy * d1y + cz * d1z : 0.0);
     }
     if (m.nb > 0) warp_add3(grad, cur, -4.0, ax, ay, az);
     warp_add3_by_owner(grad, owner[gp], 4.0, tx, ty, tz);
@@ -369,12 +374,17 @@ void launch_grad_x(const GridView& g, const double* P, int nao, int blk0, int nb
 }
 
 void launch_grad_point(const GridView& g, const int* ao_atom, const int* owner, int blk0, int nblk, int fn,
-                       double rho_cut, const char* ws, double* fdens, double* blk_sum, double* grad, cudaStream_t s) {
+                       double rho_cut, char* ws, double seed, bool want_z, double* fdens, double* blk_sum,
+                       double* grad, cudaStream_t s) {
     if (functional_is_gga(fn))
-        k_grad_point<true><<<nblk, BLOCK_PTS, 0, s>>>(g, ao_atom, owner, blk0, fn, rho_cut, ws, fdens, blk_sum, grad);
+        k_grad_point<true><<<nblk, BLOCK_PTS, 0, s>>>(g, ao_atom, owner, blk0, fn, rho_cut, ws, seed, want_z ? 1 : 0,
+                                                      fdens, blk_sum, grad);
     else
-        k_grad_point<false><<<nblk, BLOCK_PTS, 0, s>>>(g, ao_atom, owner, blk0, fn, rho_cut, ws, fdens, blk_sum, grad);
+        k_grad_point<false><<<nblk, BLOCK_PTS, 0, s>>>(g, ao_atom, owner, blk0, fn, rho_cut, ws, seed,
+                                                       want_z ? 1 : 0, fdens, blk_sum, grad);
 }
+
+int grad_z_plane(bool gga) { return grad_phi_planes(gga); }
 
 // Shared memory per CTA: 2 * natom * T doubles; 64 points per CTA while that fits
 // 200 KiB, else 32.

@@ -1268,6 +1268,20 @@ void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, boo
                                                              coef, blk_sum);
 }
 
+// The failure path of the bounded waits, exercised without a fault: one thread waits on an
+// mbarrier that nothing arrives on, through the same mbar_wait as the contraction kernels,
+// gives up after limit_ns and records code 8 in the device error word.
+__global__ void k_wait_selftest(int* err, uint64_t limit_ns) {
+    __shared__ uint64_t bar;
+    if (threadIdx.x == 0) {
+        umma::mbar_init(&bar, 1);
+        umma::mbar_init_fence();
+        if (!umma::mbar_wait(&bar, 0, err, limit_ns)) atomicExch(err, 8);
+    }
+}
+
+void launch_wait_selftest(int* err, uint64_t limit_ns, cudaStream_t s) { k_wait_selftest<<<1, 32, 0, s>>>(err, limit_ns); }
+
 void oz_p_digits(const double* P, int nao, const int* row_cols, int* e, uint32_t* words, cudaStream_t s) {
     k_p_digits<<<(nao + 7) / 8, 256, 0, s>>>(P, nao, row_cols, e, words);
 }

@@ -12,6 +12,7 @@
 #include <numeric>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "functional.cuh"
@@ -1161,6 +1162,66 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     ctx->last_profile.launches = launches;
 }
 
+// F += V for a host F from the device V (n2 elements): V goes through two pinned staging
+// buffers in pieces of at most 8 Mi elements, each piece added on the host by several threads
+// while the next one is copied.
+void accumulate_to_host(pdfxc_ctx* ctx, const double* d_V, double* F, size_t n2) {
+    constexpr size_t kPiece = size_t(8) << 20;
+    const size_t piece = std::min(kPiece, n2);
+    if (ctx->stage_elems < piece) {
+        if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
+        ctx->h_stage = nullptr;
+        ctx->stage_elems = 0;
+        if (cudaMallocHost(&ctx->h_stage, 2 * piece * sizeof(double)) != cudaSuccess) {
+            ctx->h_stage = nullptr;
+            throw std::bad_alloc();
+        }
+        ctx->stage_elems = piece;
+    }
+    cudaEvent_t ev[2];
+    PDFXC_CUDA(cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming));
+    if (cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaEventDestroy(ev[0]);
+        throw CudaError("cudaEventCreate");
+    }
+    auto add = [&](const double* src, double* dst, size_t n) {
+        const unsigned nt = n < (size_t(1) << 20) ? 1u : std::min(16u, std::max(1u, std::thread::hardware_concurrency()));
+        if (nt == 1) {
+            for (size_t i = 0; i < n; ++i) dst[i] += src[i];
+            return;
+        }
+        std::vector<std::thread> th;
+        const size_t per = (n + nt - 1) / nt;
+        for (unsigned t = 0; t < nt; ++t) {
+            const size_t a = t * per, b = std::min(n, a + per);
+            if (a < b) th.emplace_back([=]() {
+                for (size_t i = a; i < b; ++i) dst[i] += src[i];
+            });
+        }
+        for (auto& x : th) x.join();
+    };
+    try {
+        const size_t npieces = (n2 + piece - 1) / piece;
+        for (size_t k = 0; k <= npieces; ++k) {
+            if (k < npieces) {  // copy piece k while the host adds piece k - 1
+                const size_t off = k * piece, len = std::min(piece, n2 - off);
+                PDFXC_CUDA(cudaMemcpyAsync(ctx->h_stage + (k & 1) * piece, d_V + off, len * sizeof(double),
+                                           cudaMemcpyDeviceToHost, ctx->stream));
+                PDFXC_CUDA(cudaEventRecord(ev[k & 1], ctx->stream));
+            }
+            if (k >= 1) {
+                const size_t j = k - 1, off = j * piece, len = std::min(piece, n2 - off);
+                PDFXC_CUDA(cudaEventSynchronize(ev[j & 1]));
+                add(ctx->h_stage + (j & 1) * piece, F + off, len);
+            }
+        }
+    } catch (...) {
+        cudaEventDestroy(ev[0]), cudaEventDestroy(ev[1]);
+        throw;
+    }
+    cudaEventDestroy(ev[0]), cudaEventDestroy(ev[1]);
+}
+
 // After the stream has synchronised: the device error word (0 = no expired wait).
 int device_error(pdfxc_ctx* ctx) {
     int code = 0;
@@ -1335,9 +1396,7 @@ pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, i
         const size_t n2 = (size_t)ctx->nao * ctx->nao;
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, n2 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream));
         run_build(ctx, functional, ctx->d_P, incremental != 0);
-        std::vector<double> V(n2);
         double sc[2];
-        PDFXC_CUDA(cudaMemcpyAsync(V.data(), ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream));
         PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, ctx->stream));
         PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
         collect_profile(ctx);
@@ -1345,7 +1404,7 @@ pdfxc_status pdfxc_build_vxc(pdfxc_ctx* ctx, int functional, const double* PA, i
             ctx->err = "a bounded device wait expired in the tensor-core contraction (code " + std::to_string(code) + ")";
             return PDFXC_ERR_TIMEOUT;
         }
-        for (size_t i = 0; i < n2; ++i) F[i] += V[i];
+        accumulate_to_host(ctx, ctx->d_V, F, n2);
         if (exc) *exc = sc[0];
         if (nelec_alpha) *nelec_alpha = sc[1];
         ctx->rho_valid = true;
@@ -1511,10 +1570,7 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
         pdfxc::launch_finish(ctx->d_Vacc_b, ctx->d_V_b, nao, ctx->d_blk_sum_b + 2 * lo, nr, ctx->d_scalars_b, s);
         PDFXC_CUDA(cudaEventRecord(ctx->ev[1], s));
         PDFXC_CUDA(cudaGetLastError());
-        std::vector<double> Va(n2), Vb(n2);
         double sa[2], sb[2];
-        PDFXC_CUDA(cudaMemcpyAsync(Va.data(), ctx->d_V, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-        PDFXC_CUDA(cudaMemcpyAsync(Vb.data(), ctx->d_V_b, n2 * sizeof(double), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaMemcpyAsync(sa, ctx->d_scalars, sizeof(sa), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaMemcpyAsync(sb, ctx->d_scalars_b, sizeof(sb), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaStreamSynchronize(s));
@@ -1522,7 +1578,8 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
         p = pdfxc_profile{};
         PDFXC_CUDA(cudaEventElapsedTime(&p.total_ms, ctx->ev[0], ctx->ev[1]));
         p.launches = 6 * (int64_t)ctx->uplan.chunks.size() + 4;
-        for (size_t i = 0; i < n2; ++i) FA[i] += Va[i], FB[i] += Vb[i];
+        accumulate_to_host(ctx, ctx->d_V, FA, n2);
+        accumulate_to_host(ctx, ctx->d_V_b, FB, n2);
         if (exc) *exc = sa[0];
         if (nelec_alpha) *nelec_alpha = sa[1];
         if (nelec_beta) *nelec_beta = sb[0];
@@ -1581,28 +1638,37 @@ pdfxc_status pdfxc_set_rho_uks(pdfxc_ctx* ctx, int gga, const double* rho) {
     });
 }
 
-pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA, const double* w_single,
-                               const double* becke_radius, int size_adjust, double* grad_orbital, double* grad_weight,
-                               double* exc) {
+}  // extern "C"
+
+namespace {
+
+// The XC nuclear gradient (pdfxc_xc_gradient) and the adjoint of Exc (pdfxc_xc_backward): per
+// chunk phi, grad phi and the second derivatives are recomputed (k_ao_grad), X = P_sub phi
+// (k_gemm_x), then the functional and the AO-centre term per point (k_grad_point); with
+// dexc_dP, the density adjoint Z replaces X and Vacc += phi Z^T (k_gemm_v), then
+// dexc_dP = Vacc + Vacc^T. Every derivative is scaled by `seed`.
+pdfxc_status xc_derivatives(pdfxc_ctx* ctx, const char* name, int functional, const double* PA,
+                            const double* w_single, const double* becke_radius, int size_adjust, double seed,
+                            double* grad_orbital, double* grad_weight, double* dexc_dP, double* exc) {
     return guarded(ctx, [&]() -> pdfxc_status {
         if (ctx->nblk == 0) {
-            ctx->err = "pdfxc_xc_gradient: call pdfxc_set_system and pdfxc_set_grid first";
+            ctx->err = std::string(name) + ": call pdfxc_set_system and pdfxc_set_grid first";
             return PDFXC_ERR_STATE;
         }
         if (ctx->h_owner.empty()) {
-            ctx->err = "pdfxc_xc_gradient: the grid was set without owner atoms (pass atom to pdfxc_set_grid)";
+            ctx->err = std::string(name) + ": the grid was set without owner atoms (pass atom to pdfxc_set_grid)";
             return PDFXC_ERR_STATE;
         }
         if (functional < PDFXC_SVWN || functional > PDFXC_PBE || !PA || !grad_orbital) {
-            ctx->err = "pdfxc_xc_gradient: unknown functional or null pointer";
+            ctx->err = std::string(name) + ": unknown functional or null pointer";
             return PDFXC_ERR_ARG;
         }
         if (w_single && (!becke_radius || !grad_weight)) {
-            ctx->err = "pdfxc_xc_gradient: the weight term needs becke_radius and grad_weight";
+            ctx->err = std::string(name) + ": the weight term needs becke_radius and grad_weight";
             return PDFXC_ERR_ARG;
         }
         if (w_single && ctx->natom > pdfxc::grad_weight_max_atoms()) {
-            ctx->err = "pdfxc_xc_gradient: the weight term supports at most " +
+            ctx->err = std::string(name) + ": the weight term supports at most " +
                        std::to_string(pdfxc::grad_weight_max_atoms()) + " atoms";
             return PDFXC_ERR_UNSUPPORTED;
         }
@@ -1623,6 +1689,7 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         if (!ctx->d_fdens) dev_alloc(&ctx->d_fdens, nslots);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_grad, 0, sizeof(double) * 6 * natom, s));
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, sizeof(double) * nao * nao, cudaMemcpyHostToDevice, s));
+        if (dexc_dP) memset_async(ctx->d_Vacc, sizeof(double) * (size_t)nao * nao, s);
         pdfxc::GridView gv = grid_view(ctx);
         gv.meta = ctx->gplan.d_meta;
         const pdfxc::BasisView bv = basis_view(ctx);
@@ -1633,7 +1700,9 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
             pdfxc::launch_ao_grad(bv, gv, b0, n, gga, ws, s);
             pdfxc::launch_grad_x(gv, ctx->d_P, nao, b0, n, ch.max_nbp, gga, ws, s);
             pdfxc::launch_grad_point(gv, ctx->d_ao_atom, ctx->d_owner, b0, n, functional, ctx->opt.rho_cutoff, ws,
-                                     ctx->d_fdens, ctx->d_blk_sum, ctx->d_grad, s);
+                                     seed, dexc_dP != nullptr, ctx->d_fdens, ctx->d_blk_sum, ctx->d_grad, s);
+            if (dexc_dP)
+                pdfxc::launch_gemm_v_plane(gv, b0, n, ch.max_nbp, pdfxc::grad_z_plane(gga), ws, ctx->d_Vacc, nao, s);
             PDFXC_CUDA(cudaGetLastError());
         }
         pdfxc::launch_block_sums(ctx->d_blk_sum + 2 * (size_t)ctx->blk_lo, ctx->blk_hi - ctx->blk_lo, ctx->d_scalars, s);
@@ -1658,6 +1727,12 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         }
         std::vector<double> g(6 * (size_t)natom);
         double sc[2];
+        if (dexc_dP) {
+            pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum + 2 * (size_t)ctx->blk_lo,
+                                 ctx->blk_hi - ctx->blk_lo, ctx->d_scalars, s);
+            PDFXC_LAUNCHED("dExc/dP symmetrisation");
+            PDFXC_CUDA(cudaMemcpyAsync(dexc_dP, ctx->d_V, sizeof(double) * (size_t)nao * nao, cudaMemcpyDeviceToHost, s));
+        }
         PDFXC_CUDA(cudaMemcpyAsync(g.data(), ctx->d_grad, sizeof(double) * g.size(), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaMemcpyAsync(sc, ctx->d_scalars, sizeof(sc), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaStreamSynchronize(s));
@@ -1667,6 +1742,29 @@ pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA,
         return PDFXC_OK;
     });
 }
+
+}  // namespace
+
+extern "C" {
+
+pdfxc_status pdfxc_xc_gradient(pdfxc_ctx* ctx, int functional, const double* PA, const double* w_single,
+                               const double* becke_radius, int size_adjust, double* grad_orbital, double* grad_weight,
+                               double* exc) {
+    return xc_derivatives(ctx, "pdfxc_xc_gradient", functional, PA, w_single, becke_radius, size_adjust, 1.0,
+                          grad_orbital, grad_weight, nullptr, exc);
+}
+
+pdfxc_status pdfxc_xc_backward(pdfxc_ctx* ctx, int functional, const double* PA, double dexc,
+                               const double* w_single, const double* becke_radius, int size_adjust,
+                               double* dexc_dP, double* grad_orbital, double* grad_weight, double* exc) {
+    if (ctx && !dexc_dP) {
+        ctx->err = "pdfxc_xc_backward: null dexc_dP";
+        return PDFXC_ERR_ARG;
+    }
+    return xc_derivatives(ctx, "pdfxc_xc_backward", functional, PA, w_single, becke_radius, size_adjust, dexc,
+                          grad_orbital, grad_weight, dexc_dP, exc);
+}
+
 
 pdfxc_status pdfxc_set_batch(pdfxc_ctx* ctx, int nmol, const pdfxc_mol* mols) {
     if (!ctx) return PDFXC_ERR_ARG;
@@ -1920,6 +2018,27 @@ pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out) {
     return PDFXC_OK;
 }
 
+pdfxc_status pdfxc_selftest_wait(pdfxc_ctx* ctx, double limit_seconds) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        if (!(limit_seconds > 0.0) || limit_seconds > 10.0) {
+            ctx->err = "pdfxc_selftest_wait: the limit must lie in (0, 10] seconds";
+            return PDFXC_ERR_ARG;
+        }
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        pdfxc::launch_wait_selftest(ctx->d_err, (uint64_t)(limit_seconds * 1e9), ctx->stream);
+        PDFXC_LAUNCHED("k_wait_selftest");
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        const int code = device_error(ctx);
+        PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        if (code) {
+            ctx->err = "a bounded device wait expired (self test, code " + std::to_string(code) + ")";
+            return PDFXC_ERR_TIMEOUT;
+        }
+        return PDFXC_OK;
+    });
+}
+
 const char* pdfxc_last_error(const pdfxc_ctx* ctx) { return ctx ? ctx->err.c_str() : "null context"; }
 
 void pdfxc_destroy(pdfxc_ctx* ctx) {
@@ -1937,6 +2056,7 @@ void pdfxc_destroy(pdfxc_ctx* ctx) {
     for (auto& e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto& e : ctx->stage_ev) cudaEventDestroy(e);
+    if (ctx->h_stage) cudaFreeHost(ctx->h_stage);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
 }

@@ -143,6 +143,8 @@ struct pdfxc_ctx {
     int* d_row_cols = nullptr;      // batch: per AO row its molecule's columns [c0, c1) (2 ints)
     bool rho_valid = false;
     pdfxc_ctx* dens = nullptr;  // pdfxc_density: FP64 context over the requested points (same system)
+    double* h_stage = nullptr;  // pinned host staging of Vxc for the host-array builds (2 x stage_elems)
+    size_t stage_elems = 0;
     int* d_ghost = nullptr;       // [natom] dummy atoms (atomic number <= 0 given to set_system), or null
     int* d_nbr_idx = nullptr;     // Stratmann-Scuseria weights: per atom the other atoms by distance
     double* d_nbr_dist = nullptr;
@@ -236,8 +238,12 @@ int grad_workspace_planes(bool gga);  // [nbp][BLOCK_PTS] double planes per bloc
 void launch_ao_grad(const BasisView& b, const GridView& g, int blk0, int nblk, bool gga, char* ws, cudaStream_t s);
 void launch_grad_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp, bool gga, char* ws,
                    cudaStream_t s);
+// seed: the cotangent of Exc that scales every derivative; want_z: the density adjoint
+// Z = 0.5 a phi + c . grad phi replaces X (plane grad_z_plane) for the dExc/dP contraction
 void launch_grad_point(const GridView& g, const int* ao_atom, const int* owner, int blk0, int nblk, int fn,
-                       double rho_cut, const char* ws, double* fdens, double* blk_sum, double* grad, cudaStream_t s);
+                       double rho_cut, char* ws, double seed, bool want_z, double* fdens, double* blk_sum,
+                       double* grad, cudaStream_t s);
+int grad_z_plane(bool gga);
 int grad_weight_max_atoms();
 void launch_grad_weight(const double* atom_xyz, int natom, const double* inv, const double* adj, int64_t nslots,
                         const double* px, const double* py, const double* pz, const int* owner, const double* wsingle,
@@ -383,6 +389,8 @@ void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub
 void mixed_functional(const MixedArgs& a, cudaStream_t s);  // functional, Z packing
 void mixed_vxc(const MixedArgs& a, cudaStream_t s);         // Vacc += phi Z^T
 size_t umma_smem_bytes(int nterms);
+// a bounded wait on an mbarrier nothing completes; records code 8 in *err after limit_ns
+void launch_wait_selftest(int* err, uint64_t limit_ns, cudaStream_t s);
 // the same four stages with INT8 fixed-point slices (split_terms == 10)
 // once per build; row_cols (batch, may be null): each row's molecule's columns, the only ones read
 void oz_p_digits(const double* P, int nao, const int* row_cols, int* e, uint32_t* words, cudaStream_t s);

@@ -89,15 +89,16 @@ __device__ __forceinline__ uint64_t globaltimer_ns() {
 }
 
 // Bounded wait: gives up (returns false, and the caller records an error)
-// after about one second, or at once when another CTA has already recorded
-// an error in *err.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const int* err) {
+// after limit_ns (about one second by default), or at once when another CTA has
+// already recorded an error in *err.
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, const int* err,
+                                          uint64_t limit_ns = 1000000000ull) {
     const uint64_t t0 = globaltimer_ns();
     for (uint32_t i = 0; i < WAIT_LIMIT; ++i) {
         if (mbar_try_wait(bar, parity)) return true;
         if ((i & 255) == 255) {
             if (*reinterpret_cast<const volatile int*>(err) != 0) return false;
-            if (globaltimer_ns() - t0 > 1000000000ull) return false;
+            if (globaltimer_ns() - t0 > limit_ns) return false;
         }
     }
     return false;

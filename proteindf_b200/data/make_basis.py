@@ -43,7 +43,8 @@ def parse_basis2(path, name, elements):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/data/basis2"
+    ref = os.environ.get("PDFXC_REFERENCE", "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ref, "data", "basis2")
     here = os.path.dirname(os.path.abspath(__file__))
     data = {"cc-pVDZ": parse_basis2(src, "cc-pVDZ", ["H", "C", "N", "O"])}
     with open(os.path.join(here, "basis_sets.json"), "w") as f:

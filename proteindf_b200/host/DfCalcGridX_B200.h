@@ -24,7 +24,7 @@
 // and xc-update restarts keep working.
 //
 // Build: compile this file inside ProteinDF (it includes the reference's
-// headers) and link libpdfxc.so; see INTEGRATION.md.
+// headers) and link libpdfxc.so.
 #ifndef DFCALCGRIDX_B200_H
 #define DFCALCGRIDX_B200_H
 

@@ -12,7 +12,7 @@
 // atom order (the reference's OpenMP loop over atoms appends them in completion order).
 //
 // Build: compile this file inside ProteinDF (it includes the reference's headers) and link
-// libpdfxc.so; see INTEGRATION.md.
+// libpdfxc.so.
 #ifndef DFGENERATEGRID_B200_H
 #define DFGENERATEGRID_B200_H
 

@@ -24,6 +24,7 @@ EXPORTS = [
     "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
     "pdfxc_build_vxc_batched", "pdfxc_density", "pdfxc_generate_grid", "pdfxc_get_grid",
     "pdfxc_build_vxc_delta_device", "pdfxc_pack_upper", "pdfxc_unpack_upper", "pdfxc_plan_grid",
+    "pdfxc_xc_backward", "pdfxc_selftest_wait",
 ]
 
 
@@ -104,6 +105,8 @@ def load_library(path=LIB_PATH):
     L.pdfxc_build_vxc_noalloc.argtypes = [i32, i32, i32, _vp, i32, _vp, _vp, _vp, _vp, _vp, i32, i64, _vp, _vp, _vp,
                                           _vp, _vp]
     L.pdfxc_xc_gradient.argtypes = [_vp, i32, _vp, _vp, _vp, i32, _vp, _vp, _vp]
+    L.pdfxc_selftest_wait.argtypes = [_vp, f64]
+    L.pdfxc_xc_backward.argtypes = [_vp, i32, _vp, f64, _vp, _vp, i32, _vp, _vp, _vp, _vp]
     L.pdfxc_build_vxc_uks.argtypes = [_vp, i32, _vp, _vp, i32, _vp, _vp, _vp, _vp, _vp]
     L.pdfxc_get_rho_uks.argtypes = [_vp, i32, _vp]
     L.pdfxc_ss_weights.argtypes = [_vp, i64, _vp, _vp, _vp, _vp]
@@ -333,6 +336,27 @@ class XcEngine:
                                              _ptr(go), args[3], ctypes.byref(exc)), "pdfxc_xc_gradient")
         return go, gw, exc.value
 
+    def xc_backward(self, functional, PA, dexc=1.0, w_single=None, becke_radius=None, size_adjust=True):
+        """The adjoint of Exc(P, R) (pdfxc_xc_backward): returns (dexc_dP (n, n) -- dL/dP for the
+        total density P = 2 PA, equal to Vxc when dexc = 1 --, grad_orbital (natom, 3), grad_weight
+        (natom, 3) or None, exc), every derivative scaled by dexc."""
+        PA = np.ascontiguousarray(PA, dtype=np.float64)
+        dP = np.zeros((self.nao, self.nao))
+        go = np.zeros((self.natom, 3))
+        gw = None
+        args = [None, None, 0, None]
+        if w_single is not None:
+            ws = np.ascontiguousarray(w_single, dtype=np.float64)
+            br = np.ascontiguousarray(becke_radius, dtype=np.float64)
+            gw = np.zeros((self.natom, 3))
+            self._wkeep = (ws, br)
+            args = [_ptr(ws), _ptr(br), int(size_adjust), _ptr(gw)]
+        exc = ctypes.c_double()
+        self._check(self.L.pdfxc_xc_backward(self.h, FUNCTIONALS[functional], _ptr(PA), float(dexc), args[0], args[1],
+                                             args[2], _ptr(dP), _ptr(go), args[3], ctypes.byref(exc)),
+                    "pdfxc_xc_backward")
+        return dP, go, gw, exc.value
+
     def build_vxc_uks(self, functional, PA, PB, incremental=False, FA=None, FB=None):
         """Open-shell host build. Returns (exc, nelec_alpha, nelec_beta, FA, FB), FA += Vxc_A, FB += Vxc_B."""
         PA = np.ascontiguousarray(PA, dtype=np.float64)
@@ -418,6 +442,12 @@ class XcEngine:
         self._check(self.L.pdfxc_grid_stats(self.h, ctypes.byref(nb), ctypes.byref(npad), ctypes.byref(fl),
                                             ctypes.byref(mnb)), "pdfxc_grid_stats")
         return {"nblocks": nb.value, "npts_padded": npad.value, "contraction_flops": fl.value, "mean_nb": mnb.value}
+
+    def selftest_wait(self, limit_seconds=1e-3):
+        """Run the bounded-wait failure path (pdfxc_selftest_wait); returns (status, message)."""
+        st = self.L.pdfxc_selftest_wait(self.h, float(limit_seconds))
+        msg = self.L.pdfxc_last_error(self.h)
+        return st, (msg.decode() if msg else "")
 
     def set_profiling(self, enable):
         """Stage-by-stage launches (per-stage times) instead of CUDA graph replay."""

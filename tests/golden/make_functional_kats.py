@@ -42,7 +42,8 @@ def blocks(text):
 
 
 def main():
-    src = sys.argv[1] if len(sys.argv) > 1 else "/root/reference/src/unit_test"
+    ref = os.environ.get("PDFXC_REFERENCE", "/root/reference")
+    src = sys.argv[1] if len(sys.argv) > 1 else os.path.join(ref, "src", "unit_test")
     cases = []
     for comp, fname in FILES.items():
         text = strip_comments(open(os.path.join(src, fname)).read())

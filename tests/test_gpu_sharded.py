@@ -99,7 +99,8 @@ def test_nccl_front_end_world_one(water2):
         assert np.abs(FA - uks["BLYP_vxc_a"]).max() < 1e-7 and np.abs(FB - uks["BLYP_vxc_b"]).max() < 1e-7
         go, gw, eg = sh.xc_gradient("SVWN", water2["PA"])
         go1, _, eg1 = eng.xc_gradient("SVWN", water2["PA"])
-        assert gw is None and np.array_equal(go, go1) and eg == eg1
+        # two builds differ by the order of their FP64 atomic additions only
+        assert gw is None and np.abs(go - go1).max() <= 1e-13 * np.abs(go1).max() and abs(eg - eg1) <= 1e-12 * abs(eg1)
         eng.close()
     finally:
         dist.destroy_process_group()
