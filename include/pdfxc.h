@@ -60,7 +60,7 @@ typedef struct {
     double ao_cutoff;    /* drop a shell from a block when its value/gradient bound is below (default 1e-14) */
     double rho_cutoff;   /* xc-density-threshold: points with rho_A <= it are skipped (default 1e-16) */
     size_t workspace_bytes; /* device workspace budget for block intermediates (0 = default 4 GiB) */
-    int split_terms;     /* mixed path operand split: 10 (default) = four balanced base-255 INT8 digits
+    int split_terms;     /* mixed path operand split: 10 (default) = four balanced base-256 INT8 digits
                             per operand (about 31 bits), the 10 digit products of order i + j <= 5 on
                             the integer tensor cores; 3 or 6 = BF16 hi/mid(/lo) split with FP32
                             accumulation (about 1e-6 relative, for comparison only) */
@@ -304,8 +304,8 @@ pdfxc_status pdfxc_set_block_range(pdfxc_ctx* ctx, int64_t b_lo, int64_t b_hi);
  * context: what pdfxc_set_grid would build for these options, system and points
  * (same blocks, groups, screened shells and workspace chunks). Returns
  * PDFXC_ERR_UNSUPPORTED where pdfxc_set_grid would: a mixed-precision (INT8)
- * context takes at most 33,280 screened AOs per group, the bound up to which its
- * int32 accumulation is exact. No counterpart in the reference (it does not
+ * context takes at most 32,512 screened AOs per group, the bound up to which its
+ * int32 accumulation and the FP64 combination of its digit orders are exact. No counterpart in the reference (it does not
  * screen, src/libpdf/DfCalcGridX.cpp:655-665); tile and group shapes can be
  * compared with it before a context is made. */
 typedef struct {
@@ -372,7 +372,8 @@ void pdfxc_destroy(pdfxc_ctx* ctx);
  * in the reference; it exists for callers that cannot call cudaMalloc (their
  * device memory belongs to a pool or arena they do not control, or they run
  * where allocation is forbidden). Every operand is a device pointer the caller
- * owns: the shells as in pdfxc_set_system, npts grid rows (x, y, z, w), the
+ * owns: the shells as in pdfxc_set_system (each shell's primitives by ascending exponent,
+ * the reference's order), npts grid rows (x, y, z, w), the
  * n_ao x n_ao alpha density d_PA; d_V (n_ao x n_ao) is overwritten with Vxc
  * and d_exc_nelec[0..1] with Exc and sum_i w_i rho_A(r_i). The intermediates
  * live in a fixed 32 MiB __device__ array of the library, held by every GPU

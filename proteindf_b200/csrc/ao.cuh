@@ -34,13 +34,12 @@ template <bool GGA>
 __device__ __forceinline__ void shell_radial(const BasisView& bas, int s, double d2, double& S0, double& S1) {
     const int np = bas.sh_nprim[s], p0 = bas.sh_p0[s];
     S0 = 0.0, S1 = 0.0;
-    for (int k = 0; k < np; ++k) {
+    for (int k = 0; k < np; ++k) {  // exponents ascend within a shell: the rest are cut too
         const double al = bas.p_exp[p0 + k];
-        if (al * d2 <= 30.0) {
-            const double e = bas.p_coef[p0 + k] * exp(-al * d2);
-            S0 += e;
-            if (GGA) S1 += al * e;
-        }
+        if (al * d2 > 30.0) break;
+        const double e = bas.p_coef[p0 + k] * exp(-al * d2);
+        S0 += e;
+        if (GGA) S1 += al * e;
     }
 }
 
@@ -72,13 +71,12 @@ __device__ __forceinline__ void shell_radial_staged(const BasisView& bas, const 
         return;
     }
     S0 = 0.0, S1 = 0.0;
-    for (int k = 0; k < r.np; ++k) {
+    for (int k = 0; k < r.np; ++k) {  // exponents ascend within a shell: the rest are cut too
         const double al = r.alpha[k];
-        if (al * d2 <= 30.0) {
-            const double e = r.coef[k] * exp(-al * d2);
-            S0 += e;
-            if (GGA) S1 += al * e;
-        }
+        if (al * d2 > 30.0) break;
+        const double e = r.coef[k] * exp(-al * d2);
+        S0 += e;
+        if (GGA) S1 += al * e;
     }
 }
 

@@ -426,24 +426,26 @@ __global__ void __launch_bounds__(128, 1)
 // ===========================================================================
 // Fixed-point slices on the INT8 tensor cores (the split-integer product of
 // Ozaki, Ogita, Oishi and Rump, 2012, on an integer unit). Each operand row
-// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits in [-127, 127]:
-// v = 2^e (s_1 + s_2 / 255 + s_3 / 255^2 + s_4 / 255^3) / 127, the balanced base-255
-// expansion of v rounded to 127 255^3 units of 2^e: about 31 bits per operand. The
-// digit set is symmetric (digits(-v) = -digits(v)), so the dropped low-order products
-// have zero mean; a base-256 expansion, whose lower digits lie in [-128, 127], would
-// not. A_i B_j^T is an
-// exact integer product (|s_i s_j| <= 127^2, so K up to 2^15 stays inside int32),
-// accumulated exactly in int32 TMEM; the products with i + j <= 5 are kept, one
-// accumulator per order k = i + j, and the epilogue forms
-// 2^(eA + eB) sum_k D_k / (127^2 255^(k-2)) in FP64. The operands are sliced
-// from FP64 AO values (an FP32 copy of phi would cost ~3e-9 of Exc, the slices
-// cost ~1e-11), and the rho epilogue multiplies by FP64 AO values. FP32
-// accumulation, whose rounding on the tensor cores is toward zero, never occurs.
+// gets a power-of-two scale 2^e with |v| < 2^e and four signed digits in [-128, 127]:
+// v = 2^e (s_1 + s_2 / 256 + s_3 / 256^2 + s_4 / 256^3) / 127, the balanced base-256
+// expansion of v rounded to 127 256^3 units of 2^e: about 31 bits per operand. The
+// digits of q = rint(v 127 256^3 2^-e) are the bytes of q + 0x80808080 with their top
+// bits flipped, two integer operations per value. Their mean is -1/2, so the dropped
+// low-order products carry a bias, but it is about 1e-3 of their random part (a CPU
+// emulation of the chain12 quadrature: mean / rms of the error of X 0.002, the same as
+// for the symmetric base-255 digit set, which costs three divisions per value).
+// A_i B_j^T is an exact integer product (|s_i s_j| <= 128^2), accumulated exactly in
+// int32 TMEM; the products with i + j <= 5 are kept, one accumulator per order
+// k = i + j, and the epilogue forms 2^(eA + eB) sum_k D_k / (127^2 256^(k-2)) in FP64
+// (exact while K <= OZ_MAX_K). The operands are sliced from FP64 AO values (an FP32 copy
+// of phi would cost ~3e-9 of Exc, the slices cost ~1e-11), and the rho epilogue
+// multiplies by FP64 AO values. FP32 accumulation, whose rounding on the tensor cores is
+// toward zero, never occurs.
 //
 // AO values are never stored: the AO kernel keeps each shell's radial sums S0, S1
 // per point (16 bytes per shell and point instead of 32 per AO and point for phi
 // and its gradient) and every consumer forms the components from them.
-constexpr double kOzD1 = 127.0, kOzD = 255.0;
+constexpr double kOzD1 = 127.0, kOzD = 256.0;
 __device__ __forceinline__ double oz_weight(int k) {  // weight of order k = i + j
     double w = 1.0 / (kOzD1 * kOzD1);
     for (int i = 2; i < k; ++i) w /= kOzD;
@@ -465,20 +467,14 @@ __device__ __forceinline__ double oz_pow2(int e) {
     return e < -1022 ? 0.0 : __longlong_as_double((long long)(e + 1023) << 52);
 }
 
-// The digits of 16 values of one row at row scale 2^e, stored as four 16-byte digit-plane
-// pieces (plane i holds s_{i+1}): q = rint(v 127 255^3 2^-e) fits an int32 (|q| <= 127 255^3);
-// u = q + 127 (255^3 + 255^2 + 255 + 1) lies in [0, 255^4), and its base-255 digits d_i
-// (three unsigned divisions by 255) are s_i + 127. Adding 129 to every byte (mod 256, no
-// carries between bytes) turns d_i into the int8 s_i; a 4 x 4 byte transpose per four values
-// then gathers each digit plane. sc = 0 for an all-zero row.
-constexpr double kOzFull = 127.0 * 255.0 * 255.0 * 255.0;
-constexpr uint32_t kOzOff = 127u * (255u * 255u * 255u + 255u * 255u + 255u + 1u);
+// The digits of one value at row scale 2^e as one word (byte i = digit s_{4-i}):
+// q = rint(v 127 256^3 2^-e), |q| <= 127 2^24, is sum_i s_i 256^(4-i) with s_i in [-128, 127];
+// u = q + 0x80808080 (no carry out of 32 bits for that range) has the bytes s_i + 128, and
+// flipping every byte's top bit gives s_i in two's complement. sc = 0 for an all-zero row.
+constexpr double kOzFull = 127.0 * 256.0 * 256.0 * 256.0;
 __device__ __forceinline__ double oz_digit_scale(int e) { return e <= kOzZeroExp ? 0.0 : ldexp(kOzFull, -e); }
 __device__ __forceinline__ uint32_t oz_word(double v, double sc) {
-    const uint32_t u = (uint32_t)__double2int_rn(v * sc) + kOzOff;
-    const uint32_t u1 = u / 255u, u2 = u1 / 255u, u3 = u2 / 255u;
-    const uint32_t x = (u3 << 24) | ((u2 - 255u * u3) << 16) | ((u1 - 255u * u2) << 8) | (u - 255u * u1);
-    return ((x & 0x7F7F7F7Fu) + 0x01010101u) ^ ((x ^ 0x81818181u) & 0x80808080u);
+    return ((uint32_t)__double2int_rn(v * sc) + 0x80808080u) ^ 0x80808080u;
 }
 // Digit-plane layouts in HBM, in the order the contraction stages need them, so that a stage is
 // two bulk copies. Within a 64-K slab the canonical no-swizzle K-major core-matrix order of a
@@ -903,10 +899,10 @@ constexpr uint32_t oz_bar_off() {
 }
 
 // An item's int32 accumulators of orders 2..5 as one exact integer: with weights
-// w_k = 255^(5-k) w_5, sum_k d_k w_k = n w_5 with n = ((d2 255 + d3) 255 + d4) 255 + d5, whose
-// partial sums are integers below 2^53, so FP64 forms n exactly.
+// w_k = 256^(5-k) w_5, sum_k d_k w_k = n w_5 with n = ((d2 256 + d3) 256 + d4) 256 + d5, whose
+// partial sums are integers below 2^53 for K <= OZ_MAX_K, so FP64 forms n exactly.
 __device__ __forceinline__ double oz_combine(uint32_t d2, uint32_t d3, uint32_t d4, uint32_t d5) {
-    return fma(fma(fma((double)(int)d2, 255.0, (double)(int)d3), 255.0, (double)(int)d4), 255.0, (double)(int)d5);
+    return fma(fma(fma((double)(int)d2, 256.0, (double)(int)d3), 256.0, (double)(int)d4), 256.0, (double)(int)d5);
 }
 
 // The item's block (RHO) or group's first block (VXC) and tiles; false for an empty slot.

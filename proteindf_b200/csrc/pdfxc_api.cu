@@ -306,6 +306,16 @@ pdfxc_status set_host_system(pdfxc_ctx* ctx, int natom, const double* atom_xyz, 
     ctx->nao = ao;
     ctx->h_p_exp.assign(prim_exp, prim_exp + np);
     ctx->h_p_coef.assign(prim_coef, prim_coef + np);
+    // primitives by ascending exponent within each shell, the order the reference sums them in
+    // (TlOrbitalInfoObject::setCGTO, src/libpdf/TlOrbitalInfoObject.cpp:95); the kernels stop at
+    // the first primitive past the cut alpha r^2 > 30
+    for (int s = 0; s < nshell; ++s) {
+        const int p0 = ctx->h_sh_p0[s], n = shell_nprim[s];
+        std::vector<std::pair<double, double>> pr(n);
+        for (int k = 0; k < n; ++k) pr[k] = {ctx->h_p_exp[p0 + k], ctx->h_p_coef[p0 + k]};
+        std::stable_sort(pr.begin(), pr.end(), [](const auto& a, const auto& b) { return a.first < b.first; });
+        for (int k = 0; k < n; ++k) ctx->h_p_exp[p0 + k] = pr[k].first, ctx->h_p_coef[p0 + k] = pr[k].second;
+    }
     return PDFXC_OK;
 }
 
@@ -612,9 +622,9 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
             G.max_nb = std::max(G.max_nb, m.nb);
         }
     }
-    // The INT8 rho contraction runs over K = nbp screened AOs and accumulates exactly in int32:
-    // its order-5 accumulator sums four digit products of at most 127^2 per K index
-    // (kernels_mixed.cu), exact while 4 * 127^2 * K < 2^31.
+    // The INT8 rho contraction runs over K = nbp screened AOs and is exact up to OZ_MAX_K: its
+    // order-5 int32 accumulator sums four digit products of at most 128^2 per K index, and the
+    // FP64 combination of the four orders must stay below 2^53 (pdfxc_internal.cuh).
     if (mixed && ctx->opt.split_terms == 10) {
         for (int bb = 0; bb < nblk; ++bb)
             if (ctx->h_meta[bb].nbp > pdfxc::OZ_MAX_K)

@@ -315,8 +315,8 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 }
 
 // Intermediates of one block on the fixed-point (INT8 slice) path. Operands are
-// cut into OZ_SLICES signed digits in [-127, 127] with a power-of-two scale per row:
-// v = 2^e (s_1/127 + s_2/(127 254) + s_3/(127 254^2) + s_4/(127 254^3)); digit planes
+// cut into OZ_SLICES signed digits in [-128, 127] with a power-of-two scale per row:
+// v = 2^e (s_1 + s_2/256 + s_3/256^2 + s_4/256^3)/127; digit planes
 // are packed K-major in 64-byte slabs. AO values are not stored: the block keeps each
 // shell's radial sums S0, S1 at its points ([2][nsh][128] FP64) and every consumer forms
 // phi = A S0, grad phi = grad A S0 - 2 r A S1 from them. The Vxc contraction runs over
@@ -325,9 +325,11 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 // and lives only in the first block's region, after `total` (`total_lead` bytes in all).
 constexpr int OZ_SLICES = 4;
 // Largest K (screened AOs of a group, padded to 128) of the INT8 rho contraction: its order-5
-// int32 accumulator sums four digit products of at most 127^2 per K index, exact while
-// 4 * 127^2 * K <= 2^31 - 1 (K <= 33285).
-constexpr int OZ_MAX_K = 33280;
+// int32 accumulator sums four digit products of at most 128^2 per K index (exact in int32 while
+// 4 * 128^2 * K < 2^31, K < 32768), and the FP64 combination of the orders,
+// n = ((D2 256 + D3) 256 + D4) 256 + D5 with |D_k| <= (k - 1) 128^2 K, stays below 2^53 while
+// K < 32515.
+constexpr int OZ_MAX_K = 32512;
 struct OzLayout {
     size_t rad;                 // radial sums: S0 [nsh][128], then S1 [nsh][128]
     size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs

@@ -66,27 +66,29 @@ def test_plan_grid_matches_between_precisions_on_host():
 
 def test_plan_grid_refuses_int8_group_beyond_exact_bound():
     """A group that screens in more AOs than the INT8 contraction accumulates exactly
-    (33,280: four digit products of 127^2 per K index within int32) is refused with
+    (32,512: four digit products of 128^2 per K index within int32, their FP64 combination
+    below 2^53) is refused with
     PDFXC_ERR_UNSUPPORTED on the mixed path and accepted on the FP64 path."""
     import numpy as np
 
-    class Synthetic:  # 6,700 d shells on one atom: 33,500 AOs, every one of them screened in
-        natom, nshell = 1, 6700
+    class Synthetic:  # 6,600 d shells on one atom: 33,000 AOs, every one of them screened in
+        natom, nshell = 1, 6600
         atom_xyz = np.zeros((1, 3))
-        shell_atom = np.zeros(6700, np.int32)
-        shell_l = np.full(6700, 2, np.int32)
-        shell_nprim = np.ones(6700, np.int32)
-        prim_exp = np.full(6700, 0.5)
-        prim_coef = np.ones(6700)
+        shell_atom = np.zeros(6600, np.int32)
+        shell_l = np.full(6600, 2, np.int32)
+        shell_nprim = np.ones(6600, np.int32)
+        prim_exp = np.full(6600, 0.5)
+        prim_coef = np.ones(6600)
     xyzw = np.zeros((16, 4))
     xyzw[:, 0] = np.linspace(0.1, 0.5, 16)
     xyzw[:, 3] = 1.0
     f = xc.plan_grid(Synthetic, xyzw, precision="fp64")
-    assert f["max_nb"] == 33500
+    assert f["max_nb"] == 33000
     with pytest.raises(RuntimeError, match="status 6"):
         xc.plan_grid(Synthetic, xyzw, precision="mixed", split_terms=10)
-    # just inside the bound: 6,656 shells = 33,280 AOs
-    Synthetic.nshell = 6656
+    # just inside the bound: 6,502 d shells and two s shells = 32,512 AOs
+    Synthetic.nshell = 6504
     for k in ("shell_atom", "shell_l", "shell_nprim", "prim_exp", "prim_coef"):
-        setattr(Synthetic, k, getattr(Synthetic, k)[:6656])
-    assert xc.plan_grid(Synthetic, xyzw, precision="mixed", split_terms=10)["max_nb"] == 33280
+        setattr(Synthetic, k, getattr(Synthetic, k)[:6504].copy())
+    Synthetic.shell_l[:2] = 0
+    assert xc.plan_grid(Synthetic, xyzw, precision="mixed", split_terms=10)["max_nb"] == 32512
