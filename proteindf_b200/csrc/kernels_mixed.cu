@@ -905,22 +905,22 @@ __device__ __forceinline__ double oz_combine(uint32_t d2, uint32_t d3, uint32_t 
     return fma(fma(fma((double)(int)d2, 256.0, (double)(int)d3), 256.0, (double)(int)d4), 256.0, (double)(int)d5);
 }
 
-// The item's block (RHO) or group's first block (VXC) and tiles; false for an empty slot.
-template <int MODE>
-__device__ __forceinline__ bool oz_item(const GridView& g, int blk0, const int* grp, int it, int tiles_max, int& blk,
-                                        int& mt, int& nt) {
-    if (MODE == MODE_RHO) {
-        const int tn = 2 * tiles_max;
-        blk = blk0 + it / tn, mt = 0, nt = it % tn;
-        return nt < 2 * (g.meta[blk].nbp / umma::TILE_ROWS);
-    }
-    const int per = tiles_max * 2 * tiles_max;
-    blk = grp[it / per];
-    const int r = it % per;
-    mt = r / (2 * tiles_max), nt = r % (2 * tiles_max);
-    const int ntiles = g.meta[blk].nbp / umma::TILE_ROWS;
-    return mt < ntiles && nt < 2 * ntiles;
+// Work items of the persistent contraction kernels, one int2 each, in a list sorted by
+// decreasing cost (built with the grid, per chunk): RHO {block, N tile of 64 AOs}; VXC {the
+// group's first block, (M tile of 128 AOs) << 16 | N tile of 64 AOs}. x < 0 ends the list.
+__device__ __forceinline__ void oz_decode(int MODE_, int2 item, int& blk, int& mt, int& nt) {
+    blk = item.x;
+    mt = MODE_ == MODE_RHO ? 0 : item.y >> 16;
+    nt = item.y & 0xFFFF;
 }
+
+// The device-side scheduler: the copy warp claims the next item of the cost-sorted list with an
+// atomic counter (skipping items outside the launch's block range) and hands it to the MMA
+// warp and the epilogue groups through a ring of kOzRing shared-memory slots: ifull[slot]
+// (one arrival, the copy warp) and iempty[slot] (two arrivals: the MMA warp and the epilogue
+// group that takes the item). Entry q of the ring goes to epilogue group q % 2 and TMEM set
+// q % 2; the end of the list is written twice, so that both epilogue groups see it.
+constexpr int kOzRing = 4;
 
 // The 10 slice products A_i B_j^T with i + j <= 5 as six MMAs per K step. Product (i, j) goes to
 // the accumulator of order i + j, at TMEM columns 64 (i + j - 2); for one A plane the products
@@ -944,9 +944,10 @@ __device__ __forceinline__ constexpr int oz_mma_col(int t) { return (int)((0x323
 
 template <int MODE, bool GGA>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
-    k_oz(BasisView bas, GridView g, int blk0, const int* __restrict__ grp, char* ws, int* err, int nitems,
-         int tiles_max, double* rho_acc, double* Vacc, int nao) {
+    k_oz(BasisView bas, GridView g, int blk0, int nblk, const int2* __restrict__ items, int nitems, int* counter,
+         char* ws, int* err, double* rho_acc, double* Vacc, int nao) {
     extern __shared__ __align__(1024) uint8_t smem[];
+    __shared__ int2 s_item[kOzRing];
     // per epilogue group and alternate item of the group (a group writes one buffer while its
     // slower warps may still read the other): RHO the item's columns (row geometry, scale); VXC
     // the AO indices of the item's columns and rows and the columns' Z exponents
@@ -963,12 +964,15 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     uint64_t* empty = full + S;
     uint64_t* tfull = empty + S;
     uint64_t* tempty = tfull + 2;
-    uint32_t* tslot = reinterpret_cast<uint32_t*>(tempty + 2);
+    uint64_t* ifull = tempty + 2;
+    uint64_t* iempty = ifull + kOzRing;
+    uint32_t* tslot = reinterpret_cast<uint32_t*>(iempty + kOzRing);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     if (warp == 0) umma::tmem_alloc(tslot, 2 * OZ_TMEM_COLS);
     if (threadIdx.x == 32) {
         for (int st = 0; st < S; ++st) umma::mbar_init(&full[st], 1), umma::mbar_init(&empty[st], 1);
         for (int k = 0; k < 2; ++k) umma::mbar_init(&tfull[k], 1), umma::mbar_init(&tempty[k], OZ_EPI_WARPS / 2);
+        for (int k = 0; k < kOzRing; ++k) umma::mbar_init(&ifull[k], 1), umma::mbar_init(&iempty[k], 2);
         umma::mbar_init_fence();
     }
     umma::fence_before_sync();
@@ -978,12 +982,36 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     constexpr int kBlockSlabs = BLOCK_PTS / (int)umma::I8_SLAB_K;  // VXC: K slabs per block
 
     if (warp == 0) {
-        if (lane == 0) {  // copies
+        if (lane == 0) {  // the scheduler, then the item's copies
             uint32_t gj = 0;
             bool ok = true;
-            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            // entry q of the ring into its slot, once the slot's entry q - kOzRing is consumed
+            auto push = [&](int q, int2 item) {
+                const int slot = q % kOzRing;
+                if (q >= kOzRing && !umma::mbar_wait(&iempty[slot], ((q / kOzRing) - 1) & 1, err)) {
+                    atomicExch(err, 5);
+                    return false;
+                }
+                s_item[slot] = item;
+                umma::mbar_arrive(&ifull[slot]);  // release: the slot's item is visible to the consumers
+                return true;
+            };
+            for (int q = 0; ok; ++q) {
+                int2 item = make_int2(-1, 0);
+                for (;;) {  // the next item of the launch's block range
+                    const int it = atomicAdd(counter, 1);
+                    if (it >= nitems) break;
+                    item = __ldg(items + it);
+                    if (item.x >= blk0 && item.x < blk0 + nblk) break;
+                    item = make_int2(-1, 0);
+                }
+                if (!push(q, item)) break;
+                if (item.x < 0) {
+                    push(q + 1, item);
+                    break;
+                }
                 int blk, mt, nt;
-                if (!oz_item<MODE>(g, blk0, grp, it, tiles_max, blk, mt, nt)) continue;
+                oz_decode(MODE, item, blk, mt, nt);
                 const BlockMeta m = g.meta[blk];
                 const OzLayout L = oz_layout(m.nbp, m.nsh);
                 const char* base = ws + m.ws;
@@ -1029,9 +1057,17 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
             uint32_t gj = 0;
             int li = 0;
             bool ok = true;
-            for (int it = blockIdx.x; it < nitems && ok; it += gridDim.x) {
+            for (int q = 0; ok; ++q) {
+                const int slot = q % kOzRing;
+                if (!umma::mbar_wait(&ifull[slot], (q / kOzRing) & 1, err)) {
+                    atomicExch(err, 6);
+                    break;
+                }
+                const int2 item = s_item[slot];
+                umma::mbar_arrive(&iempty[slot]);
+                if (item.x < 0) break;
                 int blk, mt, nt;
-                if (!oz_item<MODE>(g, blk0, grp, it, tiles_max, blk, mt, nt)) continue;
+                oz_decode(MODE, item, blk, mt, nt);
                 const BlockMeta m = g.meta[blk];
                 const int nslabs = MODE == MODE_RHO ? m.nbp / (int)umma::I8_SLAB_K : m.gn * kBlockSlabs;
                 const int set = li & 1;
@@ -1086,17 +1122,22 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
         const double w5 = oz_weight(5);
         uint8_t* epi = smem + S * OZ_STAGE_BYTES;
         const uint32_t tq = tmem + (uint32_t)h * OZ_TMEM_COLS + ((uint32_t)(quarter * 32) << 16);
-        int li = 0;
-        for (int it = blockIdx.x; it < nitems; it += gridDim.x) {
-            int blk, mt, nt;
-            if (!oz_item<MODE>(g, blk0, grp, it, tiles_max, blk, mt, nt)) continue;
-            if ((li & 1) != h) {
-                ++li;
-                continue;
+        for (int q = h;; q += 2) {  // ring entries q = h, h + 2, ...: TMEM set h
+            const int slot = q % kOzRing;
+            bool got = umma::mbar_wait(&ifull[slot], (q / kOzRing) & 1, err);
+            got = umma::named_and(gbar, 256, got);
+            if (!got) {
+                if (gt == 0) atomicExch(err, 7);
+                break;
             }
-            ++li;
-            const int ph = ((li - 1) >> 1) & 1;  // tfull[h] parity of this item
-            const int sb = 2 * h + ph;            // the item's shared-memory buffer
+            const int2 item = s_item[slot];
+            umma::named_sync(gbar, 256);  // every thread of the group has read the slot
+            if (gt == 0) umma::mbar_arrive(&iempty[slot]);
+            if (item.x < 0) break;
+            int blk, mt, nt;
+            oz_decode(MODE, item, blk, mt, nt);
+            const int ph = (q >> 1) & 1;  // tfull[h] parity of this item
+            const int sb = 2 * h + ph;    // the item's shared-memory buffer
             const BlockMeta m = g.meta[blk];
             const OzLayout L = oz_layout(m.nbp, m.nsh);
             const char* base = ws + m.ws;
@@ -1250,7 +1291,7 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
 template <int MODE>
 size_t oz_smem_bytes() {
-    return (size_t)oz_bar_off<MODE>() + (2 * oz_stages<MODE>() + 4) * 8 + 16;
+    return (size_t)oz_bar_off<MODE>() + (2 * oz_stages<MODE>() + 4 + 2 * kOzRing) * 8 + 16;
 }
 
 void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
@@ -1303,17 +1344,17 @@ static int oz_grid(int nitems) {
 }
 
 void oz_rho(const MixedArgs& a, cudaStream_t s) {
-    const int tiles = a.max_nbp / umma::TILE_ROWS;
-    const int nitems = a.nblk * 2 * tiles;
     const size_t smem = oz_smem_bytes<MODE_RHO>();
     if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
-                                                                       tiles, a.rho_acc, a.Vacc, a.nao);
+        k_oz<MODE_RHO, true><<<oz_grid(a.n_rho), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, a.items_rho,
+                                                                        a.n_rho, a.counters, a.ws, a.err, a.rho_acc,
+                                                                        a.Vacc, a.nao);
     } else {
         cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
-                                                                        tiles, a.rho_acc, a.Vacc, a.nao);
+        k_oz<MODE_RHO, false><<<oz_grid(a.n_rho), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, a.items_rho,
+                                                                         a.n_rho, a.counters, a.ws, a.err, a.rho_acc,
+                                                                         a.Vacc, a.nao);
     }
 }
 
@@ -1332,12 +1373,11 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
 }
 
 void oz_vxc(const MixedArgs& a, cudaStream_t s) {
-    const int tiles = a.max_nbp / umma::TILE_ROWS;
-    const int nitems = a.ngrp * tiles * 2 * tiles;  // per group: M tiles of 128 AOs x N tiles of 64 AOs
     const size_t smem = oz_smem_bytes<MODE_VXC>();
     cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_oz<MODE_VXC, false><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.grp, a.ws, a.err, nitems,
-                                                                    tiles, a.rho_acc, a.Vacc, a.nao);
+    k_oz<MODE_VXC, false><<<oz_grid(a.n_vxc), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, a.items_vxc, a.n_vxc,
+                                                                     a.counters + 1, a.ws, a.err, a.rho_acc, a.Vacc,
+                                                                     a.nao);
 }
 
 size_t umma_smem_bytes(int nterms) {

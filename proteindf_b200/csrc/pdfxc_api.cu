@@ -203,6 +203,7 @@ void free_grid(pdfxc_ctx* c) {
     dev_free(c->d_meta), dev_free(c->d_blk_shells), dev_free(c->d_blk_shell_row), dev_free(c->d_blk_aos);
     dev_free(c->d_blk_row_info), dev_free(c->d_blk_row_geom);
     dev_free(c->d_seg_blk), dev_free(c->d_mol_sums), dev_free(c->d_grp);
+    dev_free(c->d_items), dev_free(c->d_counters);
     c->seg_blk.clear();
     c->h_grp.clear();
     dev_free(c->d_rho), dev_free(c->d_coef), dev_free(c->d_blk_sum), dev_free(c->d_rho_acc);
@@ -706,6 +707,34 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
     upload(&ctx->d_seg_blk, ctx->seg_blk, s);
     ctx->h_grp.assign(grp_blk.begin(), grp_blk.end() - 1);
     upload(&ctx->d_grp, ctx->h_grp, s);
+    if (mixed && ctx->opt.split_terms == 10) {
+        // the contraction work items of every chunk, largest first (longest-processing-time order
+        // for the device scheduler; a stable sort keeps a block's or group's items together)
+        std::vector<int2> items;
+        ctx->items_off_rho.clear(), ctx->items_n_rho.clear(), ctx->items_off_vxc.clear(), ctx->items_n_vxc.clear();
+        for (const Chunk& c : ctx->chunks) {
+            std::vector<std::pair<int, int2>> it;
+            for (int b = c.b0; b < c.b1; ++b)  // rho: (block, 64-AO output tile); cost ~ K = nbp
+                for (int nt = 0; nt < ctx->h_meta[b].nbp / 64; ++nt) it.push_back({ctx->h_meta[b].nbp, make_int2(b, nt)});
+            std::stable_sort(it.begin(), it.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+            ctx->items_off_rho.push_back((int)items.size());
+            ctx->items_n_rho.push_back((int)it.size());
+            for (const auto& x : it) items.push_back(x.second);
+            it.clear();
+            for (int b = c.b0; b < c.b1; ++b) {  // Vxc: (group, 128-AO row tile, 64-AO column tile); cost ~ K = points
+                const BlockMeta& m = ctx->h_meta[b];
+                if (m.lead != b) continue;
+                for (int mt = 0; mt < m.nbp / 128; ++mt)
+                    for (int nt = 0; nt < m.nbp / 64; ++nt) it.push_back({m.gn, make_int2(b, (mt << 16) | nt)});
+            }
+            std::stable_sort(it.begin(), it.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+            ctx->items_off_vxc.push_back((int)items.size());
+            ctx->items_n_vxc.push_back((int)it.size());
+            for (const auto& x : it) items.push_back(x.second);
+        }
+        upload(&ctx->d_items, items, s);
+        dev_alloc(&ctx->d_counters, 2 * ctx->chunks.size());
+    }
     dev_alloc(&ctx->d_rho, (size_t)nblk * BLOCK_PTS * 4);
     dev_alloc(&ctx->d_coef, (size_t)nblk * BLOCK_PTS * 4);
     dev_alloc(&ctx->d_blk_sum, (size_t)nblk * 2);
@@ -1091,6 +1120,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
     if (mixed) {
         memset_async(ctx->d_rho_acc, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s);
         PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+        if (ctx->d_counters) PDFXC_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int) * 2 * ctx->chunks.size(), s));
         if (ctx->opt.split_terms == 10) {
             pdfxc::oz_p_digits(d_PA, nao, ctx->d_row_cols, ctx->d_p_rowexp, ctx->d_p_words, s);
             ++launches;
@@ -1115,7 +1145,12 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
                            ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp,
-                           ctx->d_p_words};
+                           ctx->d_p_words, nullptr, 0, nullptr, 0, nullptr};
+        if (ctx->d_items) {
+            a.items_rho = ctx->d_items + ctx->items_off_rho[ci], a.n_rho = ctx->items_n_rho[ci];
+            a.items_vxc = ctx->d_items + ctx->items_off_vxc[ci], a.n_vxc = ctx->items_n_vxc[ci];
+            a.counters = ctx->d_counters + 2 * ci;
+        }
         const bool oz = ctx->opt.split_terms == 10;
         PDFXC_CUDA(cudaEventRecord(e[0], s));
         oz ? pdfxc::oz_prepare(a, s) : pdfxc::mixed_prepare(a, s);

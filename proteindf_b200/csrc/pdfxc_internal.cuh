@@ -120,6 +120,11 @@ struct pdfxc_ctx {
     int* d_seg_blk = nullptr;
     std::vector<int> h_grp;      // first block of every group, ascending (groups: consecutive blocks, one basis)
     int* d_grp = nullptr;
+    // INT8 path: per chunk the contraction work items (rho, then Vxc) sorted by decreasing cost,
+    // their offsets in d_items, and two work counters per chunk
+    std::vector<int> items_off_rho, items_n_rho, items_off_vxc, items_n_vxc;
+    int2* d_items = nullptr;
+    int* d_counters = nullptr;
     // batch of molecules (pdfxc_set_batch): AO offset and count of each molecule in the joint system
     std::vector<int> mol;        // AO offsets, size nmol + 1 (empty: a single molecule)
     double* d_mol_sums = nullptr;  // [2 * nmol]: Exc, electron count per molecule
@@ -385,6 +390,13 @@ struct MixedArgs {
     int ngrp;
     const int* p_rowexp;      // exponents of the rows of P (INT8 path)
     const uint32_t* p_words;  // the four digits of each element of P (INT8 path)
+    // INT8 path: the chunk's contraction work items, by decreasing cost (see kernels_mixed.cu),
+    // and the two work counters of the chunk's contraction launches (zero before the build)
+    const int2* items_rho;
+    int n_rho;
+    const int2* items_vxc;
+    int n_vxc;
+    int* counters;
 };
 void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
 void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue
