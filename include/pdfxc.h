@@ -64,6 +64,11 @@ typedef struct {
                             per operand (about 31 bits), the 10 digit products of order i + j <= 5 on
                             the integer tensor cores; 3 or 6 = BF16 hi/mid(/lo) split with FP32
                             accumulation (about 1e-6 relative, for comparison only) */
+    int group_blocks;    /* INT8 path: consecutive blocks per group sharing one screened basis, 1..4;
+                            0 (default) = the tuned choice for the workload class if pdfxc_autotune has
+                            made one in this process, else 4 */
+    int vxc_stages;      /* INT8 path: operand stages of the Vxc contraction, 2 or 3; 0 (default) =
+                            the tuned choice, else 3 */
 } pdfxc_options;
 
 typedef struct pdfxc_ctx pdfxc_ctx;
@@ -356,6 +361,29 @@ pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out);
  * launched stage by stage instead, so that the per-stage times of
  * pdfxc_last_profile are filled in. */
 pdfxc_status pdfxc_set_profiling(pdfxc_ctx* ctx, int enable);
+
+/* The autotuner. Times one closed-shell build of `functional` (device density d_PA, n_ao x n_ao;
+ * NULL = the context's staging matrix as it stands) for every candidate shape of the context's
+ * path -- on the INT8 path groups of 4, 2 or 1 blocks sharing one screened basis, times 3 or 2
+ * operand stages of the Vxc contraction; the FP64 path has none to choose -- on the context's own
+ * grid (re-blocked per candidate), a warm-up and the better of two timed builds each. Leaves the
+ * context on the fastest shape, and keeps it for the process under the workload's class
+ * (precision, operand split, batch or not, the AO and point counts to a factor of two): later
+ * contexts of that class whose options leave group_blocks / vxc_stages at 0 start from it. The
+ * stored densities of xc-update are dropped (call it before the first SCF build). out[0] is the
+ * winner, then the other candidates; *n_out = min(candidates, max_out). No counterpart in the
+ * reference. */
+typedef struct {
+    int group_blocks;
+    int vxc_stages;
+    int block_points;
+    float ms;           /* the build's device time with this shape */
+} pdfxc_tuning;
+pdfxc_status pdfxc_autotune(pdfxc_ctx* ctx, int functional, const double* d_PA, pdfxc_tuning* out, int max_out,
+                            int* n_out);
+/* The shapes the context's grid uses (group_blocks 1 and vxc_stages 0 on the FP64 path) and, in
+ * ms, the device time of its last build. */
+pdfxc_status pdfxc_get_tuning(pdfxc_ctx* ctx, pdfxc_tuning* out);
 
 /* The failure path of the library's bounded device waits, exercised without a fault: a kernel
  * waits on an mbarrier that nothing completes, through the same bounded wait as the tensor-core

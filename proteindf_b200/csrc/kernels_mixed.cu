@@ -893,9 +893,9 @@ template <int MODE>
 constexpr uint32_t oz_epi_bytes() {  // rho: 96 KiB of staged radial sums; Vxc: four 17 KiB tiles
     return MODE == MODE_RHO ? 4u * kOzRsCap * 2 * BLOCK_PTS * 8 : 4u * 128 * 17 * 8;
 }
-template <int MODE>
+template <int MODE, int S>
 constexpr uint32_t oz_bar_off() {
-    return oz_stages<MODE>() * OZ_STAGE_BYTES + oz_epi_bytes<MODE>();
+    return S * OZ_STAGE_BYTES + oz_epi_bytes<MODE>();
 }
 
 // An item's int32 accumulators of orders 2..5 as one exact integer: with weights
@@ -942,7 +942,7 @@ __device__ __forceinline__ constexpr int oz_mma_pair(int t) { return (int)((0x00
 __device__ __forceinline__ constexpr int oz_mma_wide(int t) { return (int)((0x010111u >> (4 * t)) & 15); }
 __device__ __forceinline__ constexpr int oz_mma_col(int t) { return (int)((0x323120u >> (4 * t)) & 15); }
 
-template <int MODE, bool GGA>
+template <int MODE, bool GGA, int S>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     k_oz(BasisView bas, GridView g, int blk0, int nblk, const int2* __restrict__ items, int nitems, int* counter,
          char* ws, int* err, double* rho_acc, double* Vacc, int nao) {
@@ -955,12 +955,11 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     __shared__ double s_cs[MODE == MODE_RHO ? 4 : 1][OZ_NT];
     __shared__ int s_acol[MODE == MODE_VXC ? 4 : 1][OZ_NT], s_ez[MODE == MODE_VXC ? 4 : 1][OZ_NT];
     __shared__ int s_arow[MODE == MODE_VXC ? 4 : 1][128];
-    constexpr int S = oz_stages<MODE>();
     __shared__ int s_abort;
     if (threadIdx.x == 0) s_abort = *reinterpret_cast<const volatile int*>(err);
     __syncthreads();
     if (s_abort) return;
-    uint64_t* full = reinterpret_cast<uint64_t*>(smem + oz_bar_off<MODE>());
+    uint64_t* full = reinterpret_cast<uint64_t*>(smem + oz_bar_off<MODE, S>());
     uint64_t* empty = full + S;
     uint64_t* tfull = empty + S;
     uint64_t* tempty = tfull + 2;
@@ -1289,9 +1288,9 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
 
 }  // namespace
 
-template <int MODE>
+template <int MODE, int S>
 size_t oz_smem_bytes() {
-    return (size_t)oz_bar_off<MODE>() + (2 * oz_stages<MODE>() + 4 + 2 * kOzRing) * 8 + 16;
+    return (size_t)oz_bar_off<MODE, S>() + (2 * S + 4 + 2 * kOzRing) * 8 + 16;
 }
 
 void launch_functional_points(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,
@@ -1343,19 +1342,20 @@ static int oz_grid(int nitems) {
     return std::max(1, std::min(nitems, nsm));
 }
 
+template <int MODE, bool GGA, int S>
+static void launch_oz(const MixedArgs& a, const int2* items, int nitems, int* counter, cudaStream_t s) {
+    const size_t smem = oz_smem_bytes<MODE, S>();
+    cudaFuncSetAttribute(k_oz<MODE, GGA, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_oz<MODE, GGA, S><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, items, nitems, counter,
+                                                                 a.ws, a.err, a.rho_acc, a.Vacc, a.nao);
+}
+
 void oz_rho(const MixedArgs& a, cudaStream_t s) {
-    const size_t smem = oz_smem_bytes<MODE_RHO>();
-    if (functional_is_gga(a.fn)) {
-        cudaFuncSetAttribute(k_oz<MODE_RHO, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, true><<<oz_grid(a.n_rho), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, a.items_rho,
-                                                                        a.n_rho, a.counters, a.ws, a.err, a.rho_acc,
-                                                                        a.Vacc, a.nao);
-    } else {
-        cudaFuncSetAttribute(k_oz<MODE_RHO, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        k_oz<MODE_RHO, false><<<oz_grid(a.n_rho), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, a.items_rho,
-                                                                         a.n_rho, a.counters, a.ws, a.err, a.rho_acc,
-                                                                         a.Vacc, a.nao);
-    }
+    constexpr int S = oz_stages<MODE_RHO>();
+    if (functional_is_gga(a.fn))
+        launch_oz<MODE_RHO, true, S>(a, a.items_rho, a.n_rho, a.counters, s);
+    else
+        launch_oz<MODE_RHO, false, S>(a, a.items_rho, a.n_rho, a.counters, s);
 }
 
 void oz_functional(const MixedArgs& a, cudaStream_t s) {
@@ -1372,12 +1372,12 @@ void oz_functional(const MixedArgs& a, cudaStream_t s) {
     }
 }
 
+// the Vxc contraction with 2 or 3 operand stages (MixedArgs::vxc_stages; 0 = 3)
 void oz_vxc(const MixedArgs& a, cudaStream_t s) {
-    const size_t smem = oz_smem_bytes<MODE_VXC>();
-    cudaFuncSetAttribute(k_oz<MODE_VXC, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_oz<MODE_VXC, false><<<oz_grid(a.n_vxc), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, a.items_vxc, a.n_vxc,
-                                                                     a.counters + 1, a.ws, a.err, a.rho_acc, a.Vacc,
-                                                                     a.nao);
+    if (a.vxc_stages == 2)
+        launch_oz<MODE_VXC, false, 2>(a, a.items_vxc, a.n_vxc, a.counters + 1, s);
+    else
+        launch_oz<MODE_VXC, false, 3>(a, a.items_vxc, a.n_vxc, a.counters + 1, s);
 }
 
 size_t umma_smem_bytes(int nterms) {

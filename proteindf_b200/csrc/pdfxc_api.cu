@@ -8,6 +8,8 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
 #include <numeric>
 #include <stdexcept>
@@ -233,6 +235,8 @@ void pdfxc_default_options(pdfxc_options* opt) {
     opt->rho_cutoff = 1e-16;
     opt->workspace_bytes = 0;
     opt->split_terms = 10;
+    opt->group_blocks = 0;
+    opt->vxc_stages = 0;
 }
 
 pdfxc_status pdfxc_create(pdfxc_ctx** out, int device, const pdfxc_options* opt) {
@@ -385,7 +389,39 @@ struct GridSegment {
 // groups of 4 x 128 points raise the contraction work by 18 % and cut the per-block
 // epilogue work (sum of nb^2) by 3.4x.
 int group_blocks(const pdfxc_ctx* ctx) {
-    return ctx->opt.precision == PDFXC_PRECISION_MIXED && ctx->opt.split_terms == 10 ? 4 : 1;
+    if (!(ctx->opt.precision == PDFXC_PRECISION_MIXED && ctx->opt.split_terms == 10)) return 1;
+    return ctx->tuned_group > 0 ? ctx->tuned_group : 4;
+}
+
+// Tile and group shapes chosen by pdfxc_autotune, kept for the process under the workload's class
+// (precision, operand split, batch or single molecule, and the AO and point counts to a factor of
+// two), so that later contexts of the same class start from them.
+struct TuneChoice {
+    int group_blocks, vxc_stages;
+};
+std::mutex g_tune_mutex;
+std::map<std::string, TuneChoice> g_tune_cache;
+
+std::string tune_class(const pdfxc_ctx* ctx, int64_t npts, size_t nseg) {
+    auto lg = [](double v) { return v > 1.0 ? (int)std::floor(std::log2(v)) : 0; };
+    return std::to_string(ctx->opt.precision) + "/" + std::to_string(ctx->opt.split_terms) + "/" +
+           std::to_string(nseg > 1) + "/" + std::to_string(lg(ctx->nao)) + "/" + std::to_string(lg((double)npts));
+}
+
+// The group size and Vxc stage count of a new grid: the options' explicit values, else the tuned
+// ones of the workload's class, else 4 and 3.
+void resolve_shapes(pdfxc_ctx* ctx, int64_t npts, size_t nseg) {
+    int g = ctx->opt.group_blocks, st = ctx->opt.vxc_stages;
+    if (g < 1 || g > 4 || (st != 2 && st != 3)) {
+        std::lock_guard<std::mutex> lock(g_tune_mutex);
+        const auto it = g_tune_cache.find(tune_class(ctx, npts, nseg));
+        if (it != g_tune_cache.end()) {
+            if (g < 1 || g > 4) g = it->second.group_blocks;
+            if (st != 2 && st != 3) st = it->second.vxc_stages;
+        }
+    }
+    ctx->tuned_group = (g >= 1 && g <= 4) ? g : 4;
+    ctx->tuned_stages = (st == 2 || st == 3) ? st : 3;
 }
 
 // Spatial blocks and basis screening, once per geometry: within each segment the points
@@ -673,6 +709,9 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
 void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom,
                 const std::vector<GridSegment>& segs) {
     free_grid(ctx);
+    resolve_shapes(ctx, npts, segs.size());
+    ctx->seg_pts.clear(), ctx->seg_sh.clear();
+    for (const GridSegment& sg : segs) ctx->seg_pts.push_back({sg.p0, sg.p1}), ctx->seg_sh.push_back({sg.sh0, sg.sh1});
     HostGrid G;
     plan_grid(ctx, npts, xyzw, atom, segs, G);
     const int nblk = G.nblk, ngrp = G.ngrp;
@@ -1145,7 +1184,7 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
                            ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp,
-                           ctx->d_p_words, nullptr, 0, nullptr, 0, nullptr};
+                           ctx->d_p_words, nullptr, 0, nullptr, 0, nullptr, ctx->tuned_stages};
         if (ctx->d_items) {
             a.items_rho = ctx->d_items + ctx->items_off_rho[ci], a.n_rho = ctx->items_n_rho[ci];
             a.items_vxc = ctx->d_items + ctx->items_off_vxc[ci], a.n_vxc = ctx->items_n_vxc[ci];
@@ -2010,6 +2049,7 @@ pdfxc_status pdfxc_plan_grid(const pdfxc_options* opt, int natom, const double* 
                                                     shell_nprim, prim_exp, prim_coef))
             return st;
         HostGrid G;
+        resolve_shapes(&c, npts, 1);
         plan_grid(&c, npts, xyzw, nullptr, {GridSegment{0, npts, 0, c.nshell}}, G);
         out->nblocks = G.nblk;
         out->ngroups = G.ngrp;
@@ -2060,6 +2100,94 @@ pdfxc_status pdfxc_set_profiling(pdfxc_ctx* ctx, int enable) {
 pdfxc_status pdfxc_last_profile(pdfxc_ctx* ctx, pdfxc_profile* out) {
     if (!ctx || !out) return PDFXC_ERR_ARG;
     *out = ctx->last_profile;
+    return PDFXC_OK;
+}
+
+pdfxc_status pdfxc_autotune(pdfxc_ctx* ctx, int functional, const double* d_PA, pdfxc_tuning* out, int max_out,
+                            int* n_out) {
+    return guarded(ctx, [&]() -> pdfxc_status {
+        pdfxc_status st = check_build(ctx, functional, 0);
+        if (st) return st;
+        const bool int8 = ctx->opt.precision == PDFXC_PRECISION_MIXED && ctx->opt.split_terms == 10;
+        // the grid as given, to block it again for every candidate
+        const int64_t npts = ctx->npts;
+        const size_t nslot = (size_t)ctx->nblk * BLOCK_PTS;
+        std::vector<double> c[4] = {std::vector<double>(nslot), std::vector<double>(nslot), std::vector<double>(nslot),
+                                    std::vector<double>(nslot)};
+        const double* src[4] = {ctx->d_px, ctx->d_py, ctx->d_pz, ctx->d_pw};
+        for (int k = 0; k < 4; ++k)
+            PDFXC_CUDA(cudaMemcpyAsync(c[k].data(), src[k], sizeof(double) * nslot, cudaMemcpyDeviceToHost, ctx->stream));
+        PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+        std::vector<double> xyzw(4 * (size_t)npts);
+        std::vector<int> atom(ctx->h_owner.empty() ? 0 : (size_t)npts);
+        for (size_t slot = 0; slot < nslot; ++slot) {
+            const int64_t i = ctx->h_src[slot];
+            if (i < 0) continue;
+            for (int k = 0; k < 4; ++k) xyzw[4 * i + k] = c[k][slot];
+            if (!atom.empty()) atom[i] = ctx->h_owner[slot];
+        }
+        std::vector<GridSegment> segs;
+        for (size_t k = 0; k < ctx->seg_pts.size(); ++k)
+            segs.push_back(GridSegment{ctx->seg_pts[k].first, ctx->seg_pts[k].second, ctx->seg_sh[k].first,
+                                       ctx->seg_sh[k].second});
+        const std::vector<int> mol = ctx->mol;
+        const double* P = d_PA ? d_PA : ctx->d_P;
+        auto reblock = [&](int g, int stg) {
+            ctx->opt.group_blocks = g, ctx->opt.vxc_stages = stg;
+            build_grid(ctx, npts, xyzw.data(), atom.empty() ? nullptr : atom.data(), segs);
+            if (mol.size() > 1) {  // a batch: its per-molecule sums
+                ctx->mol = mol;
+                dev_alloc(&ctx->d_mol_sums, 2 * (mol.size() - 1));
+            }
+        };
+        // candidates: INT8 groups of 1, 2 or 4 blocks x 2 or 3 Vxc stages; the FP64 path has no shape to choose
+        std::vector<TuneChoice> cand;
+        if (int8)
+            for (int g : {4, 2, 1})
+                for (int stg : {3, 2}) cand.push_back({g, stg});
+        else
+            cand.push_back({1, 3});
+        std::vector<float> ms(cand.size(), 0.f);
+        const bool profiling = ctx->profiling;
+        ctx->profiling = false;
+        for (size_t k = 0; k < cand.size(); ++k) {
+            if (int8) reblock(cand[k].group_blocks, cand[k].vxc_stages);
+            float best = 1e30f;
+            for (int rep = 0; rep < 3; ++rep) {  // a warm-up (graph capture), then the better of two
+                run_build(ctx, functional, P, false);
+                PDFXC_CUDA(cudaStreamSynchronize(ctx->stream));
+                collect_profile(ctx);
+                if (int code = device_error(ctx)) {
+                    ctx->profiling = profiling;
+                    ctx->err = "pdfxc_autotune: a bounded device wait expired (code " + std::to_string(code) + ")";
+                    return PDFXC_ERR_TIMEOUT;
+                }
+                if (rep > 0) best = std::min(best, ctx->last_profile.total_ms);
+            }
+            ms[k] = best;
+        }
+        ctx->profiling = profiling;
+        const size_t win = (size_t)(std::min_element(ms.begin(), ms.end()) - ms.begin());
+        if (int8) {
+            if (win != cand.size() - 1) reblock(cand[win].group_blocks, cand[win].vxc_stages);
+            std::lock_guard<std::mutex> lock(g_tune_mutex);
+            g_tune_cache[tune_class(ctx, npts, segs.size())] = cand[win];
+        }
+        const int n = (int)std::min<size_t>(cand.size(), max_out > 0 ? (size_t)max_out : 0);
+        for (int k = 0; out && k < n; ++k) {
+            const size_t j = k == 0 ? win : (k <= (int)win ? k - 1 : k);  // the winner first
+            out[k] = pdfxc_tuning{cand[j].group_blocks, cand[j].vxc_stages, ctx->opt.block_points, ms[j]};
+        }
+        if (n_out) *n_out = n;
+        return PDFXC_OK;
+    });
+}
+
+pdfxc_status pdfxc_get_tuning(pdfxc_ctx* ctx, pdfxc_tuning* out) {
+    if (!ctx || !out) return PDFXC_ERR_ARG;
+    const bool int8 = ctx->opt.precision == PDFXC_PRECISION_MIXED && ctx->opt.split_terms == 10;
+    *out = pdfxc_tuning{int8 ? ctx->tuned_group : 1, int8 ? ctx->tuned_stages : 0, ctx->opt.block_points,
+                        ctx->last_profile.total_ms};
     return PDFXC_OK;
 }
 

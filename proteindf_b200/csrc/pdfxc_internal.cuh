@@ -186,6 +186,11 @@ struct pdfxc_ctx {
     double* d_scalars_b = nullptr;  // [2]
     double *d_P_b = nullptr, *d_V_b = nullptr, *d_Vacc_b = nullptr;  // n_ao^2 each
     int rho_spin = 0;               // the stored densities: 1 closed shell, 2 open shell
+
+    // the grid as given (for re-blocking: pdfxc_autotune): its segments (one per molecule of a batch)
+    std::vector<std::pair<int64_t, int64_t>> seg_pts;  // points [p0, p1) of each segment
+    std::vector<std::pair<int, int>> seg_sh;           // shells [sh0, sh1) of each segment
+    int tuned_group = 0, tuned_stages = 0;             // the choices in use (0: not tuned)
 };
 
 namespace pdfxc {
@@ -397,6 +402,7 @@ struct MixedArgs {
     const int2* items_vxc;
     int n_vxc;
     int* counters;
+    int vxc_stages;  // operand stages of the Vxc contraction (2 or 3)
 };
 void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
 void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue

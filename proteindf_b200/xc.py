@@ -24,13 +24,20 @@ EXPORTS = [
     "pdfxc_block_costs", "pdfxc_partition_blocks", "pdfxc_set_block_range", "pdfxc_set_batch",
     "pdfxc_build_vxc_batched", "pdfxc_density", "pdfxc_generate_grid", "pdfxc_get_grid",
     "pdfxc_build_vxc_delta_device", "pdfxc_pack_upper", "pdfxc_unpack_upper", "pdfxc_plan_grid",
-    "pdfxc_xc_backward", "pdfxc_selftest_wait",
+    "pdfxc_xc_backward", "pdfxc_selftest_wait", "pdfxc_autotune", "pdfxc_get_tuning",
 ]
 
 
 class Options(ctypes.Structure):
     _fields_ = [("precision", ctypes.c_int), ("block_points", ctypes.c_int), ("ao_cutoff", ctypes.c_double),
-                ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t), ("split_terms", ctypes.c_int)]
+                ("rho_cutoff", ctypes.c_double), ("workspace_bytes", ctypes.c_size_t), ("split_terms", ctypes.c_int),
+                ("group_blocks", ctypes.c_int), ("vxc_stages", ctypes.c_int)]
+
+
+class Tuning(ctypes.Structure):
+    """pdfxc_tuning: one candidate shape of the autotuner and its build time."""
+    _fields_ = [("group_blocks", ctypes.c_int), ("vxc_stages", ctypes.c_int), ("block_points", ctypes.c_int),
+                ("ms", ctypes.c_float)]
 
 
 class GridParams(ctypes.Structure):
@@ -106,6 +113,8 @@ def load_library(path=LIB_PATH):
                                           _vp, _vp]
     L.pdfxc_xc_gradient.argtypes = [_vp, i32, _vp, _vp, _vp, i32, _vp, _vp, _vp]
     L.pdfxc_selftest_wait.argtypes = [_vp, f64]
+    L.pdfxc_autotune.argtypes = [_vp, i32, _vp, ctypes.POINTER(Tuning), i32, ctypes.POINTER(i32)]
+    L.pdfxc_get_tuning.argtypes = [_vp, ctypes.POINTER(Tuning)]
     L.pdfxc_xc_backward.argtypes = [_vp, i32, _vp, f64, _vp, _vp, i32, _vp, _vp, _vp, _vp]
     L.pdfxc_build_vxc_uks.argtypes = [_vp, i32, _vp, _vp, i32, _vp, _vp, _vp, _vp, _vp]
     L.pdfxc_get_rho_uks.argtypes = [_vp, i32, _vp]
@@ -144,7 +153,7 @@ def partition_blocks(cost, nparts):
 
 
 def make_options(precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16, workspace_bytes=0,
-                 split_terms=10):
+                 split_terms=10, group_blocks=0, vxc_stages=0):
     L = load_library()
     opt = Options()
     L.pdfxc_default_options(ctypes.byref(opt))
@@ -154,6 +163,8 @@ def make_options(precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff
     opt.rho_cutoff = rho_cutoff
     opt.workspace_bytes = workspace_bytes
     opt.split_terms = split_terms
+    opt.group_blocks = group_blocks
+    opt.vxc_stages = vxc_stages
     return opt
 
 
@@ -185,9 +196,10 @@ class XcEngine:
     """
 
     def __init__(self, device=0, precision="fp64", block_points=128, ao_cutoff=1e-14, rho_cutoff=1e-16,
-                 workspace_bytes=0, split_terms=10):
+                 workspace_bytes=0, split_terms=10, group_blocks=0, vxc_stages=0):
         self.L = load_library()
-        opt = make_options(precision, block_points, ao_cutoff, rho_cutoff, workspace_bytes, split_terms)
+        opt = make_options(precision, block_points, ao_cutoff, rho_cutoff, workspace_bytes, split_terms, group_blocks,
+                           vxc_stages)
         h = _vp()
         st = self.L.pdfxc_create(ctypes.byref(h), device, ctypes.byref(opt))
         if st != 0:
@@ -442,6 +454,20 @@ class XcEngine:
         self._check(self.L.pdfxc_grid_stats(self.h, ctypes.byref(nb), ctypes.byref(npad), ctypes.byref(fl),
                                             ctypes.byref(mnb)), "pdfxc_grid_stats")
         return {"nblocks": nb.value, "npts_padded": npad.value, "contraction_flops": fl.value, "mean_nb": mnb.value}
+
+    def autotune(self, functional, d_PA_ptr=None):
+        """pdfxc_autotune: time every candidate shape on the current grid, keep the fastest.
+        Returns a list of dicts (group_blocks, vxc_stages, block_points, ms), the winner first."""
+        out = (Tuning * 16)()
+        n = ctypes.c_int(0)
+        self._check(self.L.pdfxc_autotune(self.h, FUNCTIONALS[functional], _vp(d_PA_ptr or 0), out, 16,
+                                          ctypes.byref(n)), "pdfxc_autotune")
+        return [{k: getattr(out[i], k) for k, _ in Tuning._fields_} for i in range(n.value)]
+
+    def tuning(self):
+        t = Tuning()
+        self._check(self.L.pdfxc_get_tuning(self.h, ctypes.byref(t)), "pdfxc_get_tuning")
+        return {k: getattr(t, k) for k, _ in Tuning._fields_}
 
     def selftest_wait(self, limit_seconds=1e-3):
         """Run the bounded-wait failure path (pdfxc_selftest_wait); returns (status, message)."""
