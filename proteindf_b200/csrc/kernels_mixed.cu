@@ -718,8 +718,11 @@ __global__ void __launch_bounds__(256) k_p_digits(const double* __restrict__ P, 
 }
 
 // P_sub digits of a group: a gather of the words of P[aos[mu]][aos[nu]] (the digit words of a
-// zero are 0). A warp takes 8 rows x 64 columns (lane = row r, K group kg: 16 columns), so each
-// digit store instruction writes four whole 128-byte core matrices.
+// zero are 0). A warp takes tiles of 8 rows x 64 columns. It loads them along the rows (lane = a
+// column, 32 consecutive screened AOs per load instruction: runs of neighbouring addresses), writes
+// them to a shared-memory tile, and reads them back across (lane = row r, K group kg: 16 columns)
+// for the digit-plane stores, each of which writes four whole 128-byte core matrices. The shared
+// tile's columns are XOR-swizzled by row (a read touches each bank at most twice).
 __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* __restrict__ words, int nao,
                                                    const int* __restrict__ grp, const int* __restrict__ p_rowexp,
                                                    char* ws) {
@@ -731,6 +734,7 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* _
     // the group's AO list in shared memory (a group with more screened AOs reads it from global)
     constexpr int kAosCap = 1024;
     __shared__ int s_aos[kAosCap];
+    __shared__ uint32_t s_tile[8][8][64];  // per warp: 8 rows x 64 columns
     const bool staged = m.nb <= kAosCap;
     if (staged)
         for (int i = threadIdx.x; i < m.nb; i += blockDim.x) s_aos[i] = g.blk_aos[m.ao0 + i];
@@ -740,27 +744,36 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* _
     const int r = lane & 7, kg = lane >> 3;
     const int nk = m.nbp / 64, ntile = (m.nbp / 8) * nk;
     constexpr int kWarps = 8;  // 256 threads
-    // two warp tiles per iteration: 32 independent gathers in flight per lane
-    for (int t0 = warp; t0 < ntile; t0 += 2 * kWarps) {
-        uint32_t w[2][16];
-        int mu[2], k0[2];
+    uint32_t(*tile)[64] = s_tile[warp];
+    for (int t = warp; t < ntile; t += kWarps) {
+        const int mu0 = (t / nk) * 8, k0 = (t % nk) * 64;
+        // the tile's column AOs (two per lane) and, row by row, the words
+        const int nu0 = k0 + lane, nu1 = k0 + 32 + lane;
+        const int anu0 = nu0 < m.nb ? aos[nu0] : -1, anu1 = nu1 < m.nb ? aos[nu1] : -1;
+        uint32_t v[8][2];
 #pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            const int t = t0 + h * kWarps;
-            mu[h] = (t / nk) * 8 + r, k0[h] = (t % nk) * 64 + kg * 16;
-            const bool live = t < ntile && mu[h] < m.nb;
-            const int amu = live ? aos[mu[h]] : 0;
-            if (t < ntile && kg == 0 && k0[h] == 0) e_p[mu[h]] = live ? __ldg(p_rowexp + amu) : kOzZeroExp;
-            const uint32_t* row = words + (size_t)amu * nao;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const int nu = k0[h] + j;
-                w[h][j] = (live && nu < m.nb) ? __ldg(row + aos[nu]) : 0u;
-            }
+        for (int rr = 0; rr < 8; ++rr) {
+            const int mu = mu0 + rr;
+            const bool live = mu < m.nb;
+            const uint32_t* row = words + (size_t)(live ? aos[mu] : 0) * nao;
+            v[rr][0] = (live && anu0 >= 0) ? __ldg(row + anu0) : 0u;
+            v[rr][1] = (live && anu1 >= 0) ? __ldg(row + anu1) : 0u;
+        }
+        if (k0 == 0 && lane < 8) {
+            const int mu = mu0 + lane;
+            e_p[mu] = mu < m.nb ? __ldg(p_rowexp + aos[mu]) : kOzZeroExp;
         }
 #pragma unroll
-        for (int h = 0; h < 2; ++h)
-            if (t0 + h * kWarps < ntile) oz_store16_words(base + L.ppack, kOzPlanesB, oz_off_b(mu[h], k0[h], m.nbp), w[h]);
+        for (int rr = 0; rr < 8; ++rr) {
+            tile[rr][lane ^ rr] = v[rr][0];
+            tile[rr][(32 + lane) ^ rr] = v[rr][1];
+        }
+        __syncwarp();
+        uint32_t w[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) w[j] = tile[r][(kg * 16 + j) ^ r];
+        __syncwarp();  // the tile is read before the next one is written
+        oz_store16_words(base + L.ppack, kOzPlanesB, oz_off_b(mu0 + r, k0 + kg * 16, m.nbp), w);
     }
 }
 
