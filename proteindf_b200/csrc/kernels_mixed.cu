@@ -534,18 +534,11 @@ __device__ __forceinline__ double warp_max_d(double v) {
 // to four blocks). Pass 1: the radial sums S0, S1 of every shell of the group's basis at the
 // thread's point (stored for the later stages) and the point's exponent of phi^T rows (the
 // max over the AOs: max_c |A_c S0| = |S0| max_c |A_c|, the rounding being monotone). Pass 2,
-// per tile of 16 AO rows: phi formed once in shared memory, each row's maximum over the
-// group's points (the group's scale of phi rows, taken in shared memory, stored by the first
-// block), then every thread cuts the phi^T digits of its point (16 AOs, one 16-byte store per
-// digit plane) and a (row, 16 points) piece of the phi digits (8 consecutive rows with the
-// same points fill whole 128-byte core matrices).
+// per tile of 16 AO rows: every thread forms phi of its point shell by shell from S0 and cuts
+// its 16 digits with the point's scale (one 16-byte store per digit plane). These are the only
+// phi digits: the Vxc contraction reads them as an MN-major operand and takes the point scale
+// into Z' = 2^e_pt Z.
 constexpr int kGroupPts = 4 * BLOCK_PTS;
-struct OzPhiTile {
-    double x[kGroupPts], y[kGroupPts], z[kGroupPts];
-    double vt[16][kGroupPts + 1];
-    RowGeom rg[2][16];  // row geometry of this tile and the next (staged during this tile's row maxima)
-    int eg[16];
-};
 
 // Prefetch into L1 of the line holding p (no wait, no register).
 __device__ __forceinline__ void prefetch_l1(const void* p) { asm volatile("prefetch.global.L1 [%0];" ::"l"(p)); }
@@ -572,7 +565,6 @@ __device__ __forceinline__ void oz_stage_rows(const GridView& g, const BlockMeta
     const int k = (int)threadIdx.x - ((int)blockDim.x - 16);
     if (k >= 0) rg[k] = r0 + k < m.nb ? g.blk_row_geom[m.ao0 + r0 + k] : RowGeom{0.0, 0.0, 0.0, 0, 0};
 }
-constexpr size_t kPhiTileBytes = sizeof(OzPhiTile);
 
 // max_c |A_c| over a shell's components (the expressions of ang_poly1, without its branch per component)
 __device__ __forceinline__ double ang_max_abs(int L, double x, double y, double z) {
@@ -583,11 +575,15 @@ __device__ __forceinline__ double ang_max_abs(int L, double x, double y, double 
     return fmax(a, fmax(fabs(0.5 * (x * x - y * y)), fabs(s3 * (z * z - 0.5 * (x * x + y * y)))));
 }
 
+// Shared memory of k_phi_group: the group's shell table (pass 1), then its rows' geometry
+// (pass 2); a group whose table or rows do not fit reads them from global.
+constexpr size_t kPhiGroupBytes = 64 * 1024;
+constexpr int kPhiRowsCap = (int)(kPhiGroupBytes / sizeof(RowGeom));
+
 template <bool GGA>
 __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridView g, const int* __restrict__ grp,
                                                               char* ws) {
     extern __shared__ __align__(16) uint8_t psm[];
-    OzPhiTile& T = *reinterpret_cast<OzPhiTile*>(psm);
     const int lead = grp[blockIdx.x];
     const BlockMeta m = g.meta[lead];
     const OzLayout L = oz_layout(m.nbp, m.nsh);
@@ -595,18 +591,17 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
     const bool live = b < m.gn;
     char* base = ws + g.meta[lead + (live ? b : 0)].ws;
     double* rad = reinterpret_cast<double*>(base + L.rad);
-    int ept = kOzZeroExp;
-    // The group's shell table in the tile buffer, which pass 1 does not use (a group whose table
-    // does not fit reads the global tables; m.nsh is uniform over the CTA).
-    ShellRec* recs = reinterpret_cast<ShellRec*>(&T.vt[0][0]);
-    const bool staged = (size_t)m.nsh * sizeof(ShellRec) <= sizeof(T.vt);
+    ShellRec* recs = reinterpret_cast<ShellRec*>(psm);
+    RowGeom* rows = reinterpret_cast<RowGeom*>(psm);
+    const bool staged = (size_t)m.nsh * sizeof(ShellRec) <= kPhiGroupBytes;  // uniform over the CTA
     if (staged)
         for (int i = tid; i < m.nsh; i += blockDim.x) stage_shell(bas, g.blk_shells[m.sh0 + i], 0, recs[i]);
     __syncthreads();
+    int ept = kOzZeroExp;
+    double rx = 0.0, ry = 0.0, rz = 0.0;
     if (live) {
         const size_t gp = (size_t)(lead + b) * BLOCK_PTS + q;
-        const double rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
-        T.x[tid] = rx, T.y[tid] = ry, T.z[tid] = rz;
+        rx = g.px[gp], ry = g.py[gp], rz = g.pz[gp];
         double pm = 0.0;
         for (int i = 0; i < m.nsh; ++i) {
             double x, y, z, S0, S1;
@@ -630,68 +625,50 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
         ept = oz_exponent(pm);
         reinterpret_cast<int*>(base + L.e_pt)[q] = ept;
     }
-    const int warp = tid >> 5, lane = tid & 31;
-    oz_stage_rows(g, m, 0, T.rg[0]);
+    __syncthreads();  // the shell table is no longer read
+    const bool rows_staged = m.nb <= kPhiRowsCap;
+    if (rows_staged)
+        for (int i = tid; i < m.nb; i += blockDim.x) rows[i] = g.blk_row_geom[m.ao0 + i];
+    __syncthreads();
+    if (!live) return;
+    const RowGeom* rg = rows_staged ? rows : g.blk_row_geom + m.ao0;
+    const double sc = oz_digit_scale(ept);
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
-        const int cur = (mu0 >> 4) & 1;
-        __syncthreads();  // the previous tile's digits are cut (and the points and rows are stored)
-        if (live) {  // shell by shell over the tile's rows (uniform over the CTA), phi = A S0
-            int r = 0;
-            while (r < 16) {
-                if (mu0 + r >= m.nb) {
-                    T.vt[r][tid] = 0.0;
-                    ++r;
-                    continue;
-                }
-                const RowGeom& gq = T.rg[cur][r];
-                const int t = gq.info & 15, slot = gq.info >> 4;
-                const int Lq = t == 0 ? 0 : (t < 4 ? 1 : 2);
-                const int u0 = t - Lq * Lq;                 // the component of row r
-                const int n = min(2 * Lq + 1 - u0, 16 - r);  // the shell's rows in this tile from r
-                const double S0 = rad[(size_t)slot * BLOCK_PTS + q];
-                const double x = T.x[tid] - gq.ax, y = T.y[tid] - gq.ay, z = T.z[tid] - gq.az;
-                double pc[5];
-                if (Lq == 0) {
-                    pc[0] = S0;
-                } else if (Lq == 1) {
-                    pc[0] = x * S0, pc[1] = y * S0, pc[2] = z * S0;
-                } else {  // the products of ang_poly1
-                    const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
-                    pc[0] = (x * y) * S0, pc[1] = (z * x) * S0, pc[2] = (y * z) * S0;
-                    pc[3] = (0.5 * (x * x - y * y)) * S0, pc[4] = (s3 * (z * z - 0.5 * (x * x + y * y))) * S0;
-                }
-#pragma unroll
-                for (int k = 0; k < 5; ++k)
-                    if (k >= u0 && k < u0 + n) T.vt[r + k - u0][tid] = pc[k];
-                r += n;
+        // shell by shell over the tile's rows (uniform over the CTA), phi = A S0
+        double v[16];
+        int r = 0;
+        while (r < 16) {
+            if (mu0 + r >= m.nb) {
+                v[r] = 0.0;
+                ++r;
+                continue;
             }
-        } else {
-            for (int r = 0; r < 16; ++r) T.vt[r][tid] = 0.0;
-        }
-        __syncthreads();
-        {  // warp r: the row's maximum over the group's points
-            double mx = 0.0;
-            for (int p = lane; p < kGroupPts; p += 32) mx = fmax(mx, fabs(T.vt[warp][p]));
-            mx = warp_max_d(mx);
-            if (lane == 0) {
-                const int e = oz_exponent(mx);
-                T.eg[warp] = e;
-                reinterpret_cast<int*>(ws + m.ws + L.e_phi_g)[mu0 + warp] = e;
+            const RowGeom gq = rg[mu0 + r];
+            const int t = gq.info & 15, slot = gq.info >> 4;
+            const int Lq = t == 0 ? 0 : (t < 4 ? 1 : 2);
+            const int u0 = t - Lq * Lq;                 // the component of row r
+            const int n = min(2 * Lq + 1 - u0, 16 - r);  // the shell's rows in this tile from r
+            const double S0 = rad[(size_t)slot * BLOCK_PTS + q];
+            const double x = rx - gq.ax, y = ry - gq.ay, z = rz - gq.az;
+            double pc[5];
+            if (Lq == 0) {
+                pc[0] = S0;
+            } else if (Lq == 1) {
+                pc[0] = x * S0, pc[1] = y * S0, pc[2] = z * S0;
+            } else {  // the products of ang_poly1
+                const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
+                pc[0] = (x * y) * S0, pc[1] = (z * x) * S0, pc[2] = (y * z) * S0;
+                pc[3] = (0.5 * (x * x - y * y)) * S0, pc[4] = (s3 * (z * z - 0.5 * (x * x + y * y))) * S0;
             }
-        }
-        oz_stage_rows(g, m, mu0 + 16, T.rg[cur ^ 1]);  // every thread has formed this tile's values
-        __syncthreads();
-        if (live) {
-            oz_prefetch_rows<false>(T.rg[cur ^ 1], mu0 + 16, m, rad, q);  // the next tile's S0, under the cut
-            double v[16];
 #pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = T.vt[j][tid];
-            oz_store16(base + L.phi1, kOzPlanesA, oz_off_a(q, mu0, m.nbp), v, ept);
-            const int r = (q & 7) + 8 * (q >> 6), kg = (q >> 3) & 7;
-#pragma unroll
-            for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
-            oz_store16(base + L.phi2, kOzPlanesA, oz_off_a(mu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
+            for (int k = 0; k < 5; ++k)
+                if (k >= u0 && k < u0 + n) v[r + k - u0] = pc[k];
+            r += n;
         }
+        uint32_t w[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) w[j] = oz_word(v[j], sc);
+        oz_store16_words(base + L.phi1, kOzPlanesA, oz_off_a(q, mu0, m.nbp), w);
     }
 }
 
@@ -777,11 +754,12 @@ __global__ void __launch_bounds__(256) k_pack_p_oz(GridView g, const uint32_t* _
     }
 }
 
-// Z digits of a whole group in one CTA (512 threads, one per point of its up to four blocks):
-// per tile of 16 rows the CTA forms Z once in shared memory, takes each row's maximum over the
-// group's points (the group's row scale, stored by the first block for the Vxc epilogue), and
-// cuts the digits of every block from the same tile. One Z evaluation per value instead of two
-// (row exponents per block, then digits with the group maximum).
+// Z' digits of a whole group in one CTA (512 threads, one per point of its up to four blocks):
+// Z' = 2^e_pt Z takes the point scale of the phi^T digits, which the Vxc contraction reads as
+// its other operand (W_mu_nu = sum_p phi_p_mu Z_p_nu = sum_p (2^-e_pt phi_p_mu) Z'_p_nu). Per tile
+// of 16 rows the CTA forms Z' once in shared memory, takes each row's maximum over the group's
+// points (the group's row scale, stored by the first block for the Vxc epilogue), and cuts the
+// digits of every block from the same tile into 128-row A-operand tiles.
 struct OzGroupTile {
     double x[kGroupPts], y[kGroupPts], z[kGroupPts];
     double c[4][kGroupPts];
@@ -807,8 +785,9 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
     if (live) {
         const size_t gp = (size_t)blk * BLOCK_PTS + q;
         T.x[tid] = g.px[gp], T.y[tid] = g.py[gp], T.z[tid] = g.pz[gp];
+        const double s = oz_pow2(reinterpret_cast<const int*>(base + L.e_pt)[q]);  // the point's phi scale
 #pragma unroll
-        for (int k = 0; k < 4; ++k) T.c[k][tid] = coef[gp * 4 + k];
+        for (int k = 0; k < 4; ++k) T.c[k][tid] = coef[gp * 4 + k] * s;
     }
     const int warp = tid >> 5, lane = tid & 31;
     oz_stage_rows(g, m, 0, T.rg[0]);
@@ -864,7 +843,7 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
             double v[16];
 #pragma unroll
             for (int j = 0; j < 16; ++j) v[j] = T.vt[r][b * BLOCK_PTS + kg * 16 + j];
-            oz_store16(base + L.zpack, kOzPlanesB, oz_off_b(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
+            oz_store16(base + L.zpack, kOzPlanesA, oz_off_a(nu0 + r, kg * 16, BLOCK_PTS), v, T.eg[r]);
         }
     }
 }
@@ -958,7 +937,8 @@ __device__ __forceinline__ constexpr int oz_mma_col(int t) { return (int)((0x323
 template <int MODE, bool GGA, int S>
 __global__ void __launch_bounds__(OZ_THREADS, 1)
     k_oz(BasisView bas, GridView g, int blk0, int nblk, const int2* __restrict__ items, int nitems, int* counter,
-         char* ws, int* err, double* rho_acc, double* Vacc, int nao) {
+         char* ws, int* err, double* rho_acc, double* Vacc, int nao, const __grid_constant__ CUtensorMap phi_map,
+         int use_map) {
     extern __shared__ __align__(1024) uint8_t smem[];
     __shared__ int2 s_item[kOzRing];
     // per epilogue group and alternate item of the group (a group writes one buffer while its
@@ -994,22 +974,26 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
     constexpr int kBlockSlabs = BLOCK_PTS / (int)umma::I8_SLAB_K;  // VXC: K slabs per block
 
     if (warp == 0) {
-        if (lane == 0) {  // the scheduler, then the item's copies
-            uint32_t gj = 0;
-            bool ok = true;
-            // entry q of the ring into its slot, once the slot's entry q - kOzRing is consumed
-            auto push = [&](int q, int2 item) {
-                const int slot = q % kOzRing;
-                if (q >= kOzRing && !umma::mbar_wait(&iempty[slot], ((q / kOzRing) - 1) & 1, err)) {
-                    atomicExch(err, 5);
-                    return false;
-                }
-                s_item[slot] = item;
-                umma::mbar_arrive(&ifull[slot]);  // release: the slot's item is visible to the consumers
-                return true;
-            };
-            for (int q = 0; ok; ++q) {
-                int2 item = make_int2(-1, 0);
+        // the scheduler (lane 0), then the item's copies: lane 0 issues the A copy (and the rho B
+        // copy), and for the Vxc contraction lanes 0..15 issue the 16 pieces of its B operand at once
+        constexpr unsigned kAll = 0xffffffffu;
+        uint32_t gj = 0;
+        bool ok = true;
+        // entry q of the ring into its slot, once the slot's entry q - kOzRing is consumed (lane 0)
+        auto push = [&](int q, int2 item) {
+            const int slot = q % kOzRing;
+            if (q >= kOzRing && !umma::mbar_wait(&iempty[slot], ((q / kOzRing) - 1) & 1, err)) {
+                atomicExch(err, 5);
+                return false;
+            }
+            s_item[slot] = item;
+            umma::mbar_arrive(&ifull[slot]);  // release: the slot's item is visible to the consumers
+            return true;
+        };
+        for (int q = 0; ok; ++q) {
+            int2 item = make_int2(-1, 0);
+            int pushed = 1;
+            if (lane == 0) {
                 for (;;) {  // the next item of the launch's block range
                     const int it = atomicAdd(counter, 1);
                     if (it >= nitems) break;
@@ -1017,55 +1001,80 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     if (item.x >= blk0 && item.x < blk0 + nblk) break;
                     item = make_int2(-1, 0);
                 }
-                if (!push(q, item)) break;
-                if (item.x < 0) {
-                    push(q + 1, item);
-                    break;
-                }
-                int blk, mt, nt;
-                oz_decode(MODE, item, blk, mt, nt);
-                const BlockMeta m = g.meta[blk];
-                const OzLayout L = oz_layout(m.nbp, m.nsh);
-                const char* base = ws + m.ws;
-                const char* lead = ws + g.meta[m.lead].ws;
-                // per slab one 32 KiB A copy and one 16 KiB B copy (the layouts of oz_off_a, oz_off_b)
-                size_t Ao, Bo;
-                int nslabs, kslabs;  // slabs of the item; slabs per block of the K extent
-                if (MODE == MODE_RHO) {
-                    nslabs = kslabs = m.nbp / (int)umma::I8_SLAB_K;
-                    Ao = L.phi1;
-                    Bo = L.ppack + (size_t)nt * kslabs * 16384;
-                } else {
-                    kslabs = kBlockSlabs;
-                    nslabs = m.gn * kBlockSlabs;
-                    Ao = L.phi2 + (size_t)mt * kslabs * 32768;
-                    Bo = L.zpack + (size_t)nt * kslabs * 16384;
-                }
-                for (int j = 0; j < nslabs; ++j, ++gj) {
-                    const int st = gj % S;
+                pushed = push(q, item) ? 1 : 0;
+                if (pushed && item.x < 0) push(q + 1, item);
+            }
+            item.x = __shfl_sync(kAll, item.x, 0);
+            item.y = __shfl_sync(kAll, item.y, 0);
+            pushed = __shfl_sync(kAll, pushed, 0);
+            if (!pushed || item.x < 0) break;
+            int blk, mt, nt;
+            oz_decode(MODE, item, blk, mt, nt);
+            const BlockMeta m = g.meta[blk];
+            const OzLayout L = oz_layout(m.nbp, m.nsh);
+            const char* base = ws + m.ws;
+            const char* lead = ws + g.meta[m.lead].ws;
+            size_t Ao, Bo;
+            int nslabs, kslabs;  // slabs of the item; slabs per block of the K extent
+            if (MODE == MODE_RHO) {  // per slab one 32 KiB A copy and one 16 KiB B copy
+                nslabs = kslabs = m.nbp / (int)umma::I8_SLAB_K;
+                Ao = L.phi1;
+                Bo = L.ppack + (size_t)nt * kslabs * 16384;
+            } else {  // A: Z' rows of tile mt; B: the phi^T digits of AO slab nt, read MN-major
+                kslabs = kBlockSlabs;
+                nslabs = m.gn * kBlockSlabs;
+                Ao = L.zpack + (size_t)mt * kslabs * 32768;
+                Bo = L.phi1 + (size_t)nt * 32768;
+            }
+            for (int j = 0; j < nslabs; ++j, ++gj) {
+                const int st = gj % S;
+                int w = 1;
+                if (lane == 0) {
                     if (gj >= S && !umma::mbar_wait(&empty[st], ((gj / S) - 1) & 1, err)) {
                         atomicExch(err, 1);
-                        ok = false;
-                        break;
+                        w = 0;
+                    } else {
+                        umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
                     }
-                    uint8_t* sp = smem + st * OZ_STAGE_BYTES;
-                    umma::mbar_expect_tx(&full[st], OZ_STAGE_BYTES);
-                    const char *As = base + Ao, *Bs = lead + Bo;
-                    int js = j;
-                    if (MODE == MODE_VXC) {  // slab j: block lead + j / kBlockSlabs, its slab j % kBlockSlabs
-                        const char* bj = ws + g.meta[m.lead + j / kBlockSlabs].ws;
-                        As = bj + Ao, Bs = bj + Bo;
-                        js = j % kBlockSlabs;
-                    }
-                    umma::bulk_g2s(sp, As + (size_t)js * 32768, OZ_A_BYTES, &full[st]);
-                    umma::bulk_g2s(sp + OZ_A_BYTES, Bs + (size_t)js * 16384, OZ_STAGE_BYTES - OZ_A_BYTES, &full[st]);
+                }
+                if (!__shfl_sync(kAll, w, 0)) {
+                    ok = false;
+                    break;
+                }
+                uint8_t* sp = smem + st * OZ_STAGE_BYTES;
+                const char *As = base + Ao, *Bs = lead + Bo;
+                int js = j;
+                if (MODE == MODE_VXC) {  // slab j: block lead + j / kBlockSlabs, its slab j % kBlockSlabs
+                    const char* bj = ws + g.meta[m.lead + j / kBlockSlabs].ws;
+                    As = bj + Ao, Bs = bj + Bo;
+                    js = j % kBlockSlabs;
+                }
+                if (lane == 0) umma::bulk_g2s(sp, As + (size_t)js * 32768, OZ_A_BYTES, &full[st]);
+                if (MODE == MODE_RHO) {
+                    if (lane == 0)
+                        umma::bulk_g2s(sp + OZ_A_BYTES, Bs + (size_t)js * 16384, OZ_STAGE_BYTES - OZ_A_BYTES,
+                                       &full[st]);
+                } else if (use_map) {
+                    // the 64 points js of the slab: per plane i and 16-AO group kg the 8 core matrices of
+                    // those points (1 KiB), in the stage plane i at 4 KiB i, group kg at 1 KiB kg: one
+                    // tensor copy of the box {1 KiB, 4 groups, 4 planes} at the slab's 256-byte offset
+                    if (lane == 0)
+                        umma::tensor4_g2s(sp + OZ_A_BYTES, &phi_map, 0, 0, 0,
+                                          (int)((Bs + (size_t)js * 1024 - ws) >> 8), &full[st]);
+                } else if (lane < 16) {  // the same 16 pieces as bulk copies
+                    const int i = lane >> 2, kg = lane & 3;
+                    umma::bulk_g2s(sp + OZ_A_BYTES + i * 4096 + kg * 1024,
+                                   Bs + (size_t)i * 8192 + kg * 2048 + (size_t)js * 1024, 1024, &full[st]);
                 }
             }
         }
         __syncwarp();
     } else if (warp == 1) {
         if (lane == 0) {  // MMAs
-            const uint32_t idesc128 = umma::instr_desc_s8(128, 2 * OZ_NT), idesc64 = umma::instr_desc_s8(128, OZ_NT);
+            // Vxc: B (the phi^T digits) is MN-major (bit 16 of the instruction descriptor)
+            constexpr uint32_t bmaj = MODE == MODE_VXC ? (1u << 16) : 0u;
+            const uint32_t idesc128 = umma::instr_desc_s8(128, 2 * OZ_NT) | bmaj,
+                           idesc64 = umma::instr_desc_s8(128, OZ_NT) | bmaj;
             uint32_t gj = 0;
             int li = 0;
             bool ok = true;
@@ -1101,14 +1110,19 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                     // to the start-address field (addresses stay below 256 KiB, so it cannot carry)
                     const uint32_t sp = umma::smem_u32(smem + st * OZ_STAGE_BYTES);
                     const uint64_t ad0 = umma::smem_desc(sp, umma::LBO, umma::SBO);
-                    const uint64_t bd0 = umma::smem_desc(sp + OZ_A_BYTES, umma::LBO, umma::SBO);
+                    // B: K-major stacked pairs (rho), or MN-major planes of 64 AOs x 64 points (Vxc: in
+                    // the no-swizzle MN-major layout LBO steps K, the next 8 points 128 B on, and SBO
+                    // steps MN, the next 16 AOs 1 KiB on)
+                    const uint64_t bd0 = MODE == MODE_RHO ? umma::smem_desc(sp + OZ_A_BYTES, umma::LBO, umma::SBO)
+                                                          : umma::smem_desc(sp + OZ_A_BYTES, 128, 1024);
+                    constexpr uint32_t bk = MODE == MODE_RHO ? 4096 : 512;  // B offset of the second K step
 #pragma unroll
                     for (int kk = 0; kk < 2; ++kk) {
 #pragma unroll
                         for (int t = 0; t < 6; ++t) {
                             const int i = oz_mma_a(t);
                             const uint64_t ad = ad0 + (uint64_t)(((i - 1) * umma::I8_SLAB_BYTES + kk * 4096) >> 4);
-                            const uint64_t bd = bd0 + (uint64_t)((oz_mma_pair(t) * 8192 + kk * 4096) >> 4);
+                            const uint64_t bd = bd0 + (uint64_t)((oz_mma_pair(t) * 8192 + kk * bk) >> 4);
                             // the two MMAs of A_1 start all four accumulators
                             const bool first = (j == 0 && kk == 0 && t < 2);
                             umma::mma_s8(tacc + (uint32_t)oz_mma_col(t) * OZ_NT, ad, bd,
@@ -1241,18 +1255,21 @@ __global__ void __launch_bounds__(OZ_THREADS, 1)
                 // shared memory; per 16 columns each thread converts its row's accumulators to FP64
                 // W in its column half's transpose tile, then the half's 128 threads add the tile
                 // to Vacc (16 consecutive columns of two rows per warp instruction).
+                // rows: the Z' AOs nu of tile mt (scale 2^e_z_g); columns: the phi AOs mu of tile nt,
+                // whose point scales went into Z'. The item adds W_mu_nu at Vacc[nu][mu] (the build
+                // symmetrises Vacc).
                 const int* aos = g.blk_aos + m.ao0;
                 if (gt < OZ_NT) {
                     const int nu = nt * OZ_NT + gt;
                     s_acol[sb][gt] = nu < m.nb ? aos[nu] : -1;
-                    s_ez[sb][gt] = reinterpret_cast<const int*>(base + L.e_z_g)[nu];
+                    s_ez[sb][gt] = 0;
                 }
                 if (gt < 128) {
                     const int mu = mt * 128 + gt;
                     s_arow[sb][gt] = mu < m.nb ? aos[mu] : -1;
                 }
                 const int row = quarter * 32 + lane;
-                const int em = reinterpret_cast<const int*>(base + L.e_phi_g)[mt * 128 + row];
+                const int em = reinterpret_cast<const int*>(base + L.e_z_g)[mt * 128 + row];
                 umma::named_sync(gbar, 256);
                 bool ok = umma::mbar_wait(&tfull[h], ph, err);
                 __syncwarp();
@@ -1338,11 +1355,11 @@ void oz_p_digits(const double* P, int nao, const int* row_cols, int* e, uint32_t
 void oz_prepare(const MixedArgs& a, cudaStream_t s) {
     // per group: radial sums, row scales and the phi digits of both layouts; then P_sub
     if (functional_is_gga(a.fn)) {
-        cudaFuncSetAttribute(k_phi_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiTileBytes);
-        k_phi_group<true><<<a.ngrp, kGroupPts, kPhiTileBytes, s>>>(a.b, a.g, a.grp, a.ws);
+        cudaFuncSetAttribute(k_phi_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiGroupBytes);
+        k_phi_group<true><<<a.ngrp, kGroupPts, kPhiGroupBytes, s>>>(a.b, a.g, a.grp, a.ws);
     } else {
-        cudaFuncSetAttribute(k_phi_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiTileBytes);
-        k_phi_group<false><<<a.ngrp, kGroupPts, kPhiTileBytes, s>>>(a.b, a.g, a.grp, a.ws);
+        cudaFuncSetAttribute(k_phi_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kPhiGroupBytes);
+        k_phi_group<false><<<a.ngrp, kGroupPts, kPhiGroupBytes, s>>>(a.b, a.g, a.grp, a.ws);
     }
     k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.p_words, a.nao, a.grp, a.p_rowexp, a.ws);
 }
@@ -1359,8 +1376,42 @@ template <int MODE, bool GGA, int S>
 static void launch_oz(const MixedArgs& a, const int2* items, int nitems, int* counter, cudaStream_t s) {
     const size_t smem = oz_smem_bytes<MODE, S>();
     cudaFuncSetAttribute(k_oz<MODE, GGA, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    CUtensorMap map{};
+    if (a.phi_map) map = *a.phi_map;
     k_oz<MODE, GGA, S><<<oz_grid(nitems), OZ_THREADS, smem, s>>>(a.b, a.g, a.blk0, a.nblk, items, nitems, counter,
-                                                                 a.ws, a.err, a.rho_acc, a.Vacc, a.nao);
+                                                                 a.ws, a.err, a.rho_acc, a.Vacc, a.nao, map,
+                                                                 a.phi_map ? 1 : 0);
+}
+
+// The tensor map of the Vxc contraction's phi operand: the workspace as a 4-D tensor of 8-byte
+// elements, {128 elements = 1 KiB; 4 16-AO groups, 2 KiB apart; 4 digit planes, 8 KiB apart; the
+// offset in 256-byte units} (every region of the workspace starts on 256 bytes), box
+// {128, 4, 4, 1}: 16 KiB, landing in shared memory as [plane][group][1 KiB]. The copies it
+// serves stay inside a block's phi digits (its slab of 32 KiB).
+bool make_phi_map(const void* ws, size_t ws_bytes, CUtensorMap* map) {
+    using Encode = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+    static Encode encode = nullptr;
+    static bool looked = false;
+    if (!looked) {
+        looked = true;
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            encode = reinterpret_cast<Encode>(fn);
+        else
+            cudaGetLastError();
+    }
+    if (!encode || !ws || ws_bytes < 32768 || (reinterpret_cast<uintptr_t>(ws) & 255)) return false;
+    const cuuint64_t dims[4] = {128, 4, 4, (cuuint64_t)(ws_bytes / 256)};
+    const cuuint64_t strides[3] = {2048, 8192, 256};  // bytes, dimensions 1..3
+    const cuuint32_t box[4] = {128, 4, 4, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return encode(map, CU_TENSOR_MAP_DATA_TYPE_UINT64, 4, const_cast<void*>(ws), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
 void oz_rho(const MixedArgs& a, cudaStream_t s) {

@@ -784,6 +784,7 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
         throw std::bad_alloc();
     }
     ctx->ws_bytes = max_ws;
+    ctx->phi_map_ok = mixed && ctx->opt.split_terms == 10 && pdfxc::make_phi_map(ctx->d_ws, max_ws, &ctx->phi_map);
     ctx->nblk = nblk;
     ctx->blk_lo = 0, ctx->blk_hi = nblk;
     ctx->npts = npts;
@@ -1184,7 +1185,8 @@ void enqueue_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental)
         pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, fn, incremental ? 1 : 0, ctx->opt.split_terms, nao,
                            ctx->opt.rho_cutoff, d_PA, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
                            ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp,
-                           ctx->d_p_words, nullptr, 0, nullptr, 0, nullptr, ctx->tuned_stages};
+                           ctx->d_p_words, nullptr, 0, nullptr, 0, nullptr, ctx->tuned_stages,
+                           ctx->phi_map_ok ? &ctx->phi_map : nullptr};
         if (ctx->d_items) {
             a.items_rho = ctx->d_items + ctx->items_off_rho[ci], a.n_rho = ctx->items_n_rho[ci];
             a.items_vxc = ctx->d_items + ctx->items_off_vxc[ci], a.n_vxc = ctx->items_n_vxc[ci];

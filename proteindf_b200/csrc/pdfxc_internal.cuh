@@ -2,6 +2,7 @@
 // grid, and the launch interfaces of the kernels.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -191,6 +192,8 @@ struct pdfxc_ctx {
     std::vector<std::pair<int64_t, int64_t>> seg_pts;  // points [p0, p1) of each segment
     std::vector<std::pair<int, int>> seg_sh;           // shells [sh0, sh1) of each segment
     int tuned_group = 0, tuned_stages = 0;             // the choices in use (0: not tuned)
+    alignas(64) CUtensorMap phi_map{};                 // see MixedArgs::phi_map
+    bool phi_map_ok = false;
 };
 
 namespace pdfxc {
@@ -329,10 +332,11 @@ __host__ __device__ inline MixedLayout mixed_layout(int nbp) {
 // v = 2^e (s_1 + s_2/256 + s_3/256^2 + s_4/256^3)/127; digit planes
 // are packed K-major in 64-byte slabs. AO values are not stored: the block keeps each
 // shell's radial sums S0, S1 at its points ([2][nsh][128] FP64) and every consumer forms
-// phi = A S0, grad phi = grad A S0 - 2 r A S1 from them. The Vxc contraction runs over
-// all points of a group, so the scales of its operands (phi and Z rows) are group
-// maxima (e_phi_g, e_z_g, written by the group's first block). P_sub is shared by the group
-// and lives only in the first block's region, after `total` (`total_lead` bytes in all).
+// phi = A S0, grad phi = grad A S0 - 2 r A S1 from them. One set of phi digits serves both
+// contractions: phi^T with a scale per point (e_pt), K-major for rho and read as an MN-major
+// operand by the Vxc contraction, whose other operand is Z' = 2^e_pt Z with a scale per AO row
+// over the group's points (e_z_g, written by the group's first block). P_sub is shared by the
+// group and lives only in the first block's region, after `total` (`total_lead` bytes in all).
 constexpr int OZ_SLICES = 4;
 // Largest K (screened AOs of a group, padded to 128) of the INT8 rho contraction: its order-5
 // int32 accumulator sums four digit products of at most 128^2 per K index (exact in int32 while
@@ -342,12 +346,11 @@ constexpr int OZ_SLICES = 4;
 constexpr int OZ_MAX_K = 32512;
 struct OzLayout {
     size_t rad;                 // radial sums: S0 [nsh][128], then S1 [nsh][128]
-    size_t phi1, phi1_plane;    // phi^T slices: rows = 128 points, K = nbp AOs
-    size_t phi2, phi2_plane;    // phi slices: rows = nbp AOs, K = 128 points
-    size_t zpack, zpack_plane;  // Z slices: rows = nbp, K = 128 points
-    size_t e_pt, e_phi_g, e_z_g, e_p;  // int exponents: per point, per AO row of the group, P_sub
+    size_t phi1, phi1_plane;    // phi^T digits: rows = 128 points, K = nbp AOs
+    size_t zpack, zpack_plane;  // Z' digits: rows = nbp AOs (128-row tiles), K = 128 points
+    size_t e_pt, e_z_g, e_p;    // int exponents: per point, per AO row of the group (Z'), P_sub
     size_t total;
-    size_t ppack, ppack_plane;  // P_sub slices of the group: rows = nbp, K = nbp (first block only)
+    size_t ppack, ppack_plane;  // P_sub digits of the group: rows = nbp, K = nbp (first block only)
     size_t total_lead;
 };
 
@@ -360,15 +363,12 @@ __host__ __device__ inline OzLayout oz_layout(int nbp, int nsh) {
     L.phi1 = o;
     L.phi1_plane = (size_t)BLOCK_PTS * nbp;
     o = a256(o + OZ_SLICES * L.phi1_plane);
-    L.phi2 = o;
-    L.phi2_plane = (size_t)nbp * BLOCK_PTS;
-    o = a256(o + OZ_SLICES * L.phi2_plane);
     L.zpack = o;
     L.zpack_plane = (size_t)nbp * BLOCK_PTS;
     o = a256(o + OZ_SLICES * L.zpack_plane);
     L.e_pt = o;
     o = a256(o + sizeof(int) * BLOCK_PTS);
-    size_t* e[3] = {&L.e_phi_g, &L.e_z_g, &L.e_p};
+    size_t* e[2] = {&L.e_z_g, &L.e_p};
     for (size_t* f : e) {
         *f = o;
         o = a256(o + sizeof(int) * nbp);
@@ -403,7 +403,13 @@ struct MixedArgs {
     int n_vxc;
     int* counters;
     int vxc_stages;  // operand stages of the Vxc contraction (2 or 3)
+    // INT8 path: a tensor map over the chunk workspace that moves the Vxc contraction's phi operand
+    // of one stage (16 pieces of 1 KiB) in one copy; null: 16 bulk copies
+    const CUtensorMap* phi_map;
 };
+// The tensor map of MixedArgs::phi_map over a workspace of ws_bytes bytes (false: the driver has
+// no tensor-map encoder or refused the map; the contraction then copies piece by piece).
+bool make_phi_map(const void* ws, size_t ws_bytes, CUtensorMap* map);
 void mixed_prepare(const MixedArgs& a, cudaStream_t s);     // AO values, P_sub packing
 void mixed_rho(const MixedArgs& a, cudaStream_t s);         // X^T = phi^T P_sub + rho epilogue
 void mixed_functional(const MixedArgs& a, cudaStream_t s);  // functional, Z packing
