@@ -68,6 +68,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="chain", choices=["chain", "batch64", "chain2000"])
     ap.add_argument("--no-large", action="store_true", help="leave the 2000-atom chain and the batch out")
+    ap.add_argument("--partition", default="Becke", choices=["Becke", "SSWeight"],
+                    help="partition weights of the chain workload's grid")
     return ap.parse_args()
 
 
@@ -86,9 +88,9 @@ def workload(args, seed):
     return syms, xyz, sh, P, W, A, PA, brad
 
 
-def final_grid(eng, P, W, A, brad):
+def final_grid(eng, P, W, A, brad, partition="Becke"):
     from proteindf_b200 import grids
-    w = eng.becke_weights(P, A, W, brad)
+    w = eng.ss_weights(P, A, W) if partition == "SSWeight" else eng.becke_weights(P, A, W, brad)
     P2, W2, A2 = grids.screen_by_weight(P, w, A)
     return np.concatenate([P2, W2[:, None]], axis=1), A2
 
@@ -96,7 +98,7 @@ def final_grid(eng, P, W, A, brad):
 def config(args, npts, nao, **extra):
     c = {"workload": f"{args.natoms}-atom peptide-like chain, cc-pVDZ, {args.functional}, {args.grid} grid",
          "atoms": args.natoms, "n_ao": nao, "grid_points": int(npts), "functional": args.functional,
-         "grid": args.grid, "precision": args.precision, "nocc": args.nocc,
+         "grid": args.grid, "partition": args.partition, "precision": args.precision, "nocc": args.nocc,
          "split_terms": args.split_terms if args.precision != "fp64" else None,
          "l2": "flushed between timed steps (512 MiB write)"}
     c.update(extra)
@@ -259,7 +261,7 @@ def run_reference(args):
     syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed)
     # Becke weights from the CPU restatement: bit for bit the device's (same IEEE operations in
     # the same order), so the weight screen keeps the same points as the GPU arm's grid
-    fac = oracle.becke(xyz, brad, P, A)
+    fac = oracle.ss(xyz, P, A) if args.partition == "SSWeight" else oracle.becke(xyz, brad, P, A)
     P2, W2, A2 = grids.screen_by_weight(P, W * fac, A)
     grid5 = np.concatenate([P2, W2[:, None], A2[:, None]], axis=1)
     per_step = max(200, args.cpu_sample // 2)
@@ -325,7 +327,7 @@ def main():
     engines = {p: XcEngine(device=local, precision=p, split_terms=args.split_terms) for p in precisions}
     for e in engines.values():
         e.set_system(sh)
-    grid4, owner = final_grid(next(iter(engines.values())), P, W, A, brad)
+    grid4, owner = final_grid(next(iter(engines.values())), P, W, A, brad, args.partition)
     npts = len(grid4)
     res = {}
     clk_summary = None

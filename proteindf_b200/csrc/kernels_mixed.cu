@@ -633,7 +633,9 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
     if (!live) return;
     const RowGeom* rg = rows_staged ? rows : g.blk_row_geom + m.ao0;
     const double sc = oz_digit_scale(ept);
+    oz_prefetch_rows<false>(rg, 0, m, rad, q);
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
+        if (mu0 + 16 < m.nb) oz_prefetch_rows<false>(rg + mu0 + 16, mu0 + 16, m, rad, q);  // the next tile's S0
         // shell by shell over the tile's rows (uniform over the CTA), phi = A S0
         double v[16];
         int r = 0;
