@@ -20,6 +20,13 @@ Under torchrun (N > 1) every rank builds its own chain (seed + rank): the units
 are independent molecules, no data-path collective; value = all ranks' points
 / the slowest rank's time (weak scaling).
 
+--shard builds ONE chain over all ranks instead (the reference's distributed
+DfCalcGridX): every rank builds its cost-balanced range of grid blocks, then one
+NCCL all-reduce sums the packed upper triangle of Vxc with Exc and the electron
+count appended. A step is the rank's build (library CUDA events) plus the
+all-reduce (CUDA events on torch's stream), max over ranks; value = the chain's
+points / that time (strong scaling: the total work is fixed).
+
 The same line (N = 1, unless --no-large) carries the two large configurations,
 each built with the FP64 drop-in and the INT8 path, their speed-up and |dExc|:
   chain2000  one 2000-atom chain, cc-pVDZ (~18,600 AOs), B3LYP, USER 75x302 grid with
@@ -70,6 +77,8 @@ def parse():
     ap.add_argument("--no-large", action="store_true", help="leave the 2000-atom chain and the batch out")
     ap.add_argument("--partition", default="Becke", choices=["Becke", "SSWeight"],
                     help="partition weights of the chain workload's grid")
+    ap.add_argument("--shard", action="store_true",
+                    help="one chain over all ranks: block ranges + one NCCL all-reduce (strong scaling)")
     return ap.parse_args()
 
 
@@ -296,6 +305,8 @@ def main():
         return run_reference(args)
     if args.workload != "chain":
         return run_large(args)
+    if args.shard:
+        return run_shard(args)
     import torch
     rank, world, local = dist_env()
     torch.cuda.set_device(local)
@@ -417,6 +428,97 @@ def main():
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.destroy_process_group()
+
+
+def run_shard(args):
+    """One chain over all ranks (ShardedXcEngine): block ranges + one NCCL all-reduce per build."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from proteindf_b200.sharded import ShardedXcEngine, allreduce_partials
+    from proteindf_b200.xc import XcEngine
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    else:  # a group of one, so that the same reduce runs
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            port = so.getsockname()[1]
+        dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1,
+                                timeout=datetime.timedelta(seconds=600))
+    prec = "fp64" if args.precision == "both" else args.precision
+    syms, xyz, sh, P, W, A, PA, brad = workload(args, args.seed)  # the same molecule on every rank
+    dev = f"cuda:{local}"
+    dP = torch.tensor(PA, device=dev)
+    dV = torch.empty_like(dP)
+    flush = torch.empty(512 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    eng = XcEngine(device=local, precision=prec, split_terms=args.split_terms)
+    eng.set_system(sh)
+    grid4, owner = final_grid(eng, P, W, A, brad, args.partition)
+    shard = ShardedXcEngine(eng)
+    shard.set_grid(grid4, owner)
+    npts = len(grid4)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+
+    def step():
+        exc, nel = eng.build_vxc_device(args.functional, dP.data_ptr(), dV.data_ptr())
+        t_build = eng.last_profile()["total_ms"]
+        ev[0].record()
+        _, sc = allreduce_partials(dV, [exc, nel], None)
+        ev[1].record()
+        torch.cuda.synchronize()
+        return t_build, ev[0].elapsed_time(ev[1]), sc
+
+    for _ in range(args.warmup):
+        step()
+    t_build = t_red = 0.0
+    launches = 0
+    dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.zero_()
+            torch.cuda.synchronize()
+            tb, tr, sc = step()
+            t_build += tb
+            t_red += tr
+            launches += eng.last_profile()["launches"]
+        dist.barrier()
+        torch.cuda.synchronize()
+    mine = torch.tensor([(t_build + t_red) / args.steps, t_build / args.steps, t_red / args.steps],
+                        dtype=torch.float64, device=dev)
+    dist.all_reduce(mine, op=dist.ReduceOp.MAX)
+    ms, ms_build, ms_red = (float(x) for x in mine.cpu())
+    # end to end through the sharded host API: P from host memory, Vxc of the whole molecule back on every rank
+    e2e_t = []
+    for _ in range(max(1, args.steps)):
+        dist.barrier()
+        t0 = time.perf_counter()
+        shard.build_vxc(args.functional, PA)
+        e2e_t.append(time.perf_counter() - t0)
+    t_e2e = torch.tensor([float(np.mean(e2e_t))], dtype=torch.float64, device=dev)
+    dist.all_reduce(t_e2e, op=dist.ReduceOp.MAX)
+    nao = sh.nao
+    if rank == 0:
+        b = shard.bounds
+        line = {"metric": METRIC, "value": npts / (ms * 1e-3), "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "strong",
+                "vs_baseline": None, "dtype": "f64" if prec == "fp64" else "int8 fixed-point slices/i32/f64",
+                "data": "synthetic (seeded chain and density, ProteinDF grid recipe)",
+                "config": config(args, npts, nao, sharding="one chain, cost-balanced block ranges, "
+                                 "one NCCL all-reduce of the packed Vxc upper triangle + Exc, N",
+                                 block_ranges=[int(x) for x in b], headline=prec),
+                "exc": float(sc[0]), "nelec_alpha": float(sc[1]),
+                "ms_build_max": ms_build, "ms_allreduce_max": ms_red,
+                "allreduce_bytes": 8 * (nao * (nao + 1) // 2 + 2),
+                "e2e": {"value": npts / float(t_e2e.item()), "unit": UNIT,
+                        "h2d_bytes_per_step": nao * nao * 8, "d2h_bytes_per_step": nao * nao * 8 + 16},
+                "gpu_launches": launches, "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    eng.close()
+    dist.destroy_process_group()
 
 
 def large_workload(args, name, flush):

@@ -268,16 +268,23 @@ __device__ __forceinline__ void becke_poly(double nu, double& p1, double& p2, do
 //   grad_B P_A = s'(nu_AB) dnu grad_B mu_AB P_A / s_AB,
 // where P_i / s_iB is the product of P_i's other factors (taken as 0 when s_iB has
 // underflowed: the term is then below 1e-250).
-template <int T>
+//
+// ROWS_IN_DRAM: the two [natom] rows of every thread live in a scratch array in
+// device memory ([2][natom][gridDim.x * T], a thread's entries strided by the
+// grid's thread count, so a warp's accesses stay coalesced) instead of shared
+// memory; the form for systems whose rows do not fit shared memory.
+template <int T, bool ROWS_IN_DRAM>
 __global__ void __launch_bounds__(T) k_grad_weight(const double* __restrict__ atom_xyz, int natom,
                                                    const double* __restrict__ inv, const double* __restrict__ adj,
                                                    int64_t nslots, const double* __restrict__ px,
                                                    const double* __restrict__ py, const double* __restrict__ pz,
                                                    const int* __restrict__ owner, const double* __restrict__ wsingle,
-                                                   const double* __restrict__ fdens, double* grad) {
+                                                   const double* __restrict__ fdens, double* grad,
+                                                   double* __restrict__ scratch) {
     extern __shared__ double sm[];
-    double* rr = sm;                        // [natom][T]
-    double* Pm = sm + (size_t)natom * T;    // [natom][T]
+    const size_t stride = ROWS_IN_DRAM ? (size_t)gridDim.x * T : (size_t)T;
+    double* rr = ROWS_IN_DRAM ? scratch + (size_t)blockIdx.x * T : sm;  // [natom][stride]
+    double* Pm = rr + (size_t)natom * stride;                            // [natom][stride]
     const int t = threadIdx.x;
     constexpr double kTiny = 1e-250;
     for (int64_t i0 = blockIdx.x * (int64_t)T; i0 < nslots; i0 += (int64_t)gridDim.x * T) {
@@ -290,28 +297,28 @@ __global__ void __launch_bounds__(T) k_grad_weight(const double* __restrict__ at
         for (int m = 0; m < natom; ++m) {
             const double ax = __ldg(atom_xyz + 3 * m) - rx, ay = __ldg(atom_xyz + 3 * m + 1) - ry,
                          az = __ldg(atom_xyz + 3 * m + 2) - rz;
-            rr[m * T + t] = sqrt(ax * ax + ay * ay + az * az);
-            Pm[m * T + t] = 1.0;
+            rr[m * stride + t] = sqrt(ax * ax + ay * ay + az * az);
+            Pm[m * stride + t] = 1.0;
         }
         // partition products, each unordered pair once
         for (int m = 0; m < natom; ++m) {
-            const double rm = rr[m * T + t];
-            double pmv = Pm[m * T + t];
+            const double rm = rr[m * stride + t];
+            double pmv = Pm[m * stride + t];
             for (int n = m + 1; n < natom; ++n) {
-                double mu = (rm - rr[n * T + t]) * __ldg(inv + (size_t)m * natom + n);
+                double mu = (rm - rr[n * stride + t]) * __ldg(inv + (size_t)m * natom + n);
                 const double nu = mu + __ldg(adj + (size_t)m * natom + n) * (1.0 - mu * mu);
                 double p1, p2, p3;
                 becke_poly(nu, p1, p2, p3);
                 pmv *= 0.5 * (1.0 - p3);
-                Pm[n * T + t] *= 0.5 * (1.0 + p3);
+                Pm[n * stride + t] *= 0.5 * (1.0 + p3);
             }
-            Pm[m * T + t] = pmv;
+            Pm[m * stride + t] = pmv;
         }
         double Z = 0.0;
-        for (int m = 0; m < natom; ++m) Z += Pm[m * T + t];
+        for (int m = 0; m < natom; ++m) Z += Pm[m * stride + t];
         const bool act = c != 0.0 && Z > 0.0;
         const double invZ = act ? 1.0 / Z : 0.0;
-        const double PA = Pm[A * T + t];
+        const double PA = Pm[A * stride + t];
         const double omega = PA * invZ;
         double Tx = 0.0, Ty = 0.0, Tz = 0.0;
         for (int B = 0; B < natom; ++B) {
@@ -319,16 +326,16 @@ __global__ void __launch_bounds__(T) k_grad_weight(const double* __restrict__ at
             if (act && B != A) {
                 const double RBx = __ldg(atom_xyz + 3 * B), RBy = __ldg(atom_xyz + 3 * B + 1),
                              RBz = __ldg(atom_xyz + 3 * B + 2);
-                const double rB = rr[B * T + t];
+                const double rB = rr[B * stride + t];
                 const double irB = 1.0 / rB;
                 const double ux = (RBx - rx) * irB, uy = (RBy - ry) * irB, uz = (RBz - rz) * irB;
-                const double PB = Pm[B * T + t];
+                const double PB = Pm[B * stride + t];
                 double zx = 0.0, zy = 0.0, zz = 0.0, ax = 0.0, ay = 0.0, az = 0.0;
                 for (int n = 0; n < natom; ++n) {
                     if (n == B) continue;
                     const double iR = __ldg(inv + (size_t)n * natom + B);
                     const double a = __ldg(adj + (size_t)n * natom + B);
-                    const double mu = (rr[n * T + t] - rB) * iR;
+                    const double mu = (rr[n * stride + t] - rB) * iR;
                     const double nu = mu + a * (1.0 - mu * mu);
                     double p1, p2, p3;
                     becke_poly(nu, p1, p2, p3);
@@ -338,7 +345,7 @@ __global__ void __launch_bounds__(T) k_grad_weight(const double* __restrict__ at
                     const double ex = (RBx - __ldg(atom_xyz + 3 * n)) * iR, ey = (RBy - __ldg(atom_xyz + 3 * n + 1)) * iR,
                                  ez = (RBz - __ldg(atom_xyz + 3 * n + 2)) * iR;
                     const double gmx = -(ux + mu * ex) * iR, gmy = -(uy + mu * ey) * iR, gmz = -(uz + mu * ez) * iR;
-                    const double rn = s_nB > kTiny ? Pm[n * T + t] / s_nB : 0.0;
+                    const double rn = s_nB > kTiny ? Pm[n * stride + t] / s_nB : 0.0;
                     const double rb = s_Bn > kTiny ? PB / s_Bn : 0.0;
                     const double f = k * (rn - rb);
                     zx += f * gmx, zy += f * gmy, zz += f * gmz;
@@ -387,26 +394,38 @@ void launch_grad_point(const GridView& g, const int* ao_atom, const int* owner, 
 int grad_z_plane(bool gga) { return grad_phi_planes(gga); }
 
 // Shared memory per CTA: 2 * natom * T doubles; 64 points per CTA while that fits
-// 200 KiB, else 32.
+// 200 KiB, else 32; beyond 400 atoms the rows live in device memory
+// (grad_weight_scratch_doubles of scratch).
 int grad_weight_max_atoms() { return (int)((200u * 1024u) / (2 * sizeof(double) * 32)); }
+
+namespace {
+constexpr int kWeightDramCtas = 148 * 4;
+}
+
+size_t grad_weight_scratch_doubles(int natom) { return (size_t)2 * natom * kWeightDramCtas * 32; }
 
 void launch_grad_weight(const double* atom_xyz, int natom, const double* inv, const double* adj, int64_t nslots,
                         const double* px, const double* py, const double* pz, const int* owner, const double* wsingle,
-                        const double* fdens, double* grad, cudaStream_t s) {
+                        const double* fdens, double* grad, double* scratch, cudaStream_t s) {
     const size_t smem64 = 2 * sizeof(double) * 64 * (size_t)natom;
-    if (smem64 <= 200u * 1024u) {
+    const size_t smem32 = 2 * sizeof(double) * 32 * (size_t)natom;
+    if (scratch) {
+        int64_t blocks = (nslots + 31) / 32;
+        if (blocks > kWeightDramCtas) blocks = kWeightDramCtas;
+        k_grad_weight<32, true><<<(unsigned)blocks, 32, 0, s>>>(atom_xyz, natom, inv, adj, nslots, px, py, pz, owner,
+                                                               wsingle, fdens, grad, scratch);
+    } else if (smem64 <= 200u * 1024u) {
         int64_t blocks = (nslots + 63) / 64;
         if (blocks > 148 * 16) blocks = 148 * 16;
-        cudaFuncSetAttribute(k_grad_weight<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem64);
-        k_grad_weight<64><<<(unsigned)blocks, 64, smem64, s>>>(atom_xyz, natom, inv, adj, nslots, px, py, pz, owner,
-                                                              wsingle, fdens, grad);
+        cudaFuncSetAttribute(k_grad_weight<64, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem64);
+        k_grad_weight<64, false><<<(unsigned)blocks, 64, smem64, s>>>(atom_xyz, natom, inv, adj, nslots, px, py, pz,
+                                                                     owner, wsingle, fdens, grad, nullptr);
     } else {
-        const size_t smem32 = 2 * sizeof(double) * 32 * (size_t)natom;
         int64_t blocks = (nslots + 31) / 32;
         if (blocks > 148 * 16) blocks = 148 * 16;
-        cudaFuncSetAttribute(k_grad_weight<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32);
-        k_grad_weight<32><<<(unsigned)blocks, 32, smem32, s>>>(atom_xyz, natom, inv, adj, nslots, px, py, pz, owner,
-                                                              wsingle, fdens, grad);
+        cudaFuncSetAttribute(k_grad_weight<32, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem32);
+        k_grad_weight<32, false><<<(unsigned)blocks, 32, smem32, s>>>(atom_xyz, natom, inv, adj, nslots, px, py, pz,
+                                                                     owner, wsingle, fdens, grad, nullptr);
     }
 }
 

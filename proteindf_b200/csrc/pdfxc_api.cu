@@ -214,6 +214,7 @@ void free_grid(pdfxc_ctx* c) {
     c->h_owner.clear();
     dev_free(c->d_owner), dev_free(c->d_ao_atom), dev_free(c->d_grad);
     dev_free(c->d_fdens), dev_free(c->d_wslot), dev_free(c->d_brad), dev_free(c->d_pair);
+    dev_free(c->d_wscratch);
     free_plan(c->gplan);
     free_plan(c->uplan);
     dev_free(c->d_rho_b), dev_free(c->d_blk_sum_b);
@@ -1753,11 +1754,6 @@ pdfxc_status xc_derivatives(pdfxc_ctx* ctx, const char* name, int functional, co
             ctx->err = std::string(name) + ": the weight term needs becke_radius and grad_weight";
             return PDFXC_ERR_ARG;
         }
-        if (w_single && ctx->natom > pdfxc::grad_weight_max_atoms()) {
-            ctx->err = std::string(name) + ": the weight term supports at most " +
-                       std::to_string(pdfxc::grad_weight_max_atoms()) + " atoms";
-            return PDFXC_ERR_UNSUPPORTED;
-        }
         const bool gga = pdfxc::functional_is_gga(functional);
         const int nao = ctx->nao, natom = ctx->natom;
         cudaStream_t s = ctx->stream;
@@ -1806,9 +1802,15 @@ pdfxc_status xc_derivatives(pdfxc_ctx* ctx, const char* name, int functional, co
             // the slots of this context's block range
             const size_t s0 = (size_t)ctx->blk_lo * BLOCK_PTS;
             const int64_t ns = (int64_t)(ctx->blk_hi - ctx->blk_lo) * BLOCK_PTS;
+            // atom rows in device memory above the shared-memory limit (or when the environment asks for
+            // that form: PDFXC_GRAD_WEIGHT_ROWS=dram, used by the tests to compare the two forms)
+            const char* rows_env = std::getenv("PDFXC_GRAD_WEIGHT_ROWS");
+            const bool dram_rows = natom > pdfxc::grad_weight_max_atoms() ||
+                                   (rows_env && std::string(rows_env) == "dram");
+            if (dram_rows) dev_alloc(&ctx->d_wscratch, pdfxc::grad_weight_scratch_doubles(natom));
             pdfxc::launch_grad_weight(ctx->d_atom_xyz, natom, inv, adj, ns, ctx->d_px + s0, ctx->d_py + s0,
                                       ctx->d_pz + s0, ctx->d_owner + s0, ctx->d_wslot + s0, ctx->d_fdens + s0,
-                                      ctx->d_grad + 3 * natom, s);
+                                      ctx->d_grad + 3 * natom, dram_rows ? ctx->d_wscratch : nullptr, s);
             PDFXC_CUDA(cudaGetLastError());
         }
         std::vector<double> g(6 * (size_t)natom);

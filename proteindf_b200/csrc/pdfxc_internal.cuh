@@ -179,6 +179,7 @@ struct pdfxc_ctx {
     double* d_wslot = nullptr;  // [nblk * BLOCK_PTS] single-centre weight per slot
     double* d_brad = nullptr;   // [natom]
     double* d_pair = nullptr;   // [2 * natom^2] Becke pair constants
+    double* d_wscratch = nullptr;  // weight-term atom rows in device memory (above 400 atoms)
 
     // open-shell build (pdfxc_build_vxc_uks): beta-spin buffers beside the alpha ones above
     pdfxc::Plan uplan;
@@ -257,10 +258,13 @@ void launch_grad_point(const GridView& g, const int* ao_atom, const int* owner, 
                        double rho_cut, char* ws, double seed, bool want_z, double* fdens, double* blk_sum,
                        double* grad, cudaStream_t s);
 int grad_z_plane(bool gga);
+// the weight term keeps each point's atom rows in shared memory up to grad_weight_max_atoms()
+// atoms; above that (or when scratch is given) in grad_weight_scratch_doubles(natom) of device memory
 int grad_weight_max_atoms();
+size_t grad_weight_scratch_doubles(int natom);
 void launch_grad_weight(const double* atom_xyz, int natom, const double* inv, const double* adj, int64_t nslots,
                         const double* px, const double* py, const double* pz, const int* owner, const double* wsingle,
-                        const double* fdens, double* grad, cudaStream_t s);
+                        const double* fdens, double* grad, double* scratch, cudaStream_t s);
 
 // becke.cu
 // Stratmann-Scuseria weights (n_atom <= 6000: atoms in shared memory); inv/adj: n_atom^2 scratch each

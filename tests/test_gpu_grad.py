@@ -146,3 +146,61 @@ def test_gradient_needs_owner_atoms(gradwater):
     with pytest.raises(RuntimeError, match="owner"):
         eng.xc_gradient("SVWN", fx["PA"])
     eng.close()
+
+
+def test_weight_term_rows_in_device_memory_match_shared(monkeypatch):
+    """The weight term's two forms (atom rows in shared memory, in device memory) give the same
+    gradient on the same system (1e-12 relative: only the order of the atomic sums differs)."""
+    syms, xyz, pts, ws, own, brad, sh = _small_system(nwater=3, seed=4)
+    PA = 0.5 * systems.density_matrix(sh.nao, 15, seed=5)
+    eng = _engine(sh)
+    eng.set_grid(np.c_[pts, eng.becke_weights(pts, own, ws, brad)], own)
+    _, gw_sm, _ = eng.xc_gradient("BLYP", PA, w_single=ws, becke_radius=brad)
+    monkeypatch.setenv("PDFXC_GRAD_WEIGHT_ROWS", "dram")
+    _, gw_dram, _ = eng.xc_gradient("BLYP", PA, w_single=ws, becke_radius=brad)
+    eng.close()
+    print(f"weight term, rows in shared vs device memory: max diff {np.abs(gw_dram - gw_sm).max():.3e} "
+          f"(max |g| {np.abs(gw_sm).max():.3e})")
+    assert np.abs(gw_dram - gw_sm).max() <= 1e-12 * np.abs(gw_sm).max()
+
+
+def test_weight_term_beyond_400_atoms_finite_difference():
+    """A 420-atom chain (above the shared-memory form's 400 atoms), SVWN, on a seeded sample of
+    4000 rows of its USER 75x302 grid that moves with the atoms: the AO-centre plus weight
+    terms against central differences of the GPU energy (h = 1e-4 bohr, 4 coordinates), and
+    the weight term's sum over atoms (zero: translating the molecule moves its grid along)."""
+    from proteindf_b200.xc import XcEngine
+    syms, xyz = systems.peptide_chain(420, seed=31)
+    Z = [int(z) for z in systems.nuclear_charges(syms)]
+    b = basis.load_basis("cc-pVDZ")
+    pts, ws, own = grids.molecular_grid(xyz, Z, **grids.PRESETS["USER-75x302"])
+    rng = np.random.default_rng(32)
+    rows = np.sort(rng.choice(len(pts), 4000, replace=False))
+    pts, ws, own = pts[rows], ws[rows], own[rows]
+    brad = np.array([grids.BECKE_RADIUS[z] for z in Z])
+    d = pts - xyz[own]
+    sh = basis.ShellTable(syms, xyz, b)
+    PA = 0.5 * systems.density_matrix(sh.nao, 200, seed=33)
+    eng = XcEngine(device=0)
+
+    def energy(X):
+        eng.set_system(basis.ShellTable(syms, X, b))
+        P = X[own] + d
+        eng.set_grid(np.c_[P, eng.becke_weights(P, own, ws, brad)], own)
+        return eng.build_vxc("SVWN", PA)[0]
+
+    energy(xyz)
+    go, gw, _ = eng.xc_gradient("SVWN", PA, w_single=ws, becke_radius=brad)
+    g = go + gw
+    h, worst = 1e-4, 0.0
+    for a, k in zip(rng.choice(own, 4), rng.integers(0, 3, 4)):
+        X1, X2 = xyz.copy(), xyz.copy()
+        X1[a, k] += h
+        X2[a, k] -= h
+        worst = max(worst, abs(g[a, k] - (energy(X1) - energy(X2)) / (2 * h)))
+    eng.close()
+    print(f"420 atoms: max |g - FD| = {worst:.3e} (max |g| {np.abs(g).max():.3e}); "
+          f"|sum of weight term| = {np.abs(gw.sum(axis=0)).max():.3e}")
+    assert np.all(np.isfinite(gw)) and np.abs(gw).max() > 0
+    assert worst < 2e-6 * np.abs(g).max()
+    assert np.abs(gw.sum(axis=0)).max() < 1e-10 * np.abs(gw).max()
