@@ -855,17 +855,18 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
 // (group, 128-row M tile, 64-row N tile): W = phi Z^T (M = 128 AOs mu, N = 64 AOs nu, K = all
 // points of the group's blocks, 128 per block) with the FP64 atomic epilogue.
 //
-// One persistent CTA per SM walks the items (item = blockIdx.x + k gridDim.x) with three
-// roles: warp 0 copies operand slabs into a two-stage ring (cp.async.bulk, mbarriers full /
-// empty), warp 1 issues the MMAs of an item into one of two TMEM accumulator sets (each four
-// int32 accumulators of 64 columns, one per order i + j = 2..5; 512 columns in all) and
-// commits it to tfull[set], and warps 2..9 run the epilogue of the item before, reading set
-// and releasing it through tempty[set]. So one item's epilogue runs under the next item's
-// copies and MMAs. A stage holds the A tile's four digit planes (128 rows x 64 K, canonical
-// no-swizzle K-major layout, 8 KiB each) and the B tile's four digit planes (64 rows x 64 K) as
-// two stacked pairs [B_1; B_2], [B_3; B_4] of 128 rows in the A tiles' layout (8 KiB each): the
-// 64-row half of a packed 128-row tile is four 1 KiB core-matrix groups, and plane b's group kg
-// goes to pair b / 2, rows 64 (b % 2) onward, of the pair's k16 group kg.
+// One persistent CTA per SM takes items from the device-side scheduler below, with three
+// roles: warp 0 claims the items and copies their operand slabs into a ring of S stages
+// (mbarriers full / empty), warp 1 issues the MMAs of an item into one of two TMEM accumulator
+// sets (each four int32 accumulators of 64 columns, one per order i + j = 2..5; 512 columns in
+// all) and commits it to tfull[set], and two epilogue groups of eight warps take alternate
+// items: group h reads set h and releases it through tempty[h]. So one item's epilogue runs
+// under the next items' copies and MMAs. A stage holds the A tile's four digit planes (128 rows
+// x 64 K, canonical no-swizzle K-major layout, 8 KiB each) and the B operand's four planes of
+// 64 rows as two stacked pairs [B_1; B_2], [B_3; B_4] of 128 rows (8 KiB each). RHO: A = the
+// block's phi^T digits, B = the N tile of P_sub, both K-major, one bulk copy each. VXC: A = the
+// M tile of Z', B = the phi^T digits of the N tile's 64 AOs over the slab's 64 points, read
+// MN-major (1 KiB per plane and 16-AO group, one 4-D tensor copy per stage).
 constexpr int OZ_NT = 64;
 // operand ring stages: the Vxc contraction (K = a group's 512 points, eight slabs per item) keeps
 // three in flight, the rho contraction (K = nbp) two beside its larger radial-sum staging
