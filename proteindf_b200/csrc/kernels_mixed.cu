@@ -473,8 +473,13 @@ __device__ __forceinline__ double oz_pow2(int e) {
 // flipping every byte's top bit gives s_i in two's complement. sc = 0 for an all-zero row.
 constexpr double kOzFull = 127.0 * 256.0 * 256.0 * 256.0;
 __device__ __forceinline__ double oz_digit_scale(int e) { return e <= kOzZeroExp ? 0.0 : ldexp(kOzFull, -e); }
+// rint(t) for |t| < 2^31 is the low word of t + 1.5 2^52 (one FP64 add, round to nearest even, the
+// rounding of cvt.rni), so the cut needs no conversion instruction; the product is rounded
+// first, as in rint(v sc).
+constexpr double kOzRound = 6755399441055744.0;  // 1.5 2^52
 __device__ __forceinline__ uint32_t oz_word(double v, double sc) {
-    return ((uint32_t)__double2int_rn(v * sc) + 0x80808080u) ^ 0x80808080u;
+    const int q = __double2loint(__dadd_rn(__dmul_rn(v, sc), kOzRound));
+    return ((uint32_t)q + 0x80808080u) ^ 0x80808080u;
 }
 // Digit-plane layouts in HBM, in the order the contraction stages need them, so that a stage is
 // two bulk copies. Within a 64-K slab the canonical no-swizzle K-major core-matrix order of a
@@ -895,9 +900,15 @@ constexpr uint32_t oz_bar_off() {
 
 // An item's int32 accumulators of orders 2..5 as one exact integer: with weights
 // w_k = 256^(5-k) w_5, sum_k d_k w_k = n w_5 with n = ((d2 256 + d3) 256 + d4) 256 + d5, whose
-// partial sums are integers below 2^53 for K <= OZ_MAX_K, so FP64 forms n exactly.
+// partial sums are integers below 2^53 for K <= OZ_MAX_K: exact in 64-bit integers, and exactly
+// representable in FP64.
 __device__ __forceinline__ double oz_combine(uint32_t d2, uint32_t d3, uint32_t d4, uint32_t d5) {
-    return fma(fma(fma((double)(int)d2, 256.0, (double)(int)d3), 256.0, (double)(int)d4), 256.0, (double)(int)d5);
+    // n in 64-bit integer arithmetic (three wide multiply-adds), then one exact conversion
+    long long n = (long long)(int)d5;
+    n += (long long)(int)d4 * 256;
+    n += (long long)(int)d3 * 65536;
+    n += (long long)(int)d2 * 16777216;
+    return (double)n;
 }
 
 // Work items of the persistent contraction kernels, one int2 each, in a list sorted by
