@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -130,6 +131,51 @@ uint64_t spread3(uint64_t v) {
     v = (v | v << 4) & 0x10c30c30c30c30c3ULL;
     v = (v | v << 2) & 0x1249249249249249ULL;
     return v;
+}
+
+// Host threads for the grid planner: fn(lo, hi, t) over [0, n) in contiguous ranges, one per
+// thread (t = the range's index); small ranges run on the calling thread.
+unsigned host_threads() { return std::min(16u, std::max(1u, std::thread::hardware_concurrency())); }
+
+template <class F>
+void parallel_ranges(int64_t n, int64_t min_per_thread, F&& fn) {
+    const int64_t nt = std::max<int64_t>(1, std::min<int64_t>(host_threads(), n / std::max<int64_t>(1, min_per_thread)));
+    if (nt == 1) {
+        fn((int64_t)0, n, 0);
+        return;
+    }
+    std::vector<std::thread> th;
+    for (int64_t t = 0; t < nt; ++t)
+        th.emplace_back([&, t]() { fn(n * t / nt, n * (t + 1) / nt, (int)t); });
+    for (auto& x : th) x.join();
+}
+
+// std::sort's result (a total order: the keys are distinct) from sorted ranges merged pairwise,
+// each range and each merge on its own thread.
+template <class T>
+void parallel_sort(T* a, int64_t n) {
+    const int64_t nt = std::min<int64_t>(host_threads(), std::max<int64_t>(1, n / (1 << 18)));
+    if (nt <= 1) {
+        std::sort(a, a + n);
+        return;
+    }
+    std::vector<int64_t> cut(nt + 1);
+    for (int64_t t = 0; t <= nt; ++t) cut[t] = n * t / nt;
+    parallel_ranges(nt, 1, [&](int64_t lo, int64_t hi, int) {
+        for (int64_t t = lo; t < hi; ++t) std::sort(a + cut[t], a + cut[t + 1]);
+    });
+    std::vector<T> tmp(n);
+    T *src = a, *dst = tmp.data();
+    for (int64_t w = 1; w < nt; w *= 2) {
+        std::vector<std::thread> th;
+        for (int64_t t = 0; t < nt; t += 2 * w) {
+            const int64_t l = cut[t], m = cut[std::min(nt, t + w)], r = cut[std::min(nt, t + 2 * w)];
+            th.emplace_back([=]() { std::merge(src + l, src + m, src + m, src + r, dst + l); });
+        }
+        for (auto& x : th) x.join();
+        std::swap(src, dst);
+    }
+    if (src != a) std::copy(src, src + n, a);
 }
 
 pdfxc::BasisView basis_view(const pdfxc_ctx* c) {
@@ -458,23 +504,41 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
     ctx->seg_blk.assign(1, 0);
     for (size_t si = 0; si < segs.size(); ++si) {
         const GridSegment& sg = segs[si];
+        const int64_t np = sg.p1 - sg.p0;
+        std::vector<std::array<double, 6>> box(host_threads());
+        parallel_ranges(np, 1 << 16, [&](int64_t a, int64_t b, int t) {
+            std::array<double, 6> bx = {1e300, 1e300, 1e300, -1e300, -1e300, -1e300};
+            for (int64_t i = sg.p0 + a; i < sg.p0 + b; ++i)
+                for (int k = 0; k < 3; ++k)
+                    bx[k] = std::min(bx[k], xyzw[4 * i + k]), bx[3 + k] = std::max(bx[3 + k], xyzw[4 * i + k]);
+            box[t] = bx;
+        });
         double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-        for (int64_t i = sg.p0; i < sg.p1; ++i)
-            for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], xyzw[4 * i + k]), hi[k] = std::max(hi[k], xyzw[4 * i + k]);
+        for (const auto& bx : box)
+            for (int k = 0; k < 3; ++k) lo[k] = std::min(lo[k], bx[k]), hi[k] = std::max(hi[k], bx[3 + k]);
         const double span = std::max({hi[0] - lo[0], hi[1] - lo[1], hi[2] - lo[2], 1e-12});
-        for (int64_t i = sg.p0; i < sg.p1; ++i) {
-            const double* r = xyzw + 4 * i;
-            uint64_t q[3];
-            for (int k = 0; k < 3; ++k) q[k] = (uint64_t)std::min(2097151.0, std::floor((r[k] - lo[k]) / span * 2097151.0));
-            key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, i};
-        }
-        std::sort(key.begin() + sg.p0, key.begin() + sg.p1);
+        parallel_ranges(np, 1 << 16, [&](int64_t a, int64_t b, int) {
+            for (int64_t i = sg.p0 + a; i < sg.p0 + b; ++i) {
+                const double* r = xyzw + 4 * i;
+                uint64_t q[3];
+                for (int k = 0; k < 3; ++k)
+                    q[k] = (uint64_t)std::min(2097151.0, std::floor((r[k] - lo[k]) / span * 2097151.0));
+                key[i] = {spread3(q[0]) | spread3(q[1]) << 1 | spread3(q[2]) << 2, i};
+            }
+        });
+        parallel_sort(key.data() + sg.p0, np);
+        // the points in that order, contiguous, for the sequential cut below
+        std::vector<double> sxyz(3 * (size_t)np);
+        parallel_ranges(np, 1 << 16, [&](int64_t a, int64_t b, int) {
+            for (int64_t i = a; i < b; ++i)
+                for (int k = 0; k < 3; ++k) sxyz[3 * i + k] = xyzw[4 * key[sg.p0 + i].second + k];
+        });
         for (int64_t i0 = sg.p0; i0 < sg.p1;) {
-            const double* r0 = xyzw + 4 * key[i0].second;
+            const double* r0 = &sxyz[3 * (i0 - sg.p0)];
             double blo[3] = {r0[0], r0[1], r0[2]}, bhi[3] = {r0[0], r0[1], r0[2]};
             int64_t i1 = i0 + 1;
             for (; i1 < sg.p1 && i1 - i0 < (int64_t)gb * bp; ++i1) {
-                const double* r = xyzw + 4 * key[i1].second;
+                const double* r = &sxyz[3 * (i1 - sg.p0)];
                 double d2 = 0.0;
                 for (int k = 0; k < 3; ++k) {
                     const double l = std::min(blo[k], r[k]), h = std::max(bhi[k], r[k]);
@@ -501,51 +565,62 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
     if (atom) ctx->h_owner.assign(px.size(), 0);
     std::vector<double> cen(3 * (size_t)ngrp), rad(ngrp);
     ctx->h_meta.assign(nblk, BlockMeta{});
-    for (int gi = 0; gi < ngrp; ++gi) {
-        // the group's centre and radius (screening)
-        const int64_t g0 = runs[grp_blk[gi]].first, g1 = runs[grp_blk[gi + 1] - 1].second;
-        double gc[3] = {0, 0, 0};
-        for (int64_t i = g0; i < g1; ++i)
-            for (int k = 0; k < 3; ++k) gc[k] += xyzw[4 * key[i].second + k];
-        for (int k = 0; k < 3; ++k) gc[k] /= double(g1 - g0);
-        double gr2 = 0.0;
-        for (int64_t i = g0; i < g1; ++i) {
-            const double* r = xyzw + 4 * key[i].second;
-            gr2 = std::max(gr2, (r[0] - gc[0]) * (r[0] - gc[0]) + (r[1] - gc[1]) * (r[1] - gc[1]) +
-                                    (r[2] - gc[2]) * (r[2] - gc[2]));
-        }
-        for (int k = 0; k < 3; ++k) cen[3 * gi + k] = gc[k];
-        rad[gi] = std::sqrt(gr2);
-    }
-    for (int gi = 0; gi < ngrp; ++gi)
-        for (int b = grp_blk[gi]; b < grp_blk[gi + 1]; ++b) {
-            const int64_t i0 = runs[b].first, i1 = runs[b].second;
-            double c[3] = {0, 0, 0};
-            for (int64_t i = i0; i < i1; ++i)
-                for (int k = 0; k < 3; ++k) c[k] += xyzw[4 * key[i].second + k];
-            for (int k = 0; k < 3; ++k) c[k] /= double(i1 - i0);
-            for (int j = 0; j < BLOCK_PTS; ++j) {
-                const size_t slot = (size_t)b * BLOCK_PTS + j;
-                const int64_t i = i0 + j;
-                if (i < i1) {
-                    const double* r = xyzw + 4 * key[i].second;
-                    px[slot] = r[0], py[slot] = r[1], pz[slot] = r[2], pw[slot] = r[3];
-                    ctx->h_src[slot] = key[i].second;
-                    if (atom) ctx->h_owner[slot] = atom[key[i].second];
-                } else {
-                    px[slot] = c[0], py[slot] = c[1], pz[slot] = c[2], pw[slot] = 0.0;
-                    if (atom) ctx->h_owner[slot] = atom[key[i0].second];  // padding: weight 0
-                }
+    parallel_ranges(ngrp, 256, [&](int64_t glo, int64_t ghi, int) {
+        for (int64_t gi = glo; gi < ghi; ++gi) {
+            // the group's centre and radius (screening)
+            const int64_t g0 = runs[grp_blk[gi]].first, g1 = runs[grp_blk[gi + 1] - 1].second;
+            double gc[3] = {0, 0, 0};
+            for (int64_t i = g0; i < g1; ++i)
+                for (int k = 0; k < 3; ++k) gc[k] += xyzw[4 * key[i].second + k];
+            for (int k = 0; k < 3; ++k) gc[k] /= double(g1 - g0);
+            double gr2 = 0.0;
+            for (int64_t i = g0; i < g1; ++i) {
+                const double* r = xyzw + 4 * key[i].second;
+                gr2 = std::max(gr2, (r[0] - gc[0]) * (r[0] - gc[0]) + (r[1] - gc[1]) * (r[1] - gc[1]) +
+                                        (r[2] - gc[2]) * (r[2] - gc[2]));
             }
-            ctx->h_meta[b].npts = (int)(i1 - i0);
-            ctx->h_meta[b].lead = grp_blk[gi];
-            ctx->h_meta[b].gn = grp_blk[gi + 1] - grp_blk[gi];
+            for (int k = 0; k < 3; ++k) cen[3 * gi + k] = gc[k];
+            rad[gi] = std::sqrt(gr2);
+            for (int b = grp_blk[gi]; b < grp_blk[gi + 1]; ++b) {
+                const int64_t i0 = runs[b].first, i1 = runs[b].second;
+                double c[3] = {0, 0, 0};
+                for (int64_t i = i0; i < i1; ++i)
+                    for (int k = 0; k < 3; ++k) c[k] += xyzw[4 * key[i].second + k];
+                for (int k = 0; k < 3; ++k) c[k] /= double(i1 - i0);
+                for (int j = 0; j < BLOCK_PTS; ++j) {
+                    const size_t slot = (size_t)b * BLOCK_PTS + j;
+                    const int64_t i = i0 + j;
+                    if (i < i1) {
+                        const double* r = xyzw + 4 * key[i].second;
+                        px[slot] = r[0], py[slot] = r[1], pz[slot] = r[2], pw[slot] = r[3];
+                        ctx->h_src[slot] = key[i].second;
+                        if (atom) ctx->h_owner[slot] = atom[key[i].second];
+                    } else {
+                        px[slot] = c[0], py[slot] = c[1], pz[slot] = c[2], pw[slot] = 0.0;
+                        if (atom) ctx->h_owner[slot] = atom[key[i0].second];  // padding: weight 0
+                    }
+                }
+                ctx->h_meta[b].npts = (int)(i1 - i0);
+                ctx->h_meta[b].lead = grp_blk[gi];
+                ctx->h_meta[b].gn = grp_blk[gi + 1] - grp_blk[gi];
+            }
         }
+    });
     // 2. per-shell screening radius, then the per-block shell lists
+    // (once per distinct shell: the shells of one element's basis repeat on every such atom)
     std::vector<double> Rs(ctx->nshell);
-    for (int sh = 0; sh < ctx->nshell; ++sh)
-        Rs[sh] = shell_cutoff_radius(ctx->h_sh_l[sh], &ctx->h_p_exp[ctx->h_sh_p0[sh]], &ctx->h_p_coef[ctx->h_sh_p0[sh]],
-                                     ctx->h_sh_nprim[sh], ctx->opt.ao_cutoff);
+    std::map<std::vector<double>, double> radius_of;
+    for (int sh = 0; sh < ctx->nshell; ++sh) {
+        const int p0 = ctx->h_sh_p0[sh], np = ctx->h_sh_nprim[sh];
+        std::vector<double> k = {(double)ctx->h_sh_l[sh]};
+        k.insert(k.end(), ctx->h_p_exp.begin() + p0, ctx->h_p_exp.begin() + p0 + np);
+        k.insert(k.end(), ctx->h_p_coef.begin() + p0, ctx->h_p_coef.begin() + p0 + np);
+        auto it = radius_of.find(k);
+        if (it == radius_of.end())
+            it = radius_of.emplace(k, shell_cutoff_radius(ctx->h_sh_l[sh], &ctx->h_p_exp[p0], &ctx->h_p_coef[p0], np,
+                                                          ctx->opt.ao_cutoff)).first;
+        Rs[sh] = it->second;
+    }
     std::vector<int>&shells = G.shells, &rows = G.rows, &aos = G.aos, &row_info = G.row_info;
     shells.clear(), rows.clear(), aos.clear(), row_info.clear();
     const bool mixed = ctx->opt.precision == PDFXC_PRECISION_MIXED;
@@ -600,8 +675,8 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
         C.ok = true;
     };
     for (size_t si = 0; si < segs.size(); ++si) build_cells(si);
-    std::vector<int> cand_sh;
-    auto candidates = [&](size_t si, int gi) {  // the shells to test for group gi, in shell order
+    // the shells to test for group gi, in shell order
+    auto candidates = [&](size_t si, int gi, std::vector<int>& cand_sh, std::vector<int>& ats) {
         const AtomCells& C = cells[si];
         const GridSegment& sg = segs[si];
         cand_sh.clear();
@@ -615,7 +690,6 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
             c0[k] = std::max(0, (int)std::floor((cen[3 * gi + k] - r - C.lo[k]) / C.edge));
             c1[k] = std::min(C.dim[k] - 1, (int)std::floor((cen[3 * gi + k] + r - C.lo[k]) / C.edge));
         }
-        static thread_local std::vector<int> ats;
         ats.clear();
         for (int x = c0[0]; x <= c1[0]; ++x)
             for (int y = c0[1]; y <= c1[1]; ++y)
@@ -627,38 +701,61 @@ void plan_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* atom
         for (int a : ats)
             for (int sh = C.sh_first[a - C.a0]; sh < C.sh_end[a - C.a0]; ++sh) cand_sh.push_back(sh);
     };
-    for (int gi = 0; gi < ngrp; ++gi) {
-        const size_t si = blk_seg[grp_blk[gi]];
-        const GridSegment& sg = segs[si];
-        (void)sg;
-        const int sh0 = (int)shells.size(), ao0 = (int)aos.size();
-        int row = 0;
-        candidates(si, gi);
-        for (int sh : cand_sh) {
-            const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[sh]];
-            const double d = std::sqrt((A[0] - cen[3 * gi]) * (A[0] - cen[3 * gi]) +
-                                       (A[1] - cen[3 * gi + 1]) * (A[1] - cen[3 * gi + 1]) +
-                                       (A[2] - cen[3 * gi + 2]) * (A[2] - cen[3 * gi + 2]));
-            if (d - rad[gi] > Rs[sh]) continue;
-            shells.push_back(sh);
-            rows.push_back(row);
-            const int L = ctx->h_sh_l[sh], nc = 2 * L + 1;
-            for (int c = 0; c < nc; ++c) {
-                aos.push_back(ctx->h_sh_ao0[sh] + c);
-                row_info.push_back(16 * ((int)shells.size() - 1 - sh0) + L * L + c);
+    // Groups screened on host threads, each range of groups into its own lists (offsets local to
+    // the range), then the lists joined in group order and the offsets moved by the ranges' bases.
+    struct Part {
+        int64_t g0 = 0, g1 = 0;
+        std::vector<int> shells, rows, aos, row_info;
+    };
+    std::vector<Part> parts(host_threads());
+    std::vector<double> blk_flops(nblk, 0.0);
+    parallel_ranges(ngrp, 256, [&](int64_t glo, int64_t ghi, int t) {
+        Part& P = parts[t];
+        P.g0 = glo, P.g1 = ghi;
+        std::vector<int> cand_sh, ats;
+        for (int64_t gi = glo; gi < ghi; ++gi) {
+            const size_t si = blk_seg[grp_blk[gi]];
+            const int sh0 = (int)P.shells.size(), ao0 = (int)P.aos.size();
+            int row = 0;
+            candidates(si, (int)gi, cand_sh, ats);
+            for (int sh : cand_sh) {
+                const double* A = &ctx->h_atom_xyz[3 * ctx->h_sh_atom[sh]];
+                const double d = std::sqrt((A[0] - cen[3 * gi]) * (A[0] - cen[3 * gi]) +
+                                           (A[1] - cen[3 * gi + 1]) * (A[1] - cen[3 * gi + 1]) +
+                                           (A[2] - cen[3 * gi + 2]) * (A[2] - cen[3 * gi + 2]));
+                if (d - rad[gi] > Rs[sh]) continue;
+                P.shells.push_back(sh);
+                P.rows.push_back(row);
+                const int L = ctx->h_sh_l[sh], nc = 2 * L + 1;
+                for (int c = 0; c < nc; ++c) {
+                    P.aos.push_back(ctx->h_sh_ao0[sh] + c);
+                    P.row_info.push_back(16 * ((int)P.shells.size() - 1 - sh0) + L * L + c);
+                }
+                row += nc;
             }
-            row += nc;
+            for (int bb = grp_blk[gi]; bb < grp_blk[gi + 1]; ++bb) {
+                BlockMeta& m = ctx->h_meta[bb];
+                m.sh0 = sh0, m.ao0 = ao0;
+                m.nsh = (int)P.shells.size() - sh0;
+                m.nb = row;
+                m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
+                blk_flops[bb] = 4.0 * double(m.nb) * m.nb * m.npts;
+            }
         }
-        for (int bb = grp_blk[gi]; bb < grp_blk[gi + 1]; ++bb) {
-            BlockMeta& m = ctx->h_meta[bb];
-            m.sh0 = sh0, m.ao0 = ao0;
-            m.nsh = (int)shells.size() - sh0;
-            m.nb = row;
-            m.nbp = mixed ? std::max(128, (row + 127) / 128 * 128) : std::max(64, (row + 63) / 64 * 64);
-            flops += 4.0 * double(m.nb) * m.nb * m.npts;
-            sum_nb += m.nb;
-            G.max_nb = std::max(G.max_nb, m.nb);
-        }
+    });
+    for (const Part& P : parts) {
+        if (P.g1 <= P.g0) continue;
+        const int bsh = (int)shells.size(), bao = (int)aos.size();
+        for (int bb = grp_blk[P.g0]; bb < grp_blk[P.g1]; ++bb) ctx->h_meta[bb].sh0 += bsh, ctx->h_meta[bb].ao0 += bao;
+        shells.insert(shells.end(), P.shells.begin(), P.shells.end());
+        rows.insert(rows.end(), P.rows.begin(), P.rows.end());
+        aos.insert(aos.end(), P.aos.begin(), P.aos.end());
+        row_info.insert(row_info.end(), P.row_info.begin(), P.row_info.end());
+    }
+    for (int bb = 0; bb < nblk; ++bb) {  // in block order, as one sequential sum
+        flops += blk_flops[bb];
+        sum_nb += ctx->h_meta[bb].nb;
+        G.max_nb = std::max(G.max_nb, ctx->h_meta[bb].nb);
     }
     // The INT8 rho contraction runs over K = nbp screened AOs and is exact up to OZ_MAX_K: its
     // order-5 int32 accumulator sums four digit products of at most 128^2 per K index, and the
