@@ -16,6 +16,10 @@ The exchange: each symmetric partial Vxc is packed to its upper triangle
 is then unpacked into both triangles. On an NCCL group the buffer is a CUDA
 tensor on the rank's device (host partials are copied there and back); on a
 gloo group host partials are reduced as CPU tensors.
+
+The distributed-matrix form (build_vxc_local) takes P_A and returns Vxc as each
+rank's block-cyclic piece (BlockCyclic): an all-gather assembles P_A, the rank
+builds its block range, and a reduce-scatter returns the summed pieces.
 """
 import ctypes
 
@@ -121,6 +125,99 @@ def allreduce_vector(v, group=None, device=None):
     return t.cpu().numpy()
 
 
+class BlockCyclic:
+    """The 2-D block-cyclic layout of an n x n matrix over a pr x pc process grid (ScaLAPACK's,
+    square blocks of nb; rank r sits at grid row r // pc, column r % pc). A rank's local
+    matrix holds the global rows i with (i // nb) % pr == its grid row and the global columns j
+    with (j // nb) % pc == its grid column, in ascending order: the reference's
+    TlDenseGeneralMatrix_Scalapack::getLocalMatrix with getRowIndexTable / getColIndexTable
+    (src/libpdf/DfCalcGridX_Parallel.cpp:481-487)."""
+
+    def __init__(self, n, nb, pr, pc):
+        if n < 0 or nb < 1 or pr < 1 or pc < 1:
+            raise ValueError("BlockCyclic: n >= 0, nb >= 1 and a positive process grid")
+        self.n, self.nb, self.pr, self.pc = int(n), int(nb), int(pr), int(pc)
+
+    @property
+    def world(self):
+        return self.pr * self.pc
+
+    def rows(self, rank):
+        idx = np.arange(self.n)
+        return idx[(idx // self.nb) % self.pr == rank // self.pc]
+
+    def cols(self, rank):
+        idx = np.arange(self.n)
+        return idx[(idx // self.nb) % self.pc == rank % self.pc]
+
+    def local_shape(self, rank):
+        return len(self.rows(rank)), len(self.cols(rank))
+
+    def flat_index(self, rank):
+        """Global flat indices (i n + j) of the rank's local matrix, row-major."""
+        return (self.rows(rank)[:, None] * self.n + self.cols(rank)[None, :]).ravel()
+
+
+def gather_block_cyclic(local, layout, group=None, device=None):
+    """The whole n x n matrix from every rank's local block-cyclic piece, on every rank: one
+    all-gather of the pieces (padded to the largest), then each placed at its global indices.
+    `local` is a host array or a CUDA tensor; the result is of the same kind (a CUDA tensor on
+    `device` for an NCCL group)."""
+    import torch
+    dist = _dist()
+    world = dist.get_world_size(group)
+    if world != layout.world:
+        raise ValueError(f"gather_block_cyclic: the layout is for {layout.world} ranks, the group has {world}")
+    cuda = isinstance(local, torch.Tensor) and local.is_cuda
+    nccl = _is_nccl(group)
+    dev = (local.device if cuda else torch.device("cuda", device if device is not None else torch.cuda.current_device())
+           if nccl else torch.device("cpu"))
+    t = local if isinstance(local, torch.Tensor) else torch.from_numpy(np.ascontiguousarray(local, dtype=np.float64))
+    t = t.to(dev, dtype=torch.float64).reshape(-1)
+    m = max(int(np.prod(layout.local_shape(r))) for r in range(world))
+    buf = torch.zeros(m, dtype=torch.float64, device=dev)
+    buf[:t.numel()] = t
+    parts = [torch.empty_like(buf) for _ in range(world)]
+    dist.all_gather(parts, buf, group=group)
+    full = torch.empty(layout.n * layout.n, dtype=torch.float64, device=dev)
+    for r in range(world):
+        fi = torch.as_tensor(layout.flat_index(r), device=dev)
+        full[fi] = parts[r][:fi.numel()]
+    full = full.reshape(layout.n, layout.n)
+    return full if cuda else full.cpu().numpy()
+
+
+def reduce_scatter_block_cyclic(full, layout, group=None, device=None):
+    """Each rank's local block-cyclic piece of the sum over ranks of `full` (n x n partial
+    sums, host array or CUDA tensor). On NCCL one reduce-scatter of the pieces packed in rank
+    order (padded to the largest); on gloo, which has no reduce-scatter, an all-reduce of the
+    matrix and this rank's piece taken from it. Returns the piece (local rows x local columns)
+    in the input's kind."""
+    import torch
+    dist = _dist()
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    if world != layout.world:
+        raise ValueError(f"reduce_scatter_block_cyclic: the layout is for {layout.world} ranks, the group has {world}")
+    cuda = isinstance(full, torch.Tensor) and full.is_cuda
+    shape = layout.local_shape(rank)
+    if _is_nccl(group):
+        dev = full.device if cuda else torch.device("cuda", device if device is not None else torch.cuda.current_device())
+        f = (full if cuda else torch.from_numpy(np.ascontiguousarray(full, dtype=np.float64))).to(dev).reshape(-1)
+        m = max(int(np.prod(layout.local_shape(r))) for r in range(world))
+        send = torch.zeros(world * m, dtype=torch.float64, device=dev)
+        for r in range(world):
+            fi = torch.as_tensor(layout.flat_index(r), device=dev)
+            send[r * m:r * m + fi.numel()] = f[fi]
+        out = torch.empty(m, dtype=torch.float64, device=dev)
+        dist.reduce_scatter_tensor(out, send, group=group)
+        piece = out[:shape[0] * shape[1]].reshape(shape)
+        return piece if cuda else piece.cpu().numpy()
+    f = (full.cpu() if cuda else torch.from_numpy(np.ascontiguousarray(full, dtype=np.float64)).clone()).reshape(-1)
+    dist.all_reduce(f, group=group)
+    piece = f[torch.as_tensor(layout.flat_index(rank))].reshape(shape)
+    return piece.to(full.device) if cuda else piece.numpy()
+
+
 class ShardedXcEngine:
     """Wraps an XcEngine of this rank's GPU; rank and world come from torch.distributed."""
 
@@ -156,6 +253,20 @@ class ShardedXcEngine:
         exc, nel = self.eng.build_vxc_device(functional, PA.data_ptr(), V.data_ptr(), incremental=incremental)
         _, sc = allreduce_partials(V, [exc, nel], self.group)
         return sc[0], sc[1]
+
+    def build_vxc_local(self, functional, PA_local, layout, incremental=False):
+        """The distributed-matrix form (the reference's DfCalcGridX_Parallel with ScaLAPACK
+        matrices, src/libpdf/DfCalcGridX_Parallel.cpp:481-664): P_A arrives as this rank's
+        block-cyclic piece and Vxc leaves as this rank's piece. P_A is all-gathered, the rank
+        builds its range of grid blocks, and one reduce-scatter sums the partial Vxc into the
+        pieces (the reference instead evaluates every grid point on every rank for its local
+        rows and columns and all-reduces the grid matrix's densities). Returns (exc,
+        nelec_alpha, Vxc piece)."""
+        PA = gather_block_cyclic(PA_local, layout, self.group, self._device)
+        exc, nel, V = self.eng.build_vxc(functional, PA, incremental=incremental)
+        piece = reduce_scatter_block_cyclic(V, layout, self.group, self._device)
+        sc = allreduce_vector(np.array([exc, nel]), self.group, self._device)
+        return sc[0], sc[1], piece
 
     def build_vxc_uks(self, functional, PA, PB, incremental=False):
         exc, na, nb, FA, FB = self.eng.build_vxc_uks(functional, PA, PB, incremental=incremental)

@@ -97,6 +97,12 @@ def test_nccl_front_end_world_one(water2):
         eu, na, nb, FA, FB = sh.build_vxc_uks("BLYP", uks["PA"], uks["PB"])
         assert abs(eu - uks["BLYP_exc"][0]) < 1e-8
         assert np.abs(FA - uks["BLYP_vxc_a"]).max() < 1e-7 and np.abs(FB - uks["BLYP_vxc_b"]).max() < 1e-7
+        # the distributed-matrix form: the local piece of a 1 x 1 process grid is the whole matrix
+        from proteindf_b200.sharded import BlockCyclic
+        layout = BlockCyclic(water2["PA"].shape[0], 8, 1, 1)
+        el, nl, piece = sh.build_vxc_local("B3LYP", water2["PA"], layout)
+        assert abs(el - water2["B3LYP_exc"][0]) < 1e-8
+        assert np.abs(piece - water2["B3LYP_vxc"]).max() < 1e-7
         go, gw, eg = sh.xc_gradient("SVWN", water2["PA"])
         go1, _, eg1 = eng.xc_gradient("SVWN", water2["PA"])
         # two builds differ by the order of their FP64 atomic additions only
