@@ -204,8 +204,8 @@ pdfxc_status pdfxc_set_rho(pdfxc_ctx* ctx, int gga, const double* rho);
  * stored densities and build graphs are untouched. No weights, no functional. */
 pdfxc_status pdfxc_density(pdfxc_ctx* ctx, const double* P, int64_t npts, const double* xyz, double* rho);
 
-/* Open-shell build (FP64 path only; a mixed-precision context returns
- * PDFXC_ERR_UNSUPPORTED). Replaces the UKS overloads
+/* Open-shell build, on the FP64 path and on the INT8 digits (split_terms 10; the
+ * BF16 split returns PDFXC_ERR_UNSUPPORTED). Replaces the UKS overloads
  * DfCalcGridX::calcXCIntegForFockAndEnergy(P_A, P_B, functional, F_A, F_B)
  * (src/libpdf/DfCalcGridX.cpp:2292-2303 LDA, :2317-2328 GGA): calcRho_*_part
  * on both spin densities (:1891-1922, :1963-2016) and buildVxc(gridMatrix,

@@ -200,6 +200,61 @@ __global__ void __launch_bounds__(BLOCK_PTS) k_functional_mixed(GridView g, int 
     }
 }
 
+// The open shell (DfCalcGridX::calcRho_*_part(P_A, P_B, ...) and buildVxc(gridMatrix, functional,
+// F_A, F_B), src/libpdf/DfCalcGridX.cpp:1891-1922, :1963-2016, :2093-2135, :2195-2278): both
+// spins' rho accumulators -> the open-shell functional -> each spin's Vxc coefficients
+// (0.5 w vrho_s and c_s = w (2 vgamma_ss + vgamma_AB) grad rho_s, as the FP64 open-shell
+// kernel); a point contributes when rho_A or rho_B exceeds the cut-off.
+template <bool GGA>
+__global__ void __launch_bounds__(BLOCK_PTS) k_functional_mixed_uks(GridView g, int blk0, int fn, int incremental,
+                                                                    double rho_cut, const double* rho_acc_a,
+                                                                    const double* rho_acc_b, double* rho_store_a,
+                                                                    double* rho_store_b, double* coef_a, double* coef_b,
+                                                                    double* blk_sum, double* blk_sum_b) {
+    const int blk = blk0 + blockIdx.x;
+    const int p = threadIdx.x;
+    const size_t gp = (size_t)blk * BLOCK_PTS + p;
+    double d[2][4];
+    const double* acc[2] = {rho_acc_a + gp * 4, rho_acc_b + gp * 4};
+    double* st[2] = {rho_store_a + gp * 4, rho_store_b + gp * 4};
+#pragma unroll
+    for (int sp = 0; sp < 2; ++sp) {
+        d[sp][0] = acc[sp][0], d[sp][1] = 2.0 * acc[sp][1], d[sp][2] = 2.0 * acc[sp][2], d[sp][3] = 2.0 * acc[sp][3];
+        if (incremental)
+            for (int k = 0; k < 4; ++k) d[sp][k] += st[sp][k];
+        for (int k = 0; k < 4; ++k) st[sp][k] = d[sp][k];
+    }
+    const double w = g.pw[gp];
+    const double ra = d[0][0], rb = d[1][0];
+    double e = 0.0, a_a = 0.0, a_b = 0.0, ca[3] = {0.0, 0.0, 0.0}, cb[3] = {0.0, 0.0, 0.0};
+    if (w != 0.0 && (ra > rho_cut || rb > rho_cut)) {
+        const double gaa = d[0][1] * d[0][1] + d[0][2] * d[0][2] + d[0][3] * d[0][3];
+        const double gbb = d[1][1] * d[1][1] + d[1][2] * d[1][2] + d[1][3] * d[1][3];
+        const double gab = d[0][1] * d[1][1] + d[0][2] * d[1][2] + d[0][3] * d[1][3];
+        const XcOut o = eval_functional(fn, ra, rb, gaa, gab, gbb);
+        e = w * o.f;
+        a_a = 0.5 * w * o.va, a_b = 0.5 * w * o.vb;
+        if (GGA) {
+            const double cca = w * (2.0 * o.vgaa + o.vgab), ccb = w * (2.0 * o.vgbb + o.vgab);
+            for (int k = 0; k < 3; ++k) ca[k] = cca * d[0][1 + k], cb[k] = ccb * d[1][1 + k];
+        }
+    }
+    double* fa = coef_a + gp * 4;
+    double* fb = coef_b + gp * 4;
+    fa[0] = a_a, fa[1] = ca[0], fa[2] = ca[1], fa[3] = ca[2];
+    fb[0] = a_b, fb[1] = cb[0], fb[2] = cb[1], fb[3] = cb[2];
+    __shared__ double red[3][BLOCK_PTS / 32];
+    const double se = warp_sum_m(e), sna = warp_sum_m(w * ra), snb = warp_sum_m(w * rb);
+    if ((p & 31) == 0) red[0][p >> 5] = se, red[1][p >> 5] = sna, red[2][p >> 5] = snb;
+    __syncthreads();
+    if (p == 0) {
+        double E = 0.0, NA = 0.0, NB = 0.0;
+        for (int i = 0; i < BLOCK_PTS / 32; ++i) E += red[0][i], NA += red[1][i], NB += red[2][i];
+        blk_sum[2 * blk] = E, blk_sum[2 * blk + 1] = NA;
+        blk_sum_b[2 * blk] = NB, blk_sum_b[2 * blk + 1] = 0.0;
+    }
+}
+
 // Z[nu][p] = 0.5 w vrho phi + c . grad phi, split and packed (rows = AOs, K = points).
 template <bool GGA>
 __global__ void __launch_bounds__(256) k_pack_z(GridView g, int blk0, const double* __restrict__ coef, char* ws) {
@@ -1437,14 +1492,36 @@ void oz_rho(const MixedArgs& a, cudaStream_t s) {
 }
 
 void oz_functional(const MixedArgs& a, cudaStream_t s) {
-    if (functional_is_gga(a.fn)) {
+    if (functional_is_gga(a.fn))
         k_functional_mixed<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
                                                               a.rho_store, a.coef, a.blk_sum);
+    else
+        k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
+                                                               a.rho_store, a.coef, a.blk_sum);
+    oz_pack_z(a, s);
+}
+
+void oz_pack_p(const MixedArgs& a, cudaStream_t s) {
+    k_pack_p_oz<<<a.ngrp, 256, 0, s>>>(a.g, a.p_words, a.nao, a.grp, a.p_rowexp, a.ws);
+}
+
+void oz_functional_uks(const MixedArgs& a, const double* rho_acc_b, double* rho_store_b, double* coef_b,
+                       double* blk_sum_b, cudaStream_t s) {
+    if (functional_is_gga(a.fn))
+        k_functional_mixed_uks<true><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut,
+                                                                  a.rho_acc, rho_acc_b, a.rho_store, rho_store_b,
+                                                                  a.coef, coef_b, a.blk_sum, blk_sum_b);
+    else
+        k_functional_mixed_uks<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut,
+                                                                   a.rho_acc, rho_acc_b, a.rho_store, rho_store_b,
+                                                                   a.coef, coef_b, a.blk_sum, blk_sum_b);
+}
+
+void oz_pack_z(const MixedArgs& a, cudaStream_t s) {
+    if (functional_is_gga(a.fn)) {
         cudaFuncSetAttribute(k_pack_z_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGroupTileBytes);
         k_pack_z_group<true><<<a.ngrp, kGroupPts, kGroupTileBytes, s>>>(a.g, a.grp, a.coef, a.ws);
     } else {
-        k_functional_mixed<false><<<a.nblk, BLOCK_PTS, 0, s>>>(a.g, a.blk0, a.fn, a.incremental, a.rho_cut, a.rho_acc,
-                                                               a.rho_store, a.coef, a.blk_sum);
         cudaFuncSetAttribute(k_pack_z_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kGroupTileBytes);
         k_pack_z_group<false><<<a.ngrp, kGroupPts, kGroupTileBytes, s>>>(a.g, a.grp, a.coef, a.ws);
     }

@@ -1439,6 +1439,91 @@ void collect_profile(pdfxc_ctx* ctx) {
     p.finish_ms = dt(ctx->stage_ev[last - 1], ctx->stage_ev[last]);
 }
 
+// The open-shell build's launches on ctx->stream (FP64 path): per chunk phi (and grad phi), X_A
+// and X_B, the open-shell functional with Z_A and Z_B in place of X, and the two Vxc
+// contractions. P_A, P_B in ctx->d_P, d_P_b; Vacc, Vacc_b zeroed. Returns the launch count.
+int64_t enqueue_uks_fp64(pdfxc_ctx* ctx, int functional, bool incremental) {
+    const bool gga = pdfxc::functional_is_gga(functional);
+    const int nao = ctx->nao, nphi = gga ? 4 : 1;
+    cudaStream_t s = ctx->stream;
+    ensure_plan(ctx, ctx->uplan, nphi + 2);  // phi planes, X_A, X_B
+    pdfxc::GridView gv = grid_view(ctx);
+    gv.meta = ctx->uplan.d_meta;
+    const pdfxc::BasisView bv = basis_view(ctx);
+    char* ws = static_cast<char*>(ctx->uplan.d_ws);
+    int64_t launches = 0;
+    for (const Chunk& c : ctx->uplan.chunks) {
+        const int b0 = std::max(c.b0, ctx->blk_lo), nb = std::min(c.b1, ctx->blk_hi) - b0;
+        if (nb <= 0) continue;
+        pdfxc::launch_ao_eval(bv, gv, b0, nb, gga, ws, 0, s);
+        pdfxc::launch_gemm_x_planes(gv, ctx->d_P, nao, b0, nb, c.max_nbp, 0, nphi, 1, ws, s);
+        pdfxc::launch_gemm_x_planes(gv, ctx->d_P_b, nao, b0, nb, c.max_nbp, 0, nphi + 1, 1, ws, s);
+        pdfxc::launch_rho_functional_uks(gv, b0, nb, functional, incremental, ctx->opt.rho_cutoff, ws, ctx->d_rho,
+                                         ctx->d_rho_b, ctx->d_blk_sum, ctx->d_blk_sum_b, s);
+        pdfxc::launch_gemm_v_plane(gv, b0, nb, c.max_nbp, nphi, ws, ctx->d_Vacc, nao, s);
+        pdfxc::launch_gemm_v_plane(gv, b0, nb, c.max_nbp, nphi + 1, ws, ctx->d_Vacc_b, nao, s);
+        PDFXC_CUDA(cudaGetLastError());
+        launches += 6;
+    }
+    return launches;
+}
+
+// The open-shell build on the INT8 path, per chunk: the phi digits and P_A's P_sub digits, the
+// rho_A contraction, P_B's P_sub digits over the same region, the rho_B contraction, the
+// open-shell functional (both spins' coefficients), then per spin its Z' digits and its Vxc
+// contraction. The beta spin's P words, accumulators, coefficients and work counters have their
+// own buffers; the workspace of the closed-shell build is reused. Returns the launch count.
+int64_t enqueue_uks_int8(pdfxc_ctx* ctx, int functional, bool incremental) {
+    cudaStream_t s = ctx->stream;
+    const int nao = ctx->nao;
+    const size_t n2 = (size_t)nao * nao, nslot = (size_t)ctx->nblk * BLOCK_PTS;
+    if (!ctx->d_p_words_b) dev_alloc(&ctx->d_p_words_b, n2);
+    if (!ctx->d_p_rowexp_b) dev_alloc(&ctx->d_p_rowexp_b, (size_t)nao);
+    if (!ctx->d_rho_acc_b) dev_alloc(&ctx->d_rho_acc_b, nslot * 4);
+    if (!ctx->d_coef_b) dev_alloc(&ctx->d_coef_b, nslot * 4);
+    if (!ctx->d_counters_b) dev_alloc(&ctx->d_counters_b, 2 * ctx->chunks.size());
+    memset_async(ctx->d_rho_acc, sizeof(double) * nslot * 4, s);
+    memset_async(ctx->d_rho_acc_b, sizeof(double) * nslot * 4, s);
+    PDFXC_CUDA(cudaMemsetAsync(ctx->d_err, 0, sizeof(int), s));
+    PDFXC_CUDA(cudaMemsetAsync(ctx->d_counters, 0, sizeof(int) * 2 * ctx->chunks.size(), s));
+    PDFXC_CUDA(cudaMemsetAsync(ctx->d_counters_b, 0, sizeof(int) * 2 * ctx->chunks.size(), s));
+    pdfxc::oz_p_digits(ctx->d_P, nao, ctx->d_row_cols, ctx->d_p_rowexp, ctx->d_p_words, s);
+    pdfxc::oz_p_digits(ctx->d_P_b, nao, ctx->d_row_cols, ctx->d_p_rowexp_b, ctx->d_p_words_b, s);
+    int64_t launches = 2;
+    const pdfxc::BasisView bv = basis_view(ctx);
+    const pdfxc::GridView gv = grid_view(ctx);
+    char* ws = static_cast<char*>(ctx->d_ws);
+    for (size_t ci = 0; ci < ctx->chunks.size(); ++ci) {
+        const Chunk& c = ctx->chunks[ci];
+        const int cb0 = std::max(c.b0, ctx->blk_lo), cn = std::min(c.b1, ctx->blk_hi) - cb0;
+        if (cn <= 0) continue;
+        const int g_lo = (int)(std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), cb0) - ctx->h_grp.begin());
+        const int g_hi = (int)(std::lower_bound(ctx->h_grp.begin(), ctx->h_grp.end(), cb0 + cn) - ctx->h_grp.begin());
+        pdfxc::MixedArgs a{bv, gv, cb0, cn, c.max_nbp, functional, incremental ? 1 : 0, ctx->opt.split_terms, nao,
+                           ctx->opt.rho_cutoff, ctx->d_P, ws, ctx->d_rho_acc, ctx->d_rho, ctx->d_coef, ctx->d_blk_sum,
+                           ctx->d_Vacc, ctx->d_err, ctx->d_grp + g_lo, g_hi - g_lo, ctx->d_p_rowexp,
+                           ctx->d_p_words, ctx->d_items + ctx->items_off_rho[ci], ctx->items_n_rho[ci],
+                           ctx->d_items + ctx->items_off_vxc[ci], ctx->items_n_vxc[ci], ctx->d_counters + 2 * ci,
+                           ctx->tuned_stages, ctx->phi_map_ok ? &ctx->phi_map : nullptr};
+        pdfxc::MixedArgs b = a;  // the beta spin
+        b.P = ctx->d_P_b, b.rho_acc = ctx->d_rho_acc_b, b.rho_store = ctx->d_rho_b, b.coef = ctx->d_coef_b;
+        b.Vacc = ctx->d_Vacc_b, b.p_rowexp = ctx->d_p_rowexp_b, b.p_words = ctx->d_p_words_b;
+        b.counters = ctx->d_counters_b + 2 * ci;
+        pdfxc::oz_prepare(a, s);
+        pdfxc::oz_rho(a, s);
+        pdfxc::oz_pack_p(b, s);
+        pdfxc::oz_rho(b, s);
+        pdfxc::oz_functional_uks(a, b.rho_acc, b.rho_store, b.coef, ctx->d_blk_sum_b, s);
+        pdfxc::oz_pack_z(a, s);
+        pdfxc::oz_vxc(a, s);
+        pdfxc::oz_pack_z(b, s);
+        pdfxc::oz_vxc(b, s);
+        PDFXC_CUDA(cudaGetLastError());
+        launches += 9;
+    }
+    return launches;
+}
+
 // One build on ctx->stream. The sequence of launches is captured once into a
 // CUDA graph per (functional, incremental, density pointer) and replayed.
 void run_build(pdfxc_ctx* ctx, int fn, const double* d_PA, bool incremental) {
@@ -1703,8 +1788,10 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
             ctx->err = "pdfxc_build_vxc_uks: unknown functional or null pointer";
             return PDFXC_ERR_ARG;
         }
-        if (ctx->opt.precision != PDFXC_PRECISION_FP64) {
-            ctx->err = "pdfxc_build_vxc_uks: the open-shell build runs on the FP64 path only";
+        const bool int8 = ctx->opt.precision == PDFXC_PRECISION_MIXED;
+        if (int8 && ctx->opt.split_terms != 10) {
+            ctx->err = "pdfxc_build_vxc_uks: the open-shell build runs on the FP64 path and on the INT8 digits "
+                       "(split_terms 10), not on the BF16 split";
             return PDFXC_ERR_UNSUPPORTED;
         }
         const bool gga = pdfxc::functional_is_gga(functional);
@@ -1725,29 +1812,13 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
             PDFXC_CUDA(cudaMemsetAsync(ctx->d_rho_b, 0, sizeof(double) * (size_t)ctx->nblk * BLOCK_PTS * 4, s));
         }
         if (!ctx->d_blk_sum_b) dev_alloc(&ctx->d_blk_sum_b, (size_t)ctx->nblk * 2);
-        const int nphi = gga ? 4 : 1;
-        ensure_plan(ctx, ctx->uplan, nphi + 2);  // phi planes, X_A, X_B
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P, PA, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
         PDFXC_CUDA(cudaMemcpyAsync(ctx->d_P_b, PB, n2 * sizeof(double), cudaMemcpyHostToDevice, s));
         memset_async(ctx->d_Vacc, n2 * sizeof(double), s);
         memset_async(ctx->d_Vacc_b, n2 * sizeof(double), s);
-        pdfxc::GridView gv = grid_view(ctx);
-        gv.meta = ctx->uplan.d_meta;
-        const pdfxc::BasisView bv = basis_view(ctx);
-        char* ws = static_cast<char*>(ctx->uplan.d_ws);
         PDFXC_CUDA(cudaEventRecord(ctx->ev[0], s));
-        for (const Chunk& c : ctx->uplan.chunks) {
-            const int b0 = std::max(c.b0, ctx->blk_lo), nb = std::min(c.b1, ctx->blk_hi) - b0;
-            if (nb <= 0) continue;
-            pdfxc::launch_ao_eval(bv, gv, b0, nb, gga, ws, 0, s);
-            pdfxc::launch_gemm_x_planes(gv, ctx->d_P, nao, b0, nb, c.max_nbp, 0, nphi, 1, ws, s);
-            pdfxc::launch_gemm_x_planes(gv, ctx->d_P_b, nao, b0, nb, c.max_nbp, 0, nphi + 1, 1, ws, s);
-            pdfxc::launch_rho_functional_uks(gv, b0, nb, functional, incremental != 0, ctx->opt.rho_cutoff, ws,
-                                             ctx->d_rho, ctx->d_rho_b, ctx->d_blk_sum, ctx->d_blk_sum_b, s);
-            pdfxc::launch_gemm_v_plane(gv, b0, nb, c.max_nbp, nphi, ws, ctx->d_Vacc, nao, s);
-            pdfxc::launch_gemm_v_plane(gv, b0, nb, c.max_nbp, nphi + 1, ws, ctx->d_Vacc_b, nao, s);
-            PDFXC_CUDA(cudaGetLastError());
-        }
+        const int64_t launches = int8 ? enqueue_uks_int8(ctx, functional, incremental != 0)
+                                      : enqueue_uks_fp64(ctx, functional, incremental != 0);
         const size_t lo = ctx->blk_lo;
         const int nr = ctx->blk_hi - ctx->blk_lo;
         pdfxc::launch_finish(ctx->d_Vacc, ctx->d_V, nao, ctx->d_blk_sum + 2 * lo, nr, ctx->d_scalars, s);
@@ -1758,10 +1829,14 @@ pdfxc_status pdfxc_build_vxc_uks(pdfxc_ctx* ctx, int functional, const double* P
         PDFXC_CUDA(cudaMemcpyAsync(sa, ctx->d_scalars, sizeof(sa), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaMemcpyAsync(sb, ctx->d_scalars_b, sizeof(sb), cudaMemcpyDeviceToHost, s));
         PDFXC_CUDA(cudaStreamSynchronize(s));
+        if (int code = int8 ? device_error(ctx) : 0) {
+            ctx->err = "pdfxc_build_vxc_uks: a bounded device wait expired (code " + std::to_string(code) + ")";
+            return PDFXC_ERR_TIMEOUT;
+        }
         pdfxc_profile& p = ctx->last_profile;
         p = pdfxc_profile{};
         PDFXC_CUDA(cudaEventElapsedTime(&p.total_ms, ctx->ev[0], ctx->ev[1]));
-        p.launches = 6 * (int64_t)ctx->uplan.chunks.size() + 4;
+        p.launches = launches + 4;
         accumulate_to_host(ctx, ctx->d_V, FA, n2);
         accumulate_to_host(ctx, ctx->d_V_b, FB, n2);
         if (exc) *exc = sa[0];

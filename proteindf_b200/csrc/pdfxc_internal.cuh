@@ -187,6 +187,12 @@ struct pdfxc_ctx {
     double* d_blk_sum_b = nullptr;  // [nblk * 2]: N_beta, 0
     double* d_scalars_b = nullptr;  // [2]
     double *d_P_b = nullptr, *d_V_b = nullptr, *d_Vacc_b = nullptr;  // n_ao^2 each
+    // INT8 path: the beta spin's digit words of P (n_ao^2) and row exponents, rho accumulators and
+    // Vxc coefficients (nblk * BLOCK_PTS * 4 each), and work counters (two per chunk)
+    uint32_t* d_p_words_b = nullptr;
+    int* d_p_rowexp_b = nullptr;
+    double *d_rho_acc_b = nullptr, *d_coef_b = nullptr;
+    int* d_counters_b = nullptr;
     int rho_spin = 0;               // the stored densities: 1 closed shell, 2 open shell
 
     // the grid as given (for re-blocking: pdfxc_autotune): its segments (one per molecule of a batch)
@@ -428,5 +434,12 @@ void oz_prepare(const MixedArgs& a, cudaStream_t s);
 void oz_rho(const MixedArgs& a, cudaStream_t s);
 void oz_functional(const MixedArgs& a, cudaStream_t s);
 void oz_vxc(const MixedArgs& a, cudaStream_t s);
+// the open shell on the INT8 path: P_sub's digits alone (the phi digits stay), the open-shell
+// functional from both spins' rho accumulators (coefficients of each spin, block sums E and
+// N_alpha into a.blk_sum, N_beta and 0 into blk_sum_b), and the Z' digits of one spin
+void oz_pack_p(const MixedArgs& a, cudaStream_t s);
+void oz_functional_uks(const MixedArgs& a, const double* rho_acc_b, double* rho_store_b, double* coef_b,
+                       double* blk_sum_b, cudaStream_t s);
+void oz_pack_z(const MixedArgs& a, cudaStream_t s);
 
 }  // namespace pdfxc
