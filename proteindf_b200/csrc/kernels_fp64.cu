@@ -82,10 +82,15 @@ __device__ __forceinline__ void dmma(double& d0, double& d1, double a, double b)
 // phi and its three derivatives -> X and Y_x, Y_y, Y_z).
 constexpr int GX_BM = 64, GX_BK = 16, GX_AS = GX_BK + 2, GX_BS = BLOCK_PTS + 4;
 __global__ void __launch_bounds__(256, 2) k_gemm_x(GridView g, const double* __restrict__ P, int nao,
-                                                int blk0, char* ws, int src0, int dst0) {
-    const int blk = blk0 + blockIdx.y;
+                                                int blk0, char* ws, int src0, int dst0, int64_t t0) {
+    int blk, m0;
+    if (g.xtiles) {  // one CTA per tile of the list
+        const int2 it = g.xtiles[t0 + blockIdx.x];
+        blk = it.x, m0 = it.y * GX_BM;
+    } else {
+        blk = blk0 + blockIdx.y, m0 = blockIdx.x * GX_BM;
+    }
     const BlockMeta m = g.meta[blk];
-    const int m0 = blockIdx.x * GX_BM;
     if (m0 >= m.nbp) return;
     const size_t plane = (size_t)m.nbp * BLOCK_PTS;
     const double* phi = reinterpret_cast<const double*>(ws + m.ws) + (size_t)(src0 + blockIdx.z) * plane;
@@ -451,11 +456,16 @@ __global__ void __launch_bounds__(BLOCK_PTS, 6) k_z_rad(BasisView bas, GridView 
 // steps of 16, 4 warps as 2 x 2 warp tiles of 32 x 32 (4 x 4 DMMA tiles). Z was formed by
 // k_rho_functional in the place of X; both tiles are staged as [row][k] with 128-byte rows.
 constexpr int GV_B = 64, GV_BK = 16, GV_AS = GV_BK + 2;
-__global__ void __launch_bounds__(128) k_gemm_v(GridView g, int blk0, char* ws, int zplane, double* Vacc, int nao,
-                                                int tiles) {
-    const int blk = blk0 + blockIdx.y;
+__global__ void __launch_bounds__(128, 3) k_gemm_v(GridView g, int blk0, char* ws, int zplane, double* Vacc, int nao,
+                                                int tiles, int64_t t0) {
+    int blk, tm, tn;
+    if (g.vtiles) {  // one CTA per tile of the list
+        const int2 it = g.vtiles[t0 + blockIdx.x];
+        blk = it.x, tm = it.y >> 16, tn = it.y & 0xFFFF;
+    } else {
+        blk = blk0 + blockIdx.y, tm = blockIdx.x / tiles, tn = blockIdx.x % tiles;
+    }
     const BlockMeta m = g.meta[blk];
-    const int tm = blockIdx.x / tiles, tn = blockIdx.x % tiles;
     const int m0 = tm * GV_B, n0 = tn * GV_B;
     if (m0 >= m.nbp || n0 >= m.nbp) return;
     const double* phi = reinterpret_cast<const double*>(ws + m.ws);
@@ -649,15 +659,19 @@ void launch_ao_eval(const BasisView& b, const GridView& g, int blk0, int nblk, b
 
 void launch_gemm_x(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp,
                           int nplanes, char* ws, cudaStream_t s) {
-    dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk);
     // X follows the phi planes (1 for LDA, 4 with gradients)
-    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, 0, nplanes);
+    launch_gemm_x_planes(g, P, nao, blk0, nblk, max_nbp, 0, nplanes, 1, ws, s);
 }
 
 void launch_gemm_x_planes(const GridView& g, const double* P, int nao, int blk0, int nblk, int max_nbp, int src0,
                           int dst0, int nz, char* ws, cudaStream_t s) {
+    if (g.xtiles && g.h_xtile0) {
+        const int64_t t0 = g.h_xtile0[blk0], n = g.h_xtile0[blk0 + nblk] - t0;
+        if (n > 0) k_gemm_x<<<dim3((unsigned)n, 1, nz), 256, 0, s>>>(g, P, nao, blk0, ws, src0, dst0, t0);
+        return;
+    }
     dim3 grid((max_nbp + GX_BM - 1) / GX_BM, nblk, nz);
-    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, src0, dst0);
+    k_gemm_x<<<grid, 256, 0, s>>>(g, P, nao, blk0, ws, src0, dst0, 0);
 }
 
 void launch_ao_eval_rad(const BasisView& b, const GridView& g, int blk0, int nblk, char* ws, cudaStream_t s) {
@@ -696,8 +710,13 @@ void launch_gemm_v(const GridView& g, int blk0, int nblk, int max_nbp, bool gga,
 void launch_gemm_v_plane(const GridView& g, int blk0, int nblk, int max_nbp, int zplane, char* ws, double* Vacc,
                          int nao, cudaStream_t s) {
     const int tiles = (max_nbp + GV_B - 1) / GV_B;
+    if (g.vtiles && g.h_vtile0) {
+        const int64_t t0 = g.h_vtile0[blk0], n = g.h_vtile0[blk0 + nblk] - t0;
+        if (n > 0) k_gemm_v<<<(unsigned)n, 128, 0, s>>>(g, blk0, ws, zplane, Vacc, nao, tiles, t0);
+        return;
+    }
     dim3 grid(tiles * tiles, nblk);
-    k_gemm_v<<<grid, 128, 0, s>>>(g, blk0, ws, zplane, Vacc, nao, tiles);
+    k_gemm_v<<<grid, 128, 0, s>>>(g, blk0, ws, zplane, Vacc, nao, tiles, 0);
 }
 
 void launch_rho_functional_uks(const GridView& g, int blk0, int nblk, int fn, bool incremental, double rho_cut,

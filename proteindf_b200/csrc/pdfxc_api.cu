@@ -184,7 +184,9 @@ pdfxc::BasisView basis_view(const pdfxc_ctx* c) {
 
 pdfxc::GridView grid_view(const pdfxc_ctx* c) {
     return {c->d_px,         c->d_py,         c->d_pz,          c->d_pw,         c->d_meta,
-            c->d_blk_shells, c->d_blk_shell_row, c->d_blk_aos, c->d_blk_row_info, c->d_blk_row_geom};
+            c->d_blk_shells, c->d_blk_shell_row, c->d_blk_aos, c->d_blk_row_info, c->d_blk_row_geom,
+            c->d_xtiles,     c->d_vtiles,        c->h_xtile0.empty() ? nullptr : c->h_xtile0.data(),
+            c->h_vtile0.empty() ? nullptr : c->h_vtile0.data()};
 }
 
 void drop_graph(pdfxc_ctx* c) {
@@ -261,6 +263,8 @@ void free_grid(pdfxc_ctx* c) {
     dev_free(c->d_owner), dev_free(c->d_ao_atom), dev_free(c->d_grad);
     dev_free(c->d_fdens), dev_free(c->d_wslot), dev_free(c->d_brad), dev_free(c->d_pair);
     dev_free(c->d_wscratch);
+    dev_free(c->d_xtiles), dev_free(c->d_vtiles);
+    c->h_xtile0.clear(), c->h_vtile0.clear();
     free_plan(c->gplan);
     free_plan(c->uplan);
     dev_free(c->d_rho_b), dev_free(c->d_blk_sum_b);
@@ -842,6 +846,20 @@ void build_grid(pdfxc_ctx* ctx, int64_t npts, const double* xyzw, const int* ato
         upload(&ctx->d_blk_row_geom, geom, s);
     }
     upload(&ctx->d_seg_blk, ctx->seg_blk, s);
+    {  // the FP64 contractions' tile lists (64-AO tiles of each block's nbp rows)
+        std::vector<int2> xt, vt;
+        ctx->h_xtile0.assign(1, 0), ctx->h_vtile0.assign(1, 0);
+        for (int b = 0; b < nblk; ++b) {
+            const int nt = (ctx->h_meta[b].nbp + 63) / 64;
+            for (int i = 0; i < nt; ++i) xt.push_back(make_int2(b, i));
+            for (int i = 0; i < nt; ++i)
+                for (int j = 0; j < nt; ++j) vt.push_back(make_int2(b, (i << 16) | j));
+            ctx->h_xtile0.push_back((int64_t)xt.size());
+            ctx->h_vtile0.push_back((int64_t)vt.size());
+        }
+        upload(&ctx->d_xtiles, xt, s);
+        upload(&ctx->d_vtiles, vt, s);
+    }
     ctx->h_grp.assign(grp_blk.begin(), grp_blk.end() - 1);
     upload(&ctx->d_grp, ctx->h_grp, s);
     if (mixed && ctx->opt.split_terms == 10) {

@@ -60,6 +60,14 @@ struct GridView {
     const int* blk_aos;        // global AO index of each local row
     const int* blk_row_info;   // per local row: 16 * (shell slot in the block's list) + L^2 + component
     const struct RowGeom* blk_row_geom;  // per local row: its shell's atom and blk_row_info (INT8 path)
+    // The FP64 contractions' tiles, so that a launch has no idle CTAs: {block, 64-row M tile} for
+    // X = P_sub phi, {block, M << 16 | N} (64 x 64 tiles) for Vacc += phi Z^T, block by block; and
+    // each block's first tile (prefix sums, host memory: read by the launchers, not the kernels).
+    // Null (the no-allocation build): the launch covers max_nbp tiles per block, surplus CTAs exit.
+    const int2* xtiles;
+    const int2* vtiles;
+    const int64_t* h_xtile0;
+    const int64_t* h_vtile0;
 };
 
 // One AO row of a block's screened basis: the atom of its shell and its blk_row_info entry.
@@ -180,6 +188,8 @@ struct pdfxc_ctx {
     double* d_brad = nullptr;   // [natom]
     double* d_pair = nullptr;   // [2 * natom^2] Becke pair constants
     double* d_wscratch = nullptr;  // weight-term atom rows in device memory (above 400 atoms)
+    int2 *d_xtiles = nullptr, *d_vtiles = nullptr;  // GridView::xtiles, vtiles
+    std::vector<int64_t> h_xtile0, h_vtile0;         // GridView::h_xtile0, h_vtile0 (nblk + 1 each)
 
     // open-shell build (pdfxc_build_vxc_uks): beta-spin buffers beside the alpha ones above
     pdfxc::Plan uplan;
