@@ -594,8 +594,8 @@ __device__ __forceinline__ double warp_max_d(double v) {
 // to four blocks). Pass 1: the radial sums S0, S1 of every shell of the group's basis at the
 // thread's point (stored for the later stages) and the point's exponent of phi^T rows (the
 // max over the AOs: max_c |A_c S0| = |S0| max_c |A_c|, the rounding being monotone). Pass 2,
-// per tile of 16 AO rows: every thread forms phi of its point shell by shell from S0 and cuts
-// its 16 digits with the point's scale (one 16-byte store per digit plane). These are the only
+// per tile of 16 AO rows: every thread forms phi of its point row by row from S0 and cuts its
+// 16 digits with the point's scale (one 16-byte store per digit plane). These are the only
 // phi digits: the Vxc contraction reads them as an MN-major operand and takes the point scale
 // into Z' = 2^e_pt Z.
 constexpr int kGroupPts = 4 * BLOCK_PTS;
@@ -696,40 +696,20 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_phi_group(BasisView bas, GridV
     oz_prefetch_rows<false>(rg, 0, m, rad, q);
     for (int mu0 = 0; mu0 < m.nbp; mu0 += 16) {
         if (mu0 + 16 < m.nb) oz_prefetch_rows<false>(rg + mu0 + 16, mu0 + 16, m, rad, q);  // the next tile's S0
-        // shell by shell over the tile's rows (uniform over the CTA), phi = A S0
-        double v[16];
-        int r = 0;
-        while (r < 16) {
-            if (mu0 + r >= m.nb) {
-                v[r] = 0.0;
-                ++r;
-                continue;
-            }
-            const RowGeom gq = rg[mu0 + r];
-            const int t = gq.info & 15, slot = gq.info >> 4;
-            const int Lq = t == 0 ? 0 : (t < 4 ? 1 : 2);
-            const int u0 = t - Lq * Lq;                 // the component of row r
-            const int n = min(2 * Lq + 1 - u0, 16 - r);  // the shell's rows in this tile from r
-            const double S0 = rad[(size_t)slot * BLOCK_PTS + q];
-            const double x = rx - gq.ax, y = ry - gq.ay, z = rz - gq.az;
-            double pc[5];
-            if (Lq == 0) {
-                pc[0] = S0;
-            } else if (Lq == 1) {
-                pc[0] = x * S0, pc[1] = y * S0, pc[2] = z * S0;
-            } else {  // the products of ang_poly1
-                const double s3 = 0.57735026918962576451;  // 1/sqrt(3)
-                pc[0] = (x * y) * S0, pc[1] = (z * x) * S0, pc[2] = (y * z) * S0;
-                pc[3] = (0.5 * (x * x - y * y)) * S0, pc[4] = (s3 * (z * z - 0.5 * (x * x + y * y))) * S0;
-            }
-#pragma unroll
-            for (int k = 0; k < 5; ++k)
-                if (k >= u0 && k < u0 + n) v[r + k - u0] = pc[k];
-            r += n;
-        }
+        // row by row (uniform over the CTA; the rows of one shell read the same S0 from L1), phi = A S0,
+        // cut at once: the tile's 16 values stay in registers
         uint32_t w[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) w[j] = oz_word(v[j], sc);
+        for (int r = 0; r < 16; ++r) {
+            double v = 0.0;
+            if (mu0 + r < m.nb) {
+                const RowGeom gq = rg[mu0 + r];
+                double A, Ax, Ay, Az;
+                ang_poly1(gq.info & 15, rx - gq.ax, ry - gq.ay, rz - gq.az, A, Ax, Ay, Az);
+                v = A * rad[(size_t)(gq.info >> 4) * BLOCK_PTS + q];
+            }
+            w[r] = oz_word(v, sc);
+        }
         oz_store16_words(base + L.phi1, kOzPlanesA, oz_off_a(q, mu0, m.nbp), w);
     }
 }
