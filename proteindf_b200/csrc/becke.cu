@@ -16,6 +16,8 @@
 // the same order) bit for bit, and the weight screen keeps the same points.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "pdfxc_internal.cuh"
 
 namespace pdfxc {
@@ -94,47 +96,6 @@ __global__ void k_becke_pairs(const double* __restrict__ atom_xyz, const double*
             a = a < -0.5 ? -0.5 : (a > 0.5 ? 0.5 : a);
         }
         adj[e] = a;
-    }
-}
-
-// Same weights as k_becke, with each thread's point-atom distances kept in
-// shared memory ([atom][thread]) and the pair constants read from the table:
-// one multiply per pair instead of two square roots and a division.
-constexpr int BECKE_T = 64;
-__global__ void __launch_bounds__(BECKE_T) k_becke_tab(const double* __restrict__ atom_xyz, int natom,
-                                                       const double* __restrict__ inv, const double* __restrict__ adj,
-                                                       int64_t npts, const double* __restrict__ xyz,
-                                                       const int* __restrict__ owner,
-                                                       const double* __restrict__ w_single, double* __restrict__ w_out) {
-    extern __shared__ double rr[];  // [natom][BECKE_T]
-    const int t = threadIdx.x;
-    for (int64_t i0 = blockIdx.x * (int64_t)BECKE_T; i0 < npts; i0 += (int64_t)gridDim.x * BECKE_T) {
-        const int64_t i = i0 + t;
-        const bool live = i < npts;
-        const double rx = live ? xyz[3 * i] : 0.0, ry = live ? xyz[3 * i + 1] : 0.0, rz = live ? xyz[3 * i + 2] : 0.0;
-        for (int m = 0; m < natom; ++m) {
-            const double ax = atom_xyz[3 * m] - rx, ay = atom_xyz[3 * m + 1] - ry, az = atom_xyz[3 * m + 2] - rz;
-            rr[m * BECKE_T + t] = sqrt(ax * ax + ay * ay + az * az);
-        }
-        if (live) {
-            const int own = owner[i];
-            double tot = 0.0, pown = 0.0;
-            for (int m = 0; m < natom; ++m) {
-                const double rm = rr[m * BECKE_T + t];
-                const double* im = inv + (size_t)m * natom;
-                const double* am = adj + (size_t)m * natom;
-                double p = 1.0;
-                for (int n = 0; n < natom && p != 0.0; ++n) {
-                    if (n == m) continue;
-                    double u = (rm - rr[n * BECKE_T + t]) * __ldg(im + n);
-                    u = u + __ldg(am + n) * (1.0 - u * u);
-                    p *= becke_s(u);
-                }
-                tot += p;
-                if (m == own) pown = p;
-            }
-            w_out[i] = w_single[i] * (pown / tot);
-        }
     }
 }
 
@@ -224,20 +185,82 @@ void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, i
     k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, nullptr, natom, size_adjust, inv, adj);
 }
 
-void launch_becke_tab(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
-                      double* inv, double* adj, int64_t npts, const double* xyz, const int* owner,
-                      const double* w_single, double* w_out, cudaStream_t s) {
-    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, ghost, natom, size_adjust, inv, adj);
-    int64_t blocks = (npts + BECKE_T - 1) / BECKE_T;
-    if (blocks > 148 * 32) blocks = 148 * 32;
-    if (blocks < 1) blocks = 1;
-    const size_t smem = sizeof(double) * BECKE_T * natom;
-    cudaFuncSetAttribute(k_becke_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_becke_tab<<<(unsigned)blocks, BECKE_T, smem, s>>>(atom_xyz, natom, inv, adj, npts, xyz, owner, w_single,
-                                                        w_out);
+// The weights of k_becke with the pair constants from the table (one multiply per pair instead of
+// two square roots and a division) and a warp per point: lane l forms P_m for m = l, l + 32, ...
+// with the factors in ascending partner order, and lane 0 sums the P_m in ascending m, the
+// operations and order of k_becke. The pair constants are read from the transposed table
+// (invT[n][m] = inv[m][n], adjT[n][m] = adj[m][n]), so that the lanes' loads for one partner n
+// are consecutive; per warp, the point's distances and the P_m sit in shared memory, 16 bytes
+// per atom. (A first table form kept one point per thread, with that point's natom distances
+// per thread in shared memory: a few warps per SM, twice the time on the 100-atom chain.)
+constexpr int BECKE_WW = 8;  // warps per CTA
+__global__ void __launch_bounds__(32 * BECKE_WW) k_becke_warp(const double* __restrict__ atom_xyz, int natom,
+                                                              const double* __restrict__ invT,
+                                                              const double* __restrict__ adjT, int64_t npts,
+                                                              const double* __restrict__ xyz,
+                                                              const int* __restrict__ owner,
+                                                              const double* __restrict__ w_single,
+                                                              double* __restrict__ w_out) {
+    extern __shared__ double smw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double* rr = smw + (size_t)warp * 2 * natom;  // [natom]: |r - R_m|
+    double* ps = rr + natom;                      // [natom]: P_m(r)
+    for (int64_t i = blockIdx.x * (int64_t)BECKE_WW + warp; i < npts; i += (int64_t)gridDim.x * BECKE_WW) {
+        const double rx = xyz[3 * i], ry = xyz[3 * i + 1], rz = xyz[3 * i + 2];
+        for (int m = lane; m < natom; m += 32) {
+            const double ax = atom_xyz[3 * m] - rx, ay = atom_xyz[3 * m + 1] - ry, az = atom_xyz[3 * m + 2] - rz;
+            rr[m] = sqrt(ax * ax + ay * ay + az * az);
+        }
+        __syncwarp();
+        for (int m = lane; m < natom; m += 32) {
+            const double rm = rr[m];
+            double p = 1.0;
+            for (int n = 0; n < natom && p != 0.0; ++n) {
+                if (n == m) continue;
+                double u = (rm - rr[n]) * __ldg(invT + (size_t)n * natom + m);
+                u = u + __ldg(adjT + (size_t)n * natom + m) * (1.0 - u * u);
+                p *= becke_s(u);
+            }
+            ps[m] = p;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            double tot = 0.0;
+            for (int m = 0; m < natom; ++m) tot += ps[m];
+            w_out[i] = w_single[i] * (ps[owner[i]] / tot);
+        }
+        __syncwarp();  // rr and ps are rewritten for the next point
+    }
 }
 
-size_t becke_tab_max_atoms() { return (200u * 1024u) / (sizeof(double) * BECKE_T); }
+__global__ void k_transpose_n2(const double* __restrict__ a, double* __restrict__ at, int n) {
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * n;
+         e += (int64_t)gridDim.x * blockDim.x) {
+        const int r = (int)(e / n), c = (int)(e % n);
+        at[(int64_t)c * n + r] = a[e];
+    }
+}
+
+size_t becke_warp_max_atoms() { return (200u * 1024u) / (2 * sizeof(double) * BECKE_WW); }
+
+// tab: 4 n_atom^2 doubles (the pair table, then its transpose)
+void launch_becke_warp(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
+                       double* tab, int64_t npts, const double* xyz, const int* owner, const double* w_single,
+                       double* w_out, cudaStream_t s) {
+    const size_t n2 = (size_t)natom * natom;
+    double *inv = tab, *adj = tab + n2, *invT = tab + 2 * n2, *adjT = tab + 3 * n2;
+    k_becke_pairs<<<(unsigned)((n2 + 255) / 256), 256, 0, s>>>(atom_xyz, brad, ghost, natom, size_adjust, inv, adj);
+    const unsigned tb = (unsigned)std::min<size_t>((n2 + 255) / 256, 148 * 8);
+    k_transpose_n2<<<tb, 256, 0, s>>>(inv, invT, natom);
+    k_transpose_n2<<<tb, 256, 0, s>>>(adj, adjT, natom);
+    int64_t blocks = (npts + BECKE_WW - 1) / BECKE_WW;
+    if (blocks > 148 * 64) blocks = 148 * 64;
+    if (blocks < 1) blocks = 1;
+    const size_t smem = 2 * sizeof(double) * BECKE_WW * natom;
+    cudaFuncSetAttribute(k_becke_warp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_becke_warp<<<(unsigned)blocks, 32 * BECKE_WW, smem, s>>>(atom_xyz, natom, invT, adjT, npts, xyz, owner, w_single,
+                                                               w_out);
+}
 
 void launch_becke(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
                   int64_t npts, const double* xyz, const int* owner, const double* w_single, double* w_out,

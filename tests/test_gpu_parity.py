@@ -90,7 +90,7 @@ def test_becke_vs_reference(water2):
 def test_becke_equals_oracle_bit_for_bit():
     """The device's Becke weights (compiled without fused multiply-adds) equal the CPU
     restatement's bit for bit, so both sides keep the same points under the 1e-16 weight screen;
-    a 30-atom chain on a USER 40 x 110 grid, table form."""
+    a 30-atom chain on a USER 40 x 110 grid, the warp-per-point table form."""
     from oracle import oracle
     from proteindf_b200 import basis, grids, systems
     from proteindf_b200.xc import XcEngine
