@@ -99,6 +99,48 @@ __global__ void k_becke_pairs(const double* __restrict__ atom_xyz, const double*
     }
 }
 
+// Same weights as k_becke, one point per thread, with each thread's point-atom distances kept in
+// shared memory ([atom][thread]) and the pair constants read from the table: one multiply per
+// pair instead of two square roots and a division. Its shared memory per CTA grows with the atom
+// count, so it is the form for small molecules (becke_small_atoms), k_becke_warp the one above.
+constexpr int BECKE_T = 64;
+__global__ void __launch_bounds__(BECKE_T) k_becke_tab(const double* __restrict__ atom_xyz, int natom,
+                                                       const double* __restrict__ inv, const double* __restrict__ adj,
+                                                       int64_t npts, const double* __restrict__ xyz,
+                                                       const int* __restrict__ owner,
+                                                       const double* __restrict__ w_single, double* __restrict__ w_out) {
+    extern __shared__ double rr[];  // [natom][BECKE_T]
+    const int t = threadIdx.x;
+    for (int64_t i0 = blockIdx.x * (int64_t)BECKE_T; i0 < npts; i0 += (int64_t)gridDim.x * BECKE_T) {
+        const int64_t i = i0 + t;
+        const bool live = i < npts;
+        const double rx = live ? xyz[3 * i] : 0.0, ry = live ? xyz[3 * i + 1] : 0.0, rz = live ? xyz[3 * i + 2] : 0.0;
+        for (int m = 0; m < natom; ++m) {
+            const double ax = atom_xyz[3 * m] - rx, ay = atom_xyz[3 * m + 1] - ry, az = atom_xyz[3 * m + 2] - rz;
+            rr[m * BECKE_T + t] = sqrt(ax * ax + ay * ay + az * az);
+        }
+        if (live) {
+            const int own = owner[i];
+            double tot = 0.0, pown = 0.0;
+            for (int m = 0; m < natom; ++m) {
+                const double rm = rr[m * BECKE_T + t];
+                const double* im = inv + (size_t)m * natom;
+                const double* am = adj + (size_t)m * natom;
+                double p = 1.0;
+                for (int n = 0; n < natom && p != 0.0; ++n) {
+                    if (n == m) continue;
+                    double u = (rm - rr[n * BECKE_T + t]) * __ldg(im + n);
+                    u = u + __ldg(am + n) * (1.0 - u * u);
+                    p *= becke_s(u);
+                }
+                tot += p;
+                if (m == own) pown = p;
+            }
+            w_out[i] = w_single[i] * (pown / tot);
+        }
+    }
+}
+
 // Stratmann-Scuseria partition (DfGenerateGrid::calcMultiCenterWeight_SS,
 // src/libpdf/DfGenerateGrid.cpp:1878-1956): s = (1 - g(mu))/2 with g the
 // piecewise polynomial of a = 0.64, no size adjustment. s is exactly 0 for
@@ -191,8 +233,8 @@ void launch_becke_pairs(const double* atom_xyz, const double* brad, int natom, i
 // operations and order of k_becke. The pair constants are read from the transposed table
 // (invT[n][m] = inv[m][n], adjT[n][m] = adj[m][n]), so that the lanes' loads for one partner n
 // are consecutive; per warp, the point's distances and the P_m sit in shared memory, 16 bytes
-// per atom. (A first table form kept one point per thread, with that point's natom distances
-// per thread in shared memory: a few warps per SM, twice the time on the 100-atom chain.)
+// per atom. (k_becke_tab keeps one point per thread, with that point's natom distances per thread
+// in shared memory: at 100 atoms a few warps per SM and twice this kernel's time.)
 constexpr int BECKE_WW = 8;  // warps per CTA
 __global__ void __launch_bounds__(32 * BECKE_WW) k_becke_warp(const double* __restrict__ atom_xyz, int natom,
                                                               const double* __restrict__ invT,
@@ -240,6 +282,25 @@ __global__ void k_transpose_n2(const double* __restrict__ a, double* __restrict_
         at[(int64_t)c * n + r] = a[e];
     }
 }
+
+void launch_becke_tab(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
+                      double* inv, double* adj, int64_t npts, const double* xyz, const int* owner,
+                      const double* w_single, double* w_out, cudaStream_t s) {
+    k_becke_pairs<<<(natom * natom + 255) / 256, 256, 0, s>>>(atom_xyz, brad, ghost, natom, size_adjust, inv, adj);
+    int64_t blocks = (npts + BECKE_T - 1) / BECKE_T;
+    if (blocks > 148 * 32) blocks = 148 * 32;
+    if (blocks < 1) blocks = 1;
+    const size_t smem = sizeof(double) * BECKE_T * natom;
+    cudaFuncSetAttribute(k_becke_tab, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_becke_tab<<<(unsigned)blocks, BECKE_T, smem, s>>>(atom_xyz, natom, inv, adj, npts, xyz, owner, w_single,
+                                                        w_out);
+}
+
+// Up to this many atoms the one-point-per-thread form; above it the warp form. Measured on seeded
+// chains with USER 75 x 302 grids (ncu durations, table form / warp form): 20 atoms 0.28 / 0.48 ms,
+// 32 atoms 1.07 / 1.15 ms, 48 atoms 4.57 / 4.66 ms, 64 atoms 15.8 / 8.2 ms, 100 atoms 77 / 39 ms.
+constexpr int kBeckeSmallAtoms = 48;
+size_t becke_small_atoms() { return kBeckeSmallAtoms; }
 
 size_t becke_warp_max_atoms() { return (200u * 1024u) / (2 * sizeof(double) * BECKE_WW); }
 

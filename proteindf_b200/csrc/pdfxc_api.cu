@@ -973,6 +973,10 @@ void partition_weights_device(pdfxc_ctx* ctx, bool ss, int64_t npts, const doubl
             dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
             pdfxc::launch_ss(ctx->d_atom_xyz, ctx->natom, d_pair, d_pair + (size_t)ctx->natom * ctx->natom,
                              ctx->d_nbr_idx, ctx->d_nbr_dist, npts, d_xyz, d_own, d_ws, d_wo, s);
+        } else if ((size_t)ctx->natom <= pdfxc::becke_small_atoms()) {
+            dev_alloc(&d_pair, 2 * (size_t)ctx->natom * ctx->natom);
+            pdfxc::launch_becke_tab(ctx->d_atom_xyz, d_br, ctx->d_ghost, ctx->natom, size_adjust, d_pair,
+                                    d_pair + (size_t)ctx->natom * ctx->natom, npts, d_xyz, d_own, d_ws, d_wo, s);
         } else if ((size_t)ctx->natom <= pdfxc::becke_warp_max_atoms()) {
             dev_alloc(&d_pair, 4 * (size_t)ctx->natom * ctx->natom);
             pdfxc::launch_becke_warp(ctx->d_atom_xyz, d_br, ctx->d_ghost, ctx->natom, size_adjust, d_pair, npts, d_xyz,

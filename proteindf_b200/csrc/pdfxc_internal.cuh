@@ -295,6 +295,12 @@ void launch_becke(const double* atom_xyz, const double* brad, const int* ghost, 
                   int64_t npts, const double* xyz, const int* owner, const double* w_single,
                   double* w_out, cudaStream_t s);
 size_t becke_max_atoms();
+// the table form, one point per thread (pair constants in inv/adj, n_atom^2 doubles each), for
+// n_atom <= becke_small_atoms()
+void launch_becke_tab(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
+                      double* inv, double* adj, int64_t npts, const double* xyz, const int* owner,
+                      const double* w_single, double* w_out, cudaStream_t s);
+size_t becke_small_atoms();
 // the same weights with a warp per point (lanes over the atoms); tab: 4 n_atom^2 doubles
 void launch_becke_warp(const double* atom_xyz, const double* brad, const int* ghost, int natom, int size_adjust,
                        double* tab, int64_t npts, const double* xyz, const int* owner, const double* w_single,
