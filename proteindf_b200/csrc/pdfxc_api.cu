@@ -9,6 +9,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <exception>
 #include <map>
 #include <mutex>
 #include <new>
@@ -145,9 +146,18 @@ void parallel_ranges(int64_t n, int64_t min_per_thread, F&& fn) {
         return;
     }
     std::vector<std::thread> th;
+    std::vector<std::exception_ptr> err(nt);  // an exception of a range is rethrown on the calling thread
     for (int64_t t = 0; t < nt; ++t)
-        th.emplace_back([&, t]() { fn(n * t / nt, n * (t + 1) / nt, (int)t); });
+        th.emplace_back([&, t]() {
+            try {
+                fn(n * t / nt, n * (t + 1) / nt, (int)t);
+            } catch (...) {
+                err[t] = std::current_exception();
+            }
+        });
     for (auto& x : th) x.join();
+    for (auto& e : err)
+        if (e) std::rethrow_exception(e);
 }
 
 // std::sort's result (a total order: the keys are distinct) from sorted ranges merged pairwise,
