@@ -908,11 +908,13 @@ __global__ void __launch_bounds__(kGroupPts, 2) k_pack_z_group(GridView g, const
 // M tile of Z', B = the phi^T digits of the N tile's 64 AOs over the slab's 64 points, read
 // MN-major (1 KiB per plane and 16-AO group, one 4-D tensor copy per stage).
 constexpr int OZ_NT = 64;
-// operand ring stages: the Vxc contraction (K = a group's 512 points, eight slabs per item) keeps
-// three in flight, the rho contraction (K = nbp) two beside its larger radial-sum staging
+// operand ring stages: three in flight for both contractions (the Vxc contraction: K = a group's
+// 512 points, eight slabs per item, three stages unless the autotuner picks two; the rho contraction:
+// K = nbp, three stages beside its radial-sum staging of kOzRsCap = 8 shells per column half, 1 %
+// faster on the 2000-atom chain than two stages beside 12 shells)
 template <int MODE>
 constexpr int oz_stages() {
-    return MODE == MODE_VXC ? 3 : 2;
+    return 3;
 }
 constexpr uint32_t OZ_A_BYTES = OZ_SLICES * umma::I8_SLAB_BYTES;   // 32 KiB
 constexpr uint32_t OZ_B_SLICE = OZ_NT * umma::I8_SLAB_K;          // 4 KiB
@@ -923,9 +925,9 @@ constexpr int OZ_THREADS = 64 + 32 * OZ_EPI_WARPS;  // copies, MMAs, epilogue
 // Epilogue region after the ring, a quarter per (group, column half). RHO: the radial sums of
 // up to kOzRsCap shells of the half's columns, staged per thread. VXC: the half's [128][17]
 // FP64 transpose tile.
-constexpr int kOzRsCap = 12;
+constexpr int kOzRsCap = 8;
 template <int MODE>
-constexpr uint32_t oz_epi_bytes() {  // rho: 96 KiB of staged radial sums; Vxc: four 17 KiB tiles
+constexpr uint32_t oz_epi_bytes() {  // rho: 64 KiB of staged radial sums; Vxc: four 17 KiB tiles
     return MODE == MODE_RHO ? 4u * kOzRsCap * 2 * BLOCK_PTS * 8 : 4u * 128 * 17 * 8;
 }
 template <int MODE, int S>
