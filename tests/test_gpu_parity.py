@@ -106,6 +106,24 @@ def test_becke_equals_oracle_bit_for_bit():
     eng.close()
 
 
+def test_becke_warp_form_equals_oracle_bit_for_bit():
+    """Above 48 atoms the Becke weights come from the warp-per-point kernel (its lanes over the
+    atoms); they equal the CPU restatement's bit for bit too: a 56-atom chain on a USER 20 x 50 grid."""
+    from oracle import oracle
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    syms, xyz = systems.peptide_chain(56, seed=7)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ"))
+    P, W, A = grids.molecular_grid(xyz, sh.atom_z, nrad=20, nang=50, radial="GC", mapping="TA", pruning=True)
+    brad = np.array([grids.BECKE_RADIUS[int(z)] for z in sh.atom_z])
+    eng = XcEngine()
+    eng.set_system(sh)
+    w = eng.becke_weights(P, A, W, brad)
+    ref = W * oracle.becke(xyz, brad, P, A)
+    assert np.array_equal(w, ref), np.abs(w - ref).max()
+    eng.close()
+
+
 def test_becke_dummy_atom_vs_reference():
     """A dummy atom (atomic number 0) is left out of the partition products, as the reference's
     Ps_uij does (src/libpdf/DfGenerateGrid.cpp:2056); equal to the oracle bit for bit."""
