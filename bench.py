@@ -27,7 +27,9 @@ count appended. A step is the rank's build (library CUDA events) plus the
 all-reduce (CUDA events on torch's stream), max over ranks; value = the chain's
 points / that time (strong scaling: the total work is fixed).
 
-The same line (N = 1, unless --no-large) carries the two large configurations,
+The same line (N = 1, unless --no-large) carries the adjoint on the differentiation
+configuration (a 30-atom chain, PBE: forward and backward host-API times) and the two
+large configurations,
 each built with the FP64 drop-in and the INT8 path, their speed-up and |dExc|:
   chain2000  one 2000-atom chain, cc-pVDZ (~18,600 AOs), B3LYP, USER 75x302 grid with
              Stratmann-Scuseria weights, AO cut-off 1e-10
@@ -424,6 +426,7 @@ def main():
         torch.cuda.empty_cache()
         for name in ("chain2000", "batch64"):
             line[name] = large_workload(args, name, flush)
+        line["adjoint"] = adjoint_workload()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -519,6 +522,37 @@ def run_shard(args):
         print(json.dumps(line), flush=True)
     eng.close()
     dist.destroy_process_group()
+
+
+def adjoint_workload(reps=3):
+    """The differentiation configuration: a 30-atom chain (seed 21), the 6-31G*-shaped cc-pVDZ
+    without hydrogen p shells, PBE, USER 75x302 grid with Becke weights. Host-API wall time (the calls
+    synchronise) of the forward build and of pdfxc_xc_backward (dExc/dP, the AO-centre and the
+    Becke-weight gradient terms), best of `reps` after a warm-up, on one GPU."""
+    from proteindf_b200 import basis, grids, systems
+    from proteindf_b200.xc import XcEngine
+    syms, xyz = systems.peptide_chain(30, seed=21)
+    sh = basis.ShellTable(syms, xyz, basis.load_basis("cc-pVDZ-noHp"))
+    P, W, A = grids.molecular_grid(xyz, sh.atom_z, **grids.PRESETS["USER-75x302"])
+    brad = np.array([grids.BECKE_RADIUS[int(z)] for z in sh.atom_z])
+    PA = 0.5 * systems.density_matrix(sh.nao, 60, seed=22)
+    eng = XcEngine(device=0)
+    eng.set_system(sh)
+    eng.set_grid(np.c_[P, eng.becke_weights(P, A, W, brad)], A)
+    fwd, bwd = [], []
+    for k in range(reps + 1):
+        t0 = time.perf_counter()
+        exc, _, V = eng.build_vxc("PBE", PA)
+        t1 = time.perf_counter()
+        dP, go, gw, e2 = eng.xc_backward("PBE", PA, w_single=W, becke_radius=brad)
+        t2 = time.perf_counter()
+        if k:
+            fwd.append(t1 - t0), bwd.append(t2 - t1)
+    eng.close()
+    return {"workload": "30-atom peptide-like chain (seed 21), cc-pVDZ without H p shells, PBE, USER 75x302, "
+                        "Becke weights", "atoms": 30, "n_ao": int(sh.nao), "grid_points": int(len(P)),
+            "forward_ms": 1e3 * min(fwd), "backward_ms": 1e3 * min(bwd),
+            "max_abs_dexc_dP_minus_vxc": float(np.abs(dP - V).max()), "timing": "host API wall time"}
 
 
 def large_workload(args, name, flush):
